@@ -1,0 +1,78 @@
+/*
+ * vidstab_b200_ext.h -- entry points of libvidstab_b200 without a
+ * counterpart in the reference library.  All take plain pointers and sizes;
+ * "device" pointers are CUDA device addresses on the detector's GPU.
+ */
+#ifndef VIDSTAB_B200_EXT_H
+#define VIDSTAB_B200_EXT_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+struct _vsmotiondetect;
+struct vsvector_;
+
+/* Message of the last GPU-side failure on this thread ("" if none). */
+VS_API const char* vsb_last_error(void);
+
+/* Number of CUDA devices visible to the process. */
+VS_API int vsb_device_count(void);
+
+/* sizeof of the public structs as compiled into the library (ABI checks). */
+VS_API int vsb_sizeof(const char* type_name);
+
+/* vsMotionDetection with plane 0 already in device memory (e.g. decoded on
+   the GPU): same results, no host-to-device copy of the frame.  Planar
+   formats read the luma plane, packed formats the interleaved plane;
+   pitch is in bytes.  The `show` overlay is not drawn (no host frame). */
+VS_API int vsb_motion_detection_device(struct _vsmotiondetect* md, struct vsvector_* motions,
+                                       const uint8_t* d_plane0, int pitch);
+
+/* Kernel launches issued for this detector so far. */
+VS_API long vsb_launch_count(const struct _vsmotiondetect* md);
+
+/* Runs the detect API over a clip, frame by frame, the way a host filter
+   does: vsMotionDetectInit, vsMotionDetection per frame (frame k's plane 0
+   at frames + k*frame_bytes, row distance linesize; or, with on_device,
+   device memory read through vsb_motion_detection_device), then cleanup.
+   Every frame's motions are appended to `out` (up to out_cap records) and
+   counts[k] receives their number.  If trf_path is not NULL the .trf file is
+   written as vidstabdetect writes it.  *elapsed receives the wall time of the
+   per-frame loop.  Returns the number of records, or -1. */
+VS_API long vsb_detect_clip(int width, int height, int pformat, const uint8_t* frames,
+                            long frame_bytes, int linesize, int nframes, int on_device,
+                            int stepSize, int accuracy, int shakiness, double mincontrast,
+                            int tripod, int show, int serializationMode, const char* trf_path,
+                            void* out, long out_cap, int* counts, double* elapsed,
+                            uint8_t* show_out);
+
+/* ---- kernel-level entry points (host buffers in and out; for testing) ---- */
+
+/* luma prefilter of one W x H plane (tight rows) with box size `size`
+   (already clamped; < 2 copies) */
+VS_API int vsb_boxblur_host(uint8_t* dst, const uint8_t* src, int width, int height, int size);
+
+/* per-field, per-channel 8-bit (min,max) of an interleaved image with bpp
+   bytes per pixel: out[(i*channels+c)*2 + {0,1}] */
+VS_API int vsb_field_minmax_host(const uint8_t* img, int width, int height, int bpp,
+                                 int channels, const int16_t* x, const int16_t* y, int n,
+                                 int size, uint8_t* out);
+
+/* planar field search exactly as vsMotionDetection runs it for one field
+   set: spiral lattice of the given step within maxShift plus refinement, for
+   n fields with centres (x,y) and lattice offsets (ox,oy).  Writes per field
+   {sad, tx, ty, ok}; tx,ty relative to the offset.  tiles > 0 forces the
+   number of CTAs per field. */
+VS_API int vsb_field_search_host(const uint8_t* curr, const uint8_t* prev, int width,
+                                 int height, int size, int maxShift, int stepSize, int packed_bpp,
+                                 const int16_t* x, const int16_t* y, const int16_t* ox,
+                                 const int16_t* oy, int n, int tiles, uint32_t* sad,
+                                 int16_t* tx, int16_t* ty, int32_t* ok);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

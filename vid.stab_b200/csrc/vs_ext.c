@@ -1,0 +1,170 @@
+/*
+ * vs_ext.c -- entry points without a counterpart in the reference
+ * (declared in vidstab_b200_ext.h).
+ */
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+
+#include "vidstab_b200.h"
+#include "vsb_host.h"
+
+const char* vsb_last_error(void) { return vsbd_error(); }
+
+int vsb_device_count(void) { return vsbd_device_count(); }
+
+int vsb_sizeof(const char* t) {
+  if (!t) return -1;
+  if (!strcmp(t, "VSMotionDetect")) return (int)sizeof(VSMotionDetect);
+  if (!strcmp(t, "VSMotionDetectConfig")) return (int)sizeof(VSMotionDetectConfig);
+  if (!strcmp(t, "VSMotionDetectFields")) return (int)sizeof(VSMotionDetectFields);
+  if (!strcmp(t, "VSFrameInfo")) return (int)sizeof(VSFrameInfo);
+  if (!strcmp(t, "VSFrame")) return (int)sizeof(VSFrame);
+  if (!strcmp(t, "VSTransform")) return (int)sizeof(VSTransform);
+  if (!strcmp(t, "LocalMotion")) return (int)sizeof(LocalMotion);
+  if (!strcmp(t, "VSVector")) return (int)sizeof(VSVector);
+  if (!strcmp(t, "Field")) return (int)sizeof(Field);
+  if (!strcmp(t, "PreparedTransform")) return (int)sizeof(PreparedTransform);
+  return -1;
+}
+
+int vsb_motion_detection_device(VSMotionDetect* md, LocalMotions* motions, const uint8_t* d_plane0,
+                                int pitch) {
+  if (!md || !d_plane0) return VS_ERROR;
+  VSFrame none;
+  vsFrameNull(&none);
+  md->currorig = none;
+  return vsb_detect_common(md, motions, NULL, 0, d_plane0, pitch);
+}
+
+long vsb_launch_count(const VSMotionDetect* md) { return vsbd_launches(vsb_md_device(md)); }
+
+static double now_s(void) {
+  struct timespec ts;
+  clock_gettime(CLOCK_MONOTONIC, &ts);
+  return ts.tv_sec + ts.tv_nsec * 1e-9;
+}
+
+long vsb_detect_clip(int width, int height, int pformat, const uint8_t* frames, long frame_bytes,
+                     int linesize, int nframes, int on_device, int stepSize, int accuracy,
+                     int shakiness, double mincontrast, int tripod, int show,
+                     int serializationMode, const char* trf_path, void* out, long out_cap,
+                     int* counts, double* elapsed, uint8_t* show_out) {
+  VSFrameInfo fi;
+  VSMotionDetect md;
+  VSMotionDetectConfig conf;
+  LocalMotion* rec = (LocalMotion*)out;
+  long total = 0;
+  FILE* trf = NULL;
+  uint8_t* work = NULL;
+  uint8_t* chroma = NULL;
+  double t_acc = 0.0;
+  if (!vsFrameInfoInit(&fi, width, height, (VSPixelFormat)pformat)) return -1;
+  conf = vsMotionDetectGetDefaultConfig("vsb");
+  conf.stepSize = stepSize;
+  conf.accuracy = accuracy;
+  conf.shakiness = shakiness;
+  conf.contrastThreshold = mincontrast;
+  conf.virtualTripod = tripod;
+  conf.show = on_device ? 0 : show;
+  memset(&md, 0, sizeof(md));
+  md.serializationMode = serializationMode;
+  if (vsMotionDetectInit(&md, &conf, &fi) != VS_OK) return -1;
+  if (trf_path) {
+    trf = fopen(trf_path, "wb");
+    if (!trf || vsPrepareFile(&md, trf) != VS_OK) {
+      if (trf) fclose(trf);
+      vsMotionDetectionCleanup(&md);
+      return -1;
+    }
+  }
+  if (conf.show) work = (uint8_t*)malloc((size_t)frame_bytes);
+  chroma = (uint8_t*)calloc((size_t)width * height + 64, 1);
+  for (int k = 0; k < nframes; k++) {
+    LocalMotions lms;
+    const uint8_t* src = frames + (size_t)k * frame_bytes;
+    int rc;
+    double t0;
+    if (on_device) {
+      t0 = now_s();
+      rc = vsb_motion_detection_device(&md, &lms, src, linesize);
+    } else {
+      VSFrame f;
+      memset(&f, 0, sizeof(f));
+      if (work) {
+        memcpy(work, src, (size_t)frame_bytes);
+        src = work;
+      }
+      f.data[0] = (uint8_t*)src;
+      f.linesize[0] = linesize;
+      if (pformat < PF_PACKED)
+        for (int p = 1; p < fi.planes; p++) {
+          f.data[p] = chroma;
+          f.linesize[p] = width >> vsGetPlaneWidthSubS(&fi, p);
+        }
+      t0 = now_s();
+      rc = vsMotionDetection(&md, &lms, &f);
+    }
+    if (rc != VS_OK) {
+      counts[k] = -1;
+      total = -1;
+      break;
+    }
+    t_acc += now_s() - t0;
+    int n = vs_vector_size(&lms);
+    counts[k] = n;
+    for (int i = 0; i < n; i++) {
+      if (rec && total < out_cap) rec[total] = *LMGet(&lms, i);
+      total++;
+    }
+    if (trf) vsWriteToFile(&md, trf, &lms);
+    if (work && show_out) memcpy(show_out + (size_t)k * frame_bytes, work, (size_t)frame_bytes);
+    vs_vector_del(&lms);
+  }
+  if (trf) fclose(trf);
+  vsMotionDetectionCleanup(&md);
+  free(work);
+  free(chroma);
+  if (elapsed) *elapsed = t_acc;
+  return total;
+}
+
+int vsb_boxblur_host(uint8_t* dst, const uint8_t* src, int width, int height, int size) {
+  return vsbd_blur_host(dst, src, width, height, size) == 0 ? VS_OK : VS_ERROR;
+}
+
+int vsb_field_minmax_host(const uint8_t* img, int width, int height, int bpp, int channels,
+                          const int16_t* x, const int16_t* y, int n, int size, uint8_t* out) {
+  return vsbd_minmax_host(img, width, height, bpp, channels, x, y, n, size, out) == 0 ? VS_OK
+                                                                                       : VS_ERROR;
+}
+
+int vsb_field_search_host(const uint8_t* curr, const uint8_t* prev, int width, int height,
+                          int size, int maxShift, int stepSize, int packed_bpp, const int16_t* x,
+                          const int16_t* y, const int16_t* ox, const int16_t* oy, int n, int tiles,
+                          uint32_t* sad, int16_t* tx, int16_t* ty, int32_t* ok) {
+  vsbd_geom g;
+  int32_t* order = NULL;
+  int planar = packed_bpp <= 0;
+  if (vsb_build_geom(&g, &order, size, planar ? 1 : packed_bpp, maxShift, stepSize, planar) != 0)
+    return VS_ERROR;
+  vsbd_item* items = (vsbd_item*)malloc(sizeof(vsbd_item) * (size_t)(n > 0 ? n : 1));
+  vsbd_result* res = (vsbd_result*)malloc(sizeof(vsbd_result) * (size_t)(n > 0 ? n : 1));
+  for (int i = 0; i < n; i++) {
+    items[i].x = x[i];
+    items[i].y = y[i];
+    items[i].ox = ox ? ox[i] : 0;
+    items[i].oy = oy ? oy[i] : 0;
+  }
+  int rc = n > 0 ? vsbd_search_host(curr, prev, width, height, &g, items, n, tiles, res) : 0;
+  for (int i = 0; rc == 0 && i < n; i++) {
+    sad[i] = res[i].sad;
+    tx[i] = res[i].tx;
+    ty[i] = res[i].ty;
+    ok[i] = res[i].ok;
+  }
+  free(items);
+  free(res);
+  free(order);
+  return rc == 0 ? VS_OK : VS_ERROR;
+}

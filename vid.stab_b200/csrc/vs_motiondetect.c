@@ -1,0 +1,577 @@
+/*
+ * vs_motiondetect.c -- the detect API (src/motiondetect.h:121-147 of the
+ * reference) over the sm_100a kernels.
+ *
+ * Per frame (src/motiondetect.c:191-305):
+ *   stage A on the GPU: upload plane 0, box-blur it, 8-bit min/max of every
+ *       coarse and fine field, full coarse search of every coarse field
+ *       (speculatively: selection cannot shrink the work below "every field
+ *       with enough contrast" at the default accuracy 15, and searching all
+ *       saves a host round trip), one copy back;
+ *   host: contrasts, field selection with libc qsort and the reference's
+ *       comparator (the tie order of qsort decides which fields are kept and
+ *       the output order), coarse LocalMotions, the simple global model, the
+ *       per-field fine offsets;
+ *   stage B on the GPU: fine search of the selected fine fields, copy back;
+ *   host: mean-match filter, concatenation.
+ *
+ * Device state lives in a table keyed by the VSMotionDetect address, since
+ * the struct layout is ABI and has no slot for it.  This file is compiled
+ * with strict IEEE arithmetic: the two divisions it performs (contrast and
+ * match) are single divisions in the reference as well.
+ */
+#include <limits.h>
+#include <pthread.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "vidstab_b200.h"
+#include "vsb_device.h"
+#include "vsb_host.h"
+
+/* (contrast, field index) as the reference sorts it (src/motiondetect.c:54-57) */
+typedef struct {
+  double contrast;
+  int index;
+} contrast_idx;
+
+struct md_state {
+  const VSMotionDetect* key;
+  vsbd_ctx* dev;
+  int planar, bpp, nch;
+  double* con_c;       /* coarse contrasts */
+  double* con_f;       /* fine contrasts */
+  contrast_idx* ci;    /* selection scratch: original, */
+  contrast_idx* seg;   /* per-segment sorted copy, */
+  contrast_idx* sel;   /* result in append order */
+  vsbd_item* items;    /* fine work list */
+  int* item_sel;       /* fine item -> position in sel */
+  long frames;
+  struct md_state* next;
+};
+typedef struct md_state md_state;
+
+static pthread_mutex_t g_lock = PTHREAD_MUTEX_INITIALIZER;
+static md_state* g_states = NULL;
+
+static md_state* state_find(const VSMotionDetect* md) {
+  pthread_mutex_lock(&g_lock);
+  md_state* s = g_states;
+  while (s && s->key != md) s = s->next;
+  pthread_mutex_unlock(&g_lock);
+  return s;
+}
+
+static void state_free(md_state* s) {
+  if (!s) return;
+  vsbd_destroy(s->dev);
+  free(s->con_c);
+  free(s->con_f);
+  free(s->ci);
+  free(s->seg);
+  free(s->sel);
+  free(s->items);
+  free(s->item_sel);
+  free(s);
+}
+
+static void state_remove(const VSMotionDetect* md) {
+  pthread_mutex_lock(&g_lock);
+  md_state** pp = &g_states;
+  while (*pp && (*pp)->key != md) pp = &(*pp)->next;
+  md_state* s = *pp;
+  if (s) *pp = s->next;
+  pthread_mutex_unlock(&g_lock);
+  state_free(s);
+}
+
+static void state_insert(md_state* s) {
+  pthread_mutex_lock(&g_lock);
+  s->next = g_states;
+  g_states = s;
+  pthread_mutex_unlock(&g_lock);
+}
+
+vsbd_ctx* vsb_md_device(const VSMotionDetect* md) {
+  md_state* s = state_find(md);
+  return s ? s->dev : NULL;
+}
+
+/* ------------------------------------------------------------------------ */
+
+VSMotionDetectConfig vsMotionDetectGetDefaultConfig(const char* modName) {
+  VSMotionDetectConfig conf;
+  memset(&conf, 0, sizeof(conf));
+  conf.stepSize = 6;
+  conf.accuracy = 15;
+  conf.shakiness = 5;
+  conf.virtualTripod = 0;
+  conf.contrastThreshold = 0.25;
+  conf.show = 0;
+  conf.modName = modName;
+  conf.numThreads = 0;
+  return conf;
+}
+
+void vsMotionDetectGetConfig(VSMotionDetectConfig* conf, const VSMotionDetect* md) {
+  if (md && conf) *conf = md->conf;
+}
+
+const VSFrameInfo* vsMotionDetectGetFrameInfo(const VSMotionDetect* md) { return &md->fi; }
+
+/* field grid of src/motiondetect.c:314-358 */
+static int init_fields(VSMotionDetect* md, VSMotionDetectFields* fs, int size, int maxShift,
+                       int stepSize, int keepBorder, int spacing, double thr) {
+  fs->fieldSize = size;
+  fs->maxShift = maxShift;
+  fs->stepSize = stepSize;
+  fs->useOffset = 0;
+  fs->contrastThreshold = thr;
+  int rows = VS_MAX(3, (md->fi.height - maxShift * 2) / (size + spacing) - 1);
+  int cols = VS_MAX(3, (md->fi.width - maxShift * 2) / (size + spacing) - 1);
+  fs->fieldNum = rows * cols;
+  fs->fieldRows = rows;
+  fs->fields = (Field*)vs_malloc(sizeof(Field) * (size_t)fs->fieldNum);
+  if (!fs->fields) {
+    vs_log_error(md->conf.modName, "malloc failed!\n");
+    return 0;
+  }
+  int border = keepBorder ? size / 2 + maxShift + stepSize : stepSize;
+  int sx = (md->fi.width - 2 * border) / VS_MAX(cols - 1, 1);
+  int sy = (md->fi.height - 2 * border) / VS_MAX(rows - 1, 1);
+  for (int r = 0; r < rows; r++)
+    for (int c = 0; c < cols; c++) {
+      Field* f = &fs->fields[r * cols + c];
+      f->x = (int16_t)(border + c * sx);
+      f->y = (int16_t)(border + r * sy);
+      f->size = (int16_t)size;
+    }
+  fs->maxFields = md->conf.accuracy * fs->fieldNum / 15;
+  vs_log_info(md->conf.modName, "Fieldsize: %i, Maximal translation: %i pixel\n", size, maxShift);
+  vs_log_info(md->conf.modName, "Number of used measurement fields: %i out of %i\n",
+              fs->maxFields, fs->fieldNum);
+  return 1;
+}
+
+/* Candidate geometry of one field set for the GPU search.
+   Planar: the spiral of src/motiondetect.c:465-518 visits exactly the square
+   lattice |i|,|j| <= K*step, K = maxShift/step; rank = visiting index.
+   Packed: (0,0) first, then the raster i = -maxShift, -maxShift+step, ...
+   (outer), j likewise (inner) of :613-628. */
+int vsb_build_geom(vsbd_geom* g, int32_t** order_out, int size, int bpp, int maxShift,
+                      int step, int planar) {
+  memset(g, 0, sizeof(*g));
+  g->size = size;
+  g->bpp = bpp;
+  g->step = step;
+  int32_t* order = NULL;
+  if (planar) {
+    int K = maxShift / step;
+    g->na = g->nb = 2 * K + 1;
+    g->ax0 = g->by0 = -K * step;
+    order = (int32_t*)malloc(sizeof(int32_t) * (size_t)g->na * g->nb);
+    if (!order) return -1;
+    for (int k = 0; k < g->na * g->nb; k++) order[k] = -1;
+    /* walk the spiral: legs of 1,1,2,2,3,3,... lattice steps, turning
+       +x -> +y -> -x -> -y */
+    int a = 0, b = 0, rank = 0, leg = 0, done = 0;
+    while (!done) {
+      int len = leg / 2 + 1, d = leg & 3;
+      for (int s = 0; s < len; s++) {
+        if (a < -K || a > K || b < -K || b > K) { done = 1; break; }
+        order[(b + K) * g->na + (a + K)] = rank++;
+        a += d == 0 ? 1 : (d == 2 ? -1 : 0);
+        b += d == 1 ? 1 : (d == 3 ? -1 : 0);
+      }
+      leg++;
+    }
+    for (int k = 0; k < g->na * g->nb; k++)
+      if (order[k] < 0) { free(order); return -1; }
+    int s = step;
+    while (s > 1) {
+      if (g->nstages >= VSBD_MAX_STAGES) { free(order); return -1; }
+      int h = s / 2;
+      g->st_r[g->nstages] = s - h;
+      g->st_h[g->nstages] = h;
+      g->nstages++;
+      s = h;
+    }
+    g->limx = maxShift + s - 1;
+    g->limy = maxShift + s;
+  } else {
+    g->na = g->nb = (2 * maxShift) / step + 1;
+    g->ax0 = g->by0 = -maxShift;
+    g->has_origin = 1;
+    order = (int32_t*)malloc(sizeof(int32_t) * (size_t)g->na * g->nb);
+    if (!order) return -1;
+    for (int a = 0; a < g->na; a++)
+      for (int b = 0; b < g->nb; b++) order[b * g->na + a] = 1 + a * g->nb + b;
+    if (step > 1) {
+      g->st_r[0] = step - 1;
+      g->st_h[0] = 1;
+      g->nstages = 1;
+    }
+    g->limx = g->limy = maxShift + step - 1;
+  }
+  g->order = order;
+  *order_out = order;
+  return 0;
+}
+
+/* how far a search can reach from the field's lattice centre */
+static void geom_reach(const vsbd_geom* g, int* lo, int* hi) {
+  int refine = 0;
+  for (int k = 0; k < g->nstages; k++) refine += g->st_r[k];
+  *lo = g->ax0 - refine;
+  *hi = g->ax0 + (g->na - 1) * g->step + refine;
+  if (g->has_origin) {
+    if (*lo > 0) *lo = 0;
+    if (*hi < 0) *hi = 0;
+  }
+}
+
+/* every read of a coarse search and of a field's min/max stays inside the
+   frame; the reference has undefined behaviour otherwise */
+static int geometry_fits(const VSMotionDetect* md, const VSMotionDetectFields* fs,
+                         const vsbd_geom* g, int searched_without_offset) {
+  int lo, hi;
+  geom_reach(g, &lo, &hi);
+  for (int i = 0; i < fs->fieldNum; i++) {
+    int x0 = fs->fields[i].x - fs->fieldSize / 2, y0 = fs->fields[i].y - fs->fieldSize / 2;
+    if (x0 < 0 || y0 < 0 || x0 + fs->fieldSize > md->fi.width || y0 + fs->fieldSize > md->fi.height)
+      return 0;
+    if (searched_without_offset &&
+        (x0 + lo < 0 || y0 + lo < 0 || x0 + fs->fieldSize + hi > md->fi.width ||
+         y0 + fs->fieldSize + hi > md->fi.height))
+      return 0;
+  }
+  return 1;
+}
+
+int vsMotionDetectInit(VSMotionDetect* md, const VSMotionDetectConfig* conf, const VSFrameInfo* fi) {
+  if (!md || !conf || !fi) return VS_ERROR;
+  md->conf = *conf;
+  md->fi = *fi;
+  if (fi->pFormat <= PF_NONE || fi->pFormat == PF_PACKED || fi->pFormat >= PF_NUMBER) {
+    vs_log_warn(md->conf.modName, "unsupported Pixel Format (%i)\n", md->fi.pFormat);
+    return VS_ERROR;
+  }
+  /* a detector re-initialised without cleanup drops its previous device state */
+  state_remove(md);
+
+  vsFrameNull(&md->curr);
+  vsFrameNull(&md->currorig);
+  vsFrameNull(&md->currtmp);
+  vsFrameNull(&md->prev);
+  md->hasSeenOneFrame = 0;
+  md->frameNum = 0;
+  md->fieldscoarse.fields = NULL;
+  md->fieldsfine.fields = NULL;
+  md->initialized = 0;
+
+  /* read before written, as in the reference: anything but the two valid
+     modes (a zeroed struct included) becomes binary */
+  if (md->serializationMode != ASCII_SERIALIZATION_MODE &&
+      md->serializationMode != BINARY_SERIALIZATION_MODE)
+    md->serializationMode = BINARY_SERIALIZATION_MODE;
+
+  md->conf.shakiness = VS_MIN(10, VS_MAX(1, md->conf.shakiness));
+  md->conf.accuracy = VS_MIN(15, VS_MAX(1, md->conf.accuracy));
+  if (md->conf.accuracy < md->conf.shakiness / 2) {
+    vs_log_info(md->conf.modName, "Accuracy should not be lower than shakiness/2 -- fixed");
+    md->conf.accuracy = md->conf.shakiness / 2;
+  }
+  if (md->conf.accuracy > 9 && md->conf.stepSize > 6) {
+    vs_log_info(md->conf.modName, "For high accuracy use lower stepsize  -- set to 6 now");
+    md->conf.stepSize = 6;
+  }
+  if (md->conf.stepSize < 1) {
+    /* the reference's spiral never terminates for a step of 0 */
+    vs_log_error(md->conf.modName, "stepsize must be at least 1 (got %i)\n", md->conf.stepSize);
+    return VS_ERROR;
+  }
+
+  /* fixed geometry of src/motiondetect.c:132-149; the rounding to the next
+     multiple of 16 always adds */
+  int minDimension = VS_MIN(md->fi.width, md->fi.height);
+  int maxShift = VS_MAX(16, minDimension / 7);
+  int fieldSize = VS_MAX(16, minDimension / 10);
+  int fieldSizeFine = VS_MAX(6, minDimension / 60);
+  fieldSize = (fieldSize / 16 + 1) * 16;
+  fieldSizeFine = (fieldSizeFine / 16 + 1) * 16;
+  if (!init_fields(md, &md->fieldscoarse, fieldSize, maxShift, md->conf.stepSize, 1, 0,
+                   md->conf.contrastThreshold))
+    return VS_ERROR;
+  if (!init_fields(md, &md->fieldsfine, fieldSizeFine, fieldSizeFine, 2, 1, fieldSizeFine,
+                   md->conf.contrastThreshold / 2)) {
+    vs_free(md->fieldscoarse.fields);
+    md->fieldscoarse.fields = NULL;
+    return VS_ERROR;
+  }
+
+  md_state* st = (md_state*)calloc(1, sizeof(md_state));
+  st->key = md;
+  st->planar = md->fi.pFormat < PF_PACKED;
+  st->bpp = st->planar ? 1 : md->fi.bytesPerPixel;
+  st->nch = st->planar ? 1 : 3;
+  int nc = md->fieldscoarse.fieldNum, nf = md->fieldsfine.fieldNum;
+  int nmax = VS_MAX(nc, nf) + 1;
+  st->con_c = (double*)malloc(sizeof(double) * (size_t)(nc + 1));
+  st->con_f = (double*)malloc(sizeof(double) * (size_t)(nf + 1));
+  st->ci = (contrast_idx*)malloc(sizeof(contrast_idx) * (size_t)nmax);
+  st->seg = (contrast_idx*)malloc(sizeof(contrast_idx) * (size_t)nmax);
+  st->sel = (contrast_idx*)malloc(sizeof(contrast_idx) * (size_t)nmax);
+  st->items = (vsbd_item*)malloc(sizeof(vsbd_item) * (size_t)(nf + 1));
+  st->item_sel = (int*)malloc(sizeof(int) * (size_t)(nf + 1));
+
+  vsbd_geom gc, gf;
+  int32_t *oc = NULL, *of = NULL;
+  int ok = st->con_c && st->con_f && st->ci && st->seg && st->sel && st->items && st->item_sel;
+  ok = ok && vsb_build_geom(&gc, &oc, fieldSize, st->bpp, maxShift, md->conf.stepSize, st->planar) == 0;
+  ok = ok && vsb_build_geom(&gf, &of, fieldSizeFine, st->bpp, fieldSizeFine, 2, st->planar) == 0;
+  if (ok && (!geometry_fits(md, &md->fieldscoarse, &gc, 1) ||
+             !geometry_fits(md, &md->fieldsfine, &gf, 0))) {
+    vs_log_error(md->conf.modName,
+                 "frame %ix%i is too small for the measurement-field layout (fields or their "
+                 "search range would leave the frame)\n",
+                 md->fi.width, md->fi.height);
+    ok = 0;
+  }
+  if (ok) {
+    int16_t* xy = (int16_t*)malloc(sizeof(int16_t) * 2 * (size_t)(nc + nf + 1));
+    for (int i = 0; i < nc; i++) {
+      xy[i] = md->fieldscoarse.fields[i].x;
+      xy[nc + i] = md->fieldscoarse.fields[i].y;
+    }
+    for (int i = 0; i < nf; i++) {
+      xy[2 * nc + i] = md->fieldsfine.fields[i].x;
+      xy[2 * nc + nf + i] = md->fieldsfine.fields[i].y;
+    }
+    int blur = st->planar ? vsb_blur_size(md->conf.stepSize, md->fi.width, md->fi.height) : 0;
+    if (vsbd_create(&st->dev, md->fi.width, md->fi.height, st->bpp, blur, st->nch, &gc, xy,
+                    xy + nc, nc, &gf, xy + 2 * nc, xy + 2 * nc + nf, nf) != 0) {
+      vs_log_error(md->conf.modName, "GPU initialisation failed: %s\n", vsbd_error());
+      ok = 0;
+    }
+    free(xy);
+  }
+  free(oc);
+  free(of);
+  if (!ok) {
+    state_free(st);
+    vs_free(md->fieldscoarse.fields);
+    vs_free(md->fieldsfine.fields);
+    md->fieldscoarse.fields = NULL;
+    md->fieldsfine.fields = NULL;
+    return VS_ERROR;
+  }
+  vs_log_info(md->conf.modName, "GPU: sm_100a kernels, blur size %i\n",
+              st->planar ? vsb_blur_size(md->conf.stepSize, md->fi.width, md->fi.height) : 0);
+  state_insert(st);
+  md->initialized = 2;
+  return VS_OK;
+}
+
+void vsMotionDetectionCleanup(VSMotionDetect* md) {
+  state_remove(md);
+  if (md->fieldscoarse.fields) {
+    vs_free(md->fieldscoarse.fields);
+    md->fieldscoarse.fields = 0;
+  }
+  if (md->fieldsfine.fields) {
+    vs_free(md->fieldsfine.fields);
+    md->fieldsfine.fields = 0;
+  }
+  vsFrameFree(&md->prev);
+  vsFrameFree(&md->curr);
+  vsFrameFree(&md->currtmp);
+  md->initialized = 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* field selection (src/motiondetect.c:662-743)                              */
+/* ------------------------------------------------------------------------ */
+
+/* descending contrast; equal contrasts compare equal, so their order is
+   whatever libc qsort makes of it -- exactly as in the reference */
+static int cmp_contrast_idx(const void* a, const void* b) {
+  double x = ((const contrast_idx*)a)->contrast;
+  double y = ((const contrast_idx*)b)->contrast;
+  return x < y ? 1 : (x > y ? -1 : 0);
+}
+
+/* fills st->sel in the reference's append order; returns the count */
+static int select_fields(md_state* st, const VSMotionDetectFields* fs, const double* contrast) {
+  int n = fs->fieldNum, nsel = 0;
+  contrast_idx* ci = st->ci;
+  contrast_idx* seg = st->seg;
+  for (int i = 0; i < n; i++) {
+    ci[i].contrast = contrast[i] < fs->contrastThreshold ? 0 : contrast[i];
+    ci[i].index = i;
+  }
+  memcpy(seg, ci, sizeof(contrast_idx) * (size_t)n);
+  int numsegms = fs->fieldRows + 1;
+  int segmlen = n / (fs->fieldRows + 1) + 1;
+  int per_seg = fs->maxFields / numsegms;
+  for (int s = 0; s < numsegms; s++) {
+    int a = segmlen * s;
+    int b = VS_MIN(segmlen * (s + 1), n);
+    qsort(seg + a, (size_t)(b - a > 0 ? b - a : 0), sizeof(contrast_idx), cmp_contrast_idx);
+    for (int j = 0; j < per_seg; j++) {
+      if (a + j >= b) continue;
+      if (seg[a + j].contrast > 0) {
+        st->sel[nsel++] = ci[seg[a + j].index];
+        seg[a + j].contrast = 0;
+      }
+    }
+  }
+  int remaining = fs->maxFields - nsel;
+  if (remaining > 0) {
+    qsort(seg, (size_t)n, sizeof(contrast_idx), cmp_contrast_idx);
+    for (int j = 0; j < remaining; j++)
+      if (seg[j].contrast > 0) st->sel[nsel++] = seg[j];
+  }
+  return nsel;
+}
+
+/* Michelson contrast of one field from its 8-bit extremes
+   (src/motiondetect.c:406; packed: mean over three channels, :374-376) */
+static void field_contrasts(const md_state* st, const uint8_t* mm, int n, double* out) {
+  for (int i = 0; i < n; i++) {
+    const uint8_t* p = mm + (size_t)i * st->nch * 2;
+    if (st->nch == 1) {
+      int mini = p[0], maxi = p[1];
+      out[i] = (maxi - mini) / (maxi + mini + 0.1);
+    } else {
+      double c[3];
+      for (int k = 0; k < 3; k++) {
+        int mini = p[2 * k], maxi = p[2 * k + 1];
+        c[k] = (maxi - mini) / (maxi + mini + 0.1);
+      }
+      out[i] = vsb_mean3(c[0], c[1], c[2]);
+    }
+  }
+}
+
+static LocalMotion make_lm(const Field* f, int vx, int vy, double contrast, uint32_t sad) {
+  LocalMotion lm = null_localmotion();
+  lm.f = *f;
+  lm.v.x = (int16_t)vx;
+  lm.v.y = (int16_t)vy;
+  lm.contrast = contrast;
+  lm.match = ((double)sad) / (f->size * f->size);
+  return lm;
+}
+
+static short match_at_most(void* thresh, void* lm) {
+  return ((LocalMotion*)lm)->match <= *(double*)thresh ? 1 : 0;
+}
+
+int vsb_detect_common(VSMotionDetect* md, LocalMotions* motions, const uint8_t* host, int linesize,
+                      const uint8_t* dev, int pitch) {
+  if (!md || !motions || md->initialized != 2) {
+    vs_log_error(md ? md->conf.modName : "vid.stab", "motion detection is not initialised\n");
+    return VS_ERROR;
+  }
+  md_state* st = state_find(md);
+  if (!st) {
+    vs_log_error(md->conf.modName, "no device state for this detector\n");
+    return VS_ERROR;
+  }
+  int leadIn = md->conf.virtualTripod >= 1 && md->frameNum < md->conf.virtualTripod;
+  int search = md->hasSeenOneFrame && !leadIn;
+  const uint8_t* mm = NULL;
+  const vsbd_result* cres = NULL;
+  if (vsbd_stage_a(st->dev, host, linesize, dev, pitch, search, &mm, &cres) != 0) {
+    vs_log_error(md->conf.modName, "GPU stage A failed: %s\n", vsbd_error());
+    return VS_ERROR;
+  }
+  if (search) {
+    VSMotionDetectFields* fc = &md->fieldscoarse;
+    VSMotionDetectFields* ff = &md->fieldsfine;
+    LocalMotions coarse, fine;
+    vs_vector_init(&coarse, fc->maxFields);
+    vs_vector_init(&fine, 0);
+    field_contrasts(st, mm, fc->fieldNum, st->con_c);
+    field_contrasts(st, mm + (size_t)fc->fieldNum * st->nch * 2, ff->fieldNum, st->con_f);
+
+    int nsel = select_fields(st, fc, st->con_c);
+    for (int k = 0; k < nsel; k++) {
+      int i = st->sel[k].index;
+      const vsbd_result* r = &cres[i];
+      if (!r->ok) continue;
+      LocalMotion lm = make_lm(&fc->fields[i], r->tx, r->ty, st->sel[k].contrast, r->sad);
+      vs_vector_append_dup(&coarse, &lm, sizeof(LocalMotion));
+    }
+    int num_motions = vs_vector_size(&coarse);
+    if (num_motions < 1) {
+      vs_log_warn(md->conf.modName, "too low contrast. (no translations are detected in frame %i)\n",
+                  md->frameNum);
+    } else {
+      VSTransform t = vsSimpleMotionsToTransform(md->fi, md->conf.modName, &coarse);
+      ff->offset = t;
+      ff->useOffset = 1;
+      int nfs = select_fields(st, ff, st->con_f);
+      int nitems = 0;
+      PreparedTransform pt = prepare_transform(&ff->offset, &md->fi);
+      int border = ff->fieldSize / 2 + ff->maxShift + ff->stepSize;
+      for (int k = 0; k < nfs; k++) {
+        const Field* f = &ff->fields[st->sel[k].index];
+        Vec pos = { f->x, f->y };
+        Vec off = sub_vec(transform_vec(&pt, &pos), pos);
+        int x = pos.x + off.x, y = pos.y + off.y;
+        if (x - border < 0 || x + border >= md->fi.width || y - border < 0 ||
+            y + border >= md->fi.height)
+          continue; /* the shifted search would leave the frame (:429-433) */
+        st->items[nitems].x = f->x;
+        st->items[nitems].y = f->y;
+        st->items[nitems].ox = off.x;
+        st->items[nitems].oy = off.y;
+        st->item_sel[nitems] = k;
+        nitems++;
+      }
+      const vsbd_result* fres = NULL;
+      if (vsbd_stage_b(st->dev, st->items, nitems, &fres) != 0) {
+        vs_log_error(md->conf.modName, "GPU stage B failed: %s\n", vsbd_error());
+        vs_vector_del(&coarse);
+        vs_vector_del(&fine);
+        return VS_ERROR;
+      }
+      LocalMotions motions2;
+      vs_vector_init(&motions2, nitems > 0 ? nitems : 1);
+      for (int m = 0; m < nitems; m++) {
+        if (!fres[m].ok) continue;
+        const contrast_idx* s = &st->sel[st->item_sel[m]];
+        LocalMotion lm = make_lm(&ff->fields[s->index], fres[m].tx + st->items[m].ox,
+                                 fres[m].ty + st->items[m].oy, s->contrast, fres[m].sad);
+        vs_vector_append_dup(&motions2, &lm, sizeof(LocalMotion));
+      }
+      VSArray q = localmotionsGetMatch(&coarse);
+      double meanMatch = cleanmean(q.dat, q.len, NULL, NULL);
+      for (int m = 0; m < vs_vector_size(&motions2); m++) {
+        LocalMotion* lm = LMGet(&motions2, m);
+        if (match_at_most(&meanMatch, lm)) vs_vector_append_dup(&fine, lm, sizeof(LocalMotion));
+      }
+      vs_array_free(q);
+      vs_vector_del(&motions2);
+    }
+    if (md->conf.show) vsb_draw_motions(md, &coarse, &fine);
+    *motions = vs_vector_concat(&coarse, &fine);
+    vs_vector_fini(&coarse);
+    vs_vector_fini(&fine);
+  } else {
+    vs_vector_init(motions, 1);
+    md->hasSeenOneFrame = 1;
+  }
+  if (md->conf.virtualTripod < 1 || md->frameNum < md->conf.virtualTripod)
+    vsbd_commit_prev(st->dev);
+  md->frameNum++;
+  st->frames++;
+  return VS_OK;
+}
+
+int vsMotionDetection(VSMotionDetect* md, LocalMotions* motions, VSFrame* frame) {
+  if (!md || !frame || !frame->data[0]) return VS_ERROR;
+  md->currorig = *frame;
+  return vsb_detect_common(md, motions, frame->data[0], frame->linesize[0], NULL, 0);
+}

@@ -1,0 +1,94 @@
+/*
+ * vsb_device.h -- internal C interface between the host C library and the
+ * sm_100a CUDA code (vsb_device.cu).  Plain C types only.
+ */
+#ifndef VSB_DEVICE_H
+#define VSB_DEVICE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* One search item: a field centre and the displacement the lattice is
+   centred on (zero for the coarse pass, the transform-derived offset for the
+   fine pass). */
+typedef struct {
+  int16_t x, y;
+  int16_t ox, oy;
+} vsbd_item;
+
+/* Result of one item: minimal SAD, the best displacement relative to the
+   item's offset, and whether it passed the final range test. */
+typedef struct {
+  uint32_t sad;
+  int16_t tx, ty;
+  int32_t ok;
+} vsbd_result;
+
+#define VSBD_MAX_STAGES 8
+
+/* Candidate geometry of one field set.
+   Lattice point (a,b), 0<=a<na, 0<=b<nb, is the displacement
+   (ax0 + a*step, by0 + b*step).  order[b*na + a] is its rank in the
+   reference's visiting order: the lowest (SAD, rank) wins.  With has_origin
+   the displacement (0,0) is evaluated first with rank 0 (raster scans).
+   Refinement stage k evaluates the (2*r/h+1)^2 grid of spacing h around the
+   current best (i outer, j inner), the centre excluded.  A result is rejected
+   when |tx| >= limx or |ty| >= limy. */
+typedef struct {
+  int size, bpp, step;
+  int na, nb, ax0, by0;
+  int has_origin;
+  int nstages;
+  int st_r[VSBD_MAX_STAGES];
+  int st_h[VSBD_MAX_STAGES];
+  int limx, limy;
+  const int32_t* order; /* host array, na*nb */
+} vsbd_geom;
+
+typedef struct vsbd_ctx vsbd_ctx;
+
+/* Creates the device state of one detector.  blur_size < 2 means no blur
+   (the plane is used as is; packed formats).  channels: 1 planar, 3 packed
+   (contrast over the colour channels).  Returns 0 or -1 (vsbd_error()). */
+int vsbd_create(vsbd_ctx** out, int width, int height, int bpp, int blur_size, int channels,
+                const vsbd_geom* coarse, const int16_t* cx, const int16_t* cy, int nc,
+                const vsbd_geom* fine, const int16_t* fx, const int16_t* fy, int nf);
+void vsbd_destroy(vsbd_ctx* c);
+
+/* Stage A of one frame: take plane 0 (host pointer + linesize, or a device
+   pointer + pitch when dev != NULL), blur it into the current buffer and,
+   when search != 0, compute every field's (min,max) and run the coarse
+   search of every coarse field against the previous buffer.  Blocks until
+   the results are on the host.  minmax: (nc+nf)*channels (min,max) byte
+   pairs, coarse first; coarse: nc results. */
+int vsbd_stage_a(vsbd_ctx* c, const uint8_t* host, int linesize, const uint8_t* dev, int pitch,
+                 int search, const uint8_t** minmax, const vsbd_result** coarse);
+
+/* Stage B: fine search of n items against the previous buffer; blocks. */
+int vsbd_stage_b(vsbd_ctx* c, const vsbd_item* items, int n, const vsbd_result** fine);
+
+/* The current buffer becomes the previous one. */
+void vsbd_commit_prev(vsbd_ctx* c);
+
+/* Kernel launches issued on behalf of this detector so far. */
+long vsbd_launches(const vsbd_ctx* c);
+
+/* Message of the last failure on this thread. */
+const char* vsbd_error(void);
+
+/* ---- kernel-level entry points for parity tests (host buffers in/out) --- */
+int vsbd_blur_host(uint8_t* dst, const uint8_t* src, int width, int height, int size);
+int vsbd_minmax_host(const uint8_t* img, int width, int height, int bpp, int channels,
+                     const int16_t* x, const int16_t* y, int n, int size, uint8_t* out);
+int vsbd_search_host(const uint8_t* curr, const uint8_t* prev, int width, int height,
+                     const vsbd_geom* g, const vsbd_item* items, int n, int tiles_hint,
+                     vsbd_result* out);
+int vsbd_device_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

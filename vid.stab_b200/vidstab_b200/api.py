@@ -1,0 +1,168 @@
+"""Python calls over the C ABI: a per-frame detector mirroring the reference
+API (vsMotionDetectInit / vsMotionDetection / vsMotionDetectionCleanup) and
+a clip driver that loops in C."""
+import ctypes as C
+
+import numpy as np
+
+from ._lib import (LM_DTYPE, PF_PACKED, PF_RGBA, VSFrame, VSFrameInfo, VSMotionDetect,
+                   VSVector, lib, ptr, vector_records)
+
+
+def bpp_of(pformat):
+    if pformat < PF_PACKED:
+        return 1
+    return 4 if pformat == PF_RGBA else 3
+
+
+class MotionDetector:
+    """One detect stream (src/motiondetect.h:121-147 of the reference)."""
+
+    def __init__(self, width, height, pformat=1, stepsize=6, accuracy=15, shakiness=5,
+                 mincontrast=0.25, tripod=0, show=0, serialization_mode=0):
+        L = lib()
+        self.L = L
+        self.fi = VSFrameInfo()
+        if not L.vsFrameInfoInit(C.byref(self.fi), width, height, pformat):
+            raise ValueError("invalid frame geometry / pixel format")
+        conf = L.vsMotionDetectGetDefaultConfig(b"vidstab_b200")
+        conf.stepSize, conf.accuracy, conf.shakiness = stepsize, accuracy, shakiness
+        conf.contrastThreshold, conf.virtualTripod, conf.show = mincontrast, tripod, show
+        self.conf = conf
+        self.md = VSMotionDetect()
+        self.md.serializationMode = serialization_mode
+        if L.vsMotionDetectInit(C.byref(self.md), C.byref(conf), C.byref(self.fi)) != 0:
+            raise RuntimeError("vsMotionDetectInit failed: %s" % L.vsb_last_error().decode())
+        self.width, self.height, self.pformat = width, height, pformat
+        self._chroma = np.full(width * height + 64, 128, np.uint8)
+
+    def detect(self, plane0, linesize=None):
+        """Motions of one frame given its plane 0 (host numpy array)."""
+        plane0 = np.ascontiguousarray(plane0)
+        f = VSFrame()
+        f.data[0] = plane0.ctypes.data
+        f.linesize[0] = linesize or plane0.strides[0]
+        for p in range(1, self.fi.planes):
+            f.data[p] = self._chroma.ctypes.data
+            f.linesize[p] = self.width >> (self.fi.log2ChromaW if p in (1, 2) else 0)
+        v = VSVector()
+        if self.L.vsMotionDetection(C.byref(self.md), C.byref(v), C.byref(f)) != 0:
+            raise RuntimeError("vsMotionDetection failed: %s" % self.L.vsb_last_error().decode())
+        out = vector_records(v)
+        self.L.vs_vector_del(C.byref(v))
+        return out
+
+    def detect_device(self, dptr, pitch):
+        """Motions of one frame whose plane 0 is at CUDA address dptr."""
+        v = VSVector()
+        if self.L.vsb_motion_detection_device(C.byref(self.md), C.byref(v), C.c_void_p(dptr),
+                                              pitch) != 0:
+            raise RuntimeError("vsb_motion_detection_device failed: %s"
+                               % self.L.vsb_last_error().decode())
+        out = vector_records(v)
+        self.L.vs_vector_del(C.byref(v))
+        return out
+
+    @property
+    def frame_num(self):
+        return self.md.frameNum
+
+    def launches(self):
+        return self.L.vsb_launch_count(C.byref(self.md))
+
+    def close(self):
+        if self.md is not None and self.md.initialized:
+            self.L.vsMotionDetectionCleanup(C.byref(self.md))
+        self.md = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def detect_clip(frames, pformat=1, stepsize=6, accuracy=15, shakiness=5, mincontrast=0.25,
+                tripod=0, show=0, serialization_mode=0, trf_path=None, on_device_ptr=None,
+                frame_bytes=None, linesize=None, width=None, height=None, return_frames=False):
+    """Runs the detect API over a clip in C.
+
+    frames: numpy uint8 array (n, H, W) planar / (n, H, W*bpp) packed, or
+    with on_device_ptr a CUDA address of n frames frame_bytes apart.
+    Returns (records, counts, elapsed_seconds[, drawn frames])."""
+    L = lib()
+    if on_device_ptr is None:
+        frames = np.ascontiguousarray(frames)
+        n, H = frames.shape[0], frames.shape[1]
+        W = frames.shape[2] // bpp_of(pformat)
+        fb = frames[0].nbytes
+        ls = frames.shape[2]
+        src = frames.ctypes.data
+    else:
+        n = frames
+        H, W, fb, ls, src = height, width, frame_bytes, linesize, on_device_ptr
+    cap = n * 512 + 64
+    out = np.zeros(cap, LM_DTYPE)
+    counts = np.zeros(n, np.int32)
+    el = C.c_double(0)
+    drawn = np.zeros((n, fb), np.uint8) if (show and return_frames) else None
+    total = L.vsb_detect_clip(W, H, pformat, C.c_void_p(src), fb, ls, n,
+                              1 if on_device_ptr is not None else 0, stepsize, accuracy,
+                              shakiness, mincontrast, tripod, show, serialization_mode,
+                              trf_path.encode() if trf_path else None, ptr(out), cap, ptr(counts),
+                              C.byref(el), ptr(drawn))
+    if total < 0:
+        raise RuntimeError("vsb_detect_clip failed: %s" % L.vsb_last_error().decode())
+    res = (out[:total].copy(), counts, el.value)
+    if return_frames:
+        res = res + (drawn,)
+    return res
+
+
+def boxblur(plane, size):
+    """GPU prefilter of one tight W x H plane with (clamped) box size."""
+    L = lib()
+    plane = np.ascontiguousarray(plane, dtype=np.uint8)
+    H, W = plane.shape
+    out = np.empty_like(plane)
+    if L.vsb_boxblur_host(ptr(out), ptr(plane), W, H, size) != 0:
+        raise RuntimeError(L.vsb_last_error().decode())
+    return out
+
+
+def field_minmax(img, xs, ys, size, bpp=1, channels=1):
+    L = lib()
+    img = np.ascontiguousarray(img, dtype=np.uint8)
+    H = img.shape[0]
+    W = img.shape[1] // bpp
+    xs = np.ascontiguousarray(xs, np.int16)
+    ys = np.ascontiguousarray(ys, np.int16)
+    out = np.zeros((len(xs), channels, 2), np.uint8)
+    if L.vsb_field_minmax_host(ptr(img), W, H, bpp, channels, ptr(xs), ptr(ys), len(xs), size,
+                               ptr(out)) != 0:
+        raise RuntimeError(L.vsb_last_error().decode())
+    return out
+
+
+def field_search(curr, prev, xs, ys, size, max_shift, step, ox=None, oy=None, packed_bpp=0,
+                 tiles=0):
+    """Per-field search results (sad, tx, ty, ok) of the GPU kernel."""
+    L = lib()
+    curr = np.ascontiguousarray(curr, dtype=np.uint8)
+    prev = np.ascontiguousarray(prev, dtype=np.uint8)
+    H = curr.shape[0]
+    W = curr.shape[1] // (packed_bpp or 1)
+    n = len(xs)
+    xs = np.ascontiguousarray(xs, np.int16)
+    ys = np.ascontiguousarray(ys, np.int16)
+    ox = np.ascontiguousarray(ox if ox is not None else np.zeros(n), np.int16)
+    oy = np.ascontiguousarray(oy if oy is not None else np.zeros(n), np.int16)
+    sad = np.zeros(n, np.uint32)
+    tx = np.zeros(n, np.int16)
+    ty = np.zeros(n, np.int16)
+    ok = np.zeros(n, np.int32)
+    if L.vsb_field_search_host(ptr(curr), ptr(prev), W, H, size, max_shift, step, packed_bpp,
+                               ptr(xs), ptr(ys), ptr(ox), ptr(oy), n, tiles, ptr(sad), ptr(tx),
+                               ptr(ty), ptr(ok)) != 0:
+        raise RuntimeError(L.vsb_last_error().decode())
+    return sad, tx, ty, ok
