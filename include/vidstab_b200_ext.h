@@ -49,6 +49,23 @@ VS_API long vsb_detect_clip(int width, int height, int pformat, const uint8_t* f
                             void* out, long out_cap, int* counts, double* elapsed,
                             uint8_t* show_out);
 
+/* Per-kernel device time: with timing on, CUDA events bracket every kernel
+   of the detector on its stream.  ms[k] and count[k] for k = 0 blur,
+   1 field min/max, 2 coarse search, 3 fine search (4 entries each).
+   Turning timing on resets the totals. */
+VS_API int vsb_set_kernel_timing(struct _vsmotiondetect* md, int on);
+VS_API int vsb_kernel_times(const struct _vsmotiondetect* md, double* ms, long* count);
+
+/* Process-wide totals since load: kernels launched by the detect path, and
+   bytes it copied host-to-device (frames, work lists) and device-to-host
+   (per-field results). */
+VS_API void vsb_counters(long long* launches, long long* h2d_bytes, long long* d2h_bytes);
+
+/* Measured byte-absolute-difference throughput (per second) of the GPU's
+   packed SAD instruction sequence in a register-only loop: variant 0 the
+   accumulate form the kernels use, 1 and 2 alternative formulations. */
+VS_API int vsb_sad_peak(int variant, double* byteops_per_s);
+
 /* ---- kernel-level entry points (host buffers in and out; for testing) ---- */
 
 /* luma prefilter of one W x H plane (tight rows) with box size `size`

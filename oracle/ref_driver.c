@@ -256,3 +256,37 @@ void vsref_simple_transform(int width, int height, const LocalMotion* lms, int n
   out[0] = t.x; out[1] = t.y; out[2] = t.alpha; out[3] = t.zoom;
   vs_vector_del(&v);
 }
+
+/* the fine-search offset of one field for transform t4 = {x, y, alpha, zoom}:
+   prepare_transform + transform_vec - position, as fieldSearchOffset does
+   (src/motiondetect.c:418-427) */
+void vsref_field_offset(const double* t4, int width, int height, int fx, int fy,
+                        int16_t* ox, int16_t* oy) {
+  VSFrameInfo fi;
+  VSTransform t = null_transform();
+  vsFrameInfoInit(&fi, width, height, PF_GRAY8);
+  t.x = t4[0]; t.y = t4[1]; t.alpha = t4[2]; t.zoom = t4[3];
+  PreparedTransform pt = prepare_transform(&t, &fi);
+  Vec pos = { (int16_t)fx, (int16_t)fy };
+  Vec off = sub_vec(transform_vec(&pt, &pos), pos);
+  *ox = off.x;
+  *oy = off.y;
+}
+
+double vsref_cleanmean(double* ds, int len, double* mn, double* mx) {
+  return cleanmean(ds, len, mn, mx);
+}
+
+/* contrast of a packed field as the reference's packed detect computes it
+   (contrastSubImgPacked, src/motiondetect.c:370-377) */
+double vsref_contrast_packed(const uint8_t* I, int linesize, int width, int height, int bpp,
+                             int fx, int fy, int size) {
+  VSMotionDetect md;
+  Field f;
+  memset(&md, 0, sizeof(md));
+  vsFrameInfoInit(&md.fi, width, height, bpp == 4 ? PF_RGBA : PF_RGB24);
+  md.curr.data[0] = (uint8_t*)I;
+  md.curr.linesize[0] = linesize;
+  f.x = (int16_t)fx; f.y = (int16_t)fy; f.size = (int16_t)size;
+  return contrastSubImgPacked(&md, &f);
+}

@@ -320,7 +320,7 @@ static int orc_cmp_int(const void* a, const void* b) {
   return x < y ? -1 : (x > y ? 1 : 0);
 }
 
-double orc_cleanmean(double* ds, int len, double* mn, double* mx) {
+__attribute__((noinline)) double orc_cleanmean(double* ds, int len, double* mn, double* mx) {
   int cut = len / 5;
   double sum = 0;
   int i = 0;
@@ -334,27 +334,33 @@ double orc_cleanmean(double* ds, int len, double* mn, double* mx) {
 }
 
 /* the cleaned mean shift is accumulated and stored in int16 fields
-   (Vec, src/transformtype.c:513-534) */
-static void orc_cleanmean_shift(const orc_lm* lms, int n, int16_t* mx, int16_t* my) {
+   (Vec, src/transformtype.c:513-534); kept out of line and returned by
+   value as the reference's cleanmean_localmotions is, so that the compiler
+   treats the caller's expressions alike */
+typedef struct { int16_t x, y; } orc_vec;
+typedef struct { orc_vec v; int16_t pad[3]; double c, m; } orc_meanlm;
+
+__attribute__((noinline)) static orc_meanlm orc_cleanmean_shift(const orc_lm* lms, int n) {
   int cut = n / 5;
   int* xs = (int*)malloc(sizeof(int) * n);
   int* ys = (int*)malloc(sizeof(int) * n);
   for (int i = 0; i < n; i++) { xs[i] = lms[i].vx; ys[i] = lms[i].vy; }
-  int16_t ax = 0, ay = 0;
+  orc_meanlm m;
+  memset(&m, 0, sizeof(m));
   qsort(xs, n, sizeof(int), orc_cmp_int);
-  for (int i = cut; i < n - cut; i++) ax = (int16_t)(ax + xs[i]);
+  for (int i = cut; i < n - cut; i++) m.v.x += xs[i];
   qsort(ys, n, sizeof(int), orc_cmp_int);
-  for (int i = cut; i < n - cut; i++) ay = (int16_t)(ay + ys[i]);
+  for (int i = cut; i < n - cut; i++) m.v.y += ys[i];
   free(xs);
   free(ys);
-  ax = (int16_t)(ax / (n - (2.0 * cut)));
-  ay = (int16_t)(ay / (n - (2.0 * cut)));
-  *mx = ax;
-  *my = ay;
+  m.v.x /= (n - (2.0 * cut));
+  m.v.y /= (n - (2.0 * cut));
+  return m;
 }
 
 /* src/localmotion2transform.c:336-349 */
-static double orc_angle(int fx, int fy, int fsize, int vx, int vy, int cx, int cy) {
+__attribute__((noinline)) static double orc_angle(int fx, int fy, int fsize, int vx, int vy, int cx,
+                                                 int cy) {
   if (abs(fx - cx) + abs(fy - cy) < fsize * 2) return 0;
   double a1 = atan2(fy - cy, fx - cx);
   double a2 = atan2(fy - cy + vy, fx - cx + vx);
@@ -362,49 +368,94 @@ static double orc_angle(int fx, int fy, int fsize, int vx, int vy, int cx, int c
   return (diff > M_PI) ? diff - 2 * M_PI : ((diff < -M_PI) ? diff + 2 * M_PI : diff);
 }
 
-void orc_simple_transform(int width, int height, const orc_lm* lms, int n, double* out) {
-  out[0] = out[1] = out[2] = out[3] = 0;
-  if (n < 1) return;
+typedef struct { double x, y, alpha, zoom, barrel, rshutter; int extra; } orc_trans;
+
+/* src/localmotion2transform.c:352-402: centre of the fields, trimmed mean
+   shift, trimmed mean rotation (from 6 fields on), rotation re-centred on
+   the frame centre */
+static orc_trans orc_model(int width, int height, const orc_lm* lms, int n) {
+  orc_trans t;
+  memset(&t, 0, sizeof(t));
+  if (n < 1) return t;
   int cx = 0, cy = 0;
+  double* angles = (double*)malloc(sizeof(double) * n);
   for (int i = 0; i < n; i++) { cx += lms[i].fx; cy += lms[i].fy; }
   cx /= n;
   cy /= n;
-  int16_t mvx, mvy;
-  orc_cleanmean_shift(lms, n, &mvx, &mvy);
-  double alpha = 0;
-  if (n >= 6) {
-    double* angles = (double*)malloc(sizeof(double) * n);
+  orc_meanlm mean = orc_cleanmean_shift(lms, n);
+  if (n < 6) {
+    t.alpha = 0;
+  } else {
     for (int i = 0; i < n; i++) {
-      int16_t vx = (int16_t)(lms[i].vx - mvx), vy = (int16_t)(lms[i].vy - mvy);
+      int16_t vx = (int16_t)(lms[i].vx - mean.v.x), vy = (int16_t)(lms[i].vy - mean.v.y);
       angles[i] = orc_angle(lms[i].fx, lms[i].fy, lms[i].fsize, vx, vy, cx, cy);
     }
     double mn, mx;
-    alpha = -orc_cleanmean(angles, n, &mn, &mx);
-    if (mx - mn > 1.0) alpha = 0;
-    free(angles);
+    t.alpha = -orc_cleanmean(angles, n, &mn, &mx);
+    if (mx - mn > 1.0) t.alpha = 0;
   }
+  free(angles);
   double p_x = (cx - width / 2);
   double p_y = (cy - height / 2);
-  out[0] = mvx + (cos(alpha) - 1) * p_x - sin(alpha) * p_y;
-  out[1] = mvy + sin(alpha) * p_x + (cos(alpha) - 1) * p_y;
-  out[2] = alpha;
-  out[3] = 0;
+  t.x = mean.v.x + (cos(t.alpha) - 1) * p_x - sin(t.alpha) * p_y;
+  t.y = mean.v.y + sin(t.alpha) * p_x + (cos(t.alpha) - 1) * p_y;
+  return t;
 }
 
-/* prepare_transform + transform_vec for the similarity model, truncated to
-   int16 (src/transformtype.c:162-191, :207-208), minus the field position */
-static void orc_field_offset(const double* t, int W, int H, int fx, int fy,
+void orc_simple_transform(int width, int height, const orc_lm* lms, int n, double* out) {
+  orc_trans t = orc_model(width, height, lms, n);
+  out[0] = t.x;
+  out[1] = t.y;
+  out[2] = t.alpha;
+  out[3] = t.zoom;
+}
+
+/* prepare_transform + transform_vec for the similarity model
+   (src/transformtype.c:162-191, :207-208): the frame centre is integer,
+   the new position is truncated to int16, the offset is the difference.
+   Both steps stay out of line, as in the reference where they live in
+   another translation unit than their caller. */
+typedef struct { const orc_trans* t; double zcos, zsin, cx, cy, f, z; } orc_prep;
+
+__attribute__((noinline)) static orc_prep orc_prepare(const orc_trans* t, int W, int H) {
+  orc_prep p;
+  p.t = t;
+  double z = 1.0 + t->zoom / 100.0;
+  p.zcos = z * cos(t->alpha);
+  p.zsin = z * sin(t->alpha);
+  p.cx = W / 2;
+  p.cy = H / 2;
+  p.z = z;
+  p.f = 0.0;
+  return p;
+}
+
+__attribute__((noinline)) static orc_vec orc_apply(const orc_prep* p, int16_t vx, int16_t vy) {
+  double rx = vx - p->cx;
+  double ry = vy - p->cy;
+  double x = p->zcos * rx + p->zsin * ry + p->t->x + p->cx;
+  double y = -p->zsin * rx + p->zcos * ry + p->t->y + p->cy;
+  orc_vec r = { (int16_t)x, (int16_t)y };
+  return r;
+}
+
+static void orc_field_offset(const orc_trans* t, int W, int H, int fx, int fy,
                              int16_t* ox, int16_t* oy) {
-  double z = 1.0 + t[3] / 100.0;
-  double zcos = z * cos(t[2]);
-  double zsin = z * sin(t[2]);
-  double c_x = W / 2, c_y = H / 2;
-  double rx = fx - c_x, ry = fy - c_y;
-  double x = zcos * rx + zsin * ry + t[0] + c_x;
-  double y = -zsin * rx + zcos * ry + t[1] + c_y;
-  int16_t nx = (int16_t)x, ny = (int16_t)y;
-  *ox = (int16_t)(nx - fx);
-  *oy = (int16_t)(ny - fy);
+  orc_prep p = orc_prepare(t, W, H);
+  orc_vec n = orc_apply(&p, (int16_t)fx, (int16_t)fy);
+  *ox = (int16_t)(n.x - fx);
+  *oy = (int16_t)(n.y - fy);
+}
+
+/* offset of a field for the transform {x, y, alpha, zoom} (test hook) */
+void orc_offset(const double* t4, int W, int H, int fx, int fy, int16_t* ox, int16_t* oy) {
+  orc_trans t;
+  memset(&t, 0, sizeof(t));
+  t.x = t4[0];
+  t.y = t4[1];
+  t.alpha = t4[2];
+  t.zoom = t4[3];
+  orc_field_offset(&t, W, H, fx, fy, ox, oy);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -475,6 +526,16 @@ void orc_md_free(orc_md* md) {
   free(md);
 }
 
+/* (c0 + c1 + c2) / 3 as the reference's fast-math build evaluates it:
+   ((c0 + c1) + c2) times the double nearest 1/3 (pinned against the
+   reference by tests/test_oracle_pin.py) */
+__attribute__((optimize("no-fast-math"), noinline)) static double orc_mean3(double a, double b,
+                                                                             double c) {
+  double s = a + b;
+  s = s + c;
+  return s * (1.0 / 3.0);
+}
+
 static double orc_field_contrast(const orc_md* md, int fx, int fy, int size) {
   uint8_t mn, mx;
   if (md->planar) {
@@ -487,14 +548,14 @@ static double orc_field_contrast(const orc_md* md, int fx, int fy, int size) {
     orc_minmax(md->curr + ch, md->ls, fx, fy, size, md->bpp, &mn, &mx);
     c[ch] = orc_contrast_from_minmax(mn, mx);
   }
-  return (c[0] + c[1] + c[2]) / 3;
+  return orc_mean3(c[0], c[1], c[2]);
 }
 
 /* calcTransFields (src/motiondetect.c:752-807) for one field set; with
    use_offset the per-field search centre follows the transform t and fields
    whose search window would leave the frame are dropped
    (src/motiondetect.c:418-434) */
-static int orc_trans_fields(orc_md* md, const orc_fields* fs, int use_offset, const double* t,
+static int orc_trans_fields(orc_md* md, const orc_fields* fs, int use_offset, const orc_trans* t,
                             orc_lm* out) {
   double* con = (double*)malloc(sizeof(double) * fs->num);
   orc_ci* sel = (orc_ci*)malloc(sizeof(orc_ci) * (fs->num + 1));
@@ -552,9 +613,8 @@ int orc_md_frame(orc_md* md, const uint8_t* plane0, int linesize, orc_lm* out, i
     int nc = orc_trans_fields(md, &md->coarse, 0, NULL, coarse);
     int nf = 0;
     if (nc >= 1) {
-      double t[4];
-      orc_simple_transform(W, H, coarse, nc, t);
-      int nf2 = orc_trans_fields(md, &md->fine, 1, t, fine);
+      orc_trans t = orc_model(W, H, coarse, nc);
+      int nf2 = orc_trans_fields(md, &md->fine, 1, &t, fine);
       double* matches = (double*)malloc(sizeof(double) * nc);
       for (int i = 0; i < nc; i++) matches[i] = coarse[i].match;
       double meanMatch = orc_cleanmean(matches, nc, NULL, NULL);

@@ -109,6 +109,10 @@ void orc_md_free(orc_md* md);
    {x, y, alpha, zoom} */
 void orc_simple_transform(int width, int height, const orc_lm* lms, int n, double* out);
 
+/* fine-search offset of a field for the transform {x, y, alpha, zoom}
+   (src/motiondetect.c:418-427 with src/transformtype.c:158-209) */
+void orc_offset(const double* t4, int W, int H, int fx, int fy, int16_t* ox, int16_t* oy);
+
 /* cleanmean of src/transformtype.c:445-461 (sorts ds) */
 double orc_cleanmean(double* ds, int len, double* mn, double* mx);
 

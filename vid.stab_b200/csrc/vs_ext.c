@@ -168,3 +168,19 @@ int vsb_field_search_host(const uint8_t* curr, const uint8_t* prev, int width, i
   free(order);
   return rc == 0 ? VS_OK : VS_ERROR;
 }
+
+int vsb_set_kernel_timing(VSMotionDetect* md, int on) {
+  return vsbd_set_timing(vsb_md_device(md), on) == 0 ? VS_OK : VS_ERROR;
+}
+
+int vsb_kernel_times(const VSMotionDetect* md, double* ms, long* count) {
+  return vsbd_kernel_times(vsb_md_device(md), ms, count) == 0 ? VS_OK : VS_ERROR;
+}
+
+int vsb_sad_peak(int variant, double* byteops_per_s) {
+  return vsbd_sad_peak(variant, byteops_per_s) == 0 ? VS_OK : VS_ERROR;
+}
+
+void vsb_counters(long long* launches, long long* h2d_bytes, long long* d2h_bytes) {
+  vsbd_counters(launches, h2d_bytes, d2h_bytes);
+}

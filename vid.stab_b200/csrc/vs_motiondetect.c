@@ -434,6 +434,17 @@ static int select_fields(md_state* st, const VSMotionDetectFields* fs, const dou
   return nsel;
 }
 
+/* Mean of the three channel contrasts of a packed field
+   (src/motiondetect.c:374-376).  The reference's fast-math build evaluates
+   `(c0 + c1 + c2) / 3` as ((c0 + c1) + c2) times the double nearest 1/3;
+   that order is written out here in strict arithmetic so that no compiler
+   choice can change it. */
+double vsb_mean3(double a, double b, double c) {
+  double s = a + b;
+  s = s + c;
+  return s * (1.0 / 3.0);
+}
+
 /* Michelson contrast of one field from its 8-bit extremes
    (src/motiondetect.c:406; packed: mean over three channels, :374-376) */
 static void field_contrasts(const md_state* st, const uint8_t* mm, int n, double* out) {

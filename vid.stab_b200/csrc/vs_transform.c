@@ -210,10 +210,6 @@ VSArray localmotionsGetMatch(const LocalMotions* lms) {
   return m;
 }
 
-/* mean of the three channel contrasts of a packed field
-   (src/motiondetect.c:374-376) */
-double vsb_mean3(double a, double b, double c) { return (a + b + c) / 3; }
-
 /* src/boxblur.c:109-122: odd, at least 3, at most half the smaller frame
    dimension; below 2 nothing is blurred.  The requested size is unsigned
    there, so is the lower clamp. */

@@ -22,6 +22,7 @@
 #include <string.h>
 
 #include "vsb_device.h"
+#include "vsb_search.cuh"
 
 /* ------------------------------------------------------------------------ */
 /* error plumbing                                                            */
@@ -32,6 +33,19 @@ static void set_err(const char* what, cudaError_t e) {
   snprintf(g_err, sizeof(g_err), "%s: %s", what, cudaGetErrorString(e));
 }
 static void set_msg(const char* m) { snprintf(g_err, sizeof(g_err), "%s", m); }
+
+/* process-wide counters: kernels launched and bytes copied host<->device by
+   the per-frame path (read by benchmarks) */
+static unsigned long long g_nlaunch = 0, g_nh2d = 0, g_nd2h = 0;
+static void count_launches(long n) { __atomic_fetch_add(&g_nlaunch, (unsigned long long)n, __ATOMIC_RELAXED); }
+static void count_h2d(size_t b) { __atomic_fetch_add(&g_nh2d, (unsigned long long)b, __ATOMIC_RELAXED); }
+static void count_d2h(size_t b) { __atomic_fetch_add(&g_nd2h, (unsigned long long)b, __ATOMIC_RELAXED); }
+
+extern "C" void vsbd_counters(long long* launches, long long* h2d, long long* d2h) {
+  if (launches) *launches = (long long)__atomic_load_n(&g_nlaunch, __ATOMIC_RELAXED);
+  if (h2d) *h2d = (long long)__atomic_load_n(&g_nh2d, __ATOMIC_RELAXED);
+  if (d2h) *d2h = (long long)__atomic_load_n(&g_nd2h, __ATOMIC_RELAXED);
+}
 
 extern "C" const char* vsbd_error(void) { return g_err; }
 
@@ -100,11 +114,13 @@ __global__ void __launch_bounds__(256) k_blur(const uint8_t* __restrict__ src, i
   unsigned acc = 0;
   for (int k = 0; k < win; k++) acc += hor[rbeg + k][c];
   for (int r = rbeg; r < rbeg + BT_H / 2; r++) {
+    if (r > rbeg) { /* slide: rows [r, r + win) of hor feed output row r */
+      acc += hor[r + win - 1][c];
+      acc -= hor[r - 1][c];
+    }
     int gy = y0 + r;
     if (gy >= H) break;
     dst[(size_t)gy * dp + gx] = (uint8_t)blur_div(acc, dv);
-    acc += hor[r + win][c];
-    acc -= hor[r][c];
   }
 }
 
@@ -204,223 +220,15 @@ __global__ void __launch_bounds__(256) k_minmax(const uint8_t* __restrict__ img,
 }
 
 /* ------------------------------------------------------------------------ */
-/* SAD search                                                                */
-/* ------------------------------------------------------------------------ */
-
-struct DGeom {
-  int S, bpp, step, na, nb, ax0, by0, has_origin, nstages;
-  int st_r[VSBD_MAX_STAGES], st_h[VSBD_MAX_STAGES];
-  int limx, limy;
-  int rows_per_tile;
-  int maxq;                    /* largest refinement grid */
-  const int32_t* order;        /* rank of lattice point (a,b) at [b*na+a] */
-  const short2* point;         /* displacement of rank k */
-};
-
-/* packed 4 x u8 sum of absolute differences, accumulated */
-__device__ __forceinline__ unsigned sad4(unsigned a, unsigned b, unsigned c) {
-  unsigned d;
-  asm("vabsdiff4.u32.u32.u32.add %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
-  return d;
-}
-
-/* SAD of the staged field (rowW words per row, S rows) against the window
-   bytes starting at byte column cxb of P (row pitch WP). */
-__device__ __forceinline__ unsigned sad_window(const uint32_t* __restrict__ C, int rowW, int S,
-                                               const uint8_t* __restrict__ P, int WP, int cxb) {
-  unsigned acc = 0;
-  const int sh = (cxb & 3) << 3;
-  const int nq = rowW >> 2;
-  for (int r = 0; r < S; r++) {
-    const uint32_t* Pw = (const uint32_t*)(P + r * WP) + (cxb >> 2);
-    const uint4* C4 = (const uint4*)(C + r * rowW);
-    uint32_t lo = Pw[0];
-    for (int q = 0; q < nq; q++) {
-      uint4 c = C4[q];
-      uint32_t p1 = Pw[4 * q + 1], p2 = Pw[4 * q + 2], p3 = Pw[4 * q + 3], p4 = Pw[4 * q + 4];
-      acc = sad4(c.x, __funnelshift_r(lo, p1, sh), acc);
-      acc = sad4(c.y, __funnelshift_r(p1, p2, sh), acc);
-      acc = sad4(c.z, __funnelshift_r(p2, p3, sh), acc);
-      acc = sad4(c.w, __funnelshift_r(p3, p4, sh), acc);
-      lo = p4;
-    }
-  }
-  return acc;
-}
-
-/* SAD of the staged field against the previous frame in global memory at
-   byte column gxb, row gy0 (warp-cooperative: lanes take rows) */
-__device__ unsigned sad_global_warp(const uint32_t* __restrict__ C, int rowW, int S,
-                                    const uint8_t* __restrict__ prev, int pitch, int gxb,
-                                    int gy0, int lane) {
-  unsigned acc = 0;
-  const int sh = (gxb & 3) << 3;
-  for (int r = lane; r < S; r += 32) {
-    const uint32_t* Pw = (const uint32_t*)(prev + (size_t)(gy0 + r) * pitch) + (gxb >> 2);
-    const uint32_t* Cr = C + r * rowW;
-    uint32_t lo = Pw[0];
-    for (int w = 0; w < rowW; w++) {
-      uint32_t hi = Pw[w + 1];
-      acc = sad4(Cr[w], __funnelshift_r(lo, hi, sh), acc);
-      lo = hi;
-    }
-  }
-  return __reduce_add_sync(0xffffffffu, acc);
-}
-
-__device__ __forceinline__ unsigned long long warp_min64(unsigned long long v) {
-  for (int o = 16; o > 0; o >>= 1) {
-    unsigned long long t = __shfl_xor_sync(0xffffffffu, v, o);
-    v = t < v ? t : v;
-  }
-  return v;
-}
-
-/* grid: (tiles, items); 256 threads.  Dynamic shared memory:
-   [field S*rowB][window WH*WP][refinement SADs maxq*4] */
-__global__ void __launch_bounds__(256) k_search(const uint8_t* __restrict__ curr,
-                                                const uint8_t* __restrict__ prev, int pitch,
-                                                DGeom g, const vsbd_item* __restrict__ items,
-                                                unsigned long long* __restrict__ keys,
-                                                unsigned* __restrict__ tickets,
-                                                vsbd_result* __restrict__ res) {
-  extern __shared__ __align__(16) uint8_t sm[];
-  __shared__ unsigned long long red[8];
-  __shared__ int s_last, s_tx, s_ty;
-  __shared__ unsigned s_min;
-  const int item = blockIdx.y, tile = blockIdx.x;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  const vsbd_item it = items[item];
-  const int rowB = g.S * g.bpp, rowW = rowB >> 2;
-  uint32_t* C = (uint32_t*)sm;
-  const int b0 = tile * g.rows_per_tile;
-  const int nbt = min(g.rows_per_tile, g.nb - b0);
-  const int gx0 = (it.x - g.S / 2 + it.ox + g.ax0) * g.bpp;
-  const int gy0 = it.y - g.S / 2 + it.oy + g.by0 + b0 * g.step;
-  const int WWb = rowB + (g.na - 1) * g.step * g.bpp;
-  const int WH = g.S + (nbt - 1) * g.step;
-  const int gx0a = gx0 & ~15, e = gx0 - gx0a;
-  const int nvec = (e + WWb + 15) >> 4;
-  const int WP = (nvec + 1) << 4;
-  uint8_t* P = sm + g.S * rowB;
-  unsigned* qsad = (unsigned*)(P + (size_t)WH * WP);
-
-  /* the current field, re-aligned to word boundaries */
-  {
-    const int cx0 = (it.x - g.S / 2) * g.bpp, cy0 = it.y - g.S / 2;
-    const int sh = (cx0 & 3) << 3, cw0 = cx0 >> 2;
-    for (int i = threadIdx.x; i < g.S * rowW; i += blockDim.x) {
-      int r = i / rowW, w = i - r * rowW;
-      const uint32_t* s = (const uint32_t*)(curr + (size_t)(cy0 + r) * pitch) + cw0 + w;
-      C[i] = __funnelshift_r(s[0], s[1], sh);
-    }
-  }
-  /* the window of the previous frame this CTA's candidate rows touch */
-  for (int i = threadIdx.x; i < WH * nvec; i += blockDim.x) {
-    int r = i / nvec, v = i - r * nvec;
-    uint4 val = *(const uint4*)(prev + (size_t)(gy0 + r) * pitch + gx0a + (v << 4));
-    *(uint4*)(P + r * WP + (v << 4)) = val;
-  }
-  __syncthreads();
-
-  unsigned long long best = ~0ull;
-  const int ncand = g.na * nbt;
-  for (int c = threadIdx.x; c < ncand; c += blockDim.x) {
-    int bl = c / g.na, a = c - bl * g.na;
-    unsigned s = sad_window(C, rowW, g.S, P + bl * g.step * WP, WP, e + a * g.step * g.bpp);
-    unsigned long long key =
-        ((unsigned long long)s << 32) | (unsigned)g.order[(b0 + bl) * g.na + a];
-    best = key < best ? key : best;
-  }
-  best = warp_min64(best);
-  if (lane == 0) red[warp] = best;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int w = 1; w < nwarps; w++) best = red[w] < best ? red[w] : best;
-    atomicMin(&keys[item], best);
-    __threadfence();
-    unsigned t = atomicAdd(&tickets[item], 1u);
-    s_last = (t == gridDim.x - 1);
-  }
-  __syncthreads();
-  if (!s_last) return;
-  __threadfence();
-
-  /* last CTA of this item: origin candidate, refinement, range test */
-  if (threadIdx.x == 0) {
-    unsigned long long k = atomicAdd(&keys[item], 0ull);
-    short2 pt = g.point[(unsigned)(k & 0xffffffffu)];
-    s_min = (unsigned)(k >> 32);
-    s_tx = pt.x;
-    s_ty = pt.y;
-  }
-  __syncthreads();
-  const int fx0 = (it.x - g.S / 2 + it.ox) * g.bpp, fy0 = it.y - g.S / 2 + it.oy;
-  if (g.has_origin) {
-    if (warp == 0) {
-      unsigned s0 = sad_global_warp(C, rowW, g.S, prev, pitch, fx0, fy0, lane);
-      /* rank 0 precedes every lattice rank */
-      if (lane == 0 && s0 <= s_min) { s_min = s0; s_tx = 0; s_ty = 0; }
-    }
-    __syncthreads();
-  }
-  for (int st = 0; st < g.nstages; st++) {
-    const int r = g.st_r[st], h = g.st_h[st];
-    const int side = (2 * r) / h + 1, nq = side * side;
-    const int cx = s_tx, cy = s_ty;
-    for (int q = warp; q < nq; q += nwarps) {
-      int i = cx - r + (q / side) * h, j = cy - r + (q % side) * h;
-      unsigned s = 0xffffffffu;
-      if (!(i == cx && j == cy))
-        s = sad_global_warp(C, rowW, g.S, prev, pitch, fx0 + i * g.bpp, fy0 + j, lane);
-      if (lane == 0) qsad[q] = s;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      unsigned m = s_min;
-      int tx = cx, ty = cy;
-      for (int q = 0; q < nq; q++) {
-        int i = cx - r + (q / side) * h, j = cy - r + (q % side) * h;
-        if (i == cx && j == cy) continue;
-        if (qsad[q] < m) { m = qsad[q]; tx = i; ty = j; }
-      }
-      s_min = m;
-      s_tx = tx;
-      s_ty = ty;
-    }
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) {
-    vsbd_result o;
-    o.sad = s_min;
-    o.tx = (int16_t)s_tx;
-    o.ty = (int16_t)s_ty;
-    o.ok = !(abs(s_tx) >= g.limx || abs(s_ty) >= g.limy);
-    res[item] = o;
-    keys[item] = ~0ull;
-    tickets[item] = 0u;
-  }
-}
-
-/* ------------------------------------------------------------------------ */
-/* geometry upload                                                           */
+/* SAD search (kernels in vsb_search.cuh)                                    */
 /* ------------------------------------------------------------------------ */
 
 struct GeomDev {
   DGeom g;
   int32_t* d_order;
   short2* d_point;
-  int tiles;
   size_t smem;
 };
-
-static size_t search_smem(const DGeom& g, int rows_per_tile) {
-  int rowB = g.S * g.bpp;
-  int WWb = rowB + (g.na - 1) * g.step * g.bpp;
-  int WH = g.S + (rows_per_tile - 1) * g.step;
-  int WP = (((15 + WWb + 15) >> 4) + 1) << 4;
-  return (size_t)g.S * rowB + (size_t)WH * WP + (size_t)g.maxq * 4 + 16;
-}
 
 static int sm_count(void) {
   static int n = 0;
@@ -433,20 +241,127 @@ static int sm_count(void) {
   return n;
 }
 
-/* rows of the candidate lattice per CTA: enough CTAs for ~4 per SM, as long
-   as the window fits the shared-memory budget */
-static int pick_rows_per_tile(const DGeom& g, int nitems, int hint) {
-  int rpt = g.nb;
-  if (hint > 0) rpt = (g.nb + hint - 1) / hint;
-  else if (nitems > 0) {
-    int want = 4 * sm_count();
-    int tiles = (want + nitems - 1) / nitems;
-    if (tiles > g.nb) tiles = g.nb;
-    if (tiles < 1) tiles = 1;
-    rpt = (g.nb + tiles - 1) / tiles;
+/* largest dynamic shared memory one search CTA may request on this device
+   (the kernels' static shared memory counts against the opt-in limit) */
+static size_t search_smem_limit(void) {
+  static size_t lim = 0;
+  if (!lim) {
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    size_t stat = 0;
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, k_lattice<4>) == cudaSuccess) stat = fa.sharedSizeBytes;
+    if (cudaFuncGetAttributes(&fa, k_lattice<2>) == cudaSuccess && fa.sharedSizeBytes > stat)
+      stat = fa.sharedSizeBytes;
+    if (cudaFuncGetAttributes(&fa, k_lattice<8>) == cudaSuccess && fa.sharedSizeBytes > stat)
+      stat = fa.sharedSizeBytes;
+    lim = optin > 0 ? (size_t)optin - stat - 64 : 48 * 1024;
   }
-  while (rpt > 1 && search_smem(g, rpt) > 200 * 1024) rpt = (rpt + 1) / 2;
-  return rpt;
+  return lim;
+}
+
+/* registers per thread of the search kernel for TB rows per thread */
+static int lattice_regs(int TB) {
+  static int r[9] = { 0 };
+  if (TB < 1 || TB > 8) return 0;
+  if (!r[TB]) {
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaErrorInvalidValue;
+    if (TB == 2) e = cudaFuncGetAttributes(&fa, k_lattice<2>);
+    if (TB == 4) e = cudaFuncGetAttributes(&fa, k_lattice<4>);
+    if (TB == 8) e = cudaFuncGetAttributes(&fa, k_lattice<8>);
+    r[TB] = e == cudaSuccess ? fa.numRegs : 64;
+  }
+  return r[TB];
+}
+
+/* Candidate tile shapes (columns x rows of the lattice per CTA, rows per
+   thread, field strips) with their modelled time: SAD issue slots of the CTA
+   times the waves of CTAs the SMs can hold at once (shared memory, threads
+   and registers), with a penalty below 16 resident warps per SM, plus the
+   staging of the window.  Forced values (> 0) pin a dimension.  Returns the
+   number of candidates written (best first, at most cap). */
+struct TileCand {
+  double clk;
+  DGeom g;
+};
+
+static int tile_candidates(const DGeom& g, int nitems, int tb_force, int strip_force,
+                           int nab_force, int nbb_force, TileCand* out, int cap) {
+  const size_t lim = search_smem_limit();
+  const int sms = sm_count();
+  int n = 0;
+  const int tbs[3] = { 4, 2, 8 };
+  for (int ti = 0; ti < 3; ti++) {
+    int TB = tbs[ti];
+    if (tb_force > 0 && TB != tb_force) continue;
+    for (int ns = 1; ns <= 8; ns *= 2) {
+      if (strip_force > 0 && ns != strip_force) continue;
+      if (g.S % ns) continue;
+      int Rs = g.S / ns;
+      if (Rs < 4) continue;
+      for (int ka = 1; ka <= 16; ka++) {
+        int nab = (g.na + ka - 1) / ka;
+        if (nab_force > 0) nab = nab_force;
+        if (ka > 1 && nab_force <= 0 && nab == (g.na + ka - 2) / (ka - 1)) continue;
+        for (int m = 1; m * TB <= ((g.nb + TB - 1) / TB) * TB; m++) {
+          int nbb = m * TB;
+          if (nbb_force > 0) nbb = nbb_force;
+          if (nbb % TB) break;
+          DGeom t = g;
+          t.tb = TB;
+          t.nab = nab;
+          t.nbb = nbb;
+          t.nstrip = ns;
+          t.nta = (g.na + nab - 1) / nab;
+          t.ntb = (g.nb + nbb - 1) / nbb;
+          int threads = nab * (nbb / TB) * ns;
+          threads = (threads + 31) & ~31;
+          if (threads > 512 || threads < 32) {
+            if (nbb_force > 0) break;
+            continue;
+          }
+          t.threads = threads;
+          TileLayout L = tile_layout(t);
+          if (L.total > lim) {
+            if (nbb_force > 0) break;
+            continue;
+          }
+          long ctas = (long)nitems * t.nta * t.ntb;
+          int cps = (int)((228 * 1024) / (L.total + 1024));
+          if (2048 / threads < cps) cps = 2048 / threads;
+          int regs = lattice_regs(TB);
+          if (regs > 0 && 65536 / (threads * regs) < cps) cps = 65536 / (threads * regs);
+          if (cps > 32) cps = 32;
+          if (cps < 1) {
+            if (nbb_force > 0) break;
+            continue;
+          }
+          double eff = (double)Rs / (Rs + g.step * (TB - 1));
+          double work = (double)nab * nbb * g.S * L.rowW / eff; /* lane-SAD4 slots */
+          double warps = (double)cps * threads / 32.0;
+          double occ = warps >= 16 ? 1.0 : warps / 16.0;
+          long waves = (ctas + (long)sms * cps - 1) / ((long)sms * cps);
+          double clk = (double)waves * cps * (work / 64.0 / occ + (double)L.WH_alloc * L.WP / 32.0);
+          /* keep the cap best, sorted */
+          int pos = n < cap ? n : cap;
+          while (pos > 0 && out[pos - 1].clk > clk) {
+            if (pos < cap) out[pos] = out[pos - 1];
+            pos--;
+          }
+          if (pos < cap) {
+            out[pos].clk = clk;
+            out[pos].g = t;
+            if (n < cap) n++;
+          }
+          if (nbb_force > 0) break;
+        }
+        if (nab_force > 0) break;
+      }
+    }
+  }
+  return n;
 }
 
 static int geom_upload(const vsbd_geom* h, int nitems, int tiles_hint, GeomDev* out) {
@@ -484,10 +399,18 @@ static int geom_upload(const vsbd_geom* h, int nitems, int tiles_hint, GeomDev* 
   if (e1 != cudaSuccess || e2 != cudaSuccess) { set_err("geometry upload", e1 != cudaSuccess ? e1 : e2); return -1; }
   g.order = out->d_order;
   g.point = out->d_point;
-  g.rows_per_tile = pick_rows_per_tile(g, nitems, tiles_hint);
-  out->tiles = (g.nb + g.rows_per_tile - 1) / g.rows_per_tile;
-  out->smem = search_smem(g, g.rows_per_tile);
-  if (out->smem > 227 * 1024) { set_msg("search window exceeds shared memory"); return -1; }
+  int tb_f = 0, ns_f = 0, nab_f = 0, nbb_f = 0;
+  if (tiles_hint > 0) { /* test hook: tb*1000000 + strips*10000 + nab*100 + nbb */
+    tb_f = tiles_hint / 1000000;
+    ns_f = (tiles_hint / 10000) % 100;
+    nab_f = (tiles_hint / 100) % 100;
+    nbb_f = tiles_hint % 100;
+  }
+  TileCand cand[1];
+  int nc = tile_candidates(g, nitems > 0 ? nitems : 1, tb_f, ns_f, nab_f, nbb_f, cand, 1);
+  if (nc < 1) { set_msg("no search tiling fits in shared memory"); return -1; }
+  g = cand[0].g;
+  out->smem = tile_layout(g).total;
   return 0;
 }
 
@@ -498,18 +421,98 @@ static void geom_free(GeomDev* g) {
   g->d_point = NULL;
 }
 
+template <int TB>
+static int launch_lattice(const GeomDev& gd, const uint8_t* curr, const uint8_t* prev, int pitch,
+                          const vsbd_item* d_items, int n, unsigned long long* keys,
+                          unsigned* tickets, vsbd_result* d_res, cudaStream_t st) {
+  cudaError_t e = cudaFuncSetAttribute(k_lattice<TB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)gd.smem);
+  if (e != cudaSuccess) {
+    set_err("cudaFuncSetAttribute(k_lattice)", e);
+    return -1;
+  }
+  dim3 grid(gd.g.nta * gd.g.ntb, n);
+  k_lattice<TB><<<grid, gd.g.threads, gd.smem, st>>>(curr, prev, pitch, gd.g, d_items, keys, tickets,
+                                                     d_res);
+  return 1;
+}
+
 static int launch_search(const GeomDev& gd, const uint8_t* curr, const uint8_t* prev, int pitch,
                          const vsbd_item* d_items, int n, unsigned long long* keys,
                          unsigned* tickets, vsbd_result* d_res, cudaStream_t st) {
   if (n <= 0) return 0;
-  static int attr_done = 0;
-  if (!attr_done) {
-    cudaFuncSetAttribute(k_search, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-    attr_done = 1;
+  switch (gd.g.tb) {
+    case 2: return launch_lattice<2>(gd, curr, prev, pitch, d_items, n, keys, tickets, d_res, st);
+    case 4: return launch_lattice<4>(gd, curr, prev, pitch, d_items, n, keys, tickets, d_res, st);
+    case 8: return launch_lattice<8>(gd, curr, prev, pitch, d_items, n, keys, tickets, d_res, st);
   }
-  dim3 grid(gd.tiles, n);
-  k_search<<<grid, 256, gd.smem, st>>>(curr, prev, pitch, gd.g, d_items, keys, tickets, d_res);
-  return 1;
+  set_msg("unsupported rows-per-thread");
+  return -1;
+}
+
+/* Times the modelled best tilings of one field set on the detector's own
+   buffers and items and keeps the fastest.  The dense lattice does the same
+   work whatever the pixels hold, so the contents of the buffers do not matter.
+   Results are cached per (geometry, item count) for the process. */
+struct TuneEntry {
+  int S, bpp, step, na, nb, nstages, nitems;
+  DGeom g;
+};
+static TuneEntry g_tune[64];
+static int g_ntune = 0;
+
+static int autotune_tiling(GeomDev* gd, const uint8_t* curr, const uint8_t* prev, int pitch,
+                           const vsbd_item* d_items, int n, unsigned long long* keys,
+                           unsigned* tickets, vsbd_result* d_res, cudaStream_t st) {
+  if (n <= 0 || getenv("VSB_NO_AUTOTUNE")) return 0;
+  DGeom& g = gd->g;
+  for (int i = 0; i < g_ntune; i++) {
+    TuneEntry& e = g_tune[i];
+    if (e.S == g.S && e.bpp == g.bpp && e.step == g.step && e.na == g.na && e.nb == g.nb &&
+        e.nstages == g.nstages && e.nitems == n) {
+      DGeom t = e.g;
+      t.order = g.order;
+      t.point = g.point;
+      g = t;
+      gd->smem = tile_layout(g).total;
+      return 0;
+    }
+  }
+  TileCand cand[12];
+  int nc = tile_candidates(g, n, 0, 0, 0, 0, cand, 12);
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  float best_ms = 1e30f;
+  DGeom best = g;
+  for (int k = 0; k < nc; k++) {
+    GeomDev t = *gd;
+    t.g = cand[k].g;
+    t.smem = tile_layout(t.g).total;
+    if (launch_search(t, curr, prev, pitch, d_items, n, keys, tickets, d_res, st) < 0) continue;
+    cudaEventRecord(e0, st);
+    for (int rep = 0; rep < 3; rep++)
+      launch_search(t, curr, prev, pitch, d_items, n, keys, tickets, d_res, st);
+    cudaEventRecord(e1, st);
+    if (cudaEventSynchronize(e1) != cudaSuccess) break;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = t.g;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  CK(cudaGetLastError());
+  g = best;
+  gd->smem = tile_layout(g).total;
+  if (g_ntune < 64) {
+    TuneEntry& e = g_tune[g_ntune++];
+    e.S = g.S; e.bpp = g.bpp; e.step = g.step; e.na = g.na; e.nb = g.nb;
+    e.nstages = g.nstages; e.nitems = n; e.g = g;
+  }
+  return 0;
 }
 
 /* ------------------------------------------------------------------------ */
@@ -536,7 +539,54 @@ struct vsbd_ctx {
   vsbd_item* h_items;           /* pinned staging of fine items */
   size_t off_coarse, off_fine, out_bytes;
   long launches;
+  int timing;                   /* record CUDA events around each kernel */
+  cudaEvent_t ev[VSBD_NKT][2];
+  double kt_ms[VSBD_NKT];
+  long kt_n[VSBD_NKT];
+  int kt_pending[VSBD_NKT];
 };
+
+/* per-kernel event pairs on the detector's stream; read after the sync */
+static void kt_begin(vsbd_ctx* c, int k) {
+  if (c->timing) cudaEventRecord(c->ev[k][0], c->st);
+}
+static void kt_end(vsbd_ctx* c, int k) {
+  if (c->timing) {
+    cudaEventRecord(c->ev[k][1], c->st);
+    c->kt_pending[k] = 1;
+  }
+}
+static void kt_collect(vsbd_ctx* c) {
+  if (!c->timing) return;
+  for (int k = 0; k < VSBD_NKT; k++)
+    if (c->kt_pending[k]) {
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, c->ev[k][0], c->ev[k][1]) == cudaSuccess) {
+        c->kt_ms[k] += ms;
+        c->kt_n[k]++;
+      }
+      c->kt_pending[k] = 0;
+    }
+}
+
+extern "C" int vsbd_set_timing(vsbd_ctx* c, int on) {
+  if (!c) return -1;
+  CK(cudaSetDevice(c->dev));
+  if (on && !c->ev[0][0])
+    for (int k = 0; k < VSBD_NKT; k++) {
+      CK(cudaEventCreate(&c->ev[k][0]));
+      CK(cudaEventCreate(&c->ev[k][1]));
+    }
+  c->timing = on;
+  for (int k = 0; k < VSBD_NKT; k++) { c->kt_ms[k] = 0; c->kt_n[k] = 0; c->kt_pending[k] = 0; }
+  return 0;
+}
+
+extern "C" int vsbd_kernel_times(const vsbd_ctx* c, double* ms, long* n) {
+  if (!c) return -1;
+  for (int k = 0; k < VSBD_NKT; k++) { ms[k] = c->kt_ms[k]; n[k] = c->kt_n[k]; }
+  return 0;
+}
 
 static size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
 
@@ -550,6 +600,8 @@ extern "C" void vsbd_destroy(vsbd_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->dev);
   if (c->st) cudaStreamSynchronize(c->st);
+  for (int k = 0; k < VSBD_NKT; k++)
+    if (c->ev[k][0]) { cudaEventDestroy(c->ev[k][0]); cudaEventDestroy(c->ev[k][1]); }
   cudaFree(c->d_raw);
   cudaFree(c->d_tmp);
   cudaFree(c->d_buf[0]);
@@ -619,6 +671,22 @@ extern "C" int vsbd_create(vsbd_ctx** out, int W, int H, int bpp, int blur_size,
   c->out_bytes = c->off_fine + align16(sizeof(vsbd_result) * (nf + 1));
   CKC(cudaMalloc(&c->d_out, c->out_bytes));
   CKC(cudaMallocHost(&c->h_out, c->out_bytes));
+  /* fine items for tuning: every fine field without offset */
+  {
+    vsbd_item* it = (vsbd_item*)malloc(sizeof(vsbd_item) * (nf + 1));
+    for (int i = 0; i < nf; i++) { it[i].x = fx[i]; it[i].y = fy[i]; it[i].ox = 0; it[i].oy = 0; }
+    cudaError_t e3 = cudaMemcpy(c->d_fitems, it, sizeof(vsbd_item) * nf, cudaMemcpyHostToDevice);
+    free(it);
+    CKC(e3);
+  }
+  if (autotune_tiling(&c->gc, c->d_buf[0], c->d_buf[1], c->pitch, c->d_citems, nc, c->d_keys,
+                      c->d_tickets, (vsbd_result*)(c->d_out + c->off_coarse), c->st) != 0 ||
+      autotune_tiling(&c->gf, c->d_buf[0], c->d_buf[1], c->pitch, c->d_fitems, nf, c->d_keys + nc,
+                      c->d_tickets + nc, (vsbd_result*)(c->d_out + c->off_fine), c->st) != 0) {
+    vsbd_destroy(c);
+    return -1;
+  }
+  CKC(cudaStreamSynchronize(c->st));
 #undef CKC
   *out = c;
   return 0;
@@ -637,32 +705,48 @@ extern "C" int vsbd_stage_a(vsbd_ctx* c, const uint8_t* host, int linesize, cons
     if (!dev) {
       CK(cudaMemcpy2DAsync(c->d_raw, c->pitch, host, linesize, rowbytes, c->H,
                            cudaMemcpyHostToDevice, c->st));
+      count_h2d((size_t)rowbytes * c->H);
       src = c->d_raw;
       sp = c->pitch;
     }
-    c->launches += launch_blur(src, sp, cur, c->pitch, c->W, c->H, c->blur, c->d_tmp, c->pitch, c->st);
+    kt_begin(c, VSBD_KT_BLUR);
+    { int nb = launch_blur(src, sp, cur, c->pitch, c->W, c->H, c->blur, c->d_tmp, c->pitch, c->st); c->launches += nb; count_launches(nb); }
+    kt_end(c, VSBD_KT_BLUR);
     CK(cudaGetLastError());
   } else {
     if (dev)
       CK(cudaMemcpy2DAsync(cur, c->pitch, dev, pitch, rowbytes, c->H, cudaMemcpyDeviceToDevice, c->st));
-    else
+    else {
       CK(cudaMemcpy2DAsync(cur, c->pitch, host, linesize, rowbytes, c->H, cudaMemcpyHostToDevice, c->st));
+      count_h2d((size_t)rowbytes * c->H);
+    }
   }
   if (search) {
     int S = c->gc.g.S;
+    kt_begin(c, VSBD_KT_MINMAX);
     k_minmax<<<c->nc, 256, 0, c->st>>>(cur, c->pitch, c->d_xy, c->d_xy + c->nc, S, c->bpp, c->nch, c->d_out);
     c->launches++;
+    count_launches(1);
     if (c->nf > 0) {
       k_minmax<<<c->nf, 256, 0, c->st>>>(cur, c->pitch, c->d_xy + 2 * c->nc, c->d_xy + 2 * c->nc + c->nf,
                                          c->gf.g.S, c->bpp, c->nch, c->d_out + (size_t)c->nc * c->nch * 2);
       c->launches++;
+      count_launches(1);
     }
-    c->launches += launch_search(c->gc, cur, prv, c->pitch, c->d_citems, c->nc, c->d_keys, c->d_tickets,
-                                 (vsbd_result*)(c->d_out + c->off_coarse), c->st);
+    kt_end(c, VSBD_KT_MINMAX);
+    kt_begin(c, VSBD_KT_COARSE);
+    int nl = launch_search(c->gc, cur, prv, c->pitch, c->d_citems, c->nc, c->d_keys, c->d_tickets,
+                           (vsbd_result*)(c->d_out + c->off_coarse), c->st);
+    if (nl < 0) return -1;
+    c->launches += nl;
+    count_launches(nl);
+    kt_end(c, VSBD_KT_COARSE);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(c->h_out, c->d_out, c->off_fine, cudaMemcpyDeviceToHost, c->st));
+    count_d2h(c->off_fine);
   }
   CK(cudaStreamSynchronize(c->st));
+  kt_collect(c);
   if (minmax) *minmax = c->h_out;
   if (coarse) *coarse = (const vsbd_result*)(c->h_out + c->off_coarse);
   return 0;
@@ -675,14 +759,22 @@ extern "C" int vsbd_stage_b(vsbd_ctx* c, const vsbd_item* items, int n, const vs
   if (n <= 0) return 0;
   memcpy(c->h_items, items, sizeof(vsbd_item) * n);
   CK(cudaMemcpyAsync(c->d_fitems, c->h_items, sizeof(vsbd_item) * n, cudaMemcpyHostToDevice, c->st));
+  count_h2d(sizeof(vsbd_item) * n);
   uint8_t* cur = c->d_buf[c->cur];
   uint8_t* prv = c->d_buf[c->cur ^ 1];
-  c->launches += launch_search(c->gf, cur, prv, c->pitch, c->d_fitems, n, c->d_keys + c->nc,
-                               c->d_tickets + c->nc, (vsbd_result*)(c->d_out + c->off_fine), c->st);
+  kt_begin(c, VSBD_KT_FINE);
+  int nl = launch_search(c->gf, cur, prv, c->pitch, c->d_fitems, n, c->d_keys + c->nc,
+                         c->d_tickets + c->nc, (vsbd_result*)(c->d_out + c->off_fine), c->st);
+  if (nl < 0) return -1;
+  c->launches += nl;
+  count_launches(nl);
+  kt_end(c, VSBD_KT_FINE);
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(c->h_out + c->off_fine, c->d_out + c->off_fine, sizeof(vsbd_result) * n,
                      cudaMemcpyDeviceToHost, c->st));
+  count_d2h(sizeof(vsbd_result) * n);
   CK(cudaStreamSynchronize(c->st));
+  kt_collect(c);
   return 0;
 }
 
@@ -772,7 +864,7 @@ extern "C" int vsbd_search_host(const uint8_t* curr, const uint8_t* prev, int W,
   cudaMemcpy2D(d_c, pitch, curr, (size_t)W * bpp, (size_t)W * bpp, H, cudaMemcpyHostToDevice);
   cudaMemcpy2D(d_p, pitch, prev, (size_t)W * bpp, (size_t)W * bpp, H, cudaMemcpyHostToDevice);
   cudaMemcpy(d_items, items, sizeof(vsbd_item) * n, cudaMemcpyHostToDevice);
-  launch_search(gd, d_c, d_p, pitch, d_items, n, d_keys, d_tk, d_res, 0);
+  if (launch_search(gd, d_c, d_p, pitch, d_items, n, d_keys, d_tk, d_res, 0) < 0) goto done;
   if ((e = cudaGetLastError()) != cudaSuccess) { set_err("k_search", e); goto done; }
   if ((e = cudaMemcpy(out, d_res, sizeof(vsbd_result) * n, cudaMemcpyDeviceToHost)) != cudaSuccess) { set_err("download", e); goto done; }
   rc = 0;
@@ -785,4 +877,61 @@ done:
   cudaFree(d_keys);
   cudaFree(d_tk);
   return rc;
+}
+
+/* ------------------------------------------------------------------------ */
+/* packed-SAD throughput probe: register-only chains of one SAD formulation  */
+/* ------------------------------------------------------------------------ */
+
+template <int V>
+__device__ __forceinline__ unsigned sad_variant(unsigned a, unsigned b, unsigned c) {
+  if (V == 0) return sad4(a, b, c);
+  if (V == 1) return __vsadu4(a, b) + c;
+  return __dp4a(__vabsdiffu4(a, b), 0x01010101u, c);
+}
+
+template <int V>
+__global__ void __launch_bounds__(256) k_sad_peak(unsigned* out, int iters, unsigned seed) {
+  unsigned a[8], acc[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    a[k] = seed * (unsigned)(k + 1) + threadIdx.x * 0x9e3779b9u;
+    acc[k] = a[k] ^ 0x5a5a5a5au;
+  }
+  for (int i = 0; i < iters; i++) {
+#pragma unroll
+    for (int k = 0; k < 8; k++) acc[k] = sad_variant<V>(a[k], acc[k], acc[k]);
+  }
+  unsigned s = 0;
+#pragma unroll
+  for (int k = 0; k < 8; k++) s += acc[k];
+  out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+/* byte absolute differences per second of one SAD formulation (variant 0:
+   vabsdiff4 with accumulate, 1: __vsadu4 + add, 2: __vabsdiffu4 + dp4a) */
+extern "C" int vsbd_sad_peak(int variant, double* byteops_per_s) {
+  int blocks = sm_count() * 8, threads = 256, iters = 8192;
+  unsigned* d = NULL;
+  cudaEvent_t e0, e1;
+  CK(cudaMalloc(&d, sizeof(unsigned) * blocks * threads));
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  float best = 1e30f;
+  for (int rep = 0; rep < 4; rep++) {
+    cudaEventRecord(e0);
+    if (variant == 0) k_sad_peak<0><<<blocks, threads>>>(d, iters, 12345u + rep);
+    else if (variant == 1) k_sad_peak<1><<<blocks, threads>>>(d, iters, 12345u + rep);
+    else k_sad_peak<2><<<blocks, threads>>>(d, iters, 12345u + rep);
+    cudaEventRecord(e1);
+    CK(cudaEventSynchronize(e1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (rep > 0 && ms < best) best = ms;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(d);
+  *byteops_per_s = (double)blocks * threads * iters * 8.0 * 4.0 / (best * 1e-3);
+  return 0;
 }

@@ -76,6 +76,22 @@ void vsbd_commit_prev(vsbd_ctx* c);
 /* Kernel launches issued on behalf of this detector so far. */
 long vsbd_launches(const vsbd_ctx* c);
 
+/* per-kernel CUDA-event timing (indices VSBD_KT_*) */
+#define VSBD_KT_BLUR 0
+#define VSBD_KT_MINMAX 1
+#define VSBD_KT_COARSE 2
+#define VSBD_KT_FINE 3
+#define VSBD_NKT 4
+int vsbd_set_timing(vsbd_ctx* c, int on);
+int vsbd_kernel_times(const vsbd_ctx* c, double* ms, long* n);
+
+/* byte-absdiff throughput of a register-only SAD loop (see vsb_device.cu) */
+int vsbd_sad_peak(int variant, double* byteops_per_s);
+
+/* process-wide totals: kernel launches, host-to-device and device-to-host
+   bytes of the per-frame path */
+void vsbd_counters(long long* launches, long long* h2d, long long* d2h);
+
 /* Message of the last failure on this thread. */
 const char* vsbd_error(void);
 

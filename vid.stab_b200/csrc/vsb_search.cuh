@@ -1,0 +1,402 @@
+/*
+ * vsb_search.cuh -- the per-field SAD search of the detect pass for sm_100a
+ * (src/motiondetect.c:439-586 planar spiral, :591-660 packed raster of the
+ * reference), shared by the per-stream and the batched paths.
+ *
+ * Work split.  A field's candidate displacements form a lattice
+ * (a, b) -> (ax0 + a*step, by0 + b*step).  One CTA takes a tile of
+ * nab x nbb lattice points of one field and stages, once, the field of the
+ * current frame and the window of the previous frame those candidates
+ * touch.  A thread owns one lattice column a and TB consecutive lattice
+ * rows b, and one horizontal strip of the field's rows.  It walks the rows
+ * of the window: each previous-frame row it loads serves TB candidates at
+ * once (against TB different field rows, which are shared by the whole warp
+ * and so read as broadcasts).  Strips are summed in shared memory.
+ *
+ * Every candidate gets its FULL sum of absolute differences (the reference
+ * stops early once a row exceeds the running minimum, which never changes
+ * which candidate wins: `error < minerror` only).  The winner is the lowest
+ * (SAD, rank) pair, where rank is the candidate's position in the
+ * reference's visiting order, so equal SADs resolve exactly as the
+ * reference's strict `<` scan does.  CTAs of a field fold their best pair
+ * into one 64-bit atomicMin; the last CTA of the field (ticket counter) runs
+ * the dependent refinement rounds around the winner and the range test, and
+ * resets the field's key and ticket for the next launch.
+ */
+#ifndef VSB_SEARCH_CUH
+#define VSB_SEARCH_CUH
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "vsb_device.h"
+
+struct DGeom {
+  int S, bpp, step, na, nb, ax0, by0, has_origin, nstages;
+  int st_r[VSBD_MAX_STAGES], st_h[VSBD_MAX_STAGES];
+  int limx, limy;
+  int maxq;             /* largest refinement grid */
+  const int32_t* order; /* rank of lattice point (a,b) at [b*na + a] */
+  const short2* point;  /* displacement of rank k */
+  /* tiling, chosen on the host */
+  int tb;               /* lattice rows per thread (the kernel's template value) */
+  int nab, nbb;         /* lattice columns / rows per tile (nbb a multiple of tb) */
+  int nta, ntb;         /* tiles along a / along b */
+  int nstrip;           /* field rows split into this many strips */
+  int threads;          /* block size */
+};
+
+/* packed 4 x u8 sum of absolute differences, accumulated */
+__device__ __forceinline__ unsigned sad4(unsigned a, unsigned b, unsigned c) {
+  unsigned d;
+  asm("vabsdiff4.u32.u32.u32.add %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+  return d;
+}
+
+__device__ __forceinline__ unsigned long long warp_min64(unsigned long long v) {
+  for (int o = 16; o > 0; o >>= 1) {
+    unsigned long long t = __shfl_xor_sync(0xffffffffu, v, o);
+    v = t < v ? t : v;
+  }
+  return v;
+}
+
+/* shared-memory layout of one tile (bytes) */
+struct TileLayout {
+  int rowB, rowW, nq;
+  int WP, WH_alloc;  /* previous-frame window: row pitch, rows */
+  int RP, RH;        /* refinement window: row pitch (bytes), rows */
+  int FP;            /* row pitch of the staged current-field rows */
+  size_t off_P, off_part, off_q, total;
+};
+
+/* total reach of the refinement rounds around the lattice winner */
+__host__ __device__ inline int refine_reach(const DGeom& g) {
+  int R = 0;
+  for (int k = 0; k < g.nstages; k++) R += g.st_r[k];
+  return R;
+}
+
+__host__ __device__ inline TileLayout tile_layout(const DGeom& g) {
+  TileLayout L;
+  L.rowB = g.S * g.bpp;
+  L.rowW = L.rowB >> 2;
+  L.nq = L.rowW >> 2;
+  int wwb = L.rowB + (g.nab - 1) * g.step * g.bpp;
+  L.WP = (((15 + wwb + 15) >> 4) + 1) << 4;
+  L.WH_alloc = g.S + (g.nbb - 1) * g.step;
+  int R = refine_reach(g);
+  L.RH = g.S + 2 * R;
+  L.RP = ((3 + L.rowB + 2 * R * g.bpp + 8 + 15) >> 4) << 4;
+  L.FP = ((L.rowB + 15 + 15) >> 4 << 4) + 16;
+  L.off_P = (size_t)g.S * L.rowB;
+  size_t parea = (size_t)L.WH_alloc * L.WP;
+  size_t rarea = (size_t)L.RH * L.RP + 16;
+  size_t farea = (size_t)g.S * L.FP;
+  if (rarea > parea) parea = rarea;
+  if (farea > parea) parea = farea;
+  L.off_part = L.off_P + parea;
+  int G = g.nbb / g.tb;
+  L.off_q = L.off_part + (size_t)(g.nstrip > 1 ? g.nstrip - 1 : 0) * G * g.tb * g.nab * 4;
+  L.total = L.off_q + (size_t)g.maxq * 4 + 16;
+  return L;
+}
+
+/* SAD of the staged field C (rowW words per row) against rows of a
+   row-major byte buffer whose matching field starts at byte column bx
+   (any alignment) of row row0; lanes take field rows, the warp sums */
+__device__ __forceinline__ unsigned sad_rows_warp(const uint32_t* __restrict__ C, int rowW, int S,
+                                                  const uint8_t* __restrict__ base, size_t pitch,
+                                                  int bx, int row0, int lane) {
+  unsigned acc = 0;
+  const int sh = (bx & 3) << 3;
+  for (int r = lane; r < S; r += 32) {
+    const uint32_t* Pw = (const uint32_t*)(base + (size_t)(row0 + r) * pitch) + (bx >> 2);
+    const uint32_t* Cr = C + r * rowW;
+    uint32_t lo = Pw[0];
+    for (int w = 0; w < rowW; w++) {
+      uint32_t hi = Pw[w + 1];
+      acc = sad4(Cr[w], __funnelshift_r(lo, hi, sh), acc);
+      lo = hi;
+    }
+  }
+  return __reduce_add_sync(0xffffffffu, acc);
+}
+
+/* Last CTA of an item: origin candidate (raster scans), refinement rounds
+   (i outer, j inner, centre skipped, strict <), range test, reset.  The
+   window the rounds can reach (the field plus the sum of the round radii on
+   every side) is staged in shared memory first. */
+__device__ void refine_and_store(const DGeom& g, const TileLayout& L, const vsbd_item& it,
+                                 const uint32_t* C, uint8_t* rwin, const uint8_t* __restrict__ prev,
+                                 int pitch, unsigned long long* keys, unsigned* tickets,
+                                 vsbd_result* res, int item, unsigned* qsad) {
+  __shared__ int s_tx, s_ty;
+  __shared__ unsigned s_min;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  if (threadIdx.x == 0) {
+    unsigned long long k = atomicAdd(&keys[item], 0ull);
+    short2 pt = g.point[(unsigned)(k & 0xffffffffu)];
+    s_min = (unsigned)(k >> 32);
+    s_tx = pt.x;
+    s_ty = pt.y;
+  }
+  __syncthreads();
+  const int fx0 = (it.x - g.S / 2 + it.ox) * g.bpp, fy0 = it.y - g.S / 2 + it.oy;
+  if (g.has_origin) {
+    if (warp == 0) {
+      unsigned s0 = sad_rows_warp(C, L.rowW, g.S, prev, (size_t)pitch, fx0, fy0, lane);
+      if (lane == 0 && s0 <= s_min) { /* rank 0 precedes every lattice rank */
+        s_min = s0;
+        s_tx = 0;
+        s_ty = 0;
+      }
+    }
+    __syncthreads();
+  }
+  if (g.nstages > 0) {
+    const int R = refine_reach(g);
+    const int cx0 = s_tx, cy0 = s_ty;
+    const int wx = fx0 + (cx0 - R) * g.bpp, wy = fy0 + cy0 - R;
+    const int wxa = wx & ~3, off = wx - wxa;
+    const int nw = L.RP >> 2;
+    for (int i = threadIdx.x; i < L.RH * nw; i += blockDim.x) {
+      int r = i / nw, w = i - r * nw;
+      ((uint32_t*)rwin)[i] = *((const uint32_t*)(prev + (size_t)(wy + r) * pitch + wxa) + w);
+    }
+    __syncthreads();
+    for (int st = 0; st < g.nstages; st++) {
+      const int r = g.st_r[st], h = g.st_h[st];
+      const int side = (2 * r) / h + 1, nq = side * side;
+      const int cx = s_tx, cy = s_ty;
+      for (int q = warp; q < nq; q += nwarps) {
+        int i = cx - r + (q / side) * h, j = cy - r + (q % side) * h;
+        unsigned sd = 0xffffffffu;
+        if (!(i == cx && j == cy))
+          sd = sad_rows_warp(C, L.rowW, g.S, rwin, (size_t)L.RP, off + (i - cx0 + R) * g.bpp,
+                             j - cy0 + R, lane);
+        if (lane == 0) qsad[q] = sd;
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        unsigned m = s_min;
+        int tx = cx, ty = cy;
+        for (int q = 0; q < nq; q++) {
+          int i = cx - r + (q / side) * h, j = cy - r + (q % side) * h;
+          if (i == cx && j == cy) continue;
+          if (qsad[q] < m) {
+            m = qsad[q];
+            tx = i;
+            ty = j;
+          }
+        }
+        s_min = m;
+        s_tx = tx;
+        s_ty = ty;
+      }
+      __syncthreads();
+    }
+  }
+  if (threadIdx.x == 0) {
+    vsbd_result o;
+    o.sad = s_min;
+    o.tx = (int16_t)s_tx;
+    o.ty = (int16_t)s_ty;
+    o.ok = !(abs(s_tx) >= g.limx || abs(s_ty) >= g.limy);
+    res[item] = o;
+    keys[item] = ~0ull;
+    tickets[item] = 0u;
+  }
+}
+
+/* Rows [rb, re) of one thread's walk with candidates JLO..JHI of its TB all
+   active: per window row the row's words are loaded once, aligned to the
+   thread's column by funnel shifts, and every active candidate j adds the
+   row's SAD against its own field row rho - step*j (a warp-wide broadcast).
+   No condition inside, so the accumulation chains interleave. */
+template <int TB, int JLO, int JHI>
+__device__ __forceinline__ void rows_active(unsigned (&acc)[TB], int rb, int re, int step,
+                                            const uint8_t* __restrict__ Pb, int WP, int sh,
+                                            const uint4* __restrict__ C4, int nq) {
+  for (int rho = rb; rho < re; rho++) {
+    const uint32_t* Pw = (const uint32_t*)(Pb + rho * WP);
+    const uint4* Cj[TB];
+#pragma unroll
+    for (int j = JLO; j <= JHI; j++) Cj[j] = C4 + (rho - step * j) * nq;
+    uint32_t lo = Pw[0];
+    for (int q = 0; q < nq; q++) {
+      uint32_t p1 = Pw[4 * q + 1], p2 = Pw[4 * q + 2], p3 = Pw[4 * q + 3], p4 = Pw[4 * q + 4];
+      uint32_t w0 = __funnelshift_r(lo, p1, sh), w1 = __funnelshift_r(p1, p2, sh);
+      uint32_t w2 = __funnelshift_r(p2, p3, sh), w3 = __funnelshift_r(p3, p4, sh);
+      lo = p4;
+#pragma unroll
+      for (int j = JLO; j <= JHI; j++) {
+        uint4 c = Cj[j][q];
+        acc[j] = sad4(c.x, w0, acc[j]);
+        acc[j] = sad4(c.y, w1, acc[j]);
+        acc[j] = sad4(c.z, w2, acc[j]);
+        acc[j] = sad4(c.w, w3, acc[j]);
+      }
+    }
+  }
+}
+
+/* one segment of rows with a constant active range [jlo, jhi]: a uniform
+   switch to the body compiled for that range */
+template <int TB>
+__device__ __forceinline__ void rows_segment(unsigned (&acc)[TB], int jlo, int jhi, int rb, int re,
+                                             int step, const uint8_t* Pb, int WP, int sh,
+                                             const uint4* C4, int nq) {
+#define VSB_SEG(L, H)                                                           \
+  if (jlo == L && jhi == H) {                                                   \
+    rows_active<TB, L, H>(acc, rb, re, step, Pb, WP, sh, C4, nq);               \
+    return;                                                                     \
+  }
+  if constexpr (TB == 2) {
+    VSB_SEG(0, 0) VSB_SEG(0, 1) VSB_SEG(1, 1)
+  } else if constexpr (TB == 4) {
+    VSB_SEG(0, 0) VSB_SEG(0, 1) VSB_SEG(0, 2) VSB_SEG(0, 3)
+    VSB_SEG(1, 1) VSB_SEG(1, 2) VSB_SEG(1, 3)
+    VSB_SEG(2, 2) VSB_SEG(2, 3)
+    VSB_SEG(3, 3)
+  } else if constexpr (TB == 8) {
+    VSB_SEG(0, 0) VSB_SEG(0, 1) VSB_SEG(0, 2) VSB_SEG(0, 3) VSB_SEG(0, 4) VSB_SEG(0, 5)
+    VSB_SEG(0, 6) VSB_SEG(0, 7) VSB_SEG(1, 1) VSB_SEG(1, 2) VSB_SEG(1, 3) VSB_SEG(1, 4)
+    VSB_SEG(1, 5) VSB_SEG(1, 6) VSB_SEG(1, 7) VSB_SEG(2, 2) VSB_SEG(2, 3) VSB_SEG(2, 4)
+    VSB_SEG(2, 5) VSB_SEG(2, 6) VSB_SEG(2, 7) VSB_SEG(3, 3) VSB_SEG(3, 4) VSB_SEG(3, 5)
+    VSB_SEG(3, 6) VSB_SEG(3, 7) VSB_SEG(4, 4) VSB_SEG(4, 5) VSB_SEG(4, 6) VSB_SEG(4, 7)
+    VSB_SEG(5, 5) VSB_SEG(5, 6) VSB_SEG(5, 7) VSB_SEG(6, 6) VSB_SEG(6, 7) VSB_SEG(7, 7)
+  }
+#undef VSB_SEG
+}
+
+/* grid (nta*ntb, items); block g.threads; dynamic smem tile_layout(g).total */
+template <int TB>
+__global__ void __launch_bounds__(512, 1) k_lattice(const uint8_t* __restrict__ curr,
+                                                  const uint8_t* __restrict__ prev, int pitch,
+                                                  DGeom g, const vsbd_item* __restrict__ items,
+                                                  unsigned long long* __restrict__ keys,
+                                                  unsigned* __restrict__ tickets,
+                                                  vsbd_result* __restrict__ res) {
+  extern __shared__ __align__(16) uint8_t sm[];
+  __shared__ unsigned long long red[32];
+  __shared__ int s_last;
+  const TileLayout L = tile_layout(g);
+  const int item = blockIdx.y;
+  const int tbi = blockIdx.x / g.nta, tai = blockIdx.x - tbi * g.nta;
+  const vsbd_item it = items[item];
+  const int a0 = tai * g.nab, b0 = tbi * g.nbb;
+  const int na_t = min(g.nab, g.na - a0), nb_t = min(g.nbb, g.nb - b0);
+  const int G = g.nbb / TB;
+  const int Rs = g.S / g.nstrip;
+  uint32_t* C = (uint32_t*)sm; /* the current field, rowB bytes per row */
+  uint8_t* P = sm + L.off_P;
+  unsigned* part = (unsigned*)(sm + L.off_part);
+  unsigned* qsad = (unsigned*)(sm + L.off_q);
+
+  /* the current field: rows staged with 16-byte loads in the (not yet used)
+     window space, then re-aligned to word boundaries */
+  {
+    const int cx0 = (it.x - g.S / 2) * g.bpp, cy0 = it.y - g.S / 2;
+    const int cx0a = cx0 & ~15, ce = cx0 - cx0a;
+    const int nv = (ce + L.rowB + 15) >> 4;
+    for (int i = threadIdx.x; i < g.S * nv; i += blockDim.x) {
+      int r = i / nv, v = i - r * nv;
+      *(uint4*)(P + r * L.FP + (v << 4)) =
+          *(const uint4*)(curr + (size_t)(cy0 + r) * pitch + cx0a + (v << 4));
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < g.S * L.rowW; i += blockDim.x) {
+      int r = i / L.rowW, w = i - r * L.rowW;
+      const uint32_t* sw = (const uint32_t*)(P + r * L.FP) + (ce >> 2) + w;
+      C[i] = __funnelshift_r(sw[0], sw[1], (ce & 3) << 3);
+    }
+    __syncthreads();
+  }
+  /* the rows of the previous frame this tile's candidates touch */
+  const int gx0 = (it.x - g.S / 2 + it.ox + g.ax0 + a0 * g.step) * g.bpp;
+  const int gy0 = it.y - g.S / 2 + it.oy + g.by0 + b0 * g.step;
+  const int gx0a = gx0 & ~15, e = gx0 - gx0a;
+  {
+    const int wwb = L.rowB + (na_t - 1) * g.step * g.bpp;
+    const int wh = g.S + (nb_t - 1) * g.step;
+    const int nvec = (e + wwb + 15) >> 4;
+    for (int i = threadIdx.x; i < wh * nvec; i += blockDim.x) {
+      int r = i / nvec, v = i - r * nvec;
+      *(uint4*)(P + r * L.WP + (v << 4)) =
+          *(const uint4*)(prev + (size_t)(gy0 + r) * pitch + gx0a + (v << 4));
+    }
+  }
+  __syncthreads();
+
+  /* thread task: lattice column a (fastest), row group, field strip */
+  const int t = threadIdx.x;
+  const int ntask = g.nab * G * g.nstrip;
+  const bool active = t < ntask;
+  int al = t % g.nab, rest = t / g.nab;
+  int grp = rest % G, st = rest / G;
+  if (!active) { al = 0; grp = 0; st = 0; }
+  unsigned acc[TB];
+#pragma unroll
+  for (int j = 0; j < TB; j++) acc[j] = 0;
+  {
+    const int r0 = st * Rs;
+    const int cxb = e + al * g.step * g.bpp;
+    const int sh = (cxb & 3) << 3;
+    const uint8_t* Pb = P + (size_t)(r0 + grp * TB * g.step) * L.WP + (cxb & ~3);
+    const uint4* C4 = (const uint4*)C + r0 * L.nq;
+    /* walk the window rows; the field row of candidate j is rho - step*j,
+       inside the strip for j in [jlo(rho), jhi(rho)], a range that changes
+       only where rho or rho - Rs crosses a multiple of the step */
+    const int nrho = Rs + g.step * (TB - 1);
+    for (int rb = 0; rb < nrho;) {
+      int jhi = min(TB - 1, rb / g.step);
+      int jlo = rb < Rs ? 0 : (rb - Rs) / g.step + 1;
+      int re = jhi == TB - 1 ? nrho : min(nrho, (jhi + 1) * g.step);
+      int lo_next = Rs + jlo * g.step;
+      if (lo_next > rb && lo_next < re) re = lo_next;
+      rows_segment<TB>(acc, jlo, jhi, rb, re, g.step, Pb, L.WP, sh, C4, L.nq);
+      rb = re;
+    }
+  }
+  /* sum the strips */
+  if (g.nstrip > 1) {
+    if (active && st > 0)
+#pragma unroll
+      for (int j = 0; j < TB; j++) part[(((st - 1) * G + grp) * TB + j) * g.nab + al] = acc[j];
+    __syncthreads();
+    if (active && st == 0)
+      for (int s2 = 1; s2 < g.nstrip; s2++)
+#pragma unroll
+        for (int j = 0; j < TB; j++) acc[j] += part[(((s2 - 1) * G + grp) * TB + j) * g.nab + al];
+  }
+  unsigned long long best = ~0ull;
+  if (active && st == 0 && al < na_t) {
+#pragma unroll
+    for (int j = 0; j < TB; j++) {
+      int bl = grp * TB + j;
+      if (bl < nb_t) {
+        unsigned long long key = ((unsigned long long)acc[j] << 32) |
+                                 (unsigned)g.order[(b0 + bl) * g.na + (a0 + al)];
+        best = key < best ? key : best;
+      }
+    }
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  best = warp_min64(best);
+  if (lane == 0) red[warp] = best;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < nwarps; w++) best = red[w] < best ? red[w] : best;
+    atomicMin(&keys[item], best);
+    __threadfence();
+    unsigned tk = atomicAdd(&tickets[item], 1u);
+    s_last = (tk == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  refine_and_store(g, L, it, C, P + 16, prev, pitch, keys, tickets, res, item, qsad);
+}
+
+#endif
