@@ -89,6 +89,34 @@ VS_API int vsb_field_search_host(const uint8_t* curr, const uint8_t* prev, int w
                                  const int16_t* oy, int n, int tiles, uint32_t* sad,
                                  int16_t* tx, int16_t* ty, int32_t* ok);
 
+/* ---- allocation-free search (no counterpart in the reference) ----------
+   For callers that cannot let a library allocate GPU memory: hosts that own
+   all device memory through their own pools or budgets, or that call while
+   a CUDA graph is being recorded, where cudaMalloc is not allowed.  It runs
+   the planar per-field search of vsMotionDetection (spiral lattice of
+   maxShift/stepSize steps, halving refinement, range test) and allocates
+   nothing: its scratch (per-field running minimum and completion counter,
+   lattice rank tables; at most 4096 fields per call and 32768 lattice
+   points) lives in one static device array of about 320 KB that every GPU
+   loading the library holds until the process exits.
+     d_curr, d_prev: blurred planes on the current device, 16-byte aligned,
+       row pitch `pitch` a multiple of 16 bytes, readable up to 256 bytes past
+       the end of their last row; every field's whole search window must lie
+       inside the planes.
+     d_fields: n records {int16 x, y, ox, oy} (centre, lattice offset).
+     d_results: n records {uint32 sad; int16 tx, ty; int32 ok} (shift
+       relative to the offset; ok = passed the range test).
+     stream: a cudaStream_t (NULL: legacy default stream); the call is
+       asynchronous on it.
+   The first call on a device resolves the array's device address; make that
+   first call before any stream capture.  All calls share the one array and
+   it keeps the last call's contents, so calls whose GPU work overlaps (two
+   streams, two host threads) race: serialize them.  Larger inputs are
+   rejected with VS_ERROR and a message in vsb_last_error(). */
+VS_API int vsb_field_search_noalloc(const uint8_t* d_curr, const uint8_t* d_prev, int pitch,
+                                    int size, int maxShift, int stepSize, const void* d_fields,
+                                    int n, void* d_results, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -30,7 +30,7 @@ CC = shutil.which("gcc", path="/usr/bin:/bin") or "gcc"
 STRICT_C = ["vs_runtime.c", "vs_frameinfo.c", "vs_vector.c", "vs_serialize.c",
             "vs_motiondetect.c", "vs_ext.c", "vs_batch.c", "vs_proposal_host.c"]
 REFFP_C = ["vs_transform.c", "vs_motionmodel.c", "vs_draw.c"]
-CU = ["vsb_device.cu", "vsb_batch.cu", "vsb_proposal.cu"]
+CU = ["vsb_device.cu", "vsb_noalloc.cu", "vsb_batch.cu", "vsb_proposal.cu"]
 
 COMMON_C = ["-std=gnu99", "-O3", "-DNDEBUG", "-fPIC", "-Wall", "-fvisibility=hidden",
             "-I" + INCLUDE, "-I" + CSRC]

@@ -184,3 +184,12 @@ int vsb_sad_peak(int variant, double* byteops_per_s) {
 void vsb_counters(long long* launches, long long* h2d_bytes, long long* d2h_bytes) {
   vsbd_counters(launches, h2d_bytes, d2h_bytes);
 }
+
+int vsb_field_search_noalloc(const uint8_t* d_curr, const uint8_t* d_prev, int pitch, int size,
+                             int maxShift, int stepSize, const void* d_fields, int n,
+                             void* d_results, void* stream) {
+  return vsbd_search_noalloc(d_curr, d_prev, pitch, size, maxShift, stepSize, d_fields, n,
+                             d_results, stream) == 0
+             ? VS_OK
+             : VS_ERROR;
+}

@@ -515,6 +515,35 @@ static int autotune_tiling(GeomDev* gd, const uint8_t* curr, const uint8_t* prev
   return 0;
 }
 
+/* Tiling of a field set without uploading its tables (the caller provides
+   the rank tables): the cost model's best shape.  Used by the
+   allocation-free entry point. */
+int vsbd_plan_search(const vsbd_geom* h, int nitems, DGeom* out) {
+  DGeom g;
+  memset(&g, 0, sizeof(g));
+  g.S = h->size; g.bpp = h->bpp; g.step = h->step;
+  g.na = h->na; g.nb = h->nb; g.ax0 = h->ax0; g.by0 = h->by0;
+  g.has_origin = h->has_origin; g.nstages = h->nstages;
+  if (g.nstages > VSBD_MAX_STAGES) { set_msg("too many refinement stages"); return -1; }
+  g.maxq = 1;
+  for (int i = 0; i < g.nstages; i++) {
+    g.st_r[i] = h->st_r[i];
+    g.st_h[i] = h->st_h[i];
+    int side = (2 * h->st_r[i]) / h->st_h[i] + 1;
+    if (side * side > g.maxq) g.maxq = side * side;
+  }
+  g.limx = h->limx; g.limy = h->limy;
+  TileCand cand[1];
+  if (tile_candidates(g, nitems > 0 ? nitems : 1, 0, 0, 0, 0, cand, 1) < 1) {
+    set_msg("no search tiling fits in shared memory");
+    return -1;
+  }
+  *out = cand[0].g;
+  return 0;
+}
+
+extern "C" void vsbd_set_error(const char* msg) { set_msg(msg); }
+
 /* ------------------------------------------------------------------------ */
 /* per-detector context                                                      */
 /* ------------------------------------------------------------------------ */

@@ -94,6 +94,12 @@ void vsbd_counters(long long* launches, long long* h2d, long long* d2h);
 
 /* Message of the last failure on this thread. */
 const char* vsbd_error(void);
+void vsbd_set_error(const char* msg);
+
+/* the field search with all scratch in a static device array (vsb_noalloc.cu) */
+int vsbd_search_noalloc(const uint8_t* d_curr, const uint8_t* d_prev, int pitch, int size,
+                        int maxShift, int stepSize, const void* d_items, int n, void* d_results,
+                        void* stream);
 
 /* ---- kernel-level entry points for parity tests (host buffers in/out) --- */
 int vsbd_blur_host(uint8_t* dst, const uint8_t* src, int width, int height, int size);

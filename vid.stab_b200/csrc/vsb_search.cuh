@@ -127,7 +127,7 @@ __device__ __forceinline__ unsigned sad_rows_warp(const uint32_t* __restrict__ C
    (i outer, j inner, centre skipped, strict <), range test, reset.  The
    window the rounds can reach (the field plus the sum of the round radii on
    every side) is staged in shared memory first. */
-__device__ void refine_and_store(const DGeom& g, const TileLayout& L, const vsbd_item& it,
+static __device__ void refine_and_store(const DGeom& g, const TileLayout& L, const vsbd_item& it,
                                  const uint32_t* C, uint8_t* rwin, const uint8_t* __restrict__ prev,
                                  int pitch, unsigned long long* keys, unsigned* tickets,
                                  vsbd_result* res, int item, unsigned* qsad) {
@@ -398,5 +398,8 @@ __global__ void __launch_bounds__(512, 1) k_lattice(const uint8_t* __restrict__ 
   __threadfence();
   refine_and_store(g, L, it, C, P + 16, prev, pitch, keys, tickets, res, item, qsad);
 }
+
+/* tiling of a field set by the cost model (vsb_device.cu) */
+int vsbd_plan_search(const vsbd_geom* h, int nitems, DGeom* out);
 
 #endif
