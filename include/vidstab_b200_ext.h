@@ -31,6 +31,17 @@ VS_API int vsb_sizeof(const char* type_name);
 VS_API int vsb_motion_detection_device(struct _vsmotiondetect* md, struct vsvector_* motions,
                                        const uint8_t* d_plane0, int pitch);
 
+/* Search strategy of a detector: 0 (default) the dense search of every
+   candidate; 1 the exact pruned search -- every candidate's SAD over the
+   first quarter of its field's rows bounds its full SAD from below;
+   candidates whose bound exceeds the full SAD of the best-bounded few cannot
+   win and are not completed.  Both give identical LocalMotions.
+   VSB_PRUNED_SEARCH in the environment makes 1 the default. */
+VS_API int vsb_set_search_mode(struct _vsmotiondetect* md, int pruned);
+/* The strategy detectors initialised from now on start with (-1: back to the
+   environment's choice). */
+VS_API void vsb_set_default_search_mode(int pruned);
+
 /* Kernel launches issued for this detector so far. */
 VS_API long vsb_launch_count(const struct _vsmotiondetect* md);
 

@@ -16,6 +16,14 @@ from conftest import first_difference, records_equal
 pytestmark = pytest.mark.gpu
 
 
+@pytest.fixture(params=["pruned", "dense"])
+def search(request):
+    """runs a test under both search strategies of the library"""
+    V.lib().vsb_set_default_search_mode(1 if request.param == "pruned" else 0)
+    yield request.param
+    V.lib().vsb_set_default_search_mode(-1)
+
+
 def expected(frames, pformat=1, **kw):
     """reference output where the reference build exists, else the oracle"""
     if O.ref_available():
@@ -35,19 +43,19 @@ def check(frames, pformat=1, **kw):
 
 
 @pytest.mark.parametrize("seed", range(6))
-def test_cfg0_pair(seed):
+def test_cfg0_pair(seed, search):
     A, B, _ = S.pair(640, 480, seed=seed)
     got, counts = check(np.stack([A, B]), V.PF_YUV420P)
     assert counts[0] == 0 and counts[1] > 20
 
 
 @pytest.mark.parametrize("w,h,n", [(640, 360, 8), (1280, 720, 5), (1920, 1080, 4)])
-def test_clip(w, h, n):
+def test_clip(w, h, n, search):
     frames = S.clip(w, h, n, seed=w)
     check(frames, V.PF_YUV420P)
 
 
-def test_clip_4k():
+def test_clip_4k(search):
     frames = S.clip(3840, 2160, 3, seed=4, trans_sigma=8.0, rot_sigma_deg=0.5)
     check(frames, V.PF_YUV420P, shakiness=10)
 
@@ -56,25 +64,25 @@ def test_clip_4k():
                                 dict(stepsize=1), dict(accuracy=9, stepsize=8),
                                 dict(accuracy=4, shakiness=8), dict(mincontrast=0.4),
                                 dict(mincontrast=0.05), dict(accuracy=1)])
-def test_config_variants(kw):
+def test_config_variants(kw, search):
     frames = S.clip(640, 480, 4, seed=17)
     check(frames, V.PF_GRAY8, **kw)
 
 
 @pytest.mark.parametrize("tripod", [1, 3])
-def test_tripod(tripod):
+def test_tripod(tripod, search):
     frames = S.clip(640, 360, 7, seed=23)
     got, counts = check(frames, V.PF_YUV420P, tripod=tripod)
     assert all(c == 0 for c in counts[:tripod])
 
 
 @pytest.mark.parametrize("pformat,bpp", [(V.PF_RGB24, 3), (V.PF_BGR24, 3), (V.PF_RGBA, 4)])
-def test_packed(pformat, bpp):
+def test_packed(pformat, bpp, search):
     frames = S.to_packed(S.clip(320, 240, 4, seed=29), bpp)
     check(frames, pformat)
 
 
-def test_low_contrast_frames():
+def test_low_contrast_frames(search):
     """flat frames: no field passes the contrast threshold"""
     frames = np.full((3, 360, 640), 120, np.uint8)
     got, counts = check(frames, V.PF_GRAY8)

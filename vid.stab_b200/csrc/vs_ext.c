@@ -193,3 +193,9 @@ int vsb_field_search_noalloc(const uint8_t* d_curr, const uint8_t* d_prev, int p
              ? VS_OK
              : VS_ERROR;
 }
+
+int vsb_set_search_mode(VSMotionDetect* md, int pruned) {
+  return vsbd_set_search_mode(vsb_md_device(md), pruned) == 0 ? VS_OK : VS_ERROR;
+}
+
+void vsb_set_default_search_mode(int pruned) { vsbd_set_default_search_mode(pruned); }

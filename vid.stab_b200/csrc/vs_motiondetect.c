@@ -349,7 +349,8 @@ int vsMotionDetectInit(VSMotionDetect* md, const VSMotionDetectConfig* conf, con
     }
     int blur = st->planar ? vsb_blur_size(md->conf.stepSize, md->fi.width, md->fi.height) : 0;
     if (vsbd_create(&st->dev, md->fi.width, md->fi.height, st->bpp, blur, st->nch, &gc, xy,
-                    xy + nc, nc, &gf, xy + 2 * nc, xy + 2 * nc + nf, nf) != 0) {
+                    xy + nc, nc, &gf, xy + 2 * nc, xy + 2 * nc + nf, nf,
+                    md->fieldscoarse.contrastThreshold) != 0) {
       vs_log_error(md->conf.modName, "GPU initialisation failed: %s\n", vsbd_error());
       ok = 0;
     }

@@ -189,20 +189,28 @@ static int launch_blur(const uint8_t* src, int sp, uint8_t* dst, int dp, int W, 
 /* field min / max                                                           */
 /* ------------------------------------------------------------------------ */
 
-/* one CTA per field; channel ch of a pixel is byte ch of its bpp bytes */
+/* One CTA per field; channel ch of a pixel is byte ch of its bpp bytes.
+   With skip != NULL it also flags every field whose contrast keeps it out of
+   the selection: the reference zeroes a contrast below the threshold and
+   selects only positive contrasts (src/motiondetect.c:697-698, :719, :734).
+   The contrast is the reference's double expression, evaluated in IEEE
+   double like the host's ((c0 + c1) + c2) * (1/3) for three channels), so
+   the flag agrees with the host's selection bit for bit. */
 __global__ void __launch_bounds__(256) k_minmax(const uint8_t* __restrict__ img, int pitch,
                                                 const int16_t* __restrict__ xs,
                                                 const int16_t* __restrict__ ys, int S, int bpp,
-                                                int nch, uint8_t* __restrict__ out) {
+                                                int nch, uint8_t* __restrict__ out, double thr,
+                                                uint8_t* __restrict__ skip) {
   __shared__ unsigned smn[8], smx[8];
   const int f = blockIdx.x;
   const int x0 = xs[f] - S / 2, y0 = ys[f] - S / 2;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double c[3] = { 0.0, 0.0, 0.0 };
   for (int ch = 0; ch < nch; ch++) {
     unsigned mn = 255, mx = 0;
     for (int i = threadIdx.x; i < S * S; i += blockDim.x) {
-      int r = i / S, c = i - r * S;
-      unsigned v = img[(size_t)(y0 + r) * pitch + (size_t)(x0 + c) * bpp + ch];
+      int r = i / S, col = i - r * S;
+      unsigned v = img[(size_t)(y0 + r) * pitch + (size_t)(x0 + col) * bpp + ch];
       mn = min(mn, v);
       mx = max(mx, v);
     }
@@ -214,8 +222,18 @@ __global__ void __launch_bounds__(256) k_minmax(const uint8_t* __restrict__ img,
       for (int w = 1; w < (int)(blockDim.x >> 5); w++) { mn = min(mn, smn[w]); mx = max(mx, smx[w]); }
       out[(f * nch + ch) * 2 + 0] = (uint8_t)mn;
       out[(f * nch + ch) * 2 + 1] = (uint8_t)mx;
+      c[ch] = (double)((int)mx - (int)mn) / ((double)((int)mx + (int)mn) + 0.1);
     }
     __syncthreads();
+  }
+  if (skip && threadIdx.x == 0) {
+    double con = c[0];
+    if (nch == 3) {
+      double s = __dadd_rn(c[0], c[1]);
+      s = __dadd_rn(s, c[2]);
+      con = __dmul_rn(s, 1.0 / 3.0);
+    }
+    skip[f] = !(con >= thr && con > 0.0);
   }
 }
 
@@ -298,8 +316,9 @@ static int tile_candidates(const DGeom& g, int nitems, int tb_force, int strip_f
     if (tb_force > 0 && TB != tb_force) continue;
     for (int ns = 1; ns <= 8; ns *= 2) {
       if (strip_force > 0 && ns != strip_force) continue;
-      if (g.S % ns) continue;
-      int Rs = g.S / ns;
+      const int rows = geom_rows(g);
+      if (rows % ns) continue;
+      int Rs = rows / ns;
       if (Rs < 4) continue;
       for (int ka = 1; ka <= 16; ka++) {
         int nab = (g.na + ka - 1) / ka;
@@ -339,7 +358,7 @@ static int tile_candidates(const DGeom& g, int nitems, int tb_force, int strip_f
             continue;
           }
           double eff = (double)Rs / (Rs + g.step * (TB - 1));
-          double work = (double)nab * nbb * g.S * L.rowW / eff; /* lane-SAD4 slots */
+          double work = (double)nab * nbb * rows * L.rowW / eff; /* lane-SAD4 slots */
           double warps = (double)cps * threads / 32.0;
           double occ = warps >= 16 ? 1.0 : warps / 16.0;
           long waves = (ctas + (long)sms * cps - 1) / ((long)sms * cps);
@@ -450,12 +469,71 @@ static int launch_search(const GeomDev& gd, const uint8_t* curr, const uint8_t* 
   return -1;
 }
 
+/* the partial pass: every candidate's sum over the field's first rows */
+template <int TB>
+static int launch_emit_tb(const GeomDev& gd, const uint8_t* curr, const uint8_t* prev, int pitch,
+                          const vsbd_item* d_items, int n, cudaStream_t st) {
+  cudaError_t e = cudaFuncSetAttribute(k_lattice<TB, true>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gd.smem);
+  if (e != cudaSuccess) {
+    set_err("cudaFuncSetAttribute(k_lattice emit)", e);
+    return -1;
+  }
+  dim3 grid(gd.g.nta * gd.g.ntb, n);
+  k_lattice<TB, true><<<grid, gd.g.threads, gd.smem, st>>>(curr, prev, pitch, gd.g, d_items, NULL,
+                                                           NULL, NULL);
+  return 1;
+}
+
+static int launch_emit(const GeomDev& gd, const uint8_t* curr, const uint8_t* prev, int pitch,
+                       const vsbd_item* d_items, int n, cudaStream_t st) {
+  if (n <= 0) return 0;
+  switch (gd.g.tb) {
+    case 2: return launch_emit_tb<2>(gd, curr, prev, pitch, d_items, n, st);
+    case 4: return launch_emit_tb<4>(gd, curr, prev, pitch, d_items, n, st);
+    case 8: return launch_emit_tb<8>(gd, curr, prev, pitch, d_items, n, st);
+  }
+  set_msg("unsupported rows-per-thread");
+  return -1;
+}
+
+/* Pruned search of n items: partial pass, bound + survivors, survivors'
+   full SADs and refinement.  gp is the partial-pass geometry (rows < S, emit
+   set), gd the full one.  Returns the number of kernels launched or -1. */
+static int launch_pruned(const GeomDev& gd, const GeomDev& gp, const uint8_t* curr,
+                         const uint8_t* prev, int pitch, const vsbd_item* d_items, int n,
+                         const uint8_t* skip, unsigned* part, int* counts, int* lists,
+                         int* boxes, unsigned long long* keys, unsigned* tickets,
+                         vsbd_result* d_res, cudaStream_t st) {
+  if (n <= 0) return 0;
+  GeomDev p = gp;
+  p.g.emit = part;
+  p.g.skip = skip;
+  if (launch_emit(p, curr, prev, pitch, d_items, n, st) < 0) return -1;
+  DGeom g = gd.g;
+  g.skip = skip;
+  const size_t fs = (size_t)g.S * g.S * g.bpp + 64;
+  cudaError_t e = cudaFuncSetAttribute(k_prune, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fs);
+  if (e != cudaSuccess) { set_err("cudaFuncSetAttribute(k_prune)", e); return -1; }
+  k_prune<<<n, 256, fs, st>>>(curr, prev, pitch, g, d_items, part, 4, keys, counts, lists, boxes);
+  const size_t ss = survive_smem(g);
+  e = cudaFuncSetAttribute(k_survive, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss);
+  if (e != cudaSuccess) { set_err("cudaFuncSetAttribute(k_survive)", e); return -1; }
+  int chunks = 4 * sm_count() / n;
+  if (chunks < 1) chunks = 1;
+  if (chunks > 16) chunks = 16;
+  dim3 grid(chunks, n);
+  k_survive<<<grid, 256, ss, st>>>(curr, prev, pitch, g, geom_rows(gp.g), d_items, part, counts,
+                                   lists, boxes, keys, tickets, d_res);
+  return 3;
+}
+
 /* Times the modelled best tilings of one field set on the detector's own
    buffers and items and keeps the fastest.  The dense lattice does the same
    work whatever the pixels hold, so the contents of the buffers do not matter.
    Results are cached per (geometry, item count) for the process. */
 struct TuneEntry {
-  int S, bpp, step, na, nb, nstages, nitems;
+  int S, bpp, step, na, nb, nstages, nitems, rows;
   DGeom g;
 };
 static TuneEntry g_tune[64];
@@ -463,13 +541,14 @@ static int g_ntune = 0;
 
 static int autotune_tiling(GeomDev* gd, const uint8_t* curr, const uint8_t* prev, int pitch,
                            const vsbd_item* d_items, int n, unsigned long long* keys,
-                           unsigned* tickets, vsbd_result* d_res, cudaStream_t st) {
+                           unsigned* tickets, vsbd_result* d_res, cudaStream_t st,
+                           unsigned* emit_buf = NULL) {
   if (n <= 0 || getenv("VSB_NO_AUTOTUNE")) return 0;
   DGeom& g = gd->g;
   for (int i = 0; i < g_ntune; i++) {
     TuneEntry& e = g_tune[i];
     if (e.S == g.S && e.bpp == g.bpp && e.step == g.step && e.na == g.na && e.nb == g.nb &&
-        e.nstages == g.nstages && e.nitems == n) {
+        e.nstages == g.nstages && e.nitems == n && e.rows == g.rows) {
       DGeom t = e.g;
       t.order = g.order;
       t.point = g.point;
@@ -488,11 +567,21 @@ static int autotune_tiling(GeomDev* gd, const uint8_t* curr, const uint8_t* prev
   for (int k = 0; k < nc; k++) {
     GeomDev t = *gd;
     t.g = cand[k].g;
+    t.g.emit = emit_buf;
+    t.g.skip = NULL;
     t.smem = tile_layout(t.g).total;
-    if (launch_search(t, curr, prev, pitch, d_items, n, keys, tickets, d_res, st) < 0) continue;
+    if (emit_buf) {
+      if (launch_emit(t, curr, prev, pitch, d_items, n, st) < 0) continue;
+    } else if (launch_search(t, curr, prev, pitch, d_items, n, keys, tickets, d_res, st) < 0) {
+      continue;
+    }
     cudaEventRecord(e0, st);
-    for (int rep = 0; rep < 3; rep++)
-      launch_search(t, curr, prev, pitch, d_items, n, keys, tickets, d_res, st);
+    for (int rep = 0; rep < 3; rep++) {
+      if (emit_buf)
+        launch_emit(t, curr, prev, pitch, d_items, n, st);
+      else
+        launch_search(t, curr, prev, pitch, d_items, n, keys, tickets, d_res, st);
+    }
     cudaEventRecord(e1, st);
     if (cudaEventSynchronize(e1) != cudaSuccess) break;
     float ms = 0.f;
@@ -505,12 +594,13 @@ static int autotune_tiling(GeomDev* gd, const uint8_t* curr, const uint8_t* prev
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   CK(cudaGetLastError());
+  best.emit = NULL;
   g = best;
   gd->smem = tile_layout(g).total;
   if (g_ntune < 64) {
     TuneEntry& e = g_tune[g_ntune++];
     e.S = g.S; e.bpp = g.bpp; e.step = g.step; e.na = g.na; e.nb = g.nb;
-    e.nstages = g.nstages; e.nitems = n; e.g = g;
+    e.nstages = g.nstages; e.nitems = n; e.rows = g.rows; e.g = g;
   }
   return 0;
 }
@@ -557,12 +647,20 @@ struct vsbd_ctx {
   uint8_t* d_tmp;     /* row-pass buffer of the wide-window blur */
   uint8_t* d_buf[2];  /* blurred planes: current / previous */
   int cur;
+  double thr_coarse;  /* contrast threshold of the coarse fields */
   int16_t* d_xy;      /* coarse x | coarse y | fine x | fine y */
   GeomDev gc, gf;
   vsbd_item* d_citems;
   vsbd_item* d_fitems;
   unsigned long long* d_keys;   /* coarse nc, then fine nf */
   unsigned* d_tickets;
+  int mode;                     /* 0 dense search, 1 pruned search */
+  GeomDev gcp, gfp;             /* partial-pass geometry (first rows of the field) */
+  uint8_t* d_skip;              /* coarse fields never selected (contrast) */
+  unsigned* d_part;             /* partial sums, per item per lattice point */
+  int* d_lists;                 /* survivors, per item */
+  int* d_counts;
+  int* d_boxes;                 /* survivors' lattice bounding box, per item */
   uint8_t* d_out;               /* minmax | coarse results | fine results */
   uint8_t* h_out;               /* pinned mirror of d_out */
   vsbd_item* h_items;           /* pinned staging of fine items */
@@ -641,17 +739,41 @@ extern "C" void vsbd_destroy(vsbd_ctx* c) {
   cudaFree(c->d_keys);
   cudaFree(c->d_tickets);
   cudaFree(c->d_out);
+  cudaFree(c->d_skip);
+  cudaFree(c->d_part);
+  cudaFree(c->d_lists);
+  cudaFree(c->d_counts);
+  cudaFree(c->d_boxes);
   if (c->h_out) cudaFreeHost(c->h_out);
   if (c->h_items) cudaFreeHost(c->h_items);
   geom_free(&c->gc);
   geom_free(&c->gf);
+  /* gcp/gfp share gc/gf's tables */
   if (c->st) cudaStreamDestroy(c->st);
   free(c);
 }
 
+/* search strategy of detectors created from now on (-1: environment) */
+static int g_default_mode = -1;
+extern "C" void vsbd_set_default_search_mode(int pruned) { g_default_mode = pruned < 0 ? -1 : (pruned ? 1 : 0); }
+
+/* rows of a field the pruned search's partial pass sums: a quarter, at
+   least 4 (on blurred content this leaves a few percent of the candidates) */
+static int partial_rows(int S) {
+  int r = S / 4;
+  return r < 4 ? (S < 4 ? S : 4) : r;
+}
+
+extern "C" int vsbd_set_search_mode(vsbd_ctx* c, int pruned) {
+  if (!c) return -1;
+  c->mode = pruned ? 1 : 0;
+  return 0;
+}
+
 extern "C" int vsbd_create(vsbd_ctx** out, int W, int H, int bpp, int blur_size, int channels,
                            const vsbd_geom* coarse, const int16_t* cx, const int16_t* cy, int nc,
-                           const vsbd_geom* fine, const int16_t* fx, const int16_t* fy, int nf) {
+                           const vsbd_geom* fine, const int16_t* fx, const int16_t* fy, int nf,
+                           double coarse_threshold) {
   *out = NULL;
   int ndev = 0;
   cudaError_t e = cudaGetDeviceCount(&ndev);
@@ -663,6 +785,7 @@ extern "C" int vsbd_create(vsbd_ctx** out, int W, int H, int bpp, int blur_size,
   CK(cudaGetDevice(&c->dev));
   c->W = W; c->H = H; c->bpp = bpp; c->blur = blur_size; c->nch = channels;
   c->nc = nc; c->nf = nf;
+  c->thr_coarse = coarse_threshold;
   c->pitch = (int)(((size_t)W * bpp + 127) & ~(size_t)127);
   size_t plane = (size_t)c->pitch * H + 256; /* slack: word reads past a row end */
 #define CKC(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) { set_err(#call, e_); vsbd_destroy(c); return -1; } } while (0)
@@ -680,6 +803,35 @@ extern "C" int vsbd_create(vsbd_ctx** out, int W, int H, int bpp, int blur_size,
   CKC(cudaMemcpy(c->d_xy + 2 * nc + nf, fy, sizeof(int16_t) * nf, cudaMemcpyHostToDevice));
   if (geom_upload(coarse, nc, 0, &c->gc) != 0) { vsbd_destroy(c); return -1; }
   if (geom_upload(fine, nf, 0, &c->gf) != 0) { vsbd_destroy(c); return -1; }
+  /* the pruned search's partial pass sums the first rows of each field */
+  c->mode = g_default_mode >= 0 ? g_default_mode : (getenv("VSB_PRUNED_SEARCH") ? 1 : 0);
+  c->gcp = c->gc;
+  c->gfp = c->gf;
+  c->gcp.g.rows = partial_rows(c->gc.g.S);
+  c->gfp.g.rows = partial_rows(c->gf.g.S);
+  {
+    TileCand tc[1];
+    if (tile_candidates(c->gcp.g, nc, 0, 0, 0, 0, tc, 1) < 1 ||
+        (c->gcp.g = tc[0].g, tile_candidates(c->gfp.g, nf, 0, 0, 0, 0, tc, 1) < 1)) {
+      set_msg("no partial-pass tiling fits in shared memory");
+      vsbd_destroy(c);
+      return -1;
+    }
+    c->gfp.g = tc[0].g;
+    c->gcp.smem = tile_layout(c->gcp.g).total;
+    c->gfp.smem = tile_layout(c->gfp.g).total;
+  }
+  {
+    size_t lat = (size_t)c->gc.g.na * c->gc.g.nb * nc;
+    size_t latf = (size_t)c->gf.g.na * c->gf.g.nb * nf;
+    if (latf > lat) lat = latf;
+    CKC(cudaMalloc(&c->d_part, sizeof(unsigned) * (lat + 1)));
+    CKC(cudaMalloc(&c->d_lists, sizeof(int) * (lat + 1)));
+    CKC(cudaMalloc(&c->d_counts, sizeof(int) * (nc + nf + 1)));
+    CKC(cudaMalloc(&c->d_boxes, sizeof(int) * 4 * (nc + nf + 1)));
+    CKC(cudaMalloc(&c->d_skip, nc + 1));
+    CKC(cudaMemset(c->d_skip, 0, nc + 1));
+  }
   /* coarse items: every coarse field, no offset */
   {
     vsbd_item* it = (vsbd_item*)malloc(sizeof(vsbd_item) * (nc + 1));
@@ -711,7 +863,11 @@ extern "C" int vsbd_create(vsbd_ctx** out, int W, int H, int bpp, int blur_size,
   if (autotune_tiling(&c->gc, c->d_buf[0], c->d_buf[1], c->pitch, c->d_citems, nc, c->d_keys,
                       c->d_tickets, (vsbd_result*)(c->d_out + c->off_coarse), c->st) != 0 ||
       autotune_tiling(&c->gf, c->d_buf[0], c->d_buf[1], c->pitch, c->d_fitems, nf, c->d_keys + nc,
-                      c->d_tickets + nc, (vsbd_result*)(c->d_out + c->off_fine), c->st) != 0) {
+                      c->d_tickets + nc, (vsbd_result*)(c->d_out + c->off_fine), c->st) != 0 ||
+      autotune_tiling(&c->gcp, c->d_buf[0], c->d_buf[1], c->pitch, c->d_citems, nc, NULL, NULL,
+                      NULL, c->st, c->d_part) != 0 ||
+      autotune_tiling(&c->gfp, c->d_buf[0], c->d_buf[1], c->pitch, c->d_fitems, nf, NULL, NULL,
+                      NULL, c->st, c->d_part) != 0) {
     vsbd_destroy(c);
     return -1;
   }
@@ -753,19 +909,25 @@ extern "C" int vsbd_stage_a(vsbd_ctx* c, const uint8_t* host, int linesize, cons
   if (search) {
     int S = c->gc.g.S;
     kt_begin(c, VSBD_KT_MINMAX);
-    k_minmax<<<c->nc, 256, 0, c->st>>>(cur, c->pitch, c->d_xy, c->d_xy + c->nc, S, c->bpp, c->nch, c->d_out);
+    k_minmax<<<c->nc, 256, 0, c->st>>>(cur, c->pitch, c->d_xy, c->d_xy + c->nc, S, c->bpp, c->nch,
+                                       c->d_out, c->thr_coarse, c->mode ? c->d_skip : NULL);
     c->launches++;
     count_launches(1);
     if (c->nf > 0) {
       k_minmax<<<c->nf, 256, 0, c->st>>>(cur, c->pitch, c->d_xy + 2 * c->nc, c->d_xy + 2 * c->nc + c->nf,
-                                         c->gf.g.S, c->bpp, c->nch, c->d_out + (size_t)c->nc * c->nch * 2);
+                                         c->gf.g.S, c->bpp, c->nch, c->d_out + (size_t)c->nc * c->nch * 2,
+                                         0.0, NULL);
       c->launches++;
       count_launches(1);
     }
     kt_end(c, VSBD_KT_MINMAX);
     kt_begin(c, VSBD_KT_COARSE);
-    int nl = launch_search(c->gc, cur, prv, c->pitch, c->d_citems, c->nc, c->d_keys, c->d_tickets,
-                           (vsbd_result*)(c->d_out + c->off_coarse), c->st);
+    int nl = c->mode ? launch_pruned(c->gc, c->gcp, cur, prv, c->pitch, c->d_citems, c->nc,
+                                     c->d_skip, c->d_part, c->d_counts, c->d_lists, c->d_boxes,
+                                     c->d_keys, c->d_tickets,
+                                     (vsbd_result*)(c->d_out + c->off_coarse), c->st)
+                     : launch_search(c->gc, cur, prv, c->pitch, c->d_citems, c->nc, c->d_keys,
+                                     c->d_tickets, (vsbd_result*)(c->d_out + c->off_coarse), c->st);
     if (nl < 0) return -1;
     c->launches += nl;
     count_launches(nl);
@@ -792,8 +954,14 @@ extern "C" int vsbd_stage_b(vsbd_ctx* c, const vsbd_item* items, int n, const vs
   uint8_t* cur = c->d_buf[c->cur];
   uint8_t* prv = c->d_buf[c->cur ^ 1];
   kt_begin(c, VSBD_KT_FINE);
-  int nl = launch_search(c->gf, cur, prv, c->pitch, c->d_fitems, n, c->d_keys + c->nc,
-                         c->d_tickets + c->nc, (vsbd_result*)(c->d_out + c->off_fine), c->st);
+  int nl = c->mode ? launch_pruned(c->gf, c->gfp, cur, prv, c->pitch, c->d_fitems, n, NULL,
+                                   c->d_part, c->d_counts + c->nc, c->d_lists,
+                                   c->d_boxes + 4 * c->nc, c->d_keys + c->nc,
+                                   c->d_tickets + c->nc, (vsbd_result*)(c->d_out + c->off_fine),
+                                   c->st)
+                   : launch_search(c->gf, cur, prv, c->pitch, c->d_fitems, n, c->d_keys + c->nc,
+                                   c->d_tickets + c->nc, (vsbd_result*)(c->d_out + c->off_fine),
+                                   c->st);
   if (nl < 0) return -1;
   c->launches += nl;
   count_launches(nl);
@@ -855,7 +1023,7 @@ extern "C" int vsbd_minmax_host(const uint8_t* img, int W, int H, int bpp, int c
   if ((e = cudaMemcpy2D(d_img, pitch, img, (size_t)W * bpp, (size_t)W * bpp, H, cudaMemcpyHostToDevice)) != cudaSuccess) { set_err("upload", e); goto done; }
   cudaMemcpy(d_xy, x, sizeof(int16_t) * n, cudaMemcpyHostToDevice);
   cudaMemcpy(d_xy + n, y, sizeof(int16_t) * n, cudaMemcpyHostToDevice);
-  if (n > 0) k_minmax<<<n, 256>>>(d_img, pitch, d_xy, d_xy + n, size, bpp, channels, d_out);
+  if (n > 0) k_minmax<<<n, 256>>>(d_img, pitch, d_xy, d_xy + n, size, bpp, channels, d_out, 0.0, NULL);
   if ((e = cudaGetLastError()) != cudaSuccess) { set_err("k_minmax", e); goto done; }
   if ((e = cudaMemcpy(out, d_out, (size_t)n * channels * 2, cudaMemcpyDeviceToHost)) != cudaSuccess) { set_err("download", e); goto done; }
   rc = 0;

@@ -52,10 +52,19 @@ typedef struct vsbd_ctx vsbd_ctx;
 
 /* Creates the device state of one detector.  blur_size < 2 means no blur
    (the plane is used as is; packed formats).  channels: 1 planar, 3 packed
-   (contrast over the colour channels).  Returns 0 or -1 (vsbd_error()). */
+   (contrast over the colour channels).  coarse_threshold: the coarse
+   fields' contrast threshold (fields below it are never selected and the
+   pruned search skips them).  Returns 0 or -1 (vsbd_error()). */
 int vsbd_create(vsbd_ctx** out, int width, int height, int bpp, int blur_size, int channels,
                 const vsbd_geom* coarse, const int16_t* cx, const int16_t* cy, int nc,
-                const vsbd_geom* fine, const int16_t* fx, const int16_t* fy, int nf);
+                const vsbd_geom* fine, const int16_t* fx, const int16_t* fy, int nf,
+                double coarse_threshold);
+
+/* 1: exact pruned search (partial-row bounds, survivors only; default),
+   0: dense search of every candidate.  Both give identical results. */
+int vsbd_set_search_mode(vsbd_ctx* c, int pruned);
+/* the strategy detectors created later start with (-1: environment) */
+void vsbd_set_default_search_mode(int pruned);
 void vsbd_destroy(vsbd_ctx* c);
 
 /* Stage A of one frame: take plane 0 (host pointer + linesize, or a device

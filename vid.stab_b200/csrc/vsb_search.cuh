@@ -44,7 +44,13 @@ struct DGeom {
   int nta, ntb;         /* tiles along a / along b */
   int nstrip;           /* field rows split into this many strips */
   int threads;          /* block size */
+  int rows;             /* field rows a launch sums (0: all S); fewer rows give
+                           every candidate a lower bound of its SAD */
+  unsigned* emit;       /* emit mode: per item, per lattice point, the sum */
+  const uint8_t* skip;  /* emit mode: per item, nonzero = field never used */
 };
+
+__host__ __device__ inline int geom_rows(const DGeom& g) { return g.rows > 0 ? g.rows : g.S; }
 
 /* packed 4 x u8 sum of absolute differences, accumulated */
 __device__ __forceinline__ unsigned sad4(unsigned a, unsigned b, unsigned c) {
@@ -84,15 +90,16 @@ __host__ __device__ inline TileLayout tile_layout(const DGeom& g) {
   L.nq = L.rowW >> 2;
   int wwb = L.rowB + (g.nab - 1) * g.step * g.bpp;
   L.WP = (((15 + wwb + 15) >> 4) + 1) << 4;
-  L.WH_alloc = g.S + (g.nbb - 1) * g.step;
+  const int rows = geom_rows(g);
+  L.WH_alloc = rows + (g.nbb - 1) * g.step;
   int R = refine_reach(g);
   L.RH = g.S + 2 * R;
   L.RP = ((3 + L.rowB + 2 * R * g.bpp + 8 + 15) >> 4) << 4;
   L.FP = ((L.rowB + 15 + 15) >> 4 << 4) + 16;
-  L.off_P = (size_t)g.S * L.rowB;
+  L.off_P = (size_t)rows * L.rowB;
   size_t parea = (size_t)L.WH_alloc * L.WP;
-  size_t rarea = (size_t)L.RH * L.RP + 16;
-  size_t farea = (size_t)g.S * L.FP;
+  size_t rarea = g.rows > 0 ? 0 : (size_t)L.RH * L.RP + 16;
+  size_t farea = (size_t)rows * L.FP;
   if (rarea > parea) parea = rarea;
   if (farea > parea) parea = farea;
   L.off_part = L.off_P + parea;
@@ -108,17 +115,34 @@ __host__ __device__ inline TileLayout tile_layout(const DGeom& g) {
 __device__ __forceinline__ unsigned sad_rows_warp(const uint32_t* __restrict__ C, int rowW, int S,
                                                   const uint8_t* __restrict__ base, size_t pitch,
                                                   int bx, int row0, int lane) {
+  /* lanes stride over the field's words in raster order (consecutive lanes
+     read consecutive words: coalesced in global memory, conflict-free in
+     shared memory); four words in flight per lane */
   unsigned acc = 0;
   const int sh = (bx & 3) << 3;
-  for (int r = lane; r < S; r += 32) {
-    const uint32_t* Pw = (const uint32_t*)(base + (size_t)(row0 + r) * pitch) + (bx >> 2);
-    const uint32_t* Cr = C + r * rowW;
-    uint32_t lo = Pw[0];
-    for (int w = 0; w < rowW; w++) {
-      uint32_t hi = Pw[w + 1];
-      acc = sad4(Cr[w], __funnelshift_r(lo, hi, sh), acc);
-      lo = hi;
+  const uint8_t* b0 = base + (size_t)row0 * pitch + (bx & ~3);
+  const int total = S * rowW;
+  int r = lane / rowW, w = lane - r * rowW;
+  int i = lane;
+  for (; i + 96 < total; i += 128) {
+    uint32_t lo[4], hi[4], cw[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const uint32_t* Pw = (const uint32_t*)(b0 + (size_t)r * pitch) + w;
+      lo[u] = Pw[0];
+      hi[u] = Pw[1];
+      cw[u] = C[i + 32 * u];
+      w += 32;
+      while (w >= rowW) { w -= rowW; r++; }
     }
+#pragma unroll
+    for (int u = 0; u < 4; u++) acc = sad4(cw[u], __funnelshift_r(lo[u], hi[u], sh), acc);
+  }
+  for (; i < total; i += 32) {
+    const uint32_t* Pw = (const uint32_t*)(b0 + (size_t)r * pitch) + w;
+    acc = sad4(C[i], __funnelshift_r(Pw[0], Pw[1], sh), acc);
+    w += 32;
+    while (w >= rowW) { w -= rowW; r++; }
   }
   return __reduce_add_sync(0xffffffffu, acc);
 }
@@ -271,7 +295,7 @@ __device__ __forceinline__ void rows_segment(unsigned (&acc)[TB], int jlo, int j
 }
 
 /* grid (nta*ntb, items); block g.threads; dynamic smem tile_layout(g).total */
-template <int TB>
+template <int TB, bool EMIT = false>
 __global__ void __launch_bounds__(512, 1) k_lattice(const uint8_t* __restrict__ curr,
                                                   const uint8_t* __restrict__ prev, int pitch,
                                                   DGeom g, const vsbd_item* __restrict__ items,
@@ -288,7 +312,9 @@ __global__ void __launch_bounds__(512, 1) k_lattice(const uint8_t* __restrict__ 
   const int a0 = tai * g.nab, b0 = tbi * g.nbb;
   const int na_t = min(g.nab, g.na - a0), nb_t = min(g.nbb, g.nb - b0);
   const int G = g.nbb / TB;
-  const int Rs = g.S / g.nstrip;
+  const int rows = geom_rows(g);
+  const int Rs = rows / g.nstrip;
+  if (EMIT && g.skip && g.skip[item]) return; /* a field that is never selected */
   uint32_t* C = (uint32_t*)sm; /* the current field, rowB bytes per row */
   uint8_t* P = sm + L.off_P;
   unsigned* part = (unsigned*)(sm + L.off_part);
@@ -300,13 +326,13 @@ __global__ void __launch_bounds__(512, 1) k_lattice(const uint8_t* __restrict__ 
     const int cx0 = (it.x - g.S / 2) * g.bpp, cy0 = it.y - g.S / 2;
     const int cx0a = cx0 & ~15, ce = cx0 - cx0a;
     const int nv = (ce + L.rowB + 15) >> 4;
-    for (int i = threadIdx.x; i < g.S * nv; i += blockDim.x) {
+    for (int i = threadIdx.x; i < rows * nv; i += blockDim.x) {
       int r = i / nv, v = i - r * nv;
       *(uint4*)(P + r * L.FP + (v << 4)) =
           *(const uint4*)(curr + (size_t)(cy0 + r) * pitch + cx0a + (v << 4));
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < g.S * L.rowW; i += blockDim.x) {
+    for (int i = threadIdx.x; i < rows * L.rowW; i += blockDim.x) {
       int r = i / L.rowW, w = i - r * L.rowW;
       const uint32_t* sw = (const uint32_t*)(P + r * L.FP) + (ce >> 2) + w;
       C[i] = __funnelshift_r(sw[0], sw[1], (ce & 3) << 3);
@@ -319,7 +345,7 @@ __global__ void __launch_bounds__(512, 1) k_lattice(const uint8_t* __restrict__ 
   const int gx0a = gx0 & ~15, e = gx0 - gx0a;
   {
     const int wwb = L.rowB + (na_t - 1) * g.step * g.bpp;
-    const int wh = g.S + (nb_t - 1) * g.step;
+    const int wh = rows + (nb_t - 1) * g.step;
     const int nvec = (e + wwb + 15) >> 4;
     for (int i = threadIdx.x; i < wh * nvec; i += blockDim.x) {
       int r = i / nvec, v = i - r * nvec;
@@ -370,6 +396,17 @@ __global__ void __launch_bounds__(512, 1) k_lattice(const uint8_t* __restrict__ 
 #pragma unroll
         for (int j = 0; j < TB; j++) acc[j] += part[(((s2 - 1) * G + grp) * TB + j) * g.nab + al];
   }
+  if (EMIT) {
+    if (active && st == 0 && al < na_t) {
+      unsigned* out = g.emit + (size_t)item * g.na * g.nb;
+#pragma unroll
+      for (int j = 0; j < TB; j++) {
+        int bl = grp * TB + j;
+        if (bl < nb_t) out[(b0 + bl) * g.na + (a0 + al)] = acc[j];
+      }
+    }
+    return;
+  }
   unsigned long long best = ~0ull;
   if (active && st == 0 && al < na_t) {
 #pragma unroll
@@ -397,6 +434,237 @@ __global__ void __launch_bounds__(512, 1) k_lattice(const uint8_t* __restrict__ 
   if (!s_last) return;
   __threadfence();
   refine_and_store(g, L, it, C, P + 16, prev, pitch, keys, tickets, res, item, qsad);
+}
+
+/* Bound and survivors of one item after the partial pass (one CTA per item).
+   The topk candidates with the smallest partial sums (ties by rank) get their
+   full SAD; the smallest gives the bound B and the item's starting key.  A
+   candidate whose partial sum exceeds B has a full SAD above B and cannot be
+   the minimum (nor tie with it), so only candidates with partial <= B
+   survive.  Dynamic shared memory: the field (S rows) plus the small lists. */
+static __global__ void __launch_bounds__(256) k_prune(const uint8_t* __restrict__ curr,
+                                               const uint8_t* __restrict__ prev, int pitch,
+                                               DGeom g, const vsbd_item* __restrict__ items,
+                                               const unsigned* __restrict__ part, int topk,
+                                               unsigned long long* __restrict__ keys,
+                                               int* __restrict__ counts, int* __restrict__ lists,
+                                               int* __restrict__ boxes) {
+  extern __shared__ __align__(16) uint8_t sm[];
+  __shared__ unsigned long long red[8];
+  __shared__ int chosen[8];
+  __shared__ unsigned long long s_best;
+  __shared__ int s_count, s_box[4];
+  const int item = blockIdx.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int n = g.na * g.nb;
+  if (topk > n) topk = n;
+  if (g.skip && g.skip[item]) {
+    if (threadIdx.x == 0) {
+      counts[item] = 0;
+      keys[item] = ~0ull;
+    }
+    return;
+  }
+  const vsbd_item it = items[item];
+  const unsigned* P = part + (size_t)item * n;
+  const int rowB = g.S * g.bpp, rowW = rowB >> 2;
+  uint32_t* C = (uint32_t*)sm;
+  {
+    const int cx0 = (it.x - g.S / 2) * g.bpp, cy0 = it.y - g.S / 2;
+    const int sh = (cx0 & 3) << 3;
+    for (int i = threadIdx.x; i < g.S * rowW; i += blockDim.x) {
+      int r = i / rowW, w = i - r * rowW;
+      const uint32_t* sw = (const uint32_t*)(curr + (size_t)(cy0 + r) * pitch) + (cx0 >> 2) + w;
+      C[i] = __funnelshift_r(sw[0], sw[1], sh);
+    }
+  }
+  if (topk > 8) topk = 8;
+  for (int k = 0; k < topk; k++) {
+    unsigned long long best = ~0ull;
+    for (int c = threadIdx.x; c < n; c += blockDim.x) {
+      bool taken = false;
+      for (int q = 0; q < k; q++) taken |= chosen[q] == c;
+      if (taken) continue;
+      unsigned long long key = ((unsigned long long)P[c] << 32) | (unsigned)g.order[c];
+      best = key < best ? key : best;
+    }
+    best = warp_min64(best);
+    if (lane == 0) red[warp] = best;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int w = 1; w < nwarps; w++) best = red[w] < best ? red[w] : best;
+      short2 pt = g.point[(unsigned)(best & 0xffffffffu)];
+      chosen[k] = ((pt.y - g.by0) / g.step) * g.na + (pt.x - g.ax0) / g.step;
+    }
+    __syncthreads();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) s_best = ~0ull;
+  __syncthreads();
+  const int fx0 = (it.x - g.S / 2 + it.ox) * g.bpp, fy0 = it.y - g.S / 2 + it.oy;
+  for (int k = warp; k < topk; k += nwarps) {
+    int c = chosen[k];
+    int a = c % g.na, b = c / g.na;
+    unsigned sd = sad_rows_warp(C, rowW, g.S, prev, (size_t)pitch,
+                                fx0 + (g.ax0 + a * g.step) * g.bpp, fy0 + g.by0 + b * g.step, lane);
+    if (lane == 0) atomicMin(&s_best, ((unsigned long long)sd << 32) | (unsigned)g.order[c]);
+  }
+  if (threadIdx.x == 0) {
+    s_count = 0;
+    s_box[0] = s_box[1] = 1 << 30;
+    s_box[2] = s_box[3] = -1;
+  }
+  __syncthreads();
+  const unsigned B = (unsigned)(s_best >> 32);
+  int* L = lists + (size_t)item * n;
+  int amin = 1 << 30, bmin = 1 << 30, amax = -1, bmax = -1;
+  for (int c = threadIdx.x; c < n; c += blockDim.x)
+    if (P[c] <= B) {
+      L[atomicAdd(&s_count, 1)] = c;
+      int a = c % g.na, b = c / g.na;
+      amin = min(amin, a);
+      amax = max(amax, a);
+      bmin = min(bmin, b);
+      bmax = max(bmax, b);
+    }
+  atomicMin(&s_box[0], amin);
+  atomicMin(&s_box[1], bmin);
+  atomicMax(&s_box[2], amax);
+  atomicMax(&s_box[3], bmax);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    counts[item] = s_count;
+    keys[item] = s_best;
+    for (int k = 0; k < 4; k++) boxes[item * 4 + k] = s_box[k];
+  }
+}
+
+/* bytes of shared memory k_survive may use for the survivors' window */
+#define VSB_SURVIVE_WINDOW (96 * 1024)
+
+/* Full SADs of the survivors (rows [rows0, S) added to their partial sums),
+   folded into the item's key; the last CTA of the item refines.
+   grid (chunks, items); each CTA strides over the survivors by gridDim.x. */
+static __global__ void __launch_bounds__(256) k_survive(const uint8_t* __restrict__ curr,
+                                                 const uint8_t* __restrict__ prev, int pitch,
+                                                 DGeom g, int rows0,
+                                                 const vsbd_item* __restrict__ items,
+                                                 const unsigned* __restrict__ part,
+                                                 const int* __restrict__ counts,
+                                                 const int* __restrict__ lists,
+                                                 const int* __restrict__ boxes,
+                                                 unsigned long long* __restrict__ keys,
+                                                 unsigned* __restrict__ tickets,
+                                                 vsbd_result* __restrict__ res) {
+  extern __shared__ __align__(16) uint8_t sm[];
+  __shared__ int s_last;
+  const int item = blockIdx.y;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int n = g.na * g.nb;
+  const int cnt = counts[item];
+  const bool skipped = g.skip && g.skip[item];
+  const vsbd_item it = items[item];
+  const TileLayout L = tile_layout(g);
+  uint32_t* C = (uint32_t*)sm;
+  bool staged = false;
+  if (!skipped && (int)blockIdx.x < cnt) {
+    const int cx0 = (it.x - g.S / 2) * g.bpp, cy0 = it.y - g.S / 2;
+    const int sh = (cx0 & 3) << 3;
+    for (int i = threadIdx.x; i < g.S * L.rowW; i += blockDim.x) {
+      int r = i / L.rowW, w = i - r * L.rowW;
+      const uint32_t* sw = (const uint32_t*)(curr + (size_t)(cy0 + r) * pitch) + (cx0 >> 2) + w;
+      C[i] = __funnelshift_r(sw[0], sw[1], sh);
+    }
+    staged = true;
+    __syncthreads();
+    const int fx0 = (it.x - g.S / 2 + it.ox) * g.bpp, fy0 = it.y - g.S / 2 + it.oy;
+    const unsigned* P = part + (size_t)item * n;
+    const int* Ls = lists + (size_t)item * n;
+    /* the window of the remaining rows [rows0, S) every survivor can touch:
+       survivors' lattice bounding box, staged with 16-byte loads when it fits */
+    const int amin = boxes[item * 4], bmin = boxes[item * 4 + 1];
+    const int amax = boxes[item * 4 + 2], bmax = boxes[item * 4 + 3];
+    const int rowsR = g.S - rows0;
+    const int wx = fx0 + (g.ax0 + amin * g.step) * g.bpp;
+    const int wy = fy0 + g.by0 + bmin * g.step + rows0;
+    const int wxa = wx & ~15, we = wx - wxa;
+    const int wwb = we + L.rowB + (amax - amin) * g.step * g.bpp;
+    const int wh = rowsR + (bmax - bmin) * g.step;
+    const int nv = (wwb + 15) >> 4;
+    const int WPs = (nv + 1) << 4;
+    uint8_t* win = sm + (size_t)g.S * L.rowB + 16;
+    /* staging pays when this CTA's survivors read the window's bytes several
+       times over; otherwise they read the frame directly */
+    const int mine = (cnt - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
+    const bool in_smem = (size_t)wh * WPs + 16 <= VSB_SURVIVE_WINDOW &&
+                         (size_t)wh * WPs <= (size_t)2 * mine * rowsR * L.rowB;
+    if (in_smem) {
+      for (int i = threadIdx.x; i < wh * nv; i += blockDim.x) {
+        int r = i / nv, v = i - r * nv;
+        *(uint4*)(win + r * WPs + (v << 4)) =
+            *(const uint4*)(prev + (size_t)(wy + r) * pitch + wxa + (v << 4));
+      }
+      __syncthreads();
+    }
+    for (int q = blockIdx.x + gridDim.x * warp; q < cnt; q += gridDim.x * nwarps) {
+      int c = Ls[q];
+      int a = c % g.na, b = c / g.na;
+      unsigned sd;
+      if (in_smem)
+        sd = sad_rows_warp(C + rows0 * L.rowW, L.rowW, rowsR, win, (size_t)WPs,
+                           we + (a - amin) * g.step * g.bpp, (b - bmin) * g.step, lane);
+      else
+        sd = sad_rows_warp(C + rows0 * L.rowW, L.rowW, rowsR, prev, (size_t)pitch,
+                           fx0 + (g.ax0 + a * g.step) * g.bpp, fy0 + g.by0 + b * g.step + rows0,
+                           lane);
+      if (lane == 0)
+        atomicMin(&keys[item], ((unsigned long long)(sd + P[c]) << 32) | (unsigned)g.order[c]);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    unsigned tk = atomicAdd(&tickets[item], 1u);
+    s_last = (tk == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  if (skipped) {
+    if (threadIdx.x == 0) {
+      vsbd_result o;
+      o.sad = 0xffffffffu;
+      o.tx = o.ty = 0;
+      o.ok = 0;
+      res[item] = o;
+      keys[item] = ~0ull;
+      tickets[item] = 0u;
+    }
+    return;
+  }
+  if (!staged) {
+    const int cx0 = (it.x - g.S / 2) * g.bpp, cy0 = it.y - g.S / 2;
+    const int sh = (cx0 & 3) << 3;
+    for (int i = threadIdx.x; i < g.S * L.rowW; i += blockDim.x) {
+      int r = i / L.rowW, w = i - r * L.rowW;
+      const uint32_t* sw = (const uint32_t*)(curr + (size_t)(cy0 + r) * pitch) + (cx0 >> 2) + w;
+      C[i] = __funnelshift_r(sw[0], sw[1], sh);
+    }
+    __syncthreads();
+  }
+  uint8_t* rwin = sm + (size_t)g.S * L.rowB;
+  unsigned* qsad = (unsigned*)(rwin + (size_t)L.RH * L.RP + 32);
+  refine_and_store(g, L, it, C, rwin + 16, prev, pitch, keys, tickets, res, item, qsad);
+}
+
+/* shared memory of k_survive: field, refinement window, refinement SADs */
+__host__ inline size_t survive_smem(const DGeom& g) {
+  DGeom f = g;
+  f.rows = 0;
+  TileLayout L = tile_layout(f);
+  size_t ref = (size_t)L.RH * L.RP + 32 + (size_t)g.maxq * 4 + 16;
+  size_t win = VSB_SURVIVE_WINDOW + 32;
+  return (size_t)g.S * L.rowB + (ref > win ? ref : win);
 }
 
 /* tiling of a field set by the cost model (vsb_device.cu) */
