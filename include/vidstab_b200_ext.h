@@ -60,6 +60,18 @@ VS_API long vsb_detect_clip(int width, int height, int pformat, const uint8_t* f
                             void* out, long out_cap, int* counts, double* elapsed,
                             uint8_t* show_out);
 
+/* Runs nframes frames through an initialised detector, in order, the way a
+   host filter calls vsMotionDetection (on_device = 0: frame k's plane 0 at
+   frames + k*frame_bytes in host memory, show not drawn) or
+   vsb_motion_detection_device (on_device = 1: device addresses).  The
+   LocalMotions of every frame are appended to out (at most out_cap records,
+   LocalMotion layout) and freed; counts[k] receives their number.  The
+   detector's state (previous frame, frame number) carries over between
+   calls.  Returns the number of records, or -1. */
+VS_API long vsb_detect_run(struct _vsmotiondetect* md, const uint8_t* frames, long frame_bytes,
+                           int linesize, int nframes, int on_device, void* out, long out_cap,
+                           int* counts);
+
 /* Per-kernel device time: with timing on, CUDA events bracket every kernel
    of the detector on its stream.  ms[k] and count[k] for k = 0 blur,
    1 field min/max, 2 coarse search, 3 fine search (4 entries each).

@@ -137,3 +137,26 @@ def test_per_frame_api_and_reinit():
     again = np.concatenate([det2.detect(f) for f in frames])
     det2.close()
     assert records_equal(again, exp)
+
+
+def test_detect_run_continues_state():
+    """vsb_detect_run over a clip in two calls gives the records of one
+    detect_clip run over the whole clip, from host and from device frames."""
+    import torch
+    frames = S.clip(640, 360, 6, seed=45)
+    exp, ec, _ = V.detect_clip(frames, V.PF_YUV420P)
+    d = torch.from_numpy(frames).cuda()
+    fb = frames[0].nbytes
+    for on_device in (False, True):
+        det = V.MotionDetector(640, 360, V.PF_YUV420P)
+        out = np.zeros(6 * 512, V.LM_DTYPE)
+        cnt = np.zeros(6, np.int32)
+        base = d.data_ptr() if on_device else frames.ctypes.data
+        n1 = det.run(3, base, fb, 640, on_device, out, cnt)
+        out2 = np.zeros(6 * 512, V.LM_DTYPE)
+        cnt2 = np.zeros(3, np.int32)
+        n2 = det.run(3, base + 3 * fb, fb, 640, on_device, out2, cnt2)
+        det.close()
+        assert np.array_equal(cnt[:3], ec[:3])
+        assert np.array_equal(cnt2, ec[3:])
+        assert records_equal(np.concatenate([out[:n1], out2[:n2]]), exp)

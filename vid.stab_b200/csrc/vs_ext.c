@@ -129,6 +129,42 @@ long vsb_detect_clip(int width, int height, int pformat, const uint8_t* frames, 
   return total;
 }
 
+long vsb_detect_run(VSMotionDetect* md, const uint8_t* frames, long frame_bytes, int linesize,
+                    int nframes, int on_device, void* out, long out_cap, int* counts) {
+  if (!md || !frames || nframes < 0) return -1;
+  LocalMotion* rec = (LocalMotion*)out;
+  long total = 0;
+  for (int k = 0; k < nframes; k++) {
+    LocalMotions lms;
+    const uint8_t* src = frames + (size_t)k * frame_bytes;
+    int rc;
+    if (on_device) {
+      rc = vsb_motion_detection_device(md, &lms, src, linesize);
+    } else {
+      /* only plane 0 is read; the other plane pointers stay valid memory */
+      VSFrame f;
+      memset(&f, 0, sizeof(f));
+      for (int p = 0; p < 4; p++) {
+        f.data[p] = (uint8_t*)src;
+        f.linesize[p] = linesize;
+      }
+      rc = vsMotionDetection(md, &lms, &f);
+    }
+    if (rc != VS_OK) {
+      if (counts) counts[k] = -1;
+      return -1;
+    }
+    int n = vs_vector_size(&lms);
+    if (counts) counts[k] = n;
+    for (int i = 0; i < n; i++) {
+      if (rec && total < out_cap) rec[total] = *LMGet(&lms, i);
+      total++;
+    }
+    vs_vector_del(&lms);
+  }
+  return total;
+}
+
 int vsb_boxblur_host(uint8_t* dst, const uint8_t* src, int width, int height, int size) {
   return vsbd_blur_host(dst, src, width, height, size) == 0 ? VS_OK : VS_ERROR;
 }

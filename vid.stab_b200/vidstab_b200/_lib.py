@@ -116,6 +116,8 @@ def lib():
     L.vsb_detect_clip.restype = C.c_long
     L.vsb_detect_clip.argtypes = [i, i, i, p, C.c_long, i, i, i, i, i, i, d, i, i, i,
                                   C.c_char_p, p, C.c_long, p, p, p]
+    L.vsb_detect_run.restype = C.c_long
+    L.vsb_detect_run.argtypes = [C.POINTER(VSMotionDetect), p, C.c_long, i, i, i, p, C.c_long, p]
     L.vsb_boxblur_host.restype = i
     L.vsb_boxblur_host.argtypes = [p, p, i, i, i]
     L.vsb_field_minmax_host.restype = i

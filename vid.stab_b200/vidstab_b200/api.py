@@ -63,6 +63,19 @@ class MotionDetector:
         self.L.vs_vector_del(C.byref(v))
         return out
 
+    def run(self, n, frames_ptr, frame_bytes, linesize, on_device, out, counts):
+        """Frames n in order through this detector in C (vsb_detect_run):
+        records appended to the preallocated LM_DTYPE array out, per-frame
+        counts to the int32 array counts.  Returns the number of records."""
+        if len(out) * out.itemsize < 32 or len(counts) < n:
+            raise ValueError("output buffers too small")
+        total = self.L.vsb_detect_run(C.byref(self.md), C.c_void_p(frames_ptr), frame_bytes,
+                                      linesize, n, 1 if on_device else 0, ptr(out), len(out),
+                                      ptr(counts))
+        if total < 0:
+            raise RuntimeError("vsb_detect_run failed: %s" % self.L.vsb_last_error().decode())
+        return total
+
     @property
     def frame_num(self):
         return self.md.frameNum
