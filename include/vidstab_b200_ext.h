@@ -140,6 +140,38 @@ VS_API int vsb_field_search_noalloc(const uint8_t* d_curr, const uint8_t* d_prev
                                     int size, int maxShift, int stepSize, const void* d_fields,
                                     int n, void* d_results, void* stream);
 
+/* ---- batched multi-stream detect (no reference counterpart: the reference
+   runs one VSMotionDetect per stream; each stream here gives exactly the
+   LocalMotions a VSMotionDetect of its own would give) ---- */
+typedef struct vsb_batch vsb_batch;
+
+/* n independent streams; stream s has frames of widths[s] x heights[s] in
+   the planar format pformat and the configuration conf[s] (show is not
+   drawn).  One step of all streams runs as two launches of one persistent
+   kernel, each replayed from a captured CUDA graph; the search tilings of
+   every distinct field geometry are picked at creation by timing candidate
+   shapes in that kernel.  Returns NULL on failure (vsb_last_error()). */
+VS_API vsb_batch* vsb_batch_create(int n, const int* widths, const int* heights, int pformat,
+                                   const VSMotionDetectConfig* conf);
+/* One frame of every stream: plane 0 of stream s at planes[s] with row
+   pitch pitches[s] (device addresses with on_device != 0, else host
+   memory).  motions[s] receives the stream's LocalMotions (free with
+   vs_vector_del).  Returns VS_OK or VS_ERROR. */
+VS_API int vsb_batch_detect(vsb_batch* b, const uint8_t* const* planes, const int* pitches,
+                            int on_device, LocalMotions* motions);
+/* nframes steps over clips: frame k of stream s at clips[s] + k *
+   frame_bytes[s].  Records are appended step by step, stream by stream
+   (LocalMotion layout, at most out_cap); counts[k*n + s] receives each
+   frame's count.  Returns the number of records, or -1. */
+VS_API long vsb_batch_run(vsb_batch* b, const uint8_t* const* clips, const long* frame_bytes,
+                          const int* pitches, int nframes, int on_device, void* out,
+                          long out_cap, int* counts);
+VS_API void vsb_batch_free(vsb_batch* b);
+/* persistent-kernel launches so far */
+VS_API long vsb_batch_launch_count(const vsb_batch* b);
+/* the persistent grid: CTAs, threads per CTA, dynamic shared memory per CTA */
+VS_API int vsb_batch_grid(const vsb_batch* b, int* ctas, int* threads, long* smem);
+
 #ifdef __cplusplus
 }
 #endif

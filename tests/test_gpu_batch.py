@@ -1,0 +1,96 @@
+"""Batched multi-stream detect: every stream of a batch gives exactly the
+LocalMotions of a detector of its own (which the other GPU tests pin to the
+reference), across resolutions, frame counts and input kinds."""
+import numpy as np
+import pytest
+
+from conftest import records_equal
+import vidstab_b200 as V
+from vidstab_b200 import synthetic as S
+
+pytestmark = pytest.mark.gpu
+
+
+def per_stream(frames_list, **kw):
+    return [V.detect_clip(f, V.PF_YUV420P, **kw)[:2] for f in frames_list]
+
+
+def batch_records(b, frames_list, on_device):
+    import torch
+    n = len(frames_list)
+    T = frames_list[0].shape[0]
+    held = [torch.from_numpy(f).cuda() for f in frames_list] if on_device else frames_list
+    ptrs = [h.data_ptr() if on_device else h.ctypes.data for h in held]
+    fb = [f[0].nbytes for f in frames_list]
+    pitches = [f.shape[2] for f in frames_list]
+    out = np.zeros(T * n * 1024, V.LM_DTYPE)
+    counts = np.zeros(T * n, np.int32)
+    total = b.run(ptrs, fb, pitches, T, on_device, out, counts)
+    counts = counts.reshape(T, n)
+    # split the step-major record stream back into streams
+    per = [[] for _ in range(n)]
+    pos = 0
+    for k in range(T):
+        for s in range(n):
+            per[s].append(out[pos:pos + counts[k, s]])
+            pos += counts[k, s]
+    assert pos == total
+    return [(np.concatenate(p), counts[:, s]) for s, p in enumerate(per)]
+
+
+@pytest.mark.parametrize("on_device", [False, True])
+def test_batch_mixed_resolutions_match_single_streams(on_device):
+    sizes = [(640, 360), (1280, 720), (640, 360), (1920, 1080), (960, 540)]
+    frames = [S.clip(w, h, 5, seed=100 + i) for i, (w, h) in enumerate(sizes)]
+    b = V.Batch([w for w, _ in sizes], [h for _, h in sizes])
+    try:
+        got = batch_records(b, frames, on_device)
+        assert b.launches() == 2 * 5 - 1  # no fine pass on the first step
+    finally:
+        b.close()
+    for (g, gc), (e, ec) in zip(got, per_stream(frames)):
+        assert np.array_equal(gc, ec)
+        assert records_equal(g, e)
+
+
+def test_batch_4k_and_small_together():
+    sizes = [(3840, 2160), (640, 360), (640, 360)]
+    frames = [S.clip(w, h, 3, seed=200 + i) for i, (w, h) in enumerate(sizes)]
+    b = V.Batch([w for w, _ in sizes], [h for _, h in sizes])
+    try:
+        got = batch_records(b, frames, True)
+    finally:
+        b.close()
+    for (g, gc), (e, ec) in zip(got, per_stream(frames)):
+        assert np.array_equal(gc, ec)
+        assert records_equal(g, e)
+
+
+def test_batch_per_step_api_and_tripod():
+    sizes = [(640, 360), (640, 360)]
+    frames = [S.clip(640, 360, 5, seed=300 + i) for i in range(2)]
+    b = V.Batch([640, 640], [360, 360], tripod=2)
+    try:
+        steps = [b.detect([f[k].ctypes.data for f in frames], [640, 640], False) for k in range(5)]
+    finally:
+        b.close()
+    for s in range(2):
+        exp, ec = per_stream([frames[s]], tripod=2)[0]
+        got = np.concatenate([st[s] for st in steps])
+        assert np.array_equal([len(st[s]) for st in steps], ec)
+        assert records_equal(got, exp)
+
+
+def test_batch_many_streams_of_one_size():
+    n = 24
+    frames = [S.clip(640, 360, 3, seed=400 + i) for i in range(n)]
+    b = V.Batch([640] * n, [360] * n)
+    try:
+        ctas, threads, smem = b.grid()
+        assert ctas >= 148 and threads == 256 and smem > 0
+        got = batch_records(b, frames, True)
+    finally:
+        b.close()
+    for (g, gc), (e, ec) in zip(got, per_stream(frames)):
+        assert np.array_equal(gc, ec)
+        assert records_equal(g, e)

@@ -1,0 +1,163 @@
+/*
+ * vs_batch.c -- the detect pass over many independent streams at once
+ * (declared in vidstab_b200_ext.h; no reference counterpart: the reference
+ * runs one VSMotionDetect per stream).
+ *
+ * Every stream is a VSMotionDetect of its own (fields, selection, simple
+ * model, tripod state: the same host code as vsMotionDetection), without
+ * per-detector device state.  A batch step runs the device work of all
+ * streams as two persistent-kernel launches (vsb_batch.cu) with the
+ * per-stream host phases in between.
+ */
+#include <stdlib.h>
+#include <string.h>
+
+#include "vidstab_b200.h"
+#include "vsb_batch.h"
+#include "vsb_host.h"
+
+struct vsb_batch {
+  int n;
+  VSMotionDetect* md;
+  vsbd_batch* dev;
+  vsb_frame_work* w;
+  int* search;
+  const vsbd_item** items;
+  int* nitems;
+  const vsbd_result** fres;
+};
+
+void vsb_batch_free(vsb_batch* b) {
+  if (!b) return;
+  vsbd_batch_destroy(b->dev);
+  if (b->md)
+    for (int s = 0; s < b->n; s++)
+      if (b->md[s].initialized) vsMotionDetectionCleanup(&b->md[s]);
+  free(b->md);
+  free(b->w);
+  free(b->search);
+  free(b->items);
+  free(b->nitems);
+  free(b->fres);
+  free(b);
+}
+
+vsb_batch* vsb_batch_create(int n, const int* widths, const int* heights, int pformat,
+                            const VSMotionDetectConfig* conf) {
+  if (n < 1 || !widths || !heights || !conf) return NULL;
+  if (pformat <= PF_NONE || pformat >= PF_PACKED) {
+    vsbd_set_error("the batched path takes planar pixel formats only");
+    return NULL;
+  }
+  vsb_batch* b = (vsb_batch*)calloc(1, sizeof(vsb_batch));
+  b->n = n;
+  b->md = (VSMotionDetect*)calloc((size_t)n, sizeof(VSMotionDetect));
+  b->w = (vsb_frame_work*)calloc((size_t)n, sizeof(vsb_frame_work));
+  b->search = (int*)calloc((size_t)n, sizeof(int));
+  b->items = (const vsbd_item**)calloc((size_t)n, sizeof(vsbd_item*));
+  b->nitems = (int*)calloc((size_t)n, sizeof(int));
+  b->fres = (const vsbd_result**)calloc((size_t)n, sizeof(vsbd_result*));
+  vsb_md_layout* lay = (vsb_md_layout*)calloc((size_t)n, sizeof(vsb_md_layout));
+  vsbd_batch_stream* ds = (vsbd_batch_stream*)calloc((size_t)n, sizeof(vsbd_batch_stream));
+  int ok = b->md && b->w && b->search && b->items && b->nitems && b->fres && lay && ds;
+  for (int s = 0; ok && s < n; s++) {
+    VSFrameInfo fi;
+    VSMotionDetectConfig c = conf[s];
+    c.show = 0; /* no host frame to draw into */
+    if (!vsFrameInfoInit(&fi, widths[s], heights[s], (VSPixelFormat)pformat) ||
+        vsb_md_init(&b->md[s], &c, &fi, 0, &lay[s]) != VS_OK) {
+      ok = 0;
+      break;
+    }
+    ds[s].width = widths[s];
+    ds[s].height = heights[s];
+    ds[s].blur_size = lay[s].blur;
+    ds[s].nc = lay[s].nc;
+    ds[s].nf = lay[s].nf;
+    ds[s].xy = lay[s].xy;
+    ds[s].coarse = lay[s].coarse;
+    ds[s].fine = lay[s].fine;
+  }
+  if (ok && vsbd_batch_create(&b->dev, n, ds) != 0) ok = 0;
+  for (int s = 0; lay && s < n; s++) vsb_md_layout_free(&lay[s]);
+  free(lay);
+  free(ds);
+  if (!ok) {
+    vsb_batch_free(b);
+    return NULL;
+  }
+  return b;
+}
+
+int vsb_batch_detect(vsb_batch* b, const uint8_t* const* planes, const int* pitches,
+                     int on_device, LocalMotions* motions) {
+  if (!b || !planes || !pitches || !motions) return VS_ERROR;
+  for (int s = 0; s < b->n; s++)
+    if (vsb_frame_begin(&b->md[s], &b->search[s]) != VS_OK) return VS_ERROR;
+  if (vsbd_batch_stage_a(b->dev, planes, pitches, on_device) != 0) {
+    vs_log_error("vsb_batch", "GPU stage A failed: %s\n", vsbd_error());
+    return VS_ERROR;
+  }
+  for (int s = 0; s < b->n; s++) {
+    b->items[s] = NULL;
+    b->nitems[s] = 0;
+    if (!b->search[s]) continue;
+    const uint8_t* mm;
+    const vsbd_result* cres;
+    vsbd_batch_results_a(b->dev, s, &mm, &cres);
+    vsb_frame_host_a(&b->md[s], mm, cres, &b->w[s]);
+    if (b->w[s].fine_pass) {
+      b->items[s] = b->w[s].items;
+      b->nitems[s] = b->w[s].nitems;
+    }
+  }
+  if (vsbd_batch_stage_b(b->dev, b->items, b->nitems, b->fres) != 0) {
+    vs_log_error("vsb_batch", "GPU stage B failed: %s\n", vsbd_error());
+    for (int s = 0; s < b->n; s++)
+      if (b->search[s]) vsb_frame_discard(&b->w[s]);
+    return VS_ERROR;
+  }
+  for (int s = 0; s < b->n; s++) {
+    if (b->search[s])
+      vsb_frame_host_b(&b->md[s], b->fres[s], &b->w[s], &motions[s]);
+    else
+      vsb_frame_first(&b->md[s], &motions[s]);
+    if (vsb_frame_end(&b->md[s])) vsbd_batch_commit(b->dev, s);
+  }
+  return VS_OK;
+}
+
+long vsb_batch_run(vsb_batch* b, const uint8_t* const* clips, const long* frame_bytes,
+                   const int* pitches, int nframes, int on_device, void* out, long out_cap,
+                   int* counts) {
+  if (!b || !clips || !frame_bytes || !pitches || nframes < 0) return -1;
+  const uint8_t** planes = (const uint8_t**)malloc(sizeof(uint8_t*) * (size_t)b->n);
+  LocalMotions* lms = (LocalMotions*)malloc(sizeof(LocalMotions) * (size_t)b->n);
+  LocalMotion* rec = (LocalMotion*)out;
+  long total = 0;
+  for (int k = 0; k < nframes && total >= 0; k++) {
+    for (int s = 0; s < b->n; s++) planes[s] = clips[s] + (size_t)k * frame_bytes[s];
+    if (vsb_batch_detect(b, planes, pitches, on_device, lms) != VS_OK) {
+      total = -1;
+      break;
+    }
+    for (int s = 0; s < b->n; s++) {
+      int m = vs_vector_size(&lms[s]);
+      if (counts) counts[(size_t)k * b->n + s] = m;
+      for (int i = 0; i < m; i++) {
+        if (rec && total < out_cap) rec[total] = *LMGet(&lms[s], i);
+        total++;
+      }
+      vs_vector_del(&lms[s]);
+    }
+  }
+  free(planes);
+  free(lms);
+  return total;
+}
+
+long vsb_batch_launch_count(const vsb_batch* b) { return b ? vsbd_batch_launches(b->dev) : 0; }
+
+int vsb_batch_grid(const vsb_batch* b, int* ctas, int* threads, long* smem) {
+  return b && vsbd_batch_grid(b->dev, ctas, threads, smem) == 0 ? VS_OK : VS_ERROR;
+}

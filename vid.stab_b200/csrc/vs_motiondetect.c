@@ -249,7 +249,21 @@ static int geometry_fits(const VSMotionDetect* md, const VSMotionDetectFields* f
 }
 
 int vsMotionDetectInit(VSMotionDetect* md, const VSMotionDetectConfig* conf, const VSFrameInfo* fi) {
+  return vsb_md_init(md, conf, fi, 1, NULL);
+}
+
+void vsb_md_layout_free(vsb_md_layout* lay) {
+  if (!lay) return;
+  free(lay->order_c);
+  free(lay->order_f);
+  free(lay->xy);
+  memset(lay, 0, sizeof(*lay));
+}
+
+int vsb_md_init(VSMotionDetect* md, const VSMotionDetectConfig* conf, const VSFrameInfo* fi,
+                int with_device, vsb_md_layout* lay) {
   if (!md || !conf || !fi) return VS_ERROR;
+  if (!with_device && !lay) return VS_ERROR;
   md->conf = *conf;
   md->fi = *fi;
   if (fi->pFormat <= PF_NONE || fi->pFormat == PF_PACKED || fi->pFormat >= PF_NUMBER) {
@@ -348,9 +362,21 @@ int vsMotionDetectInit(VSMotionDetect* md, const VSMotionDetectConfig* conf, con
       xy[2 * nc + nf + i] = md->fieldsfine.fields[i].y;
     }
     int blur = st->planar ? vsb_blur_size(md->conf.stepSize, md->fi.width, md->fi.height) : 0;
-    if (vsbd_create(&st->dev, md->fi.width, md->fi.height, st->bpp, blur, st->nch, &gc, xy,
-                    xy + nc, nc, &gf, xy + 2 * nc, xy + 2 * nc + nf, nf,
-                    md->fieldscoarse.contrastThreshold) != 0) {
+    if (!with_device) {
+      /* the caller runs the device work (batched streams): hand it the layout */
+      lay->coarse = gc;
+      lay->fine = gf;
+      lay->order_c = oc;
+      lay->order_f = of;
+      lay->xy = xy;
+      lay->nc = nc;
+      lay->nf = nf;
+      lay->blur = blur;
+      oc = of = NULL;
+      xy = NULL;
+    } else if (vsbd_create(&st->dev, md->fi.width, md->fi.height, st->bpp, blur, st->nch, &gc,
+                           xy, xy + nc, nc, &gf, xy + 2 * nc, xy + 2 * nc + nf, nf,
+                           md->fieldscoarse.contrastThreshold) != 0) {
       vs_log_error(md->conf.modName, "GPU initialisation failed: %s\n", vsbd_error());
       ok = 0;
     }
@@ -366,8 +392,9 @@ int vsMotionDetectInit(VSMotionDetect* md, const VSMotionDetectConfig* conf, con
     md->fieldsfine.fields = NULL;
     return VS_ERROR;
   }
-  vs_log_info(md->conf.modName, "GPU: sm_100a kernels, blur size %i\n",
-              st->planar ? vsb_blur_size(md->conf.stepSize, md->fi.width, md->fi.height) : 0);
+  if (with_device)
+    vs_log_info(md->conf.modName, "GPU: sm_100a kernels, blur size %i\n",
+                st->planar ? vsb_blur_size(md->conf.stepSize, md->fi.width, md->fi.height) : 0);
   state_insert(st);
   md->initialized = 2;
   return VS_OK;
@@ -479,19 +506,126 @@ static short match_at_most(void* thresh, void* lm) {
   return ((LocalMotion*)lm)->match <= *(double*)thresh ? 1 : 0;
 }
 
-int vsb_detect_common(VSMotionDetect* md, LocalMotions* motions, const uint8_t* host, int linesize,
-                      const uint8_t* dev, int pitch) {
-  if (!md || !motions || md->initialized != 2) {
+int vsb_frame_begin(VSMotionDetect* md, int* search) {
+  if (!md || md->initialized != 2) {
     vs_log_error(md ? md->conf.modName : "vid.stab", "motion detection is not initialised\n");
     return VS_ERROR;
   }
-  md_state* st = state_find(md);
-  if (!st) {
+  if (!state_find(md)) {
     vs_log_error(md->conf.modName, "no device state for this detector\n");
     return VS_ERROR;
   }
   int leadIn = md->conf.virtualTripod >= 1 && md->frameNum < md->conf.virtualTripod;
-  int search = md->hasSeenOneFrame && !leadIn;
+  *search = md->hasSeenOneFrame && !leadIn;
+  return VS_OK;
+}
+
+int vsb_frame_host_a(VSMotionDetect* md, const uint8_t* mm, const vsbd_result* cres,
+                     vsb_frame_work* w) {
+  md_state* st = state_find(md);
+  VSMotionDetectFields* fc = &md->fieldscoarse;
+  VSMotionDetectFields* ff = &md->fieldsfine;
+  vs_vector_init(&w->coarse, fc->maxFields);
+  vs_vector_init(&w->fine, 0);
+  w->fine_pass = 0;
+  w->nitems = 0;
+  w->items = st->items;
+  field_contrasts(st, mm, fc->fieldNum, st->con_c);
+  field_contrasts(st, mm + (size_t)fc->fieldNum * st->nch * 2, ff->fieldNum, st->con_f);
+
+  int nsel = select_fields(st, fc, st->con_c);
+  for (int k = 0; k < nsel; k++) {
+    int i = st->sel[k].index;
+    const vsbd_result* r = &cres[i];
+    if (!r->ok) continue;
+    LocalMotion lm = make_lm(&fc->fields[i], r->tx, r->ty, st->sel[k].contrast, r->sad);
+    vs_vector_append_dup(&w->coarse, &lm, sizeof(LocalMotion));
+  }
+  int num_motions = vs_vector_size(&w->coarse);
+  if (num_motions < 1) {
+    vs_log_warn(md->conf.modName, "too low contrast. (no translations are detected in frame %i)\n",
+                md->frameNum);
+    return VS_OK;
+  }
+  VSTransform t = vsSimpleMotionsToTransform(md->fi, md->conf.modName, &w->coarse);
+  ff->offset = t;
+  ff->useOffset = 1;
+  int nfs = select_fields(st, ff, st->con_f);
+  int nitems = 0;
+  PreparedTransform pt = prepare_transform(&ff->offset, &md->fi);
+  int border = ff->fieldSize / 2 + ff->maxShift + ff->stepSize;
+  for (int k = 0; k < nfs; k++) {
+    const Field* f = &ff->fields[st->sel[k].index];
+    Vec pos = { f->x, f->y };
+    Vec off = sub_vec(transform_vec(&pt, &pos), pos);
+    int x = pos.x + off.x, y = pos.y + off.y;
+    if (x - border < 0 || x + border >= md->fi.width || y - border < 0 ||
+        y + border >= md->fi.height)
+      continue; /* the shifted search would leave the frame (:429-433) */
+    st->items[nitems].x = f->x;
+    st->items[nitems].y = f->y;
+    st->items[nitems].ox = off.x;
+    st->items[nitems].oy = off.y;
+    st->item_sel[nitems] = k;
+    nitems++;
+  }
+  w->fine_pass = 1;
+  w->nitems = nitems;
+  return VS_OK;
+}
+
+void vsb_frame_host_b(VSMotionDetect* md, const vsbd_result* fres, vsb_frame_work* w,
+                      LocalMotions* motions) {
+  md_state* st = state_find(md);
+  VSMotionDetectFields* ff = &md->fieldsfine;
+  if (w->fine_pass) {
+    LocalMotions motions2;
+    vs_vector_init(&motions2, w->nitems > 0 ? w->nitems : 1);
+    for (int m = 0; m < w->nitems; m++) {
+      if (!fres[m].ok) continue;
+      const contrast_idx* s = &st->sel[st->item_sel[m]];
+      LocalMotion lm = make_lm(&ff->fields[s->index], fres[m].tx + st->items[m].ox,
+                               fres[m].ty + st->items[m].oy, s->contrast, fres[m].sad);
+      vs_vector_append_dup(&motions2, &lm, sizeof(LocalMotion));
+    }
+    VSArray q = localmotionsGetMatch(&w->coarse);
+    double meanMatch = cleanmean(q.dat, q.len, NULL, NULL);
+    for (int m = 0; m < vs_vector_size(&motions2); m++) {
+      LocalMotion* lm = LMGet(&motions2, m);
+      if (match_at_most(&meanMatch, lm)) vs_vector_append_dup(&w->fine, lm, sizeof(LocalMotion));
+    }
+    vs_array_free(q);
+    vs_vector_del(&motions2);
+  }
+  if (md->conf.show) vsb_draw_motions(md, &w->coarse, &w->fine);
+  *motions = vs_vector_concat(&w->coarse, &w->fine);
+  vs_vector_fini(&w->coarse);
+  vs_vector_fini(&w->fine);
+}
+
+void vsb_frame_discard(vsb_frame_work* w) {
+  vs_vector_del(&w->coarse);
+  vs_vector_del(&w->fine);
+}
+
+void vsb_frame_first(VSMotionDetect* md, LocalMotions* motions) {
+  vs_vector_init(motions, 1);
+  md->hasSeenOneFrame = 1;
+}
+
+int vsb_frame_end(VSMotionDetect* md) {
+  md_state* st = state_find(md);
+  int commit = md->conf.virtualTripod < 1 || md->frameNum < md->conf.virtualTripod;
+  md->frameNum++;
+  if (st) st->frames++;
+  return commit;
+}
+
+int vsb_detect_common(VSMotionDetect* md, LocalMotions* motions, const uint8_t* host, int linesize,
+                      const uint8_t* dev, int pitch) {
+  int search = 0;
+  if (!motions || vsb_frame_begin(md, &search) != VS_OK) return VS_ERROR;
+  md_state* st = state_find(md);
   const uint8_t* mm = NULL;
   const vsbd_result* cres = NULL;
   if (vsbd_stage_a(st->dev, host, linesize, dev, pitch, search, &mm, &cres) != 0) {
@@ -499,86 +633,19 @@ int vsb_detect_common(VSMotionDetect* md, LocalMotions* motions, const uint8_t* 
     return VS_ERROR;
   }
   if (search) {
-    VSMotionDetectFields* fc = &md->fieldscoarse;
-    VSMotionDetectFields* ff = &md->fieldsfine;
-    LocalMotions coarse, fine;
-    vs_vector_init(&coarse, fc->maxFields);
-    vs_vector_init(&fine, 0);
-    field_contrasts(st, mm, fc->fieldNum, st->con_c);
-    field_contrasts(st, mm + (size_t)fc->fieldNum * st->nch * 2, ff->fieldNum, st->con_f);
-
-    int nsel = select_fields(st, fc, st->con_c);
-    for (int k = 0; k < nsel; k++) {
-      int i = st->sel[k].index;
-      const vsbd_result* r = &cres[i];
-      if (!r->ok) continue;
-      LocalMotion lm = make_lm(&fc->fields[i], r->tx, r->ty, st->sel[k].contrast, r->sad);
-      vs_vector_append_dup(&coarse, &lm, sizeof(LocalMotion));
+    vsb_frame_work w;
+    vsb_frame_host_a(md, mm, cres, &w);
+    const vsbd_result* fres = NULL;
+    if (w.fine_pass && vsbd_stage_b(st->dev, w.items, w.nitems, &fres) != 0) {
+      vs_log_error(md->conf.modName, "GPU stage B failed: %s\n", vsbd_error());
+      vsb_frame_discard(&w);
+      return VS_ERROR;
     }
-    int num_motions = vs_vector_size(&coarse);
-    if (num_motions < 1) {
-      vs_log_warn(md->conf.modName, "too low contrast. (no translations are detected in frame %i)\n",
-                  md->frameNum);
-    } else {
-      VSTransform t = vsSimpleMotionsToTransform(md->fi, md->conf.modName, &coarse);
-      ff->offset = t;
-      ff->useOffset = 1;
-      int nfs = select_fields(st, ff, st->con_f);
-      int nitems = 0;
-      PreparedTransform pt = prepare_transform(&ff->offset, &md->fi);
-      int border = ff->fieldSize / 2 + ff->maxShift + ff->stepSize;
-      for (int k = 0; k < nfs; k++) {
-        const Field* f = &ff->fields[st->sel[k].index];
-        Vec pos = { f->x, f->y };
-        Vec off = sub_vec(transform_vec(&pt, &pos), pos);
-        int x = pos.x + off.x, y = pos.y + off.y;
-        if (x - border < 0 || x + border >= md->fi.width || y - border < 0 ||
-            y + border >= md->fi.height)
-          continue; /* the shifted search would leave the frame (:429-433) */
-        st->items[nitems].x = f->x;
-        st->items[nitems].y = f->y;
-        st->items[nitems].ox = off.x;
-        st->items[nitems].oy = off.y;
-        st->item_sel[nitems] = k;
-        nitems++;
-      }
-      const vsbd_result* fres = NULL;
-      if (vsbd_stage_b(st->dev, st->items, nitems, &fres) != 0) {
-        vs_log_error(md->conf.modName, "GPU stage B failed: %s\n", vsbd_error());
-        vs_vector_del(&coarse);
-        vs_vector_del(&fine);
-        return VS_ERROR;
-      }
-      LocalMotions motions2;
-      vs_vector_init(&motions2, nitems > 0 ? nitems : 1);
-      for (int m = 0; m < nitems; m++) {
-        if (!fres[m].ok) continue;
-        const contrast_idx* s = &st->sel[st->item_sel[m]];
-        LocalMotion lm = make_lm(&ff->fields[s->index], fres[m].tx + st->items[m].ox,
-                                 fres[m].ty + st->items[m].oy, s->contrast, fres[m].sad);
-        vs_vector_append_dup(&motions2, &lm, sizeof(LocalMotion));
-      }
-      VSArray q = localmotionsGetMatch(&coarse);
-      double meanMatch = cleanmean(q.dat, q.len, NULL, NULL);
-      for (int m = 0; m < vs_vector_size(&motions2); m++) {
-        LocalMotion* lm = LMGet(&motions2, m);
-        if (match_at_most(&meanMatch, lm)) vs_vector_append_dup(&fine, lm, sizeof(LocalMotion));
-      }
-      vs_array_free(q);
-      vs_vector_del(&motions2);
-    }
-    if (md->conf.show) vsb_draw_motions(md, &coarse, &fine);
-    *motions = vs_vector_concat(&coarse, &fine);
-    vs_vector_fini(&coarse);
-    vs_vector_fini(&fine);
+    vsb_frame_host_b(md, fres, &w, motions);
   } else {
-    vs_vector_init(motions, 1);
-    md->hasSeenOneFrame = 1;
+    vsb_frame_first(md, motions);
   }
-  if (md->conf.virtualTripod < 1 || md->frameNum < md->conf.virtualTripod)
-    vsbd_commit_prev(st->dev);
-  md->frameNum++;
-  st->frames++;
+  if (vsb_frame_end(md)) vsbd_commit_prev(st->dev);
   return VS_OK;
 }
 

@@ -1,0 +1,813 @@
+/*
+ * vsb_batch.cu -- the detect pass of many independent streams at once, in
+ * one persistent kernel per stage, each stage replayed from a captured CUDA
+ * graph.
+ *
+ * A batch step advances every stream by one frame.  The device work of the
+ * step is two queues of work items:
+ *   stage A  blur tiles of every stream's new frame, then the coarse search
+ *            tiles (field x lattice tile) of every stream, then the min/max
+ *            of every stream's coarse and fine fields;
+ *   stage B  the fine search tiles of the fine work lists the host built
+ *            from stage A's results (selection, simple model, offsets --
+ *            the same host code as the per-stream detector).
+ * The persistent kernel's CTAs (as many as fit on the GPU at once) take
+ * items from the queue in order with one atomic counter.  A search or
+ * min/max item of a stream first waits until every blur tile of that
+ * stream's frame is written: all blur items sit earlier in the queue, so they
+ * were taken by CTAs that are running, and the wait always ends; it is
+ * bounded anyway (time and iterations), after which the item is skipped and
+ * an error flag is raised for the host.
+ *
+ * Each search item is exactly one CTA of the per-stream search kernel
+ * (lattice_tile), with the same tiling rules, so each stream's results are
+ * the per-stream detector's, bit for bit.  The tilings of every resolution
+ * class are picked by timing candidate shapes in the persistent kernel itself
+ * at batch creation.
+ */
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "vsb_batch.h"
+#include "vsb_plan.h"
+#include "vsb_prefilter.cuh"
+#include "vsb_search.cuh"
+
+#define VSB_BATCH_THREADS 256
+#define VSB_BATCH_MAX_STREAMS 1024
+#define VSB_BATCH_MAX_CLASSES 64
+
+/* per-stream descriptor, in device memory (rewritten every step) */
+struct BStream {
+  const uint8_t* src; /* raw plane 0 of this step's frame */
+  int sp;             /* its row pitch */
+  uint8_t* cur;       /* blurred current frame */
+  uint8_t* prev;      /* blurred previous frame */
+  int pitch, W, H, half;
+  BlurDiv dv;
+  int ntx, nty;           /* blur tiles */
+  const int16_t* xy;      /* coarse x[nc], coarse y[nc], fine x[nf], fine y[nf] */
+  int nc, nf, Sc, Sf;
+  int gc, gf;             /* geometry classes of the coarse and fine fields */
+  const vsbd_item* citems;
+  unsigned long long* keys; /* coarse [0,nc), fine [nc, nc+nf) */
+  unsigned* tickets;
+  uint8_t* mm;            /* out: (nc+nf) (min,max) pairs */
+  vsbd_result* cres;      /* out: nc */
+  vsbd_result* fres;      /* out: nf */
+};
+
+/* stage-A work item: type 0 blur tile a; 1 min/max of field a; 2 coarse search
+   tile a = item * ntiles + tile */
+struct BWork {
+  int type, stream, a, pad;
+};
+
+/* control block of one stage */
+struct BCtl {
+  unsigned head;
+  unsigned err;
+  unsigned blur_done[VSB_BATCH_MAX_STREAMS];
+  int nwork; /* set by the host; not cleared per launch */
+  int pad;
+};
+
+/* Bounded wait of one CTA until stream s has `target` blur tiles written.
+   Returns 0 if the wait gave up (the error flag is raised). */
+__device__ __forceinline__ int wait_blur(BCtl* ctl, int s, unsigned target) {
+  __shared__ int s_ok;
+  if (threadIdx.x == 0) {
+    const long long t0 = clock64();
+    unsigned spins = 0;
+    int ok = 1;
+    while (*(volatile unsigned*)&ctl->blur_done[s] < target) {
+      if (++spins > (1u << 24) || clock64() - t0 > 8000000000ll) {
+        ok = 0;
+        atomicExch(&ctl->err, 1u);
+        break;
+      }
+      __nanosleep(100);
+    }
+    __threadfence();
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok;
+}
+
+__device__ __forceinline__ void search_tile(const BStream& S, const DGeom* geoms, int cls,
+                                            const vsbd_item* items, unsigned long long* keys,
+                                            unsigned* tickets, vsbd_result* res, int item,
+                                            int tile, DGeom* sg, uint8_t* sm) {
+  if (threadIdx.x == 0) *sg = geoms[cls];
+  __syncthreads();
+  const DGeom& g = *sg;
+  const unsigned ntiles = (unsigned)(g.nta * g.ntb);
+  if (g.tb == 4)
+    lattice_tile<4, false>(S.cur, S.prev, S.pitch, g, items, keys, tickets, res, item, tile,
+                           ntiles, sm);
+  else
+    lattice_tile<2, false>(S.cur, S.prev, S.pitch, g, items, keys, tickets, res, item, tile,
+                           ntiles, sm);
+}
+
+/* Stage A: the static work list `work`.  Stage B (work == NULL): item w of
+   the fine search is found from the per-stream prefix sums (tile-granular)
+   and item offsets into the packed fine work list. */
+__global__ void __launch_bounds__(VSB_BATCH_THREADS) k_batch(const BWork* __restrict__ work,
+                                                             const BStream* __restrict__ streams,
+                                                             const DGeom* __restrict__ geoms,
+                                                             BCtl* ctl, const int* __restrict__ prefix,
+                                                             const int* __restrict__ item_off,
+                                                             const vsbd_item* __restrict__ fitems,
+                                                             int nstreams) {
+  extern __shared__ __align__(16) uint8_t sm[];
+  __shared__ int s_w;
+  __shared__ DGeom sg;
+  const int nwork = ctl->nwork;
+  for (;;) {
+    if (threadIdx.x == 0) s_w = (int)atomicAdd(&ctl->head, 1u);
+    __syncthreads();
+    const int w = s_w;
+    if (w >= nwork) break;
+    if (work) {
+      const BWork it = work[w];
+      const BStream& S = streams[it.stream];
+      if (it.type == 0) {
+        blur_tile(S.src, S.sp, S.cur, S.pitch, S.W, S.H, S.half, S.dv, it.a % S.ntx,
+                  it.a / S.ntx, sm);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+          __threadfence();
+          atomicAdd(&ctl->blur_done[it.stream], 1u);
+        }
+      } else if (wait_blur(ctl, it.stream, (unsigned)(S.ntx * S.nty))) {
+        if (it.type == 1) {
+          const int f = it.a;
+          const bool coarse = f < S.nc;
+          const int x = coarse ? S.xy[f] : S.xy[2 * S.nc + (f - S.nc)];
+          const int y = coarse ? S.xy[S.nc + f] : S.xy[2 * S.nc + S.nf + (f - S.nc)];
+          minmax_field(S.cur, S.pitch, x, y, coarse ? S.Sc : S.Sf, 1, 1, f, S.mm, 0.0, NULL);
+        } else {
+          const DGeom* gp = &geoms[S.gc];
+          const int ntiles = gp->nta * gp->ntb;
+          search_tile(S, geoms, S.gc, S.citems, S.keys, S.tickets, S.cres, it.a / ntiles,
+                      it.a % ntiles, &sg, sm);
+        }
+      }
+    } else {
+      /* stream of item w: largest s with prefix[s] <= w */
+      int lo = 0, hi = nstreams - 1;
+      while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (prefix[mid] <= w) lo = mid; else hi = mid - 1;
+      }
+      const BStream& S = streams[lo];
+      const DGeom* gp = &geoms[S.gf];
+      const int ntiles = gp->nta * gp->ntb;
+      const int local = w - prefix[lo];
+      search_tile(S, geoms, S.gf, fitems + item_off[lo], S.keys + S.nc, S.tickets + S.nc, S.fres,
+                  local / ntiles, local % ntiles, &sg, sm);
+    }
+    __syncthreads();
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* host side                                                                 */
+/* ------------------------------------------------------------------------ */
+
+struct vsbd_batch {
+  int dev, n, ncls;
+  cudaStream_t st;
+  /* geometry classes */
+  GeomDev cls[VSB_BATCH_MAX_CLASSES];
+  vsbd_geom cls_key[VSB_BATCH_MAX_CLASSES]; /* order: owned copy */
+  size_t static_smem;                       /* of k_batch */
+  int optin;                                /* per-block shared memory limit */
+  size_t nkeys;
+  DGeom* d_geoms;
+  /* streams */
+  BStream* h_streams; /* pinned */
+  BStream* d_streams;
+  uint8_t** raw;      /* per stream: raw upload buffer (host input) */
+  uint8_t** buf[2];   /* per stream: blurred planes */
+  int* cur;           /* per stream: index of the current buffer */
+  int16_t** d_xy;
+  vsbd_item** d_citems;
+  unsigned long long* d_keys;
+  unsigned* d_tickets;
+  size_t* key_off;    /* per stream: offset of its keys/tickets */
+  /* results */
+  uint8_t* d_resA;
+  uint8_t* h_resA;
+  size_t resA_bytes;
+  size_t* mm_off;
+  size_t* cres_off;
+  vsbd_result* d_resB;
+  vsbd_result* h_resB;
+  size_t* fres_off;   /* in results */
+  int nf_total;
+  /* stage A */
+  BWork* d_workA;
+  int nworkA;
+  BCtl* d_ctlA;
+  /* stage B */
+  BCtl* d_ctlB;
+  int* d_pre; /* prefix[n+1], item_off[n] */
+  int* h_pre;
+  vsbd_item* d_fitems;
+  vsbd_item* h_fitems;
+  int* h_nwork;
+  /* persistent grid */
+  size_t smem;
+  int grid;
+  cudaGraphExec_t gA, gB;
+  long launches;
+  long steps;
+};
+
+#define BCK(call)                             \
+  do {                                        \
+    cudaError_t e_ = (call);                  \
+    if (e_ != cudaSuccess) {                  \
+      vsbp_set_err(#call, e_);                \
+      return -1;                              \
+    }                                         \
+  } while (0)
+
+static size_t al16(size_t x) { return (x + 15) & ~(size_t)15; }
+
+static int same_geom(const vsbd_geom* a, const vsbd_geom* b) {
+  if (a->size != b->size || a->bpp != b->bpp || a->step != b->step || a->na != b->na ||
+      a->nb != b->nb || a->ax0 != b->ax0 || a->by0 != b->by0 || a->has_origin != b->has_origin ||
+      a->nstages != b->nstages || a->limx != b->limx || a->limy != b->limy)
+    return 0;
+  for (int k = 0; k < a->nstages; k++)
+    if (a->st_r[k] != b->st_r[k] || a->st_h[k] != b->st_h[k]) return 0;
+  return memcmp(a->order, b->order, sizeof(int32_t) * (size_t)a->na * a->nb) == 0;
+}
+
+/* a tiling the persistent kernel can run: TB 2 or 4, at most its block
+   size, tile and static shared memory within the per-block limit */
+static int tiling_ok(const vsbd_batch* b, const DGeom& g) {
+  return (g.tb == 2 || g.tb == 4) && g.threads <= VSB_BATCH_THREADS &&
+         tile_layout(g).total + b->static_smem + 64 <= (size_t)b->optin;
+}
+
+static int class_of(vsbd_batch* b, const vsbd_geom* g, int nitems) {
+  for (int k = 0; k < b->ncls; k++)
+    if (same_geom(&b->cls_key[k], g)) return k;
+  if (b->ncls >= VSB_BATCH_MAX_CLASSES) {
+    vsbp_set_msg("too many distinct field geometries in one batch");
+    return -1;
+  }
+  int k = b->ncls;
+  if (vsbp_geom_upload(g, nitems, &b->cls[k]) != 0) return -1;
+  size_t no = sizeof(int32_t) * (size_t)g->na * g->nb;
+  int32_t* own = (int32_t*)malloc(no);
+  if (!own) { vsbp_set_msg("out of host memory"); vsbp_geom_free(&b->cls[k]); return -1; }
+  memcpy(own, g->order, no);
+  b->cls_key[k] = *g;
+  b->cls_key[k].order = own;
+  b->ncls++;
+  /* the default tiling: the model's best that the persistent kernel runs */
+  TileCand cand[16];
+  int nc = vsbp_tile_candidates(b->cls[k].g, nitems, VSB_BATCH_THREADS, cand, 16);
+  for (int i = 0; i < nc; i++)
+    if (tiling_ok(b, cand[i].g)) {
+      DGeom t = cand[i].g;
+      t.order = b->cls[k].g.order;
+      t.point = b->cls[k].g.point;
+      b->cls[k].g = t;
+      b->cls[k].smem = tile_layout(t).total;
+      return k;
+    }
+  vsbp_set_msg("no search tiling of the batched kernel fits in shared memory");
+  return -1;
+}
+
+static size_t kernel_smem(const vsbd_batch* b) {
+  size_t m = BT_SMEM;
+  for (int k = 0; k < b->ncls; k++) {
+    size_t t = tile_layout(b->cls[k].g).total;
+    if (t > m) m = t;
+  }
+  return m;
+}
+
+static int set_grid(vsbd_batch* b) {
+  b->smem = kernel_smem(b);
+  BCK(cudaFuncSetAttribute(k_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem));
+  int per = 0;
+  BCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_batch, VSB_BATCH_THREADS, b->smem));
+  if (per < 1) {
+    vsbp_set_msg("the batched kernel does not fit on an SM");
+    return -1;
+  }
+  b->grid = per * vsbp_sm_count();
+  return 0;
+}
+
+static int upload_geoms(vsbd_batch* b) {
+  DGeom h[VSB_BATCH_MAX_CLASSES];
+  for (int k = 0; k < b->ncls; k++) h[k] = b->cls[k].g;
+  BCK(cudaMemcpy(b->d_geoms, h, sizeof(DGeom) * b->ncls, cudaMemcpyHostToDevice));
+  return 0;
+}
+
+/* stage-A work list: blur tiles, coarse search tiles (heaviest classes
+   first), min/max of every field */
+static int build_workA(vsbd_batch* b, BWork** out, int* count, int only_cls, int fine_cls_tune) {
+  long total = 0;
+  for (int s = 0; s < b->n; s++) {
+    const BStream& S = b->h_streams[s];
+    if (only_cls < 0) total += (long)S.ntx * S.nty + S.nc + S.nf;
+    const int cg = fine_cls_tune ? S.gf : S.gc;
+    const int ni = fine_cls_tune ? S.nf : S.nc;
+    if (only_cls < 0 || cg == only_cls)
+      total += (long)ni * b->cls[cg].g.nta * b->cls[cg].g.ntb;
+  }
+  BWork* w = (BWork*)malloc(sizeof(BWork) * (size_t)(total + 1));
+  if (!w) { vsbp_set_msg("out of host memory"); return -1; }
+  long k = 0;
+  if (only_cls < 0)
+    for (int s = 0; s < b->n; s++)
+      for (int t = 0; t < b->h_streams[s].ntx * b->h_streams[s].nty; t++) w[k++] = { 0, s, t, 0 };
+  /* search items, by class cost (descending) */
+  int order[VSB_BATCH_MAX_CLASSES];
+  for (int c = 0; c < b->ncls; c++) order[c] = c;
+  for (int i = 1; i < b->ncls; i++)
+    for (int j = i; j > 0; j--) {
+      const DGeom& x = b->cls[order[j]].g;
+      const DGeom& y = b->cls[order[j - 1]].g;
+      double cx = (double)x.S * x.S * x.na * x.nb, cy = (double)y.S * y.S * y.na * y.nb;
+      if (cx > cy) { int t = order[j]; order[j] = order[j - 1]; order[j - 1] = t; }
+    }
+  for (int oc = 0; oc < b->ncls; oc++) {
+    const int c = order[oc];
+    if (only_cls >= 0 && c != only_cls) continue;
+    for (int s = 0; s < b->n; s++) {
+      const BStream& S = b->h_streams[s];
+      const int cg = fine_cls_tune ? S.gf : S.gc;
+      if (cg != c) continue;
+      const int ni = fine_cls_tune ? S.nf : S.nc;
+      const int nt = b->cls[c].g.nta * b->cls[c].g.ntb;
+      for (int i = 0; i < ni; i++)
+        for (int t = 0; t < nt; t++) w[k++] = { 2, s, i * nt + t, 0 };
+    }
+  }
+  if (only_cls < 0)
+    for (int s = 0; s < b->n; s++)
+      for (int f = 0; f < b->h_streams[s].nc + b->h_streams[s].nf; f++) w[k++] = { 1, s, f, 0 };
+  *out = w;
+  *count = (int)k;
+  return 0;
+}
+
+static int launch_k(vsbd_batch* b, const BWork* work, BCtl* ctl, cudaStream_t st) {
+  k_batch<<<b->grid, VSB_BATCH_THREADS, b->smem, st>>>(work, b->d_streams, b->d_geoms, ctl,
+                                                       b->d_pre, b->d_pre + b->n + 1, b->d_fitems,
+                                                       b->n);
+  BCK(cudaGetLastError());
+  return 0;
+}
+
+/* Times the model's best tilings of one class inside the persistent kernel
+   (the class's search items alone, all streams of the class, zero offsets)
+   and keeps the fastest. */
+static int autotune_class(vsbd_batch* b, int c, int is_fine) {
+  int nitems = 0;
+  for (int s = 0; s < b->n; s++) {
+    const BStream& S = b->h_streams[s];
+    if ((is_fine ? S.gf : S.gc) == c) nitems += is_fine ? S.nf : S.nc;
+  }
+  if (nitems == 0 || getenv("VSB_NO_AUTOTUNE")) return 0;
+  TileCand cand[16];
+  int nc = vsbp_tile_candidates(b->cls[c].g, nitems, VSB_BATCH_THREADS, cand, 16);
+  cudaEvent_t e0, e1;
+  BCK(cudaEventCreate(&e0));
+  BCK(cudaEventCreate(&e1));
+  float best_ms = 1e30f;
+  DGeom best = b->cls[c].g;
+  int tried = 0;
+  for (int k = 0; k < nc && tried < 8; k++) {
+    if (!tiling_ok(b, cand[k].g)) continue;
+    tried++;
+    DGeom t = cand[k].g;
+    t.order = b->cls[c].g.order;
+    t.point = b->cls[c].g.point;
+    DGeom keep = b->cls[c].g;
+    b->cls[c].g = t;
+    BWork* w = NULL;
+    int nw = 0;
+    if (set_grid(b) != 0 || upload_geoms(b) != 0 || build_workA(b, &w, &nw, c, is_fine) != 0) {
+      b->cls[c].g = keep;
+      free(w);
+      continue;
+    }
+    BWork* d_w = NULL;
+    cudaError_t e = cudaMalloc(&d_w, sizeof(BWork) * (size_t)(nw + 1));
+    if (e == cudaSuccess) e = cudaMemcpy(d_w, w, sizeof(BWork) * nw, cudaMemcpyHostToDevice);
+    free(w);
+    if (e != cudaSuccess) { cudaFree(d_w); b->cls[c].g = keep; vsbp_set_err("tuning buffers", e); return -1; }
+    float ms = 0.f;
+    int ok = 1;
+    for (int rep = 0; rep < 4 && ok; rep++) {
+      /* the tuning list has no blur items: mark every stream's blur done */
+      BCtl h;
+      memset(&h, 0, sizeof(h));
+      for (int s = 0; s < b->n; s++)
+        h.blur_done[s] = (unsigned)(b->h_streams[s].ntx * b->h_streams[s].nty);
+      h.nwork = nw;
+      if (cudaMemcpyAsync(b->d_ctlA, &h, sizeof(h), cudaMemcpyHostToDevice, b->st) != cudaSuccess)
+        ok = 0;
+      if (rep == 1) cudaEventRecord(e0, b->st);
+      if (ok && launch_k(b, d_w, b->d_ctlA, b->st) != 0) ok = 0;
+      if (rep == 3) cudaEventRecord(e1, b->st);
+      if (cudaStreamSynchronize(b->st) != cudaSuccess) ok = 0;
+    }
+    if (ok) cudaEventElapsedTime(&ms, e0, e1);
+    cudaFree(d_w);
+    b->cls[c].g = keep;
+    if (ok && ms < best_ms) {
+      best_ms = ms;
+      best = t;
+    }
+    if (!ok) break;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  BCK(cudaGetLastError());
+  b->cls[c].g = best;
+  b->cls[c].smem = tile_layout(best).total;
+  return 0;
+}
+
+static int capture(vsbd_batch* b, int stageB, cudaGraphExec_t* out) {
+  cudaGraph_t g = NULL;
+  BCK(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
+  BCtl* ctl = stageB ? b->d_ctlB : b->d_ctlA;
+  cudaMemsetAsync(ctl, 0, offsetof(BCtl, nwork), b->st);
+  k_batch<<<b->grid, VSB_BATCH_THREADS, b->smem, b->st>>>(stageB ? NULL : b->d_workA,
+                                                          b->d_streams, b->d_geoms, ctl, b->d_pre,
+                                                          b->d_pre + b->n + 1, b->d_fitems, b->n);
+  if (stageB)
+    cudaMemcpyAsync(b->h_resB, b->d_resB, sizeof(vsbd_result) * (size_t)(b->nf_total + 1),
+                    cudaMemcpyDeviceToHost, b->st);
+  else
+    cudaMemcpyAsync(b->h_resA, b->d_resA, b->resA_bytes, cudaMemcpyDeviceToHost, b->st);
+  cudaMemcpyAsync(stageB ? (void*)&b->h_nwork[1] : (void*)&b->h_nwork[2], &ctl->err,
+                  sizeof(unsigned), cudaMemcpyDeviceToHost, b->st);
+  cudaError_t e = cudaStreamEndCapture(b->st, &g);
+  if (e != cudaSuccess) { vsbp_set_err("graph capture", e); return -1; }
+  e = cudaGraphInstantiate(out, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) { vsbp_set_err("graph instantiation", e); return -1; }
+  return 0;
+}
+
+extern "C" void vsbd_batch_destroy(vsbd_batch* b) {
+  if (!b) return;
+  cudaSetDevice(b->dev);
+  if (b->st) cudaStreamSynchronize(b->st);
+  if (b->gA) cudaGraphExecDestroy(b->gA);
+  if (b->gB) cudaGraphExecDestroy(b->gB);
+  for (int s = 0; s < b->n; s++) {
+    if (b->raw) cudaFree(b->raw[s]);
+    if (b->buf[0]) cudaFree(b->buf[0][s]);
+    if (b->buf[1]) cudaFree(b->buf[1][s]);
+    if (b->d_xy) cudaFree(b->d_xy[s]);
+    if (b->d_citems) cudaFree(b->d_citems[s]);
+  }
+  for (int k = 0; k < b->ncls; k++) {
+    vsbp_geom_free(&b->cls[k]);
+    free((void*)b->cls_key[k].order);
+  }
+  cudaFree(b->d_geoms);
+  cudaFree(b->d_streams);
+  cudaFreeHost(b->h_streams);
+  cudaFree(b->d_keys);
+  cudaFree(b->d_tickets);
+  cudaFree(b->d_resA);
+  cudaFreeHost(b->h_resA);
+  cudaFree(b->d_resB);
+  cudaFreeHost(b->h_resB);
+  cudaFree(b->d_workA);
+  cudaFree(b->d_ctlA);
+  cudaFree(b->d_ctlB);
+  cudaFree(b->d_pre);
+  cudaFreeHost(b->h_pre);
+  cudaFree(b->d_fitems);
+  cudaFreeHost(b->h_fitems);
+  cudaFreeHost(b->h_nwork);
+  free(b->raw);
+  free(b->buf[0]);
+  free(b->buf[1]);
+  free(b->cur);
+  free(b->d_xy);
+  free(b->d_citems);
+  free(b->key_off);
+  free(b->mm_off);
+  free(b->cres_off);
+  free(b->fres_off);
+  if (b->st) cudaStreamDestroy(b->st);
+  free(b);
+}
+
+extern "C" int vsbd_batch_create(vsbd_batch** out, int n, const vsbd_batch_stream* d) {
+  *out = NULL;
+  if (n < 1 || n > VSB_BATCH_MAX_STREAMS) {
+    vsbp_set_msg("batch size out of range (1..1024 streams)");
+    return -1;
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
+    vsbp_set_msg("no CUDA device available (the GPU path has no CPU fallback)");
+    return -1;
+  }
+  vsbd_batch* b = (vsbd_batch*)calloc(1, sizeof(vsbd_batch));
+  cudaGetDevice(&b->dev);
+  b->n = n;
+  {
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, k_batch) != cudaSuccess ||
+        cudaDeviceGetAttribute(&b->optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->dev) !=
+            cudaSuccess) {
+      vsbp_set_msg("cannot query the batched kernel");
+      free(b);
+      return -1;
+    }
+    b->static_smem = fa.sharedSizeBytes;
+  }
+#define CKB(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) { vsbp_set_err(#call, e_); vsbd_batch_destroy(b); return -1; } } while (0)
+#define FAILB() do { vsbd_batch_destroy(b); return -1; } while (0)
+  CKB(cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking));
+  b->raw = (uint8_t**)calloc(n, sizeof(uint8_t*));
+  b->buf[0] = (uint8_t**)calloc(n, sizeof(uint8_t*));
+  b->buf[1] = (uint8_t**)calloc(n, sizeof(uint8_t*));
+  b->cur = (int*)calloc(n, sizeof(int));
+  b->d_xy = (int16_t**)calloc(n, sizeof(int16_t*));
+  b->d_citems = (vsbd_item**)calloc(n, sizeof(vsbd_item*));
+  b->key_off = (size_t*)calloc(n, sizeof(size_t));
+  b->mm_off = (size_t*)calloc(n, sizeof(size_t));
+  b->cres_off = (size_t*)calloc(n, sizeof(size_t));
+  b->fres_off = (size_t*)calloc(n, sizeof(size_t));
+  CKB(cudaMallocHost(&b->h_streams, sizeof(BStream) * n));
+  memset(b->h_streams, 0, sizeof(BStream) * n);
+  CKB(cudaMalloc(&b->d_streams, sizeof(BStream) * n));
+  CKB(cudaMalloc(&b->d_geoms, sizeof(DGeom) * VSB_BATCH_MAX_CLASSES));
+  size_t nkeys = 0, resA = 0;
+  int nf_total = 0;
+  for (int s = 0; s < n; s++) {
+    const vsbd_batch_stream& q = d[s];
+    if (q.blur_size >= 2 && q.blur_size / 2 > BT_MAXHALF) {
+      vsbp_set_msg("blur window too wide for the batched kernel");
+      FAILB();
+    }
+    BStream& S = b->h_streams[s];
+    S.W = q.width;
+    S.H = q.height;
+    S.pitch = (int)(((size_t)q.width + 127) & ~(size_t)127);
+    S.half = q.blur_size >= 2 ? q.blur_size / 2 : 0;
+    make_div(q.blur_size >= 2 ? q.blur_size : 1, S.half, &S.dv);
+    if (q.blur_size < 2) { S.dv.mul = 0; S.dv.size = 1; S.dv.exact = 0; }
+    S.ntx = (q.width + BT_W - 1) / BT_W;
+    S.nty = (q.height + BT_H - 1) / BT_H;
+    S.nc = q.nc;
+    S.nf = q.nf;
+    S.Sc = q.coarse.size;
+    S.Sf = q.fine.size;
+    if (q.coarse.bpp != 1 || q.fine.bpp != 1) {
+      vsbp_set_msg("the batched path takes planar formats only");
+      FAILB();
+    }
+    int gc = class_of(b, &q.coarse, q.nc);
+    int gf = gc < 0 ? -1 : class_of(b, &q.fine, q.nf);
+    if (gc < 0 || gf < 0) FAILB();
+    S.gc = gc;
+    S.gf = gf;
+    size_t plane = (size_t)S.pitch * q.height + 256;
+    CKB(cudaMalloc(&b->raw[s], plane));
+    CKB(cudaMalloc(&b->buf[0][s], plane));
+    CKB(cudaMalloc(&b->buf[1][s], plane));
+    CKB(cudaMemset(b->buf[0][s], 0, plane));
+    CKB(cudaMemset(b->buf[1][s], 0, plane));
+    CKB(cudaMalloc(&b->d_xy[s], sizeof(int16_t) * 2 * (size_t)(q.nc + q.nf) + 16));
+    CKB(cudaMemcpy(b->d_xy[s], q.xy, sizeof(int16_t) * 2 * (size_t)(q.nc + q.nf),
+                   cudaMemcpyHostToDevice));
+    vsbd_item* it = (vsbd_item*)malloc(sizeof(vsbd_item) * (size_t)(q.nc + 1));
+    for (int i = 0; i < q.nc; i++) { it[i].x = q.xy[i]; it[i].y = q.xy[q.nc + i]; it[i].ox = 0; it[i].oy = 0; }
+    cudaError_t e3 = cudaMalloc(&b->d_citems[s], sizeof(vsbd_item) * (size_t)(q.nc + 1));
+    if (e3 == cudaSuccess)
+      e3 = cudaMemcpy(b->d_citems[s], it, sizeof(vsbd_item) * q.nc, cudaMemcpyHostToDevice);
+    free(it);
+    CKB(e3);
+    b->key_off[s] = nkeys;
+    nkeys += (size_t)q.nc + q.nf;
+    b->mm_off[s] = resA;
+    resA = al16(resA + 2 * (size_t)(q.nc + q.nf));
+    b->cres_off[s] = resA;
+    resA = al16(resA + sizeof(vsbd_result) * (size_t)q.nc);
+    b->fres_off[s] = (size_t)nf_total;
+    nf_total += q.nf;
+  }
+  b->nf_total = nf_total;
+  b->nkeys = nkeys;
+  b->resA_bytes = resA + 16;
+  CKB(cudaMalloc(&b->d_keys, sizeof(unsigned long long) * (nkeys + 1)));
+  CKB(cudaMemset(b->d_keys, 0xff, sizeof(unsigned long long) * (nkeys + 1)));
+  CKB(cudaMalloc(&b->d_tickets, sizeof(unsigned) * (nkeys + 1)));
+  CKB(cudaMemset(b->d_tickets, 0, sizeof(unsigned) * (nkeys + 1)));
+  CKB(cudaMalloc(&b->d_resA, b->resA_bytes));
+  CKB(cudaMallocHost(&b->h_resA, b->resA_bytes));
+  CKB(cudaMalloc(&b->d_resB, sizeof(vsbd_result) * (size_t)(nf_total + 1)));
+  CKB(cudaMallocHost(&b->h_resB, sizeof(vsbd_result) * (size_t)(nf_total + 1)));
+  CKB(cudaMalloc(&b->d_ctlA, sizeof(BCtl)));
+  CKB(cudaMalloc(&b->d_ctlB, sizeof(BCtl)));
+  CKB(cudaMemset(b->d_ctlA, 0, sizeof(BCtl)));
+  CKB(cudaMemset(b->d_ctlB, 0, sizeof(BCtl)));
+  CKB(cudaMalloc(&b->d_pre, sizeof(int) * (2 * (size_t)n + 2)));
+  CKB(cudaMallocHost(&b->h_pre, sizeof(int) * (2 * (size_t)n + 2)));
+  CKB(cudaMalloc(&b->d_fitems, sizeof(vsbd_item) * (size_t)(nf_total + 1)));
+  CKB(cudaMallocHost(&b->h_fitems, sizeof(vsbd_item) * (size_t)(nf_total + 1)));
+  CKB(cudaMallocHost(&b->h_nwork, sizeof(int) * 4));
+  memset(b->h_nwork, 0, sizeof(int) * 4);
+  for (int s = 0; s < n; s++) {
+    BStream& S = b->h_streams[s];
+    S.src = b->raw[s];
+    S.sp = S.pitch;
+    S.cur = b->buf[0][s];
+    S.prev = b->buf[1][s];
+    S.xy = b->d_xy[s];
+    S.citems = b->d_citems[s];
+    S.keys = b->d_keys + b->key_off[s];
+    S.tickets = b->d_tickets + b->key_off[s];
+    S.mm = b->d_resA + b->mm_off[s];
+    S.cres = (vsbd_result*)(b->d_resA + b->cres_off[s]);
+    S.fres = b->d_resB + b->fres_off[s];
+  }
+  CKB(cudaMemcpy(b->d_streams, b->h_streams, sizeof(BStream) * n, cudaMemcpyHostToDevice));
+  /* fine items for tuning: every fine field of every stream, no offset; the
+     stage-B tables of the tuning runs are not used (stage-A lists) */
+  for (int s = 0, k = 0; s < n; s++)
+    for (int i = 0; i < d[s].nf; i++, k++) {
+      b->h_fitems[k].x = d[s].xy[2 * d[s].nc + i];
+      b->h_fitems[k].y = d[s].xy[2 * d[s].nc + d[s].nf + i];
+      b->h_fitems[k].ox = b->h_fitems[k].oy = 0;
+    }
+  /* tuning of fine classes runs through the stage-A path with citems
+     replaced: point each stream's citems at its fine items for that run */
+  if (set_grid(b) != 0 || upload_geoms(b) != 0) FAILB();
+  for (int c = 0; c < b->ncls; c++) {
+    int used_c = 0, used_f = 0;
+    for (int s = 0; s < n; s++) {
+      used_c |= b->h_streams[s].gc == c;
+      used_f |= b->h_streams[s].gf == c;
+    }
+    if (used_c && autotune_class(b, c, 0) != 0) FAILB();
+    if (used_f && !used_c) {
+      /* fine classes are tuned as a stage-A search over the fine items */
+      vsbd_item* tmp = NULL;
+      CKB(cudaMalloc(&tmp, sizeof(vsbd_item) * (size_t)(nf_total + 1)));
+      cudaError_t e = cudaMemcpy(tmp, b->h_fitems, sizeof(vsbd_item) * nf_total, cudaMemcpyHostToDevice);
+      if (e != cudaSuccess) { cudaFree(tmp); CKB(e); }
+      BStream* keep = (BStream*)malloc(sizeof(BStream) * n);
+      memcpy(keep, b->h_streams, sizeof(BStream) * n);
+      for (int s = 0; s < n; s++) {
+        BStream& S = b->h_streams[s];
+        S.citems = tmp + b->fres_off[s];
+        S.cres = S.fres;
+        S.keys += S.nc;
+        S.tickets += S.nc;
+        S.gc = S.gf;
+      }
+      e = cudaMemcpy(b->d_streams, b->h_streams, sizeof(BStream) * n, cudaMemcpyHostToDevice);
+      int rc = e == cudaSuccess ? autotune_class(b, c, 1) : -1;
+      memcpy(b->h_streams, keep, sizeof(BStream) * n);
+      free(keep);
+      cudaMemcpy(b->d_streams, b->h_streams, sizeof(BStream) * n, cudaMemcpyHostToDevice);
+      cudaFree(tmp);
+      if (e != cudaSuccess) CKB(e);
+      if (rc != 0) FAILB();
+    }
+  }
+  if (set_grid(b) != 0 || upload_geoms(b) != 0) FAILB();
+  BWork* w = NULL;
+  if (build_workA(b, &w, &b->nworkA, -1, 0) != 0) FAILB();
+  cudaError_t e = cudaMalloc(&b->d_workA, sizeof(BWork) * (size_t)(b->nworkA + 1));
+  if (e == cudaSuccess)
+    e = cudaMemcpy(b->d_workA, w, sizeof(BWork) * b->nworkA, cudaMemcpyHostToDevice);
+  free(w);
+  CKB(e);
+  {
+    BCtl h;
+    memset(&h, 0, sizeof(h));
+    h.nwork = b->nworkA;
+    CKB(cudaMemcpy(b->d_ctlA, &h, sizeof(h), cudaMemcpyHostToDevice));
+  }
+  CKB(cudaStreamSynchronize(b->st));
+  if (capture(b, 0, &b->gA) != 0 || capture(b, 1, &b->gB) != 0) FAILB();
+#undef CKB
+#undef FAILB
+  *out = b;
+  return 0;
+}
+
+extern "C" int vsbd_batch_stage_a(vsbd_batch* b, const uint8_t* const* planes, const int* pitches,
+                                  int on_device) {
+  BCK(cudaSetDevice(b->dev));
+  size_t h2d = 0;
+  for (int s = 0; s < b->n; s++) {
+    BStream& S = b->h_streams[s];
+    if (on_device) {
+      S.src = planes[s];
+      S.sp = pitches[s];
+    } else {
+      S.src = b->raw[s];
+      S.sp = S.pitch;
+      BCK(cudaMemcpy2DAsync(b->raw[s], S.pitch, planes[s], pitches[s], S.W, S.H,
+                            cudaMemcpyHostToDevice, b->st));
+      h2d += (size_t)S.W * S.H;
+    }
+    S.cur = b->buf[b->cur[s]][s];
+    S.prev = b->buf[b->cur[s] ^ 1][s];
+  }
+  BCK(cudaMemcpyAsync(b->d_streams, b->h_streams, sizeof(BStream) * b->n, cudaMemcpyHostToDevice,
+                      b->st));
+  BCK(cudaGraphLaunch(b->gA, b->st));
+  BCK(cudaStreamSynchronize(b->st));
+  b->launches++;
+  vsbp_count(1, h2d + sizeof(BStream) * b->n, b->resA_bytes + 4);
+  if (b->h_nwork[2]) {
+    vsbp_set_msg("batched stage A: a wait for blur tiles gave up");
+    /* skipped tiles leave keys and tickets mid-way: start them afresh */
+    cudaMemset(b->d_keys, 0xff, sizeof(unsigned long long) * (b->nkeys + 1));
+    cudaMemset(b->d_tickets, 0, sizeof(unsigned) * (b->nkeys + 1));
+    return -1;
+  }
+  return 0;
+}
+
+extern "C" void vsbd_batch_results_a(const vsbd_batch* b, int s, const uint8_t** mm,
+                                     const vsbd_result** cres) {
+  *mm = b->h_resA + b->mm_off[s];
+  *cres = (const vsbd_result*)(b->h_resA + b->cres_off[s]);
+}
+
+extern "C" int vsbd_batch_stage_b(vsbd_batch* b, const vsbd_item* const* items, const int* nitems,
+                                  const vsbd_result** fres) {
+  BCK(cudaSetDevice(b->dev));
+  int* pre = b->h_pre;
+  int* off = b->h_pre + b->n + 1;
+  int total = 0, nit = 0;
+  for (int s = 0; s < b->n; s++) {
+    const BStream& S = b->h_streams[s];
+    const DGeom& g = b->cls[S.gf].g;
+    int ni = items && items[s] ? nitems[s] : 0;
+    if (ni > S.nf) {
+      vsbp_set_msg("more fine items than fine fields");
+      return -1;
+    }
+    pre[s] = total;
+    off[s] = nit;
+    if (ni > 0) memcpy(b->h_fitems + nit, items[s], sizeof(vsbd_item) * ni);
+    nit += ni;
+    total += ni * g.nta * g.ntb;
+  }
+  pre[b->n] = total;
+  for (int s = 0; s < b->n; s++) fres[s] = b->h_resB + b->fres_off[s];
+  if (total == 0) return 0;
+  b->h_nwork[0] = total;
+  BCK(cudaMemcpyAsync(b->d_pre, b->h_pre, sizeof(int) * (2 * (size_t)b->n + 1),
+                      cudaMemcpyHostToDevice, b->st));
+  BCK(cudaMemcpyAsync(b->d_fitems, b->h_fitems, sizeof(vsbd_item) * (size_t)nit,
+                      cudaMemcpyHostToDevice, b->st));
+  BCK(cudaMemcpyAsync(&b->d_ctlB->nwork, &b->h_nwork[0], sizeof(int), cudaMemcpyHostToDevice,
+                      b->st));
+  BCK(cudaGraphLaunch(b->gB, b->st));
+  BCK(cudaStreamSynchronize(b->st));
+  b->launches++;
+  vsbp_count(1, sizeof(int) * (2 * (size_t)b->n + 2) + sizeof(vsbd_item) * (size_t)nit,
+             sizeof(vsbd_result) * (size_t)(b->nf_total + 1) + 4);
+  if (b->h_nwork[1]) {
+    vsbp_set_msg("batched stage B: the error flag was raised");
+    return -1;
+  }
+  return 0;
+}
+
+extern "C" void vsbd_batch_commit(vsbd_batch* b, int s) { b->cur[s] ^= 1; }
+
+extern "C" long vsbd_batch_launches(const vsbd_batch* b) { return b ? b->launches : 0; }
+
+extern "C" int vsbd_batch_grid(const vsbd_batch* b, int* ctas, int* threads, long* smem) {
+  if (!b) return -1;
+  *ctas = b->grid;
+  *threads = VSB_BATCH_THREADS;
+  *smem = (long)b->smem;
+  return 0;
+}

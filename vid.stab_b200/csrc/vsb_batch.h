@@ -1,0 +1,57 @@
+/*
+ * vsb_batch.h -- internal C interface of the batched multi-stream device
+ * path (vsb_batch.cu).  Plain C types only.
+ */
+#ifndef VSB_BATCH_H
+#define VSB_BATCH_H
+
+#include <stdint.h>
+
+#include "vsb_device.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* what the device path needs of one stream (planar luma only) */
+typedef struct {
+  int width, height;
+  int blur_size;         /* < 2: no blur */
+  int nc, nf;            /* coarse / fine field counts */
+  const int16_t* xy;     /* coarse x[nc], coarse y[nc], fine x[nf], fine y[nf] */
+  vsbd_geom coarse, fine;
+} vsbd_batch_stream;
+
+typedef struct vsbd_batch vsbd_batch;
+
+/* Allocates the device state of n streams, tunes the search tilings of
+   every distinct field geometry in the persistent kernel and captures the
+   two stage graphs.  Returns 0 or -1 (vsbd_error()). */
+int vsbd_batch_create(vsbd_batch** out, int n, const vsbd_batch_stream* streams);
+void vsbd_batch_destroy(vsbd_batch* b);
+
+/* Stage A of one step: plane 0 of every stream's new frame (device
+   addresses with on_device, else host), blur, coarse search of every coarse
+   field, min/max of every field.  Blocks until the results are on the host
+   (vsbd_batch_results_a). */
+int vsbd_batch_stage_a(vsbd_batch* b, const uint8_t* const* planes, const int* pitches,
+                       int on_device);
+void vsbd_batch_results_a(const vsbd_batch* b, int stream, const uint8_t** minmax,
+                          const vsbd_result** coarse);
+
+/* Stage B: the fine work lists (items[s] of nitems[s]; NULL or 0 for none);
+   fres[s] receives stream s's results.  Blocks. */
+int vsbd_batch_stage_b(vsbd_batch* b, const vsbd_item* const* items, const int* nitems,
+                       const vsbd_result** fres);
+
+/* stream s's current blurred frame becomes its previous one */
+void vsbd_batch_commit(vsbd_batch* b, int stream);
+
+long vsbd_batch_launches(const vsbd_batch* b);
+/* persistent grid: CTAs, threads per CTA, dynamic shared memory per CTA */
+int vsbd_batch_grid(const vsbd_batch* b, int* ctas, int* threads, long* smem);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -22,6 +22,8 @@
 #include <string.h>
 
 #include "vsb_device.h"
+#include "vsb_plan.h"
+#include "vsb_prefilter.cuh"
 #include "vsb_search.cuh"
 
 /* ------------------------------------------------------------------------ */
@@ -62,66 +64,12 @@ extern "C" const char* vsbd_error(void) { return g_err; }
 /* box blur                                                                  */
 /* ------------------------------------------------------------------------ */
 
-/* floor(acc / size) as a multiply-high by ceil(2^32/size): exact whenever
-   acc_max * size < 2^32 (checked exhaustively on the host when the divisor
-   is set up; otherwise the kernel divides) */
-struct BlurDiv {
-  unsigned mul;
-  unsigned size;
-  int exact;
-};
-
-__device__ __forceinline__ unsigned blur_div(unsigned acc, BlurDiv d) {
-  return d.exact ? __umulhi(acc, d.mul) : acc / d.size;
-}
-
-#define BT_W 128
-#define BT_H 32
-#define BT_MAXHALF 32
-
-/* One CTA blurs a BT_H x BT_W output tile.  The input tile plus a halo of
-   `half` pixels is read once with clamped coordinates (edge replication),
-   the horizontal pass writes 8-bit values to shared memory and the vertical
-   pass runs a sliding sum down each column. */
+/* One CTA blurs a BT_H x BT_W output tile (blur_tile). */
 __global__ void __launch_bounds__(256) k_blur(const uint8_t* __restrict__ src, int sp,
                                               uint8_t* __restrict__ dst, int dp, int W, int H,
                                               int half, BlurDiv dv) {
-  __shared__ uint8_t raw[BT_H + 2 * BT_MAXHALF][BT_W + 2 * BT_MAXHALF + 4];
-  __shared__ uint8_t hor[BT_H + 2 * BT_MAXHALF][BT_W + 4];
-  const int x0 = blockIdx.x * BT_W, y0 = blockIdx.y * BT_H;
-  const int rows = BT_H + 2 * half, cols = BT_W + 2 * half;
-  for (int i = threadIdx.x; i < rows * cols; i += blockDim.x) {
-    int r = i / cols, c = i - r * cols;
-    int gy = min(max(y0 - half + r, 0), H - 1);
-    int gx = min(max(x0 - half + c, 0), W - 1);
-    raw[r][c] = src[(size_t)gy * sp + gx];
-  }
-  __syncthreads();
-  const int win = 2 * half + 1;
-  for (int i = threadIdx.x; i < rows * BT_W; i += blockDim.x) {
-    int r = i / BT_W, c = i - r * BT_W;
-    unsigned acc = 0;
-    for (int k = 0; k < win; k++) acc += raw[r][c + k];
-    hor[r][c] = (uint8_t)blur_div(acc, dv);
-  }
-  __syncthreads();
-  /* 256 threads: column c, upper or lower half of the tile rows */
-  const int c = threadIdx.x & (BT_W - 1);
-  const int part = threadIdx.x >> 7;
-  const int gx = x0 + c;
-  if (gx >= W) return;
-  const int rbeg = part * (BT_H / 2);
-  unsigned acc = 0;
-  for (int k = 0; k < win; k++) acc += hor[rbeg + k][c];
-  for (int r = rbeg; r < rbeg + BT_H / 2; r++) {
-    if (r > rbeg) { /* slide: rows [r, r + win) of hor feed output row r */
-      acc += hor[r + win - 1][c];
-      acc -= hor[r - 1][c];
-    }
-    int gy = y0 + r;
-    if (gy >= H) break;
-    dst[(size_t)gy * dp + gx] = (uint8_t)blur_div(acc, dv);
-  }
+  __shared__ __align__(16) uint8_t tile[BT_SMEM];
+  blur_tile(src, sp, dst, dp, W, H, half, dv, blockIdx.x, blockIdx.y, tile);
 }
 
 /* Fallback for windows wider than the fused tile's halo: one thread per row,
@@ -154,21 +102,6 @@ __global__ void k_blur_cols(const uint8_t* __restrict__ src, int sp, uint8_t* __
   }
 }
 
-static int make_div(int size, int half, BlurDiv* d) {
-  d->size = (unsigned)size;
-  d->exact = 0;
-  d->mul = 0;
-  if (size < 2) return 0;
-  unsigned long long mul = ((1ull << 32) + (unsigned)size - 1) / (unsigned)size;
-  if (mul > 0xffffffffull) return 0;
-  unsigned accmax = 255u * (unsigned)(2 * half + 1);
-  for (unsigned a = 0; a <= accmax; a++)
-    if ((unsigned)((a * mul) >> 32) != a / (unsigned)size) return 0;
-  d->mul = (unsigned)mul;
-  d->exact = 1;
-  return 0;
-}
-
 /* launches the prefilter of one plane; returns the number of kernels */
 static int launch_blur(const uint8_t* src, int sp, uint8_t* dst, int dp, int W, int H, int size,
                        uint8_t* tmp, int tp, cudaStream_t st) {
@@ -189,64 +122,20 @@ static int launch_blur(const uint8_t* src, int sp, uint8_t* dst, int dp, int W, 
 /* field min / max                                                           */
 /* ------------------------------------------------------------------------ */
 
-/* One CTA per field; channel ch of a pixel is byte ch of its bpp bytes.
-   With skip != NULL it also flags every field whose contrast keeps it out of
-   the selection: the reference zeroes a contrast below the threshold and
-   selects only positive contrasts (src/motiondetect.c:697-698, :719, :734).
-   The contrast is the reference's double expression, evaluated in IEEE
-   double like the host's ((c0 + c1) + c2) * (1/3) for three channels), so
-   the flag agrees with the host's selection bit for bit. */
+/* One CTA per field (minmax_field). */
 __global__ void __launch_bounds__(256) k_minmax(const uint8_t* __restrict__ img, int pitch,
                                                 const int16_t* __restrict__ xs,
                                                 const int16_t* __restrict__ ys, int S, int bpp,
                                                 int nch, uint8_t* __restrict__ out, double thr,
                                                 uint8_t* __restrict__ skip) {
-  __shared__ unsigned smn[8], smx[8];
   const int f = blockIdx.x;
-  const int x0 = xs[f] - S / 2, y0 = ys[f] - S / 2;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  double c[3] = { 0.0, 0.0, 0.0 };
-  for (int ch = 0; ch < nch; ch++) {
-    unsigned mn = 255, mx = 0;
-    for (int i = threadIdx.x; i < S * S; i += blockDim.x) {
-      int r = i / S, col = i - r * S;
-      unsigned v = img[(size_t)(y0 + r) * pitch + (size_t)(x0 + col) * bpp + ch];
-      mn = min(mn, v);
-      mx = max(mx, v);
-    }
-    mn = __reduce_min_sync(0xffffffffu, mn);
-    mx = __reduce_max_sync(0xffffffffu, mx);
-    if (lane == 0) { smn[warp] = mn; smx[warp] = mx; }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      for (int w = 1; w < (int)(blockDim.x >> 5); w++) { mn = min(mn, smn[w]); mx = max(mx, smx[w]); }
-      out[(f * nch + ch) * 2 + 0] = (uint8_t)mn;
-      out[(f * nch + ch) * 2 + 1] = (uint8_t)mx;
-      c[ch] = (double)((int)mx - (int)mn) / ((double)((int)mx + (int)mn) + 0.1);
-    }
-    __syncthreads();
-  }
-  if (skip && threadIdx.x == 0) {
-    double con = c[0];
-    if (nch == 3) {
-      double s = __dadd_rn(c[0], c[1]);
-      s = __dadd_rn(s, c[2]);
-      con = __dmul_rn(s, 1.0 / 3.0);
-    }
-    skip[f] = !(con >= thr && con > 0.0);
-  }
+  minmax_field(img, pitch, xs[f], ys[f], S, bpp, nch, f, out, thr, skip);
 }
 
 /* ------------------------------------------------------------------------ */
 /* SAD search (kernels in vsb_search.cuh)                                    */
 /* ------------------------------------------------------------------------ */
 
-struct GeomDev {
-  DGeom g;
-  int32_t* d_order;
-  short2* d_point;
-  size_t smem;
-};
 
 static int sm_count(void) {
   static int n = 0;
@@ -300,13 +189,10 @@ static int lattice_regs(int TB) {
    and registers), with a penalty below 16 resident warps per SM, plus the
    staging of the window.  Forced values (> 0) pin a dimension.  Returns the
    number of candidates written (best first, at most cap). */
-struct TileCand {
-  double clk;
-  DGeom g;
-};
 
 static int tile_candidates(const DGeom& g, int nitems, int tb_force, int strip_force,
-                           int nab_force, int nbb_force, TileCand* out, int cap) {
+                           int nab_force, int nbb_force, TileCand* out, int cap,
+                           int max_threads = 512) {
   const size_t lim = search_smem_limit();
   const int sms = sm_count();
   int n = 0;
@@ -337,7 +223,7 @@ static int tile_candidates(const DGeom& g, int nitems, int tb_force, int strip_f
           t.ntb = (g.nb + nbb - 1) / nbb;
           int threads = nab * (nbb / TB) * ns;
           threads = (threads + 31) & ~31;
-          if (threads > 512 || threads < 32) {
+          if (threads > max_threads || threads < 32) {
             if (nbb_force > 0) break;
             continue;
           }
@@ -1131,4 +1017,23 @@ extern "C" int vsbd_sad_peak(int variant, double* byteops_per_s) {
   cudaFree(d);
   *byteops_per_s = (double)blocks * threads * iters * 8.0 * 4.0 / (best * 1e-3);
   return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* planning helpers for the batched path (vsb_plan.h)                        */
+/* ------------------------------------------------------------------------ */
+int vsbp_geom_upload(const vsbd_geom* h, int nitems, GeomDev* out) {
+  return geom_upload(h, nitems, 0, out);
+}
+void vsbp_geom_free(GeomDev* g) { geom_free(g); }
+int vsbp_tile_candidates(const DGeom& g, int nitems, int max_threads, TileCand* out, int cap) {
+  return tile_candidates(g, nitems, 0, 0, 0, 0, out, cap, max_threads);
+}
+int vsbp_sm_count(void) { return sm_count(); }
+void vsbp_set_err(const char* what, cudaError_t e) { set_err(what, e); }
+void vsbp_set_msg(const char* m) { set_msg(m); }
+void vsbp_count(long launches, size_t h2d, size_t d2h) {
+  count_launches(launches);
+  count_h2d(h2d);
+  count_d2h(d2h);
 }

@@ -30,6 +30,49 @@ int vsb_detect_common(VSMotionDetect* md, LocalMotions* motions, const uint8_t* 
 int vsb_build_geom(vsbd_geom* g, int32_t** order_out, int size, int bpp, int maxShift, int step,
                    int planar);
 
+/* Field layout and candidate geometry of a detector initialised without
+   device state (vsb_md_init with_device = 0): the caller runs the device
+   work.  xy: coarse x[nc], coarse y[nc], fine x[nf], fine y[nf]. */
+typedef struct {
+  vsbd_geom coarse, fine;
+  int32_t* order_c;
+  int32_t* order_f;
+  int16_t* xy;
+  int nc, nf, blur;
+} vsb_md_layout;
+
+/* vsMotionDetectInit with or without the per-detector device state */
+int vsb_md_init(VSMotionDetect* md, const VSMotionDetectConfig* conf, const VSFrameInfo* fi,
+                int with_device, vsb_md_layout* lay);
+void vsb_md_layout_free(vsb_md_layout* lay);
+
+/* One frame in phases (src/motiondetect.c:191-305), the device stages
+   between them run by the caller:
+     vsb_frame_begin      checks; *search = 0 for the first frame and the
+                          tripod lead-in (vsb_frame_first then)
+     [stage A: blur, field min/max, coarse search]
+     vsb_frame_host_a     contrasts, selection, coarse motions, the simple
+                          model and the fine work list (w->items[0..nitems),
+                          valid until the next frame of this detector)
+     [stage B, when w->fine_pass: fine search of the work list]
+     vsb_frame_host_b     fine motions, mean-match filter, show, result
+     vsb_frame_end        frame count; returns 1 if the current blurred
+                          frame becomes the previous one */
+typedef struct {
+  LocalMotions coarse, fine;
+  int fine_pass;
+  int nitems;
+  const vsbd_item* items;
+} vsb_frame_work;
+int vsb_frame_begin(VSMotionDetect* md, int* search);
+int vsb_frame_host_a(VSMotionDetect* md, const uint8_t* mm, const vsbd_result* cres,
+                     vsb_frame_work* w);
+void vsb_frame_host_b(VSMotionDetect* md, const vsbd_result* fres, vsb_frame_work* w,
+                      LocalMotions* motions);
+void vsb_frame_discard(vsb_frame_work* w);
+void vsb_frame_first(VSMotionDetect* md, LocalMotions* motions);
+int vsb_frame_end(VSMotionDetect* md);
+
 /* device context of an initialised detector (NULL if none) */
 vsbd_ctx* vsb_md_device(const VSMotionDetect* md);
 

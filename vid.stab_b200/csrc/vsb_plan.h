@@ -1,0 +1,40 @@
+/*
+ * vsb_plan.h -- planning helpers of the search (tilings, geometry tables on
+ * the device) shared by the per-stream shim (vsb_device.cu) and the batched
+ * path (vsb_batch.cu).  C++ only.
+ */
+#ifndef VSB_PLAN_H
+#define VSB_PLAN_H
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+#include "vsb_device.h"
+#include "vsb_search.cuh"
+
+/* a field set's geometry with its rank/point tables in device memory */
+struct GeomDev {
+  DGeom g;
+  int32_t* d_order;
+  short2* d_point;
+  size_t smem;
+};
+
+/* a tiling with its modelled cost */
+struct TileCand {
+  double clk;
+  DGeom g;
+};
+
+/* uploads the tables and picks the cost model's best tiling */
+int vsbp_geom_upload(const vsbd_geom* h, int nitems, GeomDev* out);
+void vsbp_geom_free(GeomDev* g);
+/* the cap best tilings (model order) with at most max_threads threads */
+int vsbp_tile_candidates(const DGeom& g, int nitems, int max_threads, TileCand* out, int cap);
+int vsbp_sm_count(void);
+void vsbp_set_err(const char* what, cudaError_t e);
+void vsbp_set_msg(const char* m);
+/* process-wide counters of the per-frame path */
+void vsbp_count(long launches, size_t h2d, size_t d2h);
+
+#endif

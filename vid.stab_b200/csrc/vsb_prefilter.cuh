@@ -1,0 +1,142 @@
+/*
+ * vsb_prefilter.cuh -- per-tile and per-field bodies of the prefilter
+ * kernels (box blur, field min/max), shared by the per-stream kernels and
+ * the batched persistent kernel.
+ */
+#ifndef VSB_PREFILTER_CUH
+#define VSB_PREFILTER_CUH
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+/* floor(acc / size) as a multiply-high by ceil(2^32/size): exact whenever
+   acc_max * size < 2^32 (checked exhaustively on the host when the divisor
+   is set up; otherwise the kernel divides) */
+struct BlurDiv {
+  unsigned mul;
+  unsigned size;
+  int exact;
+};
+
+__device__ __forceinline__ unsigned blur_div(unsigned acc, BlurDiv d) {
+  return d.exact ? __umulhi(acc, d.mul) : acc / d.size;
+}
+
+#define BT_W 128
+#define BT_H 32
+#define BT_MAXHALF 32
+#define BT_RAWP (BT_W + 2 * BT_MAXHALF + 4)
+#define BT_HORP (BT_W + 4)
+/* shared memory of one blur tile: raw input with halo, horizontal pass */
+#define BT_SMEM ((BT_H + 2 * BT_MAXHALF) * (BT_RAWP + BT_HORP))
+
+/* One CTA of 256 threads blurs the BT_H x BT_W output tile (bx, by).  The
+   input tile plus a halo of `half` pixels is read once with clamped
+   coordinates (edge replication), the horizontal pass writes 8-bit values to
+   shared memory and the vertical pass runs a sliding sum down each column
+   (src/boxblur.c:190-332: window sums, floor division by the size). */
+__device__ __forceinline__ void blur_tile(const uint8_t* __restrict__ src, int sp,
+                                          uint8_t* __restrict__ dst, int dp, int W, int H,
+                                          int half, BlurDiv dv, int bx, int by, uint8_t* smem) {
+  uint8_t* raw = smem;
+  uint8_t* hor = smem + (BT_H + 2 * BT_MAXHALF) * BT_RAWP;
+  const int x0 = bx * BT_W, y0 = by * BT_H;
+  const int rows = BT_H + 2 * half, cols = BT_W + 2 * half;
+  for (int i = threadIdx.x; i < rows * cols; i += blockDim.x) {
+    int r = i / cols, c = i - r * cols;
+    int gy = min(max(y0 - half + r, 0), H - 1);
+    int gx = min(max(x0 - half + c, 0), W - 1);
+    raw[r * BT_RAWP + c] = src[(size_t)gy * sp + gx];
+  }
+  __syncthreads();
+  const int win = 2 * half + 1;
+  for (int i = threadIdx.x; i < rows * BT_W; i += blockDim.x) {
+    int r = i / BT_W, c = i - r * BT_W;
+    unsigned acc = 0;
+    for (int k = 0; k < win; k++) acc += raw[r * BT_RAWP + c + k];
+    hor[r * BT_HORP + c] = (uint8_t)blur_div(acc, dv);
+  }
+  __syncthreads();
+  /* 256 threads: column c, upper or lower half of the tile rows */
+  const int c = threadIdx.x & (BT_W - 1);
+  const int part = threadIdx.x >> 7;
+  const int gx = x0 + c;
+  if (gx >= W) return;
+  const int rbeg = part * (BT_H / 2);
+  unsigned acc = 0;
+  for (int k = 0; k < win; k++) acc += hor[(rbeg + k) * BT_HORP + c];
+  for (int r = rbeg; r < rbeg + BT_H / 2; r++) {
+    if (r > rbeg) { /* slide: rows [r, r + win) of hor feed output row r */
+      acc += hor[(r + win - 1) * BT_HORP + c];
+      acc -= hor[(r - 1) * BT_HORP + c];
+    }
+    int gy = y0 + r;
+    if (gy >= H) break;
+    dst[(size_t)gy * dp + gx] = (uint8_t)blur_div(acc, dv);
+  }
+}
+
+/* Field f of a field list, by one CTA: 8-bit min/max per channel (channel ch
+   of a pixel is byte ch of its bpp bytes) into out[(f*nch + ch)*2 + {0,1}].
+   With skip != NULL it also flags a field whose contrast keeps it out of the
+   selection: the reference zeroes a contrast below the threshold and selects
+   only positive contrasts (src/motiondetect.c:697-698, :719, :734).  The
+   contrast is the reference's double expression (:389-407), evaluated in
+   IEEE double like the host's ((c0 + c1) + c2) * (1/3) for three channels,
+   so the flag agrees with the host's selection bit for bit. */
+__device__ __forceinline__ void minmax_field(const uint8_t* __restrict__ img, int pitch, int x,
+                                             int y, int S, int bpp, int nch, int f,
+                                             uint8_t* __restrict__ out, double thr,
+                                             uint8_t* __restrict__ skip) {
+  __shared__ unsigned smn[32], smx[32];
+  const int x0 = x - S / 2, y0 = y - S / 2;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double c[3] = { 0.0, 0.0, 0.0 };
+  for (int ch = 0; ch < nch; ch++) {
+    unsigned mn = 255, mx = 0;
+    for (int i = threadIdx.x; i < S * S; i += blockDim.x) {
+      int r = i / S, col = i - r * S;
+      unsigned v = img[(size_t)(y0 + r) * pitch + (size_t)(x0 + col) * bpp + ch];
+      mn = min(mn, v);
+      mx = max(mx, v);
+    }
+    mn = __reduce_min_sync(0xffffffffu, mn);
+    mx = __reduce_max_sync(0xffffffffu, mx);
+    if (lane == 0) { smn[warp] = mn; smx[warp] = mx; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int w = 1; w < (int)(blockDim.x >> 5); w++) { mn = min(mn, smn[w]); mx = max(mx, smx[w]); }
+      out[(f * nch + ch) * 2 + 0] = (uint8_t)mn;
+      out[(f * nch + ch) * 2 + 1] = (uint8_t)mx;
+      c[ch] = (double)((int)mx - (int)mn) / ((double)((int)mx + (int)mn) + 0.1);
+    }
+    __syncthreads();
+  }
+  if (skip && threadIdx.x == 0) {
+    double con = c[0];
+    if (nch == 3) {
+      double s = __dadd_rn(c[0], c[1]);
+      s = __dadd_rn(s, c[2]);
+      con = __dmul_rn(s, 1.0 / 3.0);
+    }
+    skip[f] = !(con >= thr && con > 0.0);
+  }
+}
+
+/* divisor set-up of the blur (host) */
+static inline int make_div(int size, int half, BlurDiv* d) {
+  d->size = (unsigned)size;
+  d->exact = 0;
+  d->mul = 0;
+  if (size < 2) return 0;
+  unsigned long long mul = ((1ull << 32) + (unsigned)size - 1) / (unsigned)size;
+  if (mul > 0xffffffffull) return 0;
+  unsigned accmax = 255u * (unsigned)(2 * half + 1);
+  for (unsigned a = 0; a <= accmax; a++)
+    if ((unsigned)((a * mul) >> 32) != a / (unsigned)size) return 0;
+  d->mul = (unsigned)mul;
+  d->exact = 1;
+  return 0;
+}
+
+#endif

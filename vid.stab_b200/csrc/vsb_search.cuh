@@ -294,20 +294,21 @@ __device__ __forceinline__ void rows_segment(unsigned (&acc)[TB], int jlo, int j
 #undef VSB_SEG
 }
 
-/* grid (nta*ntb, items); block g.threads; dynamic smem tile_layout(g).total */
-template <int TB, bool EMIT = false>
-__global__ void __launch_bounds__(512, 1) k_lattice(const uint8_t* __restrict__ curr,
-                                                  const uint8_t* __restrict__ prev, int pitch,
-                                                  DGeom g, const vsbd_item* __restrict__ items,
-                                                  unsigned long long* __restrict__ keys,
-                                                  unsigned* __restrict__ tickets,
-                                                  vsbd_result* __restrict__ res) {
-  extern __shared__ __align__(16) uint8_t sm[];
+/* One lattice tile of one item, by one CTA: tile = tbi*nta + tai of the
+   item's ntiles = nta*ntb tiles; sm: tile_layout(g).total bytes of shared
+   memory.  The last of the item's CTAs to finish refines and stores. */
+template <int TB, bool EMIT>
+__device__ __forceinline__ void lattice_tile(const uint8_t* __restrict__ curr,
+                                             const uint8_t* __restrict__ prev, int pitch,
+                                             const DGeom& g, const vsbd_item* __restrict__ items,
+                                             unsigned long long* __restrict__ keys,
+                                             unsigned* __restrict__ tickets,
+                                             vsbd_result* __restrict__ res, int item, int tile,
+                                             unsigned ntiles, uint8_t* sm) {
   __shared__ unsigned long long red[32];
   __shared__ int s_last;
   const TileLayout L = tile_layout(g);
-  const int item = blockIdx.y;
-  const int tbi = blockIdx.x / g.nta, tai = blockIdx.x - tbi * g.nta;
+  const int tbi = tile / g.nta, tai = tile - tbi * g.nta;
   const vsbd_item it = items[item];
   const int a0 = tai * g.nab, b0 = tbi * g.nbb;
   const int na_t = min(g.nab, g.na - a0), nb_t = min(g.nbb, g.nb - b0);
@@ -428,12 +429,25 @@ __global__ void __launch_bounds__(512, 1) k_lattice(const uint8_t* __restrict__ 
     atomicMin(&keys[item], best);
     __threadfence();
     unsigned tk = atomicAdd(&tickets[item], 1u);
-    s_last = (tk == gridDim.x - 1);
+    s_last = (tk == ntiles - 1);
   }
   __syncthreads();
   if (!s_last) return;
   __threadfence();
   refine_and_store(g, L, it, C, P + 16, prev, pitch, keys, tickets, res, item, qsad);
+}
+
+/* grid (nta*ntb, items); block g.threads; dynamic smem tile_layout(g).total */
+template <int TB, bool EMIT = false>
+__global__ void __launch_bounds__(512, 1) k_lattice(const uint8_t* __restrict__ curr,
+                                                  const uint8_t* __restrict__ prev, int pitch,
+                                                  DGeom g, const vsbd_item* __restrict__ items,
+                                                  unsigned long long* __restrict__ keys,
+                                                  unsigned* __restrict__ tickets,
+                                                  vsbd_result* __restrict__ res) {
+  extern __shared__ __align__(16) uint8_t sm[];
+  lattice_tile<TB, EMIT>(curr, prev, pitch, g, items, keys, tickets, res, blockIdx.y, blockIdx.x,
+                         gridDim.x, sm);
 }
 
 /* Bound and survivors of one item after the partial pass (one CTA per item).

@@ -118,6 +118,18 @@ def lib():
                                   C.c_char_p, p, C.c_long, p, p, p]
     L.vsb_detect_run.restype = C.c_long
     L.vsb_detect_run.argtypes = [C.POINTER(VSMotionDetect), p, C.c_long, i, i, i, p, C.c_long, p]
+    L.vsb_batch_create.restype = p
+    L.vsb_batch_create.argtypes = [i, p, p, i, p]
+    L.vsb_batch_detect.restype = i
+    L.vsb_batch_detect.argtypes = [p, p, p, i, p]
+    L.vsb_batch_run.restype = C.c_long
+    L.vsb_batch_run.argtypes = [p, p, p, p, i, i, p, C.c_long, p]
+    L.vsb_batch_free.restype = None
+    L.vsb_batch_free.argtypes = [p]
+    L.vsb_batch_launch_count.restype = C.c_long
+    L.vsb_batch_launch_count.argtypes = [p]
+    L.vsb_batch_grid.restype = i
+    L.vsb_batch_grid.argtypes = [p, p, p, p]
     L.vsb_boxblur_host.restype = i
     L.vsb_boxblur_host.argtypes = [p, p, i, i, i]
     L.vsb_field_minmax_host.restype = i

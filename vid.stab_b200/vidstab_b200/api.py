@@ -95,6 +95,77 @@ class MotionDetector:
             pass
 
 
+class Batch:
+    """Many independent detect streams stepped together (vsb_batch_*): every
+    step runs the device work of all streams in two persistent-kernel
+    launches replayed from captured CUDA graphs.  Stream s gives the
+    LocalMotions a MotionDetector of its own would give."""
+
+    def __init__(self, widths, heights, pformat=1, stepsize=6, accuracy=15, shakiness=5,
+                 mincontrast=0.25, tripod=0):
+        L = lib()
+        self.L = L
+        self.n = len(widths)
+        conf = L.vsMotionDetectGetDefaultConfig(b"vidstab_b200")
+        conf.stepSize, conf.accuracy, conf.shakiness = stepsize, accuracy, shakiness
+        conf.contrastThreshold, conf.virtualTripod = mincontrast, tripod
+        confs = (type(conf) * self.n)(*([conf] * self.n))
+        self.widths = np.ascontiguousarray(widths, np.int32)
+        self.heights = np.ascontiguousarray(heights, np.int32)
+        self.h = L.vsb_batch_create(self.n, ptr(self.widths), ptr(self.heights), pformat,
+                                    C.cast(confs, C.c_void_p))
+        if not self.h:
+            raise RuntimeError("vsb_batch_create failed: %s" % L.vsb_last_error().decode())
+
+    def run(self, clip_ptrs, frame_bytes, pitches, nframes, on_device, out, counts):
+        """nframes steps; stream s's frame k at clip_ptrs[s] + k*frame_bytes[s].
+        Records go to the preallocated LM_DTYPE array out (step by step,
+        stream by stream), counts (int32, nframes*n) gets per-frame counts."""
+        clips = np.ascontiguousarray(clip_ptrs, np.uint64)
+        fb = np.ascontiguousarray(frame_bytes, np.int64)
+        pt = np.ascontiguousarray(pitches, np.int32)
+        if len(counts) < nframes * self.n:
+            raise ValueError("counts too small")
+        total = self.L.vsb_batch_run(self.h, ptr(clips), ptr(fb), ptr(pt), nframes,
+                                     1 if on_device else 0, ptr(out), len(out), ptr(counts))
+        if total < 0:
+            raise RuntimeError("vsb_batch_run failed: %s" % self.L.vsb_last_error().decode())
+        return total
+
+    def detect(self, planes, pitches, on_device):
+        """One step: a list of n records arrays."""
+        pl = np.ascontiguousarray(planes, np.uint64)
+        pt = np.ascontiguousarray(pitches, np.int32)
+        vs = (VSVector * self.n)()
+        if self.L.vsb_batch_detect(self.h, ptr(pl), ptr(pt), 1 if on_device else 0,
+                                   C.cast(vs, C.c_void_p)) != 0:
+            raise RuntimeError("vsb_batch_detect failed: %s" % self.L.vsb_last_error().decode())
+        out = []
+        for v in vs:
+            out.append(vector_records(v))
+            self.L.vs_vector_del(C.byref(v))
+        return out
+
+    def launches(self):
+        return self.L.vsb_batch_launch_count(self.h)
+
+    def grid(self):
+        a, b, c = C.c_int(), C.c_int(), C.c_long()
+        self.L.vsb_batch_grid(self.h, C.byref(a), C.byref(b), C.byref(c))
+        return a.value, b.value, c.value
+
+    def close(self):
+        if self.h:
+            self.L.vsb_batch_free(self.h)
+        self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def detect_clip(frames, pformat=1, stepsize=6, accuracy=15, shakiness=5, mincontrast=0.25,
                 tripod=0, show=0, serialization_mode=0, trf_path=None, on_device_ptr=None,
                 frame_bytes=None, linesize=None, width=None, height=None, return_frames=False):
