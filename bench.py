@@ -308,8 +308,8 @@ def main():
         nk = min(nfr, 60)
         for k in range(nk):
             det.detect_device(clip.data_ptr() + k * W * H, W)
-        ms = (C.c_double * 4)()
-        cnt = (C.c_long * 4)()
+        ms = (C.c_double * 6)()
+        cnt = (C.c_long * 6)()
         L.vsb_kernel_times(C.byref(det.md), ms, cnt)
         fc = det.md.fieldscoarse
         det.close()

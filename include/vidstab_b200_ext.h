@@ -74,7 +74,9 @@ VS_API long vsb_detect_run(struct _vsmotiondetect* md, const uint8_t* frames, lo
 
 /* Per-kernel device time: with timing on, CUDA events bracket every kernel
    of the detector on its stream.  ms[k] and count[k] for k = 0 blur,
-   1 field min/max, 2 coarse search, 3 fine search (4 entries each).
+   1 field min/max, 2 coarse search, 3 fine search, 4 proposal network,
+   5 full searches of items that fell back (6 entries each; with a proposal,
+   2 and 3 time the narrowed searches).
    Turning timing on resets the totals. */
 VS_API int vsb_set_kernel_timing(struct _vsmotiondetect* md, int on);
 VS_API int vsb_kernel_times(const struct _vsmotiondetect* md, double* ms, long* count);
@@ -171,6 +173,77 @@ VS_API void vsb_batch_free(vsb_batch* b);
 VS_API long vsb_batch_launch_count(const vsb_batch* b);
 /* the persistent grid: CTAs, threads per CTA, dynamic shared memory per CTA */
 VS_API int vsb_batch_grid(const vsb_batch* b, int* ctas, int* threads, long* smem);
+
+/* ---- learned search proposal (no reference counterpart) ----------------
+   The reference searches every field over its whole candidate lattice.  A
+   detector given a proposal network first predicts each field's
+   displacement from a 32x32 crop pair (2x2 averages of the 64x64
+   neighbourhood in the blurred current and previous planes), evaluates only
+   the lattice points that bracket prediction +- radius plus one ring around
+   them, and refines the winner exactly as the full search does.  An item
+   falls back to the exact full search when the network's confidence logit
+   is below conf_min, when the winner lies on the ring, or when the refined
+   SAD per field pixel exceeds match_bound.  Planar formats only.
+
+   blob: a serialized network (header "VSBP", version 1, its bf16 weights and
+   f32 biases, and the radius / conf_min / match_bound it was calibrated
+   with); NULL returns the detector to the plain full search. */
+VS_API int vsb_set_proposal(struct _vsmotiondetect* md, const void* blob, long bytes);
+/* as vsb_set_proposal, overriding the blob's radius (if >= 0), conf_min
+   (if not NaN) and match_bound (if >= 0) */
+VS_API int vsb_set_proposal_ex(struct _vsmotiondetect* md, const void* blob, long bytes,
+                               double radius, double conf_min, double match_bound);
+/* With verify on, every stage also runs the full search of every item and
+   counts the items whose result (SAD, shift, range test) is identical. */
+VS_API int vsb_set_proposal_verify(struct _vsmotiondetect* md, int on);
+/* stats[0] items searched with the proposal, [1] of them fell back to the
+   full search, [2] items verified, [3] of them identical to the full search,
+   [4] coarse items searched, [5] of them fell back, [6] fine items searched,
+   [7] of them fell back (8 entries) */
+VS_API int vsb_proposal_stats(const struct _vsmotiondetect* md, long long* stats);
+
+/* Training-data log of a plain detector: for every item the full search
+   runs on (coarse fields, then the frame's fine fields), the network input
+   (4096 bytes: [32][32][2] bf16) is appended to d_inputs and the label
+   {int16 tx, ty; uint32 sad; uint8 kind (0 coarse, 1 fine), ok, use (field
+   passes the contrast threshold), pad} (12 bytes) to d_labels, until cap
+   items; d_inputs NULL turns it off.  Device memory of the detector's GPU. */
+VS_API int vsb_set_field_log(struct _vsmotiondetect* md, void* d_inputs, void* d_labels, long cap);
+VS_API long vsb_field_log_count(const struct _vsmotiondetect* md);
+
+/* Network kernels for the offline trainer and tests (device pointers,
+   stream a cudaStream_t or NULL).  d_params: n_bf16 bf16 weights then n_f32
+   f32 biases; inputs [n][32][32][2] bf16; outputs [n][3] f32 (dx, dy in
+   units of the blob's scale, confidence logit). */
+VS_API int vsb_pnet_sizes(long* n_bf16, long* n_f32, long* act_bytes_per_item,
+                          long* work_bytes_per_item);
+/* training forward (fp32 FMA); stores the activations the backward needs */
+VS_API int vsb_pnet_forward_train(const void* d_params, const void* d_input, int n, void* d_acts,
+                                  float* d_out, void* stream);
+/* gradient of sum(out * d_dout) w.r.t. the parameters, fp32 in parameter
+   order (overwritten); d_work: work_bytes_per_item * n bytes */
+VS_API int vsb_pnet_backward(const void* d_params, const void* d_input, const void* d_acts, int n,
+                             const float* d_dout, float* d_grad, void* d_work, void* stream);
+/* the detector's inference kernel (tensor cores) on prepared inputs */
+VS_API int vsb_pnet_infer(const void* d_params, const void* d_input, int n, float* d_out,
+                          void* stream);
+/* the same kernel taking its inputs straight from two blurred planes, for
+   n items {int16 x, y, ox, oy}, as a detector runs it */
+VS_API int vsb_pnet_infer_items(const void* d_params, const uint8_t* d_curr,
+                                const uint8_t* d_prev, int pitch, int width, int height,
+                                const void* d_items, int n, float* d_out, void* stream);
+/* network inputs of n items {int16 x, y, ox, oy} on two blurred planes */
+VS_API int vsb_pnet_crops(const uint8_t* d_curr, const uint8_t* d_prev, int pitch, int width,
+                          int height, const void* d_items, int n, void* d_input, void* stream);
+/* narrowed search of one planar field set on host planes, given raw network
+   outputs pout[n][3]: per item the result (as vsb_field_search_host) and
+   the fallback flag (0 accepted, 1 falls back; the full search is not run) */
+VS_API int vsb_pnet_narrow_host(const uint8_t* curr, const uint8_t* prev, int width, int height,
+                                int size, int maxShift, int stepSize, const int16_t* x,
+                                const int16_t* y, const int16_t* ox, const int16_t* oy, int n,
+                                const float* pout, float scale, float radius, float conf_min,
+                                uint32_t sad_bound, uint32_t* sad, int16_t* tx, int16_t* ty,
+                                int32_t* ok, uint8_t* flags);
 
 #ifdef __cplusplus
 }

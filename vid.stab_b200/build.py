@@ -28,9 +28,9 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 CC = shutil.which("gcc", path="/usr/bin:/bin") or "gcc"
 
 STRICT_C = ["vs_runtime.c", "vs_frameinfo.c", "vs_vector.c", "vs_serialize.c",
-            "vs_motiondetect.c", "vs_ext.c", "vs_batch.c", "vs_proposal_host.c"]
+            "vs_motiondetect.c", "vs_ext.c", "vs_batch.c", "vs_pnet.c"]
 REFFP_C = ["vs_transform.c", "vs_motionmodel.c", "vs_draw.c"]
-CU = ["vsb_device.cu", "vsb_noalloc.cu", "vsb_batch.cu", "vsb_proposal.cu"]
+CU = ["vsb_device.cu", "vsb_noalloc.cu", "vsb_batch.cu", "vsb_pnet.cu"]
 
 COMMON_C = ["-std=gnu99", "-O3", "-DNDEBUG", "-fPIC", "-Wall", "-fvisibility=hidden",
             "-I" + INCLUDE, "-I" + CSRC]
@@ -92,7 +92,7 @@ def build(verbose=False, ptxas_v=False, force=False):
                 print(out)
     if force or newer(objs, LIB):
         run([NVCC, "-shared", "-cudart", "static", "-gencode", "arch=compute_100a,code=sm_100a",
-             "-o", LIB] + objs + ["-lpthread", "-lm", "-ldl", "-lrt"], verbose)
+             "-o", LIB, "-Xlinker", "--no-undefined"] + objs + ["-lpthread", "-lm", "-ldl", "-lrt"], verbose)
     return LIB
 
 

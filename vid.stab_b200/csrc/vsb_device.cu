@@ -23,6 +23,7 @@
 
 #include "vsb_device.h"
 #include "vsb_plan.h"
+#include "vsb_pnet.h"
 #include "vsb_prefilter.cuh"
 #include "vsb_search.cuh"
 
@@ -102,12 +103,104 @@ __global__ void k_blur_cols(const uint8_t* __restrict__ src, int sp, uint8_t* __
   }
 }
 
+/* Planar prefilter with vector memory access: one CTA of 256 threads
+   blurs a BF_H x BF_W output tile.  Input rows (clamped to the frame) are
+   staged with 16-byte loads from 16 bytes left of the tile to 16 bytes right
+   of it (tiles touching the left or right frame edge load bytewise with
+   clamped columns); the horizontal pass writes 4 outputs per task as one
+   word, the vertical pass runs 4-column sliding sums and stores words.  Same
+   arithmetic as blur_tile (window sums, floor division by the size). */
+#define BF_W 256
+#define BF_H 32
+#define BF_MAXHALF 16
+#define BF_RAWP (BF_W + 32)
+__global__ void __launch_bounds__(256) k_blur_fast(const uint8_t* __restrict__ src, int sp,
+                                                   uint8_t* __restrict__ dst, int dp, int W, int H,
+                                                   int half, BlurDiv dv) {
+  __shared__ __align__(16) uint8_t raw[(BF_H + 2 * BF_MAXHALF) * BF_RAWP];
+  __shared__ __align__(16) uint8_t hor[(BF_H + 2 * BF_MAXHALF) * BF_W];
+  const int x0 = blockIdx.x * BF_W, y0 = blockIdx.y * BF_H;
+  const int rows = BF_H + 2 * half;
+  const bool interior = x0 >= 16 && x0 + BF_W + 16 <= W;
+  if (interior) {
+    for (int i = threadIdx.x; i < rows * (BF_RAWP / 16); i += blockDim.x) {
+      const int r = i / (BF_RAWP / 16), v = i - r * (BF_RAWP / 16);
+      const int gy = min(max(y0 - half + r, 0), H - 1);
+      *(uint4*)(raw + r * BF_RAWP + (v << 4)) =
+          *(const uint4*)(src + (size_t)gy * sp + x0 - 16 + (v << 4));
+    }
+  } else {
+    for (int i = threadIdx.x; i < rows * BF_RAWP; i += blockDim.x) {
+      const int r = i / BF_RAWP, c = i - r * BF_RAWP;
+      const int gy = min(max(y0 - half + r, 0), H - 1);
+      const int gx = min(max(x0 - 16 + c, 0), W - 1);
+      raw[r * BF_RAWP + c] = src[(size_t)gy * sp + gx];
+    }
+  }
+  __syncthreads();
+  const int win = 2 * half + 1;
+  for (int i = threadIdx.x; i < rows * (BF_W / 4); i += blockDim.x) {
+    const int r = i / (BF_W / 4), c = (i - r * (BF_W / 4)) * 4;
+    const uint8_t* p = raw + r * BF_RAWP + 16 + c - half;
+    unsigned acc = 0;
+    for (int k = 0; k < win; k++) acc += p[k];
+    unsigned o = blur_div(acc, dv);
+#pragma unroll
+    for (int k = 1; k < 4; k++) {
+      acc += p[win - 1 + k];
+      acc -= p[k - 1];
+      o |= blur_div(acc, dv) << (8 * k);
+    }
+    *(unsigned*)(hor + r * BF_W + c) = o;
+  }
+  __syncthreads();
+  /* thread: 4 columns (cg), a quarter of the tile rows */
+  const int cg = threadIdx.x & 63, part = threadIdx.x >> 6;
+  const int gx = x0 + cg * 4;
+  if (gx >= W) return;
+  const int rb = part * (BF_H / 4);
+  unsigned a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+  for (int k = 0; k < win; k++) {
+    const unsigned w = *(const unsigned*)(hor + (rb + k) * BF_W + cg * 4);
+    a0 += w & 0xff;
+    a1 += (w >> 8) & 0xff;
+    a2 += (w >> 16) & 0xff;
+    a3 += w >> 24;
+  }
+  const bool full4 = gx + 4 <= W;
+  for (int r = rb; r < rb + BF_H / 4; r++) {
+    if (r > rb) {
+      const unsigned wi = *(const unsigned*)(hor + (r + win - 1) * BF_W + cg * 4);
+      const unsigned wo = *(const unsigned*)(hor + (r - 1) * BF_W + cg * 4);
+      a0 += (wi & 0xff) - (wo & 0xff);
+      a1 += ((wi >> 8) & 0xff) - ((wo >> 8) & 0xff);
+      a2 += ((wi >> 16) & 0xff) - ((wo >> 16) & 0xff);
+      a3 += (wi >> 24) - (wo >> 24);
+    }
+    const int gy = y0 + r;
+    if (gy >= H) break;
+    const unsigned o = blur_div(a0, dv) | (blur_div(a1, dv) << 8) | (blur_div(a2, dv) << 16) |
+                       (blur_div(a3, dv) << 24);
+    uint8_t* d = dst + (size_t)gy * dp + gx;
+    if (full4) {
+      *(unsigned*)d = o;
+    } else {
+      for (int k = 0; k < 4 && gx + k < W; k++) d[k] = (uint8_t)(o >> (8 * k));
+    }
+  }
+}
+
 /* launches the prefilter of one plane; returns the number of kernels */
 static int launch_blur(const uint8_t* src, int sp, uint8_t* dst, int dp, int W, int H, int size,
                        uint8_t* tmp, int tp, cudaStream_t st) {
   int half = size / 2;
   BlurDiv dv;
   make_div(size, half, &dv);
+  if (half <= BF_MAXHALF && ((((uintptr_t)src | (uintptr_t)sp | (uintptr_t)dst | (uintptr_t)dp) & 15) == 0)) {
+    dim3 grid((W + BF_W - 1) / BF_W, (H + BF_H - 1) / BF_H);
+    k_blur_fast<<<grid, 256, 0, st>>>(src, sp, dst, dp, W, H, half, dv);
+    return 1;
+  }
   if (half <= BT_MAXHALF) {
     dim3 grid((W + BT_W - 1) / BT_W, (H + BT_H - 1) / BT_H);
     k_blur<<<grid, 256, 0, st>>>(src, sp, dst, dp, W, H, half, dv);
@@ -130,6 +223,72 @@ __global__ void __launch_bounds__(256) k_minmax(const uint8_t* __restrict__ img,
                                                 uint8_t* __restrict__ skip) {
   const int f = blockIdx.x;
   minmax_field(img, pitch, xs[f], ys[f], S, bpp, nch, f, out, thr, skip);
+}
+
+/* bytes b of a word with lo <= b < hi (byte offsets) set to 0xff */
+__device__ __forceinline__ unsigned byte_mask(int lo, int hi) {
+  unsigned m = 0;
+#pragma unroll
+  for (int b = 0; b < 4; b++)
+    if (b >= lo && b < hi) m |= 0xffu << (8 * b);
+  return m;
+}
+
+/* Planar 8-bit min/max of both field sets in one launch: blocks [0, nc)
+   take the coarse fields (size Sc, threshold thr, skip flags), the rest the
+   fine fields (size Sf).  Rows are read with 16-byte loads; bytes outside
+   the field are masked to the neutral value.  Same outputs as minmax_field
+   (the contrast is the reference's double expression). */
+__global__ void __launch_bounds__(256) k_minmax_planar(const uint8_t* __restrict__ img, int pitch,
+                                                       const int16_t* __restrict__ xy, int nc,
+                                                       int nf, int Sc, int Sf,
+                                                       uint8_t* __restrict__ out, double thr,
+                                                       uint8_t* __restrict__ skip) {
+  __shared__ unsigned smn[8], smx[8];
+  const int f = blockIdx.x;
+  const bool coarse = f < nc;
+  const int S = coarse ? Sc : Sf;
+  const int x = coarse ? xy[f] : xy[2 * nc + (f - nc)];
+  const int y = coarse ? xy[nc + f] : xy[2 * nc + nf + (f - nc)];
+  const int x0 = x - S / 2, y0 = y - S / 2;
+  const int xa = x0 & ~15;
+  const int nv = (x0 + S - xa + 15) >> 4;
+  unsigned mn = 0xffffffffu, mx = 0u;
+  for (int i = threadIdx.x; i < S * nv; i += blockDim.x) {
+    const int r = i / nv, v = i - r * nv;
+    const int bx = xa + (v << 4);
+    const uint4 q = *(const uint4*)(img + (size_t)(y0 + r) * pitch + bx);
+    const unsigned w[4] = { q.x, q.y, q.z, q.w };
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const int b0 = bx + 4 * k;
+      const unsigned m = byte_mask(x0 - b0, x0 + S - b0);
+      mn = __vminu4(mn, w[k] | ~m);
+      mx = __vmaxu4(mx, w[k] & m);
+    }
+  }
+  unsigned bmn = min(min(mn & 0xff, (mn >> 8) & 0xff), min((mn >> 16) & 0xff, mn >> 24));
+  unsigned bmx = max(max(mx & 0xff, (mx >> 8) & 0xff), max((mx >> 16) & 0xff, mx >> 24));
+  bmn = __reduce_min_sync(0xffffffffu, bmn);
+  bmx = __reduce_max_sync(0xffffffffu, bmx);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    smn[warp] = bmn;
+    smx[warp] = bmx;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); w++) {
+      bmn = min(bmn, smn[w]);
+      bmx = max(bmx, smx[w]);
+    }
+    out[f * 2 + 0] = (uint8_t)bmn;
+    out[f * 2 + 1] = (uint8_t)bmx;
+    if (coarse && skip) {
+      const double con = (double)((int)bmx - (int)bmn) / ((double)((int)bmx + (int)bmn) + 0.1);
+      skip[f] = !(con >= thr && con > 0.0);
+    }
+  }
 }
 
 /* ------------------------------------------------------------------------ */
@@ -355,6 +514,45 @@ static int launch_search(const GeomDev& gd, const uint8_t* curr, const uint8_t* 
   return -1;
 }
 
+/* full search of the items in list[0 .. *count), at most n of them:
+   persistent CTAs, as many as fit on the GPU at once */
+template <int TB>
+static int launch_list_tb(const GeomDev& gd, const uint8_t* curr, const uint8_t* prev, int pitch,
+                          const vsbd_item* d_items, int n, const int* count, const int* list,
+                          unsigned long long* keys, unsigned* tickets, vsbd_result* d_res,
+                          cudaStream_t st) {
+  cudaError_t e = cudaFuncSetAttribute(k_lattice_list<TB>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gd.smem);
+  int cps = 0;
+  if (e == cudaSuccess)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cps, k_lattice_list<TB>, gd.g.threads,
+                                                      gd.smem);
+  if (e != cudaSuccess) {
+    set_err("k_lattice_list set-up", e);
+    return -1;
+  }
+  long units = (long)n * gd.g.nta * gd.g.ntb;
+  long grid = (long)sm_count() * (cps > 0 ? cps : 1);
+  if (grid > units) grid = units;
+  k_lattice_list<TB><<<(unsigned)grid, gd.g.threads, gd.smem, st>>>(curr, prev, pitch, gd.g, d_items,
+                                                                   count, list, keys, tickets, d_res);
+  return 1;
+}
+
+static int launch_list(const GeomDev& gd, const uint8_t* curr, const uint8_t* prev, int pitch,
+                       const vsbd_item* d_items, int n, const int* count, const int* list,
+                       unsigned long long* keys, unsigned* tickets, vsbd_result* d_res,
+                       cudaStream_t st) {
+  if (n <= 0) return 0;
+  switch (gd.g.tb) {
+    case 2: return launch_list_tb<2>(gd, curr, prev, pitch, d_items, n, count, list, keys, tickets, d_res, st);
+    case 4: return launch_list_tb<4>(gd, curr, prev, pitch, d_items, n, count, list, keys, tickets, d_res, st);
+    case 8: return launch_list_tb<8>(gd, curr, prev, pitch, d_items, n, count, list, keys, tickets, d_res, st);
+  }
+  set_msg("unsupported rows-per-thread");
+  return -1;
+}
+
 /* the partial pass: every candidate's sum over the field's first rows */
 template <int TB>
 static int launch_emit_tb(const GeomDev& gd, const uint8_t* curr, const uint8_t* prev, int pitch,
@@ -547,10 +745,27 @@ struct vsbd_ctx {
   int* d_lists;                 /* survivors, per item */
   int* d_counts;
   int* d_boxes;                 /* survivors' lattice bounding box, per item */
-  uint8_t* d_out;               /* minmax | coarse results | fine results */
+  uint8_t* d_out;               /* minmax | coarse results | coarse proposal flags |
+                                   fine results | fine proposal flags */
   uint8_t* h_out;               /* pinned mirror of d_out */
   vsbd_item* h_items;           /* pinned staging of fine items */
-  size_t off_coarse, off_fine, out_bytes;
+  size_t off_coarse, off_cfb, off_fine, off_ffb, out_bytes;
+  /* learned search proposal */
+  void* d_pn;                   /* network parameters: bf16 weights | f32 biases */
+  PNSearch pn;
+  float pn_match_bound;         /* trusted refined SAD per field pixel */
+  int pn_on, pn_verify;
+  float* d_pout;                /* network outputs [nc + nf][3] */
+  vsbd_result* d_vres;          /* verify: full-search results, coarse then fine */
+  vsbd_result* h_vres;
+  GeomDev gcf, gff;             /* full-search tilings for the few items that fall back */
+  int* d_fbl;                   /* fallback count, then the fallback item list */
+  long long pn_stats[8];        /* searched, fell back, verified, identical; then
+                                   coarse searched / fell back, fine searched / fell back */
+  /* training-data log */
+  uint8_t* log_in;
+  PNLabel* log_lab;
+  long log_cap, log_n;
   long launches;
   int timing;                   /* record CUDA events around each kernel */
   cudaEvent_t ev[VSBD_NKT][2];
@@ -632,6 +847,11 @@ extern "C" void vsbd_destroy(vsbd_ctx* c) {
   cudaFree(c->d_boxes);
   if (c->h_out) cudaFreeHost(c->h_out);
   if (c->h_items) cudaFreeHost(c->h_items);
+  cudaFree(c->d_pn);
+  cudaFree(c->d_pout);
+  cudaFree(c->d_fbl);
+  cudaFree(c->d_vres);
+  if (c->h_vres) cudaFreeHost(c->h_vres);
   geom_free(&c->gc);
   geom_free(&c->gf);
   /* gcp/gfp share gc/gf's tables */
@@ -734,8 +954,10 @@ extern "C" int vsbd_create(vsbd_ctx** out, int W, int H, int bpp, int blur_size,
   CKC(cudaMalloc(&c->d_tickets, sizeof(unsigned) * (nc + nf + 2)));
   CKC(cudaMemset(c->d_tickets, 0, sizeof(unsigned) * (nc + nf + 2)));
   c->off_coarse = align16((size_t)(nc + nf) * channels * 2);
-  c->off_fine = c->off_coarse + align16(sizeof(vsbd_result) * (nc + 1));
-  c->out_bytes = c->off_fine + align16(sizeof(vsbd_result) * (nf + 1));
+  c->off_cfb = c->off_coarse + align16(sizeof(vsbd_result) * (nc + 1));
+  c->off_fine = c->off_cfb + align16((size_t)nc + 1);
+  c->off_ffb = c->off_fine + align16(sizeof(vsbd_result) * (nf + 1));
+  c->out_bytes = c->off_ffb + align16((size_t)nf + 1);
   CKC(cudaMalloc(&c->d_out, c->out_bytes));
   CKC(cudaMallocHost(&c->h_out, c->out_bytes));
   /* fine items for tuning: every fine field without offset */
@@ -760,6 +982,83 @@ extern "C" int vsbd_create(vsbd_ctx** out, int W, int H, int bpp, int blur_size,
   CKC(cudaStreamSynchronize(c->st));
 #undef CKC
   *out = c;
+  return 0;
+}
+
+/* The proposal path of one field set: network, narrowed search, full
+   search of the items that fell back (and, when verifying, the full search
+   of every item into d_vres + base). */
+static int learned_search(vsbd_ctx* c, const GeomDev& gd, const GeomDev& gfull,
+                          const vsbd_item* items, int n, int base,
+                          const uint8_t* skip, unsigned long long* keys, unsigned* tickets,
+                          vsbd_result* res, uint8_t* fb) {
+  if (n <= 0) return 0;
+  uint8_t* cur = c->d_buf[c->cur];
+  uint8_t* prv = c->d_buf[c->cur ^ 1];
+  float* pout = c->d_pout + (size_t)3 * base;
+  kt_begin(c, VSBD_KT_PNET);
+  if (vsbpn_infer(c->d_pn, cur, prv, c->pitch, c->W, c->H, items, NULL, n, pout, c->st) < 0) return -1;
+  kt_end(c, VSBD_KT_PNET);
+  const int kt = base == 0 ? VSBD_KT_COARSE : VSBD_KT_FINE;
+  kt_begin(c, kt);
+  /* the SAD bound scales with the field's pixel count */
+  PNSearch ps = c->pn;
+  const double bound = (double)c->pn_match_bound * gd.g.S * gd.g.S;
+  ps.sad_bound = bound >= 4294967295.0 ? 0xffffffffu : (unsigned)bound;
+  CK(cudaMemsetAsync(c->d_fbl, 0, sizeof(int), c->st));
+  if (vsbpn_narrow(gd.g, cur, prv, c->pitch, items, n, pout, ps, skip, res, fb, c->d_fbl,
+                   c->d_fbl + 1, c->st) < 0)
+    return -1;
+  kt_end(c, kt);
+  kt_begin(c, VSBD_KT_FALLBACK);
+  int nl = launch_list(gfull, cur, prv, c->pitch, items, n, c->d_fbl, c->d_fbl + 1, keys, tickets,
+                       res, c->st);
+  if (nl < 0) return -1;
+  kt_end(c, VSBD_KT_FALLBACK);
+  c->launches += 2 + nl;
+  count_launches(2 + nl);
+  if (c->pn_verify) {
+    int nv = launch_search(gd, cur, prv, c->pitch, items, n, keys, tickets, c->d_vres + base, c->st);
+    if (nv < 0) return -1;
+    c->launches += nv;
+    count_launches(nv);
+  }
+  return 0;
+}
+
+/* counts of one stage after its results reached the host */
+static void proposal_tally(vsbd_ctx* c, const uint8_t* fb, const vsbd_result* res,
+                           const vsbd_result* vres, int n, int kind) {
+  for (int i = 0; i < n; i++) {
+    if (fb[i] == PN_FB_UNUSED) continue;
+    c->pn_stats[0]++;
+    c->pn_stats[4 + 2 * kind]++;
+    if (fb[i] == PN_FB_FULL) {
+      c->pn_stats[1]++;
+      c->pn_stats[5 + 2 * kind]++;
+    }
+    if (c->pn_verify && vres) {
+      c->pn_stats[2]++;
+      if (res[i].sad == vres[i].sad && res[i].tx == vres[i].tx && res[i].ty == vres[i].ty &&
+          res[i].ok == vres[i].ok)
+        c->pn_stats[3]++;
+    }
+  }
+}
+
+/* appends the network inputs and full-search labels of n items to the log */
+static int log_items(vsbd_ctx* c, const vsbd_item* items, int n, int kind, const vsbd_result* res,
+                     const uint8_t* skip) {
+  if (n <= 0 || c->log_n + n > c->log_cap) return 0;
+  uint8_t* cur = c->d_buf[c->cur];
+  uint8_t* prv = c->d_buf[c->cur ^ 1];
+  if (vsbpn_crops(cur, prv, c->pitch, c->W, c->H, items, n, c->log_in + (size_t)c->log_n * 4096,
+                  c->st) < 0 ||
+      vsbpn_labels(res, skip, n, kind, c->log_lab + c->log_n, c->st) < 0)
+    return -1;
+  c->launches += 2;
+  count_launches(2);
+  c->log_n += n;
   return 0;
 }
 
@@ -794,12 +1093,23 @@ extern "C" int vsbd_stage_a(vsbd_ctx* c, const uint8_t* host, int linesize, cons
   }
   if (search) {
     int S = c->gc.g.S;
+    /* the contrast flags steer the pruned and the proposal searches and mark
+       the training log's unused fields */
+    uint8_t* skip = (c->mode || c->pn_on || c->log_in) ? c->d_skip : NULL;
+    vsbd_result* cres = (vsbd_result*)(c->d_out + c->off_coarse);
     kt_begin(c, VSBD_KT_MINMAX);
+    if (c->bpp == 1 && c->nch == 1) {
+      k_minmax_planar<<<c->nc + c->nf, 256, 0, c->st>>>(cur, c->pitch, c->d_xy, c->nc, c->nf, S,
+                                                        c->gf.g.S, c->d_out, c->thr_coarse, skip);
+      c->launches++;
+      count_launches(1);
+    } else {
     k_minmax<<<c->nc, 256, 0, c->st>>>(cur, c->pitch, c->d_xy, c->d_xy + c->nc, S, c->bpp, c->nch,
-                                       c->d_out, c->thr_coarse, c->mode ? c->d_skip : NULL);
+                                       c->d_out, c->thr_coarse, skip);
     c->launches++;
     count_launches(1);
-    if (c->nf > 0) {
+    }
+    if (c->nf > 0 && !(c->bpp == 1 && c->nch == 1)) {
       k_minmax<<<c->nf, 256, 0, c->st>>>(cur, c->pitch, c->d_xy + 2 * c->nc, c->d_xy + 2 * c->nc + c->nf,
                                          c->gf.g.S, c->bpp, c->nch, c->d_out + (size_t)c->nc * c->nch * 2,
                                          0.0, NULL);
@@ -807,23 +1117,35 @@ extern "C" int vsbd_stage_a(vsbd_ctx* c, const uint8_t* host, int linesize, cons
       count_launches(1);
     }
     kt_end(c, VSBD_KT_MINMAX);
-    kt_begin(c, VSBD_KT_COARSE);
-    int nl = c->mode ? launch_pruned(c->gc, c->gcp, cur, prv, c->pitch, c->d_citems, c->nc,
-                                     c->d_skip, c->d_part, c->d_counts, c->d_lists, c->d_boxes,
-                                     c->d_keys, c->d_tickets,
-                                     (vsbd_result*)(c->d_out + c->off_coarse), c->st)
-                     : launch_search(c->gc, cur, prv, c->pitch, c->d_citems, c->nc, c->d_keys,
-                                     c->d_tickets, (vsbd_result*)(c->d_out + c->off_coarse), c->st);
-    if (nl < 0) return -1;
-    c->launches += nl;
-    count_launches(nl);
-    kt_end(c, VSBD_KT_COARSE);
+    if (c->pn_on) {
+      if (learned_search(c, c->gc, c->gcf, c->d_citems, c->nc, 0, skip, c->d_keys, c->d_tickets, cres,
+                         c->d_out + c->off_cfb) != 0)
+        return -1;
+    } else {
+      kt_begin(c, VSBD_KT_COARSE);
+      int nl = c->mode ? launch_pruned(c->gc, c->gcp, cur, prv, c->pitch, c->d_citems, c->nc,
+                                       c->d_skip, c->d_part, c->d_counts, c->d_lists, c->d_boxes,
+                                       c->d_keys, c->d_tickets, cres, c->st)
+                       : launch_search(c->gc, cur, prv, c->pitch, c->d_citems, c->nc, c->d_keys,
+                                       c->d_tickets, cres, c->st);
+      if (nl < 0) return -1;
+      c->launches += nl;
+      count_launches(nl);
+      kt_end(c, VSBD_KT_COARSE);
+      if (c->log_in && log_items(c, c->d_citems, c->nc, 0, cres, skip) != 0) return -1;
+    }
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(c->h_out, c->d_out, c->off_fine, cudaMemcpyDeviceToHost, c->st));
     count_d2h(c->off_fine);
+    if (c->pn_on && c->pn_verify)
+      CK(cudaMemcpyAsync(c->h_vres, c->d_vres, sizeof(vsbd_result) * c->nc, cudaMemcpyDeviceToHost,
+                         c->st));
   }
   CK(cudaStreamSynchronize(c->st));
   kt_collect(c);
+  if (search && c->pn_on)
+    proposal_tally(c, c->h_out + c->off_cfb, (const vsbd_result*)(c->h_out + c->off_coarse),
+                   c->h_vres, c->nc, 0);
   if (minmax) *minmax = c->h_out;
   if (coarse) *coarse = (const vsbd_result*)(c->h_out + c->off_coarse);
   return 0;
@@ -839,31 +1161,130 @@ extern "C" int vsbd_stage_b(vsbd_ctx* c, const vsbd_item* items, int n, const vs
   count_h2d(sizeof(vsbd_item) * n);
   uint8_t* cur = c->d_buf[c->cur];
   uint8_t* prv = c->d_buf[c->cur ^ 1];
-  kt_begin(c, VSBD_KT_FINE);
-  int nl = c->mode ? launch_pruned(c->gf, c->gfp, cur, prv, c->pitch, c->d_fitems, n, NULL,
-                                   c->d_part, c->d_counts + c->nc, c->d_lists,
-                                   c->d_boxes + 4 * c->nc, c->d_keys + c->nc,
-                                   c->d_tickets + c->nc, (vsbd_result*)(c->d_out + c->off_fine),
-                                   c->st)
-                   : launch_search(c->gf, cur, prv, c->pitch, c->d_fitems, n, c->d_keys + c->nc,
-                                   c->d_tickets + c->nc, (vsbd_result*)(c->d_out + c->off_fine),
-                                   c->st);
-  if (nl < 0) return -1;
-  c->launches += nl;
-  count_launches(nl);
-  kt_end(c, VSBD_KT_FINE);
+  vsbd_result* fres = (vsbd_result*)(c->d_out + c->off_fine);
+  size_t d2h = sizeof(vsbd_result) * n;
+  if (c->pn_on) {
+    if (learned_search(c, c->gf, c->gff, c->d_fitems, n, c->nc, NULL, c->d_keys + c->nc,
+                       c->d_tickets + c->nc, fres, c->d_out + c->off_ffb) != 0)
+      return -1;
+    d2h = c->off_ffb - c->off_fine + n;
+  } else {
+    kt_begin(c, VSBD_KT_FINE);
+    int nl = c->mode ? launch_pruned(c->gf, c->gfp, cur, prv, c->pitch, c->d_fitems, n, NULL,
+                                     c->d_part, c->d_counts + c->nc, c->d_lists,
+                                     c->d_boxes + 4 * c->nc, c->d_keys + c->nc,
+                                     c->d_tickets + c->nc, fres, c->st)
+                     : launch_search(c->gf, cur, prv, c->pitch, c->d_fitems, n, c->d_keys + c->nc,
+                                     c->d_tickets + c->nc, fres, c->st);
+    if (nl < 0) return -1;
+    c->launches += nl;
+    count_launches(nl);
+    kt_end(c, VSBD_KT_FINE);
+    if (c->log_in && log_items(c, c->d_fitems, n, 1, fres, NULL) != 0) return -1;
+  }
   CK(cudaGetLastError());
-  CK(cudaMemcpyAsync(c->h_out + c->off_fine, c->d_out + c->off_fine, sizeof(vsbd_result) * n,
-                     cudaMemcpyDeviceToHost, c->st));
-  count_d2h(sizeof(vsbd_result) * n);
+  CK(cudaMemcpyAsync(c->h_out + c->off_fine, c->d_out + c->off_fine, d2h, cudaMemcpyDeviceToHost,
+                     c->st));
+  count_d2h(d2h);
+  if (c->pn_on && c->pn_verify)
+    CK(cudaMemcpyAsync(c->h_vres + c->nc, c->d_vres + c->nc, sizeof(vsbd_result) * n,
+                       cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
   kt_collect(c);
+  if (c->pn_on)
+    proposal_tally(c, c->h_out + c->off_ffb, (const vsbd_result*)(c->h_out + c->off_fine),
+                   c->h_vres ? c->h_vres + c->nc : NULL, n, 1);
   return 0;
 }
 
 extern "C" void vsbd_commit_prev(vsbd_ctx* c) { c->cur ^= 1; }
 
 extern "C" long vsbd_launches(const vsbd_ctx* c) { return c ? c->launches : 0; }
+
+extern "C" long vsbd_pnet_param_bytes(void) { return (long)PN_PARAM_BYTES; }
+
+extern "C" int vsbd_set_proposal(vsbd_ctx* c, const void* params, float scale, float radius,
+                                 float conf_min, float match_bound) {
+  if (!c) return -1;
+  CK(cudaSetDevice(c->dev));
+  CK(cudaStreamSynchronize(c->st));
+  if (!params) {
+    c->pn_on = 0;
+    return 0;
+  }
+  if (c->bpp != 1 || c->gc.g.has_origin || c->gf.g.has_origin) {
+    set_msg("the search proposal serves planar formats only");
+    return -1;
+  }
+  if (!(scale > 0.f) || !(radius >= 0.f) || !(match_bound >= 0.f)) {
+    set_msg("bad proposal settings");
+    return -1;
+  }
+  if (!c->d_pn) CK(cudaMalloc(&c->d_pn, PN_PARAM_BYTES));
+  if (!c->d_pout) CK(cudaMalloc(&c->d_pout, sizeof(float) * 3 * (c->nc + c->nf + 1)));
+  if (!c->d_fbl) CK(cudaMalloc(&c->d_fbl, sizeof(int) * (c->nc + c->nf + 2)));
+  CK(cudaMemcpy(c->d_pn, params, PN_PARAM_BYTES, cudaMemcpyHostToDevice));
+  /* the full search of the items that fall back: a tiling for a handful of
+     items, so that one item's lattice is spread over many CTAs (the
+     detector's own tiling gives each item a few CTAs, and one fallback would
+     then take as long as searching every field) */
+  {
+    TileCand tc[1];
+    c->gcf = c->gc;
+    c->gff = c->gf;
+    if (tile_candidates(c->gc.g, 2, 0, 0, 0, 0, tc, 1) >= 1) {
+      c->gcf.g = tc[0].g;
+      c->gcf.smem = tile_layout(tc[0].g).total;
+    }
+    if (tile_candidates(c->gf.g, 8, 0, 0, 0, 0, tc, 1) >= 1) {
+      c->gff.g = tc[0].g;
+      c->gff.smem = tile_layout(tc[0].g).total;
+    }
+  }
+  c->pn.scale = scale;
+  c->pn.radius = radius;
+  c->pn.conf_min = conf_min;
+  c->pn.sad_bound = 0xffffffffu;
+  c->pn_match_bound = match_bound;
+  c->pn_on = 1;
+  return 0;
+}
+
+extern "C" int vsbd_set_proposal_verify(vsbd_ctx* c, int on) {
+  if (!c) return -1;
+  CK(cudaSetDevice(c->dev));
+  if (on && !c->d_vres) {
+    CK(cudaMalloc(&c->d_vres, sizeof(vsbd_result) * (c->nc + c->nf + 1)));
+    CK(cudaMallocHost(&c->h_vres, sizeof(vsbd_result) * (c->nc + c->nf + 1)));
+  }
+  c->pn_verify = on ? 1 : 0;
+  return 0;
+}
+
+extern "C" int vsbd_proposal_stats(const vsbd_ctx* c, long long* st) {
+  if (!c || !st) return -1;
+  for (int k = 0; k < 8; k++) st[k] = c->pn_stats[k];
+  return 0;
+}
+
+extern "C" int vsbd_set_field_log(vsbd_ctx* c, void* d_inputs, void* d_labels, long cap) {
+  if (!c) return -1;
+  if (d_inputs && (!d_labels || cap < 0)) {
+    set_msg("field log needs inputs, labels and a capacity");
+    return -1;
+  }
+  if (d_inputs && c->bpp != 1) {
+    set_msg("the field log serves planar formats only");
+    return -1;
+  }
+  c->log_in = (uint8_t*)d_inputs;
+  c->log_lab = (PNLabel*)d_labels;
+  c->log_cap = d_inputs ? cap : 0;
+  c->log_n = 0;
+  return 0;
+}
+
+extern "C" long vsbd_field_log_count(const vsbd_ctx* c) { return c ? c->log_n : -1; }
 
 /* ------------------------------------------------------------------------ */
 /* kernel-level entry points (parity tests)                                  */

@@ -85,12 +85,54 @@ void vsbd_commit_prev(vsbd_ctx* c);
 /* Kernel launches issued on behalf of this detector so far. */
 long vsbd_launches(const vsbd_ctx* c);
 
-/* per-kernel CUDA-event timing (indices VSBD_KT_*) */
+/* per-kernel CUDA-event timing (indices VSBD_KT_*); with a proposal
+   network, COARSE and FINE time the narrowed searches, PNET the network and
+   FALLBACK the full searches of the items that fell back */
 #define VSBD_KT_BLUR 0
 #define VSBD_KT_MINMAX 1
 #define VSBD_KT_COARSE 2
 #define VSBD_KT_FINE 3
-#define VSBD_NKT 4
+#define VSBD_KT_PNET 4
+#define VSBD_KT_FALLBACK 5
+#define VSBD_NKT 6
+
+/* ---- learned search proposal (vsb_pnet.cu) ---- */
+
+/* Turns the proposal on for this detector (params: the network's bf16
+   weights followed by its f32 biases, pn_param_bytes() bytes, host memory)
+   or off (params NULL).  scale: network units -> pixels; radius: pixels
+   around the prediction; conf_min: confidence logit threshold;
+   match_bound: largest trusted refined SAD per pixel.  Planar only. */
+int vsbd_set_proposal(vsbd_ctx* c, const void* params, float scale, float radius, float conf_min,
+                      float match_bound);
+long vsbd_pnet_param_bytes(void);
+/* with verify on, every stage also runs the full search and compares */
+int vsbd_set_proposal_verify(vsbd_ctx* c, int on);
+/* [0] items searched with a proposal, [1] of them fell back, [2] items
+   verified against the full search, [3] of them identical; [4]/[5] and
+   [6]/[7] searched / fell back of the coarse and the fine items */
+int vsbd_proposal_stats(const vsbd_ctx* c, long long* st);
+/* Training-data log: every searched item's network input (d_inputs, 4096
+   bytes each) and full-search label (d_labels, 12 bytes each) appended,
+   up to cap items; NULL turns it off.  Plain (full-search) detectors only. */
+int vsbd_set_field_log(vsbd_ctx* c, void* d_inputs, void* d_labels, long cap);
+long vsbd_field_log_count(const vsbd_ctx* c);
+
+/* network kernels (device pointers; stream may be NULL) */
+int vsbd_pnet_forward_train(const void* d_params, const void* d_input, int n, void* d_acts,
+                            float* d_out, void* stream);
+int vsbd_pnet_backward(const void* d_params, const void* d_input, const void* d_acts, int n,
+                       const float* d_dout, float* d_grad, void* d_work, void* stream);
+int vsbd_pnet_infer(const void* d_params, const void* d_input, int n, float* d_out, void* stream);
+int vsbd_pnet_infer_items(const void* d_params, const uint8_t* d_curr, const uint8_t* d_prev,
+                          int pitch, int width, int height, const void* d_items, int n,
+                          float* d_out, void* stream);
+int vsbd_pnet_crops(const uint8_t* d_curr, const uint8_t* d_prev, int pitch, int width,
+                    int height, const void* d_items, int n, void* d_input, void* stream);
+int vsbd_pnet_narrow_host(const uint8_t* curr, const uint8_t* prev, int width, int height,
+                          const vsbd_geom* g, const vsbd_item* items, int n, const float* pout,
+                          float scale, float radius, float conf_min, unsigned sad_bound,
+                          vsbd_result* out, uint8_t* flags);
 int vsbd_set_timing(vsbd_ctx* c, int on);
 int vsbd_kernel_times(const vsbd_ctx* c, double* ms, long* n);
 

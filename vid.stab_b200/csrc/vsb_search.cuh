@@ -450,6 +450,28 @@ __global__ void __launch_bounds__(512, 1) k_lattice(const uint8_t* __restrict__ 
                          gridDim.x, sm);
 }
 
+/* Full search of the items listed in list[0 .. *count) (indices into
+   items): persistent CTAs take the (item, tile) units in turn; the last
+   tile of an item to finish refines it, as in k_lattice. */
+template <int TB>
+__global__ void __launch_bounds__(512, 1) k_lattice_list(const uint8_t* __restrict__ curr,
+                                                       const uint8_t* __restrict__ prev, int pitch,
+                                                       DGeom g, const vsbd_item* __restrict__ items,
+                                                       const int* __restrict__ count,
+                                                       const int* __restrict__ list,
+                                                       unsigned long long* __restrict__ keys,
+                                                       unsigned* __restrict__ tickets,
+                                                       vsbd_result* __restrict__ res) {
+  extern __shared__ __align__(16) uint8_t sm[];
+  const int ntiles = g.nta * g.ntb;
+  const int nu = *count * ntiles;
+  for (int u = blockIdx.x; u < nu; u += gridDim.x) {
+    lattice_tile<TB, false>(curr, prev, pitch, g, items, keys, tickets, res, list[u / ntiles],
+                            u % ntiles, ntiles, sm);
+    __syncthreads();
+  }
+}
+
 /* Bound and survivors of one item after the partial pass (one CTA per item).
    The topk candidates with the smallest partial sums (ties by rank) get their
    full SAD; the smallest gives the bound B and the item's starting key.  A
