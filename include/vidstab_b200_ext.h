@@ -67,7 +67,10 @@ VS_API long vsb_detect_clip(int width, int height, int pformat, const uint8_t* f
    LocalMotions of every frame are appended to out (at most out_cap records,
    LocalMotion layout) and freed; counts[k] receives their number.  The
    detector's state (previous frame, frame number) carries over between
-   calls.  Returns the number of records, or -1. */
+   calls.  Without tripod mode or overlay, and with the dense search, frame
+   k+1's upload, blur, min/max and coarse search run on the GPU while frame
+   k's fine search runs and its motions are assembled (same results).
+   Returns the number of records, or -1. */
 VS_API long vsb_detect_run(struct _vsmotiondetect* md, const uint8_t* frames, long frame_bytes,
                            int linesize, int nframes, int on_device, void* out, long out_cap,
                            int* counts);
@@ -85,6 +88,14 @@ VS_API int vsb_kernel_times(const struct _vsmotiondetect* md, double* ms, long* 
    bytes it copied host-to-device (frames, work lists) and device-to-host
    (per-field results). */
 VS_API void vsb_counters(long long* launches, long long* h2d_bytes, long long* d2h_bytes);
+
+/* Process-wide wall time of the per-frame path since load or the last
+   reset, summed over frames: sec[0] device stage A (frame upload, blur,
+   min/max, coarse search, results back), sec[1] host part A (selection,
+   coarse motions, the simple model, fine work list), sec[2] device stage B
+   (fine search), sec[3] host part B (fine motions, mean-match filter,
+   result); *frames the number of frames. */
+VS_API void vsb_host_profile(double* sec, long* frames, int reset);
 
 /* Measured byte-absolute-difference throughput (per second) of the GPU's
    packed SAD instruction sequence in a register-only loop: variant 0 the
@@ -193,6 +204,11 @@ VS_API int vsb_set_proposal(struct _vsmotiondetect* md, const void* blob, long b
    (if not NaN) and match_bound (if >= 0) */
 VS_API int vsb_set_proposal_ex(struct _vsmotiondetect* md, const void* blob, long bytes,
                                double radius, double conf_min, double match_bound);
+/* Which fields the network serves: the coarse fields always; the fine
+   fields too with fine_net = 1.  With fine_net = 0 (the default) a fine
+   field's narrowed window is centred on the coarse model's prediction for
+   it (zero residual), with the same fallbacks. */
+VS_API int vsb_set_proposal_scope(struct _vsmotiondetect* md, int fine_net);
 /* With verify on, every stage also runs the full search of every item and
    counts the items whose result (SAD, shift, range test) is identical. */
 VS_API int vsb_set_proposal_verify(struct _vsmotiondetect* md, int on);

@@ -1,0 +1,73 @@
+"""The overlapped frame loop (vsb_detect_run: frame k+1's stage A on the GPU
+while frame k's fine search runs) gives, frame by frame, the LocalMotions of
+the per-frame API, with and without a search proposal, from host and from
+device frames."""
+import numpy as np
+import pytest
+
+import oracle as O
+import vidstab_b200 as V
+from vidstab_b200 import pnet
+from vidstab_b200 import synthetic as S
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+def _per_frame(det, clip, w, h):
+    out, cnt = [], []
+    for k in range(clip.shape[0]):
+        r = det.detect_device(clip.data_ptr() + k * w * h, w)
+        out.append(r)
+        cnt.append(len(r))
+    return np.concatenate(out), np.array(cnt, np.int32)
+
+
+def _run(det, ptr, n, w, h, on_device):
+    rec = np.zeros(n * 512 + 64, V.LM_DTYPE)
+    cnt = np.zeros(n, np.int32)
+    tot = det.run(n, ptr, w * h, w, on_device, rec, cnt)
+    return rec[:tot].copy(), cnt
+
+
+@pytest.mark.parametrize("w,h", [(640, 480), (1920, 1080)])
+def test_overlapped_equals_per_frame(w, h):
+    n = 14
+    clip = S.clip(w, h, n, seed=31, device="cuda")
+    a = V.MotionDetector(w, h, V.PF_YUV420P)
+    exp, ec = _per_frame(a, clip, w, h)
+    b = V.MotionDetector(w, h, V.PF_YUV420P)
+    got, gc = _run(b, clip.data_ptr(), n, w, h, True)
+    assert np.array_equal(gc, ec) and np.array_equal(got, exp)
+    host = clip.cpu().numpy()
+    c = V.MotionDetector(w, h, V.PF_YUV420P)
+    got2, gc2 = _run(c, host.ctypes.data, n, w, h, False)
+    assert np.array_equal(gc2, ec) and np.array_equal(got2, exp)
+
+
+def test_overlapped_matches_reference():
+    if not O.ref_available():
+        pytest.skip("reference build not present")
+    w, h, n = 640, 480, 8
+    host = S.clip(w, h, n, seed=32)
+    clip = torch.from_numpy(host).cuda()
+    det = V.MotionDetector(w, h, V.PF_YUV420P)
+    got, gc = _run(det, clip.data_ptr(), n, w, h, True)
+    exp, ec, _ = O.ref_clip(host, V.PF_YUV420P)
+    assert np.array_equal(gc, ec)
+    for k in ("vx", "vy", "fx", "fy", "fsize", "contrast", "match"):
+        assert np.array_equal(got[k], exp[k]), k
+
+
+def test_overlapped_with_proposal():
+    w, h, n = 1920, 1080, 12
+    clip = S.clip(w, h, n, seed=33, device="cuda")
+    blob = pnet.load_blob()
+    a = V.MotionDetector(w, h, V.PF_YUV420P)
+    pnet.set_proposal(a, blob)
+    exp, ec = _per_frame(a, clip, w, h)
+    b = V.MotionDetector(w, h, V.PF_YUV420P)
+    pnet.set_proposal(b, blob)
+    got, gc = _run(b, clip.data_ptr(), n, w, h, True)
+    assert np.array_equal(gc, ec) and np.array_equal(got, exp)

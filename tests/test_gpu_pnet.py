@@ -198,7 +198,7 @@ def test_detector_full_fallback_is_plain():
     plain = V.MotionDetector(w, h, V.PF_YUV420P)
     exp, ec = _run(plain, clip, w, h)
     det = V.MotionDetector(w, h, V.PF_YUV420P)
-    pnet.set_proposal(det, pnet.zero_blob(), conf_min=1e30, verify=True)
+    pnet.set_proposal(det, pnet.zero_blob(), conf_min=1e30, verify=True, fine_net=True)
     got, gc = _run(det, clip, w, h)
     st = pnet.proposal_stats(det)
     assert np.array_equal(gc, ec)

@@ -134,6 +134,9 @@ long vsb_detect_run(VSMotionDetect* md, const uint8_t* frames, long frame_bytes,
   if (!md || !frames || nframes < 0) return -1;
   LocalMotion* rec = (LocalMotion*)out;
   long total = 0;
+  if (nframes > 1 && vsb_can_overlap(md))
+    return vsb_detect_run_overlapped(md, frames, frame_bytes, linesize, nframes, on_device, rec,
+                                     out_cap, counts);
   for (int k = 0; k < nframes; k++) {
     LocalMotions lms;
     const uint8_t* src = frames + (size_t)k * frame_bytes;

@@ -24,6 +24,7 @@
 #include <pthread.h>
 #include <stdlib.h>
 #include <string.h>
+#include <time.h>
 
 #include "vidstab_b200.h"
 #include "vsb_device.h"
@@ -44,6 +45,7 @@ struct md_state {
   contrast_idx* ci;    /* selection scratch: original, */
   contrast_idx* seg;   /* per-segment sorted copy, */
   contrast_idx* sel;   /* result in append order */
+  contrast_idx* tmp;   /* merge buffer of the sort */
   vsbd_item* items;    /* fine work list */
   int* item_sel;       /* fine item -> position in sel */
   long frames;
@@ -70,6 +72,7 @@ static void state_free(md_state* s) {
   free(s->ci);
   free(s->seg);
   free(s->sel);
+  free(s->tmp);
   free(s->items);
   free(s->item_sel);
   free(s);
@@ -335,12 +338,14 @@ int vsb_md_init(VSMotionDetect* md, const VSMotionDetectConfig* conf, const VSFr
   st->ci = (contrast_idx*)malloc(sizeof(contrast_idx) * (size_t)nmax);
   st->seg = (contrast_idx*)malloc(sizeof(contrast_idx) * (size_t)nmax);
   st->sel = (contrast_idx*)malloc(sizeof(contrast_idx) * (size_t)nmax);
+  st->tmp = (contrast_idx*)malloc(sizeof(contrast_idx) * (size_t)nmax);
   st->items = (vsbd_item*)malloc(sizeof(vsbd_item) * (size_t)(nf + 1));
   st->item_sel = (int*)malloc(sizeof(int) * (size_t)(nf + 1));
 
   vsbd_geom gc, gf;
   int32_t *oc = NULL, *of = NULL;
-  int ok = st->con_c && st->con_f && st->ci && st->seg && st->sel && st->items && st->item_sel;
+  int ok = st->con_c && st->con_f && st->ci && st->seg && st->sel && st->tmp && st->items &&
+           st->item_sel;
   ok = ok && vsb_build_geom(&gc, &oc, fieldSize, st->bpp, maxShift, md->conf.stepSize, st->planar) == 0;
   ok = ok && vsb_build_geom(&gf, &of, fieldSizeFine, st->bpp, fieldSizeFine, 2, st->planar) == 0;
   if (ok && (!geometry_fits(md, &md->fieldscoarse, &gc, 1) ||
@@ -420,12 +425,34 @@ void vsMotionDetectionCleanup(VSMotionDetect* md) {
 /* field selection (src/motiondetect.c:662-743)                              */
 /* ------------------------------------------------------------------------ */
 
-/* descending contrast; equal contrasts compare equal, so their order is
-   whatever libc qsort makes of it -- exactly as in the reference */
-static int cmp_contrast_idx(const void* a, const void* b) {
-  double x = ((const contrast_idx*)a)->contrast;
-  double y = ((const contrast_idx*)b)->contrast;
-  return x < y ? 1 : (x > y ? -1 : 0);
+/* Sorts by descending contrast, keeping the order of equal contrasts.  The
+   reference sorts with libc qsort and a comparator that orders by
+   descending contrast and calls equal contrasts equal (cmp_contrast_idx,
+   src/motiondetect.c:665-669); glibc's qsort is a stable merge sort at
+   these sizes, so the permutation is the stable one, which this sort gives
+   without a comparator call per comparison.  tmp holds n elements. */
+static void sort_contrast_desc(contrast_idx* a, int n, contrast_idx* tmp) {
+  if (n < 2) return;
+  if (n <= 24) {
+    for (int i = 1; i < n; i++) {
+      contrast_idx x = a[i];
+      int j = i;
+      while (j > 0 && a[j - 1].contrast < x.contrast) {
+        a[j] = a[j - 1];
+        j--;
+      }
+      a[j] = x;
+    }
+    return;
+  }
+  int h = n / 2;
+  sort_contrast_desc(a, h, tmp);
+  sort_contrast_desc(a + h, n - h, tmp);
+  int i = 0, j = h, k = 0;
+  while (i < h && j < n) tmp[k++] = a[j].contrast > a[i].contrast ? a[j++] : a[i++];
+  while (i < h) tmp[k++] = a[i++];
+  while (j < n) tmp[k++] = a[j++];
+  memcpy(a, tmp, sizeof(contrast_idx) * (size_t)n);
 }
 
 /* fills st->sel in the reference's append order; returns the count */
@@ -444,7 +471,7 @@ static int select_fields(md_state* st, const VSMotionDetectFields* fs, const dou
   for (int s = 0; s < numsegms; s++) {
     int a = segmlen * s;
     int b = VS_MIN(segmlen * (s + 1), n);
-    qsort(seg + a, (size_t)(b - a > 0 ? b - a : 0), sizeof(contrast_idx), cmp_contrast_idx);
+    sort_contrast_desc(seg + a, b - a > 0 ? b - a : 0, st->tmp);
     for (int j = 0; j < per_seg; j++) {
       if (a + j >= b) continue;
       if (seg[a + j].contrast > 0) {
@@ -455,7 +482,7 @@ static int select_fields(md_state* st, const VSMotionDetectFields* fs, const dou
   }
   int remaining = fs->maxFields - nsel;
   if (remaining > 0) {
-    qsort(seg, (size_t)n, sizeof(contrast_idx), cmp_contrast_idx);
+    sort_contrast_desc(seg, n, st->tmp);
     for (int j = 0; j < remaining; j++)
       if (seg[j].contrast > 0) st->sel[nsel++] = seg[j];
   }
@@ -621,6 +648,29 @@ int vsb_frame_end(VSMotionDetect* md) {
   return commit;
 }
 
+/* process-wide wall-time profile of the per-frame path (seconds): device
+   stage A, host part A, device stage B, host part B (read by benchmarks) */
+static double g_prof[4];
+static long g_prof_frames;
+
+static double now_s(void) {
+  struct timespec ts;
+  clock_gettime(CLOCK_MONOTONIC, &ts);
+  return ts.tv_sec + ts.tv_nsec * 1e-9;
+}
+
+void vsb_host_profile(double* sec, long* frames, int reset) {
+  pthread_mutex_lock(&g_lock);
+  if (sec)
+    for (int k = 0; k < 4; k++) sec[k] = g_prof[k];
+  if (frames) *frames = g_prof_frames;
+  if (reset) {
+    memset(g_prof, 0, sizeof(g_prof));
+    g_prof_frames = 0;
+  }
+  pthread_mutex_unlock(&g_lock);
+}
+
 int vsb_detect_common(VSMotionDetect* md, LocalMotions* motions, const uint8_t* host, int linesize,
                       const uint8_t* dev, int pitch) {
   int search = 0;
@@ -628,25 +678,121 @@ int vsb_detect_common(VSMotionDetect* md, LocalMotions* motions, const uint8_t* 
   md_state* st = state_find(md);
   const uint8_t* mm = NULL;
   const vsbd_result* cres = NULL;
+  double t[5] = { now_s(), 0, 0, 0, 0 };
   if (vsbd_stage_a(st->dev, host, linesize, dev, pitch, search, &mm, &cres) != 0) {
     vs_log_error(md->conf.modName, "GPU stage A failed: %s\n", vsbd_error());
     return VS_ERROR;
   }
+  t[1] = now_s();
+  t[2] = t[3] = t[1];
   if (search) {
     vsb_frame_work w;
     vsb_frame_host_a(md, mm, cres, &w);
+    t[2] = now_s();
     const vsbd_result* fres = NULL;
     if (w.fine_pass && vsbd_stage_b(st->dev, w.items, w.nitems, &fres) != 0) {
       vs_log_error(md->conf.modName, "GPU stage B failed: %s\n", vsbd_error());
       vsb_frame_discard(&w);
       return VS_ERROR;
     }
+    t[3] = now_s();
     vsb_frame_host_b(md, fres, &w, motions);
   } else {
     vsb_frame_first(md, motions);
   }
   if (vsb_frame_end(md)) vsbd_commit_prev(st->dev);
+  t[4] = now_s();
+  pthread_mutex_lock(&g_lock);
+  for (int k = 0; k < 4; k++) g_prof[k] += t[k + 1] - t[k];
+  g_prof_frames++;
+  pthread_mutex_unlock(&g_lock);
   return VS_OK;
+}
+
+/* Copies a frame's motions into the record array and frees them. */
+static long append_records(LocalMotions* lms, LocalMotion* rec, long total, long cap, int* count) {
+  int n = vs_vector_size(lms);
+  if (count) *count = n;
+  for (int i = 0; i < n; i++) {
+    if (rec && total < cap) rec[total] = *LMGet(lms, i);
+    total++;
+  }
+  vs_vector_del(lms);
+  return total;
+}
+
+int vsb_can_overlap(const VSMotionDetect* md) {
+  md_state* st = state_find(md);
+  return st && md->conf.virtualTripod < 1 && !md->conf.show && vsbd_can_overlap(st->dev);
+}
+
+/* A clip through the detector with consecutive frames overlapped on the
+   GPU: while frame k's fine search runs on one stream and the host selects
+   and assembles frame k's motions, stage A of frame k+1 (upload, blur,
+   min/max, coarse search) runs on the other.  Same results, frame by frame,
+   as calling vsMotionDetection (or vsb_motion_detection_device) in order.
+   Plane 0 of frame k is at frames + k*frame_bytes (host memory, or device
+   memory with on_device).  Returns the total number of records, or -1. */
+long vsb_detect_run_overlapped(VSMotionDetect* md, const uint8_t* frames, long frame_bytes,
+                               int linesize, int nframes, int on_device, LocalMotion* rec,
+                               long out_cap, int* counts) {
+  md_state* st = state_find(md);
+  long total = 0;
+  int k = 0;
+  if (!st) return -1;
+  /* the first frame only primes the detector */
+  while (k < nframes && !md->hasSeenOneFrame) {
+    LocalMotions lms;
+    const uint8_t* src = frames + (size_t)k * frame_bytes;
+    if (vsb_detect_common(md, &lms, on_device ? NULL : src, linesize, on_device ? src : NULL,
+                          linesize) != VS_OK)
+      return -1;
+    total = append_records(&lms, rec, total, out_cap, counts ? counts + k : NULL);
+    k++;
+  }
+  if (k >= nframes) return total;
+  const uint8_t* mm = NULL;
+  const vsbd_result* cres = NULL;
+  {
+    int search = 0;
+    const uint8_t* src = frames + (size_t)k * frame_bytes;
+    if (vsb_frame_begin(md, &search) != VS_OK || !search) return -1;
+    if (vsbd_stage_a(st->dev, on_device ? NULL : src, linesize, on_device ? src : NULL, linesize,
+                     1, &mm, &cres) != 0) {
+      vs_log_error(md->conf.modName, "GPU stage A failed: %s\n", vsbd_error());
+      return -1;
+    }
+  }
+  for (; k < nframes; k++) {
+    int search = 0;
+    if (vsb_frame_begin(md, &search) != VS_OK || !search) return -1;
+    vsb_frame_work w;
+    vsb_frame_host_a(md, mm, cres, &w);
+    const int next = k + 1 < nframes;
+    const uint8_t* nsrc = frames + (size_t)(k + 1) * frame_bytes;
+    if (vsbd_stage_b_issue(st->dev, w.items, w.fine_pass ? w.nitems : 0) != 0 ||
+        (next && vsbd_stage_a_next_issue(st->dev, on_device ? NULL : nsrc, linesize,
+                                         on_device ? nsrc : NULL, linesize) != 0)) {
+      vs_log_error(md->conf.modName, "GPU stage failed: %s\n", vsbd_error());
+      vsb_frame_discard(&w);
+      return -1;
+    }
+    const vsbd_result* fres = NULL;
+    if (vsbd_stage_b_collect(st->dev, &fres) != 0) {
+      vs_log_error(md->conf.modName, "GPU stage B failed: %s\n", vsbd_error());
+      vsb_frame_discard(&w);
+      return -1;
+    }
+    LocalMotions lms;
+    vsb_frame_host_b(md, fres, &w, &lms);
+    if (vsb_frame_end(md)) vsbd_commit_prev(st->dev);
+    total = append_records(&lms, rec, total, out_cap, counts ? counts + k : NULL);
+    if (next && vsbd_stage_a_next_collect(st->dev, &mm, &cres) != 0) {
+      vs_log_error(md->conf.modName, "GPU stage A failed: %s\n", vsbd_error());
+      return -1;
+    }
+  }
+  return total;
 }
 
 int vsMotionDetection(VSMotionDetect* md, LocalMotions* motions, VSFrame* frame) {

@@ -69,6 +69,10 @@ int vsb_set_proposal(VSMotionDetect* md, const void* blob, long bytes) {
   return vsb_set_proposal_ex(md, blob, bytes, -1.0, NAN, -1.0);
 }
 
+int vsb_set_proposal_scope(VSMotionDetect* md, int fine_net) {
+  return vsbd_set_proposal_scope(vsb_md_device(md), fine_net) == 0 ? VS_OK : VS_ERROR;
+}
+
 int vsb_set_proposal_verify(VSMotionDetect* md, int on) {
   return vsbd_set_proposal_verify(vsb_md_device(md), on) == 0 ? VS_OK : VS_ERROR;
 }

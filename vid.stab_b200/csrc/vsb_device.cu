@@ -307,6 +307,19 @@ static int sm_count(void) {
   return n;
 }
 
+/* raises a kernel's dynamic shared-memory limit only when a launch needs
+   more than this device already allows it (the attribute call costs
+   microseconds of host time per launch otherwise); slot names the kernel */
+static cudaError_t ensure_smem(const void* fn, int slot, size_t smem) {
+  static size_t done[16][16];
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev >= 0 && dev < 16 && slot >= 0 && slot < 16 && done[dev][slot] >= smem) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess && dev >= 0 && dev < 16 && slot >= 0 && slot < 16) done[dev][slot] = smem;
+  return e;
+}
+
 /* largest dynamic shared memory one search CTA may request on this device
    (the kernels' static shared memory counts against the opt-in limit) */
 static size_t search_smem_limit(void) {
@@ -489,8 +502,7 @@ template <int TB>
 static int launch_lattice(const GeomDev& gd, const uint8_t* curr, const uint8_t* prev, int pitch,
                           const vsbd_item* d_items, int n, unsigned long long* keys,
                           unsigned* tickets, vsbd_result* d_res, cudaStream_t st) {
-  cudaError_t e = cudaFuncSetAttribute(k_lattice<TB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)gd.smem);
+  cudaError_t e = ensure_smem((const void*)k_lattice<TB>, TB == 2 ? 0 : (TB == 4 ? 1 : 2), gd.smem);
   if (e != cudaSuccess) {
     set_err("cudaFuncSetAttribute(k_lattice)", e);
     return -1;
@@ -521,10 +533,10 @@ static int launch_list_tb(const GeomDev& gd, const uint8_t* curr, const uint8_t*
                           const vsbd_item* d_items, int n, const int* count, const int* list,
                           unsigned long long* keys, unsigned* tickets, vsbd_result* d_res,
                           cudaStream_t st) {
-  cudaError_t e = cudaFuncSetAttribute(k_lattice_list<TB>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gd.smem);
-  int cps = 0;
-  if (e == cudaSuccess)
+  cudaError_t e = ensure_smem((const void*)k_lattice_list<TB>, TB == 2 ? 3 : (TB == 4 ? 4 : 5),
+                              gd.smem);
+  int cps = gd.list_cps;
+  if (e == cudaSuccess && cps <= 0)
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cps, k_lattice_list<TB>, gd.g.threads,
                                                       gd.smem);
   if (e != cudaSuccess) {
@@ -557,8 +569,8 @@ static int launch_list(const GeomDev& gd, const uint8_t* curr, const uint8_t* pr
 template <int TB>
 static int launch_emit_tb(const GeomDev& gd, const uint8_t* curr, const uint8_t* prev, int pitch,
                           const vsbd_item* d_items, int n, cudaStream_t st) {
-  cudaError_t e = cudaFuncSetAttribute(k_lattice<TB, true>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gd.smem);
+  cudaError_t e = ensure_smem((const void*)k_lattice<TB, true>, TB == 2 ? 6 : (TB == 4 ? 7 : 8),
+                              gd.smem);
   if (e != cudaSuccess) {
     set_err("cudaFuncSetAttribute(k_lattice emit)", e);
     return -1;
@@ -597,11 +609,11 @@ static int launch_pruned(const GeomDev& gd, const GeomDev& gp, const uint8_t* cu
   DGeom g = gd.g;
   g.skip = skip;
   const size_t fs = (size_t)g.S * g.S * g.bpp + 64;
-  cudaError_t e = cudaFuncSetAttribute(k_prune, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fs);
+  cudaError_t e = ensure_smem((const void*)k_prune, 9, fs);
   if (e != cudaSuccess) { set_err("cudaFuncSetAttribute(k_prune)", e); return -1; }
   k_prune<<<n, 256, fs, st>>>(curr, prev, pitch, g, d_items, part, 4, keys, counts, lists, boxes);
   const size_t ss = survive_smem(g);
-  e = cudaFuncSetAttribute(k_survive, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss);
+  e = ensure_smem((const void*)k_survive, 10, ss);
   if (e != cudaSuccess) { set_err("cudaFuncSetAttribute(k_survive)", e); return -1; }
   int chunks = 4 * sm_count() / n;
   if (chunks < 1) chunks = 1;
@@ -729,8 +741,13 @@ struct vsbd_ctx {
   cudaStream_t st;
   uint8_t* d_raw;     /* input plane (blurred formats) */
   uint8_t* d_tmp;     /* row-pass buffer of the wide-window blur */
-  uint8_t* d_buf[2];  /* blurred planes: current / previous */
-  int cur;
+  uint8_t* d_buf[3];  /* blurred planes: slots of the current frame, the
+                         previous one and the next one (filled ahead while
+                         the current frame's fine search runs) */
+  int cur, prv;       /* slots of the current and the previous frame */
+  cudaStream_t st2;   /* the fine stage */
+  cudaEvent_t ev_a, ev_b;
+  int a_search, b_n;  /* the pending stages' search flag / item count */
   double thr_coarse;  /* contrast threshold of the coarse fields */
   int16_t* d_xy;      /* coarse x | coarse y | fine x | fine y */
   GeomDev gc, gf;
@@ -755,10 +772,13 @@ struct vsbd_ctx {
   PNSearch pn;
   float pn_match_bound;         /* trusted refined SAD per field pixel */
   int pn_on, pn_verify;
+  int pn_fine_net;              /* fine fields: 1 network proposal, 0 the coarse model's
+                                   prediction (zero residual) */
   float* d_pout;                /* network outputs [nc + nf][3] */
   vsbd_result* d_vres;          /* verify: full-search results, coarse then fine */
   vsbd_result* h_vres;
   GeomDev gcf, gff;             /* full-search tilings for the few items that fall back */
+  int fb_last[2];               /* items that fell back in the previous frame: coarse, fine */
   int* d_fbl;                   /* fallback count, then the fallback item list */
   long long pn_stats[8];        /* searched, fell back, verified, identical; then
                                    coarse searched / fell back, fine searched / fell back */
@@ -775,12 +795,12 @@ struct vsbd_ctx {
 };
 
 /* per-kernel event pairs on the detector's stream; read after the sync */
-static void kt_begin(vsbd_ctx* c, int k) {
-  if (c->timing) cudaEventRecord(c->ev[k][0], c->st);
+static void kt_begin(vsbd_ctx* c, int k, cudaStream_t st) {
+  if (c->timing) cudaEventRecord(c->ev[k][0], st);
 }
-static void kt_end(vsbd_ctx* c, int k) {
+static void kt_end(vsbd_ctx* c, int k, cudaStream_t st) {
   if (c->timing) {
-    cudaEventRecord(c->ev[k][1], c->st);
+    cudaEventRecord(c->ev[k][1], st);
     c->kt_pending[k] = 1;
   }
 }
@@ -828,12 +848,17 @@ extern "C" void vsbd_destroy(vsbd_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->dev);
   if (c->st) cudaStreamSynchronize(c->st);
+  if (c->st2) cudaStreamSynchronize(c->st2);
   for (int k = 0; k < VSBD_NKT; k++)
     if (c->ev[k][0]) { cudaEventDestroy(c->ev[k][0]); cudaEventDestroy(c->ev[k][1]); }
   cudaFree(c->d_raw);
   cudaFree(c->d_tmp);
   cudaFree(c->d_buf[0]);
   cudaFree(c->d_buf[1]);
+  cudaFree(c->d_buf[2]);
+  if (c->ev_a) cudaEventDestroy(c->ev_a);
+  if (c->ev_b) cudaEventDestroy(c->ev_b);
+  if (c->st2) cudaStreamDestroy(c->st2);
   cudaFree(c->d_xy);
   cudaFree(c->d_citems);
   cudaFree(c->d_fitems);
@@ -898,10 +923,15 @@ extern "C" int vsbd_create(vsbd_ctx** out, int W, int H, int bpp, int blur_size,
   CKC(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
   if (blur_size >= 2) CKC(cudaMalloc(&c->d_raw, plane));
   if (blur_size >= 2 && blur_size / 2 > BT_MAXHALF) CKC(cudaMalloc(&c->d_tmp, plane));
-  CKC(cudaMalloc(&c->d_buf[0], plane));
-  CKC(cudaMalloc(&c->d_buf[1], plane));
-  CKC(cudaMemset(c->d_buf[0], 0, plane));
-  CKC(cudaMemset(c->d_buf[1], 0, plane));
+  for (int k = 0; k < 3; k++) {
+    CKC(cudaMalloc(&c->d_buf[k], plane));
+    CKC(cudaMemset(c->d_buf[k], 0, plane));
+  }
+  c->cur = 0;
+  c->prv = 1;
+  CKC(cudaStreamCreateWithFlags(&c->st2, cudaStreamNonBlocking));
+  CKC(cudaEventCreateWithFlags(&c->ev_a, cudaEventDisableTiming));
+  CKC(cudaEventCreateWithFlags(&c->ev_b, cudaEventDisableTiming));
   CKC(cudaMalloc(&c->d_xy, sizeof(int16_t) * 2 * (nc + nf) + 16));
   CKC(cudaMemcpy(c->d_xy, cx, sizeof(int16_t) * nc, cudaMemcpyHostToDevice));
   CKC(cudaMemcpy(c->d_xy + nc, cy, sizeof(int16_t) * nc, cudaMemcpyHostToDevice));
@@ -987,38 +1017,41 @@ extern "C" int vsbd_create(vsbd_ctx** out, int W, int H, int bpp, int blur_size,
 
 /* The proposal path of one field set: network, narrowed search, full
    search of the items that fell back (and, when verifying, the full search
-   of every item into d_vres + base). */
-static int learned_search(vsbd_ctx* c, const GeomDev& gd, const GeomDev& gfull,
-                          const vsbd_item* items, int n, int base,
+   of every item into d_vres + base).  fbl: this field set's fallback count
+   and list. */
+static int learned_search(vsbd_ctx* c, const GeomDev& gd, const GeomDev& gfull, uint8_t* cur,
+                          uint8_t* prv, cudaStream_t st, const vsbd_item* items, int n, int base,
                           const uint8_t* skip, unsigned long long* keys, unsigned* tickets,
-                          vsbd_result* res, uint8_t* fb) {
+                          vsbd_result* res, uint8_t* fb, int* fbl) {
   if (n <= 0) return 0;
-  uint8_t* cur = c->d_buf[c->cur];
-  uint8_t* prv = c->d_buf[c->cur ^ 1];
-  float* pout = c->d_pout + (size_t)3 * base;
-  kt_begin(c, VSBD_KT_PNET);
-  if (vsbpn_infer(c->d_pn, cur, prv, c->pitch, c->W, c->H, items, NULL, n, pout, c->st) < 0) return -1;
-  kt_end(c, VSBD_KT_PNET);
+  float* pout = NULL;
+  if (base == 0 || c->pn_fine_net) {
+    pout = c->d_pout + (size_t)3 * base;
+    kt_begin(c, VSBD_KT_PNET, st);
+    if (vsbpn_infer(c->d_pn, cur, prv, c->pitch, c->W, c->H, items, NULL, n, pout, st) < 0)
+      return -1;
+    kt_end(c, VSBD_KT_PNET, st);
+    c->launches++;
+    count_launches(1);
+  }
   const int kt = base == 0 ? VSBD_KT_COARSE : VSBD_KT_FINE;
-  kt_begin(c, kt);
+  kt_begin(c, kt, st);
   /* the SAD bound scales with the field's pixel count */
   PNSearch ps = c->pn;
   const double bound = (double)c->pn_match_bound * gd.g.S * gd.g.S;
   ps.sad_bound = bound >= 4294967295.0 ? 0xffffffffu : (unsigned)bound;
-  CK(cudaMemsetAsync(c->d_fbl, 0, sizeof(int), c->st));
-  if (vsbpn_narrow(gd.g, cur, prv, c->pitch, items, n, pout, ps, skip, res, fb, c->d_fbl,
-                   c->d_fbl + 1, c->st) < 0)
+  CK(cudaMemsetAsync(fbl, 0, sizeof(int), st));
+  if (vsbpn_narrow(gd.g, cur, prv, c->pitch, items, n, pout, ps, skip, res, fb, fbl, fbl + 1, st) < 0)
     return -1;
-  kt_end(c, kt);
-  kt_begin(c, VSBD_KT_FALLBACK);
-  int nl = launch_list(gfull, cur, prv, c->pitch, items, n, c->d_fbl, c->d_fbl + 1, keys, tickets,
-                       res, c->st);
+  kt_end(c, kt, st);
+  kt_begin(c, VSBD_KT_FALLBACK, st);
+  int nl = launch_list(gfull, cur, prv, c->pitch, items, n, fbl, fbl + 1, keys, tickets, res, st);
   if (nl < 0) return -1;
-  kt_end(c, VSBD_KT_FALLBACK);
-  c->launches += 2 + nl;
-  count_launches(2 + nl);
+  kt_end(c, VSBD_KT_FALLBACK, st);
+  c->launches += 1 + nl;
+  count_launches(1 + nl);
   if (c->pn_verify) {
-    int nv = launch_search(gd, cur, prv, c->pitch, items, n, keys, tickets, c->d_vres + base, c->st);
+    int nv = launch_search(gd, cur, prv, c->pitch, items, n, keys, tickets, c->d_vres + base, st);
     if (nv < 0) return -1;
     c->launches += nv;
     count_launches(nv);
@@ -1029,7 +1062,9 @@ static int learned_search(vsbd_ctx* c, const GeomDev& gd, const GeomDev& gfull,
 /* counts of one stage after its results reached the host */
 static void proposal_tally(vsbd_ctx* c, const uint8_t* fb, const vsbd_result* res,
                            const vsbd_result* vres, int n, int kind) {
+  c->fb_last[kind] = 0;
   for (int i = 0; i < n; i++) {
+    if (fb[i] == PN_FB_FULL) c->fb_last[kind]++;
     if (fb[i] == PN_FB_UNUSED) continue;
     c->pn_stats[0]++;
     c->pn_stats[4 + 2 * kind]++;
@@ -1047,14 +1082,13 @@ static void proposal_tally(vsbd_ctx* c, const uint8_t* fb, const vsbd_result* re
 }
 
 /* appends the network inputs and full-search labels of n items to the log */
-static int log_items(vsbd_ctx* c, const vsbd_item* items, int n, int kind, const vsbd_result* res,
+static int log_items(vsbd_ctx* c, uint8_t* cur, uint8_t* prv, cudaStream_t st,
+                     const vsbd_item* items, int n, int kind, const vsbd_result* res,
                      const uint8_t* skip) {
   if (n <= 0 || c->log_n + n > c->log_cap) return 0;
-  uint8_t* cur = c->d_buf[c->cur];
-  uint8_t* prv = c->d_buf[c->cur ^ 1];
   if (vsbpn_crops(cur, prv, c->pitch, c->W, c->H, items, n, c->log_in + (size_t)c->log_n * 4096,
-                  c->st) < 0 ||
-      vsbpn_labels(res, skip, n, kind, c->log_lab + c->log_n, c->st) < 0)
+                  st) < 0 ||
+      vsbpn_labels(res, skip, n, kind, c->log_lab + c->log_n, st) < 0)
     return -1;
   c->launches += 2;
   count_launches(2);
@@ -1062,32 +1096,35 @@ static int log_items(vsbd_ctx* c, const vsbd_item* items, int n, int kind, const
   return 0;
 }
 
-extern "C" int vsbd_stage_a(vsbd_ctx* c, const uint8_t* host, int linesize, const uint8_t* dev,
-                            int pitch, int search, const uint8_t** minmax,
-                            const vsbd_result** coarse) {
-  CK(cudaSetDevice(c->dev));
+/* Stage A of a frame whose blurred plane goes to slot ci and whose search
+   runs against slot pi, enqueued on the detector's first stream, ending with
+   the results' copy to the host and the stage-A event. */
+static int stage_a_issue(vsbd_ctx* c, const uint8_t* host, int linesize, const uint8_t* dev,
+                         int pitch, int search, int ci, int pi) {
   const int rowbytes = c->W * c->bpp;
-  uint8_t* cur = c->d_buf[c->cur];
-  uint8_t* prv = c->d_buf[c->cur ^ 1];
+  cudaStream_t st = c->st;
+  uint8_t* cur = c->d_buf[ci];
+  uint8_t* prv = c->d_buf[pi];
+  c->a_search = search;
   if (c->blur >= 2) {
     const uint8_t* src = dev;
     int sp = pitch;
     if (!dev) {
       CK(cudaMemcpy2DAsync(c->d_raw, c->pitch, host, linesize, rowbytes, c->H,
-                           cudaMemcpyHostToDevice, c->st));
+                           cudaMemcpyHostToDevice, st));
       count_h2d((size_t)rowbytes * c->H);
       src = c->d_raw;
       sp = c->pitch;
     }
-    kt_begin(c, VSBD_KT_BLUR);
-    { int nb = launch_blur(src, sp, cur, c->pitch, c->W, c->H, c->blur, c->d_tmp, c->pitch, c->st); c->launches += nb; count_launches(nb); }
-    kt_end(c, VSBD_KT_BLUR);
+    kt_begin(c, VSBD_KT_BLUR, st);
+    { int nb = launch_blur(src, sp, cur, c->pitch, c->W, c->H, c->blur, c->d_tmp, c->pitch, st); c->launches += nb; count_launches(nb); }
+    kt_end(c, VSBD_KT_BLUR, st);
     CK(cudaGetLastError());
   } else {
     if (dev)
-      CK(cudaMemcpy2DAsync(cur, c->pitch, dev, pitch, rowbytes, c->H, cudaMemcpyDeviceToDevice, c->st));
+      CK(cudaMemcpy2DAsync(cur, c->pitch, dev, pitch, rowbytes, c->H, cudaMemcpyDeviceToDevice, st));
     else {
-      CK(cudaMemcpy2DAsync(cur, c->pitch, host, linesize, rowbytes, c->H, cudaMemcpyHostToDevice, c->st));
+      CK(cudaMemcpy2DAsync(cur, c->pitch, host, linesize, rowbytes, c->H, cudaMemcpyHostToDevice, st));
       count_h2d((size_t)rowbytes * c->H);
     }
   }
@@ -1097,53 +1134,59 @@ extern "C" int vsbd_stage_a(vsbd_ctx* c, const uint8_t* host, int linesize, cons
        the training log's unused fields */
     uint8_t* skip = (c->mode || c->pn_on || c->log_in) ? c->d_skip : NULL;
     vsbd_result* cres = (vsbd_result*)(c->d_out + c->off_coarse);
-    kt_begin(c, VSBD_KT_MINMAX);
+    kt_begin(c, VSBD_KT_MINMAX, st);
     if (c->bpp == 1 && c->nch == 1) {
-      k_minmax_planar<<<c->nc + c->nf, 256, 0, c->st>>>(cur, c->pitch, c->d_xy, c->nc, c->nf, S,
-                                                        c->gf.g.S, c->d_out, c->thr_coarse, skip);
+      k_minmax_planar<<<c->nc + c->nf, 256, 0, st>>>(cur, c->pitch, c->d_xy, c->nc, c->nf, S,
+                                                     c->gf.g.S, c->d_out, c->thr_coarse, skip);
       c->launches++;
       count_launches(1);
     } else {
-    k_minmax<<<c->nc, 256, 0, c->st>>>(cur, c->pitch, c->d_xy, c->d_xy + c->nc, S, c->bpp, c->nch,
-                                       c->d_out, c->thr_coarse, skip);
-    c->launches++;
-    count_launches(1);
-    }
-    if (c->nf > 0 && !(c->bpp == 1 && c->nch == 1)) {
-      k_minmax<<<c->nf, 256, 0, c->st>>>(cur, c->pitch, c->d_xy + 2 * c->nc, c->d_xy + 2 * c->nc + c->nf,
-                                         c->gf.g.S, c->bpp, c->nch, c->d_out + (size_t)c->nc * c->nch * 2,
-                                         0.0, NULL);
+      k_minmax<<<c->nc, 256, 0, st>>>(cur, c->pitch, c->d_xy, c->d_xy + c->nc, S, c->bpp, c->nch,
+                                      c->d_out, c->thr_coarse, skip);
       c->launches++;
       count_launches(1);
+      if (c->nf > 0) {
+        k_minmax<<<c->nf, 256, 0, st>>>(cur, c->pitch, c->d_xy + 2 * c->nc,
+                                        c->d_xy + 2 * c->nc + c->nf, c->gf.g.S, c->bpp, c->nch,
+                                        c->d_out + (size_t)c->nc * c->nch * 2, 0.0, NULL);
+        c->launches++;
+        count_launches(1);
+      }
     }
-    kt_end(c, VSBD_KT_MINMAX);
+    kt_end(c, VSBD_KT_MINMAX, st);
     if (c->pn_on) {
-      if (learned_search(c, c->gc, c->gcf, c->d_citems, c->nc, 0, skip, c->d_keys, c->d_tickets, cres,
-                         c->d_out + c->off_cfb) != 0)
+      if (learned_search(c, c->gc, c->fb_last[0] >= 8 ? c->gc : c->gcf, cur, prv, st, c->d_citems,
+                         c->nc, 0, skip, c->d_keys, c->d_tickets, cres, c->d_out + c->off_cfb,
+                         c->d_fbl) != 0)
         return -1;
     } else {
-      kt_begin(c, VSBD_KT_COARSE);
+      kt_begin(c, VSBD_KT_COARSE, st);
       int nl = c->mode ? launch_pruned(c->gc, c->gcp, cur, prv, c->pitch, c->d_citems, c->nc,
                                        c->d_skip, c->d_part, c->d_counts, c->d_lists, c->d_boxes,
-                                       c->d_keys, c->d_tickets, cres, c->st)
+                                       c->d_keys, c->d_tickets, cres, st)
                        : launch_search(c->gc, cur, prv, c->pitch, c->d_citems, c->nc, c->d_keys,
-                                       c->d_tickets, cres, c->st);
+                                       c->d_tickets, cres, st);
       if (nl < 0) return -1;
       c->launches += nl;
       count_launches(nl);
-      kt_end(c, VSBD_KT_COARSE);
-      if (c->log_in && log_items(c, c->d_citems, c->nc, 0, cres, skip) != 0) return -1;
+      kt_end(c, VSBD_KT_COARSE, st);
+      if (c->log_in && log_items(c, cur, prv, st, c->d_citems, c->nc, 0, cres, skip) != 0) return -1;
     }
     CK(cudaGetLastError());
-    CK(cudaMemcpyAsync(c->h_out, c->d_out, c->off_fine, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(c->h_out, c->d_out, c->off_fine, cudaMemcpyDeviceToHost, st));
     count_d2h(c->off_fine);
     if (c->pn_on && c->pn_verify)
       CK(cudaMemcpyAsync(c->h_vres, c->d_vres, sizeof(vsbd_result) * c->nc, cudaMemcpyDeviceToHost,
-                         c->st));
+                         st));
   }
-  CK(cudaStreamSynchronize(c->st));
+  CK(cudaEventRecord(c->ev_a, st));
+  return 0;
+}
+
+static int stage_a_collect(vsbd_ctx* c, const uint8_t** minmax, const vsbd_result** coarse) {
+  CK(cudaEventSynchronize(c->ev_a));
   kt_collect(c);
-  if (search && c->pn_on)
+  if (c->a_search && c->pn_on)
     proposal_tally(c, c->h_out + c->off_cfb, (const vsbd_result*)(c->h_out + c->off_coarse),
                    c->h_vres, c->nc, 0);
   if (minmax) *minmax = c->h_out;
@@ -1151,53 +1194,103 @@ extern "C" int vsbd_stage_a(vsbd_ctx* c, const uint8_t* host, int linesize, cons
   return 0;
 }
 
-extern "C" int vsbd_stage_b(vsbd_ctx* c, const vsbd_item* items, int n, const vsbd_result** fine) {
+extern "C" int vsbd_stage_a(vsbd_ctx* c, const uint8_t* host, int linesize, const uint8_t* dev,
+                            int pitch, int search, const uint8_t** minmax,
+                            const vsbd_result** coarse) {
+  CK(cudaSetDevice(c->dev));
+  if (stage_a_issue(c, host, linesize, dev, pitch, search, c->cur, c->prv) != 0) return -1;
+  return stage_a_collect(c, minmax, coarse);
+}
+
+extern "C" int vsbd_stage_a_next_issue(vsbd_ctx* c, const uint8_t* host, int linesize,
+                                       const uint8_t* dev, int pitch) {
+  CK(cudaSetDevice(c->dev));
+  /* the next frame: blurred into the slot neither this frame nor its
+     previous one uses, searched against this frame's plane */
+  return stage_a_issue(c, host, linesize, dev, pitch, 1, 3 - c->cur - c->prv, c->cur);
+}
+
+extern "C" int vsbd_stage_a_next_collect(vsbd_ctx* c, const uint8_t** minmax,
+                                         const vsbd_result** coarse) {
+  CK(cudaSetDevice(c->dev));
+  return stage_a_collect(c, minmax, coarse);
+}
+
+extern "C" int vsbd_stage_b_issue(vsbd_ctx* c, const vsbd_item* items, int n) {
   CK(cudaSetDevice(c->dev));
   if (n > c->nf) { set_msg("more fine items than fine fields"); return -1; }
-  *fine = (const vsbd_result*)(c->h_out + c->off_fine);
+  c->b_n = n;
   if (n <= 0) return 0;
+  cudaStream_t st = c->st2;
   memcpy(c->h_items, items, sizeof(vsbd_item) * n);
-  CK(cudaMemcpyAsync(c->d_fitems, c->h_items, sizeof(vsbd_item) * n, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(c->d_fitems, c->h_items, sizeof(vsbd_item) * n, cudaMemcpyHostToDevice, st));
   count_h2d(sizeof(vsbd_item) * n);
   uint8_t* cur = c->d_buf[c->cur];
-  uint8_t* prv = c->d_buf[c->cur ^ 1];
+  uint8_t* prv = c->d_buf[c->prv];
   vsbd_result* fres = (vsbd_result*)(c->d_out + c->off_fine);
   size_t d2h = sizeof(vsbd_result) * n;
   if (c->pn_on) {
-    if (learned_search(c, c->gf, c->gff, c->d_fitems, n, c->nc, NULL, c->d_keys + c->nc,
-                       c->d_tickets + c->nc, fres, c->d_out + c->off_ffb) != 0)
+    if (learned_search(c, c->gf, c->fb_last[1] >= 8 ? c->gf : c->gff, cur, prv, st, c->d_fitems,
+                       n, c->nc, NULL, c->d_keys + c->nc, c->d_tickets + c->nc, fres,
+                       c->d_out + c->off_ffb, c->d_fbl + c->nc + 2) != 0)
       return -1;
     d2h = c->off_ffb - c->off_fine + n;
   } else {
-    kt_begin(c, VSBD_KT_FINE);
+    kt_begin(c, VSBD_KT_FINE, st);
     int nl = c->mode ? launch_pruned(c->gf, c->gfp, cur, prv, c->pitch, c->d_fitems, n, NULL,
                                      c->d_part, c->d_counts + c->nc, c->d_lists,
                                      c->d_boxes + 4 * c->nc, c->d_keys + c->nc,
-                                     c->d_tickets + c->nc, fres, c->st)
+                                     c->d_tickets + c->nc, fres, st)
                      : launch_search(c->gf, cur, prv, c->pitch, c->d_fitems, n, c->d_keys + c->nc,
-                                     c->d_tickets + c->nc, fres, c->st);
+                                     c->d_tickets + c->nc, fres, st);
     if (nl < 0) return -1;
     c->launches += nl;
     count_launches(nl);
-    kt_end(c, VSBD_KT_FINE);
-    if (c->log_in && log_items(c, c->d_fitems, n, 1, fres, NULL) != 0) return -1;
+    kt_end(c, VSBD_KT_FINE, st);
+    if (c->log_in && log_items(c, cur, prv, st, c->d_fitems, n, 1, fres, NULL) != 0) return -1;
   }
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(c->h_out + c->off_fine, c->d_out + c->off_fine, d2h, cudaMemcpyDeviceToHost,
-                     c->st));
+                     st));
   count_d2h(d2h);
   if (c->pn_on && c->pn_verify)
     CK(cudaMemcpyAsync(c->h_vres + c->nc, c->d_vres + c->nc, sizeof(vsbd_result) * n,
-                       cudaMemcpyDeviceToHost, c->st));
-  CK(cudaStreamSynchronize(c->st));
-  kt_collect(c);
-  if (c->pn_on)
-    proposal_tally(c, c->h_out + c->off_ffb, (const vsbd_result*)(c->h_out + c->off_fine),
-                   c->h_vres ? c->h_vres + c->nc : NULL, n, 1);
+                       cudaMemcpyDeviceToHost, st));
+  CK(cudaEventRecord(c->ev_b, st));
   return 0;
 }
 
-extern "C" void vsbd_commit_prev(vsbd_ctx* c) { c->cur ^= 1; }
+extern "C" int vsbd_stage_b_collect(vsbd_ctx* c, const vsbd_result** fine) {
+  CK(cudaSetDevice(c->dev));
+  *fine = (const vsbd_result*)(c->h_out + c->off_fine);
+  if (c->b_n <= 0) return 0;
+  CK(cudaEventSynchronize(c->ev_b));
+  kt_collect(c);
+  if (c->pn_on)
+    proposal_tally(c, c->h_out + c->off_ffb, (const vsbd_result*)(c->h_out + c->off_fine),
+                   c->h_vres ? c->h_vres + c->nc : NULL, c->b_n, 1);
+  return 0;
+}
+
+extern "C" int vsbd_stage_b(vsbd_ctx* c, const vsbd_item* items, int n, const vsbd_result** fine) {
+  if (vsbd_stage_b_issue(c, items, n) != 0) return -1;
+  return vsbd_stage_b_collect(c, fine);
+}
+
+/* the current plane becomes the previous one; the third slot takes the next
+   frame */
+extern "C" void vsbd_commit_prev(vsbd_ctx* c) {
+  const int f = 3 - c->cur - c->prv;
+  c->prv = c->cur;
+  c->cur = f;
+}
+
+/* whether stage A of the next frame may overlap stage B of this one: the
+   two stages then share no scratch (the pruned search's partial sums and
+   the training log are shared, and per-kernel timing needs one stream) */
+extern "C" int vsbd_can_overlap(const vsbd_ctx* c) {
+  return c && c->mode == 0 && !c->log_in && !c->timing;
+}
 
 extern "C" long vsbd_launches(const vsbd_ctx* c) { return c ? c->launches : 0; }
 
@@ -1208,6 +1301,7 @@ extern "C" int vsbd_set_proposal(vsbd_ctx* c, const void* params, float scale, f
   if (!c) return -1;
   CK(cudaSetDevice(c->dev));
   CK(cudaStreamSynchronize(c->st));
+  CK(cudaStreamSynchronize(c->st2));
   if (!params) {
     c->pn_on = 0;
     return 0;
@@ -1222,7 +1316,7 @@ extern "C" int vsbd_set_proposal(vsbd_ctx* c, const void* params, float scale, f
   }
   if (!c->d_pn) CK(cudaMalloc(&c->d_pn, PN_PARAM_BYTES));
   if (!c->d_pout) CK(cudaMalloc(&c->d_pout, sizeof(float) * 3 * (c->nc + c->nf + 1)));
-  if (!c->d_fbl) CK(cudaMalloc(&c->d_fbl, sizeof(int) * (c->nc + c->nf + 2)));
+  if (!c->d_fbl) CK(cudaMalloc(&c->d_fbl, sizeof(int) * (c->nc + c->nf + 4)));
   CK(cudaMemcpy(c->d_pn, params, PN_PARAM_BYTES, cudaMemcpyHostToDevice));
   /* the full search of the items that fall back: a tiling for a handful of
      items, so that one item's lattice is spread over many CTAs (the
@@ -1240,6 +1334,28 @@ extern "C" int vsbd_set_proposal(vsbd_ctx* c, const void* params, float scale, f
       c->gff.g = tc[0].g;
       c->gff.smem = tile_layout(tc[0].g).total;
     }
+    GeomDev* gs[4] = { &c->gc, &c->gf, &c->gcf, &c->gff };
+    for (int k = 0; k < 4; k++) {
+      GeomDev* g = gs[k];
+      int cps = 0;
+      cudaError_t e = cudaSuccess;
+      switch (g->g.tb) {
+        case 2: e = ensure_smem((const void*)k_lattice_list<2>, 3, g->smem);
+          if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cps, k_lattice_list<2>, g->g.threads, g->smem);
+          break;
+        case 4: e = ensure_smem((const void*)k_lattice_list<4>, 4, g->smem);
+          if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cps, k_lattice_list<4>, g->g.threads, g->smem);
+          break;
+        case 8: e = ensure_smem((const void*)k_lattice_list<8>, 5, g->smem);
+          if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cps, k_lattice_list<8>, g->g.threads, g->smem);
+          break;
+      }
+      if (e != cudaSuccess) {
+        set_err("fallback search set-up", e);
+        return -1;
+      }
+      g->list_cps = cps;
+    }
   }
   c->pn.scale = scale;
   c->pn.radius = radius;
@@ -1247,6 +1363,12 @@ extern "C" int vsbd_set_proposal(vsbd_ctx* c, const void* params, float scale, f
   c->pn.sad_bound = 0xffffffffu;
   c->pn_match_bound = match_bound;
   c->pn_on = 1;
+  return 0;
+}
+
+extern "C" int vsbd_set_proposal_scope(vsbd_ctx* c, int fine_net) {
+  if (!c) return -1;
+  c->pn_fine_net = fine_net ? 1 : 0;
   return 0;
 }
 

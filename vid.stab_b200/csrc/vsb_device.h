@@ -82,6 +82,19 @@ int vsbd_stage_b(vsbd_ctx* c, const vsbd_item* items, int n, const vsbd_result**
 /* The current buffer becomes the previous one. */
 void vsbd_commit_prev(vsbd_ctx* c);
 
+/* Overlapped frames (a frame loop that knows the next frame): while the
+   current frame's fine search runs (vsbd_stage_b_issue ... _collect, on a
+   second stream), stage A of the next frame is enqueued
+   (vsbd_stage_a_next_issue: its plane goes to the third buffer and is
+   searched against the current frame's) and collected after the commit
+   (vsbd_stage_a_next_collect).  Only when vsbd_can_overlap(c). */
+int vsbd_can_overlap(const vsbd_ctx* c);
+int vsbd_stage_a_next_issue(vsbd_ctx* c, const uint8_t* host, int linesize, const uint8_t* dev,
+                            int pitch);
+int vsbd_stage_a_next_collect(vsbd_ctx* c, const uint8_t** minmax, const vsbd_result** coarse);
+int vsbd_stage_b_issue(vsbd_ctx* c, const vsbd_item* items, int n);
+int vsbd_stage_b_collect(vsbd_ctx* c, const vsbd_result** fine);
+
 /* Kernel launches issued on behalf of this detector so far. */
 long vsbd_launches(const vsbd_ctx* c);
 
@@ -106,6 +119,9 @@ long vsbd_launches(const vsbd_ctx* c);
 int vsbd_set_proposal(vsbd_ctx* c, const void* params, float scale, float radius, float conf_min,
                       float match_bound);
 long vsbd_pnet_param_bytes(void);
+/* fine fields take the network's proposal (fine_net 1) or the coarse
+   model's prediction, i.e. zero residual (0, the default) */
+int vsbd_set_proposal_scope(vsbd_ctx* c, int fine_net);
 /* with verify on, every stage also runs the full search and compares */
 int vsbd_set_proposal_verify(vsbd_ctx* c, int on);
 /* [0] items searched with a proposal, [1] of them fell back, [2] items

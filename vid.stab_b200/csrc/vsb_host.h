@@ -73,6 +73,13 @@ void vsb_frame_discard(vsb_frame_work* w);
 void vsb_frame_first(VSMotionDetect* md, LocalMotions* motions);
 int vsb_frame_end(VSMotionDetect* md);
 
+/* whether vsb_detect_run_overlapped may serve this detector (no tripod,
+   no overlay, a device configuration whose stages share no scratch) */
+int vsb_can_overlap(const VSMotionDetect* md);
+long vsb_detect_run_overlapped(VSMotionDetect* md, const uint8_t* frames, long frame_bytes,
+                               int linesize, int nframes, int on_device, LocalMotion* rec,
+                               long out_cap, int* counts);
+
 /* device context of an initialised detector (NULL if none) */
 vsbd_ctx* vsb_md_device(const VSMotionDetect* md);
 

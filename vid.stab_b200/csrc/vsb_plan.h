@@ -18,6 +18,7 @@ struct GeomDev {
   int32_t* d_order;
   short2* d_point;
   size_t smem;
+  int list_cps; /* CTAs per SM of the list-driven search with this tiling (0: not known) */
 };
 
 /* a tiling with its modelled cost */

@@ -604,6 +604,8 @@ struct NarrowLayout {
   size_t off_win, off_q, total;
 };
 
+#define PN_NARROW_QMAX 64 /* candidate sums of one round (lattice window or refinement grid) */
+
 __host__ __device__ inline NarrowLayout narrow_layout(const DGeom& g, float radius) {
   NarrowLayout L;
   const int rowB = g.S * g.bpp;
@@ -616,8 +618,79 @@ __host__ __device__ inline NarrowLayout narrow_layout(const DGeom& g, float radi
   L.WH = g.S + (span - 1) * g.step + 2 * L.R;
   L.off_win = (size_t)L.fieldB + 16;
   L.off_q = L.off_win + (size_t)L.WH * L.WP + 16;
-  L.total = L.off_q + (size_t)g.maxq * 4 + 16;
+  const int q = g.maxq > PN_NARROW_QMAX ? g.maxq : PN_NARROW_QMAX;
+  L.total = L.off_q + (size_t)q * 4 + 16;
   return L;
+}
+
+/* One warp's share of a column of candidates: displacements (dx, dy0 +
+   k*hy), k < nk (<= 8), relative to the staged window's origin, summed over
+   field rows [r0, r1).  A lane owns one word of the field row (several rows
+   at once when a row has fewer than 32 words), loads the field word once per
+   row and applies it to every candidate of the column; partial sums are
+   added to sums[k] in shared memory. */
+__device__ __forceinline__ void sad_column(const uint32_t* __restrict__ C, int rowW,
+                                           const uint8_t* __restrict__ win, int WP, int e, int bpp,
+                                           int dx, int dy0, int hy, int nk, int r0, int r1,
+                                           int lane, unsigned* sums) {
+  unsigned acc[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) acc[k] = 0;
+  const int bx = e + dx * bpp;
+  const int sh = (bx & 3) << 3;
+  const int WPw = WP >> 2;
+  const int G = rowW < 32 ? 32 / rowW : 1;
+  const int g = rowW < 32 ? lane / rowW : 0;
+  const int w0 = rowW < 32 ? lane - g * rowW : lane;
+  const int wstep = rowW < 32 ? 32 : 32;
+  if (g < G) {
+    for (int w = w0; w < rowW; w += wstep) {
+      const uint32_t* Cw = C + w;
+      const uint32_t* Pw = (const uint32_t*)win + (bx >> 2) + w;
+      for (int r = r0 + g; r < r1; r += G) {
+        const uint32_t c = Cw[r * rowW];
+        const uint32_t* P = Pw + (r + dy0) * WPw;
+#pragma unroll
+        for (int k = 0; k < 8; k++)
+          if (k < nk) {
+            const uint32_t* Q = P + k * hy * WPw;
+            acc[k] = sad4(c, __funnelshift_r(Q[0], Q[1], sh), acc[k]);
+          }
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 8; k++)
+    if (k < nk) {
+      const unsigned v = __reduce_add_sync(0xffffffffu, acc[k]);
+      if (lane == 0) atomicAdd(&sums[k], v);
+    }
+}
+
+/* The SADs of a grid of candidates: columns i < ncol at dx0 + i*hx, rows
+   k < nrow at dy0 + k*hy (window coordinates), into sums[i*nrow + k].  The
+   warps take (column, row chunk of <= 8, field-row strip) tasks. */
+__device__ __forceinline__ void sad_grid(const uint32_t* C, int rowW, int S, const uint8_t* win,
+                                         int WP, int e, int bpp, int dx0, int hx, int ncol,
+                                         int dy0, int hy, int nrow, unsigned* sums) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  for (int q = threadIdx.x; q < ncol * nrow; q += blockDim.x) sums[q] = 0;
+  __syncthreads();
+  const int nch = (nrow + 7) >> 3;
+  const int units = ncol * nch;
+  int strips = nwarps / units;
+  if (strips < 1) strips = 1;
+  const int rs = (S + strips - 1) / strips;
+  for (int t = warp; t < units * strips; t += nwarps) {
+    const int u = t % units, sidx = t / units;
+    const int col = u / nch, ch = u - col * nch;
+    const int k0 = ch * 8, nk = min(8, nrow - k0);
+    const int r0 = sidx * rs, r1 = min(S, r0 + rs);
+    if (r0 < r1)
+      sad_column(C, rowW, win, WP, e, bpp, dx0 + col * hx, dy0 + k0 * hy, hy, nk, r0, r1, lane,
+                 sums + col * nrow + k0);
+  }
+  __syncthreads();
 }
 
 /* One CTA per item.  The lattice points that bracket the prediction +-
@@ -630,7 +703,7 @@ __host__ __device__ inline NarrowLayout narrow_layout(const DGeom& g, float radi
    falls back to the full search (appended to fb_list) when the confidence
    is below the threshold, the winner lies on the ring (the minimum may lie
    further out), or the refined SAD exceeds the bound. */
-static __global__ void __launch_bounds__(256) k_pn_narrow(const uint8_t* __restrict__ curr,
+static __global__ void __launch_bounds__(512) k_pn_narrow(const uint8_t* __restrict__ curr,
                                                           const uint8_t* __restrict__ prev,
                                                           int pitch, DGeom g,
                                                           const vsbd_item* __restrict__ items,
@@ -642,26 +715,13 @@ static __global__ void __launch_bounds__(256) k_pn_narrow(const uint8_t* __restr
                                                           int* __restrict__ fb_count,
                                                           int* __restrict__ fb_list) {
   extern __shared__ __align__(16) uint8_t sm[];
-  __shared__ unsigned long long red[8];
   __shared__ int s_tx, s_ty;
   __shared__ unsigned s_min;
   const int item = blockIdx.x;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const NarrowLayout L = narrow_layout(g, ps.radius);
-  if (skip && skip[item]) {
-    if (threadIdx.x == 0) {
-      vsbd_result o;
-      o.sad = 0xffffffffu;
-      o.tx = o.ty = 0;
-      o.ok = 0;
-      res[item] = o;
-      fb[item] = PN_FB_UNUSED;
-    }
-    return;
-  }
-  const vsbd_item it = items[item];
-  const float px = pout[item * 3] * ps.scale, py = pout[item * 3 + 1] * ps.scale;
-  const float cf = pout[item * 3 + 2];
+  const float* po = pout ? pout + item * 3 : NULL;
+  const float px = po ? po[0] * ps.scale : 0.f, py = po ? po[1] * ps.scale : 0.f;
+  const float cf = po ? po[2] : 3.0e38f;
   /* the bracket [lo, hi] of lattice indices covering prediction +- radius */
   int alo = 1, ahi = 0, blo = 1, bhi = 0;
   if (isfinite(px) && isfinite(py) && fabsf(px) < 30000.f && fabsf(py) < 30000.f) {
@@ -670,35 +730,26 @@ static __global__ void __launch_bounds__(256) k_pn_narrow(const uint8_t* __restr
     blo = max((int)floorf((py - ps.radius - g.by0) / g.step), 0);
     bhi = min((int)ceilf((py + ps.radius - g.by0) / g.step), g.nb - 1);
   }
-  if (alo > ahi || blo > bhi) { /* prediction outside the lattice */
-    if (threadIdx.x == 0) {
-      vsbd_result o;
-      o.sad = 0xffffffffu;
-      o.tx = o.ty = 0;
-      o.ok = 0;
-      res[item] = o;
-      fb[item] = PN_FB_FULL;
-      fb_list[atomicAdd(fb_count, 1)] = item;
-    }
-    return;
-  }
   const int wal = max(alo - 1, 0), wah = min(ahi + 1, g.na - 1);
   const int wbl = max(blo - 1, 0), wbh = min(bhi + 1, g.nb - 1);
-  const int wa = wah - wal + 1, ncand = wa * (wbh - wbl + 1);
+  const int wa = wah - wal + 1, wb = wbh - wbl + 1;
   const int span = narrow_span(ps.radius, g.step);
-  if (wa > span || wbh - wbl + 1 > span) { /* cannot happen; the window would not fit */
+  const bool unused = skip && skip[item];
+  /* prediction outside the lattice, or a window that would not fit (cannot
+     happen): no narrowed result */
+  if (unused || alo > ahi || blo > bhi || wa > span || wb > span) {
     if (threadIdx.x == 0) {
       vsbd_result o;
       o.sad = 0xffffffffu;
       o.tx = o.ty = 0;
       o.ok = 0;
       res[item] = o;
-      fb[item] = PN_FB_FULL;
-      fb_list[atomicAdd(fb_count, 1)] = item;
+      fb[item] = unused ? PN_FB_UNUSED : PN_FB_FULL;
+      if (!unused) fb_list[atomicAdd(fb_count, 1)] = item;
     }
     return;
   }
-
+  const vsbd_item it = items[item];
   uint32_t* C = (uint32_t*)sm;
   uint8_t* win = sm + L.off_win;
   unsigned* qsad = (unsigned*)(sm + L.off_q);
@@ -716,7 +767,7 @@ static __global__ void __launch_bounds__(256) k_pn_narrow(const uint8_t* __restr
       C[i] = __funnelshift_r(sw[0], sw[1], sh);
     }
     const int wwb = g.S * g.bpp + ((wa - 1) * g.step + 2 * L.R) * g.bpp;
-    const int wh = g.S + (wbh - wbl) * g.step + 2 * L.R;
+    const int wh = g.S + (wb - 1) * g.step + 2 * L.R;
     const int nv = (e + wwb + 15) >> 4;
     for (int i = threadIdx.x; i < wh * nv; i += blockDim.x) {
       const int r = i / nv, v = i - r * nv;
@@ -725,18 +776,16 @@ static __global__ void __launch_bounds__(256) k_pn_narrow(const uint8_t* __restr
     }
   }
   __syncthreads();
-  unsigned long long best = ~0ull;
-  for (int q = warp; q < ncand; q += nwarps) {
-    const int a = wal + q % wa, b = wbl + q / wa;
-    const int ddx = g.ax0 + a * g.step - dx0, ddy = g.by0 + b * g.step - dy0;
-    const unsigned sd = sad_rows_warp(C, L.rowW, g.S, win, (size_t)L.WP, e + ddx * g.bpp, ddy, lane);
-    const unsigned long long key = ((unsigned long long)sd << 32) | (unsigned)g.order[b * g.na + a];
-    best = key < best ? key : best;
-  }
-  if (lane == 0) red[warp] = best;
-  __syncthreads();
+  /* lattice window: column a - wal, row b - wbl at sums[(a-wal)*wb + (b-wbl)] */
+  sad_grid(C, L.rowW, g.S, win, L.WP, e, g.bpp, L.R, g.step, wa, L.R, g.step, wb, qsad);
   if (threadIdx.x == 0) {
-    for (int w = 1; w < nwarps; w++) best = red[w] < best ? red[w] : best;
+    unsigned long long best = ~0ull;
+    for (int q = 0; q < wa * wb; q++) {
+      const int a = wal + q / wb, b = wbl + q % wb;
+      const unsigned long long key =
+          ((unsigned long long)qsad[q] << 32) | (unsigned)g.order[b * g.na + a];
+      best = key < best ? key : best;
+    }
     const short2 pt = g.point[(unsigned)(best & 0xffffffffu)];
     s_min = (unsigned)(best >> 32);
     s_tx = pt.x;
@@ -745,31 +794,28 @@ static __global__ void __launch_bounds__(256) k_pn_narrow(const uint8_t* __restr
   __syncthreads();
   const int aw = (s_tx - g.ax0) / g.step, bw = (s_ty - g.by0) / g.step;
   const bool ring = aw < alo || aw > ahi || bw < blo || bw > bhi;
-  /* refinement rounds around the winner, inside the staged window */
+  /* refinement rounds around the winner, inside the staged window: the
+     side x side grid (centre included, ignored) */
   for (int st = 0; st < g.nstages; st++) {
     const int r = g.st_r[st], h = g.st_h[st];
-    const int side = (2 * r) / h + 1, nq = side * side;
+    const int side = (2 * r) / h + 1;
     const int cx = s_tx, cy = s_ty;
-    for (int q = warp; q < nq; q += nwarps) {
-      const int i = cx - r + (q / side) * h, j = cy - r + (q % side) * h;
-      unsigned sd = 0xffffffffu;
-      if (!(i == cx && j == cy))
-        sd = sad_rows_warp(C, L.rowW, g.S, win, (size_t)L.WP, e + (i - dx0) * g.bpp, j - dy0, lane);
-      if (lane == 0) qsad[q] = sd;
-    }
-    __syncthreads();
+    sad_grid(C, L.rowW, g.S, win, L.WP, e, g.bpp, cx - r - dx0, h, side, cy - r - dy0, h, side,
+             qsad);
     if (threadIdx.x == 0) {
       unsigned m = s_min;
       int tx = cx, ty = cy;
-      for (int q = 0; q < nq; q++) {
-        const int i = cx - r + (q / side) * h, j = cy - r + (q % side) * h;
-        if (i == cx && j == cy) continue;
-        if (qsad[q] < m) {
-          m = qsad[q];
-          tx = i;
-          ty = j;
+      /* the reference's order: i (x) outer, j (y) inner */
+      for (int ii = 0; ii < side; ii++)
+        for (int jj = 0; jj < side; jj++) {
+          const int i = cx - r + ii * h, j = cy - r + jj * h;
+          if (i == cx && j == cy) continue;
+          if (qsad[ii * side + jj] < m) {
+            m = qsad[ii * side + jj];
+            tx = i;
+            ty = j;
+          }
         }
-      }
       s_min = m;
       s_tx = tx;
       s_ty = ty;
@@ -827,6 +873,18 @@ static int pn_msg(const char* m) {
     if (e_ != cudaSuccess) return pn_fail(#call, e_); \
   } while (0)
 
+/* dynamic shared-memory limit of a kernel on the current device, raised
+   only when a launch needs more (slot names the kernel) */
+static cudaError_t pn_ensure_smem(const void* fn, int slot, size_t smem) {
+  static size_t done[16][8];
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev >= 0 && dev < 16 && done[dev][slot] >= smem) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess && dev >= 0 && dev < 16) done[dev][slot] = smem;
+  return e;
+}
+
 static int sm_count_cached(void) {
   static int n = 0;
   if (!n) n = vsbp_sm_count();
@@ -837,11 +895,7 @@ int vsbpn_infer(const void* d_params, const uint8_t* curr, const uint8_t* prev, 
                 int H, const vsbd_item* items, const void* prepared, int n, float* out,
                 cudaStream_t st) {
   if (n <= 0) return 0;
-  static int attr = 0;
-  if (!attr) {
-    PCK(cudaFuncSetAttribute(k_pn_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, PI_SMEM));
-    attr = 1;
-  }
+  PCK(pn_ensure_smem((const void*)k_pn_infer, 0, PI_SMEM));
   const int grid = min(n, sm_count_cached());
   k_pn_infer<<<grid, 256, PI_SMEM, st>>>(d_params, curr, prev, pitch, W, H, items,
                                          (const uint32_t*)prepared, n, out);
@@ -855,13 +909,11 @@ int vsbpn_narrow(const DGeom& g, const uint8_t* curr, const uint8_t* prev, int p
                  int* fb_list, cudaStream_t st) {
   if (n <= 0) return 0;
   if (g.has_origin) return pn_msg("the narrowed search serves planar field sets only");
+  if (narrow_span(ps.radius, g.step) * narrow_span(ps.radius, g.step) > PN_NARROW_QMAX)
+    return pn_msg("proposal radius too large for the narrowed search");
   const size_t smem = narrow_layout(g, ps.radius).total;
-  static size_t attr = 48 * 1024;
-  if (smem > attr) {
-    PCK(cudaFuncSetAttribute(k_pn_narrow, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr = smem;
-  }
-  k_pn_narrow<<<n, 256, smem, st>>>(curr, prev, pitch, g, items, pout, ps, skip, res, fb, fb_count,
+  if (smem > 48 * 1024) PCK(pn_ensure_smem((const void*)k_pn_narrow, 1, smem));
+  k_pn_narrow<<<n, 512, smem, st>>>(curr, prev, pitch, g, items, pout, ps, skip, res, fb, fb_count,
                                     fb_list);
   PCK(cudaGetLastError());
   return 1;
@@ -927,12 +979,8 @@ template <int CIN, int STRIDE, int HIN, bool L1>
 static int launch_bwd_weight(const float* dy, const bf16* y, const bf16* x, float* dw, float* db,
                              int n, cudaStream_t st) {
   const size_t smem = sizeof(float) * PN_PC * (32 + 9 * CIN);
-  static int attr = 0;
-  if (!attr) {
-    PCK(cudaFuncSetAttribute(k_pn_bwd_weight<CIN, STRIDE, HIN, L1>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr = 1;
-  }
+  PCK(pn_ensure_smem((const void*)k_pn_bwd_weight<CIN, STRIDE, HIN, L1>,
+                     2 + (CIN == 2 ? 0 : (HIN == 8 ? 1 : (HIN == 16 ? 2 : 3))), smem));
   constexpr int HO = HIN / STRIDE;
   const long chunks = ((long)n * HO * HO + PN_PC - 1) / PN_PC;
   const long cap = 2L * sm_count_cached();

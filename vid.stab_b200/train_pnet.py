@@ -49,6 +49,9 @@ def main():
     ap.add_argument("--rot-sigma", type=float, default=0.2)
     ap.add_argument("--conf-target", type=float, default=0.999)
     ap.add_argument("--conf-sweep", default="")
+    ap.add_argument("--val-agreement", type=float, default=1.0)
+    ap.add_argument("--train-shake", default="",
+                    help="per training seed, a factor on the camera-walk step sizes")
     a = ap.parse_args()
 
     import torch
@@ -59,9 +62,11 @@ def main():
     W, H = a.width, a.height
     t0 = time.time()
     xs, labs = [], []
-    for sd in [int(s) for s in a.train_seeds.split(",")]:
-        clip = S.clip(W, H, a.frames, seed=sd, device="cuda", trans_sigma=a.trans_sigma,
-                      rot_sigma_deg=a.rot_sigma)
+    seeds = [int(v) for v in a.train_seeds.split(",")]
+    shakes = [float(v) for v in a.train_shake.split(",")] if a.train_shake else [1.0] * len(seeds)
+    for sd, k in zip(seeds, shakes):
+        clip = S.clip(W, H, a.frames, seed=sd, device="cuda", trans_sigma=a.trans_sigma * k,
+                      rot_sigma_deg=a.rot_sigma * k)
         x, lab = pnet.field_log(clip, W, H, cap=a.pairs)
         xs.append(x)
         labs.append(lab)
@@ -92,8 +97,28 @@ def main():
     vclip = S.clip(W, H, 60, seed=a.val_seed, device="cuda", trans_sigma=a.trans_sigma,
                    rot_sigma_deg=a.rot_sigma)
     vx, vlab = pnet.field_log(vclip, W, H, cap=60 * 500)
-    del vclip
     cal = pnet.calibrate(params, vx, vlab, sizes, radius=a.radius, target=a.conf_target)
+    blob = pnet.pack_blob(bits, f32, pnet.SCALE, a.radius, cal["conf_min"], cal["match_bound"])
+    # the confidence threshold: the lowest fallback rate among the thresholds
+    # whose field agreement with the full search on the validation clip is
+    # complete (the ring and SAD-bound checks stay on)
+    sweep = []
+    for cm in sorted({round(cal["conf_min"], 3), 2.0, 0.0, -2.0, -4.0}, reverse=True):
+        det = V.MotionDetector(W, H, V.PF_YUV420P)
+        pnet.set_proposal(det, blob, conf_min=cm, verify=True)
+        rec = np.zeros(60 * 512 + 64, V.LM_DTYPE)
+        cnt = np.zeros(60, np.int32)
+        det.run(60, vclip.data_ptr(), W * H, W, True, rec, cnt)
+        st = pnet.proposal_stats(det)
+        det.close()
+        sweep.append({"conf_min": cm, "agreement": st["agreement"],
+                      "fallback_rate": st["fallback_rate"]})
+    good = [r for r in sweep if r["agreement"] is not None and r["agreement"] >= a.val_agreement]
+    if good:
+        pick = min(good, key=lambda r: (r["fallback_rate"], -r["conf_min"]))
+        cal["conf_min"] = pick["conf_min"]
+    cal["sweep"] = sweep
+    del vclip
     blob = pnet.pack_blob(bits, f32, pnet.SCALE, a.radius, cal["conf_min"], cal["match_bound"])
     os.makedirs(os.path.dirname(os.path.abspath(a.out)), exist_ok=True)
     with open(a.out, "wb") as f:
@@ -101,11 +126,12 @@ def main():
 
     ev = evaluate(blob, W, H, a.eval_seed, a.eval_frames, a.trans_sigma, a.rot_sigma,
                   [float(v) for v in a.conf_sweep.split(",")] if a.conf_sweep else ())
+    ev_shake = evaluate(blob, W, H, a.eval_seed + 1, a.eval_frames // 2, 8.0, 0.5)
     print(json.dumps({"pairs": int(len(lab)), "pairs_used": int((lab["use"] == 1).sum()),
                       "coarse_pairs": int(((lab["use"] == 1) & (lab["kind"] == 0)).sum()),
                       "data_s": t_data, "train_s": t_train, "steps": a.steps,
                       "final_loss": log[-1][1] if log else None, "calibration": cal,
-                      "eval": ev, "out": a.out}))
+                      "eval": ev, "eval_large_shake": ev_shake, "out": a.out}))
 
 
 def evaluate(blob, W, H, seed, n, trans_sigma=3.0, rot_sigma=0.2, conf_sweep=()):
@@ -133,16 +159,17 @@ def evaluate(blob, W, H, seed, n, trans_sigma=3.0, rot_sigma=0.2, conf_sweep=())
     res["plain_kernel_ms"] = pnet.kernel_ms(
         plain, lambda: plain.run(n, clip.data_ptr(), W * H, W, True, rec, cnt))
     plain.close()
-    runs = [("learned", blob, float("nan")), ("zero", pnet.zero_blob(), float("nan"))]
-    runs += [("learned_conf%g" % cm, blob, cm) for cm in conf_sweep]
-    for name, b, cm in runs:
+    runs = [("learned", blob, float("nan"), False), ("learned_fine_net", blob, float("nan"), True),
+            ("zero", pnet.zero_blob(), float("nan"), False)]
+    runs += [("learned_conf%g" % cm, blob, cm, False) for cm in conf_sweep]
+    for name, b, cm, fnet in runs:
         det = V.MotionDetector(W, H, V.PF_YUV420P)
-        pnet.set_proposal(det, b, conf_min=cm, verify=True)
+        pnet.set_proposal(det, b, conf_min=cm, verify=True, fine_net=fnet)
         det.run(n, clip.data_ptr(), W * H, W, True, rec, cnt)
         st = pnet.proposal_stats(det)
         det.close()
         det = V.MotionDetector(W, H, V.PF_YUV420P)
-        pnet.set_proposal(det, b, conf_min=cm)
+        pnet.set_proposal(det, b, conf_min=cm, fine_net=fnet)
         fps, lrec, lcnt = timed(det)
         kms = pnet.kernel_ms(det, lambda: det.run(n, clip.data_ptr(), W * H, W, True, rec, cnt))
         det.close()

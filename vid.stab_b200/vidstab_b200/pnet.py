@@ -63,6 +63,8 @@ def _L():
         L.vsb_set_proposal.argtypes = [p, p, l_]
         L.vsb_set_proposal_ex.restype = i
         L.vsb_set_proposal_ex.argtypes = [p, p, l_, C.c_double, C.c_double, C.c_double]
+        L.vsb_set_proposal_scope.restype = i
+        L.vsb_set_proposal_scope.argtypes = [p, i]
         L.vsb_set_proposal_verify.restype = i
         L.vsb_set_proposal_verify.argtypes = [p, i]
         L.vsb_proposal_stats.restype = i
@@ -122,12 +124,15 @@ def zero_blob(radius=2.0, conf_logit=10.0, match_bound=64.0):
     return pack_blob(np.zeros(N_BF16, np.uint16), f32, SCALE, radius, 0.0, match_bound)
 
 
-def set_proposal(det, blob, radius=-1.0, conf_min=float("nan"), match_bound=-1.0, verify=False):
+def set_proposal(det, blob, radius=-1.0, conf_min=float("nan"), match_bound=-1.0, verify=False,
+                 fine_net=False):
     """Gives a MotionDetector the proposal (blob None: back to plain)."""
     L = _L()
     buf = C.create_string_buffer(blob, len(blob)) if blob is not None else None
     _check(L.vsb_set_proposal_ex(C.byref(det.md), buf, len(blob) if blob else 0, radius,
                                  conf_min, match_bound), "vsb_set_proposal_ex")
+    _check(L.vsb_set_proposal_scope(C.byref(det.md), 1 if fine_net else 0),
+           "vsb_set_proposal_scope")
     _check(L.vsb_set_proposal_verify(C.byref(det.md), 1 if verify else 0), "vsb_set_proposal_verify")
 
 
