@@ -17,7 +17,13 @@ shakiness 5, mincontrast 0.25).  One step = the detect pass over the whole clip.
 * roofline: the dominant kernel (the coarse SAD search) against the measured
   packed-SAD throughput of this GPU, and the prefilter against HBM;
 * cpu_baseline: the reference's own CPU detect (compiled from its sources,
-  oracle/_ref) on this host's cores over a bounded sample of the same clip.
+  oracle/_ref) on this host's cores over a bounded sample of the same clip;
+* learned: the learned-proposal detector on the same clip (frames/s in HBM
+  and from host frames, field agreement with the exact full search over
+  every field, frames identical to the plain path);
+* batched: 64 concurrent streams of mixed resolution through one batch,
+  aggregate frames/s, against the same streams through single-stream
+  detectors one after another.
 
 With --gpus N (torchrun), every rank runs an independent clip (seed + rank):
 no data moves between GPUs; the time is the max over ranks.
@@ -54,6 +60,9 @@ def parse():
     ap.add_argument("--frames", type=int, default=300)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--batch-frames", type=int, default=30)
     return ap.parse_args()
 
 
@@ -161,6 +170,125 @@ def traffic_from_profile(name):
             except ValueError:
                 return None
     return None
+
+
+def frames_identical(a, ca, b, cb):
+    """frames whose LocalMotions are identical in two runs"""
+    oa = np.concatenate([[0], np.cumsum(ca)])
+    ob = np.concatenate([[0], np.cumsum(cb)])
+    return int(sum(1 for k in range(len(ca)) if ca[k] == cb[k] and
+                   np.array_equal(a[oa[k]:oa[k + 1]], b[ob[k]:ob[k + 1]])))
+
+
+def learned_arm(V, clip, host_np, nfr, steps, warmup, timed):
+    """The learned-proposal detector (the packaged 1080p network) on the same
+    clip: frames/s with the clip in HBM and from pinned host frames, field
+    agreement with the exact full search (verify mode, every field of the
+    clip), frames whose LocalMotions equal the plain detector's, and the
+    per-frame device time of its kernels."""
+    from vidstab_b200 import pnet
+    blob = pnet.load_blob()
+    rec = np.zeros(nfr * 512 + 64, V.LM_DTYPE)
+    cnt = np.zeros(nfr, np.int32)
+
+    def fresh(with_blob, verify=False):
+        d = V.MotionDetector(W, H, V.PF_YUV420P)
+        if with_blob:
+            pnet.set_proposal(d, blob, verify=verify)
+        return d
+
+    d = fresh(True, verify=True)
+    d.run(nfr, clip.data_ptr(), W * H, W, True, rec, cnt)
+    st = pnet.proposal_stats(d)
+    d.close()
+    d = fresh(False)
+    tp = d.run(nfr, clip.data_ptr(), W * H, W, True, rec, cnt)
+    prec, pcnt = rec[:tp].copy(), cnt.copy()
+    d.close()
+    d = fresh(True)
+    tl = d.run(nfr, clip.data_ptr(), W * H, W, True, rec, cnt)
+    same = frames_identical(prec, pcnt, rec[:tl], cnt)
+    d.close()
+    dd, dh = fresh(True), fresh(True)
+    for _ in range(warmup):
+        dd.run(nfr, clip.data_ptr(), W * H, W, True, rec, cnt)
+    td = timed(lambda: dd.run(nfr, clip.data_ptr(), W * H, W, True, rec, cnt), steps)
+    for _ in range(max(1, warmup // 2)):
+        dh.run(nfr, host_np.ctypes.data, W * H, W, False, rec, cnt)
+    th = timed(lambda: dh.run(nfr, host_np.ctypes.data, W * H, W, False, rec, cnt), steps)
+    nk = min(nfr, 60)
+    kms = pnet.kernel_ms(dd, lambda: [dd.detect_device(clip.data_ptr() + k * W * H, W)
+                                      for k in range(nk)])
+    dd.close()
+    dh.close()
+    return {"value": nfr * steps / sum(td), "unit": "frames/s",
+            "e2e": nfr * steps / sum(th),
+            "agreement": st["agreement"], "fields_verified": st["verified"],
+            "fallback_rate": st["fallback_rate"], "coarse_fallbacks": st["coarse_fell_back"],
+            "fine_fallbacks": st["fine_fell_back"],
+            "frames_identical_to_plain": same, "frames": nfr,
+            "kernel_ms_per_frame": kms,
+            "network": "packaged 1080p proposal network (vidstab_b200/data/pnet_1080p.vsbp): "
+                       "coarse fields by the network, fine fields around the coarse model"}
+
+
+def batched_arm(V, steps, warmup, timed, frames):
+    """64 concurrent streams, resolutions 640x360 / 1280x720 / 1920x1080 /
+    3840x2160 in ratio 4:3:2:1 (26/19/13/6 streams), each a camera-walk clip
+    of its own seed, through one batch (persistent kernel per stage from
+    captured CUDA graphs), against the same streams run one after another
+    through single-stream detectors on the same GPU."""
+    from vidstab_b200 import synthetic as S
+    classes = [(640, 360, 26), (1280, 720, 19), (1920, 1080, 13), (3840, 2160, 6)]
+    sizes = [(w, h) for w, h, n in classes for _ in range(n)]
+    clips = [S.clip(w, h, frames, seed=5000 + i, device="cuda") for i, (w, h) in enumerate(sizes)]
+    ptrs = [c.data_ptr() for c in clips]
+    fb = [w * h for w, h in sizes]
+    pitches = [w for w, _ in sizes]
+    n = len(sizes)
+    out = np.zeros(frames * n * 800 + 64, V.LM_DTYPE)
+    counts = np.zeros(frames * n, np.int32)
+    b = V.Batch([w for w, _ in sizes], [h for _, h in sizes])
+    tot = b.run(ptrs, fb, pitches, frames, True, out, counts)  # fresh streams: the parity run
+    out_first, counts_first = out.copy(), counts.copy()
+    for _ in range(warmup):
+        b.run(ptrs, fb, pitches, frames, True, out, counts)
+    l0 = b.launches()
+    tb = timed(lambda: b.run(ptrs, fb, pitches, frames, True, out, counts), steps)
+    launches = (b.launches() - l0) // max(steps, 1)
+    b.close()
+    out, counts = out_first, counts_first
+    # every stream through a detector of its own, one after another
+    dets = [V.MotionDetector(w, h, V.PF_YUV420P) for w, h in sizes]
+    rec = np.zeros(frames * 800 + 64, V.LM_DTYPE)
+    cnt = np.zeros(frames, np.int32)
+    cm = counts.reshape(frames, n)
+    pos = np.concatenate([[0], np.cumsum(cm.ravel())])
+    same = 0
+
+    def run_all():
+        for s in range(n):
+            dets[s].run(frames, ptrs[s], fb[s], pitches[s], True, rec, cnt)
+
+    for s in (0, n - 1):  # parity of a small and a 4K stream with their own detectors
+        d = V.MotionDetector(sizes[s][0], sizes[s][1], V.PF_YUV420P)
+        t = d.run(frames, ptrs[s], fb[s], pitches[s], True, rec, cnt)
+        d.close()
+        mine = np.concatenate([out[pos[k * n + s]:pos[k * n + s + 1]] for k in range(frames)])
+        same += int(np.array_equal(cm[:, s], cnt) and np.array_equal(mine, rec[:t]))
+    run_all()
+    ts = timed(run_all, steps)
+    for d in dets:
+        d.close()
+    agg = n * frames * steps / sum(tb)
+    seq = n * frames * steps / sum(ts)
+    return {"value": agg, "unit": "frames/s (all streams)", "streams": n,
+            "frames_per_stream": frames, "records": int(tot),
+            "streams_checked_identical": "%d of 2" % same,
+            "single_stream_detectors_sequential": seq, "speedup": agg / seq,
+            "persistent_launches_per_step": int(launches),
+            "workload": "64 streams 26x640x360 + 19x1280x720 + 13x1920x1080 + 6x3840x2160, "
+                        "camera-walk clips (seed per stream), defaults of the 1080p clip"}
 
 
 def run_reference(args):
@@ -296,6 +424,27 @@ def main():
     value = nfr * args.steps * world / tot_dev
     e2e = nfr * args.steps * world / tot_host
 
+    def timed_local(fn, steps):
+        """CUDA-event time of fn on this rank alone (no barrier)"""
+        ts = []
+        for _ in range(steps):
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1) / 1000.0)
+        return ts
+
+    learned = None
+    batched = None
+    if rank == 0 and not args.no_learned:
+        learned = learned_arm(V, clip, host_np, nfr, args.steps, args.warmup, timed_local)
+    if rank == 0 and not args.no_batched:
+        batched = batched_arm(V, args.steps, args.warmup, timed_local, args.batch_frames)
+
     # per-kernel device time on the detector's stream (separate, instrumented pass)
     roof = None
     roof_hbm = None
@@ -370,6 +519,7 @@ def main():
                     "d2h_bytes_per_step": (d1 - d0) // max(args.steps, 1)},
             "gpu_launches": l1 - l0,
             "roofline": roof, "roofline_hbm": roof_hbm, "kernel_ms": kernel_ms,
+            "learned": learned, "batched": batched,
             "cpu_baseline": cpu, "clocks": clk, "parity": parity,
         }
         print(json.dumps(line))
