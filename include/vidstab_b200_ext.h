@@ -207,8 +207,10 @@ VS_API int vsb_set_proposal_ex(struct _vsmotiondetect* md, const void* blob, lon
 /* Which fields the network serves: the coarse fields always; the fine
    fields too with fine_net = 1.  With fine_net = 0 (the default) a fine
    field's narrowed window is centred on the coarse model's prediction for
-   it (zero residual), with the same fallbacks. */
-VS_API int vsb_set_proposal_scope(struct _vsmotiondetect* md, int fine_net);
+   it (zero residual), with the same fallbacks.  fine_radius: the fine
+   fields' window radius in pixels (at most 16; negative: 4 px around the
+   model, the blob's radius around the network). */
+VS_API int vsb_set_proposal_scope(struct _vsmotiondetect* md, int fine_net, double fine_radius);
 /* With verify on, every stage also runs the full search of every item and
    counts the items whose result (SAD, shift, range test) is identical. */
 VS_API int vsb_set_proposal_verify(struct _vsmotiondetect* md, int on);

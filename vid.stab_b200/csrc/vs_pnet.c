@@ -69,8 +69,9 @@ int vsb_set_proposal(VSMotionDetect* md, const void* blob, long bytes) {
   return vsb_set_proposal_ex(md, blob, bytes, -1.0, NAN, -1.0);
 }
 
-int vsb_set_proposal_scope(VSMotionDetect* md, int fine_net) {
-  return vsbd_set_proposal_scope(vsb_md_device(md), fine_net) == 0 ? VS_OK : VS_ERROR;
+int vsb_set_proposal_scope(VSMotionDetect* md, int fine_net, double fine_radius) {
+  return vsbd_set_proposal_scope(vsb_md_device(md), fine_net, (float)fine_radius) == 0 ? VS_OK
+                                                                                       : VS_ERROR;
 }
 
 int vsb_set_proposal_verify(VSMotionDetect* md, int on) {

@@ -104,54 +104,67 @@ __global__ void k_blur_cols(const uint8_t* __restrict__ src, int sp, uint8_t* __
 }
 
 /* Planar prefilter with vector memory access: one CTA of 256 threads
-   blurs a BF_H x BF_W output tile.  Input rows (clamped to the frame) are
-   staged with 16-byte loads from 16 bytes left of the tile to 16 bytes right
-   of it (tiles touching the left or right frame edge load bytewise with
-   clamped columns); the horizontal pass writes 4 outputs per task as one
-   word, the vertical pass runs 4-column sliding sums and stores words.  Same
-   arithmetic as blur_tile (window sums, floor division by the size). */
+   blurs a BF_H x BF_W output tile, for a window half-width HALF known at
+   compile time.  Input rows (clamped to the frame) are staged with 16-byte
+   loads from 16 bytes left of the tile to 16 bytes right of it (tiles
+   touching the left or right frame edge load bytewise with clamped
+   columns).  The horizontal pass gives each task a run of 16 outputs of one
+   row: the bytes it needs are read as words once, the window sum slides
+   along the run, and the 16 results are stored as one 16-byte vector.  The
+   vertical pass runs 4-column sliding sums down a quarter of the tile and
+   stores words.  Same arithmetic as blur_tile (window sums, floor division
+   by the size). */
 #define BF_W 256
 #define BF_H 32
 #define BF_MAXHALF 16
 #define BF_RAWP (BF_W + 32)
+template <int HALF>
 __global__ void __launch_bounds__(256) k_blur_fast(const uint8_t* __restrict__ src, int sp,
                                                    uint8_t* __restrict__ dst, int dp, int W, int H,
-                                                   int half, BlurDiv dv) {
-  __shared__ __align__(16) uint8_t raw[(BF_H + 2 * BF_MAXHALF) * BF_RAWP];
-  __shared__ __align__(16) uint8_t hor[(BF_H + 2 * BF_MAXHALF) * BF_W];
+                                                   BlurDiv dv) {
+  __shared__ __align__(16) uint8_t raw[(BF_H + 2 * HALF) * BF_RAWP];
+  __shared__ __align__(16) uint8_t hor[(BF_H + 2 * HALF) * BF_W];
+  constexpr int ROWS = BF_H + 2 * HALF, WIN = 2 * HALF + 1;
   const int x0 = blockIdx.x * BF_W, y0 = blockIdx.y * BF_H;
-  const int rows = BF_H + 2 * half;
   const bool interior = x0 >= 16 && x0 + BF_W + 16 <= W;
   if (interior) {
-    for (int i = threadIdx.x; i < rows * (BF_RAWP / 16); i += blockDim.x) {
+    for (int i = threadIdx.x; i < ROWS * (BF_RAWP / 16); i += blockDim.x) {
       const int r = i / (BF_RAWP / 16), v = i - r * (BF_RAWP / 16);
-      const int gy = min(max(y0 - half + r, 0), H - 1);
+      const int gy = min(max(y0 - HALF + r, 0), H - 1);
       *(uint4*)(raw + r * BF_RAWP + (v << 4)) =
           *(const uint4*)(src + (size_t)gy * sp + x0 - 16 + (v << 4));
     }
   } else {
-    for (int i = threadIdx.x; i < rows * BF_RAWP; i += blockDim.x) {
+    for (int i = threadIdx.x; i < ROWS * BF_RAWP; i += blockDim.x) {
       const int r = i / BF_RAWP, c = i - r * BF_RAWP;
-      const int gy = min(max(y0 - half + r, 0), H - 1);
+      const int gy = min(max(y0 - HALF + r, 0), H - 1);
       const int gx = min(max(x0 - 16 + c, 0), W - 1);
       raw[r * BF_RAWP + c] = src[(size_t)gy * sp + gx];
     }
   }
   __syncthreads();
-  const int win = 2 * half + 1;
-  for (int i = threadIdx.x; i < rows * (BF_W / 4); i += blockDim.x) {
-    const int r = i / (BF_W / 4), c = (i - r * (BF_W / 4)) * 4;
-    const uint8_t* p = raw + r * BF_RAWP + 16 + c - half;
-    unsigned acc = 0;
-    for (int k = 0; k < win; k++) acc += p[k];
-    unsigned o = blur_div(acc, dv);
+  /* runs of 16 outputs at columns c0 .. c0+15 need raw bytes
+     16 + c0 - HALF .. 16 + c0 + 15 + HALF; read the words from 16 + c0 - 16 */
+  constexpr int NW = (16 + 15 + HALF) / 4 + 1; /* the words holding bytes c0 .. c0 + 31 + HALF */
+  for (int t = threadIdx.x; t < ROWS * (BF_W / 16); t += blockDim.x) {
+    const int r = t / (BF_W / 16), c0 = (t - r * (BF_W / 16)) * 16;
+    const uint32_t* wp = (const uint32_t*)(raw + r * BF_RAWP + c0); /* byte 16 + c0 - 16 */
+    uint32_t wv[NW];
 #pragma unroll
-    for (int k = 1; k < 4; k++) {
-      acc += p[win - 1 + k];
-      acc -= p[k - 1];
-      o |= blur_div(acc, dv) << (8 * k);
+    for (int k = 0; k < NW; k++) wv[k] = wp[k];
+    /* byte b of the staged row relative to c0 - 16 + 16 = c0: index 16 + b */
+#define BYTE_AT(b) ((wv[(16 + (b)) >> 2] >> (((16 + (b)) & 3) * 8)) & 0xffu)
+    unsigned acc = 0;
+#pragma unroll
+    for (int k = -HALF; k <= HALF; k++) acc += BYTE_AT(k);
+    uint32_t o[4] = { 0u, 0u, 0u, 0u };
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+      if (q > 0) acc += BYTE_AT(q + HALF) - BYTE_AT(q - 1 - HALF);
+      o[q >> 2] |= blur_div(acc, dv) << (8 * (q & 3));
     }
-    *(unsigned*)(hor + r * BF_W + c) = o;
+#undef BYTE_AT
+    *(uint4*)(hor + r * BF_W + c0) = make_uint4(o[0], o[1], o[2], o[3]);
   }
   __syncthreads();
   /* thread: 4 columns (cg), a quarter of the tile rows */
@@ -160,7 +173,8 @@ __global__ void __launch_bounds__(256) k_blur_fast(const uint8_t* __restrict__ s
   if (gx >= W) return;
   const int rb = part * (BF_H / 4);
   unsigned a0 = 0, a1 = 0, a2 = 0, a3 = 0;
-  for (int k = 0; k < win; k++) {
+#pragma unroll
+  for (int k = 0; k < WIN; k++) {
     const unsigned w = *(const unsigned*)(hor + (rb + k) * BF_W + cg * 4);
     a0 += w & 0xff;
     a1 += (w >> 8) & 0xff;
@@ -168,9 +182,10 @@ __global__ void __launch_bounds__(256) k_blur_fast(const uint8_t* __restrict__ s
     a3 += w >> 24;
   }
   const bool full4 = gx + 4 <= W;
+#pragma unroll
   for (int r = rb; r < rb + BF_H / 4; r++) {
     if (r > rb) {
-      const unsigned wi = *(const unsigned*)(hor + (r + win - 1) * BF_W + cg * 4);
+      const unsigned wi = *(const unsigned*)(hor + (r + WIN - 1) * BF_W + cg * 4);
       const unsigned wo = *(const unsigned*)(hor + (r - 1) * BF_W + cg * 4);
       a0 += (wi & 0xff) - (wo & 0xff);
       a1 += ((wi >> 8) & 0xff) - ((wo >> 8) & 0xff);
@@ -190,15 +205,30 @@ __global__ void __launch_bounds__(256) k_blur_fast(const uint8_t* __restrict__ s
   }
 }
 
+/* k_blur_fast for the window half-width of the plane (1..BF_MAXHALF) */
+static void launch_blur_fast(dim3 grid, cudaStream_t st, const uint8_t* src, int sp, uint8_t* dst,
+                             int dp, int W, int H, int half, BlurDiv dv) {
+#define VSB_BLURH(K) \
+  case K: k_blur_fast<K><<<grid, 256, 0, st>>>(src, sp, dst, dp, W, H, dv); break;
+  switch (half) {
+    VSB_BLURH(1) VSB_BLURH(2) VSB_BLURH(3) VSB_BLURH(4) VSB_BLURH(5) VSB_BLURH(6)
+    VSB_BLURH(7) VSB_BLURH(8) VSB_BLURH(9) VSB_BLURH(10) VSB_BLURH(11) VSB_BLURH(12)
+    VSB_BLURH(13) VSB_BLURH(14) VSB_BLURH(15) VSB_BLURH(16)
+    default: break;
+  }
+#undef VSB_BLURH
+}
+
 /* launches the prefilter of one plane; returns the number of kernels */
 static int launch_blur(const uint8_t* src, int sp, uint8_t* dst, int dp, int W, int H, int size,
                        uint8_t* tmp, int tp, cudaStream_t st) {
   int half = size / 2;
   BlurDiv dv;
   make_div(size, half, &dv);
-  if (half <= BF_MAXHALF && ((((uintptr_t)src | (uintptr_t)sp | (uintptr_t)dst | (uintptr_t)dp) & 15) == 0)) {
+  if (half >= 1 && half <= BF_MAXHALF &&
+      ((((uintptr_t)src | (uintptr_t)sp | (uintptr_t)dst | (uintptr_t)dp) & 15) == 0)) {
     dim3 grid((W + BF_W - 1) / BF_W, (H + BF_H - 1) / BF_H);
-    k_blur_fast<<<grid, 256, 0, st>>>(src, sp, dst, dp, W, H, half, dv);
+    launch_blur_fast(grid, st, src, sp, dst, dp, W, H, half, dv);
     return 1;
   }
   if (half <= BT_MAXHALF) {
@@ -774,6 +804,7 @@ struct vsbd_ctx {
   int pn_on, pn_verify;
   int pn_fine_net;              /* fine fields: 1 network proposal, 0 the coarse model's
                                    prediction (zero residual) */
+  float pn_fine_radius;         /* window radius of the fine fields (< 0: the default) */
   float* d_pout;                /* network outputs [nc + nf][3] */
   vsbd_result* d_vres;          /* verify: full-search results, coarse then fine */
   vsbd_result* h_vres;
@@ -929,6 +960,7 @@ extern "C" int vsbd_create(vsbd_ctx** out, int W, int H, int bpp, int blur_size,
   }
   c->cur = 0;
   c->prv = 1;
+  c->pn_fine_radius = -1.f;
   CKC(cudaStreamCreateWithFlags(&c->st2, cudaStreamNonBlocking));
   CKC(cudaEventCreateWithFlags(&c->ev_a, cudaEventDisableTiming));
   CKC(cudaEventCreateWithFlags(&c->ev_b, cudaEventDisableTiming));
@@ -1038,6 +1070,9 @@ static int learned_search(vsbd_ctx* c, const GeomDev& gd, const GeomDev& gfull, 
   kt_begin(c, kt, st);
   /* the SAD bound scales with the field's pixel count */
   PNSearch ps = c->pn;
+  if (base != 0) /* fine fields: 4 px around the coarse model, the blob's radius around the network */
+    ps.radius = c->pn_fine_radius >= 0.f ? c->pn_fine_radius
+                                         : (c->pn_fine_net ? c->pn.radius : 4.0f);
   const double bound = (double)c->pn_match_bound * gd.g.S * gd.g.S;
   ps.sad_bound = bound >= 4294967295.0 ? 0xffffffffu : (unsigned)bound;
   CK(cudaMemsetAsync(fbl, 0, sizeof(int), st));
@@ -1366,9 +1401,14 @@ extern "C" int vsbd_set_proposal(vsbd_ctx* c, const void* params, float scale, f
   return 0;
 }
 
-extern "C" int vsbd_set_proposal_scope(vsbd_ctx* c, int fine_net) {
+extern "C" int vsbd_set_proposal_scope(vsbd_ctx* c, int fine_net, float fine_radius) {
   if (!c) return -1;
+  if (fine_radius > 16.f) {
+    set_msg("fine proposal radius above 16 px");
+    return -1;
+  }
   c->pn_fine_net = fine_net ? 1 : 0;
+  c->pn_fine_radius = fine_radius;
   return 0;
 }
 

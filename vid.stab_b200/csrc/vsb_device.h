@@ -120,8 +120,10 @@ int vsbd_set_proposal(vsbd_ctx* c, const void* params, float scale, float radius
                       float match_bound);
 long vsbd_pnet_param_bytes(void);
 /* fine fields take the network's proposal (fine_net 1) or the coarse
-   model's prediction, i.e. zero residual (0, the default) */
-int vsbd_set_proposal_scope(vsbd_ctx* c, int fine_net);
+   model's prediction, i.e. zero residual (0, the default); fine_radius:
+   their window radius in pixels (< 0: 4 px around the model, the blob's
+   radius around the network) */
+int vsbd_set_proposal_scope(vsbd_ctx* c, int fine_net, float fine_radius);
 /* with verify on, every stage also runs the full search and compares */
 int vsbd_set_proposal_verify(vsbd_ctx* c, int on);
 /* [0] items searched with a proposal, [1] of them fell back, [2] items

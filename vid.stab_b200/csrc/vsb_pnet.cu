@@ -346,12 +346,13 @@ static __global__ void __launch_bounds__(256) k_pn_bwd_weight(const float* __res
 #define PI_SM_FC (PI_SM_W4 + 18432)      /* [3][512] plain */
 #define PI_SM_B (PI_SM_FC + 3072)        /* f32 [131] */
 #define PI_SM_IN (PI_SM_B + 528)         /* [34][34][2] zero-bordered input */
-#define PI_SM_A1 (PI_SM_IN + 4624)       /* im2col of 256 conv1 pixels [256][32] */
-#define PI_SM_ACT1 (PI_SM_A1 + 16384)    /* [34*34][32] */
+#define PI_SM_A1 (PI_SM_IN + 4624)       /* im2col of 512 conv1 pixels [512][32] */
+#define PI_SM_ACT1 (PI_SM_A1 + 32768)    /* [34*34][32] */
 #define PI_SM_ACT2 (PI_SM_ACT1 + 73984)  /* [18*18][32] */
 #define PI_SM_ACT3 (PI_SM_ACT2 + 20736)  /* [10*10][32] */
 #define PI_SM_ACT4 (PI_SM_ACT3 + 6400)   /* f32 [16][32] */
 #define PI_SMEM (PI_SM_ACT4 + 2048)
+#define PI_THREADS 512
 
 __device__ __forceinline__ int swz(int row, int ch) {
   return (row << 5) | ((((ch >> 3) ^ (row >> 1)) & 3) << 3) | (ch & 7);
@@ -409,15 +410,16 @@ __device__ __forceinline__ void conv_s2_mtile(const bf16* act, int WP, int oy, i
   }
 }
 
-/* grid: up to one CTA per SM, CTAs stride over the items; block 256 */
-static __global__ void __launch_bounds__(256, 1) k_pn_infer(const void* __restrict__ params,
+/* grid: up to one CTA per SM, CTAs stride over the items; block PI_THREADS
+   (16 warps) */
+static __global__ void __launch_bounds__(PI_THREADS, 1) k_pn_infer(const void* __restrict__ params,
                                                             const uint8_t* __restrict__ curr,
                                                             const uint8_t* __restrict__ prev,
                                                             int pitch, int W, int H,
                                                             const vsbd_item* __restrict__ items,
                                                             const uint32_t* __restrict__ prepared,
                                                             int n, float* __restrict__ out) {
-  extern __shared__ __align__(128) uint8_t sm[];
+  extern __shared__ __align__(16) uint8_t sm[];
   bf16* sW1 = (bf16*)(sm + PI_SM_W1);
   bf16* sW2 = (bf16*)(sm + PI_SM_W2);
   bf16* sW3 = (bf16*)(sm + PI_SM_W3);
@@ -435,19 +437,19 @@ static __global__ void __launch_bounds__(256, 1) k_pn_infer(const void* __restri
 
   /* weights, swizzled 16-byte chunks; zero every bordered buffer once (the
      borders are never written again) */
-  for (int i = tid; i < 32 * 4; i += 256) {
+  for (int i = tid; i < 32 * 4; i += PI_THREADS) {
     const int r = i >> 2, j = i & 3;
     ((uint4*)sW1)[r * 4 + (j ^ ((r >> 1) & 3))] = ((const uint4*)P.w1)[i];
   }
-  for (int i = tid; i < 288 * 4; i += 256) {
+  for (int i = tid; i < 288 * 4; i += PI_THREADS) {
     const int r = i >> 2, j = i & 3, d = r * 4 + (j ^ ((r >> 1) & 3));
     ((uint4*)sW2)[d] = ((const uint4*)P.w2)[i];
     ((uint4*)sW3)[d] = ((const uint4*)P.w3)[i];
     ((uint4*)sW4)[d] = ((const uint4*)P.w4)[i];
   }
-  for (int i = tid; i < PN_NFC / 8; i += 256) ((uint4*)sFC)[i] = ((const uint4*)P.fc)[i];
-  for (int i = tid; i < PN_NF32; i += 256) sB[i] = P.b1[i];
-  for (int i = tid; i < (PI_SM_ACT4 - PI_SM_IN) / 16; i += 256)
+  for (int i = tid; i < PN_NFC / 8; i += PI_THREADS) ((uint4*)sFC)[i] = ((const uint4*)P.fc)[i];
+  for (int i = tid; i < PN_NF32; i += PI_THREADS) sB[i] = P.b1[i];
+  for (int i = tid; i < (PI_SM_ACT4 - PI_SM_IN) / 16; i += PI_THREADS)
     ((uint4*)(sm + PI_SM_IN))[i] = make_uint4(0, 0, 0, 0);
   __syncthreads();
 
@@ -459,21 +461,21 @@ static __global__ void __launch_bounds__(256, 1) k_pn_infer(const void* __restri
     /* 1. input planes */
     if (prepared) {
       const uint32_t* src = prepared + (size_t)s * 1024;
-      for (int i = tid; i < 1024; i += 256) sIn[((i >> 5) + 1) * 34 + (i & 31) + 1] = src[i];
+      for (int i = tid; i < 1024; i += PI_THREADS) sIn[((i >> 5) + 1) * 34 + (i & 31) + 1] = src[i];
     } else {
       const vsbd_item it = items[s];
       bf16* sInh = (bf16*)sIn;
-      for (int i = tid; i < 2048; i += 256) {
+      for (int i = tid; i < 2048; i += PI_THREADS) {
         const int r = i >> 6, c = (i >> 1) & 31, ch = i & 1;
         sInh[((r + 1) * 34 + c + 1) * 2 + ch] = crop_value(curr, prev, pitch, W, H, it, ch, r, c);
       }
     }
     __syncthreads();
 
-    /* 2. conv1 (stride 1) as an im2col GEMM, 4 chunks of 8 output rows */
-    for (int ck = 0; ck < 4; ck++) {
+    /* 2. conv1 (stride 1) as an im2col GEMM, 2 chunks of 16 output rows */
+    for (int ck = 0; ck < 2; ck++) {
       {
-        const int y = ck * 8 + (tid >> 5), x = tid & 31;
+        const int y = ck * 16 + (tid >> 5), x = tid & 31;
         uint32_t wv[16];
 #pragma unroll
         for (int tap = 0; tap < 9; tap++) wv[tap] = sIn[(y + tap / 3) * 34 + x + tap % 3];
@@ -506,7 +508,7 @@ static __global__ void __launch_bounds__(256, 1) k_pn_infer(const void* __restri
 #pragma unroll
         for (int h = 0; h < 2; h++) {
           const int pl = mt * 16 + g + 8 * h; /* chunk-local pixel */
-          const int row = (ck * 8 + (pl >> 5) + 1) * 34 + (pl & 31) + 1;
+          const int row = (ck * 16 + (pl >> 5) + 1) * 34 + (pl & 31) + 1;
 #pragma unroll
           for (int t = 0; t < 4; t++) {
             const int ch = t * 8 + t2;
@@ -518,10 +520,9 @@ static __global__ void __launch_bounds__(256, 1) k_pn_infer(const void* __restri
       __syncthreads();
     }
 
-    /* 3. conv2: 16x16 outputs, m-tile = output row, warp takes rows w, w+8 */
-#pragma unroll 1
-    for (int mi = 0; mi < 2; mi++) {
-      const int oy = warp + 8 * mi;
+    /* 3. conv2: 16x16 outputs, m-tile = output row, one per warp */
+    {
+      const int oy = warp;
       float acc[4][4];
       conv_s2_mtile<2>(sAct1, 34, oy, arl, sW2, 0, acc, lane);
 #pragma unroll
@@ -537,8 +538,8 @@ static __global__ void __launch_bounds__(256, 1) k_pn_infer(const void* __restri
     }
     __syncthreads();
 
-    /* 4. conv3: 8x8 outputs = 4 m-tiles; warp: m-tile w/2, n-tiles 2(w&1).. */
-    {
+    /* 4. conv3: 8x8 outputs = 4 m-tiles; warp (< 8): m-tile w/2, n-tiles 2(w&1).. */
+    if (warp < 8) {
       const int mt = warp >> 1, np0 = warp & 1;
       const int px = mt * 16 + arl;
       float acc[2][4];
@@ -623,48 +624,61 @@ __host__ __device__ inline NarrowLayout narrow_layout(const DGeom& g, float radi
   return L;
 }
 
-/* One warp's share of a column of candidates: displacements (dx, dy0 +
-   k*hy), k < nk (<= 8), relative to the staged window's origin, summed over
-   field rows [r0, r1).  A lane owns one word of the field row (several rows
-   at once when a row has fewer than 32 words), loads the field word once per
+/* One warp's share of a column of NK candidates: displacements (dx, dy0 +
+   k*hy), k < NK, relative to the staged window's origin, summed over field
+   rows [r0, r1).  A lane owns one word of the field row (several rows at
+   once when a row has fewer than 32 words), loads the field word once per
    row and applies it to every candidate of the column; partial sums are
    added to sums[k] in shared memory. */
+template <int NK>
 __device__ __forceinline__ void sad_column(const uint32_t* __restrict__ C, int rowW,
                                            const uint8_t* __restrict__ win, int WP, int e, int bpp,
-                                           int dx, int dy0, int hy, int nk, int r0, int r1,
-                                           int lane, unsigned* sums) {
-  unsigned acc[8];
+                                           int dx, int dy0, int hy, int r0, int r1, int lane,
+                                           unsigned* sums) {
+  unsigned acc[NK];
 #pragma unroll
-  for (int k = 0; k < 8; k++) acc[k] = 0;
+  for (int k = 0; k < NK; k++) acc[k] = 0;
   const int bx = e + dx * bpp;
   const int sh = (bx & 3) << 3;
   const int WPw = WP >> 2;
   const int G = rowW < 32 ? 32 / rowW : 1;
   const int g = rowW < 32 ? lane / rowW : 0;
   const int w0 = rowW < 32 ? lane - g * rowW : lane;
-  const int wstep = rowW < 32 ? 32 : 32;
+  const int hyw = hy * WPw;
   if (g < G) {
-    for (int w = w0; w < rowW; w += wstep) {
+    for (int w = w0; w < rowW; w += 32) {
       const uint32_t* Cw = C + w;
       const uint32_t* Pw = (const uint32_t*)win + (bx >> 2) + w;
       for (int r = r0 + g; r < r1; r += G) {
         const uint32_t c = Cw[r * rowW];
         const uint32_t* P = Pw + (r + dy0) * WPw;
 #pragma unroll
-        for (int k = 0; k < 8; k++)
-          if (k < nk) {
-            const uint32_t* Q = P + k * hy * WPw;
-            acc[k] = sad4(c, __funnelshift_r(Q[0], Q[1], sh), acc[k]);
-          }
+        for (int k = 0; k < NK; k++) {
+          const uint32_t* Q = P + k * hyw;
+          acc[k] = sad4(c, __funnelshift_r(Q[0], Q[1], sh), acc[k]);
+        }
       }
     }
   }
 #pragma unroll
-  for (int k = 0; k < 8; k++)
-    if (k < nk) {
-      const unsigned v = __reduce_add_sync(0xffffffffu, acc[k]);
-      if (lane == 0) atomicAdd(&sums[k], v);
-    }
+  for (int k = 0; k < NK; k++) {
+    const unsigned v = __reduce_add_sync(0xffffffffu, acc[k]);
+    if (lane == 0) atomicAdd(&sums[k], v);
+  }
+}
+
+__device__ __forceinline__ void sad_column_n(int nk, const uint32_t* C, int rowW,
+                                             const uint8_t* win, int WP, int e, int bpp, int dx,
+                                             int dy0, int hy, int r0, int r1, int lane,
+                                             unsigned* sums) {
+#define VSB_SADCOL(K) \
+  case K: sad_column<K>(C, rowW, win, WP, e, bpp, dx, dy0, hy, r0, r1, lane, sums); break;
+  switch (nk) {
+    VSB_SADCOL(1) VSB_SADCOL(2) VSB_SADCOL(3) VSB_SADCOL(4)
+    VSB_SADCOL(5) VSB_SADCOL(6) VSB_SADCOL(7) VSB_SADCOL(8)
+    default: break;
+  }
+#undef VSB_SADCOL
 }
 
 /* The SADs of a grid of candidates: columns i < ncol at dx0 + i*hx, rows
@@ -687,8 +701,8 @@ __device__ __forceinline__ void sad_grid(const uint32_t* C, int rowW, int S, con
     const int k0 = ch * 8, nk = min(8, nrow - k0);
     const int r0 = sidx * rs, r1 = min(S, r0 + rs);
     if (r0 < r1)
-      sad_column(C, rowW, win, WP, e, bpp, dx0 + col * hx, dy0 + k0 * hy, hy, nk, r0, r1, lane,
-                 sums + col * nrow + k0);
+      sad_column_n(nk, C, rowW, win, WP, e, bpp, dx0 + col * hx, dy0 + k0 * hy, hy, r0, r1, lane,
+                   sums + col * nrow + k0);
   }
   __syncthreads();
 }
@@ -776,22 +790,31 @@ static __global__ void __launch_bounds__(512) k_pn_narrow(const uint8_t* __restr
     }
   }
   __syncthreads();
-  /* lattice window: column a - wal, row b - wbl at sums[(a-wal)*wb + (b-wbl)] */
+  /* lattice window: column a - wal, row b - wbl at sums[(a-wal)*wb + (b-wbl)];
+     the lowest (SAD, visiting rank) by a block-wide reduction */
   sad_grid(C, L.rowW, g.S, win, L.WP, e, g.bpp, L.R, g.step, wa, L.R, g.step, wb, qsad);
-  if (threadIdx.x == 0) {
+  {
+    __shared__ unsigned long long red[16];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned long long best = ~0ull;
-    for (int q = 0; q < wa * wb; q++) {
+    for (int q = threadIdx.x; q < wa * wb; q += blockDim.x) {
       const int a = wal + q / wb, b = wbl + q % wb;
       const unsigned long long key =
           ((unsigned long long)qsad[q] << 32) | (unsigned)g.order[b * g.na + a];
       best = key < best ? key : best;
     }
-    const short2 pt = g.point[(unsigned)(best & 0xffffffffu)];
-    s_min = (unsigned)(best >> 32);
-    s_tx = pt.x;
-    s_ty = pt.y;
+    best = warp_min64(best);
+    if (lane == 0) red[warp] = best;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int w = 1; w < (int)(blockDim.x >> 5); w++) best = red[w] < best ? red[w] : best;
+      const short2 pt = g.point[(unsigned)(best & 0xffffffffu)];
+      s_min = (unsigned)(best >> 32);
+      s_tx = pt.x;
+      s_ty = pt.y;
+    }
+    __syncthreads();
   }
-  __syncthreads();
   const int aw = (s_tx - g.ax0) / g.step, bw = (s_ty - g.by0) / g.step;
   const bool ring = aw < alo || aw > ahi || bw < blo || bw > bhi;
   /* refinement rounds around the winner, inside the staged window: the
@@ -897,7 +920,7 @@ int vsbpn_infer(const void* d_params, const uint8_t* curr, const uint8_t* prev, 
   if (n <= 0) return 0;
   PCK(pn_ensure_smem((const void*)k_pn_infer, 0, PI_SMEM));
   const int grid = min(n, sm_count_cached());
-  k_pn_infer<<<grid, 256, PI_SMEM, st>>>(d_params, curr, prev, pitch, W, H, items,
+  k_pn_infer<<<grid, PI_THREADS, PI_SMEM, st>>>(d_params, curr, prev, pitch, W, H, items,
                                          (const uint32_t*)prepared, n, out);
   PCK(cudaGetLastError());
   return 1;

@@ -64,7 +64,7 @@ def _L():
         L.vsb_set_proposal_ex.restype = i
         L.vsb_set_proposal_ex.argtypes = [p, p, l_, C.c_double, C.c_double, C.c_double]
         L.vsb_set_proposal_scope.restype = i
-        L.vsb_set_proposal_scope.argtypes = [p, i]
+        L.vsb_set_proposal_scope.argtypes = [p, i, C.c_double]
         L.vsb_set_proposal_verify.restype = i
         L.vsb_set_proposal_verify.argtypes = [p, i]
         L.vsb_proposal_stats.restype = i
@@ -125,13 +125,13 @@ def zero_blob(radius=2.0, conf_logit=10.0, match_bound=64.0):
 
 
 def set_proposal(det, blob, radius=-1.0, conf_min=float("nan"), match_bound=-1.0, verify=False,
-                 fine_net=False):
+                 fine_net=False, fine_radius=-1.0):
     """Gives a MotionDetector the proposal (blob None: back to plain)."""
     L = _L()
     buf = C.create_string_buffer(blob, len(blob)) if blob is not None else None
     _check(L.vsb_set_proposal_ex(C.byref(det.md), buf, len(blob) if blob else 0, radius,
                                  conf_min, match_bound), "vsb_set_proposal_ex")
-    _check(L.vsb_set_proposal_scope(C.byref(det.md), 1 if fine_net else 0),
+    _check(L.vsb_set_proposal_scope(C.byref(det.md), 1 if fine_net else 0, fine_radius),
            "vsb_set_proposal_scope")
     _check(L.vsb_set_proposal_verify(C.byref(det.md), 1 if verify else 0), "vsb_set_proposal_verify")
 
