@@ -488,10 +488,10 @@ def main():
         hbm, src = peaks()
         bb = 2.0 * W * H
         t_blur = kernel_ms["blur"] * 1e-3
-        roof_hbm = {"kernel": "k_blur (prefilter, 1080p)", "bound": "hbm",
+        roof_hbm = {"kernel": "k_blur_fast (prefilter, 1080p)", "bound": "hbm",
                     "achieved": bb / t_blur / 1e9, "peak": hbm, "unit": "GB/s",
                     "frac": bb / t_blur / 1e9 / hbm, "peak_source": src,
-                    "traffic": traffic_from_profile("k_blur_1080p.md")}
+                    "traffic": traffic_from_profile("k_blur_fast_1080p.md")}
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
