@@ -75,6 +75,20 @@ VS_API long vsb_detect_run(struct _vsmotiondetect* md, const uint8_t* frames, lo
                            int linesize, int nframes, int on_device, void* out, long out_cap,
                            int* counts);
 
+/* Many initialised detectors (one per stream, any mix of resolutions, with
+   or without a search proposal) stepped together by the calling thread:
+   every frame, the coarse stage of every detector is enqueued before any is
+   waited for, so the streams' GPU work overlaps while the host selects and
+   assembles the others' motions.  Frame k of stream s at clips[s] + k *
+   frame_bytes[s] (host memory, or device memory with on_device), row pitch
+   linesizes[s].  Records are appended frame by frame, stream by stream
+   (LocalMotion layout, at most out_cap); counts[k*n + s] receives each
+   frame's count.  Each stream's motions are its detector's own.  Returns
+   the number of records, or -1. */
+VS_API long vsb_detect_multi(struct _vsmotiondetect** mds, int n, const uint8_t* const* clips,
+                             const long* frame_bytes, const int* linesizes, int nframes,
+                             int on_device, void* out, long out_cap, int* counts);
+
 /* Per-kernel device time: with timing on, CUDA events bracket every kernel
    of the detector on its stream.  ms[k] and count[k] for k = 0 blur,
    1 field min/max, 2 coarse search, 3 fine search, 4 proposal network,
@@ -211,6 +225,13 @@ VS_API int vsb_set_proposal_ex(struct _vsmotiondetect* md, const void* blob, lon
    fields' window radius in pixels (at most 16; negative: 4 px around the
    model, the blob's radius around the network). */
 VS_API int vsb_set_proposal_scope(struct _vsmotiondetect* md, int fine_net, double fine_radius);
+/* Network passes over the coarse fields: 1, or 2 -- the first pass's
+   predictions give the frame a global motion model (median translation,
+   least-squares rotation about the centre); the second pass re-centres
+   every coarse crop on the model and predicts the residual.  For motions
+   beyond the network's reach (64x64 crops).  vsb_set_proposal picks 2 when
+   the detector's shakiness is 8 or more, else 1. */
+VS_API int vsb_set_proposal_passes(struct _vsmotiondetect* md, int passes);
 /* With verify on, every stage also runs the full search of every item and
    counts the items whose result (SAD, shift, range test) is identical. */
 VS_API int vsb_set_proposal_verify(struct _vsmotiondetect* md, int on);

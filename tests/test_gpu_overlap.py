@@ -71,3 +71,39 @@ def test_overlapped_with_proposal():
     pnet.set_proposal(b, blob)
     got, gc = _run(b, clip.data_ptr(), n, w, h, True)
     assert np.array_equal(gc, ec) and np.array_equal(got, exp)
+
+
+def test_multi_detectors_equal_their_own_runs():
+    """vsb_detect_multi: mixed resolutions, one detector with the proposal and
+    its two-pass prior, one in tripod mode; every stream's motions are its
+    own detector's"""
+    sizes = [(640, 360), (1920, 1080), (1280, 720)]
+    n = 6
+    clips = [S.clip(w, h, n, seed=40 + i, device="cuda") for i, (w, h) in enumerate(sizes)]
+    blob = pnet.load_blob()
+
+    def make(i):
+        w, h = sizes[i]
+        d = V.MotionDetector(w, h, V.PF_YUV420P, tripod=2 if i == 2 else 0)
+        if i == 1:
+            pnet.set_proposal(d, blob, passes=2)
+        return d
+
+    exp = []
+    for i, (w, h) in enumerate(sizes):
+        d = make(i)
+        exp.append(_per_frame(d, clips[i], w, h))
+        d.close()
+    dets = [make(i) for i in range(len(sizes))]
+    out = np.zeros(n * len(sizes) * 800, V.LM_DTYPE)
+    counts = np.zeros(n * len(sizes), np.int32)
+    tot = V.detect_multi(dets, [c.data_ptr() for c in clips], [w * h for w, h in sizes],
+                         [w for w, _ in sizes], n, True, out, counts)
+    cm = counts.reshape(n, len(sizes))
+    pos = np.concatenate([[0], np.cumsum(cm.ravel())])
+    assert pos[-1] == tot
+    for s in range(len(sizes)):
+        got = np.concatenate([out[pos[k * len(sizes) + s]:pos[k * len(sizes) + s + 1]]
+                              for k in range(n)])
+        assert np.array_equal(cm[:, s], exp[s][1])
+        assert np.array_equal(got, exp[s][0])

@@ -65,3 +65,15 @@ def test_network_gain_large_shake():
     _, _, zero = _run(c, pnet.zero_blob())
     assert learned["agreement"] >= 0.995
     assert learned["coarse_fell_back"] < zero["coarse_fell_back"], (learned, zero)
+
+
+def test_two_pass_prior_large_shake():
+    """the second network pass around the frame's global motion model (the
+    default for shakiness >= 8) keeps more coarse fields on the narrowed
+    search under large camera steps, with the same agreement"""
+    c = S.clip(W, H, 16, seed=403, device="cuda", trans_sigma=8.0, rot_sigma_deg=0.5)
+    blob = pnet.load_blob()
+    _, _, one = _run(c, blob, passes=1)
+    _, _, two = _run(c, blob, passes=2)
+    assert two["agreement"] >= 0.995, two
+    assert two["coarse_fell_back"] < one["coarse_fell_back"], (one, two)

@@ -168,6 +168,13 @@ long vsb_detect_run(VSMotionDetect* md, const uint8_t* frames, long frame_bytes,
   return total;
 }
 
+long vsb_detect_multi(VSMotionDetect** mds, int n, const uint8_t* const* clips,
+                      const long* frame_bytes, const int* linesizes, int nframes, int on_device,
+                      void* out, long out_cap, int* counts) {
+  return vsb_detect_multi_impl(mds, n, clips, frame_bytes, linesizes, nframes, on_device,
+                               (LocalMotion*)out, out_cap, counts);
+}
+
 int vsb_boxblur_host(uint8_t* dst, const uint8_t* src, int width, int height, int size) {
   return vsbd_blur_host(dst, src, width, height, size) == 0 ? VS_OK : VS_ERROR;
 }

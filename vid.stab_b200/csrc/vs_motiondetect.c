@@ -795,6 +795,74 @@ long vsb_detect_run_overlapped(VSMotionDetect* md, const uint8_t* frames, long f
   return total;
 }
 
+/* Many detectors stepped together by one host thread: for each frame, the
+   stage A of every detector is enqueued before any is collected, then each
+   detector's host part A runs and its fine stage is enqueued, then each fine
+   stage is collected and its motions assembled.  The GPU overlaps the
+   streams' stages while the host works on the others.  Same results, stream
+   by stream, as each detector's own frame loop.  Records are appended frame
+   by frame, detector by detector; counts[k*n + s].  Returns the number of
+   records, or -1. */
+long vsb_detect_multi_impl(VSMotionDetect** mds, int n, const uint8_t* const* clips,
+                      const long* frame_bytes, const int* linesizes, int nframes, int on_device,
+                      LocalMotion* rec, long out_cap, int* counts) {
+  long total = 0;
+  if (!mds || n < 1 || !clips || !frame_bytes || !linesizes || nframes < 0) return -1;
+  md_state** st = (md_state**)malloc(sizeof(md_state*) * (size_t)n);
+  vsb_frame_work* w = (vsb_frame_work*)malloc(sizeof(vsb_frame_work) * (size_t)n);
+  int* search = (int*)malloc(sizeof(int) * (size_t)n);
+  int* ok = (int*)calloc((size_t)n, sizeof(int));
+  long rc = -1;
+  if (!st || !w || !search || !ok) goto done;
+  for (int s = 0; s < n; s++)
+    if (!(st[s] = state_find(mds[s]))) goto done;
+  for (int k = 0; k < nframes; k++) {
+    for (int s = 0; s < n; s++) {
+      const uint8_t* src = clips[s] + (size_t)k * frame_bytes[s];
+      if (vsb_frame_begin(mds[s], &search[s]) != VS_OK ||
+          vsbd_stage_a_issue(st[s]->dev, on_device ? NULL : src, linesizes[s],
+                             on_device ? src : NULL, linesizes[s], search[s]) != 0) {
+        vs_log_error(mds[s]->conf.modName, "GPU stage A failed: %s\n", vsbd_error());
+        goto done;
+      }
+    }
+    for (int s = 0; s < n; s++) {
+      const uint8_t* mm = NULL;
+      const vsbd_result* cres = NULL;
+      ok[s] = 0;
+      if (vsbd_stage_a_next_collect(st[s]->dev, &mm, &cres) != 0) goto done;
+      if (!search[s]) continue;
+      vsb_frame_host_a(mds[s], mm, cres, &w[s]);
+      ok[s] = 1;
+      if (vsbd_stage_b_issue(st[s]->dev, w[s].items, w[s].fine_pass ? w[s].nitems : 0) != 0)
+        goto done;
+    }
+    for (int s = 0; s < n; s++) {
+      LocalMotions lms;
+      if (search[s]) {
+        const vsbd_result* fres = NULL;
+        if (vsbd_stage_b_collect(st[s]->dev, &fres) != 0) goto done;
+        vsb_frame_host_b(mds[s], fres, &w[s], &lms);
+        ok[s] = 0;
+      } else {
+        vsb_frame_first(mds[s], &lms);
+      }
+      if (vsb_frame_end(mds[s])) vsbd_commit_prev(st[s]->dev);
+      total = append_records(&lms, rec, total, out_cap, counts ? counts + (size_t)k * n + s : NULL);
+    }
+  }
+  rc = total;
+done:
+  if (rc < 0 && w && ok)
+    for (int s = 0; s < n; s++)
+      if (ok[s]) vsb_frame_discard(&w[s]);
+  free(st);
+  free(w);
+  free(search);
+  free(ok);
+  return rc;
+}
+
 int vsMotionDetection(VSMotionDetect* md, LocalMotions* motions, VSFrame* frame) {
   if (!md || !frame || !frame->data[0]) return VS_ERROR;
   md->currorig = *frame;

@@ -56,6 +56,9 @@ int vsb_set_proposal_ex(VSMotionDetect* md, const void* blob, long bytes, double
     vsbd_set_error("proposal network: not a version-1 VSBP blob of this architecture");
     return VS_ERROR;
   }
+  /* very shaky footage (shakiness >= 8): the second pass around the global
+     model keeps large motions inside the network's reach */
+  if (vsbd_set_proposal_passes(c, md->conf.shakiness >= 8 ? 2 : 1) != 0) return VS_ERROR;
   double r = radius >= 0 ? radius : h.radius;
   double cm = isnan(conf_min) ? h.conf_min : conf_min;
   double mb = match_bound >= 0 ? match_bound : h.match_bound;
@@ -72,6 +75,10 @@ int vsb_set_proposal(VSMotionDetect* md, const void* blob, long bytes) {
 int vsb_set_proposal_scope(VSMotionDetect* md, int fine_net, double fine_radius) {
   return vsbd_set_proposal_scope(vsb_md_device(md), fine_net, (float)fine_radius) == 0 ? VS_OK
                                                                                        : VS_ERROR;
+}
+
+int vsb_set_proposal_passes(VSMotionDetect* md, int passes) {
+  return vsbd_set_proposal_passes(vsb_md_device(md), passes) == 0 ? VS_OK : VS_ERROR;
 }
 
 int vsb_set_proposal_verify(VSMotionDetect* md, int on) {

@@ -805,6 +805,9 @@ struct vsbd_ctx {
   int pn_fine_net;              /* fine fields: 1 network proposal, 0 the coarse model's
                                    prediction (zero residual) */
   float pn_fine_radius;         /* window radius of the fine fields (< 0: the default) */
+  int pn_passes;                /* coarse fields: 1 network pass, 2 with a global prior */
+  vsbd_item* d_citems2;         /* second-pass items (coarse fields, prior as offset) */
+  short2* d_prior;              /* per coarse field, the rounded global-model displacement */
   float* d_pout;                /* network outputs [nc + nf][3] */
   vsbd_result* d_vres;          /* verify: full-search results, coarse then fine */
   vsbd_result* h_vres;
@@ -906,6 +909,8 @@ extern "C" void vsbd_destroy(vsbd_ctx* c) {
   cudaFree(c->d_pn);
   cudaFree(c->d_pout);
   cudaFree(c->d_fbl);
+  cudaFree(c->d_citems2);
+  cudaFree(c->d_prior);
   cudaFree(c->d_vres);
   if (c->h_vres) cudaFreeHost(c->h_vres);
   geom_free(&c->gc);
@@ -961,6 +966,7 @@ extern "C" int vsbd_create(vsbd_ctx** out, int W, int H, int bpp, int blur_size,
   c->cur = 0;
   c->prv = 1;
   c->pn_fine_radius = -1.f;
+  c->pn_passes = 1;
   CKC(cudaStreamCreateWithFlags(&c->st2, cudaStreamNonBlocking));
   CKC(cudaEventCreateWithFlags(&c->ev_a, cudaEventDisableTiming));
   CKC(cudaEventCreateWithFlags(&c->ev_b, cudaEventDisableTiming));
@@ -1057,14 +1063,27 @@ static int learned_search(vsbd_ctx* c, const GeomDev& gd, const GeomDev& gfull, 
                           vsbd_result* res, uint8_t* fb, int* fbl) {
   if (n <= 0) return 0;
   float* pout = NULL;
+  const short2* prior = NULL;
   if (base == 0 || c->pn_fine_net) {
     pout = c->d_pout + (size_t)3 * base;
     kt_begin(c, VSBD_KT_PNET, st);
     if (vsbpn_infer(c->d_pn, cur, prv, c->pitch, c->W, c->H, items, NULL, n, pout, st) < 0)
       return -1;
-    kt_end(c, VSBD_KT_PNET, st);
     c->launches++;
     count_launches(1);
+    if (base == 0 && c->pn_passes == 2) {
+      /* second pass: every coarse field's crop re-centred on the frame's
+         global motion model from the first pass; the proposal is the model
+         plus the second prediction */
+      if (vsbpn_prior(items, pout, n, c->pn.scale, c->pn.conf_min, skip, c->W, c->H, c->d_citems2,
+                      c->d_prior, st) < 0 ||
+          vsbpn_infer(c->d_pn, cur, prv, c->pitch, c->W, c->H, c->d_citems2, NULL, n, pout, st) < 0)
+        return -1;
+      prior = c->d_prior;
+      c->launches += 2;
+      count_launches(2);
+    }
+    kt_end(c, VSBD_KT_PNET, st);
   }
   const int kt = base == 0 ? VSBD_KT_COARSE : VSBD_KT_FINE;
   kt_begin(c, kt, st);
@@ -1076,7 +1095,8 @@ static int learned_search(vsbd_ctx* c, const GeomDev& gd, const GeomDev& gfull, 
   const double bound = (double)c->pn_match_bound * gd.g.S * gd.g.S;
   ps.sad_bound = bound >= 4294967295.0 ? 0xffffffffu : (unsigned)bound;
   CK(cudaMemsetAsync(fbl, 0, sizeof(int), st));
-  if (vsbpn_narrow(gd.g, cur, prv, c->pitch, items, n, pout, ps, skip, res, fb, fbl, fbl + 1, st) < 0)
+  if (vsbpn_narrow(gd.g, cur, prv, c->pitch, items, n, pout, prior, ps, skip, res, fb, fbl, fbl + 1,
+                   st) < 0)
     return -1;
   kt_end(c, kt, st);
   kt_begin(c, VSBD_KT_FALLBACK, st);
@@ -1237,6 +1257,12 @@ extern "C" int vsbd_stage_a(vsbd_ctx* c, const uint8_t* host, int linesize, cons
   return stage_a_collect(c, minmax, coarse);
 }
 
+extern "C" int vsbd_stage_a_issue(vsbd_ctx* c, const uint8_t* host, int linesize,
+                                  const uint8_t* dev, int pitch, int search) {
+  CK(cudaSetDevice(c->dev));
+  return stage_a_issue(c, host, linesize, dev, pitch, search, c->cur, c->prv);
+}
+
 extern "C" int vsbd_stage_a_next_issue(vsbd_ctx* c, const uint8_t* host, int linesize,
                                        const uint8_t* dev, int pitch) {
   CK(cudaSetDevice(c->dev));
@@ -1352,6 +1378,8 @@ extern "C" int vsbd_set_proposal(vsbd_ctx* c, const void* params, float scale, f
   if (!c->d_pn) CK(cudaMalloc(&c->d_pn, PN_PARAM_BYTES));
   if (!c->d_pout) CK(cudaMalloc(&c->d_pout, sizeof(float) * 3 * (c->nc + c->nf + 1)));
   if (!c->d_fbl) CK(cudaMalloc(&c->d_fbl, sizeof(int) * (c->nc + c->nf + 4)));
+  if (!c->d_citems2) CK(cudaMalloc(&c->d_citems2, sizeof(vsbd_item) * (c->nc + 1)));
+  if (!c->d_prior) CK(cudaMalloc(&c->d_prior, sizeof(short2) * (c->nc + 1)));
   CK(cudaMemcpy(c->d_pn, params, PN_PARAM_BYTES, cudaMemcpyHostToDevice));
   /* the full search of the items that fall back: a tiling for a handful of
      items, so that one item's lattice is spread over many CTAs (the
@@ -1409,6 +1437,15 @@ extern "C" int vsbd_set_proposal_scope(vsbd_ctx* c, int fine_net, float fine_rad
   }
   c->pn_fine_net = fine_net ? 1 : 0;
   c->pn_fine_radius = fine_radius;
+  return 0;
+}
+
+extern "C" int vsbd_set_proposal_passes(vsbd_ctx* c, int passes) {
+  if (!c || passes < 1 || passes > 2) {
+    set_msg("proposal passes must be 1 or 2");
+    return -1;
+  }
+  c->pn_passes = passes;
   return 0;
 }
 

@@ -89,6 +89,11 @@ void vsbd_commit_prev(vsbd_ctx* c);
    searched against the current frame's) and collected after the commit
    (vsbd_stage_a_next_collect).  Only when vsbd_can_overlap(c). */
 int vsbd_can_overlap(const vsbd_ctx* c);
+/* stage A of the current frame, enqueued only (collect with
+   vsbd_stage_a_next_collect): lets one host thread keep several detectors'
+   stages in flight */
+int vsbd_stage_a_issue(vsbd_ctx* c, const uint8_t* host, int linesize, const uint8_t* dev,
+                       int pitch, int search);
 int vsbd_stage_a_next_issue(vsbd_ctx* c, const uint8_t* host, int linesize, const uint8_t* dev,
                             int pitch);
 int vsbd_stage_a_next_collect(vsbd_ctx* c, const uint8_t** minmax, const vsbd_result** coarse);
@@ -124,6 +129,9 @@ long vsbd_pnet_param_bytes(void);
    their window radius in pixels (< 0: 4 px around the model, the blob's
    radius around the network) */
 int vsbd_set_proposal_scope(vsbd_ctx* c, int fine_net, float fine_radius);
+/* coarse fields: 1 network pass, or 2 (the second with crops re-centred on
+   the global motion model fitted to the first pass's predictions) */
+int vsbd_set_proposal_passes(vsbd_ctx* c, int passes);
 /* with verify on, every stage also runs the full search and compares */
 int vsbd_set_proposal_verify(vsbd_ctx* c, int on);
 /* [0] items searched with a proposal, [1] of them fell back, [2] items

@@ -80,6 +80,10 @@ long vsb_detect_run_overlapped(VSMotionDetect* md, const uint8_t* frames, long f
                                int linesize, int nframes, int on_device, LocalMotion* rec,
                                long out_cap, int* counts);
 
+long vsb_detect_multi_impl(VSMotionDetect** mds, int n, const uint8_t* const* clips,
+                           const long* frame_bytes, const int* linesizes, int nframes,
+                           int on_device, LocalMotion* rec, long out_cap, int* counts);
+
 /* device context of an initialised detector (NULL if none) */
 vsbd_ctx* vsb_md_device(const VSMotionDetect* md);
 

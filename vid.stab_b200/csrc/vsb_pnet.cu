@@ -722,6 +722,7 @@ static __global__ void __launch_bounds__(512) k_pn_narrow(const uint8_t* __restr
                                                           int pitch, DGeom g,
                                                           const vsbd_item* __restrict__ items,
                                                           const float* __restrict__ pout,
+                                                          const short2* __restrict__ prior,
                                                           PNSearch ps,
                                                           const uint8_t* __restrict__ skip,
                                                           vsbd_result* __restrict__ res,
@@ -734,7 +735,9 @@ static __global__ void __launch_bounds__(512) k_pn_narrow(const uint8_t* __restr
   const int item = blockIdx.x;
   const NarrowLayout L = narrow_layout(g, ps.radius);
   const float* po = pout ? pout + item * 3 : NULL;
-  const float px = po ? po[0] * ps.scale : 0.f, py = po ? po[1] * ps.scale : 0.f;
+  const short2 base = prior ? prior[item] : make_short2(0, 0);
+  const float px = (po ? po[0] * ps.scale : 0.f) + (float)base.x;
+  const float py = (po ? po[1] * ps.scale : 0.f) + (float)base.y;
   const float cf = po ? po[2] : 3.0e38f;
   /* the bracket [lo, hi] of lattice indices covering prediction +- radius */
   int alo = 1, ahi = 0, blo = 1, bhi = 0;
@@ -858,6 +861,100 @@ static __global__ void __launch_bounds__(512) k_pn_narrow(const uint8_t* __restr
   }
 }
 
+/* Global motion prior of a frame's coarse items from the first network
+   pass.  Translation: the per-axis median of the confident predictions (the
+   non-skipped items with a finite prediction and a logit >= conf_min; all
+   non-skipped items if fewer than three are confident).  Rotation: the small
+   angle about the frame centre that best fits, in least squares, the
+   predictions within 8 px of that translation.  Every item gets the model's
+   displacement at its centre, rounded: the search offset of its second
+   network pass (items2) and the base of its proposal (prior).  One CTA. */
+#define PN_PRIOR_MAX 1024
+static __global__ void __launch_bounds__(256) k_pn_prior(const vsbd_item* __restrict__ items,
+                                                         const float* __restrict__ pout, int n,
+                                                         float scale, float conf_min,
+                                                         const uint8_t* __restrict__ skip,
+                                                         float cx, float cy,
+                                                         vsbd_item* __restrict__ items2,
+                                                         short2* __restrict__ prior) {
+  __shared__ float vx[PN_PRIOR_MAX], vy[PN_PRIOR_MAX], jx[PN_PRIOR_MAX], jy[PN_PRIOR_MAX];
+  __shared__ int m;
+  __shared__ float med[2];
+  __shared__ float sums[2][8];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int pass = 0; pass < 2; pass++) {
+    if (tid == 0) m = 0;
+    __syncthreads();
+    for (int i = tid; i < n; i += blockDim.x) {
+      if (skip && skip[i]) continue;
+      const float px = pout[3 * i] * scale, py = pout[3 * i + 1] * scale, c = pout[3 * i + 2];
+      if (!isfinite(px) || !isfinite(py) || fabsf(px) > 4096.f || fabsf(py) > 4096.f) continue;
+      if (pass == 0 && !(c >= conf_min)) continue;
+      const int k = atomicAdd(&m, 1);
+      if (k < PN_PRIOR_MAX) {
+        vx[k] = px;
+        vy[k] = py;
+        jx[k] = -((float)items[i].y - cy); /* d(displacement)/d(angle) at the centre */
+        jy[k] = (float)items[i].x - cx;
+      }
+    }
+    __syncthreads();
+    if (m >= 3 || pass == 1) break;
+    __syncthreads();
+  }
+  const int cnt = min(m, PN_PRIOR_MAX);
+  /* per-axis medians: the element whose rank (ties by index) is cnt/2 */
+  if (tid == 0) med[0] = med[1] = 0.f;
+  __syncthreads();
+  for (int t = tid; t < 2 * cnt; t += blockDim.x) {
+    const int ax = t >= cnt, k = t - ax * cnt;
+    const float* v = ax ? vy : vx;
+    const float x = v[k];
+    int rank = 0;
+    for (int j = 0; j < cnt; j++) rank += v[j] < x || (v[j] == x && j < k);
+    if (rank == cnt / 2) med[ax] = x;
+  }
+  __syncthreads();
+  /* rotation about the centre from the inliers of the translation */
+  float num = 0.f, den = 0.f;
+  for (int k = tid; k < cnt; k += blockDim.x) {
+    const float rx = vx[k] - med[0], ry = vy[k] - med[1];
+    if (fabsf(rx) < 8.f && fabsf(ry) < 8.f) {
+      num += rx * jx[k] + ry * jy[k];
+      den += jx[k] * jx[k] + jy[k] * jy[k];
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    num += __shfl_xor_sync(0xffffffffu, num, o);
+    den += __shfl_xor_sync(0xffffffffu, den, o);
+  }
+  if (lane == 0) {
+    sums[0][warp] = num;
+    sums[1][warp] = den;
+  }
+  __syncthreads();
+  float th = 0.f;
+  {
+    float a = 0.f, b = 0.f;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+      a += sums[0][w];
+      b += sums[1][w];
+    }
+    if (b > 0.f) th = fminf(fmaxf(a / b, -0.05f), 0.05f);
+  }
+  for (int i = tid; i < n; i += blockDim.x) {
+    const vsbd_item it = items[i];
+    const float dx = med[0] + th * -((float)it.y - cy), dy = med[1] + th * ((float)it.x - cx);
+    const int ox = (int)rintf(fminf(fmaxf(dx, -4000.f), 4000.f));
+    const int oy = (int)rintf(fminf(fmaxf(dy, -4000.f), 4000.f));
+    vsbd_item o = it;
+    o.ox = (int16_t)ox;
+    o.oy = (int16_t)oy;
+    items2[i] = o;
+    prior[i] = make_short2((short)ox, (short)oy);
+  }
+}
+
 static __global__ void k_pn_labels(const vsbd_result* __restrict__ res,
                                    const uint8_t* __restrict__ skip, int n, int kind,
                                    PNLabel* __restrict__ out) {
@@ -927,17 +1024,17 @@ int vsbpn_infer(const void* d_params, const uint8_t* curr, const uint8_t* prev, 
 }
 
 int vsbpn_narrow(const DGeom& g, const uint8_t* curr, const uint8_t* prev, int pitch,
-                 const vsbd_item* items, int n, const float* pout, const PNSearch& ps,
-                 const uint8_t* skip, vsbd_result* res, uint8_t* fb, int* fb_count,
-                 int* fb_list, cudaStream_t st) {
+                 const vsbd_item* items, int n, const float* pout, const short2* prior,
+                 const PNSearch& ps, const uint8_t* skip, vsbd_result* res, uint8_t* fb,
+                 int* fb_count, int* fb_list, cudaStream_t st) {
   if (n <= 0) return 0;
   if (g.has_origin) return pn_msg("the narrowed search serves planar field sets only");
   if (narrow_span(ps.radius, g.step) * narrow_span(ps.radius, g.step) > PN_NARROW_QMAX)
     return pn_msg("proposal radius too large for the narrowed search");
   const size_t smem = narrow_layout(g, ps.radius).total;
   if (smem > 48 * 1024) PCK(pn_ensure_smem((const void*)k_pn_narrow, 1, smem));
-  k_pn_narrow<<<n, 512, smem, st>>>(curr, prev, pitch, g, items, pout, ps, skip, res, fb, fb_count,
-                                    fb_list);
+  k_pn_narrow<<<n, 512, smem, st>>>(curr, prev, pitch, g, items, pout, prior, ps, skip, res, fb,
+                                    fb_count, fb_list);
   PCK(cudaGetLastError());
   return 1;
 }
@@ -956,6 +1053,16 @@ int vsbpn_labels(const vsbd_result* res, const uint8_t* skip, int n, int kind, P
                  cudaStream_t st) {
   if (n <= 0) return 0;
   k_pn_labels<<<(n + 127) / 128, 128, 0, st>>>(res, skip, n, kind, out);
+  PCK(cudaGetLastError());
+  return 1;
+}
+
+int vsbpn_prior(const vsbd_item* items, const float* pout, int n, float scale, float conf_min,
+                const uint8_t* skip, int W, int H, vsbd_item* items2, short2* prior,
+                cudaStream_t st) {
+  if (n <= 0) return 0;
+  k_pn_prior<<<1, 256, 0, st>>>(items, pout, n, scale, conf_min, skip, (float)(W / 2),
+                                (float)(H / 2), items2, prior);
   PCK(cudaGetLastError());
   return 1;
 }
@@ -1119,7 +1226,7 @@ extern "C" int vsbd_pnet_narrow_host(const uint8_t* curr, const uint8_t* prev, i
     ps.radius = radius;
     ps.conf_min = conf_min;
     ps.sad_bound = sad_bound;
-    if (vsbpn_narrow(gd.g, dc, dp, pitch, di, n, dpo, ps, NULL, dr, dfb, dcount, dlist, 0) < 0)
+    if (vsbpn_narrow(gd.g, dc, dp, pitch, di, n, dpo, NULL, ps, NULL, dr, dfb, dcount, dlist, 0) < 0)
       goto done;
   }
   PTRY(cudaDeviceSynchronize());

@@ -53,12 +53,22 @@ int vsbpn_infer(const void* d_params, const uint8_t* curr, const uint8_t* prev, 
 
 /* narrowed search of n items of field set g: results into res, flags into
    fb (PN_FB_*); skip (may be NULL) marks items never used.  Items that fall
-   back are appended to fb_list (*fb_count, which the caller zeroes).
+   back are appended to fb_list (*fb_count, which the caller zeroes).  With
+   prior != NULL the proposal is prior[item] + the network's prediction.
    Returns launches or -1. */
 int vsbpn_narrow(const DGeom& g, const uint8_t* curr, const uint8_t* prev, int pitch,
-                 const vsbd_item* items, int n, const float* pout, const PNSearch& ps,
-                 const uint8_t* skip, vsbd_result* res, uint8_t* fb, int* fb_count,
-                 int* fb_list, cudaStream_t st);
+                 const vsbd_item* items, int n, const float* pout, const short2* prior,
+                 const PNSearch& ps, const uint8_t* skip, vsbd_result* res, uint8_t* fb,
+                 int* fb_count, int* fb_list, cudaStream_t st);
+
+/* Global motion prior of n coarse items from a first network pass (median
+   translation of the confident predictions, least-squares rotation about the
+   frame centre): items2 = items with the prior as search offset (the second
+   pass's crops), prior = the rounded model displacement per item (added to
+   the second pass's prediction).  One launch. */
+int vsbpn_prior(const vsbd_item* items, const float* pout, int n, float scale, float conf_min,
+                const uint8_t* skip, int W, int H, vsbd_item* items2, short2* prior,
+                cudaStream_t st);
 
 /* crops of n items into inputs [n][32][32][2] bf16 (training data) */
 int vsbpn_crops(const uint8_t* curr, const uint8_t* prev, int pitch, int W, int H,

@@ -166,6 +166,32 @@ class Batch:
             pass
 
 
+def detect_multi(detectors, clip_ptrs, frame_bytes, pitches, nframes, on_device, out, counts):
+    """Steps many MotionDetectors together (vsb_detect_multi): frame k of
+    stream s at clip_ptrs[s] + k*frame_bytes[s].  Records go to the
+    preallocated LM_DTYPE array out (frame by frame, stream by stream),
+    counts (int32, nframes*n) gets per-frame counts.  Returns the number of
+    records."""
+    L = lib()
+    n = len(detectors)
+    if not getattr(L, "_multi_bound", False):
+        L.vsb_detect_multi.restype = C.c_long
+        L.vsb_detect_multi.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.c_int, C.c_int, C.c_void_p, C.c_long, C.c_void_p]
+        L._multi_bound = True
+    mds = (C.POINTER(VSMotionDetect) * n)(*[C.pointer(d.md) for d in detectors])
+    clips = np.ascontiguousarray(clip_ptrs, np.uint64)
+    fb = np.ascontiguousarray(frame_bytes, np.int64)
+    pt = np.ascontiguousarray(pitches, np.int32)
+    if len(counts) < nframes * n:
+        raise ValueError("counts too small")
+    total = L.vsb_detect_multi(C.cast(mds, C.c_void_p), n, ptr(clips), ptr(fb), ptr(pt), nframes,
+                               1 if on_device else 0, ptr(out), len(out), ptr(counts))
+    if total < 0:
+        raise RuntimeError("vsb_detect_multi failed: %s" % L.vsb_last_error().decode())
+    return total
+
+
 def detect_clip(frames, pformat=1, stepsize=6, accuracy=15, shakiness=5, mincontrast=0.25,
                 tripod=0, show=0, serialization_mode=0, trf_path=None, on_device_ptr=None,
                 frame_bytes=None, linesize=None, width=None, height=None, return_frames=False):

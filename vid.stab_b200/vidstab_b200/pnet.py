@@ -65,6 +65,8 @@ def _L():
         L.vsb_set_proposal_ex.argtypes = [p, p, l_, C.c_double, C.c_double, C.c_double]
         L.vsb_set_proposal_scope.restype = i
         L.vsb_set_proposal_scope.argtypes = [p, i, C.c_double]
+        L.vsb_set_proposal_passes.restype = i
+        L.vsb_set_proposal_passes.argtypes = [p, i]
         L.vsb_set_proposal_verify.restype = i
         L.vsb_set_proposal_verify.argtypes = [p, i]
         L.vsb_proposal_stats.restype = i
@@ -125,7 +127,7 @@ def zero_blob(radius=2.0, conf_logit=10.0, match_bound=64.0):
 
 
 def set_proposal(det, blob, radius=-1.0, conf_min=float("nan"), match_bound=-1.0, verify=False,
-                 fine_net=False, fine_radius=-1.0):
+                 fine_net=False, fine_radius=-1.0, passes=None):
     """Gives a MotionDetector the proposal (blob None: back to plain)."""
     L = _L()
     buf = C.create_string_buffer(blob, len(blob)) if blob is not None else None
@@ -133,6 +135,8 @@ def set_proposal(det, blob, radius=-1.0, conf_min=float("nan"), match_bound=-1.0
                                  conf_min, match_bound), "vsb_set_proposal_ex")
     _check(L.vsb_set_proposal_scope(C.byref(det.md), 1 if fine_net else 0, fine_radius),
            "vsb_set_proposal_scope")
+    if passes is not None and blob is not None:
+        _check(L.vsb_set_proposal_passes(C.byref(det.md), passes), "vsb_set_proposal_passes")
     _check(L.vsb_set_proposal_verify(C.byref(det.md), 1 if verify else 0), "vsb_set_proposal_verify")
 
 

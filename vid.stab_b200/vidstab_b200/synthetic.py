@@ -159,15 +159,38 @@ def clip(width, height, nframes, seed=1, trans_sigma=3.0, rot_sigma_deg=0.2, zoo
     device=None: numpy on the CPU.  device="cuda"/"cpu": torch warping on that
     device, returns a torch uint8 tensor there (much faster for large clips)."""
     path = camera_path(nframes, seed, trans_sigma, rot_sigma_deg, zoom_sigma)
-    ext = np.abs(path[:, :2]).max() if nframes > 1 else 0.0
-    rot = np.abs(path[:, 2]).max() if nframes > 1 else 0.0
-    zmax = path[:, 3].max()
+    H, W = _canvas(width, height, [path], margin)
+    src = world(H, W, seed, nblobs=nblobs * max(1, (W * H) // (width * height)))
+    return _render_clip(src, path, width, height, nframes, seed, noise, device)
+
+
+def _canvas(width, height, paths, margin=None):
+    """(H, W) of a world every camera path stays inside"""
+    ext = max((np.abs(p[:, :2]).max() if len(p) > 1 else 0.0) for p in paths)
+    rot = max((np.abs(p[:, 2]).max() if len(p) > 1 else 0.0) for p in paths)
+    zmax = max(p[:, 3].max() for p in paths)
     diag = math.hypot(width, height) * max(1.0, zmax)
     if margin is None:
         margin = int(ext + (diag - min(width, height)) / 2 * (1 if rot > 0 else 0) + 32)
     W = int(max(width * zmax, diag if rot > 0 else width * zmax)) + 2 * margin
     H = int(max(height * zmax, diag if rot > 0 else height * zmax)) + 2 * margin
-    src = world(H, W, seed, nblobs=nblobs * max(1, (W * H) // (width * height)))
+    return H, W
+
+
+def clips_shared_world(width, height, nframes, seeds, world_seed, trans_sigma=3.0,
+                       rot_sigma_deg=0.2, zoom_sigma=0.002, noise=2.0, nblobs=200, device=None):
+    """One camera-walk clip per seed (its own path and sensor noise) over one
+    shared scene generated from world_seed: many streams without generating
+    a scene per stream."""
+    paths = [camera_path(nframes, sd, trans_sigma, rot_sigma_deg, zoom_sigma) for sd in seeds]
+    H, W = _canvas(width, height, paths)
+    src = world(H, W, world_seed, nblobs=nblobs * max(1, (W * H) // (width * height)))
+    return [_render_clip(src, p, width, height, nframes, sd, noise, device)
+            for p, sd in zip(paths, seeds)]
+
+
+def _render_clip(src, path, width, height, nframes, seed, noise, device):
+    H, W = src.shape
     if device is None:
         rng = np.random.default_rng(seed + 31337)
         out = np.empty((nframes, height, width), np.uint8)
