@@ -42,6 +42,12 @@ VS_API int vsb_set_search_mode(struct _vsmotiondetect* md, int pruned);
    environment's choice). */
 VS_API void vsb_set_default_search_mode(int pruned);
 
+/* The search tiling the detector picked (cost model + timing at init) for
+   its coarse (fine = 0) or fine (1) fields: desc[0..7] = lattice rows and
+   columns per thread, lattice columns and rows per CTA, field strips,
+   threads per CTA, shared memory bytes per CTA, CTAs per field. */
+VS_API int vsb_search_tiling(const struct _vsmotiondetect* md, int fine, int* desc);
+
 /* Kernel launches issued for this detector so far. */
 VS_API long vsb_launch_count(const struct _vsmotiondetect* md);
 

@@ -107,9 +107,10 @@ def orc_search(curr, prev, x, y, size, ms, step, ox=0, oy=0, bpp=0):
     return e.value, tx.value, ty.value, ok
 
 
-def enc(tb, strips, nab, nbb):
-    """forced tiling: rows per thread, field strips, lattice columns / rows per CTA"""
-    return tb * 1000000 + strips * 10000 + nab * 100 + nbb
+def enc(tb, strips, nab, nbb, ta=0):
+    """forced tiling: rows per thread, field strips, lattice columns / rows per
+    CTA, lattice columns per thread"""
+    return ta * 100000000 + tb * 1000000 + strips * 10000 + nab * 100 + nbb
 
 
 @pytest.mark.parametrize("size,ms,step,tiles", [(64, 40, 6, 0), (32, 32, 2, 0),
@@ -118,7 +119,14 @@ def enc(tb, strips, nab, nbb):
                                                 (16, 16, 2, enc(8, 1, 17, 16)),
                                                 (80, 45, 5, 0), (32, 20, 1, enc(4, 8, 41, 4)),
                                                 (48, 33, 7, enc(8, 2, 3, 8)), (224, 40, 6, 0),
-                                                (112, 154, 6, 0), (32, 32, 2, enc(4, 1, 33, 36))])
+                                                (112, 154, 6, 0), (32, 32, 2, enc(4, 1, 33, 36)),
+                                                (112, 60, 6, enc(4, 2, 8, 8, 2)),
+                                                (112, 154, 6, enc(2, 4, 14, 10, 2)),
+                                                (48, 30, 4, enc(2, 4, 6, 6, 2)),
+                                                (32, 32, 2, enc(4, 1, 34, 36, 2)),
+                                                (48, 33, 7, enc(4, 2, 4, 8, 2)),
+                                                (32, 20, 1, enc(2, 8, 42, 4, 2)),
+                                                (64, 40, 6, enc(2, 1, 2, 2, 2))])
 def test_field_search_planar(size, ms, step, tiles):
     w, h = 640, 480
     curr, prev = _blurred_pair(w, h, seed=size + step)

@@ -39,6 +39,10 @@ int vsb_motion_detection_device(VSMotionDetect* md, LocalMotions* motions, const
 
 long vsb_launch_count(const VSMotionDetect* md) { return vsbd_launches(vsb_md_device(md)); }
 
+int vsb_search_tiling(const VSMotionDetect* md, int fine, int* desc) {
+  return vsbd_search_tiling(vsb_md_device(md), fine, desc) == 0 ? VS_OK : VS_ERROR;
+}
+
 static double now_s(void) {
   struct timespec ts;
   clock_gettime(CLOCK_MONOTONIC, &ts);

@@ -254,7 +254,7 @@ static int same_geom(const vsbd_geom* a, const vsbd_geom* b) {
 /* a tiling the persistent kernel can run: TB 2 or 4, at most its block
    size, tile and static shared memory within the per-block limit */
 static int tiling_ok(const vsbd_batch* b, const DGeom& g) {
-  return (g.tb == 2 || g.tb == 4) && g.threads <= VSB_BATCH_THREADS &&
+  return (g.tb == 2 || g.tb == 4) && g.ta != 2 && g.threads <= VSB_BATCH_THREADS &&
          tile_layout(g).total + b->static_smem + 64 <= (size_t)b->optin;
 }
 

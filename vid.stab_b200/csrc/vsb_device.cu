@@ -341,12 +341,12 @@ static int sm_count(void) {
    more than this device already allows it (the attribute call costs
    microseconds of host time per launch otherwise); slot names the kernel */
 static cudaError_t ensure_smem(const void* fn, int slot, size_t smem) {
-  static size_t done[16][16];
+  static size_t done[16][32];
   int dev = 0;
   cudaGetDevice(&dev);
-  if (dev >= 0 && dev < 16 && slot >= 0 && slot < 16 && done[dev][slot] >= smem) return cudaSuccess;
+  if (dev >= 0 && dev < 16 && slot >= 0 && slot < 32 && done[dev][slot] >= smem) return cudaSuccess;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e == cudaSuccess && dev >= 0 && dev < 16 && slot >= 0 && slot < 16) done[dev][slot] = smem;
+  if (e == cudaSuccess && dev >= 0 && dev < 16 && slot >= 0 && slot < 32) done[dev][slot] = smem;
   return e;
 }
 
@@ -370,19 +370,25 @@ static size_t search_smem_limit(void) {
   return lim;
 }
 
-/* registers per thread of the search kernel for TB rows per thread */
-static int lattice_regs(int TB) {
-  static int r[9] = { 0 };
-  if (TB < 1 || TB > 8) return 0;
-  if (!r[TB]) {
+/* registers per thread of the search kernel for TB rows and TA columns per
+   thread */
+static int lattice_regs(int TB, int TA) {
+  static int r[3][9] = { { 0 } };
+  if (TB < 1 || TB > 8 || TA < 1 || TA > 2) return 0;
+  if (!r[TA][TB]) {
     cudaFuncAttributes fa;
     cudaError_t e = cudaErrorInvalidValue;
-    if (TB == 2) e = cudaFuncGetAttributes(&fa, k_lattice<2>);
-    if (TB == 4) e = cudaFuncGetAttributes(&fa, k_lattice<4>);
-    if (TB == 8) e = cudaFuncGetAttributes(&fa, k_lattice<8>);
-    r[TB] = e == cudaSuccess ? fa.numRegs : 64;
+    if (TA == 1) {
+      if (TB == 2) e = cudaFuncGetAttributes(&fa, k_lattice<2>);
+      if (TB == 4) e = cudaFuncGetAttributes(&fa, k_lattice<4>);
+      if (TB == 8) e = cudaFuncGetAttributes(&fa, k_lattice<8>);
+    } else {
+      if (TB == 2) e = cudaFuncGetAttributes(&fa, k_lattice<2, false, 2>);
+      if (TB == 4) e = cudaFuncGetAttributes(&fa, k_lattice<4, false, 2>);
+    }
+    r[TA][TB] = e == cudaSuccess ? fa.numRegs : 64;
   }
-  return r[TB];
+  return r[TA][TB];
 }
 
 /* Candidate tile shapes (columns x rows of the lattice per CTA, rows per
@@ -394,14 +400,17 @@ static int lattice_regs(int TB) {
 
 static int tile_candidates(const DGeom& g, int nitems, int tb_force, int strip_force,
                            int nab_force, int nbb_force, TileCand* out, int cap,
-                           int max_threads = 512) {
+                           int max_threads = 512, int ta_force = 0) {
   const size_t lim = search_smem_limit();
   const int sms = sm_count();
   int n = 0;
   const int tbs[3] = { 4, 2, 8 };
-  for (int ti = 0; ti < 3; ti++) {
+  for (int tv = 0; tv < 6; tv++) {
+    const int ti = tv % 3, TA = 1 + tv / 3; /* lattice columns per thread */
     int TB = tbs[ti];
     if (tb_force > 0 && TB != tb_force) continue;
+    if (TA == 2 && (TB > 4 || g.step * g.bpp > 8 || g.rows > 0)) continue;
+    if (ta_force > 0 && TA != ta_force) continue;
     for (int ns = 1; ns <= 8; ns *= 2) {
       if (strip_force > 0 && ns != strip_force) continue;
       const int rows = geom_rows(g);
@@ -416,14 +425,16 @@ static int tile_candidates(const DGeom& g, int nitems, int tb_force, int strip_f
           int nbb = m * TB;
           if (nbb_force > 0) nbb = nbb_force;
           if (nbb % TB) break;
+          if (TA == 2 && (nab & 1)) continue;
           DGeom t = g;
           t.tb = TB;
+          t.ta = TA;
           t.nab = nab;
           t.nbb = nbb;
           t.nstrip = ns;
           t.nta = (g.na + nab - 1) / nab;
           t.ntb = (g.nb + nbb - 1) / nbb;
-          int threads = nab * (nbb / TB) * ns;
+          int threads = (nab / TA) * (nbb / TB) * ns;
           threads = (threads + 31) & ~31;
           if (threads > max_threads || threads < 32) {
             if (nbb_force > 0) break;
@@ -438,7 +449,7 @@ static int tile_candidates(const DGeom& g, int nitems, int tb_force, int strip_f
           long ctas = (long)nitems * t.nta * t.ntb;
           int cps = (int)((228 * 1024) / (L.total + 1024));
           if (2048 / threads < cps) cps = 2048 / threads;
-          int regs = lattice_regs(TB);
+          int regs = lattice_regs(TB, TA);
           if (regs > 0 && 65536 / (threads * regs) < cps) cps = 65536 / (threads * regs);
           if (cps > 32) cps = 32;
           if (cps < 1) {
@@ -451,6 +462,9 @@ static int tile_candidates(const DGeom& g, int nitems, int tb_force, int strip_f
           double occ = warps >= 16 ? 1.0 : warps / 16.0;
           long waves = (ctas + (long)sms * cps - 1) / ((long)sms * cps);
           double clk = (double)waves * cps * (work / 64.0 / occ + (double)L.WH_alloc * L.WP / 32.0);
+          /* two columns per thread load each window word once for both (fewer
+             shared-memory loads per SAD than the model counts) */
+          if (TA == 2) clk *= 0.85;
           /* keep the cap best, sorted */
           int pos = n < cap ? n : cap;
           while (pos > 0 && out[pos - 1].clk > clk) {
@@ -506,15 +520,16 @@ static int geom_upload(const vsbd_geom* h, int nitems, int tiles_hint, GeomDev* 
   if (e1 != cudaSuccess || e2 != cudaSuccess) { set_err("geometry upload", e1 != cudaSuccess ? e1 : e2); return -1; }
   g.order = out->d_order;
   g.point = out->d_point;
-  int tb_f = 0, ns_f = 0, nab_f = 0, nbb_f = 0;
-  if (tiles_hint > 0) { /* test hook: tb*1000000 + strips*10000 + nab*100 + nbb */
-    tb_f = tiles_hint / 1000000;
+  int tb_f = 0, ns_f = 0, nab_f = 0, nbb_f = 0, ta_f = 0;
+  if (tiles_hint > 0) { /* test hook: ta*100000000 + tb*1000000 + strips*10000 + nab*100 + nbb */
+    ta_f = tiles_hint / 100000000;
+    tb_f = (tiles_hint / 1000000) % 100;
     ns_f = (tiles_hint / 10000) % 100;
     nab_f = (tiles_hint / 100) % 100;
     nbb_f = tiles_hint % 100;
   }
   TileCand cand[1];
-  int nc = tile_candidates(g, nitems > 0 ? nitems : 1, tb_f, ns_f, nab_f, nbb_f, cand, 1);
+  int nc = tile_candidates(g, nitems > 0 ? nitems : 1, tb_f, ns_f, nab_f, nbb_f, cand, 1, 512, ta_f);
   if (nc < 1) { set_msg("no search tiling fits in shared memory"); return -1; }
   g = cand[0].g;
   out->smem = tile_layout(g).total;
@@ -528,18 +543,19 @@ static void geom_free(GeomDev* g) {
   g->d_point = NULL;
 }
 
-template <int TB>
+template <int TB, int TA>
 static int launch_lattice(const GeomDev& gd, const uint8_t* curr, const uint8_t* prev, int pitch,
                           const vsbd_item* d_items, int n, unsigned long long* keys,
                           unsigned* tickets, vsbd_result* d_res, cudaStream_t st) {
-  cudaError_t e = ensure_smem((const void*)k_lattice<TB>, TB == 2 ? 0 : (TB == 4 ? 1 : 2), gd.smem);
+  cudaError_t e = ensure_smem((const void*)k_lattice<TB, false, TA>,
+                              (TA == 2 ? 11 : 0) + (TB == 2 ? 0 : (TB == 4 ? 1 : 2)), gd.smem);
   if (e != cudaSuccess) {
     set_err("cudaFuncSetAttribute(k_lattice)", e);
     return -1;
   }
   dim3 grid(gd.g.nta * gd.g.ntb, n);
-  k_lattice<TB><<<grid, gd.g.threads, gd.smem, st>>>(curr, prev, pitch, gd.g, d_items, keys, tickets,
-                                                     d_res);
+  k_lattice<TB, false, TA><<<grid, gd.g.threads, gd.smem, st>>>(curr, prev, pitch, gd.g, d_items,
+                                                                keys, tickets, d_res);
   return 1;
 }
 
@@ -548,9 +564,13 @@ static int launch_search(const GeomDev& gd, const uint8_t* curr, const uint8_t* 
                          unsigned* tickets, vsbd_result* d_res, cudaStream_t st) {
   if (n <= 0) return 0;
   switch (gd.g.tb) {
-    case 2: return launch_lattice<2>(gd, curr, prev, pitch, d_items, n, keys, tickets, d_res, st);
-    case 4: return launch_lattice<4>(gd, curr, prev, pitch, d_items, n, keys, tickets, d_res, st);
-    case 8: return launch_lattice<8>(gd, curr, prev, pitch, d_items, n, keys, tickets, d_res, st);
+    case 2:
+      return gd.g.ta == 2 ? launch_lattice<2, 2>(gd, curr, prev, pitch, d_items, n, keys, tickets, d_res, st)
+                          : launch_lattice<2, 1>(gd, curr, prev, pitch, d_items, n, keys, tickets, d_res, st);
+    case 4:
+      return gd.g.ta == 2 ? launch_lattice<4, 2>(gd, curr, prev, pitch, d_items, n, keys, tickets, d_res, st)
+                          : launch_lattice<4, 1>(gd, curr, prev, pitch, d_items, n, keys, tickets, d_res, st);
+    case 8: return launch_lattice<8, 1>(gd, curr, prev, pitch, d_items, n, keys, tickets, d_res, st);
   }
   set_msg("unsupported rows-per-thread");
   return -1;
@@ -558,16 +578,16 @@ static int launch_search(const GeomDev& gd, const uint8_t* curr, const uint8_t* 
 
 /* full search of the items in list[0 .. *count), at most n of them:
    persistent CTAs, as many as fit on the GPU at once */
-template <int TB>
+template <int TB, int TA>
 static int launch_list_tb(const GeomDev& gd, const uint8_t* curr, const uint8_t* prev, int pitch,
                           const vsbd_item* d_items, int n, const int* count, const int* list,
                           unsigned long long* keys, unsigned* tickets, vsbd_result* d_res,
                           cudaStream_t st) {
-  cudaError_t e = ensure_smem((const void*)k_lattice_list<TB>, TB == 2 ? 3 : (TB == 4 ? 4 : 5),
-                              gd.smem);
+  cudaError_t e = ensure_smem((const void*)k_lattice_list<TB, TA>,
+                              (TA == 2 ? 14 : 3) + (TB == 2 ? 0 : (TB == 4 ? 1 : 2)), gd.smem);
   int cps = gd.list_cps;
   if (e == cudaSuccess && cps <= 0)
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cps, k_lattice_list<TB>, gd.g.threads,
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cps, k_lattice_list<TB, TA>, gd.g.threads,
                                                       gd.smem);
   if (e != cudaSuccess) {
     set_err("k_lattice_list set-up", e);
@@ -576,7 +596,7 @@ static int launch_list_tb(const GeomDev& gd, const uint8_t* curr, const uint8_t*
   long units = (long)n * gd.g.nta * gd.g.ntb;
   long grid = (long)sm_count() * (cps > 0 ? cps : 1);
   if (grid > units) grid = units;
-  k_lattice_list<TB><<<(unsigned)grid, gd.g.threads, gd.smem, st>>>(curr, prev, pitch, gd.g, d_items,
+  k_lattice_list<TB, TA><<<(unsigned)grid, gd.g.threads, gd.smem, st>>>(curr, prev, pitch, gd.g, d_items,
                                                                    count, list, keys, tickets, d_res);
   return 1;
 }
@@ -587,9 +607,13 @@ static int launch_list(const GeomDev& gd, const uint8_t* curr, const uint8_t* pr
                        cudaStream_t st) {
   if (n <= 0) return 0;
   switch (gd.g.tb) {
-    case 2: return launch_list_tb<2>(gd, curr, prev, pitch, d_items, n, count, list, keys, tickets, d_res, st);
-    case 4: return launch_list_tb<4>(gd, curr, prev, pitch, d_items, n, count, list, keys, tickets, d_res, st);
-    case 8: return launch_list_tb<8>(gd, curr, prev, pitch, d_items, n, count, list, keys, tickets, d_res, st);
+    case 2:
+      return gd.g.ta == 2 ? launch_list_tb<2, 2>(gd, curr, prev, pitch, d_items, n, count, list, keys, tickets, d_res, st)
+                          : launch_list_tb<2, 1>(gd, curr, prev, pitch, d_items, n, count, list, keys, tickets, d_res, st);
+    case 4:
+      return gd.g.ta == 2 ? launch_list_tb<4, 2>(gd, curr, prev, pitch, d_items, n, count, list, keys, tickets, d_res, st)
+                          : launch_list_tb<4, 1>(gd, curr, prev, pitch, d_items, n, count, list, keys, tickets, d_res, st);
+    case 8: return launch_list_tb<8, 1>(gd, curr, prev, pitch, d_items, n, count, list, keys, tickets, d_res, st);
   }
   set_msg("unsupported rows-per-thread");
   return -1;
@@ -683,8 +707,12 @@ static int autotune_tiling(GeomDev* gd, const uint8_t* curr, const uint8_t* prev
       return 0;
     }
   }
-  TileCand cand[12];
-  int nc = tile_candidates(g, n, 0, 0, 0, 0, cand, 12);
+  /* the model's 10 best tilings with one lattice column per thread and its
+     8 best with two: the model does not count shared-memory loads, which is
+     where the two kinds differ, so both are timed */
+  TileCand cand[18];
+  int nc = tile_candidates(g, n, 0, 0, 0, 0, cand, 10, 512, 1);
+  nc += tile_candidates(g, n, 0, 0, 0, 0, cand + nc, 8, 512, 2);
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
@@ -1355,6 +1383,20 @@ extern "C" int vsbd_can_overlap(const vsbd_ctx* c) {
 
 extern "C" long vsbd_launches(const vsbd_ctx* c) { return c ? c->launches : 0; }
 
+extern "C" int vsbd_search_tiling(const vsbd_ctx* c, int fine, int* desc) {
+  if (!c || !desc) return -1;
+  const DGeom& g = fine ? c->gf.g : c->gc.g;
+  desc[0] = g.tb;
+  desc[1] = g.ta > 0 ? g.ta : 1;
+  desc[2] = g.nab;
+  desc[3] = g.nbb;
+  desc[4] = g.nstrip;
+  desc[5] = g.threads;
+  desc[6] = (int)(fine ? c->gf.smem : c->gc.smem);
+  desc[7] = g.nta * g.ntb;
+  return 0;
+}
+
 extern "C" long vsbd_pnet_param_bytes(void) { return (long)PN_PARAM_BYTES; }
 
 extern "C" int vsbd_set_proposal(vsbd_ctx* c, const void* params, float scale, float radius,
@@ -1402,16 +1444,15 @@ extern "C" int vsbd_set_proposal(vsbd_ctx* c, const void* params, float scale, f
       GeomDev* g = gs[k];
       int cps = 0;
       cudaError_t e = cudaSuccess;
-      switch (g->g.tb) {
-        case 2: e = ensure_smem((const void*)k_lattice_list<2>, 3, g->smem);
-          if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cps, k_lattice_list<2>, g->g.threads, g->smem);
-          break;
-        case 4: e = ensure_smem((const void*)k_lattice_list<4>, 4, g->smem);
-          if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cps, k_lattice_list<4>, g->g.threads, g->smem);
-          break;
-        case 8: e = ensure_smem((const void*)k_lattice_list<8>, 5, g->smem);
-          if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cps, k_lattice_list<8>, g->g.threads, g->smem);
-          break;
+      const void* fn = NULL;
+      int slot = 0;
+      if (g->g.tb == 2) { fn = g->g.ta == 2 ? (const void*)k_lattice_list<2, 2> : (const void*)k_lattice_list<2, 1>; slot = g->g.ta == 2 ? 14 : 3; }
+      if (g->g.tb == 4) { fn = g->g.ta == 2 ? (const void*)k_lattice_list<4, 2> : (const void*)k_lattice_list<4, 1>; slot = g->g.ta == 2 ? 15 : 4; }
+      if (g->g.tb == 8) { fn = (const void*)k_lattice_list<8, 1>; slot = 5; }
+      if (fn) {
+        e = ensure_smem(fn, slot, g->smem);
+        if (e == cudaSuccess)
+          e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cps, fn, g->g.threads, g->smem);
       }
       if (e != cudaSuccess) {
         set_err("fallback search set-up", e);

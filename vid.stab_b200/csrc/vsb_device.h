@@ -100,6 +100,11 @@ int vsbd_stage_a_next_collect(vsbd_ctx* c, const uint8_t** minmax, const vsbd_re
 int vsbd_stage_b_issue(vsbd_ctx* c, const vsbd_item* items, int n);
 int vsbd_stage_b_collect(vsbd_ctx* c, const vsbd_result** fine);
 
+/* the search tiling the detector runs for its coarse (fine = 0) or fine
+   fields: desc[0..7] = rows per thread, columns per thread, lattice columns
+   and rows per CTA, field strips, threads, shared memory bytes, CTAs per item */
+int vsbd_search_tiling(const vsbd_ctx* c, int fine, int* desc);
+
 /* Kernel launches issued on behalf of this detector so far. */
 long vsbd_launches(const vsbd_ctx* c);
 

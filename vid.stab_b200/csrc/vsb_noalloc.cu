@@ -101,15 +101,16 @@ __global__ void k_noalloc_tables(int K, int step, int32_t* order, short2* point)
   }
 }
 
-template <int TB>
+template <int TB, int TA>
 static cudaError_t launch_tb(const DGeom& g, size_t smem, const uint8_t* curr, const uint8_t* prev,
                              int pitch, const vsbd_item* items, int n, unsigned long long* keys,
                              unsigned* tickets, vsbd_result* res, cudaStream_t st) {
-  cudaError_t e =
-      cudaFuncSetAttribute(k_lattice<TB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = cudaFuncSetAttribute(k_lattice<TB, false, TA>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   dim3 grid(g.nta * g.ntb, n);
-  k_lattice<TB><<<grid, g.threads, smem, st>>>(curr, prev, pitch, g, items, keys, tickets, res);
+  k_lattice<TB, false, TA><<<grid, g.threads, smem, st>>>(curr, prev, pitch, g, items, keys,
+                                                          tickets, res);
   return cudaGetLastError();
 }
 
@@ -183,9 +184,15 @@ extern "C" int vsbd_search_noalloc(const uint8_t* d_curr, const uint8_t* d_prev,
   const vsbd_item* items = (const vsbd_item*)d_items;
   vsbd_result* res = (vsbd_result*)d_results;
   switch (g.tb) {
-    case 2: e = launch_tb<2>(g, smem, d_curr, d_prev, pitch, items, n, keys, tickets, res, st); break;
-    case 4: e = launch_tb<4>(g, smem, d_curr, d_prev, pitch, items, n, keys, tickets, res, st); break;
-    case 8: e = launch_tb<8>(g, smem, d_curr, d_prev, pitch, items, n, keys, tickets, res, st); break;
+    case 2:
+      e = g.ta == 2 ? launch_tb<2, 2>(g, smem, d_curr, d_prev, pitch, items, n, keys, tickets, res, st)
+                    : launch_tb<2, 1>(g, smem, d_curr, d_prev, pitch, items, n, keys, tickets, res, st);
+      break;
+    case 4:
+      e = g.ta == 2 ? launch_tb<4, 2>(g, smem, d_curr, d_prev, pitch, items, n, keys, tickets, res, st)
+                    : launch_tb<4, 1>(g, smem, d_curr, d_prev, pitch, items, n, keys, tickets, res, st);
+      break;
+    case 8: e = launch_tb<8, 1>(g, smem, d_curr, d_prev, pitch, items, n, keys, tickets, res, st); break;
     default: return fail("unsupported tiling", cudaSuccess);
   }
   if (e != cudaSuccess) return fail("k_lattice", e);

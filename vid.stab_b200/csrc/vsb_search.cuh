@@ -44,6 +44,8 @@ struct DGeom {
   int nta, ntb;         /* tiles along a / along b */
   int nstrip;           /* field rows split into this many strips */
   int threads;          /* block size */
+  int ta;               /* lattice columns per thread: 1 (or 0), or 2 -- a window row's words
+                           then serve two candidate columns (planar, step*bpp <= 8) */
   int rows;             /* field rows a launch sums (0: all S); fewer rows give
                            every candidate a lower bound of its SAD */
   unsigned* emit;       /* emit mode: per item, per lattice point, the sum */
@@ -294,10 +296,96 @@ __device__ __forceinline__ void rows_segment(unsigned (&acc)[TB], int jlo, int j
 #undef VSB_SEG
 }
 
+/* Rows [rb, re) for a thread owning two lattice columns (ta == 2), the
+   second DW words right of the first with its own funnel shift: each quad of
+   a window row is loaded once (four new words, three carried) and serves
+   both columns of every active candidate row. */
+template <int TB, int JLO, int JHI, int DW>
+__device__ __forceinline__ void rows_active_ta2(unsigned (&acc)[2][TB], int rb, int re, int step,
+                                                const uint8_t* __restrict__ Pb, int WP, int sh0,
+                                                int sh1, const uint4* __restrict__ C4, int nq) {
+  for (int rho = rb; rho < re; rho++) {
+    const uint32_t* Pw = (const uint32_t*)(Pb + rho * WP);
+    const uint4* Cj[TB];
+#pragma unroll
+    for (int j = JLO; j <= JHI; j++) Cj[j] = C4 + (rho - step * j) * nq;
+    uint32_t a0 = Pw[0], a1 = Pw[1], a2 = Pw[2];
+    for (int q = 0; q < nq; q++) {
+      const uint32_t b0 = Pw[4 * q + 3], b1 = Pw[4 * q + 4], b2 = Pw[4 * q + 5], b3 = Pw[4 * q + 6];
+      const uint32_t W[7] = { a0, a1, a2, b0, b1, b2, b3 };
+      const uint32_t x0 = __funnelshift_r(W[0], W[1], sh0), x1 = __funnelshift_r(W[1], W[2], sh0);
+      const uint32_t x2 = __funnelshift_r(W[2], W[3], sh0), x3 = __funnelshift_r(W[3], W[4], sh0);
+      const uint32_t y0 = __funnelshift_r(W[DW], W[DW + 1], sh1);
+      const uint32_t y1 = __funnelshift_r(W[DW + 1], W[DW + 2], sh1);
+      const uint32_t y2 = __funnelshift_r(W[DW + 2], W[DW + 3], sh1);
+      const uint32_t y3 = __funnelshift_r(W[DW + 3], W[DW + 4], sh1);
+      a0 = b1;
+      a1 = b2;
+      a2 = b3;
+#pragma unroll
+      for (int j = JLO; j <= JHI; j++) {
+        const uint4 c = Cj[j][q];
+        acc[0][j] = sad4(c.x, x0, acc[0][j]);
+        acc[1][j] = sad4(c.x, y0, acc[1][j]);
+        acc[0][j] = sad4(c.y, x1, acc[0][j]);
+        acc[1][j] = sad4(c.y, y1, acc[1][j]);
+        acc[0][j] = sad4(c.z, x2, acc[0][j]);
+        acc[1][j] = sad4(c.z, y2, acc[1][j]);
+        acc[0][j] = sad4(c.w, x3, acc[0][j]);
+        acc[1][j] = sad4(c.w, y3, acc[1][j]);
+      }
+    }
+  }
+}
+
+template <int TB, int DW>
+__device__ __forceinline__ void rows_segment_ta2_dw(unsigned (&acc)[2][TB], int jlo, int jhi,
+                                                    int rb, int re, int step, const uint8_t* Pb,
+                                                    int WP, int sh0, int sh1, const uint4* C4,
+                                                    int nq) {
+#define VSB_SEG2(L, H)                                                                 \
+  if (jlo == L && jhi == H) {                                                          \
+    rows_active_ta2<TB, L, H, DW>(acc, rb, re, step, Pb, WP, sh0, sh1, C4, nq);        \
+    return;                                                                            \
+  }
+  if constexpr (TB == 2) {
+    VSB_SEG2(0, 0) VSB_SEG2(0, 1) VSB_SEG2(1, 1)
+  } else if constexpr (TB == 4) {
+    VSB_SEG2(0, 0) VSB_SEG2(0, 1) VSB_SEG2(0, 2) VSB_SEG2(0, 3)
+    VSB_SEG2(1, 1) VSB_SEG2(1, 2) VSB_SEG2(1, 3)
+    VSB_SEG2(2, 2) VSB_SEG2(2, 3)
+    VSB_SEG2(3, 3)
+  }
+#undef VSB_SEG2
+}
+
+/* segment of a two-column thread: DW, the word distance of its second
+   column (0..2), is uniform per thread and chosen once here */
+template <int TB>
+__device__ __forceinline__ void rows_segment_ta2(unsigned (&acc)[2][TB], int jlo, int jhi, int rb,
+                                                 int re, int step, const uint8_t* Pb, int WP,
+                                                 int sh0, int sh1, int dw, const uint4* C4,
+                                                 int nq) {
+  if (dw == 1)
+    rows_segment_ta2_dw<TB, 1>(acc, jlo, jhi, rb, re, step, Pb, WP, sh0, sh1, C4, nq);
+  else if (dw == 2)
+    rows_segment_ta2_dw<TB, 2>(acc, jlo, jhi, rb, re, step, Pb, WP, sh0, sh1, C4, nq);
+  else
+    rows_segment_ta2_dw<TB, 0>(acc, jlo, jhi, rb, re, step, Pb, WP, sh0, sh1, C4, nq);
+}
+
+template <int TB, bool EMIT>
+__device__ void lattice_tile_ta2(const uint8_t* __restrict__ curr, const uint8_t* __restrict__ prev,
+                                 int pitch, const DGeom& g, const vsbd_item* __restrict__ items,
+                                 unsigned long long* __restrict__ keys,
+                                 unsigned* __restrict__ tickets, vsbd_result* __restrict__ res,
+                                 int item, int tile, unsigned ntiles, uint8_t* sm);
+
 /* One lattice tile of one item, by one CTA: tile = tbi*nta + tai of the
    item's ntiles = nta*ntb tiles; sm: tile_layout(g).total bytes of shared
-   memory.  The last of the item's CTAs to finish refines and stores. */
-template <int TB, bool EMIT>
+   memory.  The last of the item's CTAs to finish refines and stores.  TA:
+   lattice columns per thread (1, or 2 for tilings with g.ta == 2). */
+template <int TB, bool EMIT, int TA = 1>
 __device__ __forceinline__ void lattice_tile(const uint8_t* __restrict__ curr,
                                              const uint8_t* __restrict__ prev, int pitch,
                                              const DGeom& g, const vsbd_item* __restrict__ items,
@@ -305,6 +393,11 @@ __device__ __forceinline__ void lattice_tile(const uint8_t* __restrict__ curr,
                                              unsigned* __restrict__ tickets,
                                              vsbd_result* __restrict__ res, int item, int tile,
                                              unsigned ntiles, uint8_t* sm) {
+  if constexpr (TA == 2) {
+    lattice_tile_ta2<TB, EMIT>(curr, prev, pitch, g, items, keys, tickets, res, item, tile,
+                               ntiles, sm);
+    return;
+  }
   __shared__ unsigned long long red[32];
   __shared__ int s_last;
   const TileLayout L = tile_layout(g);
@@ -437,8 +530,157 @@ __device__ __forceinline__ void lattice_tile(const uint8_t* __restrict__ curr,
   refine_and_store(g, L, it, C, P + 16, prev, pitch, keys, tickets, res, item, qsad);
 }
 
-/* grid (nta*ntb, items); block g.threads; dynamic smem tile_layout(g).total */
-template <int TB, bool EMIT = false>
+/* lattice_tile for two columns per thread (g.ta == 2, nab even): thread t
+   owns columns 2*(t % (nab/2)) and the next, TB rows of a row group and a
+   strip of the field.  Same sums, keys and refinement as lattice_tile. */
+template <int TB, bool EMIT>
+__device__ void lattice_tile_ta2(const uint8_t* __restrict__ curr, const uint8_t* __restrict__ prev,
+                                 int pitch, const DGeom& g, const vsbd_item* __restrict__ items,
+                                 unsigned long long* __restrict__ keys,
+                                 unsigned* __restrict__ tickets, vsbd_result* __restrict__ res,
+                                 int item, int tile, unsigned ntiles, uint8_t* sm) {
+  __shared__ unsigned long long red[32];
+  __shared__ int s_last;
+  const TileLayout L = tile_layout(g);
+  const int tbi = tile / g.nta, tai = tile - tbi * g.nta;
+  const vsbd_item it = items[item];
+  const int a0 = tai * g.nab, b0 = tbi * g.nbb;
+  const int na_t = min(g.nab, g.na - a0), nb_t = min(g.nbb, g.nb - b0);
+  const int G = g.nbb / TB;
+  const int NAG = g.nab / 2;
+  const int rows = geom_rows(g);
+  const int Rs = rows / g.nstrip;
+  if (EMIT && g.skip && g.skip[item]) return;
+  uint32_t* C = (uint32_t*)sm;
+  uint8_t* P = sm + L.off_P;
+  unsigned* part = (unsigned*)(sm + L.off_part);
+  unsigned* qsad = (unsigned*)(sm + L.off_q);
+  {
+    const int cx0 = (it.x - g.S / 2) * g.bpp, cy0 = it.y - g.S / 2;
+    const int cx0a = cx0 & ~15, ce = cx0 - cx0a;
+    const int nv = (ce + L.rowB + 15) >> 4;
+    for (int i = threadIdx.x; i < rows * nv; i += blockDim.x) {
+      int r = i / nv, v = i - r * nv;
+      *(uint4*)(P + r * L.FP + (v << 4)) =
+          *(const uint4*)(curr + (size_t)(cy0 + r) * pitch + cx0a + (v << 4));
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < rows * L.rowW; i += blockDim.x) {
+      int r = i / L.rowW, w = i - r * L.rowW;
+      const uint32_t* sw = (const uint32_t*)(P + r * L.FP) + (ce >> 2) + w;
+      C[i] = __funnelshift_r(sw[0], sw[1], (ce & 3) << 3);
+    }
+    __syncthreads();
+  }
+  const int gx0 = (it.x - g.S / 2 + it.ox + g.ax0 + a0 * g.step) * g.bpp;
+  const int gy0 = it.y - g.S / 2 + it.oy + g.by0 + b0 * g.step;
+  const int gx0a = gx0 & ~15, e = gx0 - gx0a;
+  {
+    const int wwb = L.rowB + (na_t - 1) * g.step * g.bpp;
+    const int wh = rows + (nb_t - 1) * g.step;
+    const int nvec = (e + wwb + 15) >> 4;
+    for (int i = threadIdx.x; i < wh * nvec; i += blockDim.x) {
+      int r = i / nvec, v = i - r * nvec;
+      *(uint4*)(P + r * L.WP + (v << 4)) =
+          *(const uint4*)(prev + (size_t)(gy0 + r) * pitch + gx0a + (v << 4));
+    }
+  }
+  __syncthreads();
+
+  const int t = threadIdx.x;
+  const int ntask = NAG * G * g.nstrip;
+  const bool active = t < ntask;
+  int ag = t % NAG, rest = t / NAG;
+  int grp = rest % G, st = rest / G;
+  if (!active) { ag = 0; grp = 0; st = 0; }
+  const int al0 = 2 * ag;
+  unsigned acc[2][TB];
+#pragma unroll
+  for (int j = 0; j < TB; j++) acc[0][j] = acc[1][j] = 0;
+  {
+    const int r0 = st * Rs;
+    const int cxb = e + al0 * g.step * g.bpp;
+    const int cxb1 = cxb + g.step * g.bpp;
+    const int sh0 = (cxb & 3) << 3, sh1 = (cxb1 & 3) << 3;
+    const int dw = (cxb1 >> 2) - (cxb >> 2);
+    const uint8_t* Pb = P + (size_t)(r0 + grp * TB * g.step) * L.WP + (cxb & ~3);
+    const uint4* C4 = (const uint4*)C + r0 * L.nq;
+    const int nrho = Rs + g.step * (TB - 1);
+    for (int rb = 0; rb < nrho;) {
+      int jhi = min(TB - 1, rb / g.step);
+      int jlo = rb < Rs ? 0 : (rb - Rs) / g.step + 1;
+      int re = jhi == TB - 1 ? nrho : min(nrho, (jhi + 1) * g.step);
+      int lo_next = Rs + jlo * g.step;
+      if (lo_next > rb && lo_next < re) re = lo_next;
+      rows_segment_ta2<TB>(acc, jlo, jhi, rb, re, g.step, Pb, L.WP, sh0, sh1, dw, C4, L.nq);
+      rb = re;
+    }
+  }
+  if (g.nstrip > 1) {
+    if (active && st > 0)
+#pragma unroll
+      for (int c = 0; c < 2; c++)
+#pragma unroll
+        for (int j = 0; j < TB; j++)
+          part[(((st - 1) * G + grp) * TB + j) * g.nab + al0 + c] = acc[c][j];
+    __syncthreads();
+    if (active && st == 0)
+      for (int s2 = 1; s2 < g.nstrip; s2++)
+#pragma unroll
+        for (int c = 0; c < 2; c++)
+#pragma unroll
+          for (int j = 0; j < TB; j++)
+            acc[c][j] += part[(((s2 - 1) * G + grp) * TB + j) * g.nab + al0 + c];
+  }
+  if (EMIT) {
+    if (active && st == 0) {
+      unsigned* out = g.emit + (size_t)item * g.na * g.nb;
+#pragma unroll
+      for (int c = 0; c < 2; c++)
+        if (al0 + c < na_t)
+#pragma unroll
+          for (int j = 0; j < TB; j++) {
+            int bl = grp * TB + j;
+            if (bl < nb_t) out[(b0 + bl) * g.na + (a0 + al0 + c)] = acc[c][j];
+          }
+    }
+    return;
+  }
+  unsigned long long best = ~0ull;
+  if (active && st == 0) {
+#pragma unroll
+    for (int c = 0; c < 2; c++)
+      if (al0 + c < na_t)
+#pragma unroll
+        for (int j = 0; j < TB; j++) {
+          int bl = grp * TB + j;
+          if (bl < nb_t) {
+            unsigned long long key = ((unsigned long long)acc[c][j] << 32) |
+                                     (unsigned)g.order[(b0 + bl) * g.na + (a0 + al0 + c)];
+            best = key < best ? key : best;
+          }
+        }
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  best = warp_min64(best);
+  if (lane == 0) red[warp] = best;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < nwarps; w++) best = red[w] < best ? red[w] : best;
+    atomicMin(&keys[item], best);
+    __threadfence();
+    unsigned tk = atomicAdd(&tickets[item], 1u);
+    s_last = (tk == ntiles - 1);
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  refine_and_store(g, L, it, C, P + 16, prev, pitch, keys, tickets, res, item, qsad);
+}
+
+/* grid (nta*ntb, items); block g.threads; dynamic smem tile_layout(g).total;
+   TA == g.ta (1 for 0) */
+template <int TB, bool EMIT = false, int TA = 1>
 __global__ void __launch_bounds__(512, 1) k_lattice(const uint8_t* __restrict__ curr,
                                                   const uint8_t* __restrict__ prev, int pitch,
                                                   DGeom g, const vsbd_item* __restrict__ items,
@@ -446,14 +688,14 @@ __global__ void __launch_bounds__(512, 1) k_lattice(const uint8_t* __restrict__ 
                                                   unsigned* __restrict__ tickets,
                                                   vsbd_result* __restrict__ res) {
   extern __shared__ __align__(16) uint8_t sm[];
-  lattice_tile<TB, EMIT>(curr, prev, pitch, g, items, keys, tickets, res, blockIdx.y, blockIdx.x,
+  lattice_tile<TB, EMIT, TA>(curr, prev, pitch, g, items, keys, tickets, res, blockIdx.y, blockIdx.x,
                          gridDim.x, sm);
 }
 
 /* Full search of the items listed in list[0 .. *count) (indices into
    items): persistent CTAs take the (item, tile) units in turn; the last
    tile of an item to finish refines it, as in k_lattice. */
-template <int TB>
+template <int TB, int TA = 1>
 __global__ void __launch_bounds__(512, 1) k_lattice_list(const uint8_t* __restrict__ curr,
                                                        const uint8_t* __restrict__ prev, int pitch,
                                                        DGeom g, const vsbd_item* __restrict__ items,
@@ -466,7 +708,7 @@ __global__ void __launch_bounds__(512, 1) k_lattice_list(const uint8_t* __restri
   const int ntiles = g.nta * g.ntb;
   const int nu = *count * ntiles;
   for (int u = blockIdx.x; u < nu; u += gridDim.x) {
-    lattice_tile<TB, false>(curr, prev, pitch, g, items, keys, tickets, res, list[u / ntiles],
+    lattice_tile<TB, false, TA>(curr, prev, pitch, g, items, keys, tickets, res, list[u / ntiles],
                             u % ntiles, ntiles, sm);
     __syncthreads();
   }
