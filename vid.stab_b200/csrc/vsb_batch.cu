@@ -36,7 +36,7 @@
 #include "vsb_prefilter.cuh"
 #include "vsb_search.cuh"
 
-#define VSB_BATCH_THREADS 256
+#define VSB_BATCH_THREADS 512
 #define VSB_BATCH_MAX_STREAMS 1024
 #define VSB_BATCH_MAX_CLASSES 64
 
@@ -106,12 +106,20 @@ __device__ __forceinline__ void search_tile(const BStream& S, const DGeom* geoms
   __syncthreads();
   const DGeom& g = *sg;
   const unsigned ntiles = (unsigned)(g.nta * g.ntb);
-  if (g.tb == 4)
+  if (g.ta == 2) {
+    if (g.tb == 4)
+      lattice_tile<4, false, 2>(S.cur, S.prev, S.pitch, g, items, keys, tickets, res, item, tile,
+                                ntiles, sm);
+    else
+      lattice_tile<2, false, 2>(S.cur, S.prev, S.pitch, g, items, keys, tickets, res, item, tile,
+                                ntiles, sm);
+  } else if (g.tb == 4) {
     lattice_tile<4, false>(S.cur, S.prev, S.pitch, g, items, keys, tickets, res, item, tile,
                            ntiles, sm);
-  else
+  } else {
     lattice_tile<2, false>(S.cur, S.prev, S.pitch, g, items, keys, tickets, res, item, tile,
                            ntiles, sm);
+  }
 }
 
 /* Stage A: the static work list `work`.  Stage B (work == NULL): item w of
@@ -251,10 +259,11 @@ static int same_geom(const vsbd_geom* a, const vsbd_geom* b) {
   return memcmp(a->order, b->order, sizeof(int32_t) * (size_t)a->na * a->nb) == 0;
 }
 
-/* a tiling the persistent kernel can run: TB 2 or 4, at most its block
-   size, tile and static shared memory within the per-block limit */
+/* a tiling the persistent kernel can run: TB 2 or 4, one or two columns
+   per thread, at most its block size, tile and static shared memory within
+   the per-block limit */
 static int tiling_ok(const vsbd_batch* b, const DGeom& g) {
-  return (g.tb == 2 || g.tb == 4) && g.ta != 2 && g.threads <= VSB_BATCH_THREADS &&
+  return (g.tb == 2 || g.tb == 4) && g.threads <= VSB_BATCH_THREADS &&
          tile_layout(g).total + b->static_smem + 64 <= (size_t)b->optin;
 }
 
@@ -386,15 +395,18 @@ static int autotune_class(vsbd_batch* b, int c, int is_fine) {
     if ((is_fine ? S.gf : S.gc) == c) nitems += is_fine ? S.nf : S.nc;
   }
   if (nitems == 0 || getenv("VSB_NO_AUTOTUNE")) return 0;
+  /* both layouts (one or two lattice columns per thread): the cost model
+     does not see the shared-memory loads in which they differ */
   TileCand cand[16];
-  int nc = vsbp_tile_candidates(b->cls[c].g, nitems, VSB_BATCH_THREADS, cand, 16);
+  int nc = vsbp_tile_candidates_ta(b->cls[c].g, nitems, VSB_BATCH_THREADS, cand, 8, 1);
+  nc += vsbp_tile_candidates_ta(b->cls[c].g, nitems, VSB_BATCH_THREADS, cand + nc, 8, 2);
   cudaEvent_t e0, e1;
   BCK(cudaEventCreate(&e0));
   BCK(cudaEventCreate(&e1));
   float best_ms = 1e30f;
   DGeom best = b->cls[c].g;
   int tried = 0;
-  for (int k = 0; k < nc && tried < 8; k++) {
+  for (int k = 0; k < nc && tried < 12; k++) {
     if (!tiling_ok(b, cand[k].g)) continue;
     tried++;
     DGeom t = cand[k].g;

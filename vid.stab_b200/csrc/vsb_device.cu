@@ -1690,6 +1690,10 @@ void vsbp_geom_free(GeomDev* g) { geom_free(g); }
 int vsbp_tile_candidates(const DGeom& g, int nitems, int max_threads, TileCand* out, int cap) {
   return tile_candidates(g, nitems, 0, 0, 0, 0, out, cap, max_threads);
 }
+int vsbp_tile_candidates_ta(const DGeom& g, int nitems, int max_threads, TileCand* out, int cap,
+                            int ta) {
+  return tile_candidates(g, nitems, 0, 0, 0, 0, out, cap, max_threads, ta);
+}
 int vsbp_sm_count(void) { return sm_count(); }
 void vsbp_set_err(const char* what, cudaError_t e) { set_err(what, e); }
 void vsbp_set_msg(const char* m) { set_msg(m); }

@@ -32,6 +32,9 @@ int vsbp_geom_upload(const vsbd_geom* h, int nitems, GeomDev* out);
 void vsbp_geom_free(GeomDev* g);
 /* the cap best tilings (model order) with at most max_threads threads */
 int vsbp_tile_candidates(const DGeom& g, int nitems, int max_threads, TileCand* out, int cap);
+/* the same, with ta lattice columns per thread only (1 or 2) */
+int vsbp_tile_candidates_ta(const DGeom& g, int nitems, int max_threads, TileCand* out, int cap,
+                            int ta);
 int vsbp_sm_count(void);
 void vsbp_set_err(const char* what, cudaError_t e);
 void vsbp_set_msg(const char* m);

@@ -57,7 +57,9 @@ __device__ __forceinline__ void blur_tile(const uint8_t* __restrict__ src, int s
     hor[r * BT_HORP + c] = (uint8_t)blur_div(acc, dv);
   }
   __syncthreads();
-  /* 256 threads: column c, upper or lower half of the tile rows */
+  /* 256 threads: column c, upper or lower half of the tile rows (threads
+     beyond 256, in larger blocks, have no column) */
+  if (threadIdx.x >= 2 * BT_W) return;
   const int c = threadIdx.x & (BT_W - 1);
   const int part = threadIdx.x >> 7;
   const int gx = x0 + c;
