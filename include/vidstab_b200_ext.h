@@ -195,7 +195,11 @@ VS_API int vsb_batch_detect(vsb_batch* b, const uint8_t* const* planes, const in
 /* nframes steps over clips: frame k of stream s at clips[s] + k *
    frame_bytes[s].  Records are appended step by step, stream by stream
    (LocalMotion layout, at most out_cap); counts[k*n + s] receives each
-   frame's count.  Returns the number of records, or -1. */
+   frame's count.  Without virtual tripod on any stream, consecutive steps
+   overlap on the GPU: step k+1's upload, blur, min/max and coarse search
+   run on one CUDA stream while step k's fine search runs on another and the
+   host assembles step k's motions (the results are vsb_batch_detect's, step
+   by step).  Returns the number of records, or -1. */
 VS_API long vsb_batch_run(vsb_batch* b, const uint8_t* const* clips, const long* frame_bytes,
                           const int* pitches, int nframes, int on_device, void* out,
                           long out_cap, int* counts);
@@ -204,6 +208,14 @@ VS_API void vsb_batch_free(vsb_batch* b);
 VS_API long vsb_batch_launch_count(const vsb_batch* b);
 /* the persistent grid: CTAs, threads per CTA, dynamic shared memory per CTA */
 VS_API int vsb_batch_grid(const vsb_batch* b, int* ctas, int* threads, long* smem);
+/* the search tiling of geometry class k (streams whose coarse or fine fields
+   share size, shift range and step share a class): desc[0..11] = lattice
+   rows and columns per thread, lattice columns and rows per CTA, field
+   strips, threads, shared memory bytes per CTA, CTAs per field, search items
+   per step, time of those items alone in the persistent kernel when tuned
+   (ns), field size, lattice points per field.  Returns the number of classes
+   (for any k, desc untouched when k is out of range), -1 without a batch. */
+VS_API int vsb_batch_class(const vsb_batch* b, int k, int* desc);
 
 /* ---- learned search proposal (no reference counterpart) ----------------
    The reference searches every field over its whole candidate lattice.  A

@@ -94,3 +94,38 @@ def test_batch_many_streams_of_one_size():
     for (g, gc), (e, ec) in zip(got, per_stream(frames)):
         assert np.array_equal(gc, ec)
         assert records_equal(g, e)
+
+
+@pytest.mark.parametrize("on_device", [False, True])
+def test_batch_run_overlap_mixed_with_per_step_calls(on_device):
+    # the overlapped run continues a batch stepped by vsb_batch_detect and is
+    # continued by it: the blurred-plane slots rotate consistently across both
+    sizes = [(640, 360), (1280, 720), (960, 540)]
+    T = 8
+    frames = [S.clip(w, h, T, seed=500 + i) for i, (w, h) in enumerate(sizes)]
+    b = V.Batch([w for w, _ in sizes], [h for _, h in sizes])
+    try:
+        pitches = [w for w, _ in sizes]
+        head = [b.detect([f[k].ctypes.data for f in frames], pitches, False) for k in range(2)]
+        mid = batch_records(b, [np.ascontiguousarray(f[2:6]) for f in frames], on_device)
+        tail = [b.detect([f[k].ctypes.data for f in frames], pitches, False) for k in range(6, T)]
+    finally:
+        b.close()
+    for s, (e, ec) in enumerate(per_stream(frames)):
+        got = [st[s] for st in head] + [mid[s][0]] + [st[s] for st in tail]
+        cnt = [len(st[s]) for st in head] + list(mid[s][1]) + [len(st[s]) for st in tail]
+        assert np.array_equal(cnt, ec)
+        assert records_equal(np.concatenate(got), e)
+
+
+def test_batch_run_with_tripod_stream():
+    # a virtual-tripod stream keeps its reference frame: the run steps serially
+    frames = [S.clip(640, 360, 6, seed=600 + i) for i in range(2)]
+    b = V.Batch([640, 640], [360, 360], tripod=3)
+    try:
+        got = batch_records(b, frames, True)
+    finally:
+        b.close()
+    for (g, gc), (e, ec) in zip(got, per_stream(frames, tripod=3)):
+        assert np.array_equal(gc, ec)
+        assert records_equal(g, e)

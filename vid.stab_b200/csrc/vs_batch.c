@@ -127,6 +127,95 @@ int vsb_batch_detect(vsb_batch* b, const uint8_t* const* planes, const int* pitc
   return VS_OK;
 }
 
+/* a step's motions into the record array */
+static long emit_step(vsb_batch* b, LocalMotions* lms, int k, LocalMotion* rec, long total,
+                      long cap, int* counts) {
+  for (int s = 0; s < b->n; s++) {
+    int m = vs_vector_size(&lms[s]);
+    if (counts) counts[(size_t)k * b->n + s] = m;
+    for (int i = 0; i < m; i++) {
+      if (rec && total < cap) rec[total] = *LMGet(&lms[s], i);
+      total++;
+    }
+    vs_vector_del(&lms[s]);
+  }
+  return total;
+}
+
+/* Overlap needs every stream's current frame to become its previous one
+   (no virtual tripod) and every stream past its first frame. */
+static int can_overlap(const vsb_batch* b, int check_seen) {
+  for (int s = 0; s < b->n; s++) {
+    if (b->md[s].conf.virtualTripod >= 1) return 0;
+    if (check_seen && !b->md[s].hasSeenOneFrame) return 0;
+  }
+  return 1;
+}
+
+/* Steps k0.. with consecutive steps overlapped on the GPU: stage B of step k
+   (fine search) runs on one CUDA stream while stage A of step k+1 (upload,
+   blur, min/max, coarse search of every stream) runs on the other and the
+   host assembles step k's motions.  Same results as vsb_batch_detect step by
+   step. */
+static long run_overlapped(vsb_batch* b, const uint8_t* const* clips, const long* frame_bytes,
+                           const int* pitches, int k0, int nframes, int on_device,
+                           const uint8_t** planes, LocalMotions* lms, LocalMotion* rec,
+                           long total, long cap, int* counts) {
+  for (int s = 0; s < b->n; s++) planes[s] = clips[s] + (size_t)k0 * frame_bytes[s];
+  if (vsbd_batch_stage_a(b->dev, planes, pitches, on_device) != 0) {
+    vs_log_error("vsb_batch", "GPU stage A failed: %s\n", vsbd_error());
+    return -1;
+  }
+  for (int k = k0; k < nframes; k++) {
+    /* wall time: [0] waiting for stage A, [1] host part A, [2] waiting for
+       stage B, [3] host part B */
+    double t0 = vsb_now_s(), prof[4] = { 0, 0, 0, 0 };
+    for (int s = 0; s < b->n; s++) {
+      const uint8_t* mm;
+      const vsbd_result* cres;
+      if (vsb_frame_begin(&b->md[s], &b->search[s]) != VS_OK || !b->search[s]) {
+        for (int q = 0; q < s; q++) vsb_frame_discard(&b->w[q]);
+        return -1;
+      }
+      vsbd_batch_results_a(b->dev, s, &mm, &cres);
+      vsb_frame_host_a(&b->md[s], mm, cres, &b->w[s]);
+      b->items[s] = b->w[s].fine_pass ? b->w[s].items : NULL;
+      b->nitems[s] = b->w[s].fine_pass ? b->w[s].nitems : 0;
+    }
+    const int next = k + 1 < nframes;
+    double t1 = vsb_now_s();
+    prof[1] = t1 - t0;
+    int rc = vsbd_batch_stage_b_issue(b->dev, b->items, b->nitems);
+    if (rc == 0 && next) {
+      for (int s = 0; s < b->n; s++) planes[s] = clips[s] + (size_t)(k + 1) * frame_bytes[s];
+      rc = vsbd_batch_stage_a_issue(b->dev, planes, pitches, on_device, 1);
+    }
+    if (rc == 0) rc = vsbd_batch_stage_b_collect(b->dev, b->fres);
+    double t2 = vsb_now_s();
+    prof[2] = t2 - t1;
+    if (rc != 0) {
+      vs_log_error("vsb_batch", "GPU stage failed: %s\n", vsbd_error());
+      if (next) vsbd_batch_stage_a_collect(b->dev);
+      for (int s = 0; s < b->n; s++) vsb_frame_discard(&b->w[s]);
+      return -1;
+    }
+    for (int s = 0; s < b->n; s++) {
+      vsb_frame_host_b(&b->md[s], b->fres[s], &b->w[s], &lms[s]);
+      if (vsb_frame_end(&b->md[s])) vsbd_batch_commit(b->dev, s);
+    }
+    total = emit_step(b, lms, k, rec, total, cap, counts);
+    double t3 = vsb_now_s();
+    prof[3] = t3 - t2;
+    if (next && vsbd_batch_stage_a_collect(b->dev) != 0) {
+      vs_log_error("vsb_batch", "GPU stage A failed: %s\n", vsbd_error());
+      return -1;
+    }
+    prof[0] = vsb_now_s() - t3;
+    vsb_prof_add(prof, b->n);
+  }
+  return total;
+}
+
 long vsb_batch_run(vsb_batch* b, const uint8_t* const* clips, const long* frame_bytes,
                    const int* pitches, int nframes, int on_device, void* out, long out_cap,
                    int* counts) {
@@ -135,21 +224,20 @@ long vsb_batch_run(vsb_batch* b, const uint8_t* const* clips, const long* frame_
   LocalMotions* lms = (LocalMotions*)malloc(sizeof(LocalMotions) * (size_t)b->n);
   LocalMotion* rec = (LocalMotion*)out;
   long total = 0;
-  for (int k = 0; k < nframes && total >= 0; k++) {
+  int k = 0;
+  const int overlap = can_overlap(b, 0);
+  for (; k < nframes && total >= 0; k++) {
+    if (overlap && can_overlap(b, 1) && nframes - k > 1) {
+      total = run_overlapped(b, clips, frame_bytes, pitches, k, nframes, on_device, planes, lms,
+                             rec, total, out_cap, counts);
+      break;
+    }
     for (int s = 0; s < b->n; s++) planes[s] = clips[s] + (size_t)k * frame_bytes[s];
     if (vsb_batch_detect(b, planes, pitches, on_device, lms) != VS_OK) {
       total = -1;
       break;
     }
-    for (int s = 0; s < b->n; s++) {
-      int m = vs_vector_size(&lms[s]);
-      if (counts) counts[(size_t)k * b->n + s] = m;
-      for (int i = 0; i < m; i++) {
-        if (rec && total < out_cap) rec[total] = *LMGet(&lms[s], i);
-        total++;
-      }
-      vs_vector_del(&lms[s]);
-    }
+    total = emit_step(b, lms, k, rec, total, out_cap, counts);
   }
   free(planes);
   free(lms);
@@ -157,6 +245,10 @@ long vsb_batch_run(vsb_batch* b, const uint8_t* const* clips, const long* frame_
 }
 
 long vsb_batch_launch_count(const vsb_batch* b) { return b ? vsbd_batch_launches(b->dev) : 0; }
+
+int vsb_batch_class(const vsb_batch* b, int k, int* desc) {
+  return b ? vsbd_batch_class(b->dev, k, desc) : -1;
+}
 
 int vsb_batch_grid(const vsb_batch* b, int* ctas, int* threads, long* smem) {
   return b && vsbd_batch_grid(b->dev, ctas, threads, smem) == 0 ? VS_OK : VS_ERROR;

@@ -659,6 +659,15 @@ static double now_s(void) {
   return ts.tv_sec + ts.tv_nsec * 1e-9;
 }
 
+void vsb_prof_add(const double* sec, long frames) {
+  pthread_mutex_lock(&g_lock);
+  for (int k = 0; k < 4; k++) g_prof[k] += sec[k];
+  g_prof_frames += frames;
+  pthread_mutex_unlock(&g_lock);
+}
+
+double vsb_now_s(void) { return now_s(); }
+
 void vsb_host_profile(double* sec, long* frames, int reset) {
   pthread_mutex_lock(&g_lock);
   if (sec)

@@ -194,16 +194,24 @@ struct vsbd_batch {
   /* geometry classes */
   GeomDev cls[VSB_BATCH_MAX_CLASSES];
   vsbd_geom cls_key[VSB_BATCH_MAX_CLASSES]; /* order: owned copy */
+  int cls_items[VSB_BATCH_MAX_CLASSES];     /* search items of the class per step */
+  float cls_us[VSB_BATCH_MAX_CLASSES];      /* tuned time of those items alone */
   size_t static_smem;                       /* of k_batch */
   int optin;                                /* per-block shared memory limit */
   size_t nkeys;
   DGeom* d_geoms;
   /* streams */
-  BStream* h_streams; /* pinned */
+  BStream* h_streams; /* pinned; stage A's descriptors */
   BStream* d_streams;
+  BStream* h_streamsB; /* stage B's descriptors (a step's planes while stage A of
+                          the next step runs) */
+  BStream* d_streamsB;
+  cudaStream_t st2;    /* stage B */
+  cudaEvent_t evA, evB;
   uint8_t** raw;      /* per stream: raw upload buffer (host input) */
-  uint8_t** buf[2];   /* per stream: blurred planes */
-  int* cur;           /* per stream: index of the current buffer */
+  uint8_t** buf[3];   /* per stream: blurred planes (current, previous, next) */
+  int* cur;           /* per stream: slot of the current frame */
+  int* prv;           /* per stream: slot of the previous frame */
   int16_t** d_xy;
   vsbd_item** d_citems;
   unsigned long long* d_keys;
@@ -234,6 +242,7 @@ struct vsbd_batch {
   size_t smem;
   int grid;
   cudaGraphExec_t gA, gB;
+  int b_pending;      /* a stage B was issued and not collected */
   long launches;
   long steps;
 };
@@ -456,6 +465,8 @@ static int autotune_class(vsbd_batch* b, int c, int is_fine) {
   BCK(cudaGetLastError());
   b->cls[c].g = best;
   b->cls[c].smem = tile_layout(best).total;
+  b->cls_items[c] = nitems;
+  b->cls_us[c] = best_ms < 1e29f ? 1000.f * best_ms / 3.f : 0.f;
   return 0;
 }
 
@@ -465,7 +476,8 @@ static int capture(vsbd_batch* b, int stageB, cudaGraphExec_t* out) {
   BCtl* ctl = stageB ? b->d_ctlB : b->d_ctlA;
   cudaMemsetAsync(ctl, 0, offsetof(BCtl, nwork), b->st);
   k_batch<<<b->grid, VSB_BATCH_THREADS, b->smem, b->st>>>(stageB ? NULL : b->d_workA,
-                                                          b->d_streams, b->d_geoms, ctl, b->d_pre,
+                                                          stageB ? b->d_streamsB : b->d_streams,
+                                                          b->d_geoms, ctl, b->d_pre,
                                                           b->d_pre + b->n + 1, b->d_fitems, b->n);
   if (stageB)
     cudaMemcpyAsync(b->h_resB, b->d_resB, sizeof(vsbd_result) * (size_t)(b->nf_total + 1),
@@ -486,12 +498,14 @@ extern "C" void vsbd_batch_destroy(vsbd_batch* b) {
   if (!b) return;
   cudaSetDevice(b->dev);
   if (b->st) cudaStreamSynchronize(b->st);
+  if (b->st2) cudaStreamSynchronize(b->st2);
   if (b->gA) cudaGraphExecDestroy(b->gA);
   if (b->gB) cudaGraphExecDestroy(b->gB);
   for (int s = 0; s < b->n; s++) {
     if (b->raw) cudaFree(b->raw[s]);
     if (b->buf[0]) cudaFree(b->buf[0][s]);
     if (b->buf[1]) cudaFree(b->buf[1][s]);
+    if (b->buf[2]) cudaFree(b->buf[2][s]);
     if (b->d_xy) cudaFree(b->d_xy[s]);
     if (b->d_citems) cudaFree(b->d_citems[s]);
   }
@@ -502,6 +516,11 @@ extern "C" void vsbd_batch_destroy(vsbd_batch* b) {
   cudaFree(b->d_geoms);
   cudaFree(b->d_streams);
   cudaFreeHost(b->h_streams);
+  cudaFree(b->d_streamsB);
+  cudaFreeHost(b->h_streamsB);
+  if (b->evA) cudaEventDestroy(b->evA);
+  if (b->evB) cudaEventDestroy(b->evB);
+  if (b->st2) cudaStreamDestroy(b->st2);
   cudaFree(b->d_keys);
   cudaFree(b->d_tickets);
   cudaFree(b->d_resA);
@@ -519,7 +538,9 @@ extern "C" void vsbd_batch_destroy(vsbd_batch* b) {
   free(b->raw);
   free(b->buf[0]);
   free(b->buf[1]);
+  free(b->buf[2]);
   free(b->cur);
+  free(b->prv);
   free(b->d_xy);
   free(b->d_citems);
   free(b->key_off);
@@ -558,10 +579,16 @@ extern "C" int vsbd_batch_create(vsbd_batch** out, int n, const vsbd_batch_strea
 #define CKB(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) { vsbp_set_err(#call, e_); vsbd_batch_destroy(b); return -1; } } while (0)
 #define FAILB() do { vsbd_batch_destroy(b); return -1; } while (0)
   CKB(cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking));
+  CKB(cudaStreamCreateWithFlags(&b->st2, cudaStreamNonBlocking));
+  CKB(cudaEventCreateWithFlags(&b->evA, cudaEventDisableTiming));
+  CKB(cudaEventCreateWithFlags(&b->evB, cudaEventDisableTiming));
   b->raw = (uint8_t**)calloc(n, sizeof(uint8_t*));
   b->buf[0] = (uint8_t**)calloc(n, sizeof(uint8_t*));
   b->buf[1] = (uint8_t**)calloc(n, sizeof(uint8_t*));
+  b->buf[2] = (uint8_t**)calloc(n, sizeof(uint8_t*));
   b->cur = (int*)calloc(n, sizeof(int));
+  b->prv = (int*)calloc(n, sizeof(int));
+  for (int s = 0; s < n; s++) b->prv[s] = 1;
   b->d_xy = (int16_t**)calloc(n, sizeof(int16_t*));
   b->d_citems = (vsbd_item**)calloc(n, sizeof(vsbd_item*));
   b->key_off = (size_t*)calloc(n, sizeof(size_t));
@@ -571,6 +598,8 @@ extern "C" int vsbd_batch_create(vsbd_batch** out, int n, const vsbd_batch_strea
   CKB(cudaMallocHost(&b->h_streams, sizeof(BStream) * n));
   memset(b->h_streams, 0, sizeof(BStream) * n);
   CKB(cudaMalloc(&b->d_streams, sizeof(BStream) * n));
+  CKB(cudaMallocHost(&b->h_streamsB, sizeof(BStream) * n));
+  CKB(cudaMalloc(&b->d_streamsB, sizeof(BStream) * n));
   CKB(cudaMalloc(&b->d_geoms, sizeof(DGeom) * VSB_BATCH_MAX_CLASSES));
   size_t nkeys = 0, resA = 0;
   int nf_total = 0;
@@ -604,10 +633,10 @@ extern "C" int vsbd_batch_create(vsbd_batch** out, int n, const vsbd_batch_strea
     S.gf = gf;
     size_t plane = (size_t)S.pitch * q.height + 256;
     CKB(cudaMalloc(&b->raw[s], plane));
-    CKB(cudaMalloc(&b->buf[0][s], plane));
-    CKB(cudaMalloc(&b->buf[1][s], plane));
-    CKB(cudaMemset(b->buf[0][s], 0, plane));
-    CKB(cudaMemset(b->buf[1][s], 0, plane));
+    for (int k = 0; k < 3; k++) {
+      CKB(cudaMalloc(&b->buf[k][s], plane));
+      CKB(cudaMemset(b->buf[k][s], 0, plane));
+    }
     CKB(cudaMalloc(&b->d_xy[s], sizeof(int16_t) * 2 * (size_t)(q.nc + q.nf) + 16));
     CKB(cudaMemcpy(b->d_xy[s], q.xy, sizeof(int16_t) * 2 * (size_t)(q.nc + q.nf),
                    cudaMemcpyHostToDevice));
@@ -729,8 +758,11 @@ extern "C" int vsbd_batch_create(vsbd_batch** out, int n, const vsbd_batch_strea
   return 0;
 }
 
-extern "C" int vsbd_batch_stage_a(vsbd_batch* b, const uint8_t* const* planes, const int* pitches,
-                                  int on_device) {
+/* Stage A of a step enqueued on the first stream: every stream's frame goes
+   to slot cur (next == 0) or, for the step after the current one, to the
+   third slot, searched against the current frame (next == 1). */
+extern "C" int vsbd_batch_stage_a_issue(vsbd_batch* b, const uint8_t* const* planes,
+                                        const int* pitches, int on_device, int next) {
   BCK(cudaSetDevice(b->dev));
   size_t h2d = 0;
   for (int s = 0; s < b->n; s++) {
@@ -745,15 +777,23 @@ extern "C" int vsbd_batch_stage_a(vsbd_batch* b, const uint8_t* const* planes, c
                             cudaMemcpyHostToDevice, b->st));
       h2d += (size_t)S.W * S.H;
     }
-    S.cur = b->buf[b->cur[s]][s];
-    S.prev = b->buf[b->cur[s] ^ 1][s];
+    const int ci = next ? 3 - b->cur[s] - b->prv[s] : b->cur[s];
+    const int pi = next ? b->cur[s] : b->prv[s];
+    S.cur = b->buf[ci][s];
+    S.prev = b->buf[pi][s];
   }
   BCK(cudaMemcpyAsync(b->d_streams, b->h_streams, sizeof(BStream) * b->n, cudaMemcpyHostToDevice,
                       b->st));
   BCK(cudaGraphLaunch(b->gA, b->st));
-  BCK(cudaStreamSynchronize(b->st));
+  BCK(cudaEventRecord(b->evA, b->st));
   b->launches++;
   vsbp_count(1, h2d + sizeof(BStream) * b->n, b->resA_bytes + 4);
+  return 0;
+}
+
+extern "C" int vsbd_batch_stage_a_collect(vsbd_batch* b) {
+  BCK(cudaSetDevice(b->dev));
+  BCK(cudaEventSynchronize(b->evA));
   if (b->h_nwork[2]) {
     vsbp_set_msg("batched stage A: a wait for blur tiles gave up");
     /* skipped tiles leave keys and tickets mid-way: start them afresh */
@@ -764,14 +804,22 @@ extern "C" int vsbd_batch_stage_a(vsbd_batch* b, const uint8_t* const* planes, c
   return 0;
 }
 
+extern "C" int vsbd_batch_stage_a(vsbd_batch* b, const uint8_t* const* planes, const int* pitches,
+                                  int on_device) {
+  if (vsbd_batch_stage_a_issue(b, planes, pitches, on_device, 0) != 0) return -1;
+  return vsbd_batch_stage_a_collect(b);
+}
+
 extern "C" void vsbd_batch_results_a(const vsbd_batch* b, int s, const uint8_t** mm,
                                      const vsbd_result** cres) {
   *mm = b->h_resA + b->mm_off[s];
   *cres = (const vsbd_result*)(b->h_resA + b->cres_off[s]);
 }
 
-extern "C" int vsbd_batch_stage_b(vsbd_batch* b, const vsbd_item* const* items, const int* nitems,
-                                  const vsbd_result** fres) {
+/* Stage B of the current step enqueued on the second stream, with its own
+   descriptors (the current and previous slots of every stream). */
+extern "C" int vsbd_batch_stage_b_issue(vsbd_batch* b, const vsbd_item* const* items,
+                                        const int* nitems) {
   BCK(cudaSetDevice(b->dev));
   int* pre = b->h_pre;
   int* off = b->h_pre + b->n + 1;
@@ -791,20 +839,37 @@ extern "C" int vsbd_batch_stage_b(vsbd_batch* b, const vsbd_item* const* items, 
     total += ni * g.nta * g.ntb;
   }
   pre[b->n] = total;
-  for (int s = 0; s < b->n; s++) fres[s] = b->h_resB + b->fres_off[s];
-  if (total == 0) return 0;
   b->h_nwork[0] = total;
+  b->b_pending = total > 0;
+  if (total == 0) return 0;
+  for (int s = 0; s < b->n; s++) {
+    b->h_streamsB[s] = b->h_streams[s];
+    b->h_streamsB[s].cur = b->buf[b->cur[s]][s];
+    b->h_streamsB[s].prev = b->buf[b->prv[s]][s];
+  }
+  BCK(cudaMemcpyAsync(b->d_streamsB, b->h_streamsB, sizeof(BStream) * b->n,
+                      cudaMemcpyHostToDevice, b->st2));
   BCK(cudaMemcpyAsync(b->d_pre, b->h_pre, sizeof(int) * (2 * (size_t)b->n + 1),
-                      cudaMemcpyHostToDevice, b->st));
+                      cudaMemcpyHostToDevice, b->st2));
   BCK(cudaMemcpyAsync(b->d_fitems, b->h_fitems, sizeof(vsbd_item) * (size_t)nit,
-                      cudaMemcpyHostToDevice, b->st));
+                      cudaMemcpyHostToDevice, b->st2));
   BCK(cudaMemcpyAsync(&b->d_ctlB->nwork, &b->h_nwork[0], sizeof(int), cudaMemcpyHostToDevice,
-                      b->st));
-  BCK(cudaGraphLaunch(b->gB, b->st));
-  BCK(cudaStreamSynchronize(b->st));
+                      b->st2));
+  BCK(cudaGraphLaunch(b->gB, b->st2));
+  BCK(cudaEventRecord(b->evB, b->st2));
   b->launches++;
-  vsbp_count(1, sizeof(int) * (2 * (size_t)b->n + 2) + sizeof(vsbd_item) * (size_t)nit,
+  vsbp_count(1, sizeof(BStream) * b->n + sizeof(int) * (2 * (size_t)b->n + 2) +
+                    sizeof(vsbd_item) * (size_t)nit,
              sizeof(vsbd_result) * (size_t)(b->nf_total + 1) + 4);
+  return 0;
+}
+
+extern "C" int vsbd_batch_stage_b_collect(vsbd_batch* b, const vsbd_result** fres) {
+  BCK(cudaSetDevice(b->dev));
+  for (int s = 0; s < b->n; s++) fres[s] = b->h_resB + b->fres_off[s];
+  if (!b->b_pending) return 0;
+  BCK(cudaEventSynchronize(b->evB));
+  b->b_pending = 0;
   if (b->h_nwork[1]) {
     vsbp_set_msg("batched stage B: the error flag was raised");
     return -1;
@@ -812,9 +877,40 @@ extern "C" int vsbd_batch_stage_b(vsbd_batch* b, const vsbd_item* const* items, 
   return 0;
 }
 
-extern "C" void vsbd_batch_commit(vsbd_batch* b, int s) { b->cur[s] ^= 1; }
+extern "C" int vsbd_batch_stage_b(vsbd_batch* b, const vsbd_item* const* items, const int* nitems,
+                                  const vsbd_result** fres) {
+  if (vsbd_batch_stage_b_issue(b, items, nitems) != 0) return -1;
+  return vsbd_batch_stage_b_collect(b, fres);
+}
+
+/* stream s's current frame becomes its previous one; the third slot takes
+   the next frame */
+extern "C" void vsbd_batch_commit(vsbd_batch* b, int s) {
+  const int f = 3 - b->cur[s] - b->prv[s];
+  b->prv[s] = b->cur[s];
+  b->cur[s] = f;
+}
 
 extern "C" long vsbd_batch_launches(const vsbd_batch* b) { return b ? b->launches : 0; }
+
+extern "C" int vsbd_batch_class(const vsbd_batch* b, int k, int* desc) {
+  if (!b) return -1;
+  if (k < 0 || k >= b->ncls || !desc) return b->ncls;
+  const DGeom& g = b->cls[k].g;
+  desc[0] = g.tb;
+  desc[1] = g.ta > 0 ? g.ta : 1;
+  desc[2] = g.nab;
+  desc[3] = g.nbb;
+  desc[4] = g.nstrip;
+  desc[5] = g.threads;
+  desc[6] = (int)tile_layout(g).total;
+  desc[7] = g.nta * g.ntb;
+  desc[8] = b->cls_items[k];
+  desc[9] = (int)(b->cls_us[k] * 1000.f);
+  desc[10] = g.S;
+  desc[11] = g.na * g.nb;
+  return b->ncls;
+}
 
 extern "C" int vsbd_batch_grid(const vsbd_batch* b, int* ctas, int* threads, long* smem) {
   if (!b) return -1;

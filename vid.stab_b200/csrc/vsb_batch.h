@@ -47,9 +47,25 @@ int vsbd_batch_stage_b(vsbd_batch* b, const vsbd_item* const* items, const int* 
 /* stream s's current blurred frame becomes its previous one */
 void vsbd_batch_commit(vsbd_batch* b, int stream);
 
+/* Overlapped steps: stage A enqueued only (next != 0: the step after the
+   current one, into every stream's third plane slot) and collected later;
+   stage B enqueued on a second stream and collected later, so that the next
+   step's stage A runs beside the current step's stage B. */
+int vsbd_batch_stage_a_issue(vsbd_batch* b, const uint8_t* const* planes, const int* pitches,
+                             int on_device, int next);
+int vsbd_batch_stage_a_collect(vsbd_batch* b);
+int vsbd_batch_stage_b_issue(vsbd_batch* b, const vsbd_item* const* items, const int* nitems);
+int vsbd_batch_stage_b_collect(vsbd_batch* b, const vsbd_result** fres);
+
 long vsbd_batch_launches(const vsbd_batch* b);
 /* persistent grid: CTAs, threads per CTA, dynamic shared memory per CTA */
 int vsbd_batch_grid(const vsbd_batch* b, int* ctas, int* threads, long* smem);
+/* geometry class k of the batch: desc[0..11] = lattice rows and columns per
+   thread, lattice columns and rows per CTA, field strips, threads, shared
+   memory bytes, CTAs per field, search items per step, tuned time of those
+   items alone in the persistent kernel (ns), field size, lattice points.
+   Returns the number of classes (also for k out of range). */
+int vsbd_batch_class(const vsbd_batch* b, int k, int* desc);
 
 #ifdef __cplusplus
 }

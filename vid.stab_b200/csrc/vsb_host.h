@@ -84,6 +84,11 @@ long vsb_detect_multi_impl(VSMotionDetect** mds, int n, const uint8_t* const* cl
                            const long* frame_bytes, const int* linesizes, int nframes,
                            int on_device, LocalMotion* rec, long out_cap, int* counts);
 
+/* adds wall times (device stage A, host A, device stage B, host B) of
+   `frames` frames to the profile vsb_host_profile reads; monotonic clock */
+void vsb_prof_add(const double* sec, long frames);
+double vsb_now_s(void);
+
 /* device context of an initialised detector (NULL if none) */
 vsbd_ctx* vsb_md_device(const VSMotionDetect* md);
 

@@ -154,6 +154,20 @@ class Batch:
         self.L.vsb_batch_grid(self.h, C.byref(a), C.byref(b), C.byref(c))
         return a.value, b.value, c.value
 
+    def classes(self):
+        """Per geometry class: the search tiling and its tuned time
+        (vsb_batch_class)."""
+        keys = ("rows_per_thread", "cols_per_thread", "cols_per_cta", "rows_per_cta", "strips",
+                "threads", "smem", "ctas_per_field", "items", "tuned_ns", "field_size",
+                "lattice_points")
+        n = self.L.vsb_batch_class(self.h, -1, None)
+        out = []
+        for k in range(n):
+            d = (C.c_int * 12)()
+            self.L.vsb_batch_class(self.h, k, d)
+            out.append(dict(zip(keys, list(d))))
+        return out
+
     def close(self):
         if self.h:
             self.L.vsb_batch_free(self.h)
