@@ -43,9 +43,11 @@ VS_API int vsb_set_search_mode(struct _vsmotiondetect* md, int pruned);
 VS_API void vsb_set_default_search_mode(int pruned);
 
 /* The search tiling the detector picked (cost model + timing at init) for
-   its coarse (fine = 0) or fine (1) fields: desc[0..7] = lattice rows and
-   columns per thread, lattice columns and rows per CTA, field strips,
-   threads per CTA, shared memory bytes per CTA, CTAs per field. */
+   its coarse (fine = 0) or fine (1) fields: desc[0..7] = lattice rows per
+   thread, layout (1: one lattice column per thread; 2: two, aligned by
+   shifts; 3: two of one byte alignment, read from word-aligned window
+   copies), lattice columns and rows per CTA, field strips, threads per CTA,
+   shared memory bytes per CTA, CTAs per field. */
 VS_API int vsb_search_tiling(const struct _vsmotiondetect* md, int fine, int* desc);
 
 /* Kernel launches issued for this detector so far. */
@@ -210,7 +212,7 @@ VS_API long vsb_batch_launch_count(const vsb_batch* b);
 VS_API int vsb_batch_grid(const vsb_batch* b, int* ctas, int* threads, long* smem);
 /* the search tiling of geometry class k (streams whose coarse or fine fields
    share size, shift range and step share a class): desc[0..11] = lattice
-   rows and columns per thread, lattice columns and rows per CTA, field
+   rows per thread, layout (as vsb_search_tiling), lattice columns and rows per CTA, field
    strips, threads, shared memory bytes per CTA, CTAs per field, search items
    per step, time of those items alone in the persistent kernel when tuned
    (ns), field size, lattice points per field.  Returns the number of classes

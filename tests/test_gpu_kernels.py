@@ -109,7 +109,8 @@ def orc_search(curr, prev, x, y, size, ms, step, ox=0, oy=0, bpp=0):
 
 def enc(tb, strips, nab, nbb, ta=0):
     """forced tiling: rows per thread, field strips, lattice columns / rows per
-    CTA, lattice columns per thread"""
+    CTA, layout (1 one column per thread, 2 two columns with shifts, 3 two
+    columns from aligned window copies)"""
     return ta * 100000000 + tb * 1000000 + strips * 10000 + nab * 100 + nbb
 
 
@@ -126,7 +127,15 @@ def enc(tb, strips, nab, nbb, ta=0):
                                                 (32, 32, 2, enc(4, 1, 34, 36, 2)),
                                                 (48, 33, 7, enc(4, 2, 4, 8, 2)),
                                                 (32, 20, 1, enc(2, 8, 42, 4, 2)),
-                                                (64, 40, 6, enc(2, 1, 2, 2, 2))])
+                                                (64, 40, 6, enc(2, 1, 2, 2, 2)),
+                                                (112, 60, 6, enc(4, 2, 8, 8, 3)),
+                                                (112, 154, 6, enc(2, 4, 12, 10, 3)),
+                                                (48, 30, 4, enc(2, 4, 6, 6, 3)),
+                                                (32, 32, 2, enc(4, 1, 36, 36, 3)),
+                                                (48, 32, 8, enc(2, 2, 6, 8, 3)),
+                                                (64, 40, 6, enc(2, 1, 4, 2, 3)),
+                                                (224, 40, 6, enc(2, 4, 8, 6, 3)),
+                                                (16, 16, 2, enc(4, 2, 4, 4, 3))])
 def test_field_search_planar(size, ms, step, tiles):
     w, h = 640, 480
     curr, prev = _blurred_pair(w, h, seed=size + step)
@@ -158,10 +167,12 @@ def test_field_search_ties():
     for curr, prev in [(flat, flat), (periodic, periodic), (periodic, np.roll(periodic, 3, 1)),
                        (stripes, stripes)]:
         for size, ms, step in [(32, 30, 6), (32, 32, 2), (16, 16, 2)]:
-            sad, tx, ty, ok = V.field_search(curr, prev, xs, ys, size, ms, step, tiles=enc(4, 2, 5, 4))
-            for k in range(3):
-                exp = orc_search(curr, prev, int(xs[k]), int(ys[k]), size, ms, step)
-                assert (sad[k], tx[k], ty[k], bool(ok[k])) == (exp[0], exp[1], exp[2], bool(exp[3]))
+            for tiles in (enc(4, 2, 5, 4), enc(4, 2, 8, 4, 3)):
+                sad, tx, ty, ok = V.field_search(curr, prev, xs, ys, size, ms, step, tiles=tiles)
+                for k in range(3):
+                    exp = orc_search(curr, prev, int(xs[k]), int(ys[k]), size, ms, step)
+                    assert (sad[k], tx[k], ty[k], bool(ok[k])) == (exp[0], exp[1], exp[2],
+                                                                   bool(exp[3]))
 
 
 @pytest.mark.parametrize("bpp", [3, 4])
@@ -172,8 +183,11 @@ def test_field_search_packed(bpp):
     prev = S.to_packed(prev_l, bpp)
     xs = np.array([90, 160, 230, 120], np.int16)
     ys = np.array([90, 120, 150, 130], np.int16)
-    for size, ms, step in [(32, 34, 6), (16, 16, 2)]:
-        sad, tx, ty, ok = V.field_search(curr, prev, xs, ys, size, ms, step, packed_bpp=bpp)
+    # the aligned two-column layout serves packed rows too (step 2: 6 or 8
+    # bytes per lattice step)
+    for size, ms, step, tiles in [(32, 34, 6, 0), (16, 16, 2, 0), (16, 16, 2, enc(2, 2, 8, 4, 3))]:
+        sad, tx, ty, ok = V.field_search(curr, prev, xs, ys, size, ms, step, packed_bpp=bpp,
+                                         tiles=tiles)
         for k in range(len(xs)):
             exp = orc_search(curr, prev, int(xs[k]), int(ys[k]), size, ms, step, bpp=bpp)
             assert (sad[k], tx[k], ty[k], bool(ok[k])) == (exp[0], exp[1], exp[2], bool(exp[3]))

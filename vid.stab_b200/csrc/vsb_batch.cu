@@ -106,7 +106,14 @@ __device__ __forceinline__ void search_tile(const BStream& S, const DGeom* geoms
   __syncthreads();
   const DGeom& g = *sg;
   const unsigned ntiles = (unsigned)(g.nta * g.ntb);
-  if (g.ta == 2) {
+  if (g.ta == 3) {
+    if (g.tb == 4)
+      lattice_tile<4, false, 3>(S.cur, S.prev, S.pitch, g, items, keys, tickets, res, item, tile,
+                                ntiles, sm);
+    else
+      lattice_tile<2, false, 3>(S.cur, S.prev, S.pitch, g, items, keys, tickets, res, item, tile,
+                                ntiles, sm);
+  } else if (g.ta == 2) {
     if (g.tb == 4)
       lattice_tile<4, false, 2>(S.cur, S.prev, S.pitch, g, items, keys, tickets, res, item, tile,
                                 ntiles, sm);
@@ -404,18 +411,20 @@ static int autotune_class(vsbd_batch* b, int c, int is_fine) {
     if ((is_fine ? S.gf : S.gc) == c) nitems += is_fine ? S.nf : S.nc;
   }
   if (nitems == 0 || getenv("VSB_NO_AUTOTUNE")) return 0;
-  /* both layouts (one or two lattice columns per thread): the cost model
-     does not see the shared-memory loads in which they differ */
-  TileCand cand[16];
-  int nc = vsbp_tile_candidates_ta(b->cls[c].g, nitems, VSB_BATCH_THREADS, cand, 8, 1);
-  nc += vsbp_tile_candidates_ta(b->cls[c].g, nitems, VSB_BATCH_THREADS, cand + nc, 8, 2);
+  /* all three layouts (one lattice column per thread; two with shifts; two
+     from aligned window copies): the cost model does not see the
+     shared-memory loads and shifts in which they differ */
+  TileCand cand[20];
+  int nc = vsbp_tile_candidates_ta(b->cls[c].g, nitems, VSB_BATCH_THREADS, cand, 6, 1);
+  nc += vsbp_tile_candidates_ta(b->cls[c].g, nitems, VSB_BATCH_THREADS, cand + nc, 6, 2);
+  nc += vsbp_tile_candidates_ta(b->cls[c].g, nitems, VSB_BATCH_THREADS, cand + nc, 8, 3);
   cudaEvent_t e0, e1;
   BCK(cudaEventCreate(&e0));
   BCK(cudaEventCreate(&e1));
   float best_ms = 1e30f;
   DGeom best = b->cls[c].g;
   int tried = 0;
-  for (int k = 0; k < nc && tried < 12; k++) {
+  for (int k = 0; k < nc && tried < 16; k++) {
     if (!tiling_ok(b, cand[k].g)) continue;
     tried++;
     DGeom t = cand[k].g;

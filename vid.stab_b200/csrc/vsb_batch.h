@@ -60,8 +60,8 @@ int vsbd_batch_stage_b_collect(vsbd_batch* b, const vsbd_result** fres);
 long vsbd_batch_launches(const vsbd_batch* b);
 /* persistent grid: CTAs, threads per CTA, dynamic shared memory per CTA */
 int vsbd_batch_grid(const vsbd_batch* b, int* ctas, int* threads, long* smem);
-/* geometry class k of the batch: desc[0..11] = lattice rows and columns per
-   thread, lattice columns and rows per CTA, field strips, threads, shared
+/* geometry class k of the batch: desc[0..11] = lattice rows per thread,
+   layout (1, 2 or 3: DGeom::ta), lattice columns and rows per CTA, field strips, threads, shared
    memory bytes, CTAs per field, search items per step, tuned time of those
    items alone in the persistent kernel (ns), field size, lattice points.
    Returns the number of classes (also for k out of range). */

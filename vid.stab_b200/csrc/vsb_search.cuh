@@ -44,8 +44,10 @@ struct DGeom {
   int nta, ntb;         /* tiles along a / along b */
   int nstrip;           /* field rows split into this many strips */
   int threads;          /* block size */
-  int ta;               /* lattice columns per thread: 1 (or 0), or 2 -- a window row's words
-                           then serve two candidate columns (planar, step*bpp <= 8) */
+  int ta;               /* lattice columns per thread: 1 (or 0); 2 -- a window row's words
+                           then serve two candidate columns (step*bpp <= 8); 3 -- two columns
+                           of one byte alignment, read from window copies staged word-aligned
+                           for them (step*bpp even and <= 8): no shifts in the sums */
   int rows;             /* field rows a launch sums (0: all S); fewer rows give
                            every candidate a lower bound of its SAD */
   unsigned* emit;       /* emit mode: per item, per lattice point, the sum */
@@ -75,8 +77,16 @@ struct TileLayout {
   int WP, WH_alloc;  /* previous-frame window: row pitch, rows */
   int RP, RH;        /* refinement window: row pitch (bytes), rows */
   int FP;            /* row pitch of the staged current-field rows */
+  int CP;            /* ta == 3: distance of the second window copy from the first */
   size_t off_P, off_part, off_q, total;
 };
+
+/* window copies of a ta == 3 tile: two when the lattice step in bytes is 2
+   mod 4 (even and odd lattice columns fall on different byte alignments),
+   else one */
+__host__ __device__ inline int window_copies(const DGeom& g) {
+  return g.ta == 3 && ((g.step * g.bpp) & 3) ? 2 : 1;
+}
 
 /* total reach of the refinement rounds around the lattice winner */
 __host__ __device__ inline int refine_reach(const DGeom& g) {
@@ -99,7 +109,10 @@ __host__ __device__ inline TileLayout tile_layout(const DGeom& g) {
   L.RP = ((3 + L.rowB + 2 * R * g.bpp + 8 + 15) >> 4) << 4;
   L.FP = ((L.rowB + 15 + 15) >> 4 << 4) + 16;
   L.off_P = (size_t)rows * L.rowB;
-  size_t parea = (size_t)L.WH_alloc * L.WP;
+  /* the second copy sits one word off a 16-byte boundary, so that a warp's
+     even- and odd-column threads read different banks */
+  L.CP = L.WH_alloc * L.WP + 4;
+  size_t parea = (size_t)window_copies(g) * L.CP;
   size_t rarea = g.rows > 0 ? 0 : (size_t)L.RH * L.RP + 16;
   size_t farea = (size_t)rows * L.FP;
   if (rarea > parea) parea = rarea;
@@ -374,7 +387,102 @@ __device__ __forceinline__ void rows_segment_ta2(unsigned (&acc)[2][TB], int jlo
     rows_segment_ta2_dw<TB, 0>(acc, jlo, jhi, rb, re, step, Pb, WP, sh0, sh1, C4, nq);
 }
 
-template <int TB, bool EMIT>
+/* Rows [rb, re) for a thread owning two lattice columns of one byte
+   alignment (ta == 3): both read whole words of a window copy staged for
+   that alignment, the second DW words right of the first.  Each quad of a
+   window row is four new words (DW carried): the first column sums words
+   0..3 of carry+new, the second the four new ones. */
+template <int TB, int JLO, int JHI, int DW>
+__device__ __forceinline__ void rows_active_al(unsigned (&acc)[2][TB], int rb, int re, int step,
+                                               const uint32_t* __restrict__ Pw0, int WPw,
+                                               const uint4* __restrict__ C4, int nq) {
+  for (int rho = rb; rho < re; rho++) {
+    const uint32_t* Pw = Pw0 + rho * WPw;
+    const uint4* Cj[TB];
+#pragma unroll
+    for (int j = JLO; j <= JHI; j++) Cj[j] = C4 + (rho - step * j) * nq;
+    uint32_t cr[DW];
+#pragma unroll
+    for (int k = 0; k < DW; k++) cr[k] = Pw[k];
+    for (int q = 0; q < nq; q++) {
+      const uint32_t n0 = Pw[4 * q + DW], n1 = Pw[4 * q + DW + 1], n2 = Pw[4 * q + DW + 2],
+                     n3 = Pw[4 * q + DW + 3];
+      /* the first column's words: the first four of carry + new */
+      uint32_t X[4];
+      if constexpr (DW == 1) {
+        X[0] = cr[0]; X[1] = n0; X[2] = n1; X[3] = n2;
+        cr[0] = n3;
+      } else if constexpr (DW == 2) {
+        X[0] = cr[0]; X[1] = cr[1]; X[2] = n0; X[3] = n1;
+        cr[0] = n2; cr[1] = n3;
+      } else {
+        X[0] = cr[0]; X[1] = cr[1]; X[2] = cr[2]; X[3] = n0;
+        cr[0] = n1; cr[1] = n2; cr[2] = n3;
+      }
+#pragma unroll
+      for (int j = JLO; j <= JHI; j++) {
+        const uint4 c = Cj[j][q];
+        acc[0][j] = sad4(c.x, X[0], acc[0][j]);
+        acc[1][j] = sad4(c.x, n0, acc[1][j]);
+        acc[0][j] = sad4(c.y, X[1], acc[0][j]);
+        acc[1][j] = sad4(c.y, n1, acc[1][j]);
+        acc[0][j] = sad4(c.z, X[2], acc[0][j]);
+        acc[1][j] = sad4(c.z, n2, acc[1][j]);
+        acc[0][j] = sad4(c.w, X[3], acc[0][j]);
+        acc[1][j] = sad4(c.w, n3, acc[1][j]);
+      }
+    }
+  }
+}
+
+template <int TB, int DW>
+__device__ __forceinline__ void rows_segment_al_dw(unsigned (&acc)[2][TB], int jlo, int jhi,
+                                                   int rb, int re, int step, const uint32_t* Pw0,
+                                                   int WPw, const uint4* C4, int nq) {
+#define VSB_SEG3(L, H)                                                      \
+  if (jlo == L && jhi == H) {                                               \
+    rows_active_al<TB, L, H, DW>(acc, rb, re, step, Pw0, WPw, C4, nq);      \
+    return;                                                                 \
+  }
+  if constexpr (TB == 2) {
+    VSB_SEG3(0, 0) VSB_SEG3(0, 1) VSB_SEG3(1, 1)
+  } else if constexpr (TB == 4) {
+    VSB_SEG3(0, 0) VSB_SEG3(0, 1) VSB_SEG3(0, 2) VSB_SEG3(0, 3)
+    VSB_SEG3(1, 1) VSB_SEG3(1, 2) VSB_SEG3(1, 3)
+    VSB_SEG3(2, 2) VSB_SEG3(2, 3)
+    VSB_SEG3(3, 3)
+  }
+#undef VSB_SEG3
+}
+
+/* DW (1..3: the lattice step in bytes times the column distance, in words)
+   is uniform per tile */
+template <int TB>
+__device__ __forceinline__ void rows_segment_al(unsigned (&acc)[2][TB], int jlo, int jhi, int rb,
+                                                int re, int step, const uint32_t* Pw0, int WPw,
+                                                int dw, const uint4* C4, int nq) {
+  if (dw == 3)
+    rows_segment_al_dw<TB, 3>(acc, jlo, jhi, rb, re, step, Pw0, WPw, C4, nq);
+  else if (dw == 2)
+    rows_segment_al_dw<TB, 2>(acc, jlo, jhi, rb, re, step, Pw0, WPw, C4, nq);
+  else
+    rows_segment_al_dw<TB, 1>(acc, jlo, jhi, rb, re, step, Pw0, WPw, C4, nq);
+}
+
+/* bytes o .. o+15 of the 32 bytes lo:hi, o = 4*wo + sh/8 (wo uniform) */
+__device__ __forceinline__ uint4 extract16(uint4 lo, uint4 hi, int wo, int sh) {
+  uint32_t w0, w1, w2, w3, w4;
+  switch (wo) {
+    case 0: w0 = lo.x; w1 = lo.y; w2 = lo.z; w3 = lo.w; w4 = hi.x; break;
+    case 1: w0 = lo.y; w1 = lo.z; w2 = lo.w; w3 = hi.x; w4 = hi.y; break;
+    case 2: w0 = lo.z; w1 = lo.w; w2 = hi.x; w3 = hi.y; w4 = hi.z; break;
+    default: w0 = lo.w; w1 = hi.x; w2 = hi.y; w3 = hi.z; w4 = hi.w; break;
+  }
+  return make_uint4(__funnelshift_r(w0, w1, sh), __funnelshift_r(w1, w2, sh),
+                    __funnelshift_r(w2, w3, sh), __funnelshift_r(w3, w4, sh));
+}
+
+template <int TB, bool EMIT, bool AL>
 __device__ void lattice_tile_ta2(const uint8_t* __restrict__ curr, const uint8_t* __restrict__ prev,
                                  int pitch, const DGeom& g, const vsbd_item* __restrict__ items,
                                  unsigned long long* __restrict__ keys,
@@ -384,7 +492,7 @@ __device__ void lattice_tile_ta2(const uint8_t* __restrict__ curr, const uint8_t
 /* One lattice tile of one item, by one CTA: tile = tbi*nta + tai of the
    item's ntiles = nta*ntb tiles; sm: tile_layout(g).total bytes of shared
    memory.  The last of the item's CTAs to finish refines and stores.  TA:
-   lattice columns per thread (1, or 2 for tilings with g.ta == 2). */
+   the tiling's g.ta (1, 2 or 3; 1 for g.ta == 0). */
 template <int TB, bool EMIT, int TA = 1>
 __device__ __forceinline__ void lattice_tile(const uint8_t* __restrict__ curr,
                                              const uint8_t* __restrict__ prev, int pitch,
@@ -393,9 +501,9 @@ __device__ __forceinline__ void lattice_tile(const uint8_t* __restrict__ curr,
                                              unsigned* __restrict__ tickets,
                                              vsbd_result* __restrict__ res, int item, int tile,
                                              unsigned ntiles, uint8_t* sm) {
-  if constexpr (TA == 2) {
-    lattice_tile_ta2<TB, EMIT>(curr, prev, pitch, g, items, keys, tickets, res, item, tile,
-                               ntiles, sm);
+  if constexpr (TA == 2 || TA == 3) {
+    lattice_tile_ta2<TB, EMIT, TA == 3>(curr, prev, pitch, g, items, keys, tickets, res, item,
+                                        tile, ntiles, sm);
     return;
   }
   __shared__ unsigned long long red[32];
@@ -530,10 +638,15 @@ __device__ __forceinline__ void lattice_tile(const uint8_t* __restrict__ curr,
   refine_and_store(g, L, it, C, P + 16, prev, pitch, keys, tickets, res, item, qsad);
 }
 
-/* lattice_tile for two columns per thread (g.ta == 2, nab even): thread t
-   owns columns 2*(t % (nab/2)) and the next, TB rows of a row group and a
-   strip of the field.  Same sums, keys and refinement as lattice_tile. */
-template <int TB, bool EMIT>
+/* lattice_tile for two columns per thread, TB rows of a row group and a
+   strip of the field; same sums, keys and refinement as lattice_tile.
+   g.ta == 2 (AL false, nab even): thread t owns columns 2*(t % (nab/2)) and
+   the next, aligned by funnel shifts.  g.ta == 3 (AL true): the columns of
+   one byte alignment pair up -- a and a+2 (a = 4*(p/2) + p%2 for pair p,
+   nab a multiple of 4) when the step in bytes is 2 mod 4, else a = 2p and
+   a+1 -- and each alignment has its own window copy, staged so that its
+   columns start on word boundaries. */
+template <int TB, bool EMIT, bool AL>
 __device__ void lattice_tile_ta2(const uint8_t* __restrict__ curr, const uint8_t* __restrict__ prev,
                                  int pitch, const DGeom& g, const vsbd_item* __restrict__ items,
                                  unsigned long long* __restrict__ keys,
@@ -575,14 +688,48 @@ __device__ void lattice_tile_ta2(const uint8_t* __restrict__ curr, const uint8_t
   const int gx0 = (it.x - g.S / 2 + it.ox + g.ax0 + a0 * g.step) * g.bpp;
   const int gy0 = it.y - g.S / 2 + it.oy + g.by0 + b0 * g.step;
   const int gx0a = gx0 & ~15, e = gx0 - gx0a;
+  const int sb = g.step * g.bpp; /* lattice step in bytes */
+  const int dcol = AL && (sb & 3) ? 2 : 1;
   {
-    const int wwb = L.rowB + (na_t - 1) * g.step * g.bpp;
+    const int wwb = L.rowB + (na_t - 1) * sb;
     const int wh = rows + (nb_t - 1) * g.step;
     const int nvec = (e + wwb + 15) >> 4;
-    for (int i = threadIdx.x; i < wh * nvec; i += blockDim.x) {
-      int r = i / nvec, v = i - r * nvec;
-      *(uint4*)(P + r * L.WP + (v << 4)) =
-          *(const uint4*)(prev + (size_t)(gy0 + r) * pitch + gx0a + (v << 4));
+    if constexpr (!AL) {
+      for (int i = threadIdx.x; i < wh * nvec; i += blockDim.x) {
+        int r = i / nvec, v = i - r * nvec;
+        *(uint4*)(P + r * L.WP + (v << 4)) =
+            *(const uint4*)(prev + (size_t)(gy0 + r) * pitch + gx0a + (v << 4));
+      }
+    } else {
+      /* copy c starts at window byte c*sb: the columns c, c + 2*dcol, ... (and
+         their partners) begin on its word boundaries.  Only the aligned
+         16-byte chunks the plain staging reads are read. */
+      for (int c = 0; c < dcol; c++) {
+        const int bytes = L.rowB + max(na_t - 1 - c, 0) * sb;
+        const int ob = e + c * sb;
+        const int o = ob & 15, wo = o >> 2, sh = (o & 3) << 3, u00 = ob >> 4;
+        const int nvo = (bytes + 15) >> 4;
+        uint8_t* Pc = P + c * L.CP;
+        for (int i = threadIdx.x; i < wh * nvo; i += blockDim.x) {
+          const int r = i / nvo, v = i - r * nvo;
+          const uint8_t* row = prev + (size_t)(gy0 + r) * pitch + gx0a;
+          const int u0 = u00 + v;
+          uint4 lo = make_uint4(0u, 0u, 0u, 0u), hi = lo;
+          if (u0 < nvec) lo = *(const uint4*)(row + (u0 << 4));
+          if (o && u0 + 1 < nvec) hi = *(const uint4*)(row + ((u0 + 1) << 4));
+          const uint4 w = extract16(lo, hi, wo, sh);
+          uint8_t* dst = Pc + r * L.WP + (v << 4);
+          if (c == 0) {
+            *(uint4*)dst = w;
+          } else {
+            uint32_t* d4 = (uint32_t*)dst;
+            d4[0] = w.x;
+            d4[1] = w.y;
+            d4[2] = w.z;
+            d4[3] = w.w;
+          }
+        }
+      }
     }
   }
   __syncthreads();
@@ -593,17 +740,23 @@ __device__ void lattice_tile_ta2(const uint8_t* __restrict__ curr, const uint8_t
   int ag = t % NAG, rest = t / NAG;
   int grp = rest % G, st = rest / G;
   if (!active) { ag = 0; grp = 0; st = 0; }
-  const int al0 = 2 * ag;
+  /* the thread's two columns and, for AL, the copy it reads */
+  const int cls = dcol == 2 ? (ag & 1) : 0;
+  const int al0 = dcol == 2 ? 4 * (ag >> 1) + cls : 2 * ag;
+  const int col[2] = { al0, al0 + dcol };
   unsigned acc[2][TB];
 #pragma unroll
   for (int j = 0; j < TB; j++) acc[0][j] = acc[1][j] = 0;
   {
     const int r0 = st * Rs;
-    const int cxb = e + al0 * g.step * g.bpp;
-    const int cxb1 = cxb + g.step * g.bpp;
+    const int cxb = e + al0 * sb;
+    const int cxb1 = cxb + sb;
     const int sh0 = (cxb & 3) << 3, sh1 = (cxb1 & 3) << 3;
-    const int dw = (cxb1 >> 2) - (cxb >> 2);
-    const uint8_t* Pb = P + (size_t)(r0 + grp * TB * g.step) * L.WP + (cxb & ~3);
+    const int dw = AL ? (sb * dcol) >> 2 : (cxb1 >> 2) - (cxb >> 2);
+    const size_t rowoff = (size_t)(r0 + grp * TB * g.step) * L.WP;
+    const uint8_t* Pb = P + rowoff + (cxb & ~3);
+    /* AL: column al0 starts at byte (al0 - cls)*sb of copy cls, a word boundary */
+    const uint32_t* Pw0 = (const uint32_t*)(P + cls * L.CP + rowoff) + (((al0 - cls) * sb) >> 2);
     const uint4* C4 = (const uint4*)C + r0 * L.nq;
     const int nrho = Rs + g.step * (TB - 1);
     for (int rb = 0; rb < nrho;) {
@@ -612,7 +765,10 @@ __device__ void lattice_tile_ta2(const uint8_t* __restrict__ curr, const uint8_t
       int re = jhi == TB - 1 ? nrho : min(nrho, (jhi + 1) * g.step);
       int lo_next = Rs + jlo * g.step;
       if (lo_next > rb && lo_next < re) re = lo_next;
-      rows_segment_ta2<TB>(acc, jlo, jhi, rb, re, g.step, Pb, L.WP, sh0, sh1, dw, C4, L.nq);
+      if constexpr (AL)
+        rows_segment_al<TB>(acc, jlo, jhi, rb, re, g.step, Pw0, L.WP >> 2, dw, C4, L.nq);
+      else
+        rows_segment_ta2<TB>(acc, jlo, jhi, rb, re, g.step, Pb, L.WP, sh0, sh1, dw, C4, L.nq);
       rb = re;
     }
   }
@@ -622,7 +778,7 @@ __device__ void lattice_tile_ta2(const uint8_t* __restrict__ curr, const uint8_t
       for (int c = 0; c < 2; c++)
 #pragma unroll
         for (int j = 0; j < TB; j++)
-          part[(((st - 1) * G + grp) * TB + j) * g.nab + al0 + c] = acc[c][j];
+          part[(((st - 1) * G + grp) * TB + j) * g.nab + col[c]] = acc[c][j];
     __syncthreads();
     if (active && st == 0)
       for (int s2 = 1; s2 < g.nstrip; s2++)
@@ -630,18 +786,18 @@ __device__ void lattice_tile_ta2(const uint8_t* __restrict__ curr, const uint8_t
         for (int c = 0; c < 2; c++)
 #pragma unroll
           for (int j = 0; j < TB; j++)
-            acc[c][j] += part[(((s2 - 1) * G + grp) * TB + j) * g.nab + al0 + c];
+            acc[c][j] += part[(((s2 - 1) * G + grp) * TB + j) * g.nab + col[c]];
   }
   if (EMIT) {
     if (active && st == 0) {
       unsigned* out = g.emit + (size_t)item * g.na * g.nb;
 #pragma unroll
       for (int c = 0; c < 2; c++)
-        if (al0 + c < na_t)
+        if (col[c] < na_t)
 #pragma unroll
           for (int j = 0; j < TB; j++) {
             int bl = grp * TB + j;
-            if (bl < nb_t) out[(b0 + bl) * g.na + (a0 + al0 + c)] = acc[c][j];
+            if (bl < nb_t) out[(b0 + bl) * g.na + (a0 + col[c])] = acc[c][j];
           }
     }
     return;
@@ -650,13 +806,13 @@ __device__ void lattice_tile_ta2(const uint8_t* __restrict__ curr, const uint8_t
   if (active && st == 0) {
 #pragma unroll
     for (int c = 0; c < 2; c++)
-      if (al0 + c < na_t)
+      if (col[c] < na_t)
 #pragma unroll
         for (int j = 0; j < TB; j++) {
           int bl = grp * TB + j;
           if (bl < nb_t) {
             unsigned long long key = ((unsigned long long)acc[c][j] << 32) |
-                                     (unsigned)g.order[(b0 + bl) * g.na + (a0 + al0 + c)];
+                                     (unsigned)g.order[(b0 + bl) * g.na + (a0 + col[c])];
             best = key < best ? key : best;
           }
         }

@@ -157,7 +157,7 @@ class Batch:
     def classes(self):
         """Per geometry class: the search tiling and its tuned time
         (vsb_batch_class)."""
-        keys = ("rows_per_thread", "cols_per_thread", "cols_per_cta", "rows_per_cta", "strips",
+        keys = ("rows_per_thread", "layout", "cols_per_cta", "rows_per_cta", "strips",
                 "threads", "smem", "ctas_per_field", "items", "tuned_ns", "field_size",
                 "lattice_points")
         n = self.L.vsb_batch_class(self.h, -1, None)
