@@ -10,6 +10,7 @@ floating-point flags of the reference's shipped build (-O3 -msse2
     python vid.stab_b200/build.py [--verbose] [--ptxas-v]
 """
 import argparse
+import concurrent.futures
 import os
 import shutil
 import subprocess
@@ -79,6 +80,7 @@ def build(verbose=False, ptxas_v=False, force=False):
         if force or newer([src] + hdrs, obj):
             flags = COMMON_C + (REFFP_FLAGS if f in REFFP_C else [])
             run([CC] + flags + ["-c", src, "-o", obj], verbose)
+    jobs = []
     for f in CU:
         src = os.path.join(CSRC, f)
         if not os.path.exists(src):
@@ -87,7 +89,10 @@ def build(verbose=False, ptxas_v=False, force=False):
         objs.append(obj)
         if force or ptxas_v or newer([src] + hdrs, obj):
             extra = ["-Xptxas", "-v"] if ptxas_v else []
-            out = run([NVCC] + NVCC_FLAGS + extra + ["-c", src, "-o", obj], verbose)
+            jobs.append([NVCC] + NVCC_FLAGS + extra + ["-c", src, "-o", obj])
+    # the CUDA translation units compile independently: one nvcc each, in parallel
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        for out in ex.map(lambda cmd: run(cmd, verbose), jobs):
             if ptxas_v and out:
                 print(out)
     if force or newer(objs, LIB):

@@ -98,6 +98,20 @@ __device__ __forceinline__ int wait_blur(BCtl* ctl, int s, unsigned target) {
   return s_ok;
 }
 
+/* One search tile of a layout as a called (not inlined) function: each
+   layout's register allocation stays its own and the persistent kernel
+   compiles in a fraction of the time an inlined body of every layout takes. */
+template <int TB, int TA>
+__device__ __noinline__ void batch_tile(const uint8_t* __restrict__ cur,
+                                        const uint8_t* __restrict__ prev, int pitch,
+                                        const DGeom& g, const vsbd_item* items,
+                                        unsigned long long* keys, unsigned* tickets,
+                                        vsbd_result* res, int item, int tile, unsigned ntiles,
+                                        uint8_t* sm) {
+  lattice_tile<TB, false, TA>(cur, prev, pitch, g, items, keys, tickets, res, item, tile, ntiles,
+                              sm);
+}
+
 __device__ __forceinline__ void search_tile(const BStream& S, const DGeom* geoms, int cls,
                                             const vsbd_item* items, unsigned long long* keys,
                                             unsigned* tickets, vsbd_result* res, int item,
@@ -106,27 +120,19 @@ __device__ __forceinline__ void search_tile(const BStream& S, const DGeom* geoms
   __syncthreads();
   const DGeom& g = *sg;
   const unsigned ntiles = (unsigned)(g.nta * g.ntb);
-  if (g.ta == 3) {
-    if (g.tb == 4)
-      lattice_tile<4, false, 3>(S.cur, S.prev, S.pitch, g, items, keys, tickets, res, item, tile,
-                                ntiles, sm);
-    else
-      lattice_tile<2, false, 3>(S.cur, S.prev, S.pitch, g, items, keys, tickets, res, item, tile,
-                                ntiles, sm);
-  } else if (g.ta == 2) {
-    if (g.tb == 4)
-      lattice_tile<4, false, 2>(S.cur, S.prev, S.pitch, g, items, keys, tickets, res, item, tile,
-                                ntiles, sm);
-    else
-      lattice_tile<2, false, 2>(S.cur, S.prev, S.pitch, g, items, keys, tickets, res, item, tile,
-                                ntiles, sm);
-  } else if (g.tb == 4) {
-    lattice_tile<4, false>(S.cur, S.prev, S.pitch, g, items, keys, tickets, res, item, tile,
-                           ntiles, sm);
+#define VSB_TILE(TBv, TAv) \
+  batch_tile<TBv, TAv>(S.cur, S.prev, S.pitch, g, items, keys, tickets, res, item, tile, ntiles, sm)
+  const int ta = g.ta > 0 ? g.ta : 1;
+  if (g.tb == 4) {
+    if (ta == 3) VSB_TILE(4, 3);
+    else if (ta == 2) VSB_TILE(4, 2);
+    else VSB_TILE(4, 1);
   } else {
-    lattice_tile<2, false>(S.cur, S.prev, S.pitch, g, items, keys, tickets, res, item, tile,
-                           ntiles, sm);
+    if (ta == 3) VSB_TILE(2, 3);
+    else if (ta == 2) VSB_TILE(2, 2);
+    else VSB_TILE(2, 1);
   }
+#undef VSB_TILE
 }
 
 /* Stage A: the static work list `work`.  Stage B (work == NULL): item w of
