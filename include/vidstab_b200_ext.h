@@ -46,7 +46,9 @@ VS_API void vsb_set_default_search_mode(int pruned);
    its coarse (fine = 0) or fine (1) fields: desc[0..7] = lattice rows per
    thread, layout (1: one lattice column per thread; 2: two, aligned by
    shifts; 3: two of one byte alignment, read from word-aligned window
-   copies), lattice columns and rows per CTA, field strips, threads per CTA,
+   copies; 4: as 3 from one window copy, the odd columns against a copy of
+   the field shifted by two bytes), lattice columns and rows per CTA, field
+   strips, threads per CTA,
    shared memory bytes per CTA, CTAs per field. */
 VS_API int vsb_search_tiling(const struct _vsmotiondetect* md, int fine, int* desc);
 
@@ -116,7 +118,10 @@ VS_API void vsb_counters(long long* launches, long long* h2d_bytes, long long* d
    min/max, coarse search, results back), sec[1] host part A (selection,
    coarse motions, the simple model, fine work list), sec[2] device stage B
    (fine search), sec[3] host part B (fine motions, mean-match filter,
-   result); *frames the number of frames. */
+   result); *frames the number of frames.  Batched steps (vsb_batch_detect,
+   vsb_batch_run) add their stage times the same way, each step counting
+   one frame per stream; overlapped steps count the time spent waiting for
+   each stage rather than its duration. */
 VS_API void vsb_host_profile(double* sec, long* frames, int reset);
 
 /* Measured byte-absolute-difference throughput (per second) of the GPU's

@@ -110,7 +110,8 @@ def orc_search(curr, prev, x, y, size, ms, step, ox=0, oy=0, bpp=0):
 def enc(tb, strips, nab, nbb, ta=0):
     """forced tiling: rows per thread, field strips, lattice columns / rows per
     CTA, layout (1 one column per thread, 2 two columns with shifts, 3 two
-    columns from aligned window copies)"""
+    columns from aligned window copies, 4 two columns from one window copy
+    and a field copy shifted by two bytes)"""
     return ta * 100000000 + tb * 1000000 + strips * 10000 + nab * 100 + nbb
 
 
@@ -135,7 +136,14 @@ def enc(tb, strips, nab, nbb, ta=0):
                                                 (48, 32, 8, enc(2, 2, 6, 8, 3)),
                                                 (64, 40, 6, enc(2, 1, 4, 2, 3)),
                                                 (224, 40, 6, enc(2, 4, 8, 6, 3)),
-                                                (16, 16, 2, enc(4, 2, 4, 4, 3))])
+                                                (16, 16, 2, enc(4, 2, 4, 4, 3)),
+                                                (112, 60, 6, enc(4, 2, 8, 8, 4)),
+                                                (112, 154, 6, enc(2, 4, 12, 10, 4)),
+                                                (32, 32, 2, enc(4, 1, 36, 36, 4)),
+                                                (64, 40, 6, enc(2, 1, 4, 2, 4)),
+                                                (224, 40, 6, enc(2, 4, 12, 14, 4)),
+                                                (16, 16, 2, enc(4, 2, 4, 4, 4)),
+                                                (80, 45, 6, enc(2, 2, 16, 14, 4))])
 def test_field_search_planar(size, ms, step, tiles):
     w, h = 640, 480
     curr, prev = _blurred_pair(w, h, seed=size + step)
@@ -167,7 +175,7 @@ def test_field_search_ties():
     for curr, prev in [(flat, flat), (periodic, periodic), (periodic, np.roll(periodic, 3, 1)),
                        (stripes, stripes)]:
         for size, ms, step in [(32, 30, 6), (32, 32, 2), (16, 16, 2)]:
-            for tiles in (enc(4, 2, 5, 4), enc(4, 2, 8, 4, 3)):
+            for tiles in (enc(4, 2, 5, 4), enc(4, 2, 8, 4, 3), enc(4, 2, 8, 4, 4)):
                 sad, tx, ty, ok = V.field_search(curr, prev, xs, ys, size, ms, step, tiles=tiles)
                 for k in range(3):
                     exp = orc_search(curr, prev, int(xs[k]), int(ys[k]), size, ms, step)
@@ -185,7 +193,10 @@ def test_field_search_packed(bpp):
     ys = np.array([90, 120, 150, 130], np.int16)
     # the aligned two-column layout serves packed rows too (step 2: 6 or 8
     # bytes per lattice step)
-    for size, ms, step, tiles in [(32, 34, 6, 0), (16, 16, 2, 0), (16, 16, 2, enc(2, 2, 8, 4, 3))]:
+    cases = [(32, 34, 6, 0), (16, 16, 2, 0), (16, 16, 2, enc(2, 2, 8, 4, 3))]
+    if bpp == 3:  # 6 bytes per lattice step: the shifted-field layout too
+        cases.append((16, 16, 2, enc(2, 2, 8, 4, 4)))
+    for size, ms, step, tiles in cases:
         sad, tx, ty, ok = V.field_search(curr, prev, xs, ys, size, ms, step, packed_bpp=bpp,
                                          tiles=tiles)
         for k in range(len(xs)):

@@ -94,10 +94,13 @@ int vsb_batch_detect(vsb_batch* b, const uint8_t* const* planes, const int* pitc
   if (!b || !planes || !pitches || !motions) return VS_ERROR;
   for (int s = 0; s < b->n; s++)
     if (vsb_frame_begin(&b->md[s], &b->search[s]) != VS_OK) return VS_ERROR;
+  /* wall time: [0] stage A, [1] host part A, [2] stage B, [3] host part B */
+  double t0 = vsb_now_s(), prof[4];
   if (vsbd_batch_stage_a(b->dev, planes, pitches, on_device) != 0) {
     vs_log_error("vsb_batch", "GPU stage A failed: %s\n", vsbd_error());
     return VS_ERROR;
   }
+  double t1 = vsb_now_s();
   for (int s = 0; s < b->n; s++) {
     b->items[s] = NULL;
     b->nitems[s] = 0;
@@ -111,12 +114,14 @@ int vsb_batch_detect(vsb_batch* b, const uint8_t* const* planes, const int* pitc
       b->nitems[s] = b->w[s].nitems;
     }
   }
+  double t2 = vsb_now_s();
   if (vsbd_batch_stage_b(b->dev, b->items, b->nitems, b->fres) != 0) {
     vs_log_error("vsb_batch", "GPU stage B failed: %s\n", vsbd_error());
     for (int s = 0; s < b->n; s++)
       if (b->search[s]) vsb_frame_discard(&b->w[s]);
     return VS_ERROR;
   }
+  double t3 = vsb_now_s();
   for (int s = 0; s < b->n; s++) {
     if (b->search[s])
       vsb_frame_host_b(&b->md[s], b->fres[s], &b->w[s], &motions[s]);
@@ -124,6 +129,11 @@ int vsb_batch_detect(vsb_batch* b, const uint8_t* const* planes, const int* pitc
       vsb_frame_first(&b->md[s], &motions[s]);
     if (vsb_frame_end(&b->md[s])) vsbd_batch_commit(b->dev, s);
   }
+  prof[0] = t1 - t0;
+  prof[1] = t2 - t1;
+  prof[2] = t3 - t2;
+  prof[3] = vsb_now_s() - t3;
+  vsb_prof_add(prof, b->n);
   return VS_OK;
 }
 

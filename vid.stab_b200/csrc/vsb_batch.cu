@@ -124,11 +124,13 @@ __device__ __forceinline__ void search_tile(const BStream& S, const DGeom* geoms
   batch_tile<TBv, TAv>(S.cur, S.prev, S.pitch, g, items, keys, tickets, res, item, tile, ntiles, sm)
   const int ta = g.ta > 0 ? g.ta : 1;
   if (g.tb == 4) {
-    if (ta == 3) VSB_TILE(4, 3);
+    if (ta == 4) VSB_TILE(4, 4);
+    else if (ta == 3) VSB_TILE(4, 3);
     else if (ta == 2) VSB_TILE(4, 2);
     else VSB_TILE(4, 1);
   } else {
-    if (ta == 3) VSB_TILE(2, 3);
+    if (ta == 4) VSB_TILE(2, 4);
+    else if (ta == 3) VSB_TILE(2, 3);
     else if (ta == 2) VSB_TILE(2, 2);
     else VSB_TILE(2, 1);
   }
@@ -417,20 +419,22 @@ static int autotune_class(vsbd_batch* b, int c, int is_fine) {
     if ((is_fine ? S.gf : S.gc) == c) nitems += is_fine ? S.nf : S.nc;
   }
   if (nitems == 0 || getenv("VSB_NO_AUTOTUNE")) return 0;
-  /* all three layouts (one lattice column per thread; two with shifts; two
-     from aligned window copies): the cost model does not see the
-     shared-memory loads and shifts in which they differ */
-  TileCand cand[20];
-  int nc = vsbp_tile_candidates_ta(b->cls[c].g, nitems, VSB_BATCH_THREADS, cand, 6, 1);
-  nc += vsbp_tile_candidates_ta(b->cls[c].g, nitems, VSB_BATCH_THREADS, cand + nc, 6, 2);
-  nc += vsbp_tile_candidates_ta(b->cls[c].g, nitems, VSB_BATCH_THREADS, cand + nc, 8, 3);
+  /* all four layouts (one lattice column per thread; two with shifts; two
+     from aligned window copies; two from one copy and a shifted field copy):
+     the cost model does not see the shared-memory loads and shifts in which
+     they differ */
+  TileCand cand[24];
+  int nc = vsbp_tile_candidates_ta(b->cls[c].g, nitems, VSB_BATCH_THREADS, cand, 5, 1);
+  nc += vsbp_tile_candidates_ta(b->cls[c].g, nitems, VSB_BATCH_THREADS, cand + nc, 5, 2);
+  nc += vsbp_tile_candidates_ta(b->cls[c].g, nitems, VSB_BATCH_THREADS, cand + nc, 6, 3);
+  nc += vsbp_tile_candidates_ta(b->cls[c].g, nitems, VSB_BATCH_THREADS, cand + nc, 6, 4);
   cudaEvent_t e0, e1;
   BCK(cudaEventCreate(&e0));
   BCK(cudaEventCreate(&e1));
   float best_ms = 1e30f;
   DGeom best = b->cls[c].g;
   int tried = 0;
-  for (int k = 0; k < nc && tried < 16; k++) {
+  for (int k = 0; k < nc && tried < 18; k++) {
     if (!tiling_ok(b, cand[k].g)) continue;
     tried++;
     DGeom t = cand[k].g;

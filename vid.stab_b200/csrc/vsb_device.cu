@@ -373,8 +373,8 @@ static size_t search_smem_limit(void) {
 /* registers per thread of the search kernel for TB rows and TA columns per
    thread */
 static int lattice_regs(int TB, int TA) {
-  static int r[4][9] = { { 0 } };
-  if (TB < 1 || TB > 8 || TA < 1 || TA > 3) return 0;
+  static int r[5][9] = { { 0 } };
+  if (TB < 1 || TB > 8 || TA < 1 || TA > 4) return 0;
   if (!r[TA][TB]) {
     cudaFuncAttributes fa;
     cudaError_t e = cudaErrorInvalidValue;
@@ -385,9 +385,12 @@ static int lattice_regs(int TB, int TA) {
     } else if (TA == 2) {
       if (TB == 2) e = cudaFuncGetAttributes(&fa, k_lattice<2, false, 2>);
       if (TB == 4) e = cudaFuncGetAttributes(&fa, k_lattice<4, false, 2>);
-    } else {
+    } else if (TA == 3) {
       if (TB == 2) e = cudaFuncGetAttributes(&fa, k_lattice<2, false, 3>);
       if (TB == 4) e = cudaFuncGetAttributes(&fa, k_lattice<4, false, 3>);
+    } else {
+      if (TB == 2) e = cudaFuncGetAttributes(&fa, k_lattice<2, false, 4>);
+      if (TB == 4) e = cudaFuncGetAttributes(&fa, k_lattice<4, false, 4>);
     }
     r[TA][TB] = e == cudaSuccess ? fa.numRegs : 64;
   }
@@ -409,12 +412,15 @@ static int tile_candidates(const DGeom& g, int nitems, int tb_force, int strip_f
   int n = 0;
   const int tbs[3] = { 4, 2, 8 };
   const int sb = g.step * g.bpp;
-  for (int tv = 0; tv < 9; tv++) {
-    const int ti = tv % 3, TA = 1 + tv / 3; /* columns per thread: 1, 2, 2 from aligned copies */
+  for (int tv = 0; tv < 12; tv++) {
+    /* layouts: 1 one column per thread, 2 two with shifts, 3 two from aligned
+       window copies, 4 two from one copy and a shifted field copy */
+    const int ti = tv % 3, TA = 1 + tv / 3;
     int TB = tbs[ti];
     if (tb_force > 0 && TB != tb_force) continue;
     if (TA >= 2 && (TB > 4 || sb > 8 || g.rows > 0)) continue;
     if (TA == 3 && (sb & 1)) continue;
+    if (TA == 4 && (sb & 3) != 2) continue;
     if (ta_force > 0 && TA != ta_force) continue;
     for (int ns = 1; ns <= 8; ns *= 2) {
       if (strip_force > 0 && ns != strip_force) continue;
@@ -424,7 +430,7 @@ static int tile_candidates(const DGeom& g, int nitems, int tb_force, int strip_f
       if (Rs < 4) continue;
       /* two-column layouts need nab even (a multiple of 4 for aligned copies
          of a step of 2 mod 4 bytes): the even split rounded up */
-      const int nab_mul = TA == 1 ? 1 : (TA == 3 && (sb & 3) ? 4 : 2);
+      const int nab_mul = TA == 1 ? 1 : (TA == 4 || (TA == 3 && (sb & 3)) ? 4 : 2);
       int nab_prev = -1;
       for (int ka = 1; ka <= 16; ka++) {
         int nab = (g.na + ka - 1) / ka;
@@ -445,7 +451,10 @@ static int tile_candidates(const DGeom& g, int nitems, int tb_force, int strip_f
           t.nstrip = ns;
           t.nta = (g.na + nab - 1) / nab;
           t.ntb = (g.nb + nbb - 1) / nbb;
-          int threads = (nab / (TA == 1 ? 1 : 2)) * (nbb / TB) * ns;
+          /* layout 4: even-column pairs in the first half of the block, odd
+             ones in the second, each half whole warps */
+          int threads = TA == 4 ? 2 * (((nab / 4) * (nbb / TB) * ns + 31) & ~31)
+                                : (nab / (TA == 1 ? 1 : 2)) * (nbb / TB) * ns;
           threads = (threads + 31) & ~31;
           if (threads > max_threads || threads < 32) {
             if (nbb_force > 0) break;
@@ -478,7 +487,7 @@ static int tile_candidates(const DGeom& g, int nitems, int tb_force, int strip_f
              shared-memory loads per SAD than the model counts) */
           if (TA == 2) clk *= 0.85;
           /* ... and with aligned window copies they need no shifts */
-          if (TA == 3) clk *= 0.7;
+          if (TA >= 3) clk *= 0.7;
           /* keep the cap best, sorted */
           int pos = n < cap ? n : cap;
           while (pos > 0 && out[pos - 1].clk > clk) {
@@ -562,7 +571,8 @@ static int launch_lattice(const GeomDev& gd, const uint8_t* curr, const uint8_t*
                           const vsbd_item* d_items, int n, unsigned long long* keys,
                           unsigned* tickets, vsbd_result* d_res, cudaStream_t st) {
   cudaError_t e = ensure_smem((const void*)k_lattice<TB, false, TA>,
-                              (TA == 3 ? 20 : (TA == 2 ? 11 : 0)) + (TB == 2 ? 0 : (TB == 4 ? 1 : 2)),
+                              (TA == 4 ? 24 : (TA == 3 ? 20 : (TA == 2 ? 11 : 0))) +
+                                  (TB == 2 ? 0 : (TB == 4 ? 1 : 2)),
                               gd.smem);
   if (e != cudaSuccess) {
     set_err("cudaFuncSetAttribute(k_lattice)", e);
@@ -580,10 +590,12 @@ static int launch_search(const GeomDev& gd, const uint8_t* curr, const uint8_t* 
   if (n <= 0) return 0;
   switch (gd.g.tb) {
     case 2:
+      if (gd.g.ta == 4) return launch_lattice<2, 4>(gd, curr, prev, pitch, d_items, n, keys, tickets, d_res, st);
       if (gd.g.ta == 3) return launch_lattice<2, 3>(gd, curr, prev, pitch, d_items, n, keys, tickets, d_res, st);
       return gd.g.ta == 2 ? launch_lattice<2, 2>(gd, curr, prev, pitch, d_items, n, keys, tickets, d_res, st)
                           : launch_lattice<2, 1>(gd, curr, prev, pitch, d_items, n, keys, tickets, d_res, st);
     case 4:
+      if (gd.g.ta == 4) return launch_lattice<4, 4>(gd, curr, prev, pitch, d_items, n, keys, tickets, d_res, st);
       if (gd.g.ta == 3) return launch_lattice<4, 3>(gd, curr, prev, pitch, d_items, n, keys, tickets, d_res, st);
       return gd.g.ta == 2 ? launch_lattice<4, 2>(gd, curr, prev, pitch, d_items, n, keys, tickets, d_res, st)
                           : launch_lattice<4, 1>(gd, curr, prev, pitch, d_items, n, keys, tickets, d_res, st);
@@ -601,7 +613,8 @@ static int launch_list_tb(const GeomDev& gd, const uint8_t* curr, const uint8_t*
                           unsigned long long* keys, unsigned* tickets, vsbd_result* d_res,
                           cudaStream_t st) {
   cudaError_t e = ensure_smem((const void*)k_lattice_list<TB, TA>,
-                              (TA == 3 ? 22 : (TA == 2 ? 14 : 3)) + (TB == 2 ? 0 : (TB == 4 ? 1 : 2)),
+                              (TA == 4 ? 26 : (TA == 3 ? 22 : (TA == 2 ? 14 : 3))) +
+                                  (TB == 2 ? 0 : (TB == 4 ? 1 : 2)),
                               gd.smem);
   int cps = gd.list_cps;
   if (e == cudaSuccess && cps <= 0)
@@ -626,10 +639,12 @@ static int launch_list(const GeomDev& gd, const uint8_t* curr, const uint8_t* pr
   if (n <= 0) return 0;
   switch (gd.g.tb) {
     case 2:
+      if (gd.g.ta == 4) return launch_list_tb<2, 4>(gd, curr, prev, pitch, d_items, n, count, list, keys, tickets, d_res, st);
       if (gd.g.ta == 3) return launch_list_tb<2, 3>(gd, curr, prev, pitch, d_items, n, count, list, keys, tickets, d_res, st);
       return gd.g.ta == 2 ? launch_list_tb<2, 2>(gd, curr, prev, pitch, d_items, n, count, list, keys, tickets, d_res, st)
                           : launch_list_tb<2, 1>(gd, curr, prev, pitch, d_items, n, count, list, keys, tickets, d_res, st);
     case 4:
+      if (gd.g.ta == 4) return launch_list_tb<4, 4>(gd, curr, prev, pitch, d_items, n, count, list, keys, tickets, d_res, st);
       if (gd.g.ta == 3) return launch_list_tb<4, 3>(gd, curr, prev, pitch, d_items, n, count, list, keys, tickets, d_res, st);
       return gd.g.ta == 2 ? launch_list_tb<4, 2>(gd, curr, prev, pitch, d_items, n, count, list, keys, tickets, d_res, st)
                           : launch_list_tb<4, 1>(gd, curr, prev, pitch, d_items, n, count, list, keys, tickets, d_res, st);
@@ -728,13 +743,15 @@ static int autotune_tiling(GeomDev* gd, const uint8_t* curr, const uint8_t* prev
     }
   }
   /* the model's best tilings of each layout (one lattice column per thread;
-     two with shifts; two from aligned window copies): the model does not
+     two with shifts; two from aligned window copies; two from one copy and
+     a shifted field copy): the model does not
      count shared-memory loads and shifts, which is where the layouts
      differ, so all three are timed */
-  TileCand cand[26];
+  TileCand cand[32];
   int nc = tile_candidates(g, n, 0, 0, 0, 0, cand, 8, 512, 1);
   nc += tile_candidates(g, n, 0, 0, 0, 0, cand + nc, 6, 512, 2);
-  nc += tile_candidates(g, n, 0, 0, 0, 0, cand + nc, 12, 512, 3);
+  nc += tile_candidates(g, n, 0, 0, 0, 0, cand + nc, 8, 512, 3);
+  nc += tile_candidates(g, n, 0, 0, 0, 0, cand + nc, 10, 512, 4);
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
@@ -1472,6 +1489,8 @@ extern "C" int vsbd_set_proposal(vsbd_ctx* c, const void* params, float scale, f
       if (g->g.tb == 4) { fn = g->g.ta == 2 ? (const void*)k_lattice_list<4, 2> : (const void*)k_lattice_list<4, 1>; slot = g->g.ta == 2 ? 15 : 4; }
       if (g->g.ta == 3 && g->g.tb == 2) { fn = (const void*)k_lattice_list<2, 3>; slot = 22; }
       if (g->g.ta == 3 && g->g.tb == 4) { fn = (const void*)k_lattice_list<4, 3>; slot = 23; }
+      if (g->g.ta == 4 && g->g.tb == 2) { fn = (const void*)k_lattice_list<2, 4>; slot = 26; }
+      if (g->g.ta == 4 && g->g.tb == 4) { fn = (const void*)k_lattice_list<4, 4>; slot = 27; }
       if (g->g.tb == 8) { fn = (const void*)k_lattice_list<8, 1>; slot = 5; }
       if (fn) {
         e = ensure_smem(fn, slot, g->smem);

@@ -185,12 +185,14 @@ extern "C" int vsbd_search_noalloc(const uint8_t* d_curr, const uint8_t* d_prev,
   vsbd_result* res = (vsbd_result*)d_results;
   switch (g.tb) {
     case 2:
-      e = g.ta == 3   ? launch_tb<2, 3>(g, smem, d_curr, d_prev, pitch, items, n, keys, tickets, res, st)
+      e = g.ta == 4   ? launch_tb<2, 4>(g, smem, d_curr, d_prev, pitch, items, n, keys, tickets, res, st)
+          : g.ta == 3 ? launch_tb<2, 3>(g, smem, d_curr, d_prev, pitch, items, n, keys, tickets, res, st)
           : g.ta == 2 ? launch_tb<2, 2>(g, smem, d_curr, d_prev, pitch, items, n, keys, tickets, res, st)
                       : launch_tb<2, 1>(g, smem, d_curr, d_prev, pitch, items, n, keys, tickets, res, st);
       break;
     case 4:
-      e = g.ta == 3   ? launch_tb<4, 3>(g, smem, d_curr, d_prev, pitch, items, n, keys, tickets, res, st)
+      e = g.ta == 4   ? launch_tb<4, 4>(g, smem, d_curr, d_prev, pitch, items, n, keys, tickets, res, st)
+          : g.ta == 3 ? launch_tb<4, 3>(g, smem, d_curr, d_prev, pitch, items, n, keys, tickets, res, st)
           : g.ta == 2 ? launch_tb<4, 2>(g, smem, d_curr, d_prev, pitch, items, n, keys, tickets, res, st)
                       : launch_tb<4, 1>(g, smem, d_curr, d_prev, pitch, items, n, keys, tickets, res, st);
       break;

@@ -47,7 +47,10 @@ struct DGeom {
   int ta;               /* lattice columns per thread: 1 (or 0); 2 -- a window row's words
                            then serve two candidate columns (step*bpp <= 8); 3 -- two columns
                            of one byte alignment, read from window copies staged word-aligned
-                           for them (step*bpp even and <= 8): no shifts in the sums */
+                           for them (step*bpp even and <= 8): no shifts in the sums; 4 -- as 3
+                           for step*bpp 2 or 6, from one window copy aligned for the even
+                           columns, the odd ones summed against a copy of the field shifted
+                           by two bytes (edge bytes masked) */
   int rows;             /* field rows a launch sums (0: all S); fewer rows give
                            every candidate a lower bound of its SAD */
   unsigned* emit;       /* emit mode: per item, per lattice point, the sum */
@@ -78,7 +81,8 @@ struct TileLayout {
   int RP, RH;        /* refinement window: row pitch (bytes), rows */
   int FP;            /* row pitch of the staged current-field rows */
   int CP;            /* ta == 3: distance of the second window copy from the first */
-  size_t off_P, off_part, off_q, total;
+  int C1P;           /* ta == 4: row pitch of the shifted field copy (at off_C1) */
+  size_t off_C1, off_P, off_part, off_q, total;
 };
 
 /* window copies of a ta == 3 tile: two when the lattice step in bytes is 2
@@ -108,7 +112,9 @@ __host__ __device__ inline TileLayout tile_layout(const DGeom& g) {
   L.RH = g.S + 2 * R;
   L.RP = ((3 + L.rowB + 2 * R * g.bpp + 8 + 15) >> 4) << 4;
   L.FP = ((L.rowB + 15 + 15) >> 4 << 4) + 16;
-  L.off_P = (size_t)rows * L.rowB;
+  L.C1P = L.rowB + 16;
+  L.off_C1 = (size_t)rows * L.rowB;
+  L.off_P = L.off_C1 + (g.ta == 4 ? (size_t)rows * L.C1P : 0);
   /* the second copy sits one word off a 16-byte boundary, so that a warp's
      even- and odd-column threads read different banks */
   L.CP = L.WH_alloc * L.WP + 4;
@@ -469,6 +475,85 @@ __device__ __forceinline__ void rows_segment_al(unsigned (&acc)[2][TB], int jlo,
     rows_segment_al_dw<TB, 1>(acc, jlo, jhi, rb, re, step, Pw0, WPw, C4, nq);
 }
 
+/* Rows [rb, re) for an odd-column thread of layout 4: its columns start
+   two bytes into window words, the field copy C1 is shifted by two bytes
+   (rowW + 1 words per row, zero outside the field), so word k of a column
+   pairs with word k of C1; the halves of the first and the last word that
+   lie outside the field are masked off the window words. */
+template <int TB, int JLO, int JHI, int DW>
+__device__ __forceinline__ void rows_active_fc(unsigned (&acc)[2][TB], int rb, int re, int step,
+                                               const uint32_t* __restrict__ Pw0, int WPw,
+                                               const uint4* __restrict__ C14, int nq1, int nq) {
+  for (int rho = rb; rho < re; rho++) {
+    const uint32_t* Pw = Pw0 + rho * WPw;
+    const uint4* Cj[TB];
+#pragma unroll
+    for (int j = JLO; j <= JHI; j++) Cj[j] = C14 + (rho - step * j) * nq1;
+    uint32_t cr[DW];
+#pragma unroll
+    for (int k = 0; k < DW; k++) cr[k] = Pw[k];
+    cr[0] &= 0xffff0000u;
+    uint32_t m = 0xffff0000u;
+    for (int q = 0; q < nq; q++) {
+      const uint32_t n0 = Pw[4 * q + DW], n1 = Pw[4 * q + DW + 1], n2 = Pw[4 * q + DW + 2],
+                     n3 = Pw[4 * q + DW + 3];
+      uint32_t X[4];
+      if constexpr (DW == 1) {
+        X[0] = cr[0]; X[1] = n0; X[2] = n1; X[3] = n2;
+        cr[0] = n3;
+      } else if constexpr (DW == 2) {
+        X[0] = cr[0]; X[1] = cr[1]; X[2] = n0; X[3] = n1;
+        cr[0] = n2; cr[1] = n3;
+      } else {
+        X[0] = cr[0]; X[1] = cr[1]; X[2] = cr[2]; X[3] = n0;
+        cr[0] = n1; cr[1] = n2; cr[2] = n3;
+      }
+      const uint32_t y0 = n0 & m; /* the second column's first word, at q == 0 */
+      m = 0xffffffffu;
+#pragma unroll
+      for (int j = JLO; j <= JHI; j++) {
+        const uint4 c = Cj[j][q];
+        acc[0][j] = sad4(c.x, X[0], acc[0][j]);
+        acc[1][j] = sad4(c.x, y0, acc[1][j]);
+        acc[0][j] = sad4(c.y, X[1], acc[0][j]);
+        acc[1][j] = sad4(c.y, n1, acc[1][j]);
+        acc[0][j] = sad4(c.z, X[2], acc[0][j]);
+        acc[1][j] = sad4(c.z, n2, acc[1][j]);
+        acc[0][j] = sad4(c.w, X[3], acc[0][j]);
+        acc[1][j] = sad4(c.w, n3, acc[1][j]);
+      }
+    }
+    /* word rowW = 4*nq: the field's last two bytes in its lower half */
+    const uint32_t t0 = cr[0] & 0xffffu, t1 = Pw[4 * nq + DW] & 0xffffu;
+#pragma unroll
+    for (int j = JLO; j <= JHI; j++) {
+      const uint32_t cw = ((const uint32_t*)Cj[j])[4 * nq];
+      acc[0][j] = sad4(cw, t0, acc[0][j]);
+      acc[1][j] = sad4(cw, t1, acc[1][j]);
+    }
+  }
+}
+
+template <int TB, int DW>
+__device__ __forceinline__ void rows_segment_fc_dw(unsigned (&acc)[2][TB], int jlo, int jhi,
+                                                   int rb, int re, int step, const uint32_t* Pw0,
+                                                   int WPw, const uint4* C14, int nq1, int nq) {
+#define VSB_SEG4(L, H)                                                            \
+  if (jlo == L && jhi == H) {                                                     \
+    rows_active_fc<TB, L, H, DW>(acc, rb, re, step, Pw0, WPw, C14, nq1, nq);      \
+    return;                                                                       \
+  }
+  if constexpr (TB == 2) {
+    VSB_SEG4(0, 0) VSB_SEG4(0, 1) VSB_SEG4(1, 1)
+  } else if constexpr (TB == 4) {
+    VSB_SEG4(0, 0) VSB_SEG4(0, 1) VSB_SEG4(0, 2) VSB_SEG4(0, 3)
+    VSB_SEG4(1, 1) VSB_SEG4(1, 2) VSB_SEG4(1, 3)
+    VSB_SEG4(2, 2) VSB_SEG4(2, 3)
+    VSB_SEG4(3, 3)
+  }
+#undef VSB_SEG4
+}
+
 /* bytes o .. o+15 of the 32 bytes lo:hi, o = 4*wo + sh/8 (wo uniform) */
 __device__ __forceinline__ uint4 extract16(uint4 lo, uint4 hi, int wo, int sh) {
   uint32_t w0, w1, w2, w3, w4;
@@ -482,7 +567,7 @@ __device__ __forceinline__ uint4 extract16(uint4 lo, uint4 hi, int wo, int sh) {
                     __funnelshift_r(w2, w3, sh), __funnelshift_r(w3, w4, sh));
 }
 
-template <int TB, bool EMIT, bool AL>
+template <int TB, bool EMIT, int AL>
 __device__ void lattice_tile_ta2(const uint8_t* __restrict__ curr, const uint8_t* __restrict__ prev,
                                  int pitch, const DGeom& g, const vsbd_item* __restrict__ items,
                                  unsigned long long* __restrict__ keys,
@@ -492,7 +577,7 @@ __device__ void lattice_tile_ta2(const uint8_t* __restrict__ curr, const uint8_t
 /* One lattice tile of one item, by one CTA: tile = tbi*nta + tai of the
    item's ntiles = nta*ntb tiles; sm: tile_layout(g).total bytes of shared
    memory.  The last of the item's CTAs to finish refines and stores.  TA:
-   the tiling's g.ta (1, 2 or 3; 1 for g.ta == 0). */
+   the tiling's g.ta (1 to 4; 1 for g.ta == 0). */
 template <int TB, bool EMIT, int TA = 1>
 __device__ __forceinline__ void lattice_tile(const uint8_t* __restrict__ curr,
                                              const uint8_t* __restrict__ prev, int pitch,
@@ -501,9 +586,9 @@ __device__ __forceinline__ void lattice_tile(const uint8_t* __restrict__ curr,
                                              unsigned* __restrict__ tickets,
                                              vsbd_result* __restrict__ res, int item, int tile,
                                              unsigned ntiles, uint8_t* sm) {
-  if constexpr (TA == 2 || TA == 3) {
-    lattice_tile_ta2<TB, EMIT, TA == 3>(curr, prev, pitch, g, items, keys, tickets, res, item,
-                                        tile, ntiles, sm);
+  if constexpr (TA >= 2) {
+    lattice_tile_ta2<TB, EMIT, TA - 2>(curr, prev, pitch, g, items, keys, tickets, res, item,
+                                       tile, ntiles, sm);
     return;
   }
   __shared__ unsigned long long red[32];
@@ -645,8 +730,12 @@ __device__ __forceinline__ void lattice_tile(const uint8_t* __restrict__ curr,
    one byte alignment pair up -- a and a+2 (a = 4*(p/2) + p%2 for pair p,
    nab a multiple of 4) when the step in bytes is 2 mod 4, else a = 2p and
    a+1 -- and each alignment has its own window copy, staged so that its
-   columns start on word boundaries. */
-template <int TB, bool EMIT, bool AL>
+   columns start on word boundaries.  g.ta == 4 (AL 2, step in bytes 2 or 6,
+   nab a multiple of 4): the same pairs from one window copy aligned for the
+   even columns; odd-column threads use the field copy shifted by two bytes.
+   The first half of the threads takes the even columns, the second half the
+   odd ones, so that no warp mixes the two loops. */
+template <int TB, bool EMIT, int AL>
 __device__ void lattice_tile_ta2(const uint8_t* __restrict__ curr, const uint8_t* __restrict__ prev,
                                  int pitch, const DGeom& g, const vsbd_item* __restrict__ items,
                                  unsigned long long* __restrict__ keys,
@@ -690,11 +779,12 @@ __device__ void lattice_tile_ta2(const uint8_t* __restrict__ curr, const uint8_t
   const int gx0a = gx0 & ~15, e = gx0 - gx0a;
   const int sb = g.step * g.bpp; /* lattice step in bytes */
   const int dcol = AL && (sb & 3) ? 2 : 1;
+  const int ncopy = AL == 1 ? dcol : 1;
   {
     const int wwb = L.rowB + (na_t - 1) * sb;
     const int wh = rows + (nb_t - 1) * g.step;
     const int nvec = (e + wwb + 15) >> 4;
-    if constexpr (!AL) {
+    if constexpr (AL == 0) {
       for (int i = threadIdx.x; i < wh * nvec; i += blockDim.x) {
         int r = i / nvec, v = i - r * nvec;
         *(uint4*)(P + r * L.WP + (v << 4)) =
@@ -704,7 +794,7 @@ __device__ void lattice_tile_ta2(const uint8_t* __restrict__ curr, const uint8_t
       /* copy c starts at window byte c*sb: the columns c, c + 2*dcol, ... (and
          their partners) begin on its word boundaries.  Only the aligned
          16-byte chunks the plain staging reads are read. */
-      for (int c = 0; c < dcol; c++) {
+      for (int c = 0; c < ncopy; c++) {
         const int bytes = L.rowB + max(na_t - 1 - c, 0) * sb;
         const int ob = e + c * sb;
         const int o = ob & 15, wo = o >> 2, sh = (o & 3) << 3, u00 = ob >> 4;
@@ -730,19 +820,41 @@ __device__ void lattice_tile_ta2(const uint8_t* __restrict__ curr, const uint8_t
           }
         }
       }
+      if constexpr (AL == 2) {
+        /* the field shifted right by two bytes: word k of row r holds field
+           bytes 4k-2 .. 4k+1, zero outside the field */
+        uint32_t* C1 = (uint32_t*)(sm + L.off_C1);
+        const int c1w = L.C1P >> 2;
+        for (int i = threadIdx.x; i < rows * c1w; i += blockDim.x) {
+          const int r = i / c1w, k = i - r * c1w;
+          const uint32_t lo = k > 0 && k <= L.rowW ? C[r * L.rowW + k - 1] : 0u;
+          const uint32_t hi = k < L.rowW ? C[r * L.rowW + k] : 0u;
+          C1[i] = __funnelshift_r(lo, hi, 16);
+        }
+      }
     }
   }
   __syncthreads();
 
-  const int t = threadIdx.x;
-  const int ntask = NAG * G * g.nstrip;
+  int t = threadIdx.x;
+  int ntask = NAG * G * g.nstrip;
+  int cls = 0;
+  if constexpr (AL == 2) {
+    /* halves of the block: even-column pairs, then odd-column pairs */
+    const int half = (int)blockDim.x >> 1;
+    cls = t >= half;
+    t -= cls * half;
+    ntask >>= 1;
+  }
   const bool active = t < ntask;
-  int ag = t % NAG, rest = t / NAG;
+  const int NAGc = AL == 2 ? NAG >> 1 : NAG;
+  int ag = t % NAGc, rest = t / NAGc;
   int grp = rest % G, st = rest / G;
   if (!active) { ag = 0; grp = 0; st = 0; }
-  /* the thread's two columns and, for AL, the copy it reads */
-  const int cls = dcol == 2 ? (ag & 1) : 0;
-  const int al0 = dcol == 2 ? 4 * (ag >> 1) + cls : 2 * ag;
+  if constexpr (AL == 2) ag = 2 * ag + cls;
+  /* the thread's two columns and, for AL 1, the copy it reads */
+  if constexpr (AL == 1) cls = dcol == 2 ? (ag & 1) : 0;
+  const int al0 = dcol == 2 ? 4 * (ag >> 1) + (ag & 1) : 2 * ag;
   const int col[2] = { al0, al0 + dcol };
   unsigned acc[2][TB];
 #pragma unroll
@@ -755,8 +867,12 @@ __device__ void lattice_tile_ta2(const uint8_t* __restrict__ curr, const uint8_t
     const int dw = AL ? (sb * dcol) >> 2 : (cxb1 >> 2) - (cxb >> 2);
     const size_t rowoff = (size_t)(r0 + grp * TB * g.step) * L.WP;
     const uint8_t* Pb = P + rowoff + (cxb & ~3);
-    /* AL: column al0 starts at byte (al0 - cls)*sb of copy cls, a word boundary */
-    const uint32_t* Pw0 = (const uint32_t*)(P + cls * L.CP + rowoff) + (((al0 - cls) * sb) >> 2);
+    /* AL 1: column al0 starts at byte (al0 - cls)*sb of copy cls, a word
+       boundary; AL 2: at byte al0*sb of the one copy, two bytes into a word
+       for the odd columns */
+    const uint32_t* Pw0 =
+        AL == 2 ? (const uint32_t*)(P + rowoff) + ((al0 * sb) >> 2)
+                : (const uint32_t*)(P + cls * L.CP + rowoff) + (((al0 - cls) * sb) >> 2);
     const uint4* C4 = (const uint4*)C + r0 * L.nq;
     const int nrho = Rs + g.step * (TB - 1);
     for (int rb = 0; rb < nrho;) {
@@ -765,7 +881,19 @@ __device__ void lattice_tile_ta2(const uint8_t* __restrict__ curr, const uint8_t
       int re = jhi == TB - 1 ? nrho : min(nrho, (jhi + 1) * g.step);
       int lo_next = Rs + jlo * g.step;
       if (lo_next > rb && lo_next < re) re = lo_next;
-      if constexpr (AL)
+      if constexpr (AL == 2) {
+        if (cls) {
+          const uint4* C14 = (const uint4*)(sm + L.off_C1) + (size_t)r0 * (L.C1P >> 4);
+          if (dw == 3)
+            rows_segment_fc_dw<TB, 3>(acc, jlo, jhi, rb, re, g.step, Pw0, L.WP >> 2, C14,
+                                      L.C1P >> 4, L.nq);
+          else
+            rows_segment_fc_dw<TB, 1>(acc, jlo, jhi, rb, re, g.step, Pw0, L.WP >> 2, C14,
+                                      L.C1P >> 4, L.nq);
+        } else {
+          rows_segment_al<TB>(acc, jlo, jhi, rb, re, g.step, Pw0, L.WP >> 2, dw, C4, L.nq);
+        }
+      } else if constexpr (AL == 1)
         rows_segment_al<TB>(acc, jlo, jhi, rb, re, g.step, Pw0, L.WP >> 2, dw, C4, L.nq);
       else
         rows_segment_ta2<TB>(acc, jlo, jhi, rb, re, g.step, Pb, L.WP, sh0, sh1, dw, C4, L.nq);
