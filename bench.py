@@ -242,7 +242,8 @@ def batched_arm(V, steps, warmup, timed, frames):
     3840x2160 in ratio 4:3:2:1 (26/19/13/6 streams), each a camera-walk clip
     of its own seed, through one batch (persistent kernel per stage from
     captured CUDA graphs), against the same streams run one after another
-    through single-stream detectors on the same GPU."""
+    through single-stream detectors on the same GPU, and through the same
+    detectors stepped together by one host thread (vsb_detect_multi)."""
     from vidstab_b200 import synthetic as S
     classes = [(640, 360, 26), (1280, 720, 19), (1920, 1080, 13), (3840, 2160, 6)]
     sizes = [(w, h) for w, h, n in classes for _ in range(n)]
@@ -283,14 +284,20 @@ def batched_arm(V, steps, warmup, timed, frames):
         same += int(np.array_equal(cm[:, s], cnt) and np.array_equal(mine, rec[:t]))
     run_all()
     ts = timed(run_all, steps)
+    # the same detectors stepped together by one host thread (vsb_detect_multi)
+    mout = np.zeros(frames * n * 800 + 64, V.LM_DTYPE)
+    mcnt = np.zeros(frames * n, np.int32)
+    tm = timed(lambda: V.detect_multi(dets, ptrs, fb, pitches, frames, True, mout, mcnt), steps)
     for d in dets:
         d.close()
     agg = n * frames * steps / sum(tb)
     seq = n * frames * steps / sum(ts)
+    multi = n * frames * steps / sum(tm)
     return {"value": agg, "unit": "frames/s (all streams)", "streams": n,
             "frames_per_stream": frames, "records": int(tot),
             "streams_checked_identical": "%d of 2" % same,
             "single_stream_detectors_sequential": seq, "speedup": agg / seq,
+            "detectors_stepped_together": multi,
             "persistent_launches_per_step": int(launches),
             "workload": "64 streams 26x640x360 + 19x1280x720 + 13x1920x1080 + 6x3840x2160, "
                         "camera-walk clips (seed per stream), defaults of the 1080p clip"}
