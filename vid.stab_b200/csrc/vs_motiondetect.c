@@ -772,6 +772,14 @@ long vsb_detect_run_overlapped(VSMotionDetect* md, const uint8_t* frames, long f
       return -1;
     }
   }
+  /* host frames travel one frame ahead of their stage A: frame k+2 is copied
+     into upload slot k&1 (free: frame k's stage A, which read it, has been
+     collected) while frame k's fine stage and frame k+1's stage A run */
+  if (!on_device && k + 1 < nframes &&
+      vsbd_upload(st->dev, frames + (size_t)(k + 1) * frame_bytes, linesize, (k + 1) & 1) != 0) {
+    vs_log_error(md->conf.modName, "GPU upload failed: %s\n", vsbd_error());
+    return -1;
+  }
   for (; k < nframes; k++) {
     int search = 0;
     if (vsb_frame_begin(md, &search) != VS_OK || !search) return -1;
@@ -780,8 +788,10 @@ long vsb_detect_run_overlapped(VSMotionDetect* md, const uint8_t* frames, long f
     const int next = k + 1 < nframes;
     const uint8_t* nsrc = frames + (size_t)(k + 1) * frame_bytes;
     if (vsbd_stage_b_issue(st->dev, w.items, w.fine_pass ? w.nitems : 0) != 0 ||
-        (next && vsbd_stage_a_next_issue(st->dev, on_device ? NULL : nsrc, linesize,
-                                         on_device ? nsrc : NULL, linesize) != 0)) {
+        (next && (on_device ? vsbd_stage_a_next_issue(st->dev, NULL, linesize, nsrc, linesize)
+                            : vsbd_stage_a_next_issue_uploaded(st->dev, (k + 1) & 1)) != 0) ||
+        (!on_device && k + 2 < nframes &&
+         vsbd_upload(st->dev, frames + (size_t)(k + 2) * frame_bytes, linesize, k & 1) != 0)) {
       vs_log_error(md->conf.modName, "GPU stage failed: %s\n", vsbd_error());
       vsb_frame_discard(&w);
       return -1;

@@ -864,6 +864,11 @@ struct vsbd_ctx {
   int cur, prv;       /* slots of the current and the previous frame */
   cudaStream_t st2;   /* the fine stage */
   cudaEvent_t ev_a, ev_b;
+  /* frames uploaded ahead of their stage A (vsbd_upload), on a copy stream
+     of their own; allocated on first use */
+  uint8_t* d_up[2];
+  cudaStream_t st3;
+  cudaEvent_t ev_up[2];
   int a_search, b_n;  /* the pending stages' search flag / item count */
   double thr_coarse;  /* contrast threshold of the coarse fields */
   int16_t* d_xy;      /* coarse x | coarse y | fine x | fine y */
@@ -980,6 +985,14 @@ extern "C" void vsbd_destroy(vsbd_ctx* c) {
   if (c->ev_a) cudaEventDestroy(c->ev_a);
   if (c->ev_b) cudaEventDestroy(c->ev_b);
   if (c->st2) cudaStreamDestroy(c->st2);
+  if (c->st3) {
+    cudaStreamSynchronize(c->st3);
+    cudaStreamDestroy(c->st3);
+  }
+  for (int k = 0; k < 2; k++) {
+    cudaFree(c->d_up[k]);
+    if (c->ev_up[k]) cudaEventDestroy(c->ev_up[k]);
+  }
   cudaFree(c->d_xy);
   cudaFree(c->d_citems);
   cudaFree(c->d_fitems);
@@ -1356,6 +1369,39 @@ extern "C" int vsbd_stage_a_next_issue(vsbd_ctx* c, const uint8_t* host, int lin
   /* the next frame: blurred into the slot neither this frame nor its
      previous one uses, searched against this frame's plane */
   return stage_a_issue(c, host, linesize, dev, pitch, 1, 3 - c->cur - c->prv, c->cur);
+}
+
+extern "C" int vsbd_upload(vsbd_ctx* c, const uint8_t* host, int linesize, int slot) {
+  CK(cudaSetDevice(c->dev));
+  if (slot < 0 || slot > 1) {
+    set_msg("upload slot must be 0 or 1");
+    return -1;
+  }
+  if (!c->st3) {
+    const size_t plane = (size_t)c->pitch * c->H + 256;
+    for (int k = 0; k < 2; k++) {
+      if (!c->d_up[k]) CK(cudaMalloc(&c->d_up[k], plane));
+      if (!c->ev_up[k]) CK(cudaEventCreateWithFlags(&c->ev_up[k], cudaEventDisableTiming));
+    }
+    CK(cudaStreamCreateWithFlags(&c->st3, cudaStreamNonBlocking));
+  }
+  const int rowbytes = c->W * c->bpp;
+  CK(cudaMemcpy2DAsync(c->d_up[slot], c->pitch, host, linesize, rowbytes, c->H,
+                       cudaMemcpyHostToDevice, c->st3));
+  count_h2d((size_t)rowbytes * c->H);
+  CK(cudaEventRecord(c->ev_up[slot], c->st3));
+  return 0;
+}
+
+extern "C" int vsbd_stage_a_next_issue_uploaded(vsbd_ctx* c, int slot) {
+  CK(cudaSetDevice(c->dev));
+  if (slot < 0 || slot > 1 || !c->d_up[slot]) {
+    set_msg("no frame uploaded in that slot");
+    return -1;
+  }
+  /* the next frame's stage A starts once its upload has landed */
+  CK(cudaStreamWaitEvent(c->st, c->ev_up[slot], 0));
+  return stage_a_issue(c, NULL, 0, c->d_up[slot], c->pitch, 1, 3 - c->cur - c->prv, c->cur);
 }
 
 extern "C" int vsbd_stage_a_next_collect(vsbd_ctx* c, const uint8_t** minmax,

@@ -97,6 +97,12 @@ int vsbd_stage_a_issue(vsbd_ctx* c, const uint8_t* host, int linesize, const uin
 int vsbd_stage_a_next_issue(vsbd_ctx* c, const uint8_t* host, int linesize, const uint8_t* dev,
                             int pitch);
 int vsbd_stage_a_next_collect(vsbd_ctx* c, const uint8_t** minmax, const vsbd_result** coarse);
+/* A host frame copied ahead into upload slot 0 or 1 on a copy stream of its
+   own, so that the copy overlaps the stages of earlier frames; then the next
+   frame's stage A from that slot (it waits for the copy on the device).  A
+   slot may be refilled once the stage A that read it has been collected. */
+int vsbd_upload(vsbd_ctx* c, const uint8_t* host, int linesize, int slot);
+int vsbd_stage_a_next_issue_uploaded(vsbd_ctx* c, int slot);
 int vsbd_stage_b_issue(vsbd_ctx* c, const vsbd_item* items, int n);
 int vsbd_stage_b_collect(vsbd_ctx* c, const vsbd_result** fine);
 
