@@ -736,9 +736,10 @@ int vsb_can_overlap(const VSMotionDetect* md) {
 }
 
 /* A clip through the detector with consecutive frames overlapped on the
-   GPU: while frame k's fine search runs on one stream and the host selects
-   and assembles frame k's motions, stage A of frame k+1 (upload, blur,
-   min/max, coarse search) runs on the other.  Same results, frame by frame,
+   GPU: stage A of frame k+1 (blur, min/max, coarse search) is enqueued
+   before the host selects frame k's fields, and runs on one stream while
+   the host works and frame k's fine search runs on the other; host frames
+   are copied one frame further ahead on a third stream.  Same results, frame by frame,
    as calling vsMotionDetection (or vsb_motion_detection_device) in order.
    Plane 0 of frame k is at frames + k*frame_bytes (host memory, or device
    memory with on_device).  Returns the total number of records, or -1. */
@@ -783,18 +784,33 @@ long vsb_detect_run_overlapped(VSMotionDetect* md, const uint8_t* frames, long f
   for (; k < nframes; k++) {
     int search = 0;
     if (vsb_frame_begin(md, &search) != VS_OK || !search) return -1;
-    vsb_frame_work w;
-    vsb_frame_host_a(md, mm, cres, &w);
     const int next = k + 1 < nframes;
     const uint8_t* nsrc = frames + (size_t)(k + 1) * frame_bytes;
-    if (vsbd_stage_b_issue(st->dev, w.items, w.fine_pass ? w.nitems : 0) != 0 ||
-        (next && (on_device ? vsbd_stage_a_next_issue(st->dev, NULL, linesize, nsrc, linesize)
-                            : vsbd_stage_a_next_issue_uploaded(st->dev, (k + 1) & 1)) != 0) ||
-        (!on_device && k + 2 < nframes &&
-         vsbd_upload(st->dev, frames + (size_t)(k + 2) * frame_bytes, linesize, k & 1) != 0)) {
-      vs_log_error(md->conf.modName, "GPU stage failed: %s\n", vsbd_error());
-      vsb_frame_discard(&w);
-      return -1;
+    /* Plain search: frame k+1's stage A goes first, so that the GPU works
+       while the host selects frame k's fields (its results land in the other
+       output block; frame k's stay readable).  With a proposal network the
+       fine stage goes first: the network kernel fills every SM's shared
+       memory and would hold the fine stage back. */
+    const int a_first = !vsbd_proposal_on(st->dev);
+    vsb_frame_work w;
+    for (int pass = 0; pass < 2; pass++) {
+      if (pass == !a_first) {
+        if ((next && (on_device ? vsbd_stage_a_next_issue(st->dev, NULL, linesize, nsrc, linesize)
+                                : vsbd_stage_a_next_issue_uploaded(st->dev, (k + 1) & 1)) != 0) ||
+            (!on_device && k + 2 < nframes &&
+             vsbd_upload(st->dev, frames + (size_t)(k + 2) * frame_bytes, linesize, k & 1) != 0)) {
+          vs_log_error(md->conf.modName, "GPU stage A failed: %s\n", vsbd_error());
+          if (pass) vsb_frame_discard(&w);
+          return -1;
+        }
+      } else {
+        vsb_frame_host_a(md, mm, cres, &w);
+        if (vsbd_stage_b_issue(st->dev, w.items, w.fine_pass ? w.nitems : 0) != 0) {
+          vs_log_error(md->conf.modName, "GPU stage B failed: %s\n", vsbd_error());
+          vsb_frame_discard(&w);
+          return -1;
+        }
+      }
     }
     const vsbd_result* fres = NULL;
     if (vsbd_stage_b_collect(st->dev, &fres) != 0) {

@@ -887,6 +887,12 @@ struct vsbd_ctx {
   uint8_t* d_out;               /* minmax | coarse results | coarse proposal flags |
                                    fine results | fine proposal flags */
   uint8_t* h_out;               /* pinned mirror of d_out */
+  /* two such blocks: every stage A moves to the other one, so a frame's
+     stage A can run while the host still reads the previous frame's
+     results (d_out/h_out point at the current block) */
+  uint8_t* d_outs[2];
+  uint8_t* h_outs[2];
+  int obuf;
   vsbd_item* h_items;           /* pinned staging of fine items */
   size_t off_coarse, off_cfb, off_fine, off_ffb, out_bytes;
   /* learned search proposal */
@@ -998,13 +1004,15 @@ extern "C" void vsbd_destroy(vsbd_ctx* c) {
   cudaFree(c->d_fitems);
   cudaFree(c->d_keys);
   cudaFree(c->d_tickets);
-  cudaFree(c->d_out);
+  cudaFree(c->d_outs[0]);
+  cudaFree(c->d_outs[1]);
   cudaFree(c->d_skip);
   cudaFree(c->d_part);
   cudaFree(c->d_lists);
   cudaFree(c->d_counts);
   cudaFree(c->d_boxes);
-  if (c->h_out) cudaFreeHost(c->h_out);
+  if (c->h_outs[0]) cudaFreeHost(c->h_outs[0]);
+  if (c->h_outs[1]) cudaFreeHost(c->h_outs[1]);
   if (c->h_items) cudaFreeHost(c->h_items);
   cudaFree(c->d_pn);
   cudaFree(c->d_pout);
@@ -1126,8 +1134,13 @@ extern "C" int vsbd_create(vsbd_ctx** out, int W, int H, int bpp, int blur_size,
   c->off_fine = c->off_cfb + align16((size_t)nc + 1);
   c->off_ffb = c->off_fine + align16(sizeof(vsbd_result) * (nf + 1));
   c->out_bytes = c->off_ffb + align16((size_t)nf + 1);
-  CKC(cudaMalloc(&c->d_out, c->out_bytes));
-  CKC(cudaMallocHost(&c->h_out, c->out_bytes));
+  for (int k = 0; k < 2; k++) {
+    CKC(cudaMalloc(&c->d_outs[k], c->out_bytes));
+    CKC(cudaMallocHost(&c->h_outs[k], c->out_bytes));
+  }
+  c->obuf = 0;
+  c->d_out = c->d_outs[0];
+  c->h_out = c->h_outs[0];
   /* fine items for tuning: every fine field without offset */
   {
     vsbd_item* it = (vsbd_item*)malloc(sizeof(vsbd_item) * (nf + 1));
@@ -1261,6 +1274,11 @@ static int stage_a_issue(vsbd_ctx* c, const uint8_t* host, int linesize, const u
   uint8_t* cur = c->d_buf[ci];
   uint8_t* prv = c->d_buf[pi];
   c->a_search = search;
+  /* this stage's results go to the other output block: the previous frame's
+     stay readable until the next stage A */
+  c->obuf ^= 1;
+  c->d_out = c->d_outs[c->obuf];
+  c->h_out = c->h_outs[c->obuf];
   if (c->blur >= 2) {
     const uint8_t* src = dev;
     int sp = pitch;
@@ -1370,6 +1388,8 @@ extern "C" int vsbd_stage_a_next_issue(vsbd_ctx* c, const uint8_t* host, int lin
      previous one uses, searched against this frame's plane */
   return stage_a_issue(c, host, linesize, dev, pitch, 1, 3 - c->cur - c->prv, c->cur);
 }
+
+extern "C" int vsbd_proposal_on(const vsbd_ctx* c) { return c && c->pn_on; }
 
 extern "C" int vsbd_upload(vsbd_ctx* c, const uint8_t* host, int linesize, int slot) {
   CK(cudaSetDevice(c->dev));

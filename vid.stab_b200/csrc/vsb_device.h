@@ -102,6 +102,8 @@ int vsbd_stage_a_next_collect(vsbd_ctx* c, const uint8_t** minmax, const vsbd_re
    frame's stage A from that slot (it waits for the copy on the device).  A
    slot may be refilled once the stage A that read it has been collected. */
 int vsbd_upload(vsbd_ctx* c, const uint8_t* host, int linesize, int slot);
+/* whether the detector searches with a proposal network */
+int vsbd_proposal_on(const vsbd_ctx* c);
 int vsbd_stage_a_next_issue_uploaded(vsbd_ctx* c, int slot);
 int vsbd_stage_b_issue(vsbd_ctx* c, const vsbd_item* items, int n);
 int vsbd_stage_b_collect(vsbd_ctx* c, const vsbd_result** fine);
