@@ -78,8 +78,10 @@ VS_API long vsb_detect_clip(int width, int height, int pformat, const uint8_t* f
    LocalMotion layout) and freed; counts[k] receives their number.  The
    detector's state (previous frame, frame number) carries over between
    calls.  Without tripod mode or overlay, and with the dense search, frame
-   k+1's upload, blur, min/max and coarse search run on the GPU while frame
-   k's fine search runs and its motions are assembled (same results).
+   k+1's blur, min/max and coarse search run on the GPU while frame k's fine
+   search runs and its motions are assembled (for the plain search also while
+   frame k's fields are selected), and host frames are copied one frame
+   further ahead on a stream of their own (same results).
    Returns the number of records, or -1. */
 VS_API long vsb_detect_run(struct _vsmotiondetect* md, const uint8_t* frames, long frame_bytes,
                            int linesize, int nframes, int on_device, void* out, long out_cap,
