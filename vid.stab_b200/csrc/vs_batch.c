@@ -162,11 +162,12 @@ static int can_overlap(const vsb_batch* b, int check_seen) {
   return 1;
 }
 
-/* Steps k0.. with consecutive steps overlapped on the GPU: stage B of step k
-   (fine search) runs on one CUDA stream while stage A of step k+1 (upload,
-   blur, min/max, coarse search of every stream) runs on the other and the
-   host assembles step k's motions.  Same results as vsb_batch_detect step by
-   step. */
+/* Steps k0.. with consecutive steps overlapped on the GPU.  Two stage As
+   are kept in flight: step k+1's runs while the host selects step k's
+   fields and step k's fine search runs after it, and step k+2's is enqueued
+   as soon as step k's fine search is collected, so the GPU works while the
+   host assembles step k's motions.  Same results as vsb_batch_detect step
+   by step. */
 static long run_overlapped(vsb_batch* b, const uint8_t* const* clips, const long* frame_bytes,
                            const int* pitches, int k0, int nframes, int on_device,
                            const uint8_t** planes, LocalMotions* lms, LocalMotion* rec,
@@ -175,6 +176,14 @@ static long run_overlapped(vsb_batch* b, const uint8_t* const* clips, const long
   if (vsbd_batch_stage_a(b->dev, planes, pitches, on_device) != 0) {
     vs_log_error("vsb_batch", "GPU stage A failed: %s\n", vsbd_error());
     return -1;
+  }
+  if (k0 + 1 < nframes) {
+    for (int s = 0; s < b->n; s++) planes[s] = clips[s] + (size_t)(k0 + 1) * frame_bytes[s];
+    if (vsbd_batch_stage_a_issue(b->dev, planes, pitches, on_device, 1) != 0) {
+      vs_log_error("vsb_batch", "GPU stage A failed: %s\n", vsbd_error());
+      vsbd_batch_drain(b->dev);
+      return -1;
+    }
   }
   for (int k = k0; k < nframes; k++) {
     /* wall time: [0] waiting for stage A, [1] host part A, [2] waiting for
@@ -185,6 +194,7 @@ static long run_overlapped(vsb_batch* b, const uint8_t* const* clips, const long
       const vsbd_result* cres;
       if (vsb_frame_begin(&b->md[s], &b->search[s]) != VS_OK || !b->search[s]) {
         for (int q = 0; q < s; q++) vsb_frame_discard(&b->w[q]);
+        vsbd_batch_drain(b->dev);
         return -1;
       }
       vsbd_batch_results_a(b->dev, s, &mm, &cres);
@@ -192,20 +202,19 @@ static long run_overlapped(vsb_batch* b, const uint8_t* const* clips, const long
       b->items[s] = b->w[s].fine_pass ? b->w[s].items : NULL;
       b->nitems[s] = b->w[s].fine_pass ? b->w[s].nitems : 0;
     }
-    const int next = k + 1 < nframes;
     double t1 = vsb_now_s();
     prof[1] = t1 - t0;
     int rc = vsbd_batch_stage_b_issue(b->dev, b->items, b->nitems);
-    if (rc == 0 && next) {
-      for (int s = 0; s < b->n; s++) planes[s] = clips[s] + (size_t)(k + 1) * frame_bytes[s];
-      rc = vsbd_batch_stage_a_issue(b->dev, planes, pitches, on_device, 1);
-    }
     if (rc == 0) rc = vsbd_batch_stage_b_collect(b->dev, b->fres);
     double t2 = vsb_now_s();
     prof[2] = t2 - t1;
+    if (rc == 0 && k + 2 < nframes) {
+      for (int s = 0; s < b->n; s++) planes[s] = clips[s] + (size_t)(k + 2) * frame_bytes[s];
+      rc = vsbd_batch_stage_a_issue(b->dev, planes, pitches, on_device, 2);
+    }
     if (rc != 0) {
       vs_log_error("vsb_batch", "GPU stage failed: %s\n", vsbd_error());
-      if (next) vsbd_batch_stage_a_collect(b->dev);
+      vsbd_batch_drain(b->dev);
       for (int s = 0; s < b->n; s++) vsb_frame_discard(&b->w[s]);
       return -1;
     }
@@ -216,8 +225,9 @@ static long run_overlapped(vsb_batch* b, const uint8_t* const* clips, const long
     total = emit_step(b, lms, k, rec, total, cap, counts);
     double t3 = vsb_now_s();
     prof[3] = t3 - t2;
-    if (next && vsbd_batch_stage_a_collect(b->dev) != 0) {
+    if (k + 1 < nframes && vsbd_batch_stage_a_collect(b->dev) != 0) {
       vs_log_error("vsb_batch", "GPU stage A failed: %s\n", vsbd_error());
+      vsbd_batch_drain(b->dev);
       return -1;
     }
     prof[0] = vsb_now_s() - t3;

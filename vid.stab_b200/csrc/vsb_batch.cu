@@ -235,6 +235,7 @@ struct vsbd_batch {
   /* results */
   uint8_t* d_resA;
   uint8_t* h_resA;
+  uint8_t* h_resA2;   /* second stage-A result buffer (gA2 copies into it) */
   size_t resA_bytes;
   size_t* mm_off;
   size_t* cres_off;
@@ -257,6 +258,13 @@ struct vsbd_batch {
   size_t smem;
   int grid;
   cudaGraphExec_t gA, gB;
+  cudaGraphExec_t gA2; /* stage A with its results copied to h_resA2 (error flag h_nwork[3]) */
+  BStream* h_desc[2]; /* pinned per-buffer copies of h_streams, the source of each
+                         stage A's descriptor upload */
+  cudaEvent_t evA2;   /* end of a stage A of buffer 1 */
+  int a_buf;          /* result buffer of the stage A issued last (0: h_resA) */
+  int res_buf;        /* result buffer of the stage A collected last */
+  int a_fifo[2], a_n; /* buffers of the stage As in flight, oldest first */
   int b_pending;      /* a stage B was issued and not collected */
   long launches;
   long steps;
@@ -489,7 +497,7 @@ static int autotune_class(vsbd_batch* b, int c, int is_fine) {
   return 0;
 }
 
-static int capture(vsbd_batch* b, int stageB, cudaGraphExec_t* out) {
+static int capture(vsbd_batch* b, int stageB, uint8_t* h_res, int flag, cudaGraphExec_t* out) {
   cudaGraph_t g = NULL;
   BCK(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
   BCtl* ctl = stageB ? b->d_ctlB : b->d_ctlA;
@@ -502,8 +510,8 @@ static int capture(vsbd_batch* b, int stageB, cudaGraphExec_t* out) {
     cudaMemcpyAsync(b->h_resB, b->d_resB, sizeof(vsbd_result) * (size_t)(b->nf_total + 1),
                     cudaMemcpyDeviceToHost, b->st);
   else
-    cudaMemcpyAsync(b->h_resA, b->d_resA, b->resA_bytes, cudaMemcpyDeviceToHost, b->st);
-  cudaMemcpyAsync(stageB ? (void*)&b->h_nwork[1] : (void*)&b->h_nwork[2], &ctl->err,
+    cudaMemcpyAsync(h_res, b->d_resA, b->resA_bytes, cudaMemcpyDeviceToHost, b->st);
+  cudaMemcpyAsync((void*)&b->h_nwork[flag], &ctl->err,
                   sizeof(unsigned), cudaMemcpyDeviceToHost, b->st);
   cudaError_t e = cudaStreamEndCapture(b->st, &g);
   if (e != cudaSuccess) { vsbp_set_err("graph capture", e); return -1; }
@@ -519,6 +527,7 @@ extern "C" void vsbd_batch_destroy(vsbd_batch* b) {
   if (b->st) cudaStreamSynchronize(b->st);
   if (b->st2) cudaStreamSynchronize(b->st2);
   if (b->gA) cudaGraphExecDestroy(b->gA);
+  if (b->gA2) cudaGraphExecDestroy(b->gA2);
   if (b->gB) cudaGraphExecDestroy(b->gB);
   for (int s = 0; s < b->n; s++) {
     if (b->raw) cudaFree(b->raw[s]);
@@ -538,12 +547,16 @@ extern "C" void vsbd_batch_destroy(vsbd_batch* b) {
   cudaFree(b->d_streamsB);
   cudaFreeHost(b->h_streamsB);
   if (b->evA) cudaEventDestroy(b->evA);
+  if (b->evA2) cudaEventDestroy(b->evA2);
+  for (int k = 0; k < 2; k++)
+    if (b->h_desc[k]) cudaFreeHost(b->h_desc[k]);
   if (b->evB) cudaEventDestroy(b->evB);
   if (b->st2) cudaStreamDestroy(b->st2);
   cudaFree(b->d_keys);
   cudaFree(b->d_tickets);
   cudaFree(b->d_resA);
   cudaFreeHost(b->h_resA);
+  if (b->h_resA2) cudaFreeHost(b->h_resA2);
   cudaFree(b->d_resB);
   cudaFreeHost(b->h_resB);
   cudaFree(b->d_workA);
@@ -600,6 +613,7 @@ extern "C" int vsbd_batch_create(vsbd_batch** out, int n, const vsbd_batch_strea
   CKB(cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking));
   CKB(cudaStreamCreateWithFlags(&b->st2, cudaStreamNonBlocking));
   CKB(cudaEventCreateWithFlags(&b->evA, cudaEventDisableTiming));
+  CKB(cudaEventCreateWithFlags(&b->evA2, cudaEventDisableTiming));
   CKB(cudaEventCreateWithFlags(&b->evB, cudaEventDisableTiming));
   b->raw = (uint8_t**)calloc(n, sizeof(uint8_t*));
   b->buf[0] = (uint8_t**)calloc(n, sizeof(uint8_t*));
@@ -618,6 +632,7 @@ extern "C" int vsbd_batch_create(vsbd_batch** out, int n, const vsbd_batch_strea
   memset(b->h_streams, 0, sizeof(BStream) * n);
   CKB(cudaMalloc(&b->d_streams, sizeof(BStream) * n));
   CKB(cudaMallocHost(&b->h_streamsB, sizeof(BStream) * n));
+  for (int k = 0; k < 2; k++) CKB(cudaMallocHost(&b->h_desc[k], sizeof(BStream) * n));
   CKB(cudaMalloc(&b->d_streamsB, sizeof(BStream) * n));
   CKB(cudaMalloc(&b->d_geoms, sizeof(DGeom) * VSB_BATCH_MAX_CLASSES));
   size_t nkeys = 0, resA = 0;
@@ -684,6 +699,7 @@ extern "C" int vsbd_batch_create(vsbd_batch** out, int n, const vsbd_batch_strea
   CKB(cudaMemset(b->d_tickets, 0, sizeof(unsigned) * (nkeys + 1)));
   CKB(cudaMalloc(&b->d_resA, b->resA_bytes));
   CKB(cudaMallocHost(&b->h_resA, b->resA_bytes));
+  CKB(cudaMallocHost(&b->h_resA2, b->resA_bytes));
   CKB(cudaMalloc(&b->d_resB, sizeof(vsbd_result) * (size_t)(nf_total + 1)));
   CKB(cudaMallocHost(&b->h_resB, sizeof(vsbd_result) * (size_t)(nf_total + 1)));
   CKB(cudaMalloc(&b->d_ctlA, sizeof(BCtl)));
@@ -770,19 +786,28 @@ extern "C" int vsbd_batch_create(vsbd_batch** out, int n, const vsbd_batch_strea
     CKB(cudaMemcpy(b->d_ctlA, &h, sizeof(h), cudaMemcpyHostToDevice));
   }
   CKB(cudaStreamSynchronize(b->st));
-  if (capture(b, 0, &b->gA) != 0 || capture(b, 1, &b->gB) != 0) FAILB();
+  if (capture(b, 0, b->h_resA, 2, &b->gA) != 0 || capture(b, 0, b->h_resA2, 3, &b->gA2) != 0 ||
+      capture(b, 1, NULL, 1, &b->gB) != 0)
+    FAILB();
 #undef CKB
 #undef FAILB
   *out = b;
   return 0;
 }
 
-/* Stage A of a step enqueued on the first stream: every stream's frame goes
-   to slot cur (next == 0) or, for the step after the current one, to the
-   third slot, searched against the current frame (next == 1). */
+/* Stage A of a step enqueued on the first stream.  mode 0: every stream's
+   frame goes to slot cur, searched against slot prv; 1: the step after the
+   current one, into the third slot, against cur; 2: the step after that,
+   into slot prv (free once the current step's fine stage is collected),
+   against the third slot, which mode 1 filled.  At most two stage As are in
+   flight; vsbd_batch_stage_a_collect takes the older. */
 extern "C" int vsbd_batch_stage_a_issue(vsbd_batch* b, const uint8_t* const* planes,
-                                        const int* pitches, int on_device, int next) {
+                                        const int* pitches, int on_device, int mode) {
   BCK(cudaSetDevice(b->dev));
+  if (b->a_n >= 2) {
+    vsbp_set_msg("batched stage A: two steps already in flight");
+    return -1;
+  }
   size_t h2d = 0;
   for (int s = 0; s < b->n; s++) {
     BStream& S = b->h_streams[s];
@@ -796,15 +821,21 @@ extern "C" int vsbd_batch_stage_a_issue(vsbd_batch* b, const uint8_t* const* pla
                             cudaMemcpyHostToDevice, b->st));
       h2d += (size_t)S.W * S.H;
     }
-    const int ci = next ? 3 - b->cur[s] - b->prv[s] : b->cur[s];
-    const int pi = next ? b->cur[s] : b->prv[s];
+    const int third = 3 - b->cur[s] - b->prv[s];
+    const int ci = mode == 0 ? b->cur[s] : (mode == 1 ? third : b->prv[s]);
+    const int pi = mode == 0 ? b->prv[s] : (mode == 1 ? b->cur[s] : third);
     S.cur = b->buf[ci][s];
     S.prev = b->buf[pi][s];
   }
-  BCK(cudaMemcpyAsync(b->d_streams, b->h_streams, sizeof(BStream) * b->n, cudaMemcpyHostToDevice,
-                      b->st));
-  BCK(cudaGraphLaunch(b->gA, b->st));
-  BCK(cudaEventRecord(b->evA, b->st));
+  /* alternate result buffers (and descriptor copies): the host may still read
+     the previous stage A's results while this one runs */
+  b->a_buf ^= 1;
+  memcpy(b->h_desc[b->a_buf], b->h_streams, sizeof(BStream) * b->n);
+  BCK(cudaMemcpyAsync(b->d_streams, b->h_desc[b->a_buf], sizeof(BStream) * b->n,
+                      cudaMemcpyHostToDevice, b->st));
+  BCK(cudaGraphLaunch(b->a_buf ? b->gA2 : b->gA, b->st));
+  BCK(cudaEventRecord(b->a_buf ? b->evA2 : b->evA, b->st));
+  b->a_fifo[b->a_n++] = b->a_buf;
   b->launches++;
   vsbp_count(1, h2d + sizeof(BStream) * b->n, b->resA_bytes + 4);
   return 0;
@@ -812,15 +843,32 @@ extern "C" int vsbd_batch_stage_a_issue(vsbd_batch* b, const uint8_t* const* pla
 
 extern "C" int vsbd_batch_stage_a_collect(vsbd_batch* b) {
   BCK(cudaSetDevice(b->dev));
-  BCK(cudaEventSynchronize(b->evA));
-  if (b->h_nwork[2]) {
+  if (b->a_n < 1) {
+    vsbp_set_msg("batched stage A: nothing in flight");
+    return -1;
+  }
+  const int buf = b->a_fifo[0];
+  b->a_fifo[0] = b->a_fifo[1];
+  b->a_n--;
+  BCK(cudaEventSynchronize(buf ? b->evA2 : b->evA));
+  b->res_buf = buf;
+  if (b->h_nwork[buf ? 3 : 2]) {
     vsbp_set_msg("batched stage A: a wait for blur tiles gave up");
     /* skipped tiles leave keys and tickets mid-way: start them afresh */
+    cudaStreamSynchronize(b->st);
+    b->a_n = 0;
     cudaMemset(b->d_keys, 0xff, sizeof(unsigned long long) * (b->nkeys + 1));
     cudaMemset(b->d_tickets, 0, sizeof(unsigned) * (b->nkeys + 1));
     return -1;
   }
   return 0;
+}
+
+/* waits for every stage A in flight, keeping the last error message */
+extern "C" void vsbd_batch_drain(vsbd_batch* b) {
+  cudaSetDevice(b->dev);
+  cudaStreamSynchronize(b->st);
+  b->a_n = 0;
 }
 
 extern "C" int vsbd_batch_stage_a(vsbd_batch* b, const uint8_t* const* planes, const int* pitches,
@@ -831,8 +879,9 @@ extern "C" int vsbd_batch_stage_a(vsbd_batch* b, const uint8_t* const* planes, c
 
 extern "C" void vsbd_batch_results_a(const vsbd_batch* b, int s, const uint8_t** mm,
                                      const vsbd_result** cres) {
-  *mm = b->h_resA + b->mm_off[s];
-  *cres = (const vsbd_result*)(b->h_resA + b->cres_off[s]);
+  const uint8_t* h = b->res_buf ? b->h_resA2 : b->h_resA;
+  *mm = h + b->mm_off[s];
+  *cres = (const vsbd_result*)(h + b->cres_off[s]);
 }
 
 /* Stage B of the current step enqueued on the second stream, with its own

@@ -47,13 +47,17 @@ int vsbd_batch_stage_b(vsbd_batch* b, const vsbd_item* const* items, const int* 
 /* stream s's current blurred frame becomes its previous one */
 void vsbd_batch_commit(vsbd_batch* b, int stream);
 
-/* Overlapped steps: stage A enqueued only (next != 0: the step after the
-   current one, into every stream's third plane slot) and collected later;
-   stage B enqueued on a second stream and collected later, so that the next
-   step's stage A runs beside the current step's stage B. */
+/* Overlapped steps: stage A enqueued only and collected later, at most two
+   in flight (mode 0: the current step; 1: the next one, into every stream's
+   third plane slot; 2: the one after, into the previous step's slot, once
+   the current step's fine stage is collected); stage B enqueued on a second
+   stream and collected later.  vsbd_batch_stage_a_collect takes the older
+   stage A in flight and makes its results the ones vsbd_batch_results_a
+   returns; vsbd_batch_drain waits for all. */
 int vsbd_batch_stage_a_issue(vsbd_batch* b, const uint8_t* const* planes, const int* pitches,
-                             int on_device, int next);
+                             int on_device, int mode);
 int vsbd_batch_stage_a_collect(vsbd_batch* b);
+void vsbd_batch_drain(vsbd_batch* b);
 int vsbd_batch_stage_b_issue(vsbd_batch* b, const vsbd_item* const* items, const int* nitems);
 int vsbd_batch_stage_b_collect(vsbd_batch* b, const vsbd_result** fres);
 

@@ -893,6 +893,8 @@ struct vsbd_ctx {
   uint8_t* d_outs[2];
   uint8_t* h_outs[2];
   int obuf;
+  uint8_t* b_hout;              /* host block the pending stage B copies into (a
+                                   stage A may switch d_out/h_out meanwhile) */
   vsbd_item* h_items;           /* pinned staging of fine items */
   size_t off_coarse, off_cfb, off_fine, off_ffb, out_bytes;
   /* learned search proposal */
@@ -1434,6 +1436,7 @@ extern "C" int vsbd_stage_b_issue(vsbd_ctx* c, const vsbd_item* items, int n) {
   CK(cudaSetDevice(c->dev));
   if (n > c->nf) { set_msg("more fine items than fine fields"); return -1; }
   c->b_n = n;
+  c->b_hout = c->h_out;
   if (n <= 0) return 0;
   cudaStream_t st = c->st2;
   memcpy(c->h_items, items, sizeof(vsbd_item) * n);
@@ -1476,12 +1479,13 @@ extern "C" int vsbd_stage_b_issue(vsbd_ctx* c, const vsbd_item* items, int n) {
 
 extern "C" int vsbd_stage_b_collect(vsbd_ctx* c, const vsbd_result** fine) {
   CK(cudaSetDevice(c->dev));
-  *fine = (const vsbd_result*)(c->h_out + c->off_fine);
+  uint8_t* h = c->b_hout ? c->b_hout : c->h_out;
+  *fine = (const vsbd_result*)(h + c->off_fine);
   if (c->b_n <= 0) return 0;
   CK(cudaEventSynchronize(c->ev_b));
   kt_collect(c);
   if (c->pn_on)
-    proposal_tally(c, c->h_out + c->off_ffb, (const vsbd_result*)(c->h_out + c->off_fine),
+    proposal_tally(c, h + c->off_ffb, (const vsbd_result*)(h + c->off_fine),
                    c->h_vres ? c->h_vres + c->nc : NULL, c->b_n, 1);
   return 0;
 }
