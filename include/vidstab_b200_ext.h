@@ -213,6 +213,15 @@ VS_API long vsb_batch_run(vsb_batch* b, const uint8_t* const* clips, const long*
                           const int* pitches, int nframes, int on_device, void* out,
                           long out_cap, int* counts);
 VS_API void vsb_batch_free(vsb_batch* b);
+/* The .trf output of vidstabdetect for batched streams: paths[s] (NULL:
+   none) is created and started for stream s in serialization_mode
+   (ASCII_SERIALIZATION_MODE or BINARY_SERIALIZATION_MODE), and every later
+   step (vsb_batch_detect, vsb_batch_run) appends that stream's frame to it,
+   byte for byte what vsWriteToFile writes after vsMotionDetection for a
+   detector of its own.  Closing (or vsb_batch_free) ends the files.  Returns
+   VS_OK or VS_ERROR (no file stays open then). */
+VS_API int vsb_batch_open_trf(vsb_batch* b, const char* const* paths, int serialization_mode);
+VS_API int vsb_batch_close_trf(vsb_batch* b);
 /* persistent-kernel launches so far */
 VS_API long vsb_batch_launch_count(const vsb_batch* b);
 /* the persistent grid: CTAs, threads per CTA, dynamic shared memory per CTA */

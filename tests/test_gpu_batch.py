@@ -129,3 +129,32 @@ def test_batch_run_with_tripod_stream():
     for (g, gc), (e, ec) in zip(got, per_stream(frames, tripod=3)):
         assert np.array_equal(gc, ec)
         assert records_equal(g, e)
+
+
+@pytest.mark.parametrize("mode", [1, 2])
+def test_batch_trf_matches_single_stream(tmp_path, mode):
+    # the batch's .trf files equal, byte for byte, those a detector of its
+    # own writes for the stream; per-step calls and the overlapped run both
+    # append; a stream without a path writes nothing
+    sizes = [(640, 360), (1280, 720), (640, 360)]
+    T = 6
+    frames = [S.clip(w, h, T, seed=700 + i) for i, (w, h) in enumerate(sizes)]
+    paths = [str(tmp_path / ("batch%d_%d.trf" % (mode, s))) for s in range(len(sizes))]
+    paths[2] = None
+    b = V.Batch([w for w, _ in sizes], [h for _, h in sizes])
+    try:
+        b.open_trf(paths, mode)
+        pitches = [w for w, _ in sizes]
+        for k in range(2):
+            b.detect([f[k].ctypes.data for f in frames], pitches, False)
+        batch_records(b, [np.ascontiguousarray(f[2:]) for f in frames], True)
+        b.close_trf()
+    finally:
+        b.close()
+    for s, p in enumerate(paths):
+        if p is None:
+            continue
+        exp = str(tmp_path / ("single%d_%d.trf" % (mode, s)))
+        V.detect_clip(frames[s], V.PF_YUV420P, serialization_mode=mode, trf_path=exp)
+        with open(p, "rb") as fa, open(exp, "rb") as fb:
+            assert fa.read() == fb.read(), s

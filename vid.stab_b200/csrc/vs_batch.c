@@ -9,6 +9,7 @@
  * streams as two persistent-kernel launches (vsb_batch.cu) with the
  * per-stream host phases in between.
  */
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -25,10 +26,52 @@ struct vsb_batch {
   const vsbd_item** items;
   int* nitems;
   const vsbd_result** fres;
+  FILE** trf; /* per stream: the .trf file its motions go to (NULL: none) */
 };
+
+/* after a stream's frame ended (frame number advanced, as vidstabdetect
+   writes after vsMotionDetection): its motions to the stream's .trf */
+static int write_trf(vsb_batch* b, int s, const LocalMotions* lms) {
+  if (!b->trf || !b->trf[s]) return VS_OK;
+  if (vsWriteToFile(&b->md[s], b->trf[s], lms) != VS_OK) {
+    vs_log_error("vsb_batch", "writing the .trf of stream %d failed\n", s);
+    return VS_ERROR;
+  }
+  return VS_OK;
+}
+
+int vsb_batch_close_trf(vsb_batch* b) {
+  if (!b) return VS_ERROR;
+  int rc = VS_OK;
+  if (b->trf)
+    for (int s = 0; s < b->n; s++)
+      if (b->trf[s] && fclose(b->trf[s]) != 0) rc = VS_ERROR;
+  free(b->trf);
+  b->trf = NULL;
+  return rc;
+}
+
+int vsb_batch_open_trf(vsb_batch* b, const char* const* paths, int serialization_mode) {
+  if (!b || !paths) return VS_ERROR;
+  vsb_batch_close_trf(b);
+  b->trf = (FILE**)calloc((size_t)b->n, sizeof(FILE*));
+  if (!b->trf) return VS_ERROR;
+  for (int s = 0; s < b->n; s++) {
+    if (!paths[s]) continue;
+    b->md[s].serializationMode = serialization_mode;
+    b->trf[s] = fopen(paths[s], "wb");
+    if (!b->trf[s] || vsPrepareFile(&b->md[s], b->trf[s]) != VS_OK) {
+      vs_log_error("vsb_batch", "cannot start the .trf of stream %d (%s)\n", s, paths[s]);
+      vsb_batch_close_trf(b);
+      return VS_ERROR;
+    }
+  }
+  return VS_OK;
+}
 
 void vsb_batch_free(vsb_batch* b) {
   if (!b) return;
+  vsb_batch_close_trf(b);
   vsbd_batch_destroy(b->dev);
   if (b->md)
     for (int s = 0; s < b->n; s++)
@@ -122,19 +165,21 @@ int vsb_batch_detect(vsb_batch* b, const uint8_t* const* planes, const int* pitc
     return VS_ERROR;
   }
   double t3 = vsb_now_s();
+  int trf_rc = VS_OK;
   for (int s = 0; s < b->n; s++) {
     if (b->search[s])
       vsb_frame_host_b(&b->md[s], b->fres[s], &b->w[s], &motions[s]);
     else
       vsb_frame_first(&b->md[s], &motions[s]);
     if (vsb_frame_end(&b->md[s])) vsbd_batch_commit(b->dev, s);
+    if (write_trf(b, s, &motions[s]) != VS_OK) trf_rc = VS_ERROR;
   }
   prof[0] = t1 - t0;
   prof[1] = t2 - t1;
   prof[2] = t3 - t2;
   prof[3] = vsb_now_s() - t3;
   vsb_prof_add(prof, b->n);
-  return VS_OK;
+  return trf_rc;
 }
 
 /* a step's motions into the record array */
@@ -218,11 +263,17 @@ static long run_overlapped(vsb_batch* b, const uint8_t* const* clips, const long
       for (int s = 0; s < b->n; s++) vsb_frame_discard(&b->w[s]);
       return -1;
     }
+    int trf_rc = VS_OK;
     for (int s = 0; s < b->n; s++) {
       vsb_frame_host_b(&b->md[s], b->fres[s], &b->w[s], &lms[s]);
       if (vsb_frame_end(&b->md[s])) vsbd_batch_commit(b->dev, s);
+      if (write_trf(b, s, &lms[s]) != VS_OK) trf_rc = VS_ERROR;
     }
     total = emit_step(b, lms, k, rec, total, cap, counts);
+    if (trf_rc != VS_OK) {
+      vsbd_batch_drain(b->dev);
+      return -1;
+    }
     double t3 = vsb_now_s();
     prof[3] = t3 - t2;
     if (k + 1 < nframes && vsbd_batch_stage_a_collect(b->dev) != 0) {

@@ -132,6 +132,10 @@ def lib():
     L.vsb_batch_grid.argtypes = [p, p, p, p]
     L.vsb_batch_class.restype = i
     L.vsb_batch_class.argtypes = [p, i, p]
+    L.vsb_batch_open_trf.restype = i
+    L.vsb_batch_open_trf.argtypes = [p, p, i]
+    L.vsb_batch_close_trf.restype = i
+    L.vsb_batch_close_trf.argtypes = [p]
     L.vsb_boxblur_host.restype = i
     L.vsb_boxblur_host.argtypes = [p, p, i, i, i]
     L.vsb_field_minmax_host.restype = i

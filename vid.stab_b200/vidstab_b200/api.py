@@ -154,6 +154,18 @@ class Batch:
         self.L.vsb_batch_grid(self.h, C.byref(a), C.byref(b), C.byref(c))
         return a.value, b.value, c.value
 
+    def open_trf(self, paths, serialization_mode=1):
+        """Starts a .trf file per stream (None: no file for that stream);
+        later steps append to them (vsb_batch_open_trf)."""
+        enc = [p.encode() if p is not None else None for p in paths]
+        arr = (C.c_char_p * self.n)(*enc)
+        if self.L.vsb_batch_open_trf(self.h, C.cast(arr, C.c_void_p), serialization_mode) != 0:
+            raise RuntimeError("vsb_batch_open_trf failed")
+
+    def close_trf(self):
+        if self.L.vsb_batch_close_trf(self.h) != 0:
+            raise RuntimeError("vsb_batch_close_trf failed")
+
     def classes(self):
         """Per geometry class: the search tiling and its tuned time
         (vsb_batch_class)."""
