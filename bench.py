@@ -583,6 +583,11 @@ def main():
             fps, n, el = r
             cpu = {"value": fps, "unit": "frames/s", "cores": cores, "kind": "reference",
                    "sample": "first %d frames of the same clip (%.1f s)" % (n, el)}
+            r1 = cpu_reference(host_np, min(args.cpu_seconds, 5.0), 1)
+            if r1:
+                cpu["one_thread"] = {"value": r1[0], "unit": "frames/s", "cores": 1,
+                                     "sample": "first %d frames of the same clip (%.1f s)"
+                                               % (r1[1], r1[2])}
 
     if rank == 0:
         line = {
