@@ -37,6 +37,10 @@
 #include "vsb_search.cuh"
 
 #define VSB_BATCH_THREADS 512
+/* stage B (fine search only) runs the same kernel with 256-thread CTAs, two
+   per SM: fine-field tiles need at most 256 threads, and a second CTA hides
+   each tile's staging and reductions */
+#define VSB_BATCH_THREADS_B 256
 #define VSB_BATCH_MAX_STREAMS 1024
 #define VSB_BATCH_MAX_CLASSES 64
 
@@ -140,7 +144,8 @@ __device__ __forceinline__ void search_tile(const BStream& S, const DGeom* geoms
 /* Stage A: the static work list `work`.  Stage B (work == NULL): item w of
    the fine search is found from the per-stream prefix sums (tile-granular)
    and item offsets into the packed fine work list. */
-__global__ void __launch_bounds__(VSB_BATCH_THREADS) k_batch(const BWork* __restrict__ work,
+template <int NT>
+__global__ void __launch_bounds__(NT, VSB_BATCH_THREADS / NT) k_batch_t(const BWork* __restrict__ work,
                                                              const BStream* __restrict__ streams,
                                                              const DGeom* __restrict__ geoms,
                                                              BCtl* ctl, const int* __restrict__ prefix,
@@ -211,7 +216,10 @@ struct vsbd_batch {
   vsbd_geom cls_key[VSB_BATCH_MAX_CLASSES]; /* order: owned copy */
   int cls_items[VSB_BATCH_MAX_CLASSES];     /* search items of the class per step */
   float cls_us[VSB_BATCH_MAX_CLASSES];      /* tuned time of those items alone */
-  size_t static_smem;                       /* of k_batch */
+  size_t static_smem;                       /* of the kernel (larger of both block sizes) */
+  int cls_nt[VSB_BATCH_MAX_CLASSES];        /* block size a class's tiling must fit */
+  size_t smem_b;                            /* stage B: dynamic shared memory, grid */
+  int grid_b;
   int optin;                                /* per-block shared memory limit */
   size_t nkeys;
   DGeom* d_geoms;
@@ -294,9 +302,26 @@ static int same_geom(const vsbd_geom* a, const vsbd_geom* b) {
 /* a tiling the persistent kernel can run: TB 2 or 4, one or two columns
    per thread, at most its block size, tile and static shared memory within
    the per-block limit */
-static int tiling_ok(const vsbd_batch* b, const DGeom& g) {
-  return (g.tb == 2 || g.tb == 4) && g.threads <= VSB_BATCH_THREADS &&
+static int tiling_ok(const vsbd_batch* b, const DGeom& g, int nt = VSB_BATCH_THREADS) {
+  return (g.tb == 2 || g.tb == 4) && g.threads <= nt &&
          tile_layout(g).total + b->static_smem + 64 <= (size_t)b->optin;
+}
+
+/* the model's best tiling of class k that fits blocks of nt threads */
+static int default_tiling(vsbd_batch* b, int k, int nitems, int nt) {
+  TileCand cand[16];
+  int nc = vsbp_tile_candidates(b->cls[k].g, nitems, nt, cand, 16);
+  for (int i = 0; i < nc; i++)
+    if (tiling_ok(b, cand[i].g, nt)) {
+      DGeom t = cand[i].g;
+      t.order = b->cls[k].g.order;
+      t.point = b->cls[k].g.point;
+      b->cls[k].g = t;
+      b->cls[k].smem = tile_layout(t).total;
+      return 0;
+    }
+  vsbp_set_msg("no search tiling of the batched kernel fits in shared memory");
+  return -1;
 }
 
 static int class_of(vsbd_batch* b, const vsbd_geom* g, int nitems) {
@@ -315,20 +340,9 @@ static int class_of(vsbd_batch* b, const vsbd_geom* g, int nitems) {
   b->cls_key[k] = *g;
   b->cls_key[k].order = own;
   b->ncls++;
+  b->cls_nt[k] = VSB_BATCH_THREADS;
   /* the default tiling: the model's best that the persistent kernel runs */
-  TileCand cand[16];
-  int nc = vsbp_tile_candidates(b->cls[k].g, nitems, VSB_BATCH_THREADS, cand, 16);
-  for (int i = 0; i < nc; i++)
-    if (tiling_ok(b, cand[i].g)) {
-      DGeom t = cand[i].g;
-      t.order = b->cls[k].g.order;
-      t.point = b->cls[k].g.point;
-      b->cls[k].g = t;
-      b->cls[k].smem = tile_layout(t).total;
-      return k;
-    }
-  vsbp_set_msg("no search tiling of the batched kernel fits in shared memory");
-  return -1;
+  return default_tiling(b, k, nitems, VSB_BATCH_THREADS) == 0 ? k : -1;
 }
 
 static size_t kernel_smem(const vsbd_batch* b) {
@@ -342,14 +356,36 @@ static size_t kernel_smem(const vsbd_batch* b) {
 
 static int set_grid(vsbd_batch* b) {
   b->smem = kernel_smem(b);
-  BCK(cudaFuncSetAttribute(k_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem));
+  BCK(cudaFuncSetAttribute(k_batch_t<VSB_BATCH_THREADS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)b->smem));
   int per = 0;
-  BCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_batch, VSB_BATCH_THREADS, b->smem));
+  BCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_batch_t<VSB_BATCH_THREADS>,
+                                                    VSB_BATCH_THREADS, b->smem));
   if (per < 1) {
     vsbp_set_msg("the batched kernel does not fit on an SM");
     return -1;
   }
   b->grid = per * vsbp_sm_count();
+  return 0;
+}
+
+/* stage B's grid: shared memory of the classes that serve fine fields */
+static int set_grid_b(vsbd_batch* b) {
+  size_t m = 16;
+  for (int k = 0; k < b->ncls; k++)
+    if (b->cls_nt[k] == VSB_BATCH_THREADS_B && tile_layout(b->cls[k].g).total > m)
+      m = tile_layout(b->cls[k].g).total;
+  b->smem_b = m;
+  BCK(cudaFuncSetAttribute(k_batch_t<VSB_BATCH_THREADS_B>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem_b));
+  int per = 0;
+  BCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_batch_t<VSB_BATCH_THREADS_B>,
+                                                    VSB_BATCH_THREADS_B, b->smem_b));
+  if (per < 1) {
+    vsbp_set_msg("the batched fine-search kernel does not fit on an SM");
+    return -1;
+  }
+  b->grid_b = per * vsbp_sm_count();
   return 0;
 }
 
@@ -409,10 +445,13 @@ static int build_workA(vsbd_batch* b, BWork** out, int* count, int only_cls, int
   return 0;
 }
 
-static int launch_k(vsbd_batch* b, const BWork* work, BCtl* ctl, cudaStream_t st) {
-  k_batch<<<b->grid, VSB_BATCH_THREADS, b->smem, st>>>(work, b->d_streams, b->d_geoms, ctl,
-                                                       b->d_pre, b->d_pre + b->n + 1, b->d_fitems,
-                                                       b->n);
+static int launch_k(vsbd_batch* b, const BWork* work, BCtl* ctl, cudaStream_t st, int nt) {
+  if (nt == VSB_BATCH_THREADS_B)
+    k_batch_t<VSB_BATCH_THREADS_B><<<b->grid_b, VSB_BATCH_THREADS_B, b->smem_b, st>>>(
+        work, b->d_streams, b->d_geoms, ctl, b->d_pre, b->d_pre + b->n + 1, b->d_fitems, b->n);
+  else
+    k_batch_t<VSB_BATCH_THREADS><<<b->grid, VSB_BATCH_THREADS, b->smem, st>>>(
+        work, b->d_streams, b->d_geoms, ctl, b->d_pre, b->d_pre + b->n + 1, b->d_fitems, b->n);
   BCK(cudaGetLastError());
   return 0;
 }
@@ -431,11 +470,14 @@ static int autotune_class(vsbd_batch* b, int c, int is_fine) {
      from aligned window copies; two from one copy and a shifted field copy):
      the cost model does not see the shared-memory loads and shifts in which
      they differ */
+  /* fine classes run in stage B's 256-thread blocks and are timed there */
+  const int nt = b->cls_nt[c];
+  const int kernel_nt = is_fine ? VSB_BATCH_THREADS_B : VSB_BATCH_THREADS;
   TileCand cand[24];
-  int nc = vsbp_tile_candidates_ta(b->cls[c].g, nitems, VSB_BATCH_THREADS, cand, 5, 1);
-  nc += vsbp_tile_candidates_ta(b->cls[c].g, nitems, VSB_BATCH_THREADS, cand + nc, 5, 2);
-  nc += vsbp_tile_candidates_ta(b->cls[c].g, nitems, VSB_BATCH_THREADS, cand + nc, 6, 3);
-  nc += vsbp_tile_candidates_ta(b->cls[c].g, nitems, VSB_BATCH_THREADS, cand + nc, 6, 4);
+  int nc = vsbp_tile_candidates_ta(b->cls[c].g, nitems, nt, cand, 5, 1);
+  nc += vsbp_tile_candidates_ta(b->cls[c].g, nitems, nt, cand + nc, 5, 2);
+  nc += vsbp_tile_candidates_ta(b->cls[c].g, nitems, nt, cand + nc, 6, 3);
+  nc += vsbp_tile_candidates_ta(b->cls[c].g, nitems, nt, cand + nc, 6, 4);
   cudaEvent_t e0, e1;
   BCK(cudaEventCreate(&e0));
   BCK(cudaEventCreate(&e1));
@@ -443,7 +485,7 @@ static int autotune_class(vsbd_batch* b, int c, int is_fine) {
   DGeom best = b->cls[c].g;
   int tried = 0;
   for (int k = 0; k < nc && tried < 18; k++) {
-    if (!tiling_ok(b, cand[k].g)) continue;
+    if (!tiling_ok(b, cand[k].g, nt)) continue;
     tried++;
     DGeom t = cand[k].g;
     t.order = b->cls[c].g.order;
@@ -452,7 +494,8 @@ static int autotune_class(vsbd_batch* b, int c, int is_fine) {
     b->cls[c].g = t;
     BWork* w = NULL;
     int nw = 0;
-    if (set_grid(b) != 0 || upload_geoms(b) != 0 || build_workA(b, &w, &nw, c, is_fine) != 0) {
+    if ((kernel_nt == VSB_BATCH_THREADS_B ? set_grid_b(b) : set_grid(b)) != 0 ||
+        upload_geoms(b) != 0 || build_workA(b, &w, &nw, c, is_fine) != 0) {
       b->cls[c].g = keep;
       free(w);
       continue;
@@ -474,7 +517,7 @@ static int autotune_class(vsbd_batch* b, int c, int is_fine) {
       if (cudaMemcpyAsync(b->d_ctlA, &h, sizeof(h), cudaMemcpyHostToDevice, b->st) != cudaSuccess)
         ok = 0;
       if (rep == 1) cudaEventRecord(e0, b->st);
-      if (ok && launch_k(b, d_w, b->d_ctlA, b->st) != 0) ok = 0;
+      if (ok && launch_k(b, d_w, b->d_ctlA, b->st, kernel_nt) != 0) ok = 0;
       if (rep == 3) cudaEventRecord(e1, b->st);
       if (cudaStreamSynchronize(b->st) != cudaSuccess) ok = 0;
     }
@@ -502,10 +545,13 @@ static int capture(vsbd_batch* b, int stageB, uint8_t* h_res, int flag, cudaGrap
   BCK(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
   BCtl* ctl = stageB ? b->d_ctlB : b->d_ctlA;
   cudaMemsetAsync(ctl, 0, offsetof(BCtl, nwork), b->st);
-  k_batch<<<b->grid, VSB_BATCH_THREADS, b->smem, b->st>>>(stageB ? NULL : b->d_workA,
-                                                          stageB ? b->d_streamsB : b->d_streams,
-                                                          b->d_geoms, ctl, b->d_pre,
-                                                          b->d_pre + b->n + 1, b->d_fitems, b->n);
+  if (stageB)
+    k_batch_t<VSB_BATCH_THREADS_B><<<b->grid_b, VSB_BATCH_THREADS_B, b->smem_b, b->st>>>(
+        NULL, b->d_streamsB, b->d_geoms, ctl, b->d_pre, b->d_pre + b->n + 1, b->d_fitems, b->n);
+  else
+    k_batch_t<VSB_BATCH_THREADS><<<b->grid, VSB_BATCH_THREADS, b->smem, b->st>>>(
+        b->d_workA, b->d_streams, b->d_geoms, ctl, b->d_pre, b->d_pre + b->n + 1, b->d_fitems,
+        b->n);
   if (stageB)
     cudaMemcpyAsync(b->h_resB, b->d_resB, sizeof(vsbd_result) * (size_t)(b->nf_total + 1),
                     cudaMemcpyDeviceToHost, b->st);
@@ -598,15 +644,17 @@ extern "C" int vsbd_batch_create(vsbd_batch** out, int n, const vsbd_batch_strea
   cudaGetDevice(&b->dev);
   b->n = n;
   {
-    cudaFuncAttributes fa;
-    if (cudaFuncGetAttributes(&fa, k_batch) != cudaSuccess ||
+    cudaFuncAttributes fa, fb;
+    if (cudaFuncGetAttributes(&fa, k_batch_t<VSB_BATCH_THREADS>) != cudaSuccess ||
+        cudaFuncGetAttributes(&fb, k_batch_t<VSB_BATCH_THREADS_B>) != cudaSuccess ||
         cudaDeviceGetAttribute(&b->optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->dev) !=
             cudaSuccess) {
       vsbp_set_msg("cannot query the batched kernel");
       free(b);
       return -1;
     }
-    b->static_smem = fa.sharedSizeBytes;
+    b->static_smem = fa.sharedSizeBytes > fb.sharedSizeBytes ? fa.sharedSizeBytes
+                                                             : fb.sharedSizeBytes;
   }
 #define CKB(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) { vsbp_set_err(#call, e_); vsbd_batch_destroy(b); return -1; } } while (0)
 #define FAILB() do { vsbd_batch_destroy(b); return -1; } while (0)
@@ -737,7 +785,21 @@ extern "C" int vsbd_batch_create(vsbd_batch** out, int n, const vsbd_batch_strea
     }
   /* tuning of fine classes runs through the stage-A path with citems
      replaced: point each stream's citems at its fine items for that run */
-  if (set_grid(b) != 0 || upload_geoms(b) != 0) FAILB();
+  /* classes that serve fine fields run in stage B's smaller blocks */
+  for (int c = 0; c < b->ncls; c++) {
+    int used_f = 0, nitems = 0;
+    for (int s = 0; s < n; s++)
+      if (b->h_streams[s].gf == c) {
+        used_f = 1;
+        nitems += b->h_streams[s].nf;
+      }
+    if (!used_f) continue;
+    b->cls_nt[c] = VSB_BATCH_THREADS_B;
+    if (b->cls[c].g.threads > VSB_BATCH_THREADS_B &&
+        default_tiling(b, c, nitems, VSB_BATCH_THREADS_B) != 0)
+      FAILB();
+  }
+  if (set_grid(b) != 0 || set_grid_b(b) != 0 || upload_geoms(b) != 0) FAILB();
   for (int c = 0; c < b->ncls; c++) {
     int used_c = 0, used_f = 0;
     for (int s = 0; s < n; s++) {
@@ -771,7 +833,7 @@ extern "C" int vsbd_batch_create(vsbd_batch** out, int n, const vsbd_batch_strea
       if (rc != 0) FAILB();
     }
   }
-  if (set_grid(b) != 0 || upload_geoms(b) != 0) FAILB();
+  if (set_grid(b) != 0 || set_grid_b(b) != 0 || upload_geoms(b) != 0) FAILB();
   BWork* w = NULL;
   if (build_workA(b, &w, &b->nworkA, -1, 0) != 0) FAILB();
   cudaError_t e = cudaMalloc(&b->d_workA, sizeof(BWork) * (size_t)(b->nworkA + 1));
