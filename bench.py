@@ -9,11 +9,12 @@ shakiness 5, mincontrast 0.25).  One step = the detect pass over the whole clip.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
-* value: frames/s with the clip resident in HBM, through
-  vsb_motion_detection_device (no host copies of frames);
-* e2e: frames/s through the drop-in C API vsMotionDetection with the frames in
-  pinned host memory (the luma copy to the device and the per-field results
-  back are inside the timed region);
+* value: frames/s with the clip resident in HBM, through the library's frame
+  loop vsb_detect_run over device frames (the results of
+  vsb_motion_detection_device frame by frame; no host copies of frames);
+* e2e: frames/s through the same frame loop with the frames in pinned host
+  memory (vsMotionDetection's results frame by frame; the luma copy to the
+  device and the per-field results back are inside the timed region);
 * roofline: the dominant kernel (the coarse SAD search) against the measured
   packed-SAD throughput of this GPU, and the prefilter against HBM;
 * cpu_baseline: the reference's own CPU detect (compiled from its sources,
@@ -598,8 +599,10 @@ def main():
             "config": {"workload": WORKLOAD, "frames_per_step": nfr, "width": W, "height": H,
                        "l2": "inputs (%d MB of luma) larger than L2" % (nfr * W * H // 2**20),
                        "parallelism": "replicas x%d (independent clips, no collective)" % world,
-                       "timed_step": "the clip's frames through one initialised detector "
-                                     "(vsMotionDetection per frame, records copied out)",
+                       "timed_step": "the clip's frames through one initialised detector's "
+                                     "frame loop (vsb_detect_run: vsMotionDetection's results "
+                                     "frame by frame, consecutive frames overlapped on the "
+                                     "GPU, records copied out)",
                        "vs_baseline_ref": "docs/simd.md 1080p AVX2 19-thread figure (4.43 ms/frame)"},
             "e2e": {"value": e2e, "unit": "frames/s",
                     "h2d_bytes_per_step": (h1 - h0) // max(args.steps, 1),
