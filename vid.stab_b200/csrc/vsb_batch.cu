@@ -165,8 +165,12 @@ __global__ void __launch_bounds__(NT, VSB_BATCH_THREADS / NT) k_batch_t(const BW
       const BWork it = work[w];
       const BStream& S = streams[it.stream];
       if (it.type == 0) {
-        blur_tile(S.src, S.sp, S.cur, S.pitch, S.W, S.H, S.half, S.dv, it.a % S.ntx,
-                  it.a / S.ntx, sm);
+        if (S.half <= BTF_MAXHALF)
+          blur_tile_fast(S.src, S.sp, S.cur, S.pitch, S.W, S.H, S.half, S.dv, it.a % S.ntx,
+                         it.a / S.ntx, sm);
+        else
+          blur_tile(S.src, S.sp, S.cur, S.pitch, S.W, S.H, S.half, S.dv, it.a % S.ntx,
+                    it.a / S.ntx, sm);
         __syncthreads();
         if (threadIdx.x == 0) {
           __threadfence();
@@ -346,7 +350,7 @@ static int class_of(vsbd_batch* b, const vsbd_geom* g, int nitems) {
 }
 
 static size_t kernel_smem(const vsbd_batch* b) {
-  size_t m = BT_SMEM;
+  size_t m = BT_SMEM > BTF_SMEM ? BT_SMEM : BTF_SMEM;
   for (int k = 0; k < b->ncls; k++) {
     size_t t = tile_layout(b->cls[k].g).total;
     if (t > m) m = t;
@@ -698,7 +702,10 @@ extern "C" int vsbd_batch_create(vsbd_batch** out, int n, const vsbd_batch_strea
     S.half = q.blur_size >= 2 ? q.blur_size / 2 : 0;
     make_div(q.blur_size >= 2 ? q.blur_size : 1, S.half, &S.dv);
     if (q.blur_size < 2) { S.dv.mul = 0; S.dv.size = 1; S.dv.exact = 0; }
-    S.ntx = (q.width + BT_W - 1) / BT_W;
+    /* blur tiles: 256 x 32 with vector access up to half-width 16, else the
+       128 x 32 byte tile */
+    const int tw = S.half <= BTF_MAXHALF ? BTF_W : BT_W;
+    S.ntx = (q.width + tw - 1) / tw;
     S.nty = (q.height + BT_H - 1) / BT_H;
     S.nc = q.nc;
     S.nf = q.nf;

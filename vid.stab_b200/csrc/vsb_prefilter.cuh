@@ -78,6 +78,97 @@ __device__ __forceinline__ void blur_tile(const uint8_t* __restrict__ src, int s
   }
 }
 
+/* The same blur over a BTF_H x BTF_W output tile with vector memory access,
+   for half-widths up to BTF_MAXHALF given at run time (at least 256
+   threads).  Input rows with clamped coordinates are staged from 16 bytes
+   left of the tile to 16 bytes right of it, with 16-byte loads when the tile
+   is interior and the source 16-byte aligned, else bytewise.  The
+   horizontal pass gives each task a run of 16 outputs of one row (a sliding
+   window sum, one 16-byte store); the vertical pass runs 4-column sliding
+   sums down a quarter of the tile and stores words (threads beyond 256 have
+   no column).  Same window sums and floor division as blur_tile. */
+#define BTF_W 256
+#define BTF_H 32
+#define BTF_MAXHALF 16
+#define BTF_RAWP (BTF_W + 32)
+#define BTF_SMEM ((BTF_H + 2 * BTF_MAXHALF) * (BTF_RAWP + BTF_W))
+
+__device__ __forceinline__ void blur_tile_fast(const uint8_t* __restrict__ src, int sp,
+                                               uint8_t* __restrict__ dst, int dp, int W, int H,
+                                               int half, BlurDiv dv, int bx, int by,
+                                               uint8_t* smem) {
+  const int rows = BTF_H + 2 * half, win = 2 * half + 1;
+  uint8_t* raw = smem;
+  uint8_t* hor = smem + rows * BTF_RAWP;
+  const int x0 = bx * BTF_W, y0 = by * BTF_H;
+  const bool vec = x0 >= 16 && x0 + BTF_W + 16 <= W &&
+                   ((((uintptr_t)src) | (uintptr_t)(unsigned)sp) & 15) == 0;
+  if (vec) {
+    for (int i = threadIdx.x; i < rows * (BTF_RAWP / 16); i += blockDim.x) {
+      const int r = i / (BTF_RAWP / 16), v = i - r * (BTF_RAWP / 16);
+      const int gy = min(max(y0 - half + r, 0), H - 1);
+      *(uint4*)(raw + r * BTF_RAWP + (v << 4)) =
+          *(const uint4*)(src + (size_t)gy * sp + x0 - 16 + (v << 4));
+    }
+  } else {
+    for (int i = threadIdx.x; i < rows * BTF_RAWP; i += blockDim.x) {
+      const int r = i / BTF_RAWP, c = i - r * BTF_RAWP;
+      const int gy = min(max(y0 - half + r, 0), H - 1);
+      const int gx = min(max(x0 - 16 + c, 0), W - 1);
+      raw[r * BTF_RAWP + c] = src[(size_t)gy * sp + gx];
+    }
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < rows * (BTF_W / 16); t += blockDim.x) {
+    const int r = t / (BTF_W / 16), c0 = (t - r * (BTF_W / 16)) * 16;
+    const uint8_t* rp = raw + r * BTF_RAWP + 16 + c0; /* the byte of column c0 */
+    unsigned acc = 0;
+    for (int k = -half; k <= half; k++) acc += rp[k];
+    uint32_t o[4] = { 0u, 0u, 0u, 0u };
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+      if (q > 0) acc += (unsigned)rp[q + half] - (unsigned)rp[q - 1 - half];
+      o[q >> 2] |= blur_div(acc, dv) << (8 * (q & 3));
+    }
+    *(uint4*)(hor + r * BTF_W + c0) = make_uint4(o[0], o[1], o[2], o[3]);
+  }
+  __syncthreads();
+  if (threadIdx.x >= 256) return;
+  const int cg = threadIdx.x & 63, part = threadIdx.x >> 6;
+  const int gx = x0 + cg * 4;
+  if (gx >= W) return;
+  const int rb = part * (BTF_H / 4);
+  unsigned a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+  for (int k = 0; k < win; k++) {
+    const unsigned w = *(const unsigned*)(hor + (rb + k) * BTF_W + cg * 4);
+    a0 += w & 0xff;
+    a1 += (w >> 8) & 0xff;
+    a2 += (w >> 16) & 0xff;
+    a3 += w >> 24;
+  }
+  const bool full4 = gx + 4 <= W;
+  for (int r = rb; r < rb + BTF_H / 4; r++) {
+    if (r > rb) {
+      const unsigned wi = *(const unsigned*)(hor + (r + win - 1) * BTF_W + cg * 4);
+      const unsigned wo = *(const unsigned*)(hor + (r - 1) * BTF_W + cg * 4);
+      a0 += (wi & 0xff) - (wo & 0xff);
+      a1 += ((wi >> 8) & 0xff) - ((wo >> 8) & 0xff);
+      a2 += ((wi >> 16) & 0xff) - ((wo >> 16) & 0xff);
+      a3 += (wi >> 24) - (wo >> 24);
+    }
+    const int gy = y0 + r;
+    if (gy >= H) break;
+    const unsigned o = blur_div(a0, dv) | (blur_div(a1, dv) << 8) | (blur_div(a2, dv) << 16) |
+                       (blur_div(a3, dv) << 24);
+    uint8_t* d = dst + (size_t)gy * dp + gx;
+    if (full4) {
+      *(unsigned*)d = o;
+    } else {
+      for (int k = 0; k < 4 && gx + k < W; k++) d[k] = (uint8_t)(o >> (8 * k));
+    }
+  }
+}
+
 /* Field f of a field list, by one CTA: 8-bit min/max per channel (channel ch
    of a pixel is byte ch of its bpp bytes) into out[(f*nch + ch)*2 + {0,1}].
    With skip != NULL it also flags a field whose contrast keeps it out of the
