@@ -41,6 +41,8 @@
    per SM: fine-field tiles need at most 256 threads, and a second CTA hides
    each tile's staging and reductions */
 #define VSB_BATCH_THREADS_B 256
+/* fields per min/max work item (one warp each; stage A has 16 warps) */
+#define VSB_MM_GROUP 16
 #define VSB_BATCH_MAX_STREAMS 1024
 #define VSB_BATCH_MAX_CLASSES 64
 
@@ -178,11 +180,14 @@ __global__ void __launch_bounds__(NT, VSB_BATCH_THREADS / NT) k_batch_t(const BW
         }
       } else if (wait_blur(ctl, it.stream, (unsigned)(S.ntx * S.nty))) {
         if (it.type == 1) {
-          const int f = it.a;
-          const bool coarse = f < S.nc;
-          const int x = coarse ? S.xy[f] : S.xy[2 * S.nc + (f - S.nc)];
-          const int y = coarse ? S.xy[S.nc + f] : S.xy[2 * S.nc + S.nf + (f - S.nc)];
-          minmax_field(S.cur, S.pitch, x, y, coarse ? S.Sc : S.Sf, 1, 1, f, S.mm, 0.0, NULL);
+          /* fields a*MM_GROUP .. +MM_GROUP, one warp each */
+          const int f = it.a * VSB_MM_GROUP + (int)(threadIdx.x >> 5);
+          if ((int)(threadIdx.x >> 5) < VSB_MM_GROUP && f < S.nc + S.nf) {
+            const bool coarse = f < S.nc;
+            const int x = coarse ? S.xy[f] : S.xy[2 * S.nc + (f - S.nc)];
+            const int y = coarse ? S.xy[S.nc + f] : S.xy[2 * S.nc + S.nf + (f - S.nc)];
+            minmax_field_warp(S.cur, S.pitch, x, y, coarse ? S.Sc : S.Sf, f, S.mm);
+          }
         } else {
           const DGeom* gp = &geoms[S.gc];
           const int ntiles = gp->nta * gp->ntb;
@@ -443,7 +448,8 @@ static int build_workA(vsbd_batch* b, BWork** out, int* count, int only_cls, int
   }
   if (only_cls < 0)
     for (int s = 0; s < b->n; s++)
-      for (int f = 0; f < b->h_streams[s].nc + b->h_streams[s].nf; f++) w[k++] = { 1, s, f, 0 };
+      for (int g = 0; g * VSB_MM_GROUP < b->h_streams[s].nc + b->h_streams[s].nf; g++)
+        w[k++] = { 1, s, g, 0 };
   *out = w;
   *count = (int)k;
   return 0;

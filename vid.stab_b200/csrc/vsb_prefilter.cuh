@@ -216,6 +216,50 @@ __device__ __forceinline__ void minmax_field(const uint8_t* __restrict__ img, in
   }
 }
 
+/* 8-bit min/max of one planar field by one warp (out[f*2 + {0,1}]): rows
+   read with 16-byte loads from the 16-byte boundary at or left of the
+   field, bytes outside the field masked to the neutral value.  The plane's
+   rows must start on 16-byte boundaries, with readable bytes up to 15 past
+   the field's right edge. */
+__device__ __forceinline__ unsigned mm_byte_mask(int lo, int hi) {
+  unsigned m = 0;
+#pragma unroll
+  for (int b = 0; b < 4; b++)
+    if (b >= lo && b < hi) m |= 0xffu << (8 * b);
+  return m;
+}
+
+__device__ __forceinline__ void minmax_field_warp(const uint8_t* __restrict__ img, int pitch,
+                                                  int x, int y, int S, int f,
+                                                  uint8_t* __restrict__ out) {
+  const int lane = threadIdx.x & 31;
+  const int x0 = x - S / 2, y0 = y - S / 2;
+  const int xa = x0 & ~15;
+  const int nv = (x0 + S - xa + 15) >> 4;
+  unsigned mn = 0xffffffffu, mx = 0u;
+  for (int i = lane; i < S * nv; i += 32) {
+    const int r = i / nv, v = i - r * nv;
+    const int bx = xa + (v << 4);
+    const uint4 q = *(const uint4*)(img + (size_t)(y0 + r) * pitch + bx);
+    const unsigned w[4] = { q.x, q.y, q.z, q.w };
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const int b0 = bx + 4 * k;
+      const unsigned m = mm_byte_mask(x0 - b0, x0 + S - b0);
+      mn = __vminu4(mn, w[k] | ~m);
+      mx = __vmaxu4(mx, w[k] & m);
+    }
+  }
+  unsigned bmn = min(min(mn & 0xff, (mn >> 8) & 0xff), min((mn >> 16) & 0xff, mn >> 24));
+  unsigned bmx = max(max(mx & 0xff, (mx >> 8) & 0xff), max((mx >> 16) & 0xff, mx >> 24));
+  bmn = __reduce_min_sync(0xffffffffu, bmn);
+  bmx = __reduce_max_sync(0xffffffffu, bmx);
+  if (lane == 0) {
+    out[f * 2 + 0] = (uint8_t)bmn;
+    out[f * 2 + 1] = (uint8_t)bmx;
+  }
+}
+
 /* divisor set-up of the blur (host) */
 static inline int make_div(int size, int half, BlurDiv* d) {
   d->size = (unsigned)size;
