@@ -79,6 +79,23 @@ def dist_env():
     return rank, world, local
 
 
+def reduce_max(vals, dist, device):
+    """Each of vals, maxed over the ranks in one all-reduce (vals as they are
+    without a process group): every rank's timed totals become the slowest
+    rank's."""
+    if not dist:
+        return [float(v) for v in vals]
+    import torch
+    t = torch.tensor([float(v) for v in vals], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t]
+
+
+def aggregate_fps(frames_per_step, steps, world, seconds):
+    """whole-job frames/s: every rank's frames over the slowest rank's time"""
+    return frames_per_step * steps * world / seconds
+
+
 def host_cores():
     try:
         return len(os.sched_getaffinity(0))
@@ -497,12 +514,9 @@ def main():
     det_host.close()
     tot_dev = sum(dev_times)
     tot_host = sum(host_times)
-    if dist:
-        t = torch.tensor([tot_dev, tot_host], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tot_dev, tot_host = float(t[0]), float(t[1])
-    value = nfr * args.steps * world / tot_dev
-    e2e = nfr * args.steps * world / tot_host
+    tot_dev, tot_host = reduce_max([tot_dev, tot_host], dist, "cuda")
+    value = aggregate_fps(nfr, args.steps, world, tot_dev)
+    e2e = aggregate_fps(nfr, args.steps, world, tot_host)
 
     def timed_local(fn, steps):
         """CUDA-event time of fn on this rank alone (no barrier)"""
