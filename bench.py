@@ -31,6 +31,23 @@ shakiness 5, mincontrast 0.25).  One step = the detect pass over the whole clip.
 
 With --gpus N (torchrun), every rank runs an independent clip (seed + rank):
 no data moves between GPUs; the time is the max over ranks.
+
+Every timed step's LocalMotions (all frames of the clip) are compared with
+the reference's CPU detect of the same clip (oracle/_ref, compiled from the
+reference's sources; the C restatement where that build is absent).
+
+Profiling modes (no JSON line; an NVTX range around the last frames or
+steps, for ncu --nvtx --nvtx-include "detect/" or "batch/"):
+
+  python bench.py --profile detect [--width 1920 --height 1080]
+      [--profile-frames 4] [--profiled 1] [--search dense|pruned]
+      [--proposal default|PATH] [--conf-min X] [--host-profile]
+  python bench.py --profile batch [--mix 64|small] [--profile-frames 4] [--profiled 1]
+
+"detect" runs the per-frame API over a clip in device memory
+(vsb_motion_detection_device); "batch" steps the 64-stream mix with the
+per-step batch API.  The frames (steps) before the range prime the detector
+(first frame, autotuning).
 """
 import argparse
 import ctypes as C
@@ -66,9 +83,23 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
-    ap.add_argument("--batch-frames", type=int, default=30)
+    ap.add_argument("--batch-frames", type=int, default=120)
     ap.add_argument("--no-shake4k", action="store_true")
-    ap.add_argument("--shake4k-frames", type=int, default=10)
+    ap.add_argument("--shake4k-frames", type=int, default=120)
+    ap.add_argument("--side-steps", type=int, default=2,
+                    help="timed steps of the batched and 4K arms (each a whole 120-frame run)")
+    ap.add_argument("--side-warmup", type=int, default=1)
+    ap.add_argument("--no-per-frame", action="store_true")
+    ap.add_argument("--profile", choices=["none", "detect", "batch"], default="none")
+    ap.add_argument("--width", type=int, default=W)
+    ap.add_argument("--height", type=int, default=H)
+    ap.add_argument("--profile-frames", type=int, default=4)
+    ap.add_argument("--profiled", type=int, default=1)
+    ap.add_argument("--search", choices=["dense", "pruned"], default="dense")
+    ap.add_argument("--proposal", default=None)
+    ap.add_argument("--conf-min", type=float, default=float("nan"))
+    ap.add_argument("--host-profile", action="store_true")
+    ap.add_argument("--mix", choices=["64", "small"], default="64")
     return ap.parse_args()
 
 
@@ -195,6 +226,27 @@ def traffic_from_profile(name):
     return None
 
 
+LM_FIELDS = ("vx", "vy", "fx", "fy", "fsize", "contrast", "match")
+
+
+def same_records(a, b):
+    """LocalMotions equality over all seven fields, in order (the predicate of
+    tests/test_determinism.c:356-361 of the reference)"""
+    return len(a) == len(b) and all(np.array_equal(a[k], b[k]) for k in LM_FIELDS)
+
+
+def reference_records(frames_np, threads, pformat=1, **kw):
+    """LocalMotions of the reference's CPU detect over a clip (the C
+    restatement where the reference build is absent): records, per-frame
+    counts, checker name"""
+    import oracle as O
+    if O.ref_available():
+        r, c, _ = O.ref_clip(frames_np, pformat, threads=threads, **kw)
+        return r, c, "reference (oracle/_ref)"
+    r, c = O.oracle_clip(frames_np, pformat, **kw)
+    return r, c, "oracle restatement"
+
+
 def frames_identical(a, ca, b, cb):
     """frames whose LocalMotions are identical in two runs"""
     oa = np.concatenate([[0], np.cumsum(ca)])
@@ -261,7 +313,9 @@ def batched_arm(V, steps, warmup, timed, frames):
     of its own seed, through one batch (persistent kernel per stage from
     captured CUDA graphs), against the same streams run one after another
     through single-stream detectors on the same GPU, and through the same
-    detectors stepped together by one host thread (vsb_detect_multi)."""
+    detectors stepped together by one host thread (vsb_detect_multi).
+    Every stream's batch output is compared with its own detector's, and
+    the first stream of each resolution with the reference's CPU detect."""
     from vidstab_b200 import synthetic as S
     classes = [(640, 360, 26), (1280, 720, 19), (1920, 1080, 13), (3840, 2160, 6)]
     sizes = [(w, h) for w, h, n in classes for _ in range(n)]
@@ -274,37 +328,49 @@ def batched_arm(V, steps, warmup, timed, frames):
     counts = np.zeros(frames * n, np.int32)
     b = V.Batch([w for w, _ in sizes], [h for _, h in sizes])
     tot = b.run(ptrs, fb, pitches, frames, True, out, counts)  # fresh streams: the parity run
-    out_first, counts_first = out.copy(), counts.copy()
+    cm = counts.reshape(frames, n).copy()
+    pos = np.concatenate([[0], np.cumsum(cm.ravel())])
+
+    def batch_stream(s):
+        return np.concatenate([out[pos[k * n + s]:pos[k * n + s + 1]] for k in range(frames)])
+
+    mine = [batch_stream(s) for s in range(n)]
     for _ in range(warmup):
         b.run(ptrs, fb, pitches, frames, True, out, counts)
     l0 = b.launches()
     tb = timed(lambda: b.run(ptrs, fb, pitches, frames, True, out, counts), steps)
     launches = (b.launches() - l0) // max(steps, 1)
     b.close()
-    out, counts = out_first, counts_first
-    # every stream through a detector of its own, one after another
+    # every stream through a detector of its own, one after another; the
+    # first (untimed) pass checks every stream against the batch
     dets = [V.MotionDetector(w, h, V.PF_YUV420P) for w, h in sizes]
     rec = np.zeros(frames * 800 + 64, V.LM_DTYPE)
     cnt = np.zeros(frames, np.int32)
-    cm = counts.reshape(frames, n)
-    pos = np.concatenate([[0], np.cumsum(cm.ravel())])
     same = 0
+    for s in range(n):
+        t = dets[s].run(frames, ptrs[s], fb[s], pitches[s], True, rec, cnt)
+        same += int(np.array_equal(cm[:, s], cnt) and same_records(mine[s], rec[:t]))
 
     def run_all():
         for s in range(n):
             dets[s].run(frames, ptrs[s], fb[s], pitches[s], True, rec, cnt)
 
-    for s in (0, n - 1):  # parity of a small and a 4K stream with their own detectors
-        d = V.MotionDetector(sizes[s][0], sizes[s][1], V.PF_YUV420P)
-        t = d.run(frames, ptrs[s], fb[s], pitches[s], True, rec, cnt)
-        d.close()
-        mine = np.concatenate([out[pos[k * n + s]:pos[k * n + s + 1]] for k in range(frames)])
-        same += int(np.array_equal(cm[:, s], cnt) and np.array_equal(mine, rec[:t]))
-    run_all()
+    # the first stream of each resolution against the reference's CPU detect
+    ref_same, checker = [], None
+    first = 0
+    for w, h, k in classes:
+        r, c, checker = reference_records(clips[first].cpu().numpy(), host_cores())
+        ref_same.append("%dx%d: %s" % (w, h, "identical" if np.array_equal(c, cm[:, first]) and
+                                        same_records(r, mine[first]) else "DIFFERENT"))
+        first += k
+    for _ in range(warmup):
+        run_all()
     ts = timed(run_all, steps)
     # the same detectors stepped together by one host thread (vsb_detect_multi)
     mout = np.zeros(frames * n * 800 + 64, V.LM_DTYPE)
     mcnt = np.zeros(frames * n, np.int32)
+    for _ in range(warmup):
+        V.detect_multi(dets, ptrs, fb, pitches, frames, True, mout, mcnt)
     tm = timed(lambda: V.detect_multi(dets, ptrs, fb, pitches, frames, True, mout, mcnt), steps)
     for d in dets:
         d.close()
@@ -312,8 +378,10 @@ def batched_arm(V, steps, warmup, timed, frames):
     seq = n * frames * steps / sum(ts)
     multi = n * frames * steps / sum(tm)
     return {"value": agg, "unit": "frames/s (all streams)", "streams": n,
-            "frames_per_stream": frames, "records": int(tot),
-            "streams_checked_identical": "%d of 2" % same,
+            "frames_per_stream": frames, "records": int(tot), "steps": steps, "warmup": warmup,
+            "streams_checked_identical": "%d of %d (batch vs each stream's own detector, all "
+                                         "frames)" % (same, n),
+            "reference_check": {"checker": checker, "streams": ref_same},
             "single_stream_detectors_sequential": seq, "speedup": agg / seq,
             "detectors_stepped_together": multi,
             "persistent_launches_per_step": int(launches),
@@ -389,6 +457,9 @@ def shake4k_arm(V, steps, warmup, timed, frames):
 
 
 def run_reference(args):
+    """The reference's own CPU detect (oracle/_ref, compiled from its
+    sources) over the same 300-frame clip the GPU arm runs (same generator,
+    seed and device), every step the whole clip, all host threads."""
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
@@ -396,10 +467,18 @@ def run_reference(args):
     if not O.ref_available():
         print(json.dumps({"impl": "reference", "unavailable": "reference build (oracle/_ref) not present"}))
         return 0
-    from vidstab_b200 import synthetic as S
     cores = host_cores()
-    n = 20
-    frames = S.clip(W, H, n, seed=1)
+    n = args.frames
+    device = "cpu"
+    try:
+        import torch
+        if torch.cuda.is_available():
+            device = "cuda"
+    except Exception:
+        pass
+    clip = make_clip(n, seed=1, device=device)
+    frames = clip.cpu().numpy()
+    del clip
     for _ in range(args.warmup):
         O.ref_clip(frames[:3], 1, threads=cores)
     times = []
@@ -407,7 +486,8 @@ def run_reference(args):
         _, _, el = O.ref_clip(frames, 1, threads=cores)
         times.append(el)
     fps = n / statistics.median(times)
-    sample = "first %d frames of the 1920x1080 clip per step (frame 0 only primes the detector)" % n
+    sample = ("the whole %d-frame 1920x1080 clip per step, the clip the GPU arm times "
+              "(seed 1, generated on %s)" % (n, device))
     print(json.dumps({
         "metric": METRIC, "value": fps, "unit": "frames/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * statistics.median(times),
@@ -421,8 +501,96 @@ def run_reference(args):
     return 0
 
 
+def profile_detect(a):
+    """NVTX range "detect" around the last a.profiled frames of the per-frame
+    API over a clip in device memory"""
+    import ctypes as C
+    import torch
+    import vidstab_b200 as V
+    from vidstab_b200 import synthetic as S
+    w, h = a.width, a.height
+    n = max(a.profile_frames, a.profiled + 2)
+    clip = S.clip(w, h, n, seed=1, device="cuda")
+    torch.cuda.synchronize()
+    V.lib().vsb_set_default_search_mode(1 if a.search == "pruned" else 0)
+    det = V.MotionDetector(w, h, V.PF_YUV420P)
+    if a.proposal:
+        from vidstab_b200 import pnet
+        blob = pnet.load_blob(None if a.proposal == "default" else a.proposal)
+        pnet.set_proposal(det, blob, conf_min=a.conf_min)
+    L = V.lib()
+    L.vsb_host_profile.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
+    L.vsb_host_profile.restype = None
+    first = n - a.profiled
+    records = 0
+    for k in range(n):
+        if k == first:
+            torch.cuda.synchronize()
+            L.vsb_host_profile(None, None, 1)
+            torch.cuda.nvtx.range_push("detect")
+        records += len(det.detect_device(clip.data_ptr() + k * w * h, w))
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
+    if a.host_profile:
+        sec = (C.c_double * 4)()
+        nf = C.c_long()
+        L.vsb_host_profile(sec, C.byref(nf), 0)
+        per = [1e6 * v / max(nf.value, 1) for v in sec]
+        print("per frame (us): device stage A %.1f, host A %.1f, device stage B %.1f, host B %.1f,"
+              " total %.1f" % (per[0], per[1], per[2], per[3], sum(per)))
+    det.close()
+    print("frames %d (%d in the range), %d local motions" % (n, a.profiled, records))
+    return 0
+
+
+def profile_batch(a):
+    """NVTX range "batch" around the last a.profiled steps of a batch of
+    camera-walk streams stepped with the per-step API"""
+    import ctypes as C
+    import torch
+    import vidstab_b200 as V
+    from vidstab_b200 import synthetic as S
+    mixes = {"64": [(640, 360, 26), (1280, 720, 19), (1920, 1080, 13), (3840, 2160, 6)],
+             "small": [(640, 360, 4), (1280, 720, 2), (1920, 1080, 1)]}
+    sizes = [(w, h) for w, h, n in mixes[a.mix] for _ in range(n)]
+    steps = max(a.profile_frames, a.profiled + 2)
+    clips = [S.clip(w, h, steps, seed=5000 + i, device="cuda") for i, (w, h) in enumerate(sizes)]
+    torch.cuda.synchronize()
+    pitches = [w for w, _ in sizes]
+    b = V.Batch([w for w, _ in sizes], [h for _, h in sizes])
+    L = V.lib()
+    L.vsb_host_profile.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
+    first = steps - a.profiled
+    records = 0
+    try:
+        for k in range(steps):
+            if k == first:
+                torch.cuda.synchronize()
+                L.vsb_host_profile(None, None, 1)
+                torch.cuda.nvtx.range_push("batch")
+            planes = [c.data_ptr() + k * w * h for c, (w, h) in zip(clips, sizes)]
+            records += sum(len(r) for r in b.detect(planes, pitches, True))
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
+        sec = (C.c_double * 4)()
+        nf = C.c_long()
+        L.vsb_host_profile(sec, C.byref(nf), 0)
+        per = [1e3 * v / max(nf.value / len(sizes), 1) for v in sec]
+        print("per step (ms): stage A %.2f, host A %.2f, stage B %.2f, host B %.2f"
+              % (per[0], per[1], per[2], per[3]))
+        print("streams %d, steps %d (%d in the range), %d local motions, grid %s"
+              % (len(sizes), steps, a.profiled, records, b.grid()))
+    finally:
+        b.close()
+    return 0
+
+
 def main():
     args = parse()
+    if args.profile == "detect":
+        return profile_detect(args)
+    if args.profile == "batch":
+        return profile_batch(args)
     if args.impl == "reference":
         return run_reference(args)
     import torch
@@ -463,24 +631,19 @@ def main():
     def run_host():
         return det_host.run(nfr, host_np.ctypes.data, W * H, W, False, rec, cnt)
 
-    # parity of the timed path against the reference on a prefix of the clip
-    parity = None
-    if rank == 0:
-        import oracle as O
-        npar = 8
-        got, gc, _ = V.detect_clip(npar, V.PF_YUV420P, on_device_ptr=clip.data_ptr(),
-                                   frame_bytes=W * H, linesize=W, width=W, height=H)
-        if O.ref_available():
-            exp, ec, _ = O.ref_clip(host_np[:npar], 1, threads=host_cores())
-            checker = "reference (oracle/_ref)"
-        else:
-            exp, ec = O.oracle_clip(host_np[:npar], 1)
-            checker = "oracle restatement"
-        same = bool(np.array_equal(gc, ec) and all(np.array_equal(got[k], exp[k]) for k in (
-            "vx", "vy", "fx", "fy", "fsize", "contrast", "match")))
-        parity = {"frames": npar, "records": int(len(got)), "identical": same, "checker": checker}
+    # the reference's LocalMotions of the whole clip: every timed step's
+    # output is compared with them (every rank checks its own clip)
+    ref_rec, ref_cnt, checker = reference_records(host_np, max(1, host_cores() // world))
+    checks = {"device": [], "host": [], "per_frame": []}
 
-    def timed(fn, steps):
+    def check(kind, cnt_now, total):
+        checks[kind].append(bool(total == len(ref_rec) and np.array_equal(cnt_now, ref_cnt) and
+                                 same_records(rec[:total], ref_rec)))
+
+    def timed(fn, steps, after=None):
+        """CUDA-event time of each of `steps` calls of fn, bracketed by a
+        barrier and a device synchronize on both sides; after(result) runs
+        outside the timed region"""
         ts = []
         for _ in range(steps):
             if dist:
@@ -489,12 +652,14 @@ def main():
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record()
-            fn()
+            r = fn()
             e1.record()
             torch.cuda.synchronize()
             if dist:
                 dist.barrier()
             ts.append(e0.elapsed_time(e1) / 1000.0)
+            if after:
+                after(r)
         return ts
 
     for _ in range(args.warmup):
@@ -502,21 +667,49 @@ def main():
     clocks = Clocks(local)
     clocks.start()
     l0, _, _ = counters()
-    dev_times = timed(run_device, args.steps)
+    dev_times = timed(run_device, args.steps, lambda t: check("device", cnt, t))
     l1, _, _ = counters()
     clk = clocks.stop()
     for _ in range(max(1, args.warmup // 2)):
         run_host()
     _, h0, d0 = counters()
-    host_times = timed(run_host, args.steps)
+    host_times = timed(run_host, args.steps, lambda t: check("host", cnt, t))
     _, h1, d1 = counters()
     det_dev.close()
     det_host.close()
+    # the drop-in's per-frame path: one vsMotionDetection call per frame
+    # (what vidstabdetect calls), pinned host frames, no overlap between frames
+    per_frame = None
+    if not args.no_per_frame:
+        det_pf = V.MotionDetector(W, H, V.PF_YUV420P)
+
+        def run_pf():
+            return det_pf.run_frames(nfr, host_np.ctypes.data, W * H, W, False, rec, cnt)
+
+        for _ in range(max(1, args.warmup // 2)):
+            run_pf()
+        p0, _, _ = counters()
+        pf_times = timed(run_pf, args.steps, lambda t: check("per_frame", cnt, t))
+        p1, _, _ = counters()
+        det_pf.close()
+        (tot_pf,) = reduce_max([sum(pf_times)], dist, "cuda")
+        per_frame = {"value": aggregate_fps(nfr, args.steps, world, tot_pf), "unit": "frames/s",
+                     "launches_per_frame": (p1 - p0) / float(nfr * args.steps),
+                     "api": "vsMotionDetection once per frame, pinned host frames, each call "
+                            "returning the frame's motions (vsb_detect_frames)"}
     tot_dev = sum(dev_times)
     tot_host = sum(host_times)
     tot_dev, tot_host = reduce_max([tot_dev, tot_host], dist, "cuda")
     value = aggregate_fps(nfr, args.steps, world, tot_dev)
     e2e = aggregate_fps(nfr, args.steps, world, tot_host)
+    identical = all(checks["device"]) and all(checks["host"]) and all(checks["per_frame"])
+    (all_ranks,) = reduce_max([0.0 if identical else 1.0], dist, "cuda")
+    parity = {"frames": nfr, "records": int(len(ref_rec)), "checker": checker,
+              "steps_checked": {k: len(v) for k, v in checks.items()},
+              "identical": bool(identical), "all_ranks_identical": all_ranks == 0.0,
+              "checked": "the LocalMotions of every timed step (value, e2e and per_frame "
+                         "loops), all frames, all seven fields, against the checker's detect "
+                         "of the same clip"}
 
     def timed_local(fn, steps):
         """CUDA-event time of fn on this rank alone (no barrier)"""
@@ -537,10 +730,11 @@ def main():
     if rank == 0 and not args.no_learned:
         learned = learned_arm(V, clip, host_np, nfr, args.steps, args.warmup, timed_local)
     if rank == 0 and not args.no_batched:
-        batched = batched_arm(V, args.steps, args.warmup, timed_local, args.batch_frames)
+        batched = batched_arm(V, args.side_steps, args.side_warmup, timed_local, args.batch_frames)
     shake4k = None
     if rank == 0 and not args.no_shake4k:
-        shake4k = shake4k_arm(V, args.steps, args.warmup, timed_local, args.shake4k_frames)
+        shake4k = shake4k_arm(V, args.side_steps, args.side_warmup, timed_local,
+                              args.shake4k_frames)
 
     # per-kernel device time on the detector's stream (separate, instrumented pass)
     roof = None
@@ -624,7 +818,7 @@ def main():
             "gpu_launches": l1 - l0,
             "roofline": roof, "roofline_hbm": roof_hbm, "kernel_ms": kernel_ms,
             "learned": learned, "batched": batched, "large_shake_4k": shake4k,
-            "cpu_baseline": cpu, "clocks": clk, "parity": parity,
+            "cpu_baseline": cpu, "clocks": clk, "parity": parity, "per_frame": per_frame,
         }
         print(json.dumps(line))
     if dist:

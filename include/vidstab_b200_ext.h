@@ -87,6 +87,14 @@ VS_API long vsb_detect_run(struct _vsmotiondetect* md, const uint8_t* frames, lo
                            int linesize, int nframes, int on_device, void* out, long out_cap,
                            int* counts);
 
+/* As vsb_detect_run, without the overlap: each frame is one call of
+   vsMotionDetection (or vsb_motion_detection_device) that returns only
+   when the frame's motions are complete -- the call sequence of a host
+   filter such as vidstabdetect, timed as the drop-in's per-frame path. */
+VS_API long vsb_detect_frames(struct _vsmotiondetect* md, const uint8_t* frames,
+                              long frame_bytes, int linesize, int nframes, int on_device,
+                              void* out, long out_cap, int* counts);
+
 /* Many initialised detectors (one per stream, any mix of resolutions, with
    or without a search proposal) stepped together by the calling thread:
    every frame, the coarse stage of every detector is enqueued before any is
@@ -126,6 +134,14 @@ VS_API void vsb_counters(long long* launches, long long* h2d_bytes, long long* d
    each stage rather than its duration. */
 VS_API void vsb_host_profile(double* sec, long* frames, int reset);
 
+/* Test hook for the out-of-memory paths, host side only: returns the number
+   of device allocations (cudaMalloc) the library has made since load; with
+   fail_after >= 0 the allocation fail_after calls from now fails with
+   cudaErrorMemoryAllocation (sticky != 0: that one and every later one),
+   -1 disarms it.  The calls that meet the failure return VS_ERROR (or NULL)
+   with the reason in vsb_last_error() and free what they had allocated. */
+VS_API long long vsb_test_device_alloc(int fail_after, int sticky);
+
 /* Measured byte-absolute-difference throughput (per second) of the GPU's
    packed SAD instruction sequence in a register-only loop: variant 0 the
    accumulate form the kernels use, 1 and 2 alternative formulations. */
@@ -156,14 +172,15 @@ VS_API int vsb_field_search_host(const uint8_t* curr, const uint8_t* prev, int w
 
 /* ---- allocation-free search (no counterpart in the reference) ----------
    For callers that cannot let a library allocate GPU memory: hosts that own
-   all device memory through their own pools or budgets, or that call while
-   a CUDA graph is being recorded, where cudaMalloc is not allowed.  It runs
+   all device memory through their own pools or budgets, where a cudaMalloc
+   they did not make breaks the pool's accounting or the budget.  It runs
    the planar per-field search of vsMotionDetection (spiral lattice of
    maxShift/stepSize steps, halving refinement, range test) and allocates
    nothing: its scratch (per-field running minimum and completion counter,
-   lattice rank tables; at most 4096 fields per call and 32768 lattice
-   points) lives in one static device array of about 320 KB that every GPU
-   loading the library holds until the process exits.
+   lattice rank tables; at most 4096 fields per call, 32768 lattice points
+   and maxShift + stepSize <= 32767) lives in one static device array of
+   311,300 bytes that every GPU loading the library holds until the process
+   exits.
      d_curr, d_prev: blurred planes on the current device, 16-byte aligned,
        row pitch `pitch` a multiple of 16 bytes, readable up to 256 bytes past
        the end of their last row; every field's whole search window must lie
@@ -222,6 +239,19 @@ VS_API void vsb_batch_free(vsb_batch* b);
    VS_OK or VS_ERROR (no file stays open then). */
 VS_API int vsb_batch_open_trf(vsb_batch* b, const char* const* paths, int serialization_mode);
 VS_API int vsb_batch_close_trf(vsb_batch* b);
+/* Limits of the persistent kernel's bounded waits: a search or min/max item
+   that waits for its stream's blur tiles gives up after `spins` polls
+   (100 ns apart) or `cycles` SM clock cycles, whichever comes first; the
+   step then fails with VS_ERROR ("a wait for blur tiles gave up" in
+   vsb_last_error()), the step's frame is dropped for every stream, and the
+   next step starts clean.  Defaults 2^24 polls and 8e9 cycles; a wait only
+   runs out when the device work list is broken. */
+VS_API int vsb_batch_set_wait_limit(vsb_batch* b, unsigned spins, long long cycles);
+/* Fault injection for tests, on the host side: stage A's work list leaves
+   out stream `stream`'s blur tiles (a negative stream restores the full
+   list), so that stream's waits run out and the step fails as above.  No
+   GPU fault is involved: the waits end at their limits. */
+VS_API int vsb_batch_test_withhold_blur(vsb_batch* b, int stream);
 /* persistent-kernel launches so far */
 VS_API long vsb_batch_launch_count(const vsb_batch* b);
 /* the persistent grid: CTAs, threads per CTA, dynamic shared memory per CTA */

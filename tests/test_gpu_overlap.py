@@ -107,3 +107,31 @@ def test_multi_detectors_equal_their_own_runs():
                               for k in range(n)])
         assert np.array_equal(cm[:, s], exp[s][1])
         assert np.array_equal(got, exp[s][0])
+
+
+def test_headline_clip_frame_loops_match_reference():
+    """The benchmark's workload whole: the 300-frame 1920x1080 camera-walk
+    clip (seed 1) through the overlapped frame loop from device and from host
+    frames, and through the per-frame loop (vsb_detect_frames), each equal to
+    the reference's CPU detect of the same clip, every frame, all seven fields
+    (tests/test_determinism.c:356-361 of the reference)."""
+    if not O.ref_available():
+        pytest.skip("reference build not present")
+    w, h, n = 1920, 1080, 300
+    clip = S.clip(w, h, n, seed=1, device="cuda")
+    host = clip.cpu().numpy()
+    exp, ec, _ = O.ref_clip(host, V.PF_YUV420P, threads=8)
+    a = V.MotionDetector(w, h, V.PF_YUV420P)
+    got, gc = _run(a, clip.data_ptr(), n, w, h, True)
+    assert np.array_equal(gc, ec)
+    for k in ("vx", "vy", "fx", "fy", "fsize", "contrast", "match"):
+        assert np.array_equal(got[k], exp[k]), k
+    pinned = torch.from_numpy(host).pin_memory()
+    b = V.MotionDetector(w, h, V.PF_YUV420P)
+    got, gc = _run(b, pinned.data_ptr(), n, w, h, False)
+    assert np.array_equal(gc, ec) and np.array_equal(got, exp.astype(V.LM_DTYPE))
+    c = V.MotionDetector(w, h, V.PF_YUV420P)
+    rec = np.zeros(n * 512 + 64, V.LM_DTYPE)
+    cnt = np.zeros(n, np.int32)
+    tot = c.run_frames(n, pinned.data_ptr(), w * h, w, False, rec, cnt)
+    assert np.array_equal(cnt, ec) and np.array_equal(rec[:tot], exp.astype(V.LM_DTYPE))

@@ -40,6 +40,16 @@ static int write_trf(vsb_batch* b, int s, const LocalMotions* lms) {
   return VS_OK;
 }
 
+int vsb_batch_set_wait_limit(vsb_batch* b, unsigned spins, long long cycles) {
+  if (!b) return VS_ERROR;
+  return vsbd_batch_set_wait_limit(b->dev, spins, cycles) == 0 ? VS_OK : VS_ERROR;
+}
+
+int vsb_batch_test_withhold_blur(vsb_batch* b, int stream) {
+  if (!b) return VS_ERROR;
+  return vsbd_batch_withhold_blur(b->dev, stream) == 0 ? VS_OK : VS_ERROR;
+}
+
 int vsb_batch_close_trf(vsb_batch* b) {
   if (!b) return VS_ERROR;
   int rc = VS_OK;
@@ -166,11 +176,22 @@ int vsb_batch_detect(vsb_batch* b, const uint8_t* const* planes, const int* pitc
   }
   double t3 = vsb_now_s();
   int trf_rc = VS_OK;
+  /* the host parts of every stream first: a failed allocation in one drops
+     the step for all, before any stream's frame ends */
+  int bad = -1;
   for (int s = 0; s < b->n; s++) {
-    if (b->search[s])
-      vsb_frame_host_b(&b->md[s], b->fres[s], &b->w[s], &motions[s]);
-    else
-      vsb_frame_first(&b->md[s], &motions[s]);
+    int rc = b->search[s] ? vsb_frame_host_b(&b->md[s], b->fres[s], &b->w[s], &motions[s])
+                          : vsb_frame_first(&b->md[s], &motions[s]);
+    if (rc != VS_OK) {
+      bad = s;
+      for (int q = 0; q < s; q++) vs_vector_del(&motions[q]);
+      for (int q = s + 1; q < b->n; q++)
+        if (b->search[q]) vsb_frame_discard(&b->w[q]);
+      break;
+    }
+  }
+  if (bad >= 0) return VS_ERROR;
+  for (int s = 0; s < b->n; s++) {
     if (vsb_frame_end(&b->md[s])) vsbd_batch_commit(b->dev, s);
     if (write_trf(b, s, &motions[s]) != VS_OK) trf_rc = VS_ERROR;
   }
@@ -264,8 +285,14 @@ static long run_overlapped(vsb_batch* b, const uint8_t* const* clips, const long
       return -1;
     }
     int trf_rc = VS_OK;
+    for (int s = 0; s < b->n; s++)
+      if (vsb_frame_host_b(&b->md[s], b->fres[s], &b->w[s], &lms[s]) != VS_OK) {
+        for (int q = 0; q < s; q++) vs_vector_del(&lms[q]);
+        for (int q = s + 1; q < b->n; q++) vsb_frame_discard(&b->w[q]);
+        vsbd_batch_drain(b->dev);
+        return -1;
+      }
     for (int s = 0; s < b->n; s++) {
-      vsb_frame_host_b(&b->md[s], b->fres[s], &b->w[s], &lms[s]);
       if (vsb_frame_end(&b->md[s])) vsbd_batch_commit(b->dev, s);
       if (write_trf(b, s, &lms[s]) != VS_OK) trf_rc = VS_ERROR;
     }

@@ -133,14 +133,11 @@ long vsb_detect_clip(int width, int height, int pformat, const uint8_t* frames, 
   return total;
 }
 
-long vsb_detect_run(VSMotionDetect* md, const uint8_t* frames, long frame_bytes, int linesize,
-                    int nframes, int on_device, void* out, long out_cap, int* counts) {
-  if (!md || !frames || nframes < 0) return -1;
-  LocalMotion* rec = (LocalMotion*)out;
+/* frames through the per-frame entry points, one call per frame */
+static long run_per_frame(VSMotionDetect* md, const uint8_t* frames, long frame_bytes,
+                          int linesize, int nframes, int on_device, LocalMotion* rec,
+                          long out_cap, int* counts) {
   long total = 0;
-  if (nframes > 1 && vsb_can_overlap(md))
-    return vsb_detect_run_overlapped(md, frames, frame_bytes, linesize, nframes, on_device, rec,
-                                     out_cap, counts);
   for (int k = 0; k < nframes; k++) {
     LocalMotions lms;
     const uint8_t* src = frames + (size_t)k * frame_bytes;
@@ -170,6 +167,23 @@ long vsb_detect_run(VSMotionDetect* md, const uint8_t* frames, long frame_bytes,
     vs_vector_del(&lms);
   }
   return total;
+}
+
+long vsb_detect_run(VSMotionDetect* md, const uint8_t* frames, long frame_bytes, int linesize,
+                    int nframes, int on_device, void* out, long out_cap, int* counts) {
+  if (!md || !frames || nframes < 0) return -1;
+  if (nframes > 1 && vsb_can_overlap(md))
+    return vsb_detect_run_overlapped(md, frames, frame_bytes, linesize, nframes, on_device,
+                                     (LocalMotion*)out, out_cap, counts);
+  return run_per_frame(md, frames, frame_bytes, linesize, nframes, on_device, (LocalMotion*)out,
+                       out_cap, counts);
+}
+
+long vsb_detect_frames(VSMotionDetect* md, const uint8_t* frames, long frame_bytes, int linesize,
+                       int nframes, int on_device, void* out, long out_cap, int* counts) {
+  if (!md || !frames || nframes < 0) return -1;
+  return run_per_frame(md, frames, frame_bytes, linesize, nframes, on_device, (LocalMotion*)out,
+                       out_cap, counts);
 }
 
 long vsb_detect_multi(VSMotionDetect** mds, int n, const uint8_t* const* clips,
@@ -229,6 +243,10 @@ int vsb_kernel_times(const VSMotionDetect* md, double* ms, long* count) {
 
 int vsb_sad_peak(int variant, double* byteops_per_s) {
   return vsbd_sad_peak(variant, byteops_per_s) == 0 ? VS_OK : VS_ERROR;
+}
+
+long long vsb_test_device_alloc(int fail_after, int sticky) {
+  return vsbd_test_device_alloc(fail_after, sticky);
 }
 
 void vsb_counters(long long* launches, long long* h2d_bytes, long long* d2h_bytes) {

@@ -8,8 +8,9 @@
  *       (speculatively: selection cannot shrink the work below "every field
  *       with enough contrast" at the default accuracy 15, and searching all
  *       saves a host round trip), one copy back;
- *   host: contrasts, field selection with libc qsort and the reference's
- *       comparator (the tie order of qsort decides which fields are kept and
+ *   host: contrasts, field selection with a stable merge sort that gives
+ *       the permutation glibc's qsort gives with the reference's comparator
+ *       (the tie order decides which fields are kept and
  *       the output order), coarse LocalMotions, the simple global model, the
  *       per-field fine offsets;
  *   stage B on the GPU: fine search of the selected fine fields, copy back;
@@ -327,6 +328,14 @@ int vsb_md_init(VSMotionDetect* md, const VSMotionDetectConfig* conf, const VSFr
   }
 
   md_state* st = (md_state*)calloc(1, sizeof(md_state));
+  if (!st) {
+    vs_log_error(md->conf.modName, "malloc failed!\n");
+    vs_free(md->fieldscoarse.fields);
+    vs_free(md->fieldsfine.fields);
+    md->fieldscoarse.fields = NULL;
+    md->fieldsfine.fields = NULL;
+    return VS_ERROR;
+  }
   st->key = md;
   st->planar = md->fi.pFormat < PF_PACKED;
   st->bpp = st->planar ? 1 : md->fi.bytesPerPixel;
@@ -358,6 +367,10 @@ int vsb_md_init(VSMotionDetect* md, const VSMotionDetectConfig* conf, const VSFr
   }
   if (ok) {
     int16_t* xy = (int16_t*)malloc(sizeof(int16_t) * 2 * (size_t)(nc + nf + 1));
+    if (!xy) {
+      ok = 0;
+      nc = nf = 0; /* nothing to fill */
+    }
     for (int i = 0; i < nc; i++) {
       xy[i] = md->fieldscoarse.fields[i].x;
       xy[nc + i] = md->fieldscoarse.fields[i].y;
@@ -367,7 +380,9 @@ int vsb_md_init(VSMotionDetect* md, const VSMotionDetectConfig* conf, const VSFr
       xy[2 * nc + nf + i] = md->fieldsfine.fields[i].y;
     }
     int blur = st->planar ? vsb_blur_size(md->conf.stepSize, md->fi.width, md->fi.height) : 0;
-    if (!with_device) {
+    if (!ok) {
+      /* no memory for the field table */
+    } else if (!with_device) {
       /* the caller runs the device work (batched streams): hand it the layout */
       lay->coarse = gc;
       lay->fine = gf;
@@ -552,6 +567,7 @@ int vsb_frame_host_a(VSMotionDetect* md, const uint8_t* mm, const vsbd_result* c
   md_state* st = state_find(md);
   VSMotionDetectFields* fc = &md->fieldscoarse;
   VSMotionDetectFields* ff = &md->fieldsfine;
+  w->oom0 = vsb_oom_count();
   vs_vector_init(&w->coarse, fc->maxFields);
   vs_vector_init(&w->fine, 0);
   w->fine_pass = 0;
@@ -601,8 +617,8 @@ int vsb_frame_host_a(VSMotionDetect* md, const uint8_t* mm, const vsbd_result* c
   return VS_OK;
 }
 
-void vsb_frame_host_b(VSMotionDetect* md, const vsbd_result* fres, vsb_frame_work* w,
-                      LocalMotions* motions) {
+int vsb_frame_host_b(VSMotionDetect* md, const vsbd_result* fres, vsb_frame_work* w,
+                     LocalMotions* motions) {
   md_state* st = state_find(md);
   VSMotionDetectFields* ff = &md->fieldsfine;
   if (w->fine_pass) {
@@ -624,10 +640,23 @@ void vsb_frame_host_b(VSMotionDetect* md, const vsbd_result* fres, vsb_frame_wor
     vs_array_free(q);
     vs_vector_del(&motions2);
   }
+  if (vsb_oom_count() != w->oom0) {
+    /* an allocation through the host's hooks failed: no partial result */
+    vsb_frame_discard(w);
+    vs_vector_init(motions, 0);
+    vs_log_error(md->conf.modName, "out of memory in frame %i: frame dropped\n", md->frameNum);
+    return VS_ERROR;
+  }
   if (md->conf.show) vsb_draw_motions(md, &w->coarse, &w->fine);
   *motions = vs_vector_concat(&w->coarse, &w->fine);
+  if (vsb_oom_count() != w->oom0) {
+    vsb_frame_discard(w);
+    vs_log_error(md->conf.modName, "out of memory in frame %i: frame dropped\n", md->frameNum);
+    return VS_ERROR;
+  }
   vs_vector_fini(&w->coarse);
   vs_vector_fini(&w->fine);
+  return VS_OK;
 }
 
 void vsb_frame_discard(vsb_frame_work* w) {
@@ -635,9 +664,13 @@ void vsb_frame_discard(vsb_frame_work* w) {
   vs_vector_del(&w->fine);
 }
 
-void vsb_frame_first(VSMotionDetect* md, LocalMotions* motions) {
-  vs_vector_init(motions, 1);
+int vsb_frame_first(VSMotionDetect* md, LocalMotions* motions) {
+  if (vs_vector_init(motions, 1) != VS_OK) {
+    vs_log_error(md->conf.modName, "out of memory in frame %i: frame dropped\n", md->frameNum);
+    return VS_ERROR;
+  }
   md->hasSeenOneFrame = 1;
+  return VS_OK;
 }
 
 int vsb_frame_end(VSMotionDetect* md) {
@@ -705,9 +738,9 @@ int vsb_detect_common(VSMotionDetect* md, LocalMotions* motions, const uint8_t* 
       return VS_ERROR;
     }
     t[3] = now_s();
-    vsb_frame_host_b(md, fres, &w, motions);
-  } else {
-    vsb_frame_first(md, motions);
+    if (vsb_frame_host_b(md, fres, &w, motions) != VS_OK) return VS_ERROR;
+  } else if (vsb_frame_first(md, motions) != VS_OK) {
+    return VS_ERROR;
   }
   if (vsb_frame_end(md)) vsbd_commit_prev(st->dev);
   t[4] = now_s();
@@ -819,7 +852,11 @@ long vsb_detect_run_overlapped(VSMotionDetect* md, const uint8_t* frames, long f
       return -1;
     }
     LocalMotions lms;
-    vsb_frame_host_b(md, fres, &w, &lms);
+    if (vsb_frame_host_b(md, fres, &w, &lms) != VS_OK) {
+      /* frame k+1's stage A may still be in flight: let it finish */
+      if (next) vsbd_stage_a_next_collect(st->dev, &mm, &cres);
+      return -1;
+    }
     if (vsb_frame_end(md)) vsbd_commit_prev(st->dev);
     total = append_records(&lms, rec, total, out_cap, counts ? counts + k : NULL);
     if (next && vsbd_stage_a_next_collect(st->dev, &mm, &cres) != 0) {
@@ -877,10 +914,14 @@ long vsb_detect_multi_impl(VSMotionDetect** mds, int n, const uint8_t* const* cl
       if (search[s]) {
         const vsbd_result* fres = NULL;
         if (vsbd_stage_b_collect(st[s]->dev, &fres) != 0) goto done;
-        vsb_frame_host_b(mds[s], fres, &w[s], &lms);
         ok[s] = 0;
-      } else {
-        vsb_frame_first(mds[s], &lms);
+        if (vsb_frame_host_b(mds[s], fres, &w[s], &lms) != VS_OK) {
+          for (int q = s + 1; q < n; q++)
+            if (search[q]) vsbd_stage_b_collect(st[q]->dev, &fres);
+          goto done;
+        }
+      } else if (vsb_frame_first(mds[s], &lms) != VS_OK) {
+        goto done;
       }
       if (vsb_frame_end(mds[s])) vsbd_commit_prev(st[s]->dev);
       total = append_records(&lms, rec, total, out_cap, counts ? counts + (size_t)k * n + s : NULL);

@@ -10,6 +10,7 @@
 #include <stdlib.h>
 
 #include "vidstab_b200.h"
+#include "vsb_host.h"
 
 #ifndef M_PI
 #define M_PI 3.14159265358979323846
@@ -33,6 +34,10 @@ VSTransform vsSimpleMotionsToTransform(VSFrameInfo fi, const char* modName,
   int num_motions = vs_vector_size(motions);
   if (num_motions < 1) return t;
   double* angles = (double*)vs_malloc(sizeof(double) * num_motions);
+  if (!angles) { /* counted as a failed allocation: the frame is dropped */
+    vsb_note_oom();
+    return t;
+  }
   LocalMotion meanmotion;
   int i;
 

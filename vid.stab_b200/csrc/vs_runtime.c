@@ -49,3 +49,10 @@ int VS_ERROR = -1;
 int VS_OK = 0;
 
 int vs_log_level = 4;
+
+/* allocation failures through the hooks above, counted per thread: the
+   detect path compares the count before and after a frame's host work and
+   fails the frame (VS_ERROR) when it moved, whatever helper met the failure */
+static __thread int g_oom;
+void vsb_note_oom(void) { g_oom++; }
+int vsb_oom_count(void) { return g_oom; }

@@ -14,6 +14,7 @@
 #include <string.h>
 
 #include "vidstab_b200.h"
+#include "vsb_host.h"
 
 #ifndef M_PI
 #define M_PI 3.14159265358979323846
@@ -165,6 +166,10 @@ LocalMotion null_localmotion(void) {
 int* localmotions_getx(const LocalMotions* lms) {
   int n = vs_vector_size(lms);
   int* xs = (int*)vs_malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+  if (!xs) {
+    vsb_note_oom();
+    return NULL;
+  }
   for (int i = 0; i < n; i++) xs[i] = LMGet(lms, i)->v.x;
   return xs;
 }
@@ -172,6 +177,10 @@ int* localmotions_getx(const LocalMotions* lms) {
 int* localmotions_gety(const LocalMotions* lms) {
   int n = vs_vector_size(lms);
   int* ys = (int*)vs_malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+  if (!ys) {
+    vsb_note_oom();
+    return NULL;
+  }
   for (int i = 0; i < n; i++) ys[i] = LMGet(lms, i)->v.y;
   return ys;
 }
@@ -191,6 +200,11 @@ LocalMotion cleanmean_localmotions(const LocalMotions* lms) {
   int* xs = localmotions_getx(lms);
   int* ys = localmotions_gety(lms);
   LocalMotion m = null_localmotion();
+  if (!xs || !ys) { /* counted as a failed allocation: the frame is dropped */
+    if (xs) vs_free(xs);
+    if (ys) vs_free(ys);
+    return m;
+  }
   m.v.x = 0;
   m.v.y = 0;
   qsort(xs, len, sizeof(int), cmp_int);

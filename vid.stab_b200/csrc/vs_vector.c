@@ -7,11 +7,13 @@
 #include <string.h>
 
 #include "vidstab_b200.h"
+#include "vsb_host.h"
 
 static int grow_to(VSVector* V, int newsize) {
   if (newsize < 1) newsize = 1;
   void** d = (void**)vs_realloc(V->data, (size_t)newsize * sizeof(void*));
   if (!d) {
+    vsb_note_oom();
     vs_log_error("VS_Vector", "out of memory!");
     return VS_ERROR;
   }
@@ -24,7 +26,11 @@ static int grow_to(VSVector* V, int newsize) {
 int vs_vector_init(VSVector* V, int buffersize) {
   if (buffersize > 0) {
     V->data = (void**)vs_zalloc(sizeof(void*) * (size_t)buffersize);
-    if (!V->data) return VS_ERROR;
+    if (!V->data) {
+      vsb_note_oom();
+      V->buffersize = V->nelems = 0;
+      return VS_ERROR;
+    }
   } else {
     V->data = 0;
     buffersize = 0;
@@ -69,7 +75,10 @@ int vs_vector_append(VSVector* V, void* data) {
 
 int vs_vector_append_dup(VSVector* V, void* data, int data_size) {
   void* d = vs_malloc((size_t)data_size);
-  if (!d) return VS_ERROR;
+  if (!d) {
+    vsb_note_oom();
+    return VS_ERROR;
+  }
   memcpy(d, data, (size_t)data_size);
   if (vs_vector_append(V, d) != VS_OK) {
     vs_free(d);
@@ -108,7 +117,10 @@ int vs_vector_set(VSVector* V, int pos, void* data, void** old) {
 int vs_vector_set_dup(VSVector* V, int pos, void* data, int data_size, void** old) {
   if (old) *old = 0;
   void* d = vs_malloc((size_t)data_size);
-  if (!d) return VS_ERROR;
+  if (!d) {
+    vsb_note_oom();
+    return VS_ERROR;
+  }
   memcpy(d, data, (size_t)data_size);
   int rc = vs_vector_set(V, pos, d, old);
   if (rc != VS_OK) vs_free(d);
@@ -125,7 +137,7 @@ VSVector vs_vector_filter(const VSVector* V, short (*pred)(void*, void*), void* 
 
 VSVector vs_vector_concat(const VSVector* V1, const VSVector* V2) {
   VSVector r;
-  vs_vector_init(&r, V1->nelems + V2->nelems);
+  if (vs_vector_init(&r, V1->nelems + V2->nelems) != VS_OK) return r; /* empty, no data */
   if (V1->nelems) memcpy(r.data, V1->data, sizeof(void*) * (size_t)V1->nelems);
   if (V2->nelems) memcpy(r.data + V1->nelems, V2->data, sizeof(void*) * (size_t)V2->nelems);
   r.nelems = V1->nelems + V2->nelems;
@@ -135,7 +147,8 @@ VSVector vs_vector_concat(const VSVector* V1, const VSVector* V2) {
 VSArray vs_array_new(int len) {
   VSArray a;
   a.dat = (double*)vs_zalloc(sizeof(double) * (size_t)(len > 0 ? len : 1));
-  a.len = len;
+  a.len = a.dat ? len : 0;
+  if (!a.dat) vsb_note_oom();
   return a;
 }
 

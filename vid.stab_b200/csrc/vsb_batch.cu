@@ -72,13 +72,19 @@ struct BWork {
   int type, stream, a, pad;
 };
 
+/* default limits of the bounded waits: polls (100 ns apart) and SM clock
+   cycles, about 1.7 s and 4 s on a B200 */
+#define VSB_WAIT_SPINS (1u << 24)
+#define VSB_WAIT_CYCLES 8000000000ll
+
 /* control block of one stage */
 struct BCtl {
   unsigned head;
   unsigned err;
   unsigned blur_done[VSB_BATCH_MAX_STREAMS];
-  int nwork; /* set by the host; not cleared per launch */
-  int pad;
+  int nwork; /* set by the host; not cleared per launch (nor are the fields below) */
+  unsigned spin_limit;    /* a wait gives up after this many polls ... */
+  long long cycle_limit;  /* ... or this many SM clock cycles */
 };
 
 /* Bounded wait of one CTA until stream s has `target` blur tiles written.
@@ -87,10 +93,12 @@ __device__ __forceinline__ int wait_blur(BCtl* ctl, int s, unsigned target) {
   __shared__ int s_ok;
   if (threadIdx.x == 0) {
     const long long t0 = clock64();
+    const unsigned spin_limit = ctl->spin_limit;
+    const long long cycle_limit = ctl->cycle_limit;
     unsigned spins = 0;
     int ok = 1;
     while (*(volatile unsigned*)&ctl->blur_done[s] < target) {
-      if (++spins > (1u << 24) || clock64() - t0 > 8000000000ll) {
+      if (++spins > spin_limit || clock64() - t0 > cycle_limit) {
         ok = 0;
         atomicExch(&ctl->err, 1u);
         break;
@@ -285,7 +293,21 @@ struct vsbd_batch {
   int b_pending;      /* a stage B was issued and not collected */
   long launches;
   long steps;
+  unsigned wait_spins;  /* limits of the bounded waits (BCtl) */
+  long long wait_cycles;
+  int withheld;         /* stream whose blur items stage A's list leaves out (test hook; -1) */
 };
+
+/* a control block as the host uploads it: zero counters, the work count and
+   the wait limits */
+static BCtl ctl_init(const vsbd_batch* b, int nwork) {
+  BCtl h;
+  memset(&h, 0, sizeof(h));
+  h.nwork = nwork;
+  h.spin_limit = b->wait_spins;
+  h.cycle_limit = b->wait_cycles;
+  return h;
+}
 
 #define BCK(call)                             \
   do {                                        \
@@ -519,8 +541,7 @@ static int autotune_class(vsbd_batch* b, int c, int is_fine) {
     int ok = 1;
     for (int rep = 0; rep < 4 && ok; rep++) {
       /* the tuning list has no blur items: mark every stream's blur done */
-      BCtl h;
-      memset(&h, 0, sizeof(h));
+      BCtl h = ctl_init(b, 0);
       for (int s = 0; s < b->n; s++)
         h.blur_done[s] = (unsigned)(b->h_streams[s].ntx * b->h_streams[s].nty);
       h.nwork = nw;
@@ -765,8 +786,14 @@ extern "C" int vsbd_batch_create(vsbd_batch** out, int n, const vsbd_batch_strea
   CKB(cudaMallocHost(&b->h_resB, sizeof(vsbd_result) * (size_t)(nf_total + 1)));
   CKB(cudaMalloc(&b->d_ctlA, sizeof(BCtl)));
   CKB(cudaMalloc(&b->d_ctlB, sizeof(BCtl)));
-  CKB(cudaMemset(b->d_ctlA, 0, sizeof(BCtl)));
-  CKB(cudaMemset(b->d_ctlB, 0, sizeof(BCtl)));
+  b->wait_spins = VSB_WAIT_SPINS;
+  b->wait_cycles = VSB_WAIT_CYCLES;
+  b->withheld = -1;
+  {
+    BCtl h = ctl_init(b, 0);
+    CKB(cudaMemcpy(b->d_ctlA, &h, sizeof(h), cudaMemcpyHostToDevice));
+    CKB(cudaMemcpy(b->d_ctlB, &h, sizeof(h), cudaMemcpyHostToDevice));
+  }
   CKB(cudaMalloc(&b->d_pre, sizeof(int) * (2 * (size_t)n + 2)));
   CKB(cudaMallocHost(&b->h_pre, sizeof(int) * (2 * (size_t)n + 2)));
   CKB(cudaMalloc(&b->d_fitems, sizeof(vsbd_item) * (size_t)(nf_total + 1)));
@@ -855,9 +882,7 @@ extern "C" int vsbd_batch_create(vsbd_batch** out, int n, const vsbd_batch_strea
   free(w);
   CKB(e);
   {
-    BCtl h;
-    memset(&h, 0, sizeof(h));
-    h.nwork = b->nworkA;
+    BCtl h = ctl_init(b, b->nworkA);
     CKB(cudaMemcpy(b->d_ctlA, &h, sizeof(h), cudaMemcpyHostToDevice));
   }
   CKB(cudaStreamSynchronize(b->st));
@@ -936,6 +961,50 @@ extern "C" int vsbd_batch_stage_a_collect(vsbd_batch* b) {
     cudaMemset(b->d_tickets, 0, sizeof(unsigned) * (b->nkeys + 1));
     return -1;
   }
+  return 0;
+}
+
+extern "C" int vsbd_batch_set_wait_limit(vsbd_batch* b, unsigned spins, long long cycles) {
+  BCK(cudaSetDevice(b->dev));
+  if (spins < 1 || cycles < 1) {
+    vsbp_set_msg("wait limits must be positive");
+    return -1;
+  }
+  BCK(cudaStreamSynchronize(b->st));
+  BCK(cudaStreamSynchronize(b->st2));
+  b->wait_spins = spins;
+  b->wait_cycles = cycles;
+  BCtl h = ctl_init(b, 0);
+  const size_t off = offsetof(BCtl, spin_limit);
+  BCK(cudaMemcpy((uint8_t*)b->d_ctlA + off, (uint8_t*)&h + off, sizeof(BCtl) - off,
+                 cudaMemcpyHostToDevice));
+  BCK(cudaMemcpy((uint8_t*)b->d_ctlB + off, (uint8_t*)&h + off, sizeof(BCtl) - off,
+                 cudaMemcpyHostToDevice));
+  return 0;
+}
+
+/* Stage A's work list without stream s's blur items (s < 0: the full list):
+   the captured graphs read the list and its length from device memory, so
+   they run the new list as they are. */
+extern "C" int vsbd_batch_withhold_blur(vsbd_batch* b, int stream) {
+  BCK(cudaSetDevice(b->dev));
+  if (stream >= b->n) {
+    vsbp_set_msg("no such stream");
+    return -1;
+  }
+  BCK(cudaStreamSynchronize(b->st));
+  BCK(cudaStreamSynchronize(b->st2));
+  BWork* w = NULL;
+  int nw = 0;
+  if (build_workA(b, &w, &nw, -1, 0) != 0) return -1;
+  int k = 0;
+  for (int i = 0; i < nw; i++)
+    if (stream < 0 || !(w[i].type == 0 && w[i].stream == stream)) w[k++] = w[i];
+  cudaError_t e = cudaMemcpy(b->d_workA, w, sizeof(BWork) * (size_t)k, cudaMemcpyHostToDevice);
+  free(w);
+  BCK(e);
+  BCK(cudaMemcpy(&b->d_ctlA->nwork, &k, sizeof(int), cudaMemcpyHostToDevice));
+  b->withheld = stream;
   return 0;
 }
 

@@ -61,6 +61,12 @@ void vsbd_batch_drain(vsbd_batch* b);
 int vsbd_batch_stage_b_issue(vsbd_batch* b, const vsbd_item* const* items, const int* nitems);
 int vsbd_batch_stage_b_collect(vsbd_batch* b, const vsbd_result** fres);
 
+/* limits of the persistent kernel's bounded waits (polls, SM clock cycles) */
+int vsbd_batch_set_wait_limit(vsbd_batch* b, unsigned spins, long long cycles);
+/* test hook: stage A's work list leaves out stream s's blur items (s < 0:
+   the full list again), so that stream's waits run out */
+int vsbd_batch_withhold_blur(vsbd_batch* b, int stream);
+
 long vsbd_batch_launches(const vsbd_batch* b);
 /* persistent grid: CTAs, threads per CTA, dynamic shared memory per CTA */
 int vsbd_batch_grid(const vsbd_batch* b, int* ctas, int* threads, long* smem);

@@ -16,6 +16,7 @@
  *               (src/motiondetect.c:439-586 planar, :591-660 packed).
  */
 #include <cuda_runtime.h>
+#include <pthread.h>
 #include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -26,6 +27,7 @@
 #include "vsb_pnet.h"
 #include "vsb_prefilter.cuh"
 #include "vsb_search.cuh"
+#include "vsb_sweep.cuh"
 
 /* ------------------------------------------------------------------------ */
 /* error plumbing                                                            */
@@ -51,6 +53,29 @@ extern "C" void vsbd_counters(long long* launches, long long* h2d, long long* d2
 }
 
 extern "C" const char* vsbd_error(void) { return g_err; }
+
+/* device allocations: counted, and the one `g_alloc_fail` calls from now
+   fails (and, sticky, every later one) -- a test hook for the out-of-memory
+   paths; (cudaMalloc) names the runtime's function, not the counting macro */
+static long long g_alloc_calls = 0;
+static int g_alloc_fail = -1, g_alloc_sticky = 0;
+extern "C" cudaError_t vsbd_dev_malloc(void** p, size_t bytes) {
+  __atomic_fetch_add(&g_alloc_calls, 1ll, __ATOMIC_RELAXED);
+  int k = __atomic_load_n(&g_alloc_fail, __ATOMIC_RELAXED);
+  if (k == 0) {
+    if (!g_alloc_sticky) __atomic_store_n(&g_alloc_fail, -1, __ATOMIC_RELAXED);
+    *p = NULL;
+    return cudaErrorMemoryAllocation;
+  }
+  if (k > 0) __atomic_store_n(&g_alloc_fail, k - 1, __ATOMIC_RELAXED);
+  return (cudaMalloc)(p, bytes);
+}
+
+extern "C" long long vsbd_test_device_alloc(int fail_after, int sticky) {
+  g_alloc_sticky = sticky;
+  __atomic_store_n(&g_alloc_fail, fail_after < 0 ? -1 : fail_after, __ATOMIC_RELAXED);
+  return __atomic_load_n(&g_alloc_calls, __ATOMIC_RELAXED);
+}
 
 #define CK(call)                                 \
   do {                                           \
@@ -326,37 +351,49 @@ __global__ void __launch_bounds__(256) k_minmax_planar(const uint8_t* __restrict
 /* ------------------------------------------------------------------------ */
 
 
+#define VSB_MAX_DEVICES 64
+
+static int current_device(void) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  return dev >= 0 && dev < VSB_MAX_DEVICES ? dev : 0;
+}
+
+/* SMs of the current device (kept per device; a benign race fills an entry
+   with the same value twice at worst) */
 static int sm_count(void) {
-  static int n = 0;
-  if (!n) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-    if (n <= 0) n = 148;
+  static int n[VSB_MAX_DEVICES];
+  const int dev = current_device();
+  int v = __atomic_load_n(&n[dev], __ATOMIC_RELAXED);
+  if (!v) {
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+    if (v <= 0) v = 148;
+    __atomic_store_n(&n[dev], v, __ATOMIC_RELAXED);
   }
-  return n;
+  return v;
 }
 
 /* raises a kernel's dynamic shared-memory limit only when a launch needs
    more than this device already allows it (the attribute call costs
    microseconds of host time per launch otherwise); slot names the kernel */
 static cudaError_t ensure_smem(const void* fn, int slot, size_t smem) {
-  static size_t done[16][32];
+  static size_t done[16][64];
   int dev = 0;
   cudaGetDevice(&dev);
-  if (dev >= 0 && dev < 16 && slot >= 0 && slot < 32 && done[dev][slot] >= smem) return cudaSuccess;
+  if (dev >= 0 && dev < 16 && slot >= 0 && slot < 64 && done[dev][slot] >= smem) return cudaSuccess;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e == cudaSuccess && dev >= 0 && dev < 16 && slot >= 0 && slot < 32) done[dev][slot] = smem;
+  if (e == cudaSuccess && dev >= 0 && dev < 16 && slot >= 0 && slot < 64) done[dev][slot] = smem;
   return e;
 }
 
 /* largest dynamic shared memory one search CTA may request on this device
    (the kernels' static shared memory counts against the opt-in limit) */
 static size_t search_smem_limit(void) {
-  static size_t lim = 0;
+  static size_t lims[VSB_MAX_DEVICES];
+  const int dev = current_device();
+  size_t lim = __atomic_load_n(&lims[dev], __ATOMIC_RELAXED);
   if (!lim) {
-    int dev = 0, optin = 0;
-    cudaGetDevice(&dev);
+    int optin = 0;
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     size_t stat = 0;
     cudaFuncAttributes fa;
@@ -366,6 +403,7 @@ static size_t search_smem_limit(void) {
     if (cudaFuncGetAttributes(&fa, k_lattice<8>) == cudaSuccess && fa.sharedSizeBytes > stat)
       stat = fa.sharedSizeBytes;
     lim = optin > 0 ? (size_t)optin - stat - 64 : 48 * 1024;
+    __atomic_store_n(&lims[dev], lim, __ATOMIC_RELAXED);
   }
   return lim;
 }
@@ -605,6 +643,136 @@ static int launch_search(const GeomDev& gd, const uint8_t* curr, const uint8_t* 
   return -1;
 }
 
+/* ---- the persistent TMA-staged sweep (vsb_sweep.cuh) ---- */
+
+/* the (step, field size) pairs the sweep is compiled for: the defaults'
+   coarse fields (step 6; 48 to 112 pixels, 360p to 1080p) and fine fields
+   (step 2; 16 to 48 pixels, 360p to 4K) */
+#define VSB_SWEEP_CASES(X) \
+  X(6, 3) X(6, 4) X(6, 5) X(6, 7) X(2, 1) X(2, 2) X(2, 3)
+
+static bool sweep_supported(const DGeom& g) {
+  if (g.bpp != 1 || g.has_origin || g.rows > 0 || g.S % 16) return false;
+  const int NQ = g.S / 16;
+#define VSB_SW_SUP(ST, NQv) if (g.step == ST && NQ == NQv) return true;
+  VSB_SWEEP_CASES(VSB_SW_SUP)
+#undef VSB_SW_SUP
+  return false;
+}
+
+/* registers per thread of a sweep instantiation (0 if not compiled) */
+static int sweep_regs(int step, int NQ) {
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaErrorInvalidValue;
+#define VSB_SW_REG(ST, NQv) \
+  if (step == ST && NQ == NQv) e = cudaFuncGetAttributes(&fa, k_sweep<NQv, ST>);
+  VSB_SWEEP_CASES(VSB_SW_REG)
+#undef VSB_SW_REG
+  return e == cudaSuccess ? fa.numRegs : 0;
+}
+
+/* Candidate sweep plans, best first by a cost model: lattice-column groups
+   (the whole width, or the width split in two or three), lattice rows per
+   tile and field strips; the persistent grid holds as many CTAs as fit on
+   the GPU at once. */
+static int sweep_candidates(const DGeom& g, int nitems, TileCand* out, int cap) {
+  if (!sweep_supported(g) || nitems < 1) return 0;
+  const size_t lim = search_smem_limit();
+  const int sms = sm_count();
+  const int regs = sweep_regs(g.step, g.S / 16);
+  if (regs <= 0) return 0;
+  int n = 0, ncg_prev = -1;
+  for (int split = 1; split <= 3; split++) {
+    const int ncg = ((g.na + split - 1) / split + SW_TA - 1) / SW_TA;
+    if (ncg == ncg_prev) continue;
+    ncg_prev = ncg;
+    for (int nbb = 1; nbb <= 24 && nbb <= g.nb; nbb++)
+      for (int ns = 1; ns <= 16; ns *= 2) {
+        if (g.S % ns || g.S / ns < 2) continue;
+        const int ntask = ncg * nbb * ns;
+        const int threads = (ntask + 31) & ~31;
+        if (threads > SW_MAX_THREADS || threads < 64) continue;
+        DGeom t = g;
+        t.ta = 5;
+        t.tb = 1;
+        t.nab = ncg * SW_TA;
+        t.nbb = nbb;
+        t.nta = (g.na + t.nab - 1) / t.nab;
+        t.ntb = (g.nb + nbb - 1) / nbb;
+        t.nstrip = ns;
+        t.threads = threads;
+        const SweepLayout L = sweep_layout(t);
+        if (L.total > lim) continue;
+        int cps = (int)((228 * 1024) / (L.total + 2048));
+        if (2048 / threads < cps) cps = 2048 / threads;
+        if (65536 / (threads * regs) < cps) cps = 65536 / (threads * regs);
+        if (cps < 1) continue;
+        if (cps > 4) cps = 4;
+        const long T = (long)nitems * t.nta * t.ntb;
+        t.ctas = (int)(T < (long)sms * cps ? T : (long)sms * cps);
+        const long per_cta = (T + t.ctas - 1) / t.ctas;
+        /* a tile's lane-SAD slots (padded columns and rows included), the
+           per-row loads of each thread, and a fixed cost per tile */
+        const int Rs = g.S / ns;
+        const double work = (double)t.nab * nbb * g.S * (g.S / 4) +
+                            (double)ntask * Rs * (sw_chunks(g.step, g.S / 16) + 2 * (g.S / 16) + 12);
+        const double warps = (double)cps * threads / 32.0;
+        const double occ = warps >= 12 ? 1.0 : warps / 12.0;
+        const double clk = (double)per_cta * (work / (64.0 / cps) / occ + 2500.0);
+        int pos = n < cap ? n : cap;
+        while (pos > 0 && out[pos - 1].clk > clk) {
+          if (pos < cap) out[pos] = out[pos - 1];
+          pos--;
+        }
+        if (pos < cap) {
+          out[pos].clk = clk;
+          out[pos].g = t;
+          if (n < cap) n++;
+        }
+      }
+  }
+  return n;
+}
+
+template <int NQ, int STEP>
+static int launch_sweep_t(const DGeom& g, size_t smem, int slot, const uint8_t* curr,
+                          const uint8_t* prev, int pitch, const vsbd_item* d_items, int n,
+                          unsigned long long* keys, unsigned* tickets, vsbd_result* d_res,
+                          unsigned* err, cudaStream_t st) {
+  cudaError_t e = ensure_smem((const void*)k_sweep<NQ, STEP>, slot, smem);
+  if (e != cudaSuccess) {
+    set_err("cudaFuncSetAttribute(k_sweep)", e);
+    return -1;
+  }
+  k_sweep<NQ, STEP><<<g.ctas, g.threads, smem, st>>>(curr, prev, pitch, g, d_items, n, keys,
+                                                     tickets, d_res, err);
+  return 1;
+}
+
+/* the sweep of items[0 .. n) with plan g (ta == 5); err: a device-visible
+   word the kernel raises when a wait for its copies runs out */
+static int launch_sweep(const DGeom& g, const uint8_t* curr, const uint8_t* prev, int pitch,
+                        const vsbd_item* d_items, int n, unsigned long long* keys,
+                        unsigned* tickets, vsbd_result* d_res, unsigned* err, cudaStream_t st) {
+  if (n <= 0) return 0;
+  if ((pitch & 15) || ((uintptr_t)prev & 15) || ((uintptr_t)curr & 15)) {
+    set_msg("the sweep needs 16-byte aligned planes and pitch");
+    return -1;
+  }
+  const size_t smem = sweep_layout(g).total;
+  const int NQ = g.S / 16;
+  int slot = 40;
+#define VSB_SW_LAUNCH(ST, NQv)                                                                  \
+  if (g.step == ST && NQ == NQv)                                                                \
+    return launch_sweep_t<NQv, ST>(g, smem, slot, curr, prev, pitch, d_items, n, keys, tickets, \
+                                   d_res, err, st);                                             \
+  slot++;
+  VSB_SWEEP_CASES(VSB_SW_LAUNCH)
+#undef VSB_SW_LAUNCH
+  set_msg("no sweep compiled for this field geometry");
+  return -1;
+}
+
 /* full search of the items in list[0 .. *count), at most n of them:
    persistent CTAs, as many as fit on the GPU at once */
 template <int TB, int TA>
@@ -718,21 +886,33 @@ static int launch_pruned(const GeomDev& gd, const GeomDev& gp, const uint8_t* cu
    work whatever the pixels hold, so the contents of the buffers do not matter.
    Results are cached per (geometry, item count) for the process. */
 struct TuneEntry {
-  int S, bpp, step, na, nb, nstages, nitems, rows;
+  int dev, S, bpp, step, na, nb, nstages, nitems, rows;
   DGeom g;
 };
+/* the cache, and the tuning itself, are serialised by g_tune_lock:
+   detectors may be created from several host threads at once, and timings
+   taken concurrently on one GPU would mislead each other */
 static TuneEntry g_tune[64];
 static int g_ntune = 0;
+static pthread_mutex_t g_tune_lock = PTHREAD_MUTEX_INITIALIZER;
+
+struct TuneLock {
+  TuneLock() { pthread_mutex_lock(&g_tune_lock); }
+  ~TuneLock() { pthread_mutex_unlock(&g_tune_lock); }
+};
 
 static int autotune_tiling(GeomDev* gd, const uint8_t* curr, const uint8_t* prev, int pitch,
                            const vsbd_item* d_items, int n, unsigned long long* keys,
                            unsigned* tickets, vsbd_result* d_res, cudaStream_t st,
                            unsigned* emit_buf = NULL) {
   if (n <= 0 || getenv("VSB_NO_AUTOTUNE")) return 0;
+  TuneLock lock;
+  const int dev = current_device();
   DGeom& g = gd->g;
   for (int i = 0; i < g_ntune; i++) {
     TuneEntry& e = g_tune[i];
-    if (e.S == g.S && e.bpp == g.bpp && e.step == g.step && e.na == g.na && e.nb == g.nb &&
+    if (e.dev == dev && e.S == g.S && e.bpp == g.bpp && e.step == g.step && e.na == g.na &&
+        e.nb == g.nb &&
         e.nstages == g.nstages && e.nitems == n && e.rows == g.rows) {
       DGeom t = e.g;
       t.order = g.order;
@@ -812,8 +992,114 @@ static int autotune_tiling(GeomDev* gd, const uint8_t* curr, const uint8_t* prev
   gd->smem = tile_layout(g).total;
   if (g_ntune < 64) {
     TuneEntry& e = g_tune[g_ntune++];
+    e.dev = dev;
     e.S = g.S; e.bpp = g.bpp; e.step = g.step; e.na = g.na; e.nb = g.nb;
     e.nstages = g.nstages; e.nitems = n; e.rows = g.rows; e.g = g;
+  }
+  return 0;
+}
+
+/* Whether the persistent sweep beats the tuned per-tile search for a field
+   set: the tuned tiling and the sweep's best modelled plans are timed on the
+   detector's own buffers and items (the dense search does the same work
+   whatever the pixels hold) and the faster is kept; cached per geometry,
+   item count and device for the process.  *on = 1 with *plan the sweep's
+   plan, else 0.  err: the sweep's error word (device-visible). */
+struct SweepTune {
+  int dev, S, step, na, nb, nstages, nitems, on;
+  DGeom g;
+};
+static SweepTune g_swtune[64];
+static int g_nswtune = 0;
+
+static int autotune_sweep(const GeomDev& gd, const uint8_t* curr, const uint8_t* prev, int pitch,
+                          const vsbd_item* d_items, int n, unsigned long long* keys,
+                          unsigned* tickets, vsbd_result* d_res, unsigned* err,
+                          volatile unsigned* h_err, cudaStream_t st, DGeom* plan, int* on) {
+  *on = 0;
+  if (n <= 0 || !sweep_supported(gd.g) || getenv("VSB_NO_SWEEP") || getenv("VSB_NO_AUTOTUNE"))
+    return 0;
+  /* VSB_FORCE_SWEEP: the sweep's best plan whatever the timings say (tests) */
+  const bool force = getenv("VSB_FORCE_SWEEP") != NULL;
+  TuneLock lock;
+  const int dev = current_device();
+  const DGeom& g = gd.g;
+  for (int i = 0; !force && i < g_nswtune; i++) {
+    const SweepTune& e = g_swtune[i];
+    if (e.dev == dev && e.S == g.S && e.step == g.step && e.na == g.na && e.nb == g.nb &&
+        e.nstages == g.nstages && e.nitems == n) {
+      *on = e.on;
+      *plan = e.g;
+      plan->order = g.order;
+      plan->point = g.point;
+      return 0;
+    }
+  }
+  TileCand cand[12];
+  const int nc = sweep_candidates(g, n, cand, 10);
+  if (nc > 0) {
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    auto time_of = [&](const DGeom* sw, int reps) -> float {
+      auto one = [&]() {
+        return sw ? launch_sweep(*sw, curr, prev, pitch, d_items, n, keys, tickets, d_res, err, st)
+                  : launch_search(gd, curr, prev, pitch, d_items, n, keys, tickets, d_res, st);
+      };
+      if (one() < 0) return -1.f;
+      cudaEventRecord(e0, st);
+      for (int r = 0; r < reps; r++) one();
+      cudaEventRecord(e1, st);
+      if (cudaEventSynchronize(e1) != cudaSuccess) return -1.f;
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      return ms / reps;
+    };
+    for (int w = 0; w < 3; w++) time_of(NULL, 3); /* clocks up */
+    float lat_ms = time_of(NULL, 5);
+    float ms_of[12];
+    for (int k = 0; k < nc; k++) ms_of[k] = time_of(&cand[k].g, 3);
+    int top[3] = { -1, -1, -1 };
+    for (int k = 0; k < nc; k++) {
+      if (ms_of[k] < 0.f) continue;
+      for (int p = 0; p < 3; p++)
+        if (top[p] < 0 || ms_of[k] < ms_of[top[p]]) {
+          for (int q = 2; q > p; q--) top[q] = top[q - 1];
+          top[p] = k;
+          break;
+        }
+    }
+    float best_ms = 1e30f;
+    int best = -1;
+    for (int round = 0; round < 2; round++) {
+      const float lm = time_of(NULL, 5);
+      if (lm >= 0.f && lm < lat_ms) lat_ms = lm;
+      for (int p = 0; p < 3; p++) {
+        if (top[p] < 0) continue;
+        const float ms = time_of(&cand[top[p]].g, 5);
+        if (ms >= 0.f && ms < best_ms) {
+          best_ms = ms;
+          best = top[p];
+        }
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    CK(cudaGetLastError());
+    if (*h_err) {
+      *h_err = 0;
+      set_msg("the search sweep's staging did not complete while tuning");
+      return -1;
+    }
+    if (best >= 0 && lat_ms >= 0.f && (force || best_ms < lat_ms)) {
+      *on = 1;
+      *plan = cand[best].g;
+    }
+  }
+  if (!force && g_nswtune < 64) {
+    SweepTune& e = g_swtune[g_nswtune++];
+    e.dev = dev; e.S = g.S; e.step = g.step; e.na = g.na; e.nb = g.nb;
+    e.nstages = g.nstages; e.nitems = n; e.on = *on; e.g = *plan;
   }
   return 0;
 }
@@ -873,6 +1159,13 @@ struct vsbd_ctx {
   double thr_coarse;  /* contrast threshold of the coarse fields */
   int16_t* d_xy;      /* coarse x | coarse y | fine x | fine y */
   GeomDev gc, gf;
+  /* the persistent sweep, where it beats the per-tile search (autotuned):
+     plans of the coarse and the fine fields, on flags, and the error words
+     its bounded waits raise ([0] coarse, [1] fine; mapped pinned memory) */
+  DGeom swc, swf;
+  int sw_c, sw_f;
+  unsigned* h_swerr;
+  unsigned* d_swerr;
   vsbd_item* d_citems;
   vsbd_item* d_fitems;
   unsigned long long* d_keys;   /* coarse nc, then fine nf */
@@ -1016,6 +1309,7 @@ extern "C" void vsbd_destroy(vsbd_ctx* c) {
   if (c->h_outs[0]) cudaFreeHost(c->h_outs[0]);
   if (c->h_outs[1]) cudaFreeHost(c->h_outs[1]);
   if (c->h_items) cudaFreeHost(c->h_items);
+  if (c->h_swerr) cudaFreeHost(c->h_swerr);
   cudaFree(c->d_pn);
   cudaFree(c->d_pout);
   cudaFree(c->d_fbl);
@@ -1159,6 +1453,18 @@ extern "C" int vsbd_create(vsbd_ctx** out, int W, int H, int bpp, int blur_size,
                       NULL, c->st, c->d_part) != 0 ||
       autotune_tiling(&c->gfp, c->d_buf[0], c->d_buf[1], c->pitch, c->d_fitems, nf, NULL, NULL,
                       NULL, c->st, c->d_part) != 0) {
+    vsbd_destroy(c);
+    return -1;
+  }
+  CKC(cudaHostAlloc(&c->h_swerr, 2 * sizeof(unsigned), cudaHostAllocMapped));
+  c->h_swerr[0] = c->h_swerr[1] = 0;
+  CKC(cudaHostGetDevicePointer((void**)&c->d_swerr, c->h_swerr, 0));
+  if (autotune_sweep(c->gc, c->d_buf[0], c->d_buf[1], c->pitch, c->d_citems, nc, c->d_keys,
+                     c->d_tickets, (vsbd_result*)(c->d_out + c->off_coarse), c->d_swerr,
+                     c->h_swerr, c->st, &c->swc, &c->sw_c) != 0 ||
+      autotune_sweep(c->gf, c->d_buf[0], c->d_buf[1], c->pitch, c->d_fitems, nf,
+                     c->d_keys + nc, c->d_tickets + nc, (vsbd_result*)(c->d_out + c->off_fine),
+                     c->d_swerr + 1, c->h_swerr + 1, c->st, &c->swf, &c->sw_f) != 0) {
     vsbd_destroy(c);
     return -1;
   }
@@ -1339,6 +1645,8 @@ static int stage_a_issue(vsbd_ctx* c, const uint8_t* host, int linesize, const u
       int nl = c->mode ? launch_pruned(c->gc, c->gcp, cur, prv, c->pitch, c->d_citems, c->nc,
                                        c->d_skip, c->d_part, c->d_counts, c->d_lists, c->d_boxes,
                                        c->d_keys, c->d_tickets, cres, st)
+               : c->sw_c ? launch_sweep(c->swc, cur, prv, c->pitch, c->d_citems, c->nc, c->d_keys,
+                                        c->d_tickets, cres, c->d_swerr, st)
                        : launch_search(c->gc, cur, prv, c->pitch, c->d_citems, c->nc, c->d_keys,
                                        c->d_tickets, cres, st);
       if (nl < 0) return -1;
@@ -1358,9 +1666,23 @@ static int stage_a_issue(vsbd_ctx* c, const uint8_t* host, int linesize, const u
   return 0;
 }
 
+/* a sweep whose bounded wait ran out left its fields' keys and counters
+   mid-way: report, and start them afresh */
+static int sweep_failed(vsbd_ctx* c, int k) {
+  if (!c->h_swerr || !((volatile unsigned*)c->h_swerr)[k]) return 0;
+  cudaStreamSynchronize(c->st);
+  cudaStreamSynchronize(c->st2);
+  c->h_swerr[k] = 0;
+  cudaMemset(c->d_keys, 0xff, sizeof(unsigned long long) * (c->nc + c->nf + 2));
+  cudaMemset(c->d_tickets, 0, sizeof(unsigned) * (c->nc + c->nf + 2));
+  set_msg(k ? "fine search: a wait for staged rows gave up" : "coarse search: a wait for staged rows gave up");
+  return 1;
+}
+
 static int stage_a_collect(vsbd_ctx* c, const uint8_t** minmax, const vsbd_result** coarse) {
   CK(cudaEventSynchronize(c->ev_a));
   kt_collect(c);
+  if (sweep_failed(c, 0)) return -1;
   if (c->a_search && c->pn_on)
     proposal_tally(c, c->h_out + c->off_cfb, (const vsbd_result*)(c->h_out + c->off_coarse),
                    c->h_vres, c->nc, 0);
@@ -1458,6 +1780,8 @@ extern "C" int vsbd_stage_b_issue(vsbd_ctx* c, const vsbd_item* items, int n) {
                                      c->d_part, c->d_counts + c->nc, c->d_lists,
                                      c->d_boxes + 4 * c->nc, c->d_keys + c->nc,
                                      c->d_tickets + c->nc, fres, st)
+             : c->sw_f ? launch_sweep(c->swf, cur, prv, c->pitch, c->d_fitems, n, c->d_keys + c->nc,
+                                      c->d_tickets + c->nc, fres, c->d_swerr + 1, st)
                      : launch_search(c->gf, cur, prv, c->pitch, c->d_fitems, n, c->d_keys + c->nc,
                                      c->d_tickets + c->nc, fres, st);
     if (nl < 0) return -1;
@@ -1484,6 +1808,7 @@ extern "C" int vsbd_stage_b_collect(vsbd_ctx* c, const vsbd_result** fine) {
   if (c->b_n <= 0) return 0;
   CK(cudaEventSynchronize(c->ev_b));
   kt_collect(c);
+  if (sweep_failed(c, 1)) return -1;
   if (c->pn_on)
     proposal_tally(c, h + c->off_ffb, (const vsbd_result*)(h + c->off_fine),
                    c->h_vres ? c->h_vres + c->nc : NULL, c->b_n, 1);
@@ -1514,15 +1839,16 @@ extern "C" long vsbd_launches(const vsbd_ctx* c) { return c ? c->launches : 0; }
 
 extern "C" int vsbd_search_tiling(const vsbd_ctx* c, int fine, int* desc) {
   if (!c || !desc) return -1;
-  const DGeom& g = fine ? c->gf.g : c->gc.g;
+  const int sw = fine ? c->sw_f : c->sw_c;
+  const DGeom& g = sw ? (fine ? c->swf : c->swc) : (fine ? c->gf.g : c->gc.g);
   desc[0] = g.tb;
   desc[1] = g.ta > 0 ? g.ta : 1;
   desc[2] = g.nab;
   desc[3] = g.nbb;
   desc[4] = g.nstrip;
   desc[5] = g.threads;
-  desc[6] = (int)(fine ? c->gf.smem : c->gc.smem);
-  desc[7] = g.nta * g.ntb;
+  desc[6] = (int)(sw ? sweep_layout(g).total : (fine ? c->gf.smem : c->gc.smem));
+  desc[7] = sw ? g.ctas : g.nta * g.ntb;
   return 0;
 }
 
@@ -1729,7 +2055,23 @@ extern "C" int vsbd_search_host(const uint8_t* curr, const uint8_t* prev, int W,
   memset(&gd, 0, sizeof(gd));
   int rc = -1;
   cudaError_t e;
-  if (geom_upload(geom, n, tiles_hint, &gd) != 0) goto done;
+  /* tiles_hint < 0: the sweep, with the plan of that rank in its candidate
+     list (-1 the model's best) */
+  DGeom swg;
+  unsigned* d_err = NULL;
+  unsigned h_err = 0;
+  if (geom_upload(geom, n, tiles_hint > 0 ? tiles_hint : 0, &gd) != 0) goto done;
+  if (tiles_hint < 0) {
+    TileCand cand[12];
+    const int nc = sweep_candidates(gd.g, n, cand, 12);
+    if (-tiles_hint > nc) {
+      set_msg("no sweep plan of that rank for this field geometry");
+      goto done;
+    }
+    swg = cand[-tiles_hint - 1].g;
+    if ((e = cudaMalloc(&d_err, sizeof(unsigned))) != cudaSuccess) { set_err("cudaMalloc", e); goto done; }
+    cudaMemset(d_err, 0, sizeof(unsigned));
+  }
   if ((e = cudaMalloc(&d_c, plane)) != cudaSuccess) { set_err("cudaMalloc", e); goto done; }
   if ((e = cudaMalloc(&d_p, plane)) != cudaSuccess) { set_err("cudaMalloc", e); goto done; }
   if ((e = cudaMalloc(&d_items, sizeof(vsbd_item) * (n + 1))) != cudaSuccess) { set_err("cudaMalloc", e); goto done; }
@@ -1741,7 +2083,13 @@ extern "C" int vsbd_search_host(const uint8_t* curr, const uint8_t* prev, int W,
   cudaMemcpy2D(d_c, pitch, curr, (size_t)W * bpp, (size_t)W * bpp, H, cudaMemcpyHostToDevice);
   cudaMemcpy2D(d_p, pitch, prev, (size_t)W * bpp, (size_t)W * bpp, H, cudaMemcpyHostToDevice);
   cudaMemcpy(d_items, items, sizeof(vsbd_item) * n, cudaMemcpyHostToDevice);
-  if (launch_search(gd, d_c, d_p, pitch, d_items, n, d_keys, d_tk, d_res, 0) < 0) goto done;
+  if (tiles_hint < 0) {
+    if (launch_sweep(swg, d_c, d_p, pitch, d_items, n, d_keys, d_tk, d_res, d_err, 0) < 0) goto done;
+    if ((e = cudaMemcpy(&h_err, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost)) != cudaSuccess) { set_err("k_sweep", e); goto done; }
+    if (h_err) { set_msg("search sweep: a wait for staged rows gave up"); goto done; }
+  } else if (launch_search(gd, d_c, d_p, pitch, d_items, n, d_keys, d_tk, d_res, 0) < 0) {
+    goto done;
+  }
   if ((e = cudaGetLastError()) != cudaSuccess) { set_err("k_search", e); goto done; }
   if ((e = cudaMemcpy(out, d_res, sizeof(vsbd_result) * n, cudaMemcpyDeviceToHost)) != cudaSuccess) { set_err("download", e); goto done; }
   rc = 0;
@@ -1753,6 +2101,7 @@ done:
   cudaFree(d_res);
   cudaFree(d_keys);
   cudaFree(d_tk);
+  cudaFree(d_err);
   return rc;
 }
 

@@ -182,6 +182,10 @@ int vsbd_sad_peak(int variant, double* byteops_per_s);
    bytes of the per-frame path */
 void vsbd_counters(long long* launches, long long* h2d, long long* d2h);
 
+/* device allocations made so far; fail_after >= 0 makes the allocation that
+   many calls later fail (sticky: that one and all later ones), -1 disarms */
+long long vsbd_test_device_alloc(int fail_after, int sticky);
+
 /* Message of the last failure on this thread. */
 const char* vsbd_error(void);
 void vsbd_set_error(const char* msg);

@@ -11,6 +11,11 @@
 extern "C" {
 #endif
 
+/* a failed allocation through vs_malloc / vs_zalloc / vs_realloc (counted
+   per thread), and the count so far */
+void vsb_note_oom(void);
+int vsb_oom_count(void);
+
 /* effective box size of the luma prefilter for a requested size
    (src/boxblur.c:109-122); < 2 means no blur */
 int vsb_blur_size(int requested, int width, int height);
@@ -55,7 +60,9 @@ void vsb_md_layout_free(vsb_md_layout* lay);
                           model and the fine work list (w->items[0..nitems),
                           valid until the next frame of this detector)
      [stage B, when w->fine_pass: fine search of the work list]
-     vsb_frame_host_b     fine motions, mean-match filter, show, result
+     vsb_frame_host_b     fine motions, mean-match filter, show, result;
+                          VS_ERROR (nothing returned, the frame to be
+                          dropped) if an allocation failed in either part
      vsb_frame_end        frame count; returns 1 if the current blurred
                           frame becomes the previous one */
 typedef struct {
@@ -63,14 +70,15 @@ typedef struct {
   int fine_pass;
   int nitems;
   const vsbd_item* items;
+  int oom0; /* vsb_oom_count() when the frame's host work began */
 } vsb_frame_work;
 int vsb_frame_begin(VSMotionDetect* md, int* search);
 int vsb_frame_host_a(VSMotionDetect* md, const uint8_t* mm, const vsbd_result* cres,
                      vsb_frame_work* w);
-void vsb_frame_host_b(VSMotionDetect* md, const vsbd_result* fres, vsb_frame_work* w,
-                      LocalMotions* motions);
+int vsb_frame_host_b(VSMotionDetect* md, const vsbd_result* fres, vsb_frame_work* w,
+                     LocalMotions* motions);
 void vsb_frame_discard(vsb_frame_work* w);
-void vsb_frame_first(VSMotionDetect* md, LocalMotions* motions);
+int vsb_frame_first(VSMotionDetect* md, LocalMotions* motions);
 int vsb_frame_end(VSMotionDetect* md);
 
 /* whether vsb_detect_run_overlapped may serve this detector (no tripod,

@@ -3,10 +3,10 @@
  * allocate GPU memory.
  *
  * Some hosts own every byte of device memory themselves: a decoder or
- * encoder pipeline that hands out frames from a fixed pool, a process that
- * runs under a memory budget enforced by its own allocator, or code running
- * while a CUDA graph is being built, where allocating is not allowed.  They
- * cannot let a library call cudaMalloc behind their back.  This entry point
+ * encoder pipeline that hands out frames from a fixed pool, or a process
+ * that runs under a memory budget enforced by its own allocator.  A
+ * cudaMalloc behind their back would break the pool's accounting or the
+ * budget, so they cannot let a library allocate.  This entry point
  * runs the same search kernel as vsMotionDetection's planar path, but all of
  * its scratch memory (per-field running minimum and completion counter, the
  * lattice's visiting-rank tables) lives in one statically sized array that
@@ -23,7 +23,9 @@
 #include "vsb_search.cuh"
 
 /* sizes of the static scratch: up to VSB_NOALLOC_MAX_ITEMS fields per call and
-   lattices of up to VSB_NOALLOC_MAX_LATTICE points (e.g. maxShift/step <= 90) */
+   lattices of up to VSB_NOALLOC_MAX_LATTICE points (e.g. maxShift/step <= 90).
+   In bytes: keys 8 x 4096 + counters 4 x 4096 + rank table 4 x 32768 +
+   displacement table 4 x 32769 = 311,300 (304 KiB) */
 #define VSB_NOALLOC_MAX_ITEMS 4096
 #define VSB_NOALLOC_MAX_LATTICE 32768
 #define VSB_NOALLOC_OFF_KEYS 0
@@ -130,6 +132,13 @@ extern "C" int vsbd_search_noalloc(const uint8_t* d_curr, const uint8_t* d_prev,
              "invalid input: size %d (multiple of 16 needed), maxShift %d, step %d, pitch %d "
              "(multiple of 16 needed), planes 16-byte aligned",
              size, maxShift, stepSize, pitch);
+    return fail(msg, cudaSuccess);
+  }
+  if (maxShift + stepSize > 32767) {
+    char msg[160];
+    snprintf(msg, sizeof(msg),
+             "maxShift %d + step %d: shifts must stay within 16 bits (sum at most 32767)",
+             maxShift, stepSize);
     return fail(msg, cudaSuccess);
   }
   const int K = maxShift / stepSize;

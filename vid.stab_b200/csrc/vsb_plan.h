@@ -35,10 +35,22 @@ int vsbp_tile_candidates(const DGeom& g, int nitems, int max_threads, TileCand* 
 /* the same, with ta lattice columns per thread only (1 or 2) */
 int vsbp_tile_candidates_ta(const DGeom& g, int nitems, int max_threads, TileCand* out, int cap,
                             int ta);
+/* SMs of the current device */
 int vsbp_sm_count(void);
 void vsbp_set_err(const char* what, cudaError_t e);
 void vsbp_set_msg(const char* m);
 /* process-wide counters of the per-frame path */
 void vsbp_count(long launches, size_t h2d, size_t d2h);
+
+/* Every device allocation of the library's CUDA units that include this
+   header goes through vsbd_dev_malloc, which counts them and can be told to
+   fail one (vsb_test_device_alloc): the library's handling of an
+   out-of-memory GPU is then testable without exhausting a GPU. */
+extern "C" cudaError_t vsbd_dev_malloc(void** p, size_t bytes);
+template <class T>
+static inline cudaError_t vsbp_cuda_malloc(T** p, size_t bytes) {
+  return vsbd_dev_malloc((void**)p, bytes);
+}
+#define cudaMalloc(p, bytes) vsbp_cuda_malloc((p), (bytes))
 
 #endif

@@ -53,6 +53,7 @@ struct DGeom {
                            by two bytes (edge bytes masked) */
   int rows;             /* field rows a launch sums (0: all S); fewer rows give
                            every candidate a lower bound of its SAD */
+  int ctas;             /* ta == 5 (the persistent sweep, vsb_sweep.cuh): its grid */
   unsigned* emit;       /* emit mode: per item, per lattice point, the sum */
   const uint8_t* skip;  /* emit mode: per item, nonzero = field never used */
 };
@@ -130,12 +131,13 @@ __host__ __device__ inline TileLayout tile_layout(const DGeom& g) {
   return L;
 }
 
-/* SAD of the staged field C (rowW words per row) against rows of a
-   row-major byte buffer whose matching field starts at byte column bx
-   (any alignment) of row row0; lanes take field rows, the warp sums */
-__device__ __forceinline__ unsigned sad_rows_warp(const uint32_t* __restrict__ C, int rowW, int S,
-                                                  const uint8_t* __restrict__ base, size_t pitch,
-                                                  int bx, int row0, int lane) {
+/* SAD of the staged field C (rowW words per row, cpw words apart) against
+   rows of a row-major byte buffer whose matching field starts at byte
+   column bx (any alignment) of row row0; lanes take field rows, the warp
+   sums */
+__device__ __forceinline__ unsigned sad_rows_warp(const uint32_t* __restrict__ C, int rowW, int cpw,
+                                                  int S, const uint8_t* __restrict__ base,
+                                                  size_t pitch, int bx, int row0, int lane) {
   /* lanes stride over the field's words in raster order (consecutive lanes
      read consecutive words: coalesced in global memory, conflict-free in
      shared memory); four words in flight per lane */
@@ -152,7 +154,7 @@ __device__ __forceinline__ unsigned sad_rows_warp(const uint32_t* __restrict__ C
       const uint32_t* Pw = (const uint32_t*)(b0 + (size_t)r * pitch) + w;
       lo[u] = Pw[0];
       hi[u] = Pw[1];
-      cw[u] = C[i + 32 * u];
+      cw[u] = C[r * cpw + w];
       w += 32;
       while (w >= rowW) { w -= rowW; r++; }
     }
@@ -161,7 +163,7 @@ __device__ __forceinline__ unsigned sad_rows_warp(const uint32_t* __restrict__ C
   }
   for (; i < total; i += 32) {
     const uint32_t* Pw = (const uint32_t*)(b0 + (size_t)r * pitch) + w;
-    acc = sad4(C[i], __funnelshift_r(Pw[0], Pw[1], sh), acc);
+    acc = sad4(C[r * cpw + w], __funnelshift_r(Pw[0], Pw[1], sh), acc);
     w += 32;
     while (w >= rowW) { w -= rowW; r++; }
   }
@@ -171,11 +173,13 @@ __device__ __forceinline__ unsigned sad_rows_warp(const uint32_t* __restrict__ C
 /* Last CTA of an item: origin candidate (raster scans), refinement rounds
    (i outer, j inner, centre skipped, strict <), range test, reset.  The
    window the rounds can reach (the field plus the sum of the round radii on
-   every side) is staged in shared memory first. */
-static __device__ void refine_and_store(const DGeom& g, const TileLayout& L, const vsbd_item& it,
-                                 const uint32_t* C, uint8_t* rwin, const uint8_t* __restrict__ prev,
-                                 int pitch, unsigned long long* keys, unsigned* tickets,
-                                 vsbd_result* res, int item, unsigned* qsad) {
+   every side, RH rows of RP bytes) is staged in shared memory (rwin) first.
+   C: the field, rowW words per row, cpw words apart. */
+static __device__ void refine_and_store(const DGeom& g, int rowW, int cpw, int RH, int RP,
+                                        const vsbd_item& it, const uint32_t* C, uint8_t* rwin,
+                                        const uint8_t* __restrict__ prev, int pitch,
+                                        unsigned long long* keys, unsigned* tickets,
+                                        vsbd_result* res, int item, unsigned* qsad) {
   __shared__ int s_tx, s_ty;
   __shared__ unsigned s_min;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
@@ -190,7 +194,7 @@ static __device__ void refine_and_store(const DGeom& g, const TileLayout& L, con
   const int fx0 = (it.x - g.S / 2 + it.ox) * g.bpp, fy0 = it.y - g.S / 2 + it.oy;
   if (g.has_origin) {
     if (warp == 0) {
-      unsigned s0 = sad_rows_warp(C, L.rowW, g.S, prev, (size_t)pitch, fx0, fy0, lane);
+      unsigned s0 = sad_rows_warp(C, rowW, cpw, g.S, prev, (size_t)pitch, fx0, fy0, lane);
       if (lane == 0 && s0 <= s_min) { /* rank 0 precedes every lattice rank */
         s_min = s0;
         s_tx = 0;
@@ -204,8 +208,8 @@ static __device__ void refine_and_store(const DGeom& g, const TileLayout& L, con
     const int cx0 = s_tx, cy0 = s_ty;
     const int wx = fx0 + (cx0 - R) * g.bpp, wy = fy0 + cy0 - R;
     const int wxa = wx & ~3, off = wx - wxa;
-    const int nw = L.RP >> 2;
-    for (int i = threadIdx.x; i < L.RH * nw; i += blockDim.x) {
+    const int nw = RP >> 2;
+    for (int i = threadIdx.x; i < RH * nw; i += blockDim.x) {
       int r = i / nw, w = i - r * nw;
       ((uint32_t*)rwin)[i] = *((const uint32_t*)(prev + (size_t)(wy + r) * pitch + wxa) + w);
     }
@@ -218,7 +222,7 @@ static __device__ void refine_and_store(const DGeom& g, const TileLayout& L, con
         int i = cx - r + (q / side) * h, j = cy - r + (q % side) * h;
         unsigned sd = 0xffffffffu;
         if (!(i == cx && j == cy))
-          sd = sad_rows_warp(C, L.rowW, g.S, rwin, (size_t)L.RP, off + (i - cx0 + R) * g.bpp,
+          sd = sad_rows_warp(C, rowW, cpw, g.S, rwin, (size_t)RP, off + (i - cx0 + R) * g.bpp,
                              j - cy0 + R, lane);
         if (lane == 0) qsad[q] = sd;
       }
@@ -720,7 +724,8 @@ __device__ __forceinline__ void lattice_tile(const uint8_t* __restrict__ curr,
   __syncthreads();
   if (!s_last) return;
   __threadfence();
-  refine_and_store(g, L, it, C, P + 16, prev, pitch, keys, tickets, res, item, qsad);
+  refine_and_store(g, L.rowW, L.rowW, L.RH, L.RP, it, C, P + 16, prev, pitch, keys, tickets, res,
+                   item, qsad);
 }
 
 /* lattice_tile for two columns per thread, TB rows of a row group and a
@@ -959,7 +964,8 @@ __device__ void lattice_tile_ta2(const uint8_t* __restrict__ curr, const uint8_t
   __syncthreads();
   if (!s_last) return;
   __threadfence();
-  refine_and_store(g, L, it, C, P + 16, prev, pitch, keys, tickets, res, item, qsad);
+  refine_and_store(g, L.rowW, L.rowW, L.RH, L.RP, it, C, P + 16, prev, pitch, keys, tickets, res,
+                   item, qsad);
 }
 
 /* grid (nta*ntb, items); block g.threads; dynamic smem tile_layout(g).total;
@@ -1067,7 +1073,7 @@ static __global__ void __launch_bounds__(256) k_prune(const uint8_t* __restrict_
   for (int k = warp; k < topk; k += nwarps) {
     int c = chosen[k];
     int a = c % g.na, b = c / g.na;
-    unsigned sd = sad_rows_warp(C, rowW, g.S, prev, (size_t)pitch,
+    unsigned sd = sad_rows_warp(C, rowW, rowW, g.S, prev, (size_t)pitch,
                                 fx0 + (g.ax0 + a * g.step) * g.bpp, fy0 + g.by0 + b * g.step, lane);
     if (lane == 0) atomicMin(&s_best, ((unsigned long long)sd << 32) | (unsigned)g.order[c]);
   }
@@ -1173,10 +1179,10 @@ static __global__ void __launch_bounds__(256) k_survive(const uint8_t* __restric
       int a = c % g.na, b = c / g.na;
       unsigned sd;
       if (in_smem)
-        sd = sad_rows_warp(C + rows0 * L.rowW, L.rowW, rowsR, win, (size_t)WPs,
+        sd = sad_rows_warp(C + rows0 * L.rowW, L.rowW, L.rowW, rowsR, win, (size_t)WPs,
                            we + (a - amin) * g.step * g.bpp, (b - bmin) * g.step, lane);
       else
-        sd = sad_rows_warp(C + rows0 * L.rowW, L.rowW, rowsR, prev, (size_t)pitch,
+        sd = sad_rows_warp(C + rows0 * L.rowW, L.rowW, L.rowW, rowsR, prev, (size_t)pitch,
                            fx0 + (g.ax0 + a * g.step) * g.bpp, fy0 + g.by0 + b * g.step + rows0,
                            lane);
       if (lane == 0)
@@ -1216,7 +1222,8 @@ static __global__ void __launch_bounds__(256) k_survive(const uint8_t* __restric
   }
   uint8_t* rwin = sm + (size_t)g.S * L.rowB;
   unsigned* qsad = (unsigned*)(rwin + (size_t)L.RH * L.RP + 32);
-  refine_and_store(g, L, it, C, rwin + 16, prev, pitch, keys, tickets, res, item, qsad);
+  refine_and_store(g, L.rowW, L.rowW, L.RH, L.RP, it, C, rwin + 16, prev, pitch, keys, tickets,
+                   res, item, qsad);
 }
 
 /* shared memory of k_survive: field, refinement window, refinement SADs */

@@ -118,6 +118,9 @@ def lib():
                                   C.c_char_p, p, C.c_long, p, p, p]
     L.vsb_detect_run.restype = C.c_long
     L.vsb_detect_run.argtypes = [C.POINTER(VSMotionDetect), p, C.c_long, i, i, i, p, C.c_long, p]
+    L.vsb_detect_frames.restype = C.c_long
+    L.vsb_detect_frames.argtypes = [C.POINTER(VSMotionDetect), p, C.c_long, i, i, i, p, C.c_long,
+                                    p]
     L.vsb_batch_create.restype = p
     L.vsb_batch_create.argtypes = [i, p, p, i, p]
     L.vsb_batch_detect.restype = i
@@ -136,6 +139,10 @@ def lib():
     L.vsb_batch_open_trf.argtypes = [p, p, i]
     L.vsb_batch_close_trf.restype = i
     L.vsb_batch_close_trf.argtypes = [p]
+    L.vsb_batch_set_wait_limit.argtypes = [p, C.c_uint, C.c_longlong]
+    L.vsb_batch_test_withhold_blur.argtypes = [p, i]
+    L.vsb_test_device_alloc.restype = C.c_longlong
+    L.vsb_test_device_alloc.argtypes = [i, i]
     L.vsb_boxblur_host.restype = i
     L.vsb_boxblur_host.argtypes = [p, p, i, i, i]
     L.vsb_field_minmax_host.restype = i

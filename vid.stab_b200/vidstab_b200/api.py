@@ -76,6 +76,18 @@ class MotionDetector:
             raise RuntimeError("vsb_detect_run failed: %s" % self.L.vsb_last_error().decode())
         return total
 
+    def run_frames(self, n, frames_ptr, frame_bytes, linesize, on_device, out, counts):
+        """As run, one vsMotionDetection call per frame with no overlap
+        between frames (vsb_detect_frames): a host filter's call sequence."""
+        if len(out) * out.itemsize < 32 or len(counts) < n:
+            raise ValueError("output buffers too small")
+        total = self.L.vsb_detect_frames(C.byref(self.md), C.c_void_p(frames_ptr), frame_bytes,
+                                         linesize, n, 1 if on_device else 0, ptr(out), len(out),
+                                         ptr(counts))
+        if total < 0:
+            raise RuntimeError("vsb_detect_frames failed: %s" % self.L.vsb_last_error().decode())
+        return total
+
     @property
     def frame_num(self):
         return self.md.frameNum
