@@ -52,6 +52,11 @@ VS_API void vsb_set_default_search_mode(int pruned);
    shared memory bytes per CTA, CTAs per field. */
 VS_API int vsb_search_tiling(const struct _vsmotiondetect* md, int fine, int* desc);
 
+/* The prefilter tile the detector picked by timing at init: desc[0] width,
+   desc[1] height (output pixels per CTA), desc[2] its time per frame in ns
+   (0 when it was not timed). */
+VS_API int vsb_blur_tiling(const struct _vsmotiondetect* md, int* desc);
+
 /* Kernel launches issued for this detector so far. */
 VS_API long vsb_launch_count(const struct _vsmotiondetect* md);
 
@@ -152,6 +157,11 @@ VS_API int vsb_sad_peak(int variant, double* byteops_per_s);
 /* luma prefilter of one W x H plane (tight rows) with box size `size`
    (already clamped; < 2 copies) */
 VS_API int vsb_boxblur_host(uint8_t* dst, const uint8_t* src, int width, int height, int size);
+/* the same with vector-blur tile shape `shape` (0: 256x32, 1: 128x16,
+   2: 128x32, 3: 64x32; shapes 1-3 serve box sizes up to 17, larger boxes
+   take shape 0) */
+VS_API int vsb_boxblur_host_tile(uint8_t* dst, const uint8_t* src, int width, int height,
+                                 int size, int shape);
 
 /* per-field, per-channel 8-bit (min,max) of an interleaved image with bpp
    bytes per pixel: out[(i*channels+c)*2 + {0,1}] */

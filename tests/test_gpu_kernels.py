@@ -44,6 +44,18 @@ def test_blur_geometry_sweep():
     assert n > 300
 
 
+@pytest.mark.parametrize("shape", [0, 1, 2, 3])
+def test_blur_tile_shapes(shape):
+    """every tile shape the blur autotuner picks from, frame sizes that leave
+    ragged edge tiles and box sizes 3 to 17, against the oracle"""
+    rng = np.random.default_rng(shape)
+    for w, h in [(1920, 1080), (640, 360), (333, 201), (96, 70), (1280, 720)]:
+        src = rng.integers(0, 256, size=(h, w), dtype=np.uint8)
+        for size in (3, 5, 7, 9, 13, 17):
+            got = V.boxblur_tile(src, size, shape)
+            assert np.array_equal(got, orc_blur(src, size)), (w, h, size)
+
+
 @pytest.mark.parametrize("w,h,step", [(1920, 1080, 6), (640, 480, 6), (3840, 2160, 6),
                                       (1280, 720, 14), (333, 201, 3)])
 def test_blur_frame(w, h, step):

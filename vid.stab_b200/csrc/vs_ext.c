@@ -197,6 +197,15 @@ int vsb_boxblur_host(uint8_t* dst, const uint8_t* src, int width, int height, in
   return vsbd_blur_host(dst, src, width, height, size) == 0 ? VS_OK : VS_ERROR;
 }
 
+int vsb_boxblur_host_tile(uint8_t* dst, const uint8_t* src, int width, int height, int size,
+                          int shape) {
+  return vsbd_blur_host_shape(dst, src, width, height, size, shape) == 0 ? VS_OK : VS_ERROR;
+}
+
+int vsb_blur_tiling(const VSMotionDetect* md, int* desc) {
+  return vsbd_blur_tiling(vsb_md_device(md), desc) == 0 ? VS_OK : VS_ERROR;
+}
+
 int vsb_field_minmax_host(const uint8_t* img, int width, int height, int bpp, int channels,
                           const int16_t* x, const int16_t* y, int n, int size, uint8_t* out) {
   return vsbd_minmax_host(img, width, height, bpp, channels, x, y, n, size, out) == 0 ? VS_OK

@@ -15,6 +15,7 @@
  *               dependent refinement rounds and the range test
  *               (src/motiondetect.c:439-586 planar, :591-660 packed).
  */
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 #include <pthread.h>
 #include <stdint.h>
@@ -129,8 +130,9 @@ __global__ void k_blur_cols(const uint8_t* __restrict__ src, int sp, uint8_t* __
 }
 
 /* Planar prefilter with vector memory access: one CTA of 256 threads
-   blurs a BF_H x BF_W output tile, for a window half-width HALF known at
-   compile time.  Input rows (clamped to the frame) are staged with 16-byte
+   blurs a BH x BW output tile (BW a multiple of 64 up to 256, BH a multiple
+   of 1024/BW), for a window half-width HALF known at compile time; the
+   tile shape is picked per detector by timing (autotune_blur).  Input rows (clamped to the frame) are staged with 16-byte
    loads from 16 bytes left of the tile to 16 bytes right of it (tiles
    touching the left or right frame edge load bytewise with clamped
    columns).  The horizontal pass gives each task a run of 16 outputs of one
@@ -139,14 +141,14 @@ __global__ void k_blur_cols(const uint8_t* __restrict__ src, int sp, uint8_t* __
    vertical pass runs 4-column sliding sums down a quarter of the tile and
    stores words.  Same arithmetic as blur_tile (window sums, floor division
    by the size). */
-#define BF_W 256
-#define BF_H 32
 #define BF_MAXHALF 16
-#define BF_RAWP (BF_W + 32)
-template <int HALF>
+template <int HALF, int BF_W = 256, int BF_H = 32>
 __global__ void __launch_bounds__(256) k_blur_fast(const uint8_t* __restrict__ src, int sp,
                                                    uint8_t* __restrict__ dst, int dp, int W, int H,
                                                    BlurDiv dv) {
+  constexpr int BF_RAWP = BF_W + 32;
+  constexpr int PARTS = 1024 / BF_W; /* vertical pass: threads per column group */
+  static_assert(BF_W % 64 == 0 && BF_W <= 256 && BF_H % PARTS == 0, "blur tile shape");
   __shared__ __align__(16) uint8_t raw[(BF_H + 2 * HALF) * BF_RAWP];
   __shared__ __align__(16) uint8_t hor[(BF_H + 2 * HALF) * BF_W];
   constexpr int ROWS = BF_H + 2 * HALF, WIN = 2 * HALF + 1;
@@ -192,11 +194,11 @@ __global__ void __launch_bounds__(256) k_blur_fast(const uint8_t* __restrict__ s
     *(uint4*)(hor + r * BF_W + c0) = make_uint4(o[0], o[1], o[2], o[3]);
   }
   __syncthreads();
-  /* thread: 4 columns (cg), a quarter of the tile rows */
-  const int cg = threadIdx.x & 63, part = threadIdx.x >> 6;
+  /* thread: 4 columns (cg), a part of the tile rows */
+  const int cg = threadIdx.x % (BF_W / 4), part = threadIdx.x / (BF_W / 4);
   const int gx = x0 + cg * 4;
   if (gx >= W) return;
-  const int rb = part * (BF_H / 4);
+  const int rb = part * (BF_H / PARTS);
   unsigned a0 = 0, a1 = 0, a2 = 0, a3 = 0;
 #pragma unroll
   for (int k = 0; k < WIN; k++) {
@@ -208,7 +210,7 @@ __global__ void __launch_bounds__(256) k_blur_fast(const uint8_t* __restrict__ s
   }
   const bool full4 = gx + 4 <= W;
 #pragma unroll
-  for (int r = rb; r < rb + BF_H / 4; r++) {
+  for (int r = rb; r < rb + BF_H / PARTS; r++) {
     if (r > rb) {
       const unsigned wi = *(const unsigned*)(hor + (r + WIN - 1) * BF_W + cg * 4);
       const unsigned wo = *(const unsigned*)(hor + (r - 1) * BF_W + cg * 4);
@@ -230,30 +232,56 @@ __global__ void __launch_bounds__(256) k_blur_fast(const uint8_t* __restrict__ s
   }
 }
 
-/* k_blur_fast for the window half-width of the plane (1..BF_MAXHALF) */
-static void launch_blur_fast(dim3 grid, cudaStream_t st, const uint8_t* src, int sp, uint8_t* dst,
+/* tile shapes (width, height) of the vector blur; shape 0 serves every
+   half-width, the others half-widths up to 8 (box sizes up to 17) */
+#define VSB_BLUR_SHAPES 4
+static const int g_blur_shape[VSB_BLUR_SHAPES][2] = { { 256, 32 }, { 128, 16 }, { 128, 32 },
+                                                      { 64, 32 } };
+
+static int blur_shape_ok(int shape, int half) {
+  if (shape == 0) return half >= 1 && half <= BF_MAXHALF;
+  return shape > 0 && shape < VSB_BLUR_SHAPES && half >= 1 && half <= 8;
+}
+
+/* k_blur_fast for the window half-width of the plane and a tile shape */
+static void launch_blur_fast(int shape, cudaStream_t st, const uint8_t* src, int sp, uint8_t* dst,
                              int dp, int W, int H, int half, BlurDiv dv) {
-#define VSB_BLURH(K) \
-  case K: k_blur_fast<K><<<grid, 256, 0, st>>>(src, sp, dst, dp, W, H, dv); break;
-  switch (half) {
-    VSB_BLURH(1) VSB_BLURH(2) VSB_BLURH(3) VSB_BLURH(4) VSB_BLURH(5) VSB_BLURH(6)
-    VSB_BLURH(7) VSB_BLURH(8) VSB_BLURH(9) VSB_BLURH(10) VSB_BLURH(11) VSB_BLURH(12)
-    VSB_BLURH(13) VSB_BLURH(14) VSB_BLURH(15) VSB_BLURH(16)
-    default: break;
+  const dim3 grid((W + g_blur_shape[shape][0] - 1) / g_blur_shape[shape][0],
+                  (H + g_blur_shape[shape][1] - 1) / g_blur_shape[shape][1]);
+#define VSB_BLURH(K, BW, BH) \
+  case K: k_blur_fast<K, BW, BH><<<grid, 256, 0, st>>>(src, sp, dst, dp, W, H, dv); break;
+#define VSB_BLUR8(BW, BH) \
+  VSB_BLURH(1, BW, BH) VSB_BLURH(2, BW, BH) VSB_BLURH(3, BW, BH) VSB_BLURH(4, BW, BH) \
+  VSB_BLURH(5, BW, BH) VSB_BLURH(6, BW, BH) VSB_BLURH(7, BW, BH) VSB_BLURH(8, BW, BH)
+  if (shape == 0) {
+    switch (half) {
+      VSB_BLUR8(256, 32)
+      VSB_BLURH(9, 256, 32) VSB_BLURH(10, 256, 32) VSB_BLURH(11, 256, 32)
+      VSB_BLURH(12, 256, 32) VSB_BLURH(13, 256, 32) VSB_BLURH(14, 256, 32)
+      VSB_BLURH(15, 256, 32) VSB_BLURH(16, 256, 32)
+      default: break;
+    }
+  } else if (shape == 1) {
+    switch (half) { VSB_BLUR8(128, 16) default: break; }
+  } else if (shape == 2) {
+    switch (half) { VSB_BLUR8(128, 32) default: break; }
+  } else {
+    switch (half) { VSB_BLUR8(64, 32) default: break; }
   }
+#undef VSB_BLUR8
 #undef VSB_BLURH
 }
 
-/* launches the prefilter of one plane; returns the number of kernels */
+/* launches the prefilter of one plane with vector-blur tile shape `shape`
+   (where the plane allows the vector blur); returns the number of kernels */
 static int launch_blur(const uint8_t* src, int sp, uint8_t* dst, int dp, int W, int H, int size,
-                       uint8_t* tmp, int tp, cudaStream_t st) {
+                       uint8_t* tmp, int tp, cudaStream_t st, int shape = 0) {
   int half = size / 2;
   BlurDiv dv;
   make_div(size, half, &dv);
   if (half >= 1 && half <= BF_MAXHALF &&
       ((((uintptr_t)src | (uintptr_t)sp | (uintptr_t)dst | (uintptr_t)dp) & 15) == 0)) {
-    dim3 grid((W + BF_W - 1) / BF_W, (H + BF_H - 1) / BF_H);
-    launch_blur_fast(grid, st, src, sp, dst, dp, W, H, half, dv);
+    launch_blur_fast(blur_shape_ok(shape, half) ? shape : 0, st, src, sp, dst, dp, W, H, half, dv);
     return 1;
   }
   if (half <= BT_MAXHALF) {
@@ -619,6 +647,14 @@ static int launch_lattice(const GeomDev& gd, const uint8_t* curr, const uint8_t*
   dim3 grid(gd.g.nta * gd.g.ntb, n);
   k_lattice<TB, false, TA><<<grid, gd.g.threads, gd.smem, st>>>(curr, prev, pitch, gd.g, d_items,
                                                                 keys, tickets, d_res);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    char what[160];
+    snprintf(what, sizeof(what), "k_lattice<%d,%d> launch (%d x %d CTAs x %d threads, %zu B shared)",
+             TB, TA, gd.g.nta * gd.g.ntb, n, gd.g.threads, gd.smem);
+    set_err(what, e);
+    return -1;
+  }
   return 1;
 }
 
@@ -734,9 +770,80 @@ static int sweep_candidates(const DGeom& g, int nitems, TileCand* out, int cap) 
   return n;
 }
 
+/* cuTensorMapEncodeTiled of the driver, resolved through the runtime */
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder(void) {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = NULL;
+  static pthread_mutex_t lock = PTHREAD_MUTEX_INITIALIZER;
+  pthread_mutex_lock(&lock);
+  if (!fn) {
+    void* p = NULL;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+  }
+  pthread_mutex_unlock(&lock);
+  return fn;
+}
+
+/* A tensor map viewing a plane (row pitch `pitch`, H rows) as
+   [H][pitch/16][16] bytes with boxes of box1 16-byte chunks x box2 rows;
+   the last few maps built on this thread are kept. */
+static int sweep_map(CUtensorMap* out, const uint8_t* plane, int pitch, int H, int box1,
+                     int box2) {
+  struct Entry {
+    const uint8_t* plane;
+    int pitch, H, box1, box2;
+    CUtensorMap map;
+  };
+  static thread_local Entry cache[8];
+  static thread_local int next = 0;
+  for (int i = 0; i < 8; i++) {
+    const Entry& c = cache[i];
+    if (c.plane == plane && c.pitch == pitch && c.H == H && c.box1 == box1 && c.box2 == box2) {
+      *out = c.map;
+      return 0;
+    }
+  }
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc) {
+    set_msg("cuTensorMapEncodeTiled is not available from the driver");
+    return -1;
+  }
+  if ((pitch & 15) || ((uintptr_t)plane & 15) || box1 < 1 || box1 > 256 || box2 < 1 ||
+      box2 > 256) {
+    set_msg("tensor map of a plane: unaligned plane or box out of range");
+    return -1;
+  }
+  cuuint64_t dims[3] = { 16, (cuuint64_t)(pitch / 16), (cuuint64_t)H };
+  cuuint64_t strides[2] = { 16, (cuuint64_t)pitch };
+  cuuint32_t box[3] = { 16, (cuuint32_t)box1, (cuuint32_t)box2 };
+  cuuint32_t es[3] = { 1, 1, 1 };
+  Entry& c = cache[next];
+  const CUresult r = enc(&c.map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, (void*)plane, dims, strides,
+                         box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    c.plane = NULL;
+    char m[96];
+    snprintf(m, sizeof(m), "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    set_msg(m);
+    return -1;
+  }
+  c.plane = plane;
+  c.pitch = pitch;
+  c.H = H;
+  c.box1 = box1;
+  c.box2 = box2;
+  *out = c.map;
+  next = (next + 1) & 7;
+  return 0;
+}
+
 template <int NQ, int STEP>
 static int launch_sweep_t(const DGeom& g, size_t smem, int slot, const uint8_t* curr,
-                          const uint8_t* prev, int pitch, const vsbd_item* d_items, int n,
+                          const uint8_t* prev, int pitch, int H, const vsbd_item* d_items, int n,
                           unsigned long long* keys, unsigned* tickets, vsbd_result* d_res,
                           unsigned* err, cudaStream_t st) {
   cudaError_t e = ensure_smem((const void*)k_sweep<NQ, STEP>, slot, smem);
@@ -744,14 +851,28 @@ static int launch_sweep_t(const DGeom& g, size_t smem, int slot, const uint8_t* 
     set_err("cudaFuncSetAttribute(k_sweep)", e);
     return -1;
   }
-  k_sweep<NQ, STEP><<<g.ctas, g.threads, smem, st>>>(curr, prev, pitch, g, d_items, n, keys,
+  const SweepLayout L = sweep_layout(g);
+  CUtensorMap tw, tf;
+  if (sweep_map(&tw, prev, pitch, H, L.WPc, STEP) != 0 ||
+      sweep_map(&tf, curr, pitch, H, NQ + 1, g.S) != 0)
+    return -1;
+  k_sweep<NQ, STEP><<<g.ctas, g.threads, smem, st>>>(tw, tf, prev, pitch, g, d_items, n, keys,
                                                      tickets, d_res, err);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    char what[160];
+    snprintf(what, sizeof(what), "k_sweep<%d,%d> launch (%d CTAs x %d threads, %zu B shared)",
+             NQ, STEP, g.ctas, g.threads, smem);
+    set_err(what, e);
+    return -1;
+  }
   return 1;
 }
 
-/* the sweep of items[0 .. n) with plan g (ta == 5); err: a device-visible
-   word the kernel raises when a wait for its copies runs out */
-static int launch_sweep(const DGeom& g, const uint8_t* curr, const uint8_t* prev, int pitch,
+/* the sweep of items[0 .. n) with plan g (ta == 5) over planes of H rows;
+   err: a device-visible word the kernel raises when a wait for its copies
+   runs out */
+static int launch_sweep(const DGeom& g, const uint8_t* curr, const uint8_t* prev, int pitch, int H,
                         const vsbd_item* d_items, int n, unsigned long long* keys,
                         unsigned* tickets, vsbd_result* d_res, unsigned* err, cudaStream_t st) {
   if (n <= 0) return 0;
@@ -764,8 +885,8 @@ static int launch_sweep(const DGeom& g, const uint8_t* curr, const uint8_t* prev
   int slot = 40;
 #define VSB_SW_LAUNCH(ST, NQv)                                                                  \
   if (g.step == ST && NQ == NQv)                                                                \
-    return launch_sweep_t<NQv, ST>(g, smem, slot, curr, prev, pitch, d_items, n, keys, tickets, \
-                                   d_res, err, st);                                             \
+    return launch_sweep_t<NQv, ST>(g, smem, slot, curr, prev, pitch, H, d_items, n, keys,       \
+                                   tickets, d_res, err, st);                                    \
   slot++;
   VSB_SWEEP_CASES(VSB_SW_LAUNCH)
 #undef VSB_SW_LAUNCH
@@ -835,6 +956,14 @@ static int launch_emit_tb(const GeomDev& gd, const uint8_t* curr, const uint8_t*
   dim3 grid(gd.g.nta * gd.g.ntb, n);
   k_lattice<TB, true><<<grid, gd.g.threads, gd.smem, st>>>(curr, prev, pitch, gd.g, d_items, NULL,
                                                            NULL, NULL);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    char what[160];
+    snprintf(what, sizeof(what), "k_lattice<%d> partial-pass launch (%d x %d CTAs x %d threads, "
+             "%zu B shared)", TB, gd.g.nta * gd.g.ntb, n, gd.g.threads, gd.smem);
+    set_err(what, e);
+    return -1;
+  }
   return 1;
 }
 
@@ -947,7 +1076,14 @@ static int autotune_tiling(GeomDev* gd, const uint8_t* curr, const uint8_t* prev
       return emit_buf ? launch_emit(t, curr, prev, pitch, d_items, n, st)
                       : launch_search(t, curr, prev, pitch, d_items, n, keys, tickets, d_res, st);
     };
-    if (one() < 0) return -1.f;
+    if (one() < 0) {
+      const cudaError_t le = cudaGetLastError();
+      if (getenv("VSB_DEBUG_TUNE"))
+        fprintf(stderr, "tiling tuning: tiling skipped (tb %d ta %d %dx%d, %d strips, %d threads: "
+                "%s; %s)\n", cg.tb, cg.ta, cg.nab, cg.nbb, cg.nstrip, cg.threads, vsbd_error(),
+                cudaGetErrorString(le));
+      return -1.f;
+    }
     cudaEventRecord(e0, st);
     for (int rep = 0; rep < reps; rep++) one();
     cudaEventRecord(e1, st);
@@ -986,7 +1122,13 @@ static int autotune_tiling(GeomDev* gd, const uint8_t* curr, const uint8_t* prev
     }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  CK(cudaGetLastError());
+  {
+    const cudaError_t le = cudaGetLastError();
+    if (le != cudaSuccess) {
+      set_err(emit_buf ? "partial-pass tiling tuning" : "search tiling tuning", le);
+      return -1;
+    }
+  }
   best.emit = NULL;
   g = best;
   gd->smem = tile_layout(g).total;
@@ -1013,7 +1155,7 @@ static SweepTune g_swtune[64];
 static int g_nswtune = 0;
 
 static int autotune_sweep(const GeomDev& gd, const uint8_t* curr, const uint8_t* prev, int pitch,
-                          const vsbd_item* d_items, int n, unsigned long long* keys,
+                          int H, const vsbd_item* d_items, int n, unsigned long long* keys,
                           unsigned* tickets, vsbd_result* d_res, unsigned* err,
                           volatile unsigned* h_err, cudaStream_t st, DGeom* plan, int* on) {
   *on = 0;
@@ -1043,10 +1185,19 @@ static int autotune_sweep(const GeomDev& gd, const uint8_t* curr, const uint8_t*
     CK(cudaEventCreate(&e1));
     auto time_of = [&](const DGeom* sw, int reps) -> float {
       auto one = [&]() {
-        return sw ? launch_sweep(*sw, curr, prev, pitch, d_items, n, keys, tickets, d_res, err, st)
+        return sw ? launch_sweep(*sw, curr, prev, pitch, H, d_items, n, keys, tickets, d_res, err,
+                                 st)
                   : launch_search(gd, curr, prev, pitch, d_items, n, keys, tickets, d_res, st);
       };
-      if (one() < 0) return -1.f;
+      if (one() < 0) {
+        /* a plan that cannot launch here is skipped; its error is not
+           the tuning's */
+        const cudaError_t le = cudaGetLastError();
+        if (getenv("VSB_DEBUG_TUNE"))
+          fprintf(stderr, "sweep tuning: plan skipped (%s; %s)\n", vsbd_error(),
+                  cudaGetErrorString(le));
+        return -1.f;
+      }
       cudaEventRecord(e0, st);
       for (int r = 0; r < reps; r++) one();
       cudaEventRecord(e1, st);
@@ -1085,11 +1236,24 @@ static int autotune_sweep(const GeomDev& gd, const uint8_t* curr, const uint8_t*
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    CK(cudaGetLastError());
+    const cudaError_t le = cudaGetLastError();
+    if (le != cudaSuccess) {
+      set_err("search sweep tuning", le);
+      return -1;
+    }
     if (*h_err) {
       *h_err = 0;
       set_msg("the search sweep's staging did not complete while tuning");
       return -1;
+    }
+    if (getenv("VSB_DEBUG_TUNE")) {
+      fprintf(stderr, "sweep tuning S=%d step=%d na=%d items=%d: per-tile search %.1f us\n", g.S,
+              g.step, g.na, n, 1000.f * lat_ms);
+      for (int k = 0; k < nc; k++)
+        fprintf(stderr, "  plan %d: %d cols x %d rows, %d strips, %d threads, %d CTAs, %zu B: "
+                "%.1f us%s\n", k, cand[k].g.nab, cand[k].g.nbb, cand[k].g.nstrip,
+                cand[k].g.threads, cand[k].g.ctas, sweep_layout(cand[k].g).total, 1000.f * ms_of[k],
+                k == best ? " (best)" : "");
     }
     if (best >= 0 && lat_ms >= 0.f && (force || best_ms < lat_ms)) {
       *on = 1;
@@ -1143,6 +1307,8 @@ struct vsbd_ctx {
   int nc, nf;
   cudaStream_t st;
   uint8_t* d_raw;     /* input plane (blurred formats) */
+  int blur_shape;     /* vector-blur tile shape (g_blur_shape), picked by timing */
+  float blur_us;      /* its tuned time per frame */
   uint8_t* d_tmp;     /* row-pass buffer of the wide-window blur */
   uint8_t* d_buf[3];  /* blurred planes: slots of the current frame, the
                          previous one and the next one (filled ahead while
@@ -1324,6 +1490,69 @@ extern "C" void vsbd_destroy(vsbd_ctx* c) {
   free(c);
 }
 
+/* The vector blur's tile shape for a plane geometry: every shape that
+   serves the window is timed on the detector's own planes and the fastest
+   kept; cached per (device, width, height, box size). */
+struct BlurTune {
+  int dev, W, H, size, shape;
+  float us;
+};
+static BlurTune g_blurtune[64];
+static int g_nblurtune = 0;
+
+static int autotune_blur(vsbd_ctx* c, const uint8_t* src, uint8_t* dst) {
+  c->blur_shape = 0;
+  c->blur_us = 0.f;
+  const int half = c->blur / 2;
+  if (c->blur < 2 || half > 8 || getenv("VSB_NO_AUTOTUNE")) return 0;
+  TuneLock lock;
+  const int dev = current_device();
+  for (int i = 0; i < g_nblurtune; i++)
+    if (g_blurtune[i].dev == dev && g_blurtune[i].W == c->W && g_blurtune[i].H == c->H &&
+        g_blurtune[i].size == c->blur) {
+      c->blur_shape = g_blurtune[i].shape;
+      c->blur_us = g_blurtune[i].us;
+      return 0;
+    }
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  float best = 1e30f;
+  for (int round = 0; round < 3; round++)
+    for (int s = 0; s < VSB_BLUR_SHAPES; s++) {
+      if (!blur_shape_ok(s, half)) continue;
+      launch_blur(src, c->pitch, dst, c->pitch, c->W, c->H, c->blur, c->d_tmp, c->pitch, c->st, s);
+      cudaEventRecord(e0, c->st);
+      for (int r = 0; r < 10; r++)
+        launch_blur(src, c->pitch, dst, c->pitch, c->W, c->H, c->blur, c->d_tmp, c->pitch, c->st,
+                    s);
+      cudaEventRecord(e1, c->st);
+      if (cudaEventSynchronize(e1) != cudaSuccess) break;
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      /* the first round warms the clocks up */
+      if (round > 0 && ms < best) {
+        best = ms;
+        c->blur_shape = s;
+      }
+    }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  {
+    const cudaError_t le = cudaGetLastError();
+    if (le != cudaSuccess) {
+      set_err("blur tile tuning", le);
+      return -1;
+    }
+  }
+  c->blur_us = best < 1e29f ? 100.f * best : 0.f;
+  if (g_nblurtune < 64) {
+    BlurTune& b = g_blurtune[g_nblurtune++];
+    b.dev = dev; b.W = c->W; b.H = c->H; b.size = c->blur; b.shape = c->blur_shape; b.us = c->blur_us;
+  }
+  return 0;
+}
+
 /* search strategy of detectors created from now on (-1: environment) */
 static int g_default_mode = -1;
 extern "C" void vsbd_set_default_search_mode(int pruned) { g_default_mode = pruned < 0 ? -1 : (pruned ? 1 : 0); }
@@ -1456,13 +1685,17 @@ extern "C" int vsbd_create(vsbd_ctx** out, int W, int H, int bpp, int blur_size,
     vsbd_destroy(c);
     return -1;
   }
+  if (autotune_blur(c, c->d_raw ? c->d_raw : c->d_buf[0], c->d_buf[2]) != 0) {
+    vsbd_destroy(c);
+    return -1;
+  }
   CKC(cudaHostAlloc(&c->h_swerr, 2 * sizeof(unsigned), cudaHostAllocMapped));
   c->h_swerr[0] = c->h_swerr[1] = 0;
   CKC(cudaHostGetDevicePointer((void**)&c->d_swerr, c->h_swerr, 0));
-  if (autotune_sweep(c->gc, c->d_buf[0], c->d_buf[1], c->pitch, c->d_citems, nc, c->d_keys,
+  if (autotune_sweep(c->gc, c->d_buf[0], c->d_buf[1], c->pitch, c->H, c->d_citems, nc, c->d_keys,
                      c->d_tickets, (vsbd_result*)(c->d_out + c->off_coarse), c->d_swerr,
                      c->h_swerr, c->st, &c->swc, &c->sw_c) != 0 ||
-      autotune_sweep(c->gf, c->d_buf[0], c->d_buf[1], c->pitch, c->d_fitems, nf,
+      autotune_sweep(c->gf, c->d_buf[0], c->d_buf[1], c->pitch, c->H, c->d_fitems, nf,
                      c->d_keys + nc, c->d_tickets + nc, (vsbd_result*)(c->d_out + c->off_fine),
                      c->d_swerr + 1, c->h_swerr + 1, c->st, &c->swf, &c->sw_f) != 0) {
     vsbd_destroy(c);
@@ -1598,7 +1831,12 @@ static int stage_a_issue(vsbd_ctx* c, const uint8_t* host, int linesize, const u
       sp = c->pitch;
     }
     kt_begin(c, VSBD_KT_BLUR, st);
-    { int nb = launch_blur(src, sp, cur, c->pitch, c->W, c->H, c->blur, c->d_tmp, c->pitch, st); c->launches += nb; count_launches(nb); }
+    {
+      int nb = launch_blur(src, sp, cur, c->pitch, c->W, c->H, c->blur, c->d_tmp, c->pitch, st,
+                           c->blur_shape);
+      c->launches += nb;
+      count_launches(nb);
+    }
     kt_end(c, VSBD_KT_BLUR, st);
     CK(cudaGetLastError());
   } else {
@@ -1645,7 +1883,7 @@ static int stage_a_issue(vsbd_ctx* c, const uint8_t* host, int linesize, const u
       int nl = c->mode ? launch_pruned(c->gc, c->gcp, cur, prv, c->pitch, c->d_citems, c->nc,
                                        c->d_skip, c->d_part, c->d_counts, c->d_lists, c->d_boxes,
                                        c->d_keys, c->d_tickets, cres, st)
-               : c->sw_c ? launch_sweep(c->swc, cur, prv, c->pitch, c->d_citems, c->nc, c->d_keys,
+               : c->sw_c ? launch_sweep(c->swc, cur, prv, c->pitch, c->H, c->d_citems, c->nc, c->d_keys,
                                         c->d_tickets, cres, c->d_swerr, st)
                        : launch_search(c->gc, cur, prv, c->pitch, c->d_citems, c->nc, c->d_keys,
                                        c->d_tickets, cres, st);
@@ -1780,7 +2018,7 @@ extern "C" int vsbd_stage_b_issue(vsbd_ctx* c, const vsbd_item* items, int n) {
                                      c->d_part, c->d_counts + c->nc, c->d_lists,
                                      c->d_boxes + 4 * c->nc, c->d_keys + c->nc,
                                      c->d_tickets + c->nc, fres, st)
-             : c->sw_f ? launch_sweep(c->swf, cur, prv, c->pitch, c->d_fitems, n, c->d_keys + c->nc,
+             : c->sw_f ? launch_sweep(c->swf, cur, prv, c->pitch, c->H, c->d_fitems, n, c->d_keys + c->nc,
                                       c->d_tickets + c->nc, fres, c->d_swerr + 1, st)
                      : launch_search(c->gf, cur, prv, c->pitch, c->d_fitems, n, c->d_keys + c->nc,
                                      c->d_tickets + c->nc, fres, st);
@@ -1849,6 +2087,14 @@ extern "C" int vsbd_search_tiling(const vsbd_ctx* c, int fine, int* desc) {
   desc[5] = g.threads;
   desc[6] = (int)(sw ? sweep_layout(g).total : (fine ? c->gf.smem : c->gc.smem));
   desc[7] = sw ? g.ctas : g.nta * g.ntb;
+  return 0;
+}
+
+extern "C" int vsbd_blur_tiling(const vsbd_ctx* c, int* desc) {
+  if (!c || !desc) return -1;
+  desc[0] = g_blur_shape[c->blur_shape][0];
+  desc[1] = g_blur_shape[c->blur_shape][1];
+  desc[2] = (int)(1000.f * c->blur_us);
   return 0;
 }
 
@@ -1989,7 +2235,8 @@ extern "C" long vsbd_field_log_count(const vsbd_ctx* c) { return c ? c->log_n : 
 /* kernel-level entry points (parity tests)                                  */
 /* ------------------------------------------------------------------------ */
 
-extern "C" int vsbd_blur_host(uint8_t* dst, const uint8_t* src, int W, int H, int size) {
+extern "C" int vsbd_blur_host_shape(uint8_t* dst, const uint8_t* src, int W, int H, int size,
+                                    int shape) {
   int pitch = (W + 127) & ~127;
   size_t plane = (size_t)pitch * H + 256;
   uint8_t *d_src = NULL, *d_dst = NULL, *d_tmp = NULL;
@@ -2002,7 +2249,7 @@ extern "C" int vsbd_blur_host(uint8_t* dst, const uint8_t* src, int W, int H, in
   if (size < 2) {
     e = cudaMemcpy2D(d_dst, pitch, d_src, pitch, W, H, cudaMemcpyDeviceToDevice);
   } else {
-    launch_blur(d_src, pitch, d_dst, pitch, W, H, size, d_tmp, pitch, 0);
+    launch_blur(d_src, pitch, d_dst, pitch, W, H, size, d_tmp, pitch, 0, shape);
     e = cudaGetLastError();
   }
   if (e != cudaSuccess) { set_err("blur", e); goto done; }
@@ -2013,6 +2260,10 @@ done:
   cudaFree(d_dst);
   cudaFree(d_tmp);
   return rc;
+}
+
+extern "C" int vsbd_blur_host(uint8_t* dst, const uint8_t* src, int W, int H, int size) {
+  return vsbd_blur_host_shape(dst, src, W, H, size, 0);
 }
 
 extern "C" int vsbd_minmax_host(const uint8_t* img, int W, int H, int bpp, int channels,
@@ -2084,7 +2335,8 @@ extern "C" int vsbd_search_host(const uint8_t* curr, const uint8_t* prev, int W,
   cudaMemcpy2D(d_p, pitch, prev, (size_t)W * bpp, (size_t)W * bpp, H, cudaMemcpyHostToDevice);
   cudaMemcpy(d_items, items, sizeof(vsbd_item) * n, cudaMemcpyHostToDevice);
   if (tiles_hint < 0) {
-    if (launch_sweep(swg, d_c, d_p, pitch, d_items, n, d_keys, d_tk, d_res, d_err, 0) < 0) goto done;
+    if (launch_sweep(swg, d_c, d_p, pitch, H, d_items, n, d_keys, d_tk, d_res, d_err, 0) < 0)
+      goto done;
     if ((e = cudaMemcpy(&h_err, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost)) != cudaSuccess) { set_err("k_sweep", e); goto done; }
     if (h_err) { set_msg("search sweep: a wait for staged rows gave up"); goto done; }
   } else if (launch_search(gd, d_c, d_p, pitch, d_items, n, d_keys, d_tk, d_res, 0) < 0) {

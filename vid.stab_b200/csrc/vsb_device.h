@@ -113,6 +113,10 @@ int vsbd_stage_b_collect(vsbd_ctx* c, const vsbd_result** fine);
    and rows per CTA, field strips, threads, shared memory bytes, CTAs per item */
 int vsbd_search_tiling(const vsbd_ctx* c, int fine, int* desc);
 
+/* the prefilter's tile (desc[0] width, desc[1] height) and its tuned time
+   per frame in ns (desc[2]; 0 when not tuned) */
+int vsbd_blur_tiling(const vsbd_ctx* c, int* desc);
+
 /* Kernel launches issued on behalf of this detector so far. */
 long vsbd_launches(const vsbd_ctx* c);
 
@@ -197,6 +201,8 @@ int vsbd_search_noalloc(const uint8_t* d_curr, const uint8_t* d_prev, int pitch,
 
 /* ---- kernel-level entry points for parity tests (host buffers in/out) --- */
 int vsbd_blur_host(uint8_t* dst, const uint8_t* src, int width, int height, int size);
+int vsbd_blur_host_shape(uint8_t* dst, const uint8_t* src, int width, int height, int size,
+                         int shape);
 int vsbd_minmax_host(const uint8_t* img, int width, int height, int bpp, int channels,
                      const int16_t* x, const int16_t* y, int n, int size, uint8_t* out);
 int vsbd_search_host(const uint8_t* curr, const uint8_t* prev, int width, int height,

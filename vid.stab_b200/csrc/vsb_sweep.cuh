@@ -8,9 +8,12 @@
  * The kernel is persistent: CTA c takes the tiles [c*T/G, (c+1)*T/G) of the
  * T tiles of the launch in order, so consecutive tiles mostly share a field.
  * Each tile's previous-frame window (and, when the field changes, the
- * current frame's field rows) is staged in shared memory by the TMA unit:
- * one cp.async.bulk per row, completing on an mbarrier.  Two buffers: tile
- * k+1's copies are in flight while tile k is summed.
+ * current frame's field rows) is staged in shared memory by the TMA unit
+ * from tensor maps over the blurred planes: the plane is viewed as
+ * [rows][16-byte chunks][16 bytes], so one box spans a whole window row
+ * (up to 256 chunks) and STEP rows; the field is one box.  The copies
+ * complete on an mbarrier.  Two buffers: tile k+1's copies are in flight
+ * while tile k is summed.
  *
  * Sums.  A thread owns 8 consecutive lattice columns of one lattice row and
  * a strip of the field's rows.  Its columns start at byte E + c*STEP of a
@@ -42,6 +45,7 @@
 #ifndef VSB_SWEEP_CUH
 #define VSB_SWEEP_CUH
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -66,18 +70,19 @@ __host__ __device__ constexpr int sw_chunks(int STEP, int NQ) {
 }
 
 /* shared-memory layout of the sweep for a tiling (g.ncg = g.nab / 8
-   column groups, g.nbb lattice rows, g.nstrip strips) */
+   column groups, g.nbb lattice rows, g.nstrip strips).  The window is
+   staged in groups of STEP rows (one tensor box each), D chunks apart so
+   that every box starts on a 128-byte boundary; rows of a group are WPc
+   chunks apart. */
 struct SweepLayout {
-  int NQ, WPc, X, WH, FR, FCP;
+  int NQ, WPc, D, NG, WH, FR, FCP;
   size_t win_bytes, fraw_bytes, fc_bytes;
   size_t off_win[2], off_fraw[2], off_fc, off_part, off_q, total;
 };
 
-/* chunk offset of window row r: rows STEP apart differ by an odd multiple
-   of the thread stride, so the 16-byte loads of 8 consecutive threads hit
-   distinct bank groups */
-__host__ __device__ inline int sw_row_off(int r, int WPc, int X, int step) {
-  return r * WPc + (r / step) * X;
+/* chunk offset of window row r */
+__host__ __device__ inline int sw_row_off(int r, int WPc, int D, int step) {
+  return (r / step) * D + (r % step) * WPc;
 }
 
 __host__ __device__ inline SweepLayout sweep_layout(const DGeom& g) {
@@ -86,11 +91,12 @@ __host__ __device__ inline SweepLayout sweep_layout(const DGeom& g) {
   const int ncg = g.nab / SW_TA;
   const int cs = g.step / 2; /* chunks between column groups */
   L.WPc = (ncg - 1) * cs + sw_chunks(g.step, L.NQ);
-  L.X = (((cs * ncg - g.step * L.WPc) % 8) + 8) % 8;
+  L.D = (g.step * L.WPc + 7) & ~7;
   L.WH = g.S + (g.nbb - 1) * g.step;
+  L.NG = (L.WH + g.step - 1) / g.step;
   L.FR = g.S + 16;
   L.FCP = (L.NQ + 1) * 16;
-  L.win_bytes = (size_t)16 * (sw_row_off(L.WH - 1, L.WPc, L.X, g.step) + L.WPc);
+  L.win_bytes = (size_t)16 * L.D * L.NG;
   /* the refinement window of a field reuses a tile buffer */
   const int R = refine_reach(g);
   const size_t rwin = (size_t)(g.S + 2 * R) * (((3 + g.S + 2 * R + 8 + 15) >> 4) << 4) + 16;
@@ -171,6 +177,17 @@ __device__ __forceinline__ void sw_bulk_load(void* dst, const void* src, unsigne
       : "memory");
 }
 
+/* one box of a 3-D tensor map (coordinates innermost first) into shared
+   memory (128-byte aligned), completing on bar */
+__device__ __forceinline__ void sw_box_load(void* dst, const CUtensorMap* map, int c0, int c1,
+                                            int c2, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(sw_smem_addr(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(sw_smem_addr(bar))
+      : "memory");
+}
+
 /* generic-proxy accesses of shared memory before the async proxy's writes */
 __device__ __forceinline__ void sw_fence_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -198,29 +215,37 @@ __device__ __forceinline__ bool sw_bar_wait(uint64_t* bar, unsigned parity) {
   return false;
 }
 
-/* Issues tile t's copies into buffer b (warp 0, all lanes): its window rows
-   and, with field, the rows of its field in the current frame. */
+/* row groups (boxes) of tile T's window */
 template <int STEP>
-__device__ __forceinline__ void sweep_issue(const DGeom& g, const SweepLayout& L, const SweepTile& T,
-                                            bool field, const uint8_t* __restrict__ curr,
-                                            const uint8_t* __restrict__ prev, int pitch,
-                                            uint8_t* win, uint8_t* fraw, uint64_t* bar, int lane) {
-  const int nvec = (T.e + (T.na_t - 1) * STEP + g.S + 15) >> 4;
-  const int wh = g.S + (T.nb_t - 1) * STEP;
-  const int nvf = (T.ce + g.S + 15) >> 4;
-  const unsigned bytes = (unsigned)(wh * nvec * 16 + (field ? g.S * nvf * 16 : 0));
-  if (lane == 0) {
-    sw_fence_async_smem();
-    sw_bar_expect(bar, bytes);
+__device__ __forceinline__ int sweep_groups(const DGeom& g, const SweepTile& T) {
+  return (g.S + (T.nb_t - 1) * STEP + STEP - 1) / STEP;
+}
+
+/* bytes tile T's boxes bring: its window's row groups (WPc chunks x STEP
+   rows each) and, with field, the field box ((NQ+1) chunks x S rows) */
+template <int STEP>
+__device__ __forceinline__ unsigned sweep_bytes(const DGeom& g, const SweepLayout& L,
+                                                const SweepTile& T, bool field) {
+  return (unsigned)(sweep_groups<STEP>(g, T) * 16 * L.WPc * STEP + (field ? L.FR * g.S : 0));
+}
+
+/* Issues tile T's boxes into a buffer, one box per thread of the first
+   warps; the buffer's mbarrier already expects their bytes (sweep_bytes).
+   tm_win: the previous plane with boxes of WPc chunks x STEP rows; tm_fld:
+   the current plane with boxes of NQ+1 chunks x S rows.  Boxes reaching
+   past the plane are filled with zeros by the TMA unit. */
+template <int STEP>
+__device__ __forceinline__ void sweep_copies(const DGeom& g, const SweepLayout& L, const SweepTile& T,
+                                             bool field, const CUtensorMap* tm_win,
+                                             const CUtensorMap* tm_fld, uint8_t* win,
+                                             uint8_t* fraw, uint64_t* bar) {
+  const int ng = sweep_groups<STEP>(g, T);
+  for (int k = threadIdx.x; k < ng + (field ? 1 : 0); k += blockDim.x) {
+    if (k < ng)
+      sw_box_load(win + (size_t)16 * L.D * k, tm_win, 0, T.gx0a >> 4, T.gy0 + k * STEP, bar);
+    else
+      sw_box_load(fraw, tm_fld, 0, T.cx0a >> 4, T.cy0, bar);
   }
-  __syncwarp();
-  for (int r = lane; r < wh; r += 32)
-    sw_bulk_load(win + 16 * sw_row_off(r, L.WPc, L.X, STEP),
-                 prev + (size_t)(T.gy0 + r) * pitch + T.gx0a, (unsigned)nvec * 16u, bar);
-  if (field)
-    for (int r = lane; r < g.S; r += 32)
-      sw_bulk_load(fraw + (size_t)r * L.FR, curr + (size_t)(T.cy0 + r) * pitch + T.cx0a,
-                   (unsigned)nvf * 16u, bar);
 }
 
 /* Builds the field copies of one field from its raw rows: slot 0 the field
@@ -263,7 +288,7 @@ __device__ __forceinline__ void sweep_field_copies(const DGeom& g, const SweepLa
    wr0 .. wr0+Rs-1.  fA / fB: the field copies of the even / odd columns. */
 template <int NQ, int STEP, int E>
 __device__ __forceinline__ void sweep_sums(unsigned (&acc)[SW_TA], const uint8_t* __restrict__ win,
-                                           int WPc, int X, int cgoff, int wr0,
+                                           int WPc, int D, int cgoff, int wr0,
                                            const uint8_t* __restrict__ fA,
                                            const uint8_t* __restrict__ fB, int FCP, int r0,
                                            int Rs) {
@@ -272,7 +297,7 @@ __device__ __forceinline__ void sweep_sums(unsigned (&acc)[SW_TA], const uint8_t
   const uint4* __restrict__ W0 = (const uint4*)win + cgoff;
   for (int r = 0; r < Rs; r++) {
     const int wr = wr0 + r;
-    const uint4* __restrict__ W4 = W0 + sw_row_off(wr, WPc, X, STEP);
+    const uint4* __restrict__ W4 = W0 + sw_row_off(wr, WPc, D, STEP);
     const uint4* __restrict__ FA4 = (const uint4*)(fA + (size_t)(r0 + r) * FCP);
     const uint4* __restrict__ FB4 = (const uint4*)(fB + (size_t)(r0 + r) * FCP);
     uint32_t w[4 * NCH];
@@ -290,12 +315,14 @@ __device__ __forceinline__ void sweep_sums(unsigned (&acc)[SW_TA], const uint8_t
       const uint4 fb = SB == SA ? fa : FB4[q];
       const uint32_t fav[4] = { fa.x, fa.y, fa.z, fa.w };
       const uint32_t fbv[4] = { fb.x, fb.y, fb.z, fb.w };
+      /* word-major: the eight columns' accumulations are independent, so
+         consecutive packed SADs never wait on one another */
 #pragma unroll
-      for (int c = 0; c < SW_TA; c++) {
-        const int o = E + c * STEP, wc = o >> 2, s = o & 3;
+      for (int i = 0; i < 4; i++) {
+        const int k = 4 * q + i;
 #pragma unroll
-        for (int i = 0; i < 4; i++) {
-          const int k = 4 * q + i;
+        for (int c = 0; c < SW_TA; c++) {
+          const int o = E + c * STEP, wc = o >> 2, s = o & 3;
           uint32_t ww = w[wc + k];
           if (k == 0 && s) ww &= 0xffffffffu << (8 * s);
           acc[c] = sad4(((c & 1) && SB != SA) ? fbv[i] : fav[i], ww, acc[c]);
@@ -324,11 +351,11 @@ __device__ __forceinline__ void sweep_sums(unsigned (&acc)[SW_TA], const uint8_t
 
 template <int NQ, int STEP>
 __device__ __forceinline__ void sweep_sums_e(int E, unsigned (&acc)[SW_TA], const uint8_t* win,
-                                             int WPc, int X, int cgoff, int wr0,
+                                             int WPc, int D, int cgoff, int wr0,
                                              const uint8_t* fA, const uint8_t* fB, int FCP,
                                              int r0, int Rs) {
 #define SW_E(v) \
-  case v: sweep_sums<NQ, STEP, v>(acc, win, WPc, X, cgoff, wr0, fA, fB, FCP, r0, Rs); break;
+  case v: sweep_sums<NQ, STEP, v>(acc, win, WPc, D, cgoff, wr0, fA, fB, FCP, r0, Rs); break;
   switch (E) {
     SW_E(0) SW_E(1) SW_E(2) SW_E(3) SW_E(4) SW_E(5) SW_E(6) SW_E(7)
     SW_E(8) SW_E(9) SW_E(10) SW_E(11) SW_E(12) SW_E(13) SW_E(14) SW_E(15)
@@ -337,10 +364,12 @@ __device__ __forceinline__ void sweep_sums_e(int E, unsigned (&acc)[SW_TA], cons
 }
 
 /* grid: g.ctas persistent CTAs; block g.threads; dynamic shared memory
-   sweep_layout(g).total.  Tiles of items[0 .. n). */
+   sweep_layout(g).total.  Tiles of items[0 .. n).  tm_win / tm_fld: tensor
+   maps of prev / curr (sweep_map). */
 template <int NQ, int STEP>
 __global__ void __launch_bounds__(SW_MAX_THREADS, 1)
-    k_sweep(const uint8_t* __restrict__ curr, const uint8_t* __restrict__ prev, int pitch, DGeom g,
+    k_sweep(const __grid_constant__ CUtensorMap tm_win, const __grid_constant__ CUtensorMap tm_fld,
+            const uint8_t* __restrict__ prev, int pitch, DGeom g,
             const vsbd_item* __restrict__ items, int n, unsigned long long* __restrict__ keys,
             unsigned* __restrict__ tickets, vsbd_result* __restrict__ res, unsigned* err) {
   extern __shared__ __align__(128) uint8_t sm[];
@@ -356,12 +385,6 @@ __global__ void __launch_bounds__(SW_MAX_THREADS, 1)
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   if (nmine <= 0) return;
   uint8_t* fc = sm + L.off_fc;
-  if (threadIdx.x == 0) {
-    sw_bar_init(&bars[0], 1);
-    sw_bar_init(&bars[1], 1);
-    sw_bar_init_fence();
-  }
-  __syncthreads();
   /* whether tile t needs its field staged: the first tile, a new field, or a
      new alignment of the window (which picks the field copies) */
   auto needs_field = [&](int t, const SweepTile& Tt) -> bool {
@@ -369,12 +392,21 @@ __global__ void __launch_bounds__(SW_MAX_THREADS, 1)
     const SweepTile Tp = sweep_tile(g, items, t - 1);
     return Tp.item != Tt.item || ((Tp.e ^ Tt.e) & 3);
   };
-  if (warp == 0)
+  if (threadIdx.x == 0) {
+    sw_bar_init(&bars[0], 1);
+    sw_bar_init(&bars[1], 1);
+    sw_bar_init_fence();
     for (int k = 0; k < 2 && k < nmine; k++) {
       const SweepTile Tt = sweep_tile(g, items, t_begin + k);
-      sweep_issue<STEP>(g, L, Tt, needs_field(t_begin + k, Tt), curr, prev, pitch,
-                        sm + L.off_win[k], sm + L.off_fraw[k], &bars[k], lane);
+      sw_bar_expect(&bars[k], sweep_bytes<STEP>(g, L, Tt, needs_field(t_begin + k, Tt)));
     }
+  }
+  __syncthreads();
+  for (int k = 0; k < 2 && k < nmine; k++) {
+    const SweepTile Tt = sweep_tile(g, items, t_begin + k);
+    sweep_copies<STEP>(g, L, Tt, needs_field(t_begin + k, Tt), &tm_win, &tm_fld,
+                       sm + L.off_win[k], sm + L.off_fraw[k], &bars[k]);
+  }
   /* thread task: column group, lattice row of the tile, field strip */
   const int tps = ncg * g.nbb;
   const int ntask = tps * g.nstrip;
@@ -413,7 +445,7 @@ __global__ void __launch_bounds__(SW_MAX_THREADS, 1)
     if (active) {
       const uint8_t* fA = fc + (size_t)(sA ? 1 : 0) * g.S * L.FCP;
       const uint8_t* fB = fc + (size_t)(sB ? 2 : 0) * g.S * L.FCP;
-      sweep_sums_e<NQ, STEP>(T.e, acc, win, L.WPc, L.X, cg * (STEP / 2), st * Rs + bl * STEP, fA,
+      sweep_sums_e<NQ, STEP>(T.e, acc, win, L.WPc, L.D, cg * (STEP / 2), st * Rs + bl * STEP, fA,
                              fB, L.FCP, st * Rs, Rs);
     }
     /* the strips' partial sums */
@@ -466,14 +498,21 @@ __global__ void __launch_bounds__(SW_MAX_THREADS, 1)
                        (unsigned*)(sm + L.off_q));
     }
     /* every thread's reads (and the refinement's writes) of buffer b are
-       ordered before the bulk copies that refill it */
+       ordered before the bulk copies that refill it; the barrier then
+       expects tile k+2's bytes before any copy is issued */
     sw_fence_async_smem();
-    __syncthreads();
-    if (warp == 0 && k + 2 < nmine) {
-      const SweepTile Tn = sweep_tile(g, items, tt + 2);
-      sweep_issue<STEP>(g, L, Tn, needs_field(tt + 2, Tn), curr, prev, pitch, sm + L.off_win[b],
-                        sm + L.off_fraw[b], &bars[b], lane);
+    const bool more = k + 2 < nmine;
+    SweepTile Tn;
+    bool fn = false;
+    if (more) {
+      Tn = sweep_tile(g, items, tt + 2);
+      fn = needs_field(tt + 2, Tn);
+      if (threadIdx.x == 0) sw_bar_expect(&bars[b], sweep_bytes<STEP>(g, L, Tn, fn));
     }
+    __syncthreads();
+    if (more)
+      sweep_copies<STEP>(g, L, Tn, fn, &tm_win, &tm_fld, sm + L.off_win[b], sm + L.off_fraw[b],
+                         &bars[b]);
   }
 }
 

@@ -5,9 +5,10 @@ binds it for tests, benchmarks and Python callers.
 """
 from ._lib import (LM_DTYPE, PF_BGR24, PF_GRAY8, PF_RGB24, PF_RGBA, PF_YUV420P, PF_YUVA420P,
                    ASCII_SERIALIZATION_MODE, BINARY_SERIALIZATION_MODE, lib)
-from .api import (Batch, MotionDetector, detect_clip, detect_multi, boxblur, field_minmax,
-                  field_search, bpp_of)
+from .api import (Batch, MotionDetector, detect_clip, detect_multi, boxblur, boxblur_tile,
+                  field_minmax, field_search, bpp_of)
 
 __all__ = ["LM_DTYPE", "PF_GRAY8", "PF_YUV420P", "PF_YUVA420P", "PF_RGB24", "PF_BGR24", "PF_RGBA",
            "ASCII_SERIALIZATION_MODE", "BINARY_SERIALIZATION_MODE", "lib", "Batch", "MotionDetector",
-           "detect_clip", "detect_multi", "boxblur", "field_minmax", "field_search", "bpp_of"]
+           "detect_clip", "detect_multi", "boxblur", "boxblur_tile", "field_minmax", "field_search",
+           "bpp_of"]

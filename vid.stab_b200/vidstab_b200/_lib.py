@@ -145,6 +145,10 @@ def lib():
     L.vsb_test_device_alloc.argtypes = [i, i]
     L.vsb_boxblur_host.restype = i
     L.vsb_boxblur_host.argtypes = [p, p, i, i, i]
+    L.vsb_boxblur_host_tile.restype = i
+    L.vsb_boxblur_host_tile.argtypes = [p, p, i, i, i, i]
+    L.vsb_blur_tiling.restype = i
+    L.vsb_blur_tiling.argtypes = [C.POINTER(VSMotionDetect), p]
     L.vsb_field_minmax_host.restype = i
     L.vsb_field_minmax_host.argtypes = [p, i, i, i, i, p, p, i, i, p]
     L.vsb_field_search_host.restype = i

@@ -278,6 +278,18 @@ def boxblur(plane, size):
     return out
 
 
+def boxblur_tile(plane, size, shape):
+    """GPU prefilter with a given vector-blur tile shape (0: 256x32,
+    1: 128x16, 2: 128x32, 3: 64x32)."""
+    L = lib()
+    plane = np.ascontiguousarray(plane, dtype=np.uint8)
+    H, W = plane.shape
+    out = np.empty_like(plane)
+    if L.vsb_boxblur_host_tile(ptr(out), ptr(plane), W, H, size, shape) != 0:
+        raise RuntimeError(L.vsb_last_error().decode())
+    return out
+
+
 def field_minmax(img, xs, ys, size, bpp=1, channels=1):
     L = lib()
     img = np.ascontiguousarray(img, dtype=np.uint8)
