@@ -65,6 +65,12 @@ sys.path.insert(0, os.path.join(REPO, "oracle"))
 
 import numpy as np  # noqa: E402
 
+
+def records_per_frame(width, height):
+    """an upper bound of the LocalMotions one frame gives (every coarse and
+    fine field; fine fields are at least 16 pixels apart)"""
+    return 256 + (width // 16 + 1) * (height // 16 + 1)
+
 METRIC = "1080p detect frames/s: plain GPU (bit-exact) vs learned-proposal (≥99.5% agree)"
 W, H = 1920, 1080
 PUBLISHED_FPS = 1000.0 / 4.43  # docs/simd.md: 1080p detect, AVX2, 19 threads, Ryzen 9 9900X
@@ -263,7 +269,7 @@ def learned_arm(V, clip, host_np, nfr, steps, warmup, timed):
     per-frame device time of its kernels."""
     from vidstab_b200 import pnet
     blob = pnet.load_blob()
-    rec = np.zeros(nfr * 512 + 64, V.LM_DTYPE)
+    rec = np.zeros(nfr * records_per_frame(W, H) + 64, V.LM_DTYPE)
     cnt = np.zeros(nfr, np.int32)
 
     def fresh(with_blob, verify=False):
@@ -324,7 +330,8 @@ def batched_arm(V, steps, warmup, timed, frames):
     fb = [w * h for w, h in sizes]
     pitches = [w for w, _ in sizes]
     n = len(sizes)
-    out = np.zeros(frames * n * 800 + 64, V.LM_DTYPE)
+    per = [records_per_frame(w, h) for w, h in sizes]
+    out = np.zeros(frames * sum(per) + 64, V.LM_DTYPE)
     counts = np.zeros(frames * n, np.int32)
     b = V.Batch([w for w, _ in sizes], [h for _, h in sizes])
     tot = b.run(ptrs, fb, pitches, frames, True, out, counts)  # fresh streams: the parity run
@@ -344,7 +351,7 @@ def batched_arm(V, steps, warmup, timed, frames):
     # every stream through a detector of its own, one after another; the
     # first (untimed) pass checks every stream against the batch
     dets = [V.MotionDetector(w, h, V.PF_YUV420P) for w, h in sizes]
-    rec = np.zeros(frames * 800 + 64, V.LM_DTYPE)
+    rec = np.zeros(frames * max(per) + 64, V.LM_DTYPE)
     cnt = np.zeros(frames, np.int32)
     same = 0
     for s in range(n):
@@ -367,7 +374,7 @@ def batched_arm(V, steps, warmup, timed, frames):
         run_all()
     ts = timed(run_all, steps)
     # the same detectors stepped together by one host thread (vsb_detect_multi)
-    mout = np.zeros(frames * n * 800 + 64, V.LM_DTYPE)
+    mout = np.zeros(frames * sum(per) + 64, V.LM_DTYPE)
     mcnt = np.zeros(frames * n, np.int32)
     for _ in range(warmup):
         V.detect_multi(dets, ptrs, fb, pitches, frames, True, mout, mcnt)
@@ -404,7 +411,7 @@ def shake4k_arm(V, steps, warmup, timed, frames):
     ptrs = [c.data_ptr() for c in clips]
     fb, pt = [w * h] * n, [w] * n
     blob = pnet.load_blob()
-    out = np.zeros(frames * n * 1200 + 64, V.LM_DTYPE)
+    out = np.zeros(frames * n * records_per_frame(w, h) + 64, V.LM_DTYPE)
     counts = np.zeros(frames * n, np.int32)
 
     def dets(learned, verify=False):
@@ -620,7 +627,7 @@ def main():
     # one detector per arm, initialised before timing (vsMotionDetectInit:
     # device buffers, tiling lookup); each step runs the clip's frames through
     # it in C and copies every LocalMotion into a preallocated record buffer
-    rec = np.zeros(nfr * 512 + 64, V.LM_DTYPE)
+    rec = np.zeros(nfr * records_per_frame(W, H) + 64, V.LM_DTYPE)
     cnt = np.zeros(nfr, np.int32)
     det_dev = V.MotionDetector(W, H, V.PF_YUV420P)
     det_host = V.MotionDetector(W, H, V.PF_YUV420P)

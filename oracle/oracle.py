@@ -161,6 +161,12 @@ def oracle_clip(frames, pformat=1, **kw):
     return (np.concatenate(recs) if recs else np.zeros(0, LM_DTYPE)), np.array(counts, np.int32)
 
 
+def records_per_frame(width, height):
+    """an upper bound of the LocalMotions one frame can give: every coarse
+    and every fine field (fine fields are at least 16 pixels apart)"""
+    return 256 + (width // 16 + 1) * (height // 16 + 1)
+
+
 def ref_clip(frames, pformat=1, stepsize=6, accuracy=15, shakiness=5, mincontrast=0.25, tripod=0,
              show=0, threads=1, serialization_mode=0, trf_path=None, return_frames=False):
     """The unmodified reference's public detect API over a clip (CPU)."""
@@ -168,7 +174,7 @@ def ref_clip(frames, pformat=1, stepsize=6, accuracy=15, shakiness=5, mincontras
     frames = np.ascontiguousarray(frames, np.uint8)
     n, H = frames.shape[0], frames.shape[1]
     W = frames.shape[2] // _bpp(pformat)
-    cap = n * 512 + 64
+    cap = n * records_per_frame(W, H) + 64
     out = np.zeros(cap, LM_DTYPE)
     counts = np.zeros(n, np.int32)
     el = C.c_double(0)
@@ -179,6 +185,8 @@ def ref_clip(frames, pformat=1, stepsize=6, accuracy=15, shakiness=5, mincontras
                                 _p(out), cap, _p(counts), C.byref(el), _p(drawn))
     if total < 0:
         raise RuntimeError("reference detect failed")
+    if total > cap:
+        raise RuntimeError("reference detect: %d records do not fit the buffer of %d" % (total, cap))
     res = (out[:total].copy(), counts, el.value)
     if return_frames:
         res = res + (drawn,)

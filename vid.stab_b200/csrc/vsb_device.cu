@@ -15,7 +15,6 @@
  *               dependent refinement rounds and the range test
  *               (src/motiondetect.c:439-586 planar, :591-660 packed).
  */
-#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 #include <pthread.h>
 #include <stdint.h>
@@ -770,80 +769,9 @@ static int sweep_candidates(const DGeom& g, int nitems, TileCand* out, int cap) 
   return n;
 }
 
-/* cuTensorMapEncodeTiled of the driver, resolved through the runtime */
-static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder(void) {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = NULL;
-  static pthread_mutex_t lock = PTHREAD_MUTEX_INITIALIZER;
-  pthread_mutex_lock(&lock);
-  if (!fn) {
-    void* p = NULL;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
-            cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
-  }
-  pthread_mutex_unlock(&lock);
-  return fn;
-}
-
-/* A tensor map viewing a plane (row pitch `pitch`, H rows) as
-   [H][pitch/16][16] bytes with boxes of box1 16-byte chunks x box2 rows;
-   the last few maps built on this thread are kept. */
-static int sweep_map(CUtensorMap* out, const uint8_t* plane, int pitch, int H, int box1,
-                     int box2) {
-  struct Entry {
-    const uint8_t* plane;
-    int pitch, H, box1, box2;
-    CUtensorMap map;
-  };
-  static thread_local Entry cache[8];
-  static thread_local int next = 0;
-  for (int i = 0; i < 8; i++) {
-    const Entry& c = cache[i];
-    if (c.plane == plane && c.pitch == pitch && c.H == H && c.box1 == box1 && c.box2 == box2) {
-      *out = c.map;
-      return 0;
-    }
-  }
-  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
-  if (!enc) {
-    set_msg("cuTensorMapEncodeTiled is not available from the driver");
-    return -1;
-  }
-  if ((pitch & 15) || ((uintptr_t)plane & 15) || box1 < 1 || box1 > 256 || box2 < 1 ||
-      box2 > 256) {
-    set_msg("tensor map of a plane: unaligned plane or box out of range");
-    return -1;
-  }
-  cuuint64_t dims[3] = { 16, (cuuint64_t)(pitch / 16), (cuuint64_t)H };
-  cuuint64_t strides[2] = { 16, (cuuint64_t)pitch };
-  cuuint32_t box[3] = { 16, (cuuint32_t)box1, (cuuint32_t)box2 };
-  cuuint32_t es[3] = { 1, 1, 1 };
-  Entry& c = cache[next];
-  const CUresult r = enc(&c.map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, (void*)plane, dims, strides,
-                         box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                         CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) {
-    c.plane = NULL;
-    char m[96];
-    snprintf(m, sizeof(m), "cuTensorMapEncodeTiled failed (%d)", (int)r);
-    set_msg(m);
-    return -1;
-  }
-  c.plane = plane;
-  c.pitch = pitch;
-  c.H = H;
-  c.box1 = box1;
-  c.box2 = box2;
-  *out = c.map;
-  next = (next + 1) & 7;
-  return 0;
-}
-
 template <int NQ, int STEP>
 static int launch_sweep_t(const DGeom& g, size_t smem, int slot, const uint8_t* curr,
-                          const uint8_t* prev, int pitch, int H, const vsbd_item* d_items, int n,
+                          const uint8_t* prev, int pitch, const vsbd_item* d_items, int n,
                           unsigned long long* keys, unsigned* tickets, vsbd_result* d_res,
                           unsigned* err, cudaStream_t st) {
   cudaError_t e = ensure_smem((const void*)k_sweep<NQ, STEP>, slot, smem);
@@ -851,12 +779,7 @@ static int launch_sweep_t(const DGeom& g, size_t smem, int slot, const uint8_t* 
     set_err("cudaFuncSetAttribute(k_sweep)", e);
     return -1;
   }
-  const SweepLayout L = sweep_layout(g);
-  CUtensorMap tw, tf;
-  if (sweep_map(&tw, prev, pitch, H, L.WPc, STEP) != 0 ||
-      sweep_map(&tf, curr, pitch, H, NQ + 1, g.S) != 0)
-    return -1;
-  k_sweep<NQ, STEP><<<g.ctas, g.threads, smem, st>>>(tw, tf, prev, pitch, g, d_items, n, keys,
+  k_sweep<NQ, STEP><<<g.ctas, g.threads, smem, st>>>(curr, prev, pitch, g, d_items, n, keys,
                                                      tickets, d_res, err);
   e = cudaGetLastError();
   if (e != cudaSuccess) {
@@ -869,10 +792,9 @@ static int launch_sweep_t(const DGeom& g, size_t smem, int slot, const uint8_t* 
   return 1;
 }
 
-/* the sweep of items[0 .. n) with plan g (ta == 5) over planes of H rows;
-   err: a device-visible word the kernel raises when a wait for its copies
-   runs out */
-static int launch_sweep(const DGeom& g, const uint8_t* curr, const uint8_t* prev, int pitch, int H,
+/* the sweep of items[0 .. n) with plan g (ta == 5); err: a device-visible
+   word the kernel raises when a wait for its copies runs out */
+static int launch_sweep(const DGeom& g, const uint8_t* curr, const uint8_t* prev, int pitch,
                         const vsbd_item* d_items, int n, unsigned long long* keys,
                         unsigned* tickets, vsbd_result* d_res, unsigned* err, cudaStream_t st) {
   if (n <= 0) return 0;
@@ -885,7 +807,7 @@ static int launch_sweep(const DGeom& g, const uint8_t* curr, const uint8_t* prev
   int slot = 40;
 #define VSB_SW_LAUNCH(ST, NQv)                                                                  \
   if (g.step == ST && NQ == NQv)                                                                \
-    return launch_sweep_t<NQv, ST>(g, smem, slot, curr, prev, pitch, H, d_items, n, keys,       \
+    return launch_sweep_t<NQv, ST>(g, smem, slot, curr, prev, pitch, d_items, n, keys,          \
                                    tickets, d_res, err, st);                                    \
   slot++;
   VSB_SWEEP_CASES(VSB_SW_LAUNCH)
@@ -1155,7 +1077,7 @@ static SweepTune g_swtune[64];
 static int g_nswtune = 0;
 
 static int autotune_sweep(const GeomDev& gd, const uint8_t* curr, const uint8_t* prev, int pitch,
-                          int H, const vsbd_item* d_items, int n, unsigned long long* keys,
+                          const vsbd_item* d_items, int n, unsigned long long* keys,
                           unsigned* tickets, vsbd_result* d_res, unsigned* err,
                           volatile unsigned* h_err, cudaStream_t st, DGeom* plan, int* on) {
   *on = 0;
@@ -1185,7 +1107,7 @@ static int autotune_sweep(const GeomDev& gd, const uint8_t* curr, const uint8_t*
     CK(cudaEventCreate(&e1));
     auto time_of = [&](const DGeom* sw, int reps) -> float {
       auto one = [&]() {
-        return sw ? launch_sweep(*sw, curr, prev, pitch, H, d_items, n, keys, tickets, d_res, err,
+        return sw ? launch_sweep(*sw, curr, prev, pitch, d_items, n, keys, tickets, d_res, err,
                                  st)
                   : launch_search(gd, curr, prev, pitch, d_items, n, keys, tickets, d_res, st);
       };
@@ -1692,10 +1614,10 @@ extern "C" int vsbd_create(vsbd_ctx** out, int W, int H, int bpp, int blur_size,
   CKC(cudaHostAlloc(&c->h_swerr, 2 * sizeof(unsigned), cudaHostAllocMapped));
   c->h_swerr[0] = c->h_swerr[1] = 0;
   CKC(cudaHostGetDevicePointer((void**)&c->d_swerr, c->h_swerr, 0));
-  if (autotune_sweep(c->gc, c->d_buf[0], c->d_buf[1], c->pitch, c->H, c->d_citems, nc, c->d_keys,
+  if (autotune_sweep(c->gc, c->d_buf[0], c->d_buf[1], c->pitch, c->d_citems, nc, c->d_keys,
                      c->d_tickets, (vsbd_result*)(c->d_out + c->off_coarse), c->d_swerr,
                      c->h_swerr, c->st, &c->swc, &c->sw_c) != 0 ||
-      autotune_sweep(c->gf, c->d_buf[0], c->d_buf[1], c->pitch, c->H, c->d_fitems, nf,
+      autotune_sweep(c->gf, c->d_buf[0], c->d_buf[1], c->pitch, c->d_fitems, nf,
                      c->d_keys + nc, c->d_tickets + nc, (vsbd_result*)(c->d_out + c->off_fine),
                      c->d_swerr + 1, c->h_swerr + 1, c->st, &c->swf, &c->sw_f) != 0) {
     vsbd_destroy(c);
@@ -1883,7 +1805,7 @@ static int stage_a_issue(vsbd_ctx* c, const uint8_t* host, int linesize, const u
       int nl = c->mode ? launch_pruned(c->gc, c->gcp, cur, prv, c->pitch, c->d_citems, c->nc,
                                        c->d_skip, c->d_part, c->d_counts, c->d_lists, c->d_boxes,
                                        c->d_keys, c->d_tickets, cres, st)
-               : c->sw_c ? launch_sweep(c->swc, cur, prv, c->pitch, c->H, c->d_citems, c->nc, c->d_keys,
+               : c->sw_c ? launch_sweep(c->swc, cur, prv, c->pitch, c->d_citems, c->nc, c->d_keys,
                                         c->d_tickets, cres, c->d_swerr, st)
                        : launch_search(c->gc, cur, prv, c->pitch, c->d_citems, c->nc, c->d_keys,
                                        c->d_tickets, cres, st);
@@ -2018,7 +1940,7 @@ extern "C" int vsbd_stage_b_issue(vsbd_ctx* c, const vsbd_item* items, int n) {
                                      c->d_part, c->d_counts + c->nc, c->d_lists,
                                      c->d_boxes + 4 * c->nc, c->d_keys + c->nc,
                                      c->d_tickets + c->nc, fres, st)
-             : c->sw_f ? launch_sweep(c->swf, cur, prv, c->pitch, c->H, c->d_fitems, n, c->d_keys + c->nc,
+             : c->sw_f ? launch_sweep(c->swf, cur, prv, c->pitch, c->d_fitems, n, c->d_keys + c->nc,
                                       c->d_tickets + c->nc, fres, c->d_swerr + 1, st)
                      : launch_search(c->gf, cur, prv, c->pitch, c->d_fitems, n, c->d_keys + c->nc,
                                      c->d_tickets + c->nc, fres, st);
@@ -2335,7 +2257,7 @@ extern "C" int vsbd_search_host(const uint8_t* curr, const uint8_t* prev, int W,
   cudaMemcpy2D(d_p, pitch, prev, (size_t)W * bpp, (size_t)W * bpp, H, cudaMemcpyHostToDevice);
   cudaMemcpy(d_items, items, sizeof(vsbd_item) * n, cudaMemcpyHostToDevice);
   if (tiles_hint < 0) {
-    if (launch_sweep(swg, d_c, d_p, pitch, H, d_items, n, d_keys, d_tk, d_res, d_err, 0) < 0)
+    if (launch_sweep(swg, d_c, d_p, pitch, d_items, n, d_keys, d_tk, d_res, d_err, 0) < 0)
       goto done;
     if ((e = cudaMemcpy(&h_err, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost)) != cudaSuccess) { set_err("k_sweep", e); goto done; }
     if (h_err) { set_msg("search sweep: a wait for staged rows gave up"); goto done; }

@@ -8,12 +8,9 @@
  * The kernel is persistent: CTA c takes the tiles [c*T/G, (c+1)*T/G) of the
  * T tiles of the launch in order, so consecutive tiles mostly share a field.
  * Each tile's previous-frame window (and, when the field changes, the
- * current frame's field rows) is staged in shared memory by the TMA unit
- * from tensor maps over the blurred planes: the plane is viewed as
- * [rows][16-byte chunks][16 bytes], so one box spans a whole window row
- * (up to 256 chunks) and STEP rows; the field is one box.  The copies
- * complete on an mbarrier.  Two buffers: tile k+1's copies are in flight
- * while tile k is summed.
+ * current frame's field rows) is staged in shared memory by the TMA unit:
+ * one cp.async.bulk per row, completing on an mbarrier.  Two buffers: tile
+ * k+1's copies are in flight while tile k is summed.
  *
  * Sums.  A thread owns 8 consecutive lattice columns of one lattice row and
  * a strip of the field's rows.  Its columns start at byte E + c*STEP of a
@@ -45,7 +42,6 @@
 #ifndef VSB_SWEEP_CUH
 #define VSB_SWEEP_CUH
 
-#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -70,19 +66,18 @@ __host__ __device__ constexpr int sw_chunks(int STEP, int NQ) {
 }
 
 /* shared-memory layout of the sweep for a tiling (g.ncg = g.nab / 8
-   column groups, g.nbb lattice rows, g.nstrip strips).  The window is
-   staged in groups of STEP rows (one tensor box each), D chunks apart so
-   that every box starts on a 128-byte boundary; rows of a group are WPc
-   chunks apart. */
+   column groups, g.nbb lattice rows, g.nstrip strips) */
 struct SweepLayout {
-  int NQ, WPc, D, NG, WH, FR, FCP;
+  int NQ, WPc, X, WH, FR, FCP;
   size_t win_bytes, fraw_bytes, fc_bytes;
   size_t off_win[2], off_fraw[2], off_fc, off_part, off_q, total;
 };
 
-/* chunk offset of window row r */
-__host__ __device__ inline int sw_row_off(int r, int WPc, int D, int step) {
-  return (r / step) * D + (r % step) * WPc;
+/* chunk offset of window row r: rows STEP apart differ by an odd multiple
+   of the thread stride, so the 16-byte loads of 8 consecutive threads hit
+   distinct bank groups */
+__host__ __device__ inline int sw_row_off(int r, int WPc, int X, int step) {
+  return r * WPc + (r / step) * X;
 }
 
 __host__ __device__ inline SweepLayout sweep_layout(const DGeom& g) {
@@ -91,12 +86,11 @@ __host__ __device__ inline SweepLayout sweep_layout(const DGeom& g) {
   const int ncg = g.nab / SW_TA;
   const int cs = g.step / 2; /* chunks between column groups */
   L.WPc = (ncg - 1) * cs + sw_chunks(g.step, L.NQ);
-  L.D = (g.step * L.WPc + 7) & ~7;
+  L.X = (((cs * ncg - g.step * L.WPc) % 8) + 8) % 8;
   L.WH = g.S + (g.nbb - 1) * g.step;
-  L.NG = (L.WH + g.step - 1) / g.step;
   L.FR = g.S + 16;
   L.FCP = (L.NQ + 1) * 16;
-  L.win_bytes = (size_t)16 * L.D * L.NG;
+  L.win_bytes = (size_t)16 * (sw_row_off(L.WH - 1, L.WPc, L.X, g.step) + L.WPc);
   /* the refinement window of a field reuses a tile buffer */
   const int R = refine_reach(g);
   const size_t rwin = (size_t)(g.S + 2 * R) * (((3 + g.S + 2 * R + 8 + 15) >> 4) << 4) + 16;
@@ -110,7 +104,7 @@ __host__ __device__ inline SweepLayout sweep_layout(const DGeom& g) {
   L.off_fraw[1] = L.off_fraw[0] + L.fraw_bytes;
   L.off_fc = L.off_fraw[1] + L.fraw_bytes;
   L.off_part = L.off_fc + L.fc_bytes;
-  L.off_q = L.off_part + (size_t)(g.nstrip > 1 ? g.nstrip - 1 : 0) * ncg * g.nbb * SW_TA * 4;
+  L.off_q = L.off_part + (size_t)g.nstrip * ncg * g.nbb * SW_TA * 4;
   L.total = L.off_q + (size_t)g.maxq * 4 + 16;
   return L;
 }
@@ -177,17 +171,6 @@ __device__ __forceinline__ void sw_bulk_load(void* dst, const void* src, unsigne
       : "memory");
 }
 
-/* one box of a 3-D tensor map (coordinates innermost first) into shared
-   memory (128-byte aligned), completing on bar */
-__device__ __forceinline__ void sw_box_load(void* dst, const CUtensorMap* map, int c0, int c1,
-                                            int c2, uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(sw_smem_addr(dst)),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(sw_smem_addr(bar))
-      : "memory");
-}
-
 /* generic-proxy accesses of shared memory before the async proxy's writes */
 __device__ __forceinline__ void sw_fence_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -215,36 +198,36 @@ __device__ __forceinline__ bool sw_bar_wait(uint64_t* bar, unsigned parity) {
   return false;
 }
 
-/* row groups (boxes) of tile T's window */
+/* bytes tile T's copies bring: its window rows and, with field, the rows
+   of its field in the current frame */
 template <int STEP>
-__device__ __forceinline__ int sweep_groups(const DGeom& g, const SweepTile& T) {
-  return (g.S + (T.nb_t - 1) * STEP + STEP - 1) / STEP;
+__device__ __forceinline__ unsigned sweep_bytes(const DGeom& g, const SweepTile& T, bool field) {
+  const int nvec = (T.e + (T.na_t - 1) * STEP + g.S + 15) >> 4;
+  const int wh = g.S + (T.nb_t - 1) * STEP;
+  const int nvf = (T.ce + g.S + 15) >> 4;
+  return (unsigned)(wh * nvec * 16 + (field ? g.S * nvf * 16 : 0));
 }
 
-/* bytes tile T's boxes bring: its window's row groups (WPc chunks x STEP
-   rows each) and, with field, the field box ((NQ+1) chunks x S rows) */
-template <int STEP>
-__device__ __forceinline__ unsigned sweep_bytes(const DGeom& g, const SweepLayout& L,
-                                                const SweepTile& T, bool field) {
-  return (unsigned)(sweep_groups<STEP>(g, T) * 16 * L.WPc * STEP + (field ? L.FR * g.S : 0));
-}
-
-/* Issues tile T's boxes into a buffer, one box per thread of the first
-   warps; the buffer's mbarrier already expects their bytes (sweep_bytes).
-   tm_win: the previous plane with boxes of WPc chunks x STEP rows; tm_fld:
-   the current plane with boxes of NQ+1 chunks x S rows.  Boxes reaching
-   past the plane are filled with zeros by the TMA unit. */
+/* Issues tile T's copies into a buffer, one row per copy, the rows spread
+   over all threads of the CTA (issuing a copy costs its thread time, so no
+   warp carries them all); the buffer's mbarrier already expects their bytes
+   (sweep_bytes). */
 template <int STEP>
 __device__ __forceinline__ void sweep_copies(const DGeom& g, const SweepLayout& L, const SweepTile& T,
-                                             bool field, const CUtensorMap* tm_win,
-                                             const CUtensorMap* tm_fld, uint8_t* win,
-                                             uint8_t* fraw, uint64_t* bar) {
-  const int ng = sweep_groups<STEP>(g, T);
-  for (int k = threadIdx.x; k < ng + (field ? 1 : 0); k += blockDim.x) {
-    if (k < ng)
-      sw_box_load(win + (size_t)16 * L.D * k, tm_win, 0, T.gx0a >> 4, T.gy0 + k * STEP, bar);
+                                             bool field, const uint8_t* __restrict__ curr,
+                                             const uint8_t* __restrict__ prev, int pitch,
+                                             uint8_t* win, uint8_t* fraw, uint64_t* bar) {
+  const int nvec = (T.e + (T.na_t - 1) * STEP + g.S + 15) >> 4;
+  const int wh = g.S + (T.nb_t - 1) * STEP;
+  const int nvf = (T.ce + g.S + 15) >> 4;
+  const int nrows = wh + (field ? g.S : 0);
+  for (int r = threadIdx.x; r < nrows; r += blockDim.x) {
+    if (r < wh)
+      sw_bulk_load(win + 16 * sw_row_off(r, L.WPc, L.X, STEP),
+                   prev + (size_t)(T.gy0 + r) * pitch + T.gx0a, (unsigned)nvec * 16u, bar);
     else
-      sw_box_load(fraw, tm_fld, 0, T.cx0a >> 4, T.cy0, bar);
+      sw_bulk_load(fraw + (size_t)(r - wh) * L.FR,
+                   curr + (size_t)(T.cy0 + r - wh) * pitch + T.cx0a, (unsigned)nvf * 16u, bar);
   }
 }
 
@@ -288,7 +271,7 @@ __device__ __forceinline__ void sweep_field_copies(const DGeom& g, const SweepLa
    wr0 .. wr0+Rs-1.  fA / fB: the field copies of the even / odd columns. */
 template <int NQ, int STEP, int E>
 __device__ __forceinline__ void sweep_sums(unsigned (&acc)[SW_TA], const uint8_t* __restrict__ win,
-                                           int WPc, int D, int cgoff, int wr0,
+                                           int WPc, int X, int cgoff, int wr0,
                                            const uint8_t* __restrict__ fA,
                                            const uint8_t* __restrict__ fB, int FCP, int r0,
                                            int Rs) {
@@ -297,7 +280,7 @@ __device__ __forceinline__ void sweep_sums(unsigned (&acc)[SW_TA], const uint8_t
   const uint4* __restrict__ W0 = (const uint4*)win + cgoff;
   for (int r = 0; r < Rs; r++) {
     const int wr = wr0 + r;
-    const uint4* __restrict__ W4 = W0 + sw_row_off(wr, WPc, D, STEP);
+    const uint4* __restrict__ W4 = W0 + sw_row_off(wr, WPc, X, STEP);
     const uint4* __restrict__ FA4 = (const uint4*)(fA + (size_t)(r0 + r) * FCP);
     const uint4* __restrict__ FB4 = (const uint4*)(fB + (size_t)(r0 + r) * FCP);
     uint32_t w[4 * NCH];
@@ -351,11 +334,11 @@ __device__ __forceinline__ void sweep_sums(unsigned (&acc)[SW_TA], const uint8_t
 
 template <int NQ, int STEP>
 __device__ __forceinline__ void sweep_sums_e(int E, unsigned (&acc)[SW_TA], const uint8_t* win,
-                                             int WPc, int D, int cgoff, int wr0,
+                                             int WPc, int X, int cgoff, int wr0,
                                              const uint8_t* fA, const uint8_t* fB, int FCP,
                                              int r0, int Rs) {
 #define SW_E(v) \
-  case v: sweep_sums<NQ, STEP, v>(acc, win, WPc, D, cgoff, wr0, fA, fB, FCP, r0, Rs); break;
+  case v: sweep_sums<NQ, STEP, v>(acc, win, WPc, X, cgoff, wr0, fA, fB, FCP, r0, Rs); break;
   switch (E) {
     SW_E(0) SW_E(1) SW_E(2) SW_E(3) SW_E(4) SW_E(5) SW_E(6) SW_E(7)
     SW_E(8) SW_E(9) SW_E(10) SW_E(11) SW_E(12) SW_E(13) SW_E(14) SW_E(15)
@@ -364,12 +347,10 @@ __device__ __forceinline__ void sweep_sums_e(int E, unsigned (&acc)[SW_TA], cons
 }
 
 /* grid: g.ctas persistent CTAs; block g.threads; dynamic shared memory
-   sweep_layout(g).total.  Tiles of items[0 .. n).  tm_win / tm_fld: tensor
-   maps of prev / curr (sweep_map). */
+   sweep_layout(g).total.  Tiles of items[0 .. n). */
 template <int NQ, int STEP>
 __global__ void __launch_bounds__(SW_MAX_THREADS, 1)
-    k_sweep(const __grid_constant__ CUtensorMap tm_win, const __grid_constant__ CUtensorMap tm_fld,
-            const uint8_t* __restrict__ prev, int pitch, DGeom g,
+    k_sweep(const uint8_t* __restrict__ curr, const uint8_t* __restrict__ prev, int pitch, DGeom g,
             const vsbd_item* __restrict__ items, int n, unsigned long long* __restrict__ keys,
             unsigned* __restrict__ tickets, vsbd_result* __restrict__ res, unsigned* err) {
   extern __shared__ __align__(128) uint8_t sm[];
@@ -398,13 +379,13 @@ __global__ void __launch_bounds__(SW_MAX_THREADS, 1)
     sw_bar_init_fence();
     for (int k = 0; k < 2 && k < nmine; k++) {
       const SweepTile Tt = sweep_tile(g, items, t_begin + k);
-      sw_bar_expect(&bars[k], sweep_bytes<STEP>(g, L, Tt, needs_field(t_begin + k, Tt)));
+      sw_bar_expect(&bars[k], sweep_bytes<STEP>(g, Tt, needs_field(t_begin + k, Tt)));
     }
   }
   __syncthreads();
   for (int k = 0; k < 2 && k < nmine; k++) {
     const SweepTile Tt = sweep_tile(g, items, t_begin + k);
-    sweep_copies<STEP>(g, L, Tt, needs_field(t_begin + k, Tt), &tm_win, &tm_fld,
+    sweep_copies<STEP>(g, L, Tt, needs_field(t_begin + k, Tt), curr, prev, pitch,
                        sm + L.off_win[k], sm + L.off_fraw[k], &bars[k]);
   }
   /* thread task: column group, lattice row of the tile, field strip */
@@ -445,35 +426,29 @@ __global__ void __launch_bounds__(SW_MAX_THREADS, 1)
     if (active) {
       const uint8_t* fA = fc + (size_t)(sA ? 1 : 0) * g.S * L.FCP;
       const uint8_t* fB = fc + (size_t)(sB ? 2 : 0) * g.S * L.FCP;
-      sweep_sums_e<NQ, STEP>(T.e, acc, win, L.WPc, L.D, cg * (STEP / 2), st * Rs + bl * STEP, fA,
+      sweep_sums_e<NQ, STEP>(T.e, acc, win, L.WPc, L.X, cg * (STEP / 2), st * Rs + bl * STEP, fA,
                              fB, L.FCP, st * Rs, Rs);
     }
-    /* the strips' partial sums */
-    if (g.nstrip > 1) {
-      if (active && st > 0) {
-        uint4* p = (uint4*)(part + ((size_t)(st - 1) * tps + rem) * SW_TA);
-        p[0] = make_uint4(acc[0], acc[1], acc[2], acc[3]);
-        p[1] = make_uint4(acc[4], acc[5], acc[6], acc[7]);
-      }
-      __syncthreads();
-      if (active && st == 0)
-        for (int s2 = 1; s2 < g.nstrip; s2++) {
-          const uint4* p = (const uint4*)(part + ((size_t)(s2 - 1) * tps + rem) * SW_TA);
-          const uint4 u = p[0], v = p[1];
-          acc[0] += u.x; acc[1] += u.y; acc[2] += u.z; acc[3] += u.w;
-          acc[4] += v.x; acc[5] += v.y; acc[6] += v.z; acc[7] += v.w;
-        }
+    /* every strip's partial sums go to shared memory; then the whole CTA
+       totals the tile's candidates over the strips, each thread a few, and
+       keeps the lowest (SAD, rank) */
+    if (active) {
+      uint4* p = (uint4*)(part + ((size_t)st * tps + rem) * SW_TA);
+      p[0] = make_uint4(acc[0], acc[1], acc[2], acc[3]);
+      p[1] = make_uint4(acc[4], acc[5], acc[6], acc[7]);
     }
-    /* the tile's lowest (SAD, rank) */
+    __syncthreads();
     unsigned long long best = ~0ull;
-    if (active && st == 0 && bl < T.nb_t) {
-      const int32_t* ord = g.order + (size_t)(T.b0 + bl) * g.na + T.a0 + cg * SW_TA;
-#pragma unroll
-      for (int c = 0; c < SW_TA; c++)
-        if (cg * SW_TA + c < T.na_t) {
-          const unsigned long long key = ((unsigned long long)acc[c] << 32) | (unsigned)ord[c];
-          best = key < best ? key : best;
-        }
+    for (int q = threadIdx.x; q < tps * SW_TA; q += blockDim.x) {
+      const int r2 = q / SW_TA, c = q - r2 * SW_TA;
+      const int bl2 = r2 / ncg, cg2 = r2 - bl2 * ncg;
+      if (bl2 >= T.nb_t || cg2 * SW_TA + c >= T.na_t) continue;
+      unsigned sum = 0;
+      for (int s2 = 0; s2 < g.nstrip; s2++) sum += part[((size_t)s2 * tps + r2) * SW_TA + c];
+      const unsigned long long key =
+          ((unsigned long long)sum << 32) |
+          (unsigned)g.order[(size_t)(T.b0 + bl2) * g.na + T.a0 + cg2 * SW_TA + c];
+      best = key < best ? key : best;
     }
     best = warp_min64(best);
     if (lane == 0) red[warp] = best;
@@ -498,8 +473,8 @@ __global__ void __launch_bounds__(SW_MAX_THREADS, 1)
                        (unsigned*)(sm + L.off_q));
     }
     /* every thread's reads (and the refinement's writes) of buffer b are
-       ordered before the bulk copies that refill it; the barrier then
-       expects tile k+2's bytes before any copy is issued */
+       ordered before the bulk copies that refill it; the mbarrier expects
+       tile k+2's bytes before any of its copies is issued */
     sw_fence_async_smem();
     const bool more = k + 2 < nmine;
     SweepTile Tn;
@@ -507,11 +482,11 @@ __global__ void __launch_bounds__(SW_MAX_THREADS, 1)
     if (more) {
       Tn = sweep_tile(g, items, tt + 2);
       fn = needs_field(tt + 2, Tn);
-      if (threadIdx.x == 0) sw_bar_expect(&bars[b], sweep_bytes<STEP>(g, L, Tn, fn));
+      if (threadIdx.x == 0) sw_bar_expect(&bars[b], sweep_bytes<STEP>(g, Tn, fn));
     }
     __syncthreads();
     if (more)
-      sweep_copies<STEP>(g, L, Tn, fn, &tm_win, &tm_fld, sm + L.off_win[b], sm + L.off_fraw[b],
+      sweep_copies<STEP>(g, L, Tn, fn, curr, prev, pitch, sm + L.off_win[b], sm + L.off_fraw[b],
                          &bars[b]);
   }
 }

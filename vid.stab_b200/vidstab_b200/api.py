@@ -9,6 +9,18 @@ from ._lib import (LM_DTYPE, PF_PACKED, PF_RGBA, VSFrame, VSFrameInfo, VSMotionD
                    VSVector, lib, ptr, vector_records)
 
 
+def records_per_frame(width, height):
+    """an upper bound of the LocalMotions one frame can give: every coarse
+    and every fine field (fine fields are at least 16 pixels apart)"""
+    return 256 + (width // 16 + 1) * (height // 16 + 1)
+
+
+def _check_fits(total, out):
+    """the C loops copy at most len(out) records but count them all"""
+    if total > len(out):
+        raise ValueError("%d LocalMotions do not fit the record buffer of %d" % (total, len(out)))
+
+
 def bpp_of(pformat):
     if pformat < PF_PACKED:
         return 1
@@ -74,6 +86,7 @@ class MotionDetector:
                                       ptr(counts))
         if total < 0:
             raise RuntimeError("vsb_detect_run failed: %s" % self.L.vsb_last_error().decode())
+        _check_fits(total, out)
         return total
 
     def run_frames(self, n, frames_ptr, frame_bytes, linesize, on_device, out, counts):
@@ -86,6 +99,7 @@ class MotionDetector:
                                          ptr(counts))
         if total < 0:
             raise RuntimeError("vsb_detect_frames failed: %s" % self.L.vsb_last_error().decode())
+        _check_fits(total, out)
         return total
 
     @property
@@ -142,6 +156,7 @@ class Batch:
                                      1 if on_device else 0, ptr(out), len(out), ptr(counts))
         if total < 0:
             raise RuntimeError("vsb_batch_run failed: %s" % self.L.vsb_last_error().decode())
+        _check_fits(total, out)
         return total
 
     def detect(self, planes, pitches, on_device):
@@ -227,6 +242,7 @@ def detect_multi(detectors, clip_ptrs, frame_bytes, pitches, nframes, on_device,
                                1 if on_device else 0, ptr(out), len(out), ptr(counts))
     if total < 0:
         raise RuntimeError("vsb_detect_multi failed: %s" % L.vsb_last_error().decode())
+    _check_fits(total, out)
     return total
 
 
@@ -249,7 +265,7 @@ def detect_clip(frames, pformat=1, stepsize=6, accuracy=15, shakiness=5, mincont
     else:
         n = frames
         H, W, fb, ls, src = height, width, frame_bytes, linesize, on_device_ptr
-    cap = n * 512 + 64
+    cap = n * records_per_frame(W, H) + 64
     out = np.zeros(cap, LM_DTYPE)
     counts = np.zeros(n, np.int32)
     el = C.c_double(0)
@@ -261,6 +277,7 @@ def detect_clip(frames, pformat=1, stepsize=6, accuracy=15, shakiness=5, mincont
                               C.byref(el), ptr(drawn))
     if total < 0:
         raise RuntimeError("vsb_detect_clip failed: %s" % L.vsb_last_error().decode())
+    _check_fits(total, out)
     res = (out[:total].copy(), counts, el.value)
     if return_frames:
         res = res + (drawn,)
