@@ -754,6 +754,7 @@ def main():
     roof = None
     roof_hbm = None
     kernel_ms = None
+    tiling = None
     if rank == 0:
         det = V.MotionDetector(W, H, V.PF_YUV420P)
         L.vsb_set_kernel_timing.argtypes = [C.c_void_p, C.c_int]
@@ -766,6 +767,18 @@ def main():
         cnt = (C.c_long * 6)()
         L.vsb_kernel_times(C.byref(det.md), ms, cnt)
         fc = det.md.fieldscoarse
+        tiling = {}
+        for name, fine in (("coarse", 0), ("fine", 1)):
+            desc = (C.c_int * 8)()
+            L.vsb_search_tiling(C.byref(det.md), fine, desc)
+            tiling[name] = {"kernel": "k_sweep" if desc[1] == 5 else "k_lattice",
+                            "layout": desc[1], "lattice_cols_per_tile": desc[2],
+                            "lattice_rows_per_tile": desc[3], "strips": desc[4],
+                            "threads": desc[5], "smem": desc[6],
+                            ("ctas" if desc[1] == 5 else "ctas_per_field"): desc[7]}
+        bdesc = (C.c_int * 3)()
+        L.vsb_blur_tiling(C.byref(det.md), bdesc)
+        tiling["blur_tile"] = [bdesc[0], bdesc[1]]
         det.close()
         kernel_ms = {n: (ms[i] / cnt[i] if cnt[i] else None) for i, n in
                      enumerate(["blur", "field_minmax", "coarse_search", "fine_search"])}
@@ -785,9 +798,10 @@ def main():
         t_coarse = kernel_ms["coarse_search"] * 1e-3
         achieved = ops / t_coarse / 1e12
         peak = peak_sad.value / 1e12
-        roof = {"kernel": "k_lattice (coarse SAD search, 1080p)", "bound": "int-alu",
+        kname = tiling["coarse"]["kernel"]
+        roof = {"kernel": "%s (coarse SAD search, 1080p)" % kname, "bound": "int-alu",
                 "achieved": achieved, "peak": peak, "unit": "Tbyte-absdiff/s", "frac": achieved / peak,
-                "traffic": traffic_from_profile("k_lattice_coarse_1080p.md"),
+                "traffic": traffic_from_profile("%s_coarse_1080p.md" % kname),
                 "algorithmic_per_launch": ops,
                 "peak_source": "measured live: register-only vabsdiff4 loop (vsb_sad_peak)"}
         hbm, src = peaks()
@@ -831,6 +845,7 @@ def main():
                     "d2h_bytes_per_step": (d1 - d0) // max(args.steps, 1)},
             "gpu_launches": l1 - l0,
             "roofline": roof, "roofline_hbm": roof_hbm, "kernel_ms": kernel_ms,
+            "tiling": tiling,
             "learned": learned, "batched": batched, "large_shake_4k": shake4k,
             "cpu_baseline": cpu, "clocks": clk, "parity": parity, "per_frame": per_frame,
         }

@@ -1422,6 +1422,34 @@ struct BlurTune {
 static BlurTune g_blurtune[64];
 static int g_nblurtune = 0;
 
+/* Every kernel of a detector's frame prefers the largest shared-memory
+   carveout: the search kernels need it, and a small-memory kernel between
+   them (blur, min/max) that asked for a different split would make the SMs
+   reconfigure between launches.  Set once per process (the attribute
+   belongs to the function, per device context). */
+static void prefer_shared_carveout(void) {
+  static int done[VSB_MAX_DEVICES];
+  const int dev = current_device();
+  if (__atomic_load_n(&done[dev], __ATOMIC_RELAXED)) return;
+  const int pref = cudaSharedmemCarveoutMaxShared;
+#define VSB_CARVE(fn) cudaFuncSetAttribute((const void*)(fn), cudaFuncAttributePreferredSharedMemoryCarveout, pref);
+#define VSB_CARVE_BLUR(BW, BH) \
+  VSB_CARVE((k_blur_fast<1, BW, BH>)) VSB_CARVE((k_blur_fast<2, BW, BH>)) VSB_CARVE((k_blur_fast<3, BW, BH>)) \
+  VSB_CARVE((k_blur_fast<4, BW, BH>)) VSB_CARVE((k_blur_fast<5, BW, BH>)) VSB_CARVE((k_blur_fast<6, BW, BH>)) \
+  VSB_CARVE((k_blur_fast<7, BW, BH>)) VSB_CARVE((k_blur_fast<8, BW, BH>))
+  VSB_CARVE_BLUR(256, 32)
+  VSB_CARVE_BLUR(128, 16)
+  VSB_CARVE_BLUR(128, 32)
+  VSB_CARVE_BLUR(64, 32)
+  VSB_CARVE(k_minmax_planar)
+  VSB_CARVE(k_minmax)
+  VSB_CARVE(k_blur)
+#undef VSB_CARVE_BLUR
+#undef VSB_CARVE
+  cudaGetLastError(); /* a hint the device may not take is not an error */
+  __atomic_store_n(&done[dev], 1, __ATOMIC_RELAXED);
+}
+
 static int autotune_blur(vsbd_ctx* c, const uint8_t* src, uint8_t* dst) {
   c->blur_shape = 0;
   c->blur_us = 0.f;
@@ -1607,6 +1635,7 @@ extern "C" int vsbd_create(vsbd_ctx** out, int W, int H, int bpp, int blur_size,
     vsbd_destroy(c);
     return -1;
   }
+  prefer_shared_carveout();
   if (autotune_blur(c, c->d_raw ? c->d_raw : c->d_buf[0], c->d_buf[2]) != 0) {
     vsbd_destroy(c);
     return -1;

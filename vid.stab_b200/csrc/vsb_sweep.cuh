@@ -231,38 +231,169 @@ __device__ __forceinline__ void sweep_copies(const DGeom& g, const SweepLayout& 
   }
 }
 
-/* Builds the field copies of one field from its raw rows: slot 0 the field
-   aligned (shift 0), slot 1 shifted by sA bytes, slot 2 by sB (slots 1 and
-   2 only for nonzero shifts).  Word k of the copy for shift s holds field
-   bytes 4k-s .. 4k-s+3, zero outside the field. */
-__device__ __forceinline__ void sweep_field_copies(const DGeom& g, const SweepLayout& L,
-                                                   const uint8_t* fraw, int ce, int sA, int sB,
+/* Builds the field copies of one field from its raw rows (S = 16*NQ rows of
+   S+16 bytes, the field starting at byte ce): slot 0 the field aligned
+   (shift 0), slot 1 shifted by sA bytes, slot 2 by sB (slots 1 and 2 only
+   for nonzero shifts).  Word k of the copy for shift s holds field bytes
+   4k-s .. 4k-s+3, zero outside the field.  A thread builds one 16-byte
+   quad of a copy row from five raw words. */
+template <int NQ>
+__device__ __forceinline__ void sweep_field_copies(const uint8_t* fraw, int ce, int sA, int sB,
                                                    uint8_t* fc) {
-  const int wpr = L.FCP >> 2; /* words per copy row */
-  const int nw = g.S * wpr;
-  const int rowW = g.S >> 2;
-  for (int i = threadIdx.x; i < 3 * nw; i += blockDim.x) {
-    const int slot = i / nw, j = i - slot * nw;
+  constexpr int S = 16 * NQ, Q = NQ + 1, FRW = (S + 16) / 4, ROWW = 4 * NQ;
+  constexpr int PER_SLOT = S * Q;
+  for (int i = threadIdx.x; i < 3 * PER_SLOT; i += blockDim.x) {
+    const int slot = i / PER_SLOT;
+    const int j = i - slot * PER_SLOT;
+    const int r = j / Q, m = j - r * Q;
     const int s = slot == 0 ? 0 : (slot == 1 ? sA : sB);
     if (slot > 0 && s == 0) continue;
-    const int r = j / wpr, k = j - r * wpr;
-    /* field bytes 4k-s .. 4k-s+3 sit at raw bytes ce+4k-s ..; outside the
-       field they are zero */
-    uint32_t v = 0;
-    if (k <= rowW) {
-      const int b0 = ce + 4 * k - s; /* raw byte of field byte 4k-s */
-      const int a = b0 & ~3, sh = (b0 & 3) * 8;
-      const uint8_t* row = fraw + (size_t)r * L.FR;
-      const uint32_t lo = a >= 0 ? *(const uint32_t*)(row + a) : 0u;
-      const uint32_t hi = a + 4 < L.FR ? *(const uint32_t*)(row + a + 4) : 0u;
-      v = sh ? __funnelshift_r(lo, hi, sh) : lo;
-      /* zero the bytes outside the field: field byte 4k-s+m for m = 0..3 */
-      uint32_t keep = 0xffffffffu;
-      if (k == 0 && s) keep &= 0xffffffffu << (8 * s);
-      if (k == rowW) keep = s ? (0xffffffffu >> (32 - 8 * s)) : 0u;
-      v &= keep;
+    const uint32_t* row = (const uint32_t*)(fraw + (size_t)r * (S + 16));
+    const int b0 = ce + 16 * m - s; /* raw byte of field byte 16m-s (at least -3) */
+    const int a0 = b0 >> 2, sh = (b0 & 3) * 8;
+    uint32_t w[5];
+#pragma unroll
+    for (int t = 0; t < 5; t++) w[t] = (a0 + t >= 0 && a0 + t < FRW) ? row[a0 + t] : 0u;
+    uint32_t v[4];
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+      const int k = 4 * m + t;
+      uint32_t x = sh ? __funnelshift_r(w[t], w[t + 1], sh) : w[t];
+      if (k == 0 && s) x &= 0xffffffffu << (8 * s);
+      if (k == ROWW) x &= s ? (0xffffffffu >> (32 - 8 * s)) : 0u;
+      if (k > ROWW) x = 0u;
+      v[t] = x;
     }
-    ((uint32_t*)(fc + (size_t)slot * g.S * L.FCP))[j] = v;
+    *(uint4*)(fc + (size_t)slot * S * Q * 16 + (size_t)r * Q * 16 + 16 * m) =
+        make_uint4(v[0], v[1], v[2], v[3]);
+  }
+}
+
+/* The refinement of one item by the whole CTA (the rounds of
+   src/motiondetect.c:545-567 after the lattice winner: i outer, j inner,
+   centre skipped, strict <, then the range test of :573-574).  The window
+   the rounds can reach is staged with 16-byte loads into rwin; every
+   round's candidate SADs are split over the threads by (candidate, group
+   of field rows) and totalled in shared memory; thread 0 then scans them
+   in the reference's order.  F0: the aligned field copy ((NQ+1) quads per
+   row).  Resets the item's key and ticket. */
+template <int NQ>
+__device__ void sweep_refine(const DGeom& g, const vsbd_item& it, const uint8_t* F0, uint8_t* rwin,
+                             const uint8_t* __restrict__ prev, int pitch,
+                             unsigned long long* keys, unsigned* tickets, vsbd_result* res,
+                             int item, unsigned* part, unsigned* qsad) {
+  constexpr int S = 16 * NQ, Q = NQ + 1;
+  __shared__ int s_tx, s_ty, s_cx0, s_cy0;
+  __shared__ unsigned s_min;
+  if (threadIdx.x == 0) {
+    const unsigned long long k = atomicAdd(&keys[item], 0ull);
+    const short2 pt = g.point[(unsigned)(k & 0xffffffffu)];
+    s_min = (unsigned)(k >> 32);
+    s_tx = s_cx0 = pt.x;
+    s_ty = s_cy0 = pt.y;
+  }
+  __syncthreads();
+  const int R = refine_reach(g);
+  const int fx0 = it.x - S / 2 + it.ox, fy0 = it.y - S / 2 + it.oy;
+  if (g.nstages > 0) {
+    /* rows fy0 + cy0 - R .. + S + 2R, bytes from fx0 + cx0 - R */
+    const int cx0 = s_cx0, cy0 = s_cy0;
+    const int wx = fx0 + cx0 - R, wy = fy0 + cy0 - R;
+    const int wxa = wx & ~15, off = wx - wxa;
+    const int nc = (off + S + 2 * R + 4 + 15) / 16; /* chunks a row's SADs can read */
+    const int RH = S + 2 * R;
+    const int tot = RH * nc;
+    for (int i0 = threadIdx.x; i0 < tot; i0 += 4 * blockDim.x) {
+      uint4 v[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const int i = i0 + u * blockDim.x;
+        if (i < tot) {
+          const int r = i / nc, c = i - r * nc;
+          v[u] = *(const uint4*)(prev + (size_t)(wy + r) * pitch + wxa + 16 * c);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const int i = i0 + u * blockDim.x;
+        if (i < tot) *(uint4*)(rwin + 16 * (size_t)i) = v[u];
+      }
+    }
+    __syncthreads();
+    const int rp = 16 * nc; /* staged row pitch */
+    for (int st = 0; st < g.nstages; st++) {
+      const int r = g.st_r[st], h = g.st_h[st];
+      const int side = (2 * r) / h + 1, nq = side * side;
+      const int cx = s_tx, cy = s_ty;
+      const int G = (int)blockDim.x / nq; /* row groups */
+      const int t = threadIdx.x;
+      unsigned acc = 0, a1 = 0, a2 = 0, a3 = 0; /* four chains: one per word of a quad */
+      if (G > 0 && t < nq * G) {
+        const int q = t % nq, grp = t / nq;
+        const int i = cx - r + (q / side) * h, j = cy - r + (q % side) * h;
+        if (!(i == cx && j == cy)) {
+          const int bx = off + (i - cx0 + R); /* byte of the candidate's column 0 */
+          const int sh = (bx & 3) * 8;
+          for (int rr = grp; rr < S; rr += G) {
+            const uint32_t* W = (const uint32_t*)(rwin + (size_t)(j - cy0 + R + rr) * rp) + (bx >> 2);
+            const uint4* F = (const uint4*)(F0 + (size_t)rr * Q * 16);
+            uint32_t lo = W[0];
+#pragma unroll
+            for (int qq = 0; qq < NQ; qq++) {
+              const uint4 f = F[qq];
+              const uint32_t w1 = W[4 * qq + 1], w2 = W[4 * qq + 2], w3 = W[4 * qq + 3],
+                             w4 = W[4 * qq + 4];
+              acc = sad4(f.x, sh ? __funnelshift_r(lo, w1, sh) : lo, acc);
+              a1 = sad4(f.y, sh ? __funnelshift_r(w1, w2, sh) : w1, a1);
+              a2 = sad4(f.z, sh ? __funnelshift_r(w2, w3, sh) : w2, a2);
+              a3 = sad4(f.w, sh ? __funnelshift_r(w3, w4, sh) : w3, a3);
+              lo = w4;
+            }
+          }
+          acc += a1 + a2 + a3;
+        } else {
+          acc = 0xffffffffu; /* the centre is not a candidate */
+        }
+        part[grp * nq + q] = acc;
+      }
+      __syncthreads();
+      /* each candidate's total over the row groups (the centre's is never
+         compared) */
+      if (threadIdx.x < nq) {
+        unsigned sd = 0;
+        for (int gg = 0; gg < G; gg++) sd += part[gg * nq + threadIdx.x];
+        qsad[threadIdx.x] = sd;
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        unsigned m = s_min;
+        int tx = cx, ty = cy;
+        for (int q = 0; q < nq; q++) {
+          const int i = cx - r + (q / side) * h, j = cy - r + (q % side) * h;
+          if (i == cx && j == cy) continue;
+          const unsigned sd = qsad[q];
+          if (sd < m) {
+            m = sd;
+            tx = i;
+            ty = j;
+          }
+        }
+        s_min = m;
+        s_tx = tx;
+        s_ty = ty;
+      }
+      __syncthreads();
+    }
+  }
+  if (threadIdx.x == 0) {
+    vsbd_result o;
+    o.sad = s_min;
+    o.tx = (int16_t)s_tx;
+    o.ty = (int16_t)s_ty;
+    o.ok = !(abs(s_tx) >= g.limx || abs(s_ty) >= g.limy);
+    res[item] = o;
+    keys[item] = ~0ull;
+    tickets[item] = 0u;
   }
 }
 
@@ -416,8 +547,23 @@ __global__ void __launch_bounds__(SW_MAX_THREADS, 1)
     }
     const int sA = T.e & 3, sB = (T.e + STEP) & 3;
     if (field) {
-      sweep_field_copies(g, L, sm + L.off_fraw[b], T.ce, sA, sB, fc);
+      sweep_field_copies<NQ>(sm + L.off_fraw[b], T.ce, sA, sB, fc);
       __syncthreads();
+    }
+    /* the rank of each candidate this thread totals after the sums, fetched
+       now so that the load's latency hides behind them */
+    constexpr int RK = 3; /* candidates per thread the prefetch covers */
+    int32_t rank[RK];
+#pragma unroll
+    for (int u = 0; u < RK; u++) {
+      const int q = threadIdx.x + u * (int)blockDim.x;
+      rank[u] = -1;
+      if (q < tps * SW_TA) {
+        const int r2 = q / SW_TA, c = q - r2 * SW_TA;
+        const int bl2 = r2 / ncg, cg2 = r2 - bl2 * ncg;
+        if (bl2 < T.nb_t && cg2 * SW_TA + c < T.na_t)
+          rank[u] = g.order[(size_t)(T.b0 + bl2) * g.na + T.a0 + cg2 * SW_TA + c];
+      }
     }
     const uint8_t* win = sm + L.off_win[b];
     unsigned acc[SW_TA];
@@ -439,15 +585,15 @@ __global__ void __launch_bounds__(SW_MAX_THREADS, 1)
     }
     __syncthreads();
     unsigned long long best = ~0ull;
-    for (int q = threadIdx.x; q < tps * SW_TA; q += blockDim.x) {
+    for (int u = 0, q = threadIdx.x; q < tps * SW_TA; u++, q += blockDim.x) {
       const int r2 = q / SW_TA, c = q - r2 * SW_TA;
       const int bl2 = r2 / ncg, cg2 = r2 - bl2 * ncg;
       if (bl2 >= T.nb_t || cg2 * SW_TA + c >= T.na_t) continue;
       unsigned sum = 0;
       for (int s2 = 0; s2 < g.nstrip; s2++) sum += part[((size_t)s2 * tps + r2) * SW_TA + c];
-      const unsigned long long key =
-          ((unsigned long long)sum << 32) |
-          (unsigned)g.order[(size_t)(T.b0 + bl2) * g.na + T.a0 + cg2 * SW_TA + c];
+      const int32_t rk =
+          u < RK ? rank[u] : g.order[(size_t)(T.b0 + bl2) * g.na + T.a0 + cg2 * SW_TA + c];
+      const unsigned long long key = ((unsigned long long)sum << 32) | (unsigned)rk;
       best = key < best ? key : best;
     }
     best = warp_min64(best);
@@ -466,11 +612,8 @@ __global__ void __launch_bounds__(SW_MAX_THREADS, 1)
          this tile's (now free) buffer as the refinement window */
       __threadfence();
       const vsbd_item it = items[T.item];
-      const int R = refine_reach(g);
-      refine_and_store(g, g.S >> 2, L.FCP >> 2, g.S + 2 * R,
-                       ((3 + g.S + 2 * R + 8 + 15) >> 4) << 4, it, (const uint32_t*)fc,
-                       sm + L.off_win[b] + 16, prev, pitch, keys, tickets, res, T.item,
-                       (unsigned*)(sm + L.off_q));
+      sweep_refine<NQ>(g, it, fc, sm + L.off_win[b], prev, pitch, keys, tickets, res, T.item,
+                       part, (unsigned*)(sm + L.off_q));
     }
     /* every thread's reads (and the refinement's writes) of buffer b are
        ordered before the bulk copies that refill it; the mbarrier expects
