@@ -96,6 +96,7 @@ def parse():
                     help="timed steps of the batched and 4K arms (each a whole 120-frame run)")
     ap.add_argument("--side-warmup", type=int, default=1)
     ap.add_argument("--no-per-frame", action="store_true")
+    ap.add_argument("--no-second-pass", action="store_true")
     ap.add_argument("--profile", choices=["none", "detect", "batch"], default="none")
     ap.add_argument("--width", type=int, default=W)
     ap.add_argument("--height", type=int, default=H)
@@ -463,6 +464,87 @@ def shake4k_arm(V, steps, warmup, timed, frames):
                         "N(0,0.5 deg), zoom N(0,0.2%%), shakiness 10, one shared scene" % frames}
 
 
+def second_pass_arm(V, recs, counts, width, height, steps, warmup, timed):
+    """The second pass (vsLocalmotions2Transforms' fit: one transform per
+    frame, one GPU warp per frame) over the clip's LocalMotions: frames/s with
+    the records resident in device memory (value) and from host records
+    through vsb_motions_to_transforms (e2e, copies included), against the
+    reference's vsLocalmotions2Transforms on the same records (single-threaded
+    there); parity per frame against the reference's transforms."""
+    import ctypes as C
+    import torch
+    import oracle as O
+    L = V.lib()
+    recs = np.ascontiguousarray(recs, V.LM_DTYPE)
+    counts = np.asarray(counts, np.int64)
+    n = len(counts)
+    first = np.zeros(n + 1, np.int64)
+    first[1:] = np.cumsum(counts)
+    d_recs = torch.from_numpy(recs.view(np.uint8).copy()).cuda()
+    d_first = torch.from_numpy(first).cuda()
+    d_out = torch.zeros(n * V.TRANSFORM_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+    maxn = int(counts.max()) if n else 0
+
+    def run_dev():
+        rc = L.vsb_motions_to_transforms_device(d_recs.data_ptr(), d_first.data_ptr(), n, maxn,
+                                                width, height, 0.0, 0, d_out.data_ptr(), None,
+                                                None, st)
+        assert rc == 0, L.vsb_last_error()
+
+    host_out = np.zeros(n, V.TRANSFORM_DTYPE)
+
+    def run_host():
+        rc = L.vsb_motions_to_transforms(recs.ctypes.data, first.ctypes.data, n, width, height,
+                                         0.0, 0, host_out.ctypes.data, None, None)
+        assert rc == 0, L.vsb_last_error()
+
+    for _ in range(max(3, warmup)):
+        run_dev()
+        run_host()
+    dev_t = timed(run_dev, steps)
+    host_t = timed(run_host, steps)
+    dev_out = d_out.cpu().numpy().view(V.TRANSFORM_DTYPE)
+    res = {"value": n * len(dev_t) / sum(dev_t), "unit": "frames/s",
+           "e2e": n * len(host_t) / sum(host_t),
+           "kernel_ms": 1000.0 * min(dev_t), "frames": n, "records": int(len(recs)),
+           "h2d_bytes_per_step": int(recs.nbytes + first.nbytes),
+           "d2h_bytes_per_step": int(n * V.TRANSFORM_DTYPE.itemsize),
+           "launches_per_step": 1,
+           "workload": "the 300-frame clip's LocalMotions (as detected), similarity model, "
+                       "smoothZoom 0, lens estimate off"}
+    mine = np.stack([dev_out["x"], dev_out["y"], dev_out["alpha"], dev_out["zoom"],
+                     dev_out["extra"].astype(np.float64)], 1)
+    if O.ref_available():
+        R = O.ref()
+        R.vsref_motions_to_transforms.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                                  C.c_int, C.c_double, C.c_int, C.c_int,
+                                                  C.c_void_p, C.c_void_p]
+        TD = np.dtype([("x", "<f8"), ("y", "<f8"), ("alpha", "<f8"), ("zoom", "<f8"),
+                       ("barrel", "<f8"), ("rshutter", "<f8"), ("extra", "<i4"), ("pad", "<i4")])
+        ref = np.zeros(n, TD)
+        best = None
+        for _ in range(3):
+            el = C.c_double()
+            R.vsref_motions_to_transforms(width, height, recs.ctypes.data, first.ctypes.data, n,
+                                          0.0, 0, 0, ref.ctypes.data, C.byref(el))
+            best = el.value if best is None else min(best, el.value)
+        refrows = np.stack([ref["x"], ref["y"], ref["alpha"], ref["zoom"],
+                            ref["extra"].astype(np.float64)], 1)
+        res["reference"] = {"value": n / best, "unit": "frames/s", "cores": 1,
+                            "kind": "reference",
+                            "sample": "the same %d frames, vsLocalmotions2Transforms (best of 3)"
+                                      % n}
+        res["parity"] = {"checker": "reference (oracle/_ref)",
+                         "frames_identical": int((mine == refrows).all(1).sum()),
+                         "extra_identical": bool(np.array_equal(mine[:, 4], refrows[:, 4])),
+                         "max_abs_diff": float(np.abs(mine[:, :4] - refrows[:, :4]).max())
+                         if n else 0.0,
+                         "host_equals_device": bool(np.array_equal(host_out.view(np.uint8),
+                                                                   dev_out.view(np.uint8)))}
+    return res
+
+
 def run_reference(args):
     """The reference's own CPU detect (oracle/_ref, compiled from its
     sources) over the same 300-frame clip the GPU arm runs (same generator,
@@ -745,6 +827,9 @@ def main():
         learned = learned_arm(V, clip, host_np, nfr, args.steps, args.warmup, timed_local)
     if rank == 0 and not args.no_batched:
         batched = batched_arm(V, args.side_steps, args.side_warmup, timed_local, args.batch_frames)
+    second = None
+    if rank == 0 and not args.no_second_pass:
+        second = second_pass_arm(V, ref_rec, ref_cnt, W, H, args.steps, args.warmup, timed_local)
     shake4k = None
     if rank == 0 and not args.no_shake4k:
         shake4k = shake4k_arm(V, args.side_steps, args.side_warmup, timed_local,
@@ -847,6 +932,7 @@ def main():
             "roofline": roof, "roofline_hbm": roof_hbm, "kernel_ms": kernel_ms,
             "tiling": tiling,
             "learned": learned, "batched": batched, "large_shake_4k": shake4k,
+            "second_pass": second,
             "cpu_baseline": cpu, "clocks": clk, "parity": parity, "per_frame": per_frame,
         }
         print(json.dumps(line))

@@ -294,6 +294,92 @@ VS_API int vsReadFileVersion(FILE* f, const int serializationMode);    /* :81 */
 VS_API int vsReadFromFile(FILE* f, LocalMotions* lms, const int serializationMode); /* :87 */
 VS_API int vsReadLocalMotionsFile(FILE* f, VSManyLocalMotions* lms);   /* :98 */
 
+/* ---- second pass: local motions -> one global transform per frame --------
+   The transform pass's configuration, read through the caller's pointer, with
+   the reference's member order and sizes (src/transform.h:60-66, :88-160,
+   src/lensmap.h:52-110).  Only fiSrc and conf are read here; the remaining
+   members are declared so that offsets and size agree. */
+typedef enum { VS_Zero, VS_Linear, VS_BiLinear, VS_BiCubic, VS_NBInterPolTypes } VSInterpolType;
+typedef enum { VSKeepBorder = 0, VSCropBorder } VSBorderType;
+typedef enum { VSOptimalL1 = 0, VSGaussian, VSAvg } VSCamPathAlgo;
+typedef enum { VSLensCorrectOff = 0, VSLensCorrectWobble, VSLensCorrectFull } VSLensCorrectMode;
+typedef void (*vsInterpolateFun)(uint8_t* rv, int32_t x, int32_t y, const uint8_t* img,
+                                 int linesize, int width, int height, uint8_t def);
+
+typedef struct _VSTransformConfig {
+  int relative;
+  int smoothing;
+  VSBorderType crop;
+  int invert;
+  double zoom;
+  int optZoom;
+  double zoomSpeed;
+  VSInterpolType interpolType;
+  int maxShift;
+  double maxAngle;
+  const char* modName;
+  int verbose;
+  int simpleMotionCalculation;  /* 1: vsSimpleMotionsToTransform per frame */
+  int storeTransforms;          /* write global_motions.trf */
+  int smoothZoom;               /* 0: the fitted zoom is dropped */
+  VSCamPathAlgo camPathAlgo;
+  int estimateLensDistortion;   /* the lens estimate is not supported: must be 0
+                                   unless simpleMotionCalculation is set */
+  VSLensCorrectMode lensCorrection;
+  double lensK;
+  double fov;                   /* > 0: rotational model, degrees across the width */
+} VSTransformConfig;
+
+typedef struct _vslensplanemap {
+  int active;
+  VSLensCorrectMode mode;
+  double k, cdx, cdy, csx, csy, tMaxU, tMaxD, tDomD, invRho2, f;
+  int sxShift, syShift;
+  int32_t idxScaleU, idxScaleD;
+  int32_t* gU;
+  int32_t* gD;
+} VSLensPlaneMap;
+
+typedef struct _VSTransformData {
+  VSFrameInfo fiSrc;
+  VSFrameInfo fiDest;
+  VSFrame src;
+  VSFrame destbuf;
+  VSFrame dest;
+  short srcMalloced;
+  vsInterpolateFun interpolate;
+  VSTransformConfig conf;
+  VSLensCorrectMode lensMode;
+  int lensActive;
+  double lensK;
+  double lensMapK;
+  VSLensPlaneMap lensMaps[3];
+  int initialized;
+} VSTransformData;
+
+typedef struct _vstransformations {  /* src/transform.h:44-49 */
+  VSTransform* ts;
+  int current;
+  int len;
+  short warned_end;
+} VSTransformations;
+
+/* Fits one transform per frame of `motions` (src/localmotion2transform.c:
+   40-121): the similarity model (or the rotational one when conf.fov > 0) by
+   the reference's masked gradient descent, every frame on the GPU at once; or
+   vsSimpleMotionsToTransform per frame when conf.simpleMotionCalculation is
+   set.  trans->ts is allocated with vs_malloc and trans->len set.  With
+   conf.storeTransforms the per-frame lines of global_motions.trf are written
+   as the reference writes them.  VS_ERROR (and a log line) when
+   conf.estimateLensDistortion is set without simpleMotionCalculation, or on a
+   device failure. */
+VS_API int vsLocalmotions2Transforms(VSTransformData* td, const VSManyLocalMotions* motions,
+                                     VSTransformations* trans);  /* src/localmotion2transform.h:38 */
+/* One frame of the above (src/localmotion2transform.c:220-284); f, when not
+   NULL, receives the frame's global_motions.trf line. */
+VS_API VSTransform vsMotionsToTransform(VSTransformData* td, const LocalMotions* motions,
+                                        FILE* f);               /* src/localmotion2transform.h:65 */
+
 #ifdef __cplusplus
 }
 #endif

@@ -360,6 +360,35 @@ VS_API int vsb_pnet_narrow_host(const uint8_t* curr, const uint8_t* prev, int wi
                                 uint32_t sad_bound, uint32_t* sad, int16_t* tx, int16_t* ty,
                                 int32_t* ok, uint8_t* flags);
 
+/* ---- second pass over many frames (vsLocalmotions2Transforms' fit,
+   src/localmotion2transform.c:137-330, one GPU warp per frame) ---------
+   Frame k's LocalMotions are recs[first[k] .. first[k+1]) (32-byte
+   records).  Per frame: out[k] the transform vsMotionsToTransform returns,
+   residual[k] the final objective value (NaN for a frame without motions),
+   info[3k..3k+2] = gradient-descent rounds as the reference counts them (the
+   last number of its global_motions.trf line), fields disabled for their
+   match quality, fields disabled as outliers.  width/height: the frame;
+   fov: degrees across the width (0: similarity model); smooth_zoom 0 drops
+   the fitted zoom.  residual and info may be NULL.  One frame may hold up to
+   vsb_motions_to_transforms_capacity() motions.  Host pointers; blocking. */
+VS_API int vsb_motions_to_transforms(const LocalMotion* recs, const long* first, int nframes,
+                                     int width, int height, double fov, int smooth_zoom,
+                                     VSTransform* out, double* residual, int* info);
+/* the same on device pointers, enqueued on `stream` (a cudaStream_t or
+   NULL); max_motions: the largest first[k+1] - first[k] (shared memory is
+   sized by it; a frame holding more is not fitted: extra = 1, info rounds
+   -1) */
+VS_API int vsb_motions_to_transforms_device(const LocalMotion* d_recs, const long* d_first,
+                                            int nframes, int max_motions, int width, int height,
+                                            double fov, int smooth_zoom, VSTransform* d_out,
+                                            double* d_residual, int* d_info, void* stream);
+VS_API int vsb_motions_to_transforms_capacity(void);
+/* sizes and member offsets of VSTransformData, VSTransformConfig and
+   VSTransformations, in a fixed order (ABI checks) */
+VS_API int vsb_transform_layout(long* out, int cap);
+/* kernel launches of the second pass since the library was loaded */
+VS_API long vsb_motions_to_transforms_launches(void);
+
 #ifdef __cplusplus
 }
 #endif

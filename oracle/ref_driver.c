@@ -9,8 +9,10 @@
  * clip held in one buffer, and flattens every frame's LocalMotions into
  * plain 32-byte records so that Python can compare them field by field.
  * It also exposes the reference's leaf kernels (blur passes, SAD, contrast,
- * field search) for unit-level pinning of the oracle restatement.
+ * field search) for unit-level pinning of the oracle restatement, and the
+ * second pass (local motions -> per-frame transforms) over a whole clip.
  */
+#include <stddef.h>
 #include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -20,6 +22,7 @@
 #include "motiondetect.h"
 #include "motiondetect_internal.h"
 #include "localmotion2transform.h"
+#include "transform.h"
 #include "serialize.h"
 #include "boxblur.h"
 #include "transformtype_operations.h"
@@ -289,4 +292,134 @@ double vsref_contrast_packed(const uint8_t* I, int linesize, int width, int heig
   md.curr.linesize[0] = linesize;
   f.x = (int16_t)fx; f.y = (int16_t)fy; f.size = (int16_t)size;
   return contrastSubImgPacked(&md, &f);
+}
+
+/* exported by src/localmotion2transform.c:140 but not declared in its header */
+double calcTransformQuality(VSArray params, void* dat);
+
+/* ---- second pass: local motions -> one transform per frame ---------------
+ * Runs the reference's vsLocalmotions2Transforms (src/localmotion2transform.c:
+ * 40-121) over a clip whose frame k holds the records recs[first[k] ..
+ * first[k+1]).  The VSTransformData is the reference's own default transform
+ * configuration (src/transform.c vsTransformGetDefaultConfig) with the lens
+ * estimate switched off and fov / smoothZoom / simpleMotionCalculation set
+ * from the arguments.  *elapsed receives the wall time of the call alone. */
+int vsref_motions_to_transforms(int width, int height, const LocalMotion* recs,
+                                const long* first, int nframes, double fov, int smoothZoom,
+                                int simple, VSTransform* out, double* elapsed) {
+  VSTransformData td;
+  VSManyLocalMotions mlms;
+  VSTransformations trans;
+  int k, rc;
+  quiet_log();
+  memset(&td, 0, sizeof(td));
+  if (!vsFrameInfoInit(&td.fiSrc, width, height, PF_YUV420P)) return -1;
+  td.fiDest = td.fiSrc;
+  td.conf = vsTransformGetDefaultConfig("vsref");
+  td.conf.estimateLensDistortion = 0;
+  td.conf.fov = fov;
+  td.conf.smoothZoom = smoothZoom;
+  td.conf.simpleMotionCalculation = simple;
+  vs_vector_init(&mlms, nframes > 0 ? nframes : 1);
+  for (k = 0; k < nframes; k++) {
+    LocalMotions lms;
+    long i;
+    vs_vector_init(&lms, (int)(first[k + 1] - first[k]) + 1);
+    for (i = first[k]; i < first[k + 1]; i++)
+      vs_vector_append_dup(&lms, (void*)&recs[i], sizeof(LocalMotion));
+    vs_vector_append_dup(&mlms, &lms, sizeof(LocalMotions));
+  }
+  vsTransformationsInit(&trans);
+  double t0 = now_s();
+  rc = vsLocalmotions2Transforms(&td, &mlms, &trans);
+  if (elapsed) *elapsed = now_s() - t0;
+  for (k = 0; rc == VS_OK && k < trans.len && k < nframes; k++) out[k] = trans.ts[k];
+  vsTransformationsCleanup(&trans);
+  for (k = 0; k < vs_vector_size(&mlms); k++) vs_vector_del(VSMLMGet(&mlms, k));
+  vs_vector_del(&mlms);
+  return rc == VS_OK ? 0 : -1;
+}
+
+/* calcTransformQuality (src/localmotion2transform.c:140-172) on one frame's
+ * records with the given mask / missmatch array (updated in place). */
+double vsref_transform_quality(int width, int height, const LocalMotion* recs, int n,
+                               const double* params4, double fov, double* missmatches) {
+  VSTransformData td;
+  LocalMotions lms;
+  struct { VSTransformData* td; const LocalMotions* motions; VSArray mm; } dat;
+  VSArray p;
+  double r;
+  int i;
+  memset(&td, 0, sizeof(td));
+  vsFrameInfoInit(&td.fiSrc, width, height, PF_YUV420P);
+  td.conf = vsTransformGetDefaultConfig("vsref");
+  td.conf.fov = fov;
+  vs_vector_init(&lms, n + 1);
+  for (i = 0; i < n; i++) vs_vector_append_dup(&lms, (void*)&recs[i], sizeof(LocalMotion));
+  dat.td = &td;
+  dat.motions = &lms;
+  dat.mm.dat = missmatches;
+  dat.mm.len = n;
+  p = vs_array((double*)params4, 4);
+  r = calcTransformQuality(p, &dat);
+  vs_array_free(p);
+  vs_vector_del(&lms);
+  return r;
+}
+
+/* layout of the structures the second pass reads through a caller's pointer */
+int vsref_transform_layout(long* out, int cap) {
+  long v[] = {
+    (long)sizeof(VSTransformData), (long)sizeof(VSTransformConfig),
+    (long)sizeof(VSTransformations),
+    (long)offsetof(VSTransformData, fiSrc), (long)offsetof(VSTransformData, conf),
+    (long)offsetof(VSTransformData, initialized),
+    (long)offsetof(VSTransformConfig, modName), (long)offsetof(VSTransformConfig, verbose),
+    (long)offsetof(VSTransformConfig, simpleMotionCalculation),
+    (long)offsetof(VSTransformConfig, storeTransforms),
+    (long)offsetof(VSTransformConfig, smoothZoom),
+    (long)offsetof(VSTransformConfig, estimateLensDistortion),
+    (long)offsetof(VSTransformConfig, lensK), (long)offsetof(VSTransformConfig, fov),
+    (long)offsetof(VSTransformations, ts), (long)offsetof(VSTransformations, len),
+  };
+  int n = (int)(sizeof(v) / sizeof(v[0])), i;
+  for (i = 0; i < n && i < cap; i++) out[i] = v[i];
+  return n;
+}
+
+/* The transform pass's input path as a host application takes it: the
+ * reference's vsReadLocalMotionsFile on a .trf file, then
+ * vsLocalmotions2Transforms (lens estimate off; storeTransforms writes
+ * global_motions.trf into the working directory).  Returns the number of
+ * frames (their transforms in out[0 .. min(n, cap))) or -1. */
+int vsref_trf_to_transforms(const char* trf_path, int width, int height, double fov,
+                            int smoothZoom, int store, VSTransform* out, int cap) {
+  VSTransformData td;
+  VSManyLocalMotions mlms;
+  VSTransformations trans;
+  FILE* f;
+  int k, n, rc;
+  quiet_log();
+  f = fopen(trf_path, "rb");
+  if (!f) return -1;
+  memset(&mlms, 0, sizeof(mlms));
+  rc = vsReadLocalMotionsFile(f, &mlms);
+  fclose(f);
+  if (rc != VS_OK) return -1;
+  memset(&td, 0, sizeof(td));
+  vsFrameInfoInit(&td.fiSrc, width, height, PF_YUV420P);
+  td.fiDest = td.fiSrc;
+  td.conf = vsTransformGetDefaultConfig("vsref");
+  td.conf.estimateLensDistortion = 0;
+  td.conf.fov = fov;
+  td.conf.smoothZoom = smoothZoom;
+  td.conf.storeTransforms = store;
+  vsTransformationsInit(&trans);
+  rc = vsLocalmotions2Transforms(&td, &mlms, &trans);
+  n = rc == VS_OK ? trans.len : -1;
+  for (k = 0; k < n && k < cap; k++) out[k] = trans.ts[k];
+  vsTransformationsCleanup(&trans);
+  for (k = 0; k < vs_vector_size(&mlms); k++) vs_vector_del(VSMLMGet(&mlms, k));
+  vs_vector_del(&mlms);
+  return n;
 }

@@ -29,9 +29,12 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 CC = shutil.which("gcc", path="/usr/bin:/bin") or "gcc"
 
 STRICT_C = ["vs_runtime.c", "vs_frameinfo.c", "vs_vector.c", "vs_serialize.c",
-            "vs_motiondetect.c", "vs_ext.c", "vs_batch.c", "vs_pnet.c"]
+            "vs_motiondetect.c", "vs_ext.c", "vs_batch.c", "vs_pnet.c", "vs_l2t.c"]
 REFFP_C = ["vs_transform.c", "vs_motionmodel.c", "vs_draw.c"]
-CU = ["vsb_device.cu", "vsb_noalloc.cu", "vsb_batch.cu", "vsb_pnet.cu"]
+CU = ["vsb_device.cu", "vsb_noalloc.cu", "vsb_batch.cu", "vsb_pnet.cu", "vsb_l2t.cu"]
+# the second pass follows the reference's rounding step by step: no fused
+# multiply-adds there
+CU_EXTRA = {"vsb_l2t.cu": ["--fmad=false"]}
 
 COMMON_C = ["-std=gnu99", "-O3", "-DNDEBUG", "-fPIC", "-Wall", "-fvisibility=hidden",
             "-I" + INCLUDE, "-I" + CSRC]
@@ -89,7 +92,7 @@ def build(verbose=False, ptxas_v=False, force=False):
         objs.append(obj)
         if force or ptxas_v or newer([src] + hdrs, obj):
             extra = ["-Xptxas", "-v"] if ptxas_v else []
-            jobs.append([NVCC] + NVCC_FLAGS + extra + ["-c", src, "-o", obj])
+            jobs.append([NVCC] + NVCC_FLAGS + CU_EXTRA.get(f, []) + extra + ["-c", src, "-o", obj])
     # the CUDA translation units compile independently: one nvcc each, in parallel
     with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
         for out in ex.map(lambda cmd: run(cmd, verbose), jobs):

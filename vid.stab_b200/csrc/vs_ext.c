@@ -2,6 +2,7 @@
  * vs_ext.c -- entry points without a counterpart in the reference
  * (declared in vidstab_b200_ext.h).
  */
+#include <stddef.h>
 #include <stdlib.h>
 #include <string.h>
 #include <time.h>
@@ -25,7 +26,29 @@ int vsb_sizeof(const char* t) {
   if (!strcmp(t, "VSVector")) return (int)sizeof(VSVector);
   if (!strcmp(t, "Field")) return (int)sizeof(Field);
   if (!strcmp(t, "PreparedTransform")) return (int)sizeof(PreparedTransform);
+  if (!strcmp(t, "VSTransformData")) return (int)sizeof(VSTransformData);
+  if (!strcmp(t, "VSTransformConfig")) return (int)sizeof(VSTransformConfig);
+  if (!strcmp(t, "VSTransformations")) return (int)sizeof(VSTransformations);
   return -1;
+}
+
+int vsb_transform_layout(long* out, int cap) {
+  long v[] = {
+    (long)sizeof(VSTransformData), (long)sizeof(VSTransformConfig),
+    (long)sizeof(VSTransformations),
+    (long)offsetof(VSTransformData, fiSrc), (long)offsetof(VSTransformData, conf),
+    (long)offsetof(VSTransformData, initialized),
+    (long)offsetof(VSTransformConfig, modName), (long)offsetof(VSTransformConfig, verbose),
+    (long)offsetof(VSTransformConfig, simpleMotionCalculation),
+    (long)offsetof(VSTransformConfig, storeTransforms),
+    (long)offsetof(VSTransformConfig, smoothZoom),
+    (long)offsetof(VSTransformConfig, estimateLensDistortion),
+    (long)offsetof(VSTransformConfig, lensK), (long)offsetof(VSTransformConfig, fov),
+    (long)offsetof(VSTransformations, ts), (long)offsetof(VSTransformations, len),
+  };
+  int n = (int)(sizeof(v) / sizeof(v[0])), i;
+  for (i = 0; i < n && i < cap; i++) out[i] = v[i];
+  return n;
 }
 
 int vsb_motion_detection_device(VSMotionDetect* md, LocalMotions* motions, const uint8_t* d_plane0,

@@ -67,8 +67,48 @@ class VSMotionDetect(C.Structure):
                 ("serializationMode", C.c_int), ("frameNum", C.c_int)]
 
 
+# VSTransform as an array element (56 bytes + 8 padding on x86-64)
+TRANSFORM_DTYPE = np.dtype({"names": ["x", "y", "alpha", "zoom", "barrel", "rshutter", "extra"],
+                            "formats": ["<f8", "<f8", "<f8", "<f8", "<f8", "<f8", "<i4"],
+                            "offsets": [0, 8, 16, 24, 32, 40, 48], "itemsize": 56})
+
+
 class VSVector(C.Structure):
     _fields_ = [("data", C.POINTER(C.c_void_p)), ("buffersize", C.c_int), ("nelems", C.c_int)]
+
+
+class VSTransformConfig(C.Structure):
+    """src/transform.h:88-150 of the reference"""
+    _fields_ = [("relative", C.c_int), ("smoothing", C.c_int), ("crop", C.c_int),
+                ("invert", C.c_int), ("zoom", C.c_double), ("optZoom", C.c_int),
+                ("zoomSpeed", C.c_double), ("interpolType", C.c_int), ("maxShift", C.c_int),
+                ("maxAngle", C.c_double), ("modName", C.c_char_p), ("verbose", C.c_int),
+                ("simpleMotionCalculation", C.c_int), ("storeTransforms", C.c_int),
+                ("smoothZoom", C.c_int), ("camPathAlgo", C.c_int),
+                ("estimateLensDistortion", C.c_int), ("lensCorrection", C.c_int),
+                ("lensK", C.c_double), ("fov", C.c_double)]
+
+
+class VSLensPlaneMap(C.Structure):
+    _fields_ = [("active", C.c_int), ("mode", C.c_int)] + \
+        [(n, C.c_double) for n in ("k", "cdx", "cdy", "csx", "csy", "tMaxU", "tMaxD", "tDomD",
+                                   "invRho2", "f")] + \
+        [("sxShift", C.c_int), ("syShift", C.c_int), ("idxScaleU", C.c_int32),
+         ("idxScaleD", C.c_int32), ("gU", C.c_void_p), ("gD", C.c_void_p)]
+
+
+class VSTransformData(C.Structure):
+    """src/transform.h:152-178 of the reference"""
+    _fields_ = [("fiSrc", VSFrameInfo), ("fiDest", VSFrameInfo), ("src", VSFrame),
+                ("destbuf", VSFrame), ("dest", VSFrame), ("srcMalloced", C.c_short),
+                ("interpolate", C.c_void_p), ("conf", VSTransformConfig), ("lensMode", C.c_int),
+                ("lensActive", C.c_int), ("lensK", C.c_double), ("lensMapK", C.c_double),
+                ("lensMaps", VSLensPlaneMap * 3), ("initialized", C.c_int)]
+
+
+class VSTransformations(C.Structure):
+    _fields_ = [("ts", C.POINTER(VSTransform)), ("current", C.c_int), ("len", C.c_int),
+                ("warned_end", C.c_short)]
 
 
 _lib = None
@@ -153,6 +193,19 @@ def lib():
     L.vsb_field_minmax_host.argtypes = [p, i, i, i, i, p, p, i, i, p]
     L.vsb_field_search_host.restype = i
     L.vsb_field_search_host.argtypes = [p, p, i, i, i, i, i, i, p, p, p, p, i, i, p, p, p, p]
+    L.vsLocalmotions2Transforms.restype = i
+    L.vsLocalmotions2Transforms.argtypes = [C.POINTER(VSTransformData), C.POINTER(VSVector),
+                                            C.POINTER(VSTransformations)]
+    L.vsMotionsToTransform.restype = VSTransform
+    L.vsMotionsToTransform.argtypes = [C.POINTER(VSTransformData), C.POINTER(VSVector), p]
+    L.vsb_transform_layout.restype = i
+    L.vsb_transform_layout.argtypes = [p, i]
+    L.vsb_motions_to_transforms.restype = i
+    L.vsb_motions_to_transforms.argtypes = [p, p, i, i, i, d, i, p, p, p]
+    L.vsb_motions_to_transforms_device.restype = i
+    L.vsb_motions_to_transforms_device.argtypes = [p, p, i, i, i, i, d, i, p, p, p, p]
+    L.vsb_motions_to_transforms_capacity.restype = i
+    L.vsb_motions_to_transforms_launches.restype = C.c_long
     _lib = L
     return L
 

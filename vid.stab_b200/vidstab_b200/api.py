@@ -5,8 +5,8 @@ import ctypes as C
 
 import numpy as np
 
-from ._lib import (LM_DTYPE, PF_PACKED, PF_RGBA, VSFrame, VSFrameInfo, VSMotionDetect,
-                   VSVector, lib, ptr, vector_records)
+from ._lib import (LM_DTYPE, PF_PACKED, PF_RGBA, TRANSFORM_DTYPE, VSFrame, VSFrameInfo,
+                   VSMotionDetect, VSVector, lib, ptr, vector_records)
 
 
 def records_per_frame(width, height):
@@ -343,3 +343,27 @@ def field_search(curr, prev, xs, ys, size, max_shift, step, ox=None, oy=None, pa
                                ptr(ty), ptr(ok)) != 0:
         raise RuntimeError(L.vsb_last_error().decode())
     return sad, tx, ty, ok
+
+
+def motions_to_transforms(recs, counts, width, height, fov=0.0, smooth_zoom=0):
+    """The second pass (vsLocalmotions2Transforms' fit, one GPU warp per
+    frame) over frames whose LocalMotions are `recs` (LM_DTYPE), frame k
+    holding counts[k] of them in order.  Returns (transforms as
+    TRANSFORM_DTYPE, residuals, info[n, 3] = rounds, fields masked for their
+    match, fields masked as outliers)."""
+    L = lib()
+    recs = np.ascontiguousarray(recs, LM_DTYPE)
+    counts = np.asarray(counts, np.int64)
+    n = len(counts)
+    first = np.zeros(n + 1, np.int64)
+    first[1:] = np.cumsum(counts)
+    if first[-1] != len(recs):
+        raise ValueError("counts add up to %d, %d records given" % (first[-1], len(recs)))
+    out = np.zeros(n, TRANSFORM_DTYPE)
+    resid = np.zeros(n, np.float64)
+    info = np.zeros((n, 3), np.int32)
+    rc = L.vsb_motions_to_transforms(ptr(recs) if len(recs) else None, ptr(first), n, width,
+                                     height, fov, smooth_zoom, ptr(out), ptr(resid), ptr(info))
+    if rc != 0:
+        raise RuntimeError("second pass failed: %s" % L.vsb_last_error().decode())
+    return out, resid, info
