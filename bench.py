@@ -861,9 +861,12 @@ def main():
                             "lattice_rows_per_tile": desc[3], "strips": desc[4],
                             "threads": desc[5], "smem": desc[6],
                             ("ctas" if desc[1] == 5 else "ctas_per_field"): desc[7]}
-        bdesc = (C.c_int * 3)()
+        bdesc = (C.c_int * 4)()
         L.vsb_blur_tiling(C.byref(det.md), bdesc)
-        tiling["blur_tile"] = [bdesc[0], bdesc[1]]
+        fused = bool(bdesc[3])
+        tiling["prefilter"] = ("k_blurmm: blur + field min/max, one launch, 128x8 warp blocks"
+                               if fused else "k_blur_fast tile %dx%d + k_minmax_planar"
+                               % (bdesc[0], bdesc[1]))
         det.close()
         kernel_ms = {n: (ms[i] / cnt[i] if cnt[i] else None) for i, n in
                      enumerate(["blur", "field_minmax", "coarse_search", "fine_search"])}
@@ -892,10 +895,12 @@ def main():
         hbm, src = peaks()
         bb = 2.0 * W * H
         t_blur = kernel_ms["blur"] * 1e-3
-        roof_hbm = {"kernel": "k_blur_fast (prefilter, 1080p)", "bound": "hbm",
+        pname = "k_blurmm" if fused else "k_blur_fast"
+        roof_hbm = {"kernel": "%s (prefilter%s, 1080p)" % (pname, " + field min/max" if fused
+                                                             else ""), "bound": "hbm",
                     "achieved": bb / t_blur / 1e9, "peak": hbm, "unit": "GB/s",
                     "frac": bb / t_blur / 1e9 / hbm, "peak_source": src,
-                    "traffic": traffic_from_profile("k_blur_fast_1080p.md")}
+                    "traffic": traffic_from_profile("%s_1080p.md" % pname)}
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:

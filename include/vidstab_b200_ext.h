@@ -52,9 +52,11 @@ VS_API void vsb_set_default_search_mode(int pruned);
    shared memory bytes per CTA, CTAs per field. */
 VS_API int vsb_search_tiling(const struct _vsmotiondetect* md, int fine, int* desc);
 
-/* The prefilter tile the detector picked by timing at init: desc[0] width,
-   desc[1] height (output pixels per CTA), desc[2] its time per frame in ns
-   (0 when it was not timed). */
+/* The prefilter of the detector: desc[0], desc[1] the width and height
+   (output pixels per CTA) of the separate blur's tile, picked by timing at
+   init, desc[2] its time per frame in ns (0 when it was not timed), desc[3]
+   1 when the blur and the field min/max run as one launch (k_blurmm; planar
+   frames, box sizes 3..9), in which case the tile is not used. */
 VS_API int vsb_blur_tiling(const struct _vsmotiondetect* md, int* desc);
 
 /* Kernel launches issued for this detector so far. */

@@ -5,6 +5,7 @@ import pytest
 import oracle as O
 import vidstab_b200 as V
 from vidstab_b200 import synthetic as S
+from conftest import first_difference, records_equal
 
 pytestmark = pytest.mark.gpu
 
@@ -220,3 +221,21 @@ def test_sad_peak_probe():
     d = O.C.c_double()
     assert V.lib().vsb_sad_peak(0, O.C.byref(d)) == 0
     assert d.value > 1e12
+
+
+@pytest.mark.parametrize("w,h,step", [(642, 482, 6), (1000, 562, 4), (1282, 722, 8),
+                                      (1921, 1081, 2), (800, 600, 5)])
+def test_fused_prefilter_matches_two_launch_path(w, h, step, monkeypatch):
+    """k_blurmm (blur + every field's min/max in one launch, box half-widths
+    1..4) against the two-launch path (VSB_NO_BLURMM) and the reference, on
+    frames whose width and height are not multiples of the 128 x 16 warp
+    block (ragged last blocks, edge words loaded and stored bytewise)"""
+    frames = S.clip(w, h, 3, seed=w + h)
+    fused, fc, _ = V.detect_clip(frames, V.PF_GRAY8, stepsize=step)
+    monkeypatch.setenv("VSB_NO_BLURMM", "1")
+    two, tc, _ = V.detect_clip(frames, V.PF_GRAY8, stepsize=step)
+    monkeypatch.delenv("VSB_NO_BLURMM")
+    assert np.array_equal(fc, tc) and records_equal(fused, two), first_difference(fused, two)
+    if O.ref_available():
+        ref, rc, _ = O.ref_clip(np.asarray(frames), V.PF_GRAY8, stepsize=step)
+        assert np.array_equal(fc, rc) and records_equal(fused, ref), first_difference(fused, ref)

@@ -84,6 +84,10 @@ def forced_sweep(monkeypatch):
 
 @pytest.mark.parametrize("w,h,n", [(640, 360, 6), (1280, 720, 5), (1920, 1080, 5)])
 def test_detect_on_sweep_matches_reference(w, h, n, forced_sweep):
+    """whole detect passes on the sweep; the fine plan is sized for every
+    fine field, so a frame's fine launch (the selected fields only) has fewer
+    tiles than CTAs at 640x360 and empty CTAs lie between the CTAs holding a
+    field's tiles"""
     frames = S.clip(w, h, n, seed=w + 7)
     det = V.MotionDetector(w, h, V.PF_YUV420P)
     desc = (O.C.c_int * 8)()

@@ -22,12 +22,16 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
+#include <vector>
+
 #include "vsb_device.h"
 #include "vsb_plan.h"
 #include "vsb_pnet.h"
 #include "vsb_prefilter.cuh"
 #include "vsb_search.cuh"
 #include "vsb_sweep.cuh"
+#include "vsb_blurmm.cuh"
 
 /* ------------------------------------------------------------------------ */
 /* error plumbing                                                            */
@@ -1261,6 +1265,13 @@ struct vsbd_ctx {
   int mode;                     /* 0 dense search, 1 pruned search */
   GeomDev gcp, gfp;             /* partial-pass geometry (first rows of the field) */
   uint8_t* d_skip;              /* coarse fields never selected (contrast) */
+  /* blur and field min/max in one launch (k_blurmm): per 128x16 warp block
+     the fields meeting it, the running min/max of every field, the ticket */
+  int bm_on, bm_nbx, bm_grid_x, bm_grid_y;
+  int* d_bm_lofs;
+  uint2* d_bm_list;
+  unsigned* d_bm_acc;
+  unsigned* d_bm_ticket;
   unsigned* d_part;             /* partial sums, per item per lattice point */
   int* d_lists;                 /* survivors, per item */
   int* d_counts;
@@ -1390,6 +1401,10 @@ extern "C" void vsbd_destroy(vsbd_ctx* c) {
   cudaFree(c->d_outs[0]);
   cudaFree(c->d_outs[1]);
   cudaFree(c->d_skip);
+  cudaFree(c->d_bm_lofs);
+  cudaFree(c->d_bm_list);
+  cudaFree(c->d_bm_acc);
+  cudaFree(c->d_bm_ticket);
   cudaFree(c->d_part);
   cudaFree(c->d_lists);
   cudaFree(c->d_counts);
@@ -1520,6 +1535,117 @@ extern "C" int vsbd_set_search_mode(vsbd_ctx* c, int pruned) {
   return 0;
 }
 
+/* The fused prefilter's tables (planar frames, box half-width 1..4): for
+   every 128-column x 16-row warp block of the frame, the fields whose
+   square meets it, with the block's column range and row mask of the
+   intersection; the fields' min/max accumulators start at (255.., 0). */
+static int blurmm_setup(vsbd_ctx* c, const int16_t* cx, const int16_t* cy, const int16_t* fx,
+                        const int16_t* fy) {
+  const int half = c->blur / 2;
+  const int nfield = c->nc + c->nf;
+  c->bm_on = 0;
+  /* VSB_NO_BLURMM: the two-launch prefilter (blur, then field min/max) */
+  if (c->blur < 2 || half < 1 || half > BM_MAXHALF || c->bpp != 1 || c->nch != 1 ||
+      nfield > 65535 || c->W < 4 || getenv("VSB_NO_BLURMM"))
+    return 0;
+  {
+    /* the kernel divides by the multiply-high alone */
+    BlurDiv dv;
+    make_div(c->blur, half, &dv);
+    if (!dv.exact) return 0;
+  }
+  const int nbx = (c->W + BM_COLS - 1) / BM_COLS;
+  const int nbands = (c->H + BM_ROWS - 1) / BM_ROWS;
+  const int gy = (nbands + BM_WARPS - 1) / BM_WARPS;
+  const size_t nwb = (size_t)gy * BM_WARPS * nbx; /* every warp of the grid has a slot */
+  std::vector<std::vector<uint2>> per(nwb);
+  for (int f = 0; f < nfield; f++) {
+    const bool coarse = f < c->nc;
+    const int S = coarse ? c->gc.g.S : c->gf.g.S;
+    const int x = coarse ? cx[f] : fx[f - c->nc];
+    const int y = coarse ? cy[f] : fy[f - c->nc];
+    const int xa = x - S / 2, ya = y - S / 2;
+    if (xa < 0 || ya < 0 || xa + S > c->W || ya + S > c->H) return 0; /* not expected */
+    for (int b = ya / BM_ROWS; b * BM_ROWS < ya + S; b++) {
+      unsigned rows = 0;
+      for (int r = 0; r < BM_ROWS; r++) {
+        const int yy = b * BM_ROWS + r;
+        if (yy >= ya && yy < ya + S) rows |= 1u << r;
+      }
+      for (int bx = xa / BM_COLS; bx * BM_COLS < xa + S; bx++) {
+        const int lo = std::max(xa, bx * BM_COLS) - bx * BM_COLS;
+        const int hi = std::min(xa + S, (bx + 1) * BM_COLS) - bx * BM_COLS;
+        per[(size_t)b * nbx + bx].push_back(
+            make_uint2((unsigned)f | ((unsigned)lo << 16) | ((unsigned)hi << 24), rows));
+      }
+    }
+  }
+  std::vector<int> ofs(nwb + 1, 0);
+  std::vector<uint2> list;
+  for (size_t i = 0; i < nwb; i++) {
+    ofs[i] = (int)list.size();
+    list.insert(list.end(), per[i].begin(), per[i].end());
+  }
+  ofs[nwb] = (int)list.size();
+  std::vector<unsigned> acc(2 * (size_t)nfield);
+  for (int f = 0; f < nfield; f++) {
+    acc[2 * f] = 0xffffffffu;
+    acc[2 * f + 1] = 0u;
+  }
+  CK(cudaMalloc(&c->d_bm_lofs, sizeof(int) * (nwb + 1)));
+  CK(cudaMalloc(&c->d_bm_list, sizeof(uint2) * (list.size() + 1)));
+  CK(cudaMalloc(&c->d_bm_acc, sizeof(unsigned) * (acc.size() + 2)));
+  CK(cudaMalloc(&c->d_bm_ticket, sizeof(unsigned)));
+  CK(cudaMemcpy(c->d_bm_lofs, ofs.data(), sizeof(int) * (nwb + 1), cudaMemcpyHostToDevice));
+  if (!list.empty())
+    CK(cudaMemcpy(c->d_bm_list, list.data(), sizeof(uint2) * list.size(), cudaMemcpyHostToDevice));
+  if (!acc.empty())
+    CK(cudaMemcpy(c->d_bm_acc, acc.data(), sizeof(unsigned) * acc.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemset(c->d_bm_ticket, 0, sizeof(unsigned)));
+  c->bm_nbx = nbx;
+  c->bm_grid_x = nbx;
+  c->bm_grid_y = gy;
+  c->bm_on = 1;
+  return 0;
+}
+
+/* k_blurmm over plane `src` into `cur`: the blurred plane, the (min, max)
+   byte pairs of every field into c->d_out and the coarse contrast flags */
+static int launch_blurmm(vsbd_ctx* c, const uint8_t* src, int sp, uint8_t* cur, uint8_t* skip,
+                         cudaStream_t st) {
+  BMArgs A;
+  A.src = src;
+  A.sp = sp;
+  A.dst = cur;
+  A.dp = c->pitch;
+  A.W = c->W;
+  A.H = c->H;
+  make_div(c->blur, c->blur / 2, &A.dv);
+  A.lofs = c->d_bm_lofs;
+  A.list = c->d_bm_list;
+  A.nbx = c->bm_nbx;
+  A.acc = c->d_bm_acc;
+  A.ticket = c->d_bm_ticket;
+  A.nc = c->nc;
+  A.nfields = c->nc + c->nf;
+  A.out = c->d_out;
+  A.thr = c->thr_coarse;
+  A.skip = skip;
+  const dim3 grid(c->bm_grid_x, c->bm_grid_y);
+  switch (c->blur / 2) {
+    case 1: k_blurmm<1><<<grid, 32 * BM_WARPS, 0, st>>>(A); break;
+    case 2: k_blurmm<2><<<grid, 32 * BM_WARPS, 0, st>>>(A); break;
+    case 3: k_blurmm<3><<<grid, 32 * BM_WARPS, 0, st>>>(A); break;
+    case 4: k_blurmm<4><<<grid, 32 * BM_WARPS, 0, st>>>(A); break;
+    default: set_msg("k_blurmm: unsupported box size"); return -1;
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) { set_err("k_blurmm launch", e); return -1; }
+  c->launches++;
+  count_launches(1);
+  return 0;
+}
+
 extern "C" int vsbd_create(vsbd_ctx** out, int W, int H, int bpp, int blur_size, int channels,
                            const vsbd_geom* coarse, const int16_t* cx, const int16_t* cy, int nc,
                            const vsbd_geom* fine, const int16_t* fx, const int16_t* fy, int nf,
@@ -1589,6 +1715,7 @@ extern "C" int vsbd_create(vsbd_ctx** out, int W, int H, int bpp, int blur_size,
     CKC(cudaMalloc(&c->d_skip, nc + 1));
     CKC(cudaMemset(c->d_skip, 0, nc + 1));
   }
+  if (blurmm_setup(c, cx, cy, fx, fy) != 0) { vsbd_destroy(c); return -1; }
   /* coarse items: every coarse field, no offset */
   {
     vsbd_item* it = (vsbd_item*)malloc(sizeof(vsbd_item) * (nc + 1));
@@ -1771,6 +1898,10 @@ static int stage_a_issue(vsbd_ctx* c, const uint8_t* host, int linesize, const u
   c->obuf ^= 1;
   c->d_out = c->d_outs[c->obuf];
   c->h_out = c->h_outs[c->obuf];
+  /* the contrast flags steer the pruned and the proposal searches and mark
+     the training log's unused fields */
+  uint8_t* skip = (c->mode || c->pn_on || c->log_in) ? c->d_skip : NULL;
+  bool fused = false; /* blur and field min/max in one launch */
   if (c->blur >= 2) {
     const uint8_t* src = dev;
     int sp = pitch;
@@ -1781,8 +1912,12 @@ static int stage_a_issue(vsbd_ctx* c, const uint8_t* host, int linesize, const u
       src = c->d_raw;
       sp = c->pitch;
     }
+    fused = c->bm_on &&
+            ((((uintptr_t)src | (uintptr_t)sp | (uintptr_t)cur | (uintptr_t)c->pitch) & 3) == 0);
     kt_begin(c, VSBD_KT_BLUR, st);
-    {
+    if (fused) {
+      if (launch_blurmm(c, src, sp, cur, skip, st) != 0) return -1;
+    } else {
       int nb = launch_blur(src, sp, cur, c->pitch, c->W, c->H, c->blur, c->d_tmp, c->pitch, st,
                            c->blur_shape);
       c->launches += nb;
@@ -1800,12 +1935,11 @@ static int stage_a_issue(vsbd_ctx* c, const uint8_t* host, int linesize, const u
   }
   if (search) {
     int S = c->gc.g.S;
-    /* the contrast flags steer the pruned and the proposal searches and mark
-       the training log's unused fields */
-    uint8_t* skip = (c->mode || c->pn_on || c->log_in) ? c->d_skip : NULL;
     vsbd_result* cres = (vsbd_result*)(c->d_out + c->off_coarse);
-    kt_begin(c, VSBD_KT_MINMAX, st);
-    if (c->bpp == 1 && c->nch == 1) {
+    if (!fused) kt_begin(c, VSBD_KT_MINMAX, st);
+    if (fused) {
+      /* done by k_blurmm */
+    } else if (c->bpp == 1 && c->nch == 1) {
       k_minmax_planar<<<c->nc + c->nf, 256, 0, st>>>(cur, c->pitch, c->d_xy, c->nc, c->nf, S,
                                                      c->gf.g.S, c->d_out, c->thr_coarse, skip);
       c->launches++;
@@ -1823,7 +1957,7 @@ static int stage_a_issue(vsbd_ctx* c, const uint8_t* host, int linesize, const u
         count_launches(1);
       }
     }
-    kt_end(c, VSBD_KT_MINMAX, st);
+    if (!fused) kt_end(c, VSBD_KT_MINMAX, st);
     if (c->pn_on) {
       if (learned_search(c, c->gc, c->fb_last[0] >= 8 ? c->gc : c->gcf, cur, prv, st, c->d_citems,
                          c->nc, 0, skip, c->d_keys, c->d_tickets, cres, c->d_out + c->off_cfb,
@@ -2046,6 +2180,7 @@ extern "C" int vsbd_blur_tiling(const vsbd_ctx* c, int* desc) {
   desc[0] = g_blur_shape[c->blur_shape][0];
   desc[1] = g_blur_shape[c->blur_shape][1];
   desc[2] = (int)(1000.f * c->blur_us);
+  desc[3] = c->bm_on;
   return 0;
 }
 

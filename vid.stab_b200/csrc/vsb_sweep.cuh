@@ -29,11 +29,15 @@
  *
  * Winner.  Every candidate gets its full sum; the lowest (SAD, rank) pair
  * wins, rank being the candidate's position in the reference's visiting
- * order, so equal SADs resolve as its strict `<` scan does.  Tiles fold
- * their best pair into the field's 64-bit key with atomicMin; the last tile
- * of a field (ticket counter) runs the refinement rounds and the range test
- * and resets the key and ticket, exactly as the one-launch-per-tile search
- * (vsb_search.cuh) does.
+ * order, so equal SADs resolve as its strict `<` scan does.  Each thread
+ * keeps its lowest pair over the CTA's consecutive tiles of one field; after
+ * its last tile of that field the CTA folds the best pair into the field's
+ * 64-bit key with one atomicMin and takes a ticket.  The tile ranges are
+ * fixed by the grid, so the number of CTAs that have tiles of a field is
+ * known; the CTA drawing the last of those tickets runs the refinement
+ * rounds and the range test and resets the key and ticket, as the
+ * one-launch-per-tile search (vsb_search.cuh) does after a field's last
+ * tile.
  *
  * Waits on the mbarriers are bounded (polls and clock cycles); a wait that
  * runs out raises *err, waits once more (bounded) for the CTA's copies and
@@ -490,9 +494,9 @@ __global__ void __launch_bounds__(SW_MAX_THREADS, 1)
   __shared__ int s_last;
   const SweepLayout L = sweep_layout(g);
   const int ncg = g.nab / SW_TA;
-  const long T = (long)n * g.nta * g.ntb;
-  const int t_begin = (int)((long)blockIdx.x * T / gridDim.x);
-  const int t_end = (int)((long)(blockIdx.x + 1) * T / gridDim.x);
+  const long T_ = (long)n * g.nta * g.ntb; /* tiles of the launch */
+  const int t_begin = (int)((long)blockIdx.x * T_ / gridDim.x);
+  const int t_end = (int)((long)(blockIdx.x + 1) * T_ / gridDim.x);
   const int nmine = t_end - t_begin;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   if (nmine <= 0) return;
@@ -529,6 +533,11 @@ __global__ void __launch_bounds__(SW_MAX_THREADS, 1)
   const int bl = rem / ncg, cg = rem - bl * ncg;
   const int Rs = g.S / g.nstrip;
   unsigned* part = (unsigned*)(sm + L.off_part);
+  /* the lowest (SAD, rank) this thread has seen in the current field's
+     tiles: the CTA folds it into the field's key once, after its last tile
+     of the field */
+  unsigned long long best = ~0ull;
+  const int per_item = g.nta * g.ntb;
   for (int k = 0; k < nmine; k++) {
     const int tt = t_begin + k;
     const int b = k & 1;
@@ -584,7 +593,6 @@ __global__ void __launch_bounds__(SW_MAX_THREADS, 1)
       p[1] = make_uint4(acc[4], acc[5], acc[6], acc[7]);
     }
     __syncthreads();
-    unsigned long long best = ~0ull;
     for (int u = 0, q = threadIdx.x; q < tps * SW_TA; u++, q += blockDim.x) {
       const int r2 = q / SW_TA, c = q - r2 * SW_TA;
       const int bl2 = r2 / ncg, cg2 = r2 - bl2 * ncg;
@@ -596,18 +604,35 @@ __global__ void __launch_bounds__(SW_MAX_THREADS, 1)
       const unsigned long long key = ((unsigned long long)sum << 32) | (unsigned)rk;
       best = key < best ? key : best;
     }
-    best = warp_min64(best);
-    if (lane == 0) red[warp] = best;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      for (int w2 = 1; w2 < nwarps; w2++) best = red[w2] < best ? red[w2] : best;
-      atomicMin(&keys[T.item], best);
-      __threadfence();
-      const unsigned tk = atomicAdd(&tickets[T.item], 1u);
-      s_last = tk == (unsigned)(g.nta * g.ntb) - 1;
+    /* the CTA's last tile of this field: fold the field's best into its key
+       and take a ticket; the field's tickets are counted per CTA that has
+       tiles of it (the tile ranges are fixed by the grid) */
+    const bool field_end = k + 1 == nmine || (tt + 1) / per_item != T.item;
+    bool last = false;
+    if (field_end) {
+      best = warp_min64(best);
+      if (lane == 0) red[warp] = best;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        for (int w2 = 1; w2 < nwarps; w2++) best = red[w2] < best ? red[w2] : best;
+        atomicMin(&keys[T.item], best);
+        __threadfence();
+        const unsigned tk = atomicAdd(&tickets[T.item], 1u);
+        /* CTAs holding tiles of the field: with at least as many tiles as
+           CTAs every CTA has some, so they are the owners of the field's
+           first and last tiles and those between; with fewer, a CTA has at
+           most one tile (and empty CTAs lie between the owners) */
+        const long G = gridDim.x;
+        const long f0 = (long)T.item * per_item, f1 = f0 + per_item - 1;
+        const long c0 = ((f0 + 1) * G + T_ - 1) / T_ - 1, c1 = ((f1 + 1) * G + T_ - 1) / T_ - 1;
+        const long holders = T_ >= G ? c1 - c0 + 1 : per_item;
+        s_last = tk == (unsigned)(holders - 1);
+      }
+      __syncthreads();
+      last = s_last;
+      best = ~0ull;
     }
-    __syncthreads();
-    if (s_last) {
+    if (last) {
       /* the field's last tile: refinement, with the aligned field copy and
          this tile's (now free) buffer as the refinement window */
       __threadfence();
