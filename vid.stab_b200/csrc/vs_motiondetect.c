@@ -768,6 +768,22 @@ int vsb_can_overlap(const VSMotionDetect* md) {
   return st && md->conf.virtualTripod < 1 && !md->conf.show && vsbd_can_overlap(st->dev);
 }
 
+/* Issues stage A of frame j of the clip (the frame after the last one
+   issued) and, for host frames, copies frame j+1 into its upload slot
+   (j+1) % 3; frame j was copied into slot j % 3 before.  0 or -1. */
+static int issue_next_frame(VSMotionDetect* md, md_state* st, const uint8_t* frames,
+                            long frame_bytes, int linesize, int nframes, int on_device, int j) {
+  if ((on_device ? vsbd_stage_a_next_issue(st->dev, NULL, linesize,
+                                           frames + (size_t)j * frame_bytes, linesize)
+                 : vsbd_stage_a_next_issue_uploaded(st->dev, j % 3)) != 0 ||
+      (!on_device && j + 1 < nframes &&
+       vsbd_upload(st->dev, frames + (size_t)(j + 1) * frame_bytes, linesize, (j + 1) % 3) != 0)) {
+    vs_log_error(md->conf.modName, "GPU stage A failed: %s\n", vsbd_error());
+    return -1;
+  }
+  return 0;
+}
+
 /* A clip through the detector with consecutive frames overlapped on the
    GPU: stage A of frame k+1 (blur, min/max, coarse search) is enqueued
    before the host selects frame k's fields, and runs on one stream while
@@ -806,65 +822,68 @@ long vsb_detect_run_overlapped(VSMotionDetect* md, const uint8_t* frames, long f
       return -1;
     }
   }
-  /* host frames travel one frame ahead of their stage A: frame k+2 is copied
-     into upload slot k&1 (free: frame k's stage A, which read it, has been
-     collected) while frame k's fine stage and frame k+1's stage A run */
+  /* Host frames travel ahead of their stage A: frame j is copied into
+     upload slot j % 3 on the copy stream.  Plain search: two frames' stage A
+     are kept in flight, so frame k+2's stage A is issued right after frame
+     k's fine stage, before the host waits for that stage and assembles frame
+     k; the GPU then has queued work while the host does.  With a proposal
+     network only frame k+1's, issued after frame k's fine stage (the network
+     kernel fills every SM's shared memory and would hold the fine stage
+     back). */
+  const int a_first = !vsbd_proposal_on(st->dev);
+  const int depth = a_first ? 2 : 1;
+  int issued = k; /* the last frame whose stage A is issued */
   if (!on_device && k + 1 < nframes &&
-      vsbd_upload(st->dev, frames + (size_t)(k + 1) * frame_bytes, linesize, (k + 1) & 1) != 0) {
+      vsbd_upload(st->dev, frames + (size_t)(k + 1) * frame_bytes, linesize, (k + 1) % 3) != 0) {
     vs_log_error(md->conf.modName, "GPU upload failed: %s\n", vsbd_error());
     return -1;
   }
+  if (a_first && issued + 1 < nframes) {
+    if (issue_next_frame(md, st, frames, frame_bytes, linesize, nframes, on_device, issued + 1))
+      goto fail;
+    issued++;
+  }
   for (; k < nframes; k++) {
     int search = 0;
-    if (vsb_frame_begin(md, &search) != VS_OK || !search) return -1;
-    const int next = k + 1 < nframes;
-    const uint8_t* nsrc = frames + (size_t)(k + 1) * frame_bytes;
-    /* Plain search: frame k+1's stage A goes first, so that the GPU works
-       while the host selects frame k's fields (its results land in the other
-       output block; frame k's stay readable).  With a proposal network the
-       fine stage goes first: the network kernel fills every SM's shared
-       memory and would hold the fine stage back. */
-    const int a_first = !vsbd_proposal_on(st->dev);
+    if (vsb_frame_begin(md, &search) != VS_OK || !search) goto fail;
     vsb_frame_work w;
-    for (int pass = 0; pass < 2; pass++) {
-      if (pass == !a_first) {
-        if ((next && (on_device ? vsbd_stage_a_next_issue(st->dev, NULL, linesize, nsrc, linesize)
-                                : vsbd_stage_a_next_issue_uploaded(st->dev, (k + 1) & 1)) != 0) ||
-            (!on_device && k + 2 < nframes &&
-             vsbd_upload(st->dev, frames + (size_t)(k + 2) * frame_bytes, linesize, k & 1) != 0)) {
-          vs_log_error(md->conf.modName, "GPU stage A failed: %s\n", vsbd_error());
-          if (pass) vsb_frame_discard(&w);
-          return -1;
-        }
-      } else {
-        vsb_frame_host_a(md, mm, cres, &w);
-        if (vsbd_stage_b_issue(st->dev, w.items, w.fine_pass ? w.nitems : 0) != 0) {
-          vs_log_error(md->conf.modName, "GPU stage B failed: %s\n", vsbd_error());
-          vsb_frame_discard(&w);
-          return -1;
-        }
+    vsb_frame_host_a(md, mm, cres, &w);
+    if (vsbd_stage_b_issue(st->dev, w.items, w.fine_pass ? w.nitems : 0) != 0) {
+      vs_log_error(md->conf.modName, "GPU stage B failed: %s\n", vsbd_error());
+      vsb_frame_discard(&w);
+      goto fail;
+    }
+    while (issued < k + depth && issued + 1 < nframes) {
+      if (issue_next_frame(md, st, frames, frame_bytes, linesize, nframes, on_device,
+                           issued + 1)) {
+        const vsbd_result* unused;
+        vsb_frame_discard(&w);
+        vsbd_stage_b_collect(st->dev, &unused);
+        goto fail;
       }
+      issued++;
     }
     const vsbd_result* fres = NULL;
     if (vsbd_stage_b_collect(st->dev, &fres) != 0) {
       vs_log_error(md->conf.modName, "GPU stage B failed: %s\n", vsbd_error());
       vsb_frame_discard(&w);
-      return -1;
+      goto fail;
     }
     LocalMotions lms;
-    if (vsb_frame_host_b(md, fres, &w, &lms) != VS_OK) {
-      /* frame k+1's stage A may still be in flight: let it finish */
-      if (next) vsbd_stage_a_next_collect(st->dev, &mm, &cres);
-      return -1;
-    }
+    if (vsb_frame_host_b(md, fres, &w, &lms) != VS_OK) goto fail;
     if (vsb_frame_end(md)) vsbd_commit_prev(st->dev);
     total = append_records(&lms, rec, total, out_cap, counts ? counts + k : NULL);
-    if (next && vsbd_stage_a_next_collect(st->dev, &mm, &cres) != 0) {
+    if (k + 1 < nframes && vsbd_stage_a_next_collect(st->dev, &mm, &cres) != 0) {
       vs_log_error(md->conf.modName, "GPU stage A failed: %s\n", vsbd_error());
-      return -1;
+      goto fail;
     }
   }
   return total;
+fail:
+  /* let the stage A's still in flight finish */
+  while (vsbd_stage_a_next_collect(st->dev, &mm, &cres) == 0) {
+  }
+  return -1;
 }
 
 /* Many detectors stepped together by one host thread: for each frame, the

@@ -1236,17 +1236,18 @@ struct vsbd_ctx {
   int blur_shape;     /* vector-blur tile shape (g_blur_shape), picked by timing */
   float blur_us;      /* its tuned time per frame */
   uint8_t* d_tmp;     /* row-pass buffer of the wide-window blur */
-  uint8_t* d_buf[3];  /* blurred planes: slots of the current frame, the
-                         previous one and the next one (filled ahead while
-                         the current frame's fine search runs) */
+  uint8_t* d_buf[4];  /* blurred planes: slots of the current frame, the
+                         previous one and up to two next ones (filled ahead
+                         while the current frame's fine search runs) */
   int cur, prv;       /* slots of the current and the previous frame */
+  int nxt[2], nnxt;   /* slots of next frames whose stage A is issued, in order */
   cudaStream_t st2;   /* the fine stage */
-  cudaEvent_t ev_a, ev_b;
+  cudaEvent_t ev_b;
   /* frames uploaded ahead of their stage A (vsbd_upload), on a copy stream
      of their own; allocated on first use */
-  uint8_t* d_up[2];
+  uint8_t* d_up[3];
   cudaStream_t st3;
-  cudaEvent_t ev_up[2];
+  cudaEvent_t ev_up[3];
   int a_search, b_n;  /* the pending stages' search flag / item count */
   double thr_coarse;  /* contrast threshold of the coarse fields */
   int16_t* d_xy;      /* coarse x | coarse y | fine x | fine y */
@@ -1279,12 +1280,16 @@ struct vsbd_ctx {
   uint8_t* d_out;               /* minmax | coarse results | coarse proposal flags |
                                    fine results | fine proposal flags */
   uint8_t* h_out;               /* pinned mirror of d_out */
-  /* two such blocks: every stage A moves to the other one, so a frame's
-     stage A can run while the host still reads the previous frame's
-     results (d_out/h_out point at the current block) */
-  uint8_t* d_outs[2];
-  uint8_t* h_outs[2];
+  /* three such blocks: every stage A moves to the next one, so up to two
+     frames' stage A can run while the host still reads an earlier frame's
+     results (d_out/h_out point at the latest block) */
+  uint8_t* d_outs[3];
+  uint8_t* h_outs[3];
   int obuf;
+  /* issued stage A's not yet collected, oldest first: their output block,
+     search flag and completion event */
+  int aq_blk[3], aq_search[3], naq;
+  cudaEvent_t ev_ablk[3];
   uint8_t* b_hout;              /* host block the pending stage B copies into (a
                                    stage A may switch d_out/h_out meanwhile) */
   vsbd_item* h_items;           /* pinned staging of fine items */
@@ -1379,17 +1384,14 @@ extern "C" void vsbd_destroy(vsbd_ctx* c) {
     if (c->ev[k][0]) { cudaEventDestroy(c->ev[k][0]); cudaEventDestroy(c->ev[k][1]); }
   cudaFree(c->d_raw);
   cudaFree(c->d_tmp);
-  cudaFree(c->d_buf[0]);
-  cudaFree(c->d_buf[1]);
-  cudaFree(c->d_buf[2]);
-  if (c->ev_a) cudaEventDestroy(c->ev_a);
+  for (int k = 0; k < 4; k++) cudaFree(c->d_buf[k]);
   if (c->ev_b) cudaEventDestroy(c->ev_b);
   if (c->st2) cudaStreamDestroy(c->st2);
   if (c->st3) {
     cudaStreamSynchronize(c->st3);
     cudaStreamDestroy(c->st3);
   }
-  for (int k = 0; k < 2; k++) {
+  for (int k = 0; k < 3; k++) {
     cudaFree(c->d_up[k]);
     if (c->ev_up[k]) cudaEventDestroy(c->ev_up[k]);
   }
@@ -1398,8 +1400,10 @@ extern "C" void vsbd_destroy(vsbd_ctx* c) {
   cudaFree(c->d_fitems);
   cudaFree(c->d_keys);
   cudaFree(c->d_tickets);
-  cudaFree(c->d_outs[0]);
-  cudaFree(c->d_outs[1]);
+  for (int k = 0; k < 3; k++) {
+    cudaFree(c->d_outs[k]);
+    if (c->ev_ablk[k]) cudaEventDestroy(c->ev_ablk[k]);
+  }
   cudaFree(c->d_skip);
   cudaFree(c->d_bm_lofs);
   cudaFree(c->d_bm_list);
@@ -1409,8 +1413,8 @@ extern "C" void vsbd_destroy(vsbd_ctx* c) {
   cudaFree(c->d_lists);
   cudaFree(c->d_counts);
   cudaFree(c->d_boxes);
-  if (c->h_outs[0]) cudaFreeHost(c->h_outs[0]);
-  if (c->h_outs[1]) cudaFreeHost(c->h_outs[1]);
+  for (int k = 0; k < 3; k++)
+    if (c->h_outs[k]) cudaFreeHost(c->h_outs[k]);
   if (c->h_items) cudaFreeHost(c->h_items);
   if (c->h_swerr) cudaFreeHost(c->h_swerr);
   cudaFree(c->d_pn);
@@ -1668,16 +1672,16 @@ extern "C" int vsbd_create(vsbd_ctx** out, int W, int H, int bpp, int blur_size,
   CKC(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
   if (blur_size >= 2) CKC(cudaMalloc(&c->d_raw, plane));
   if (blur_size >= 2 && blur_size / 2 > BT_MAXHALF) CKC(cudaMalloc(&c->d_tmp, plane));
-  for (int k = 0; k < 3; k++) {
+  for (int k = 0; k < 4; k++) {
     CKC(cudaMalloc(&c->d_buf[k], plane));
     CKC(cudaMemset(c->d_buf[k], 0, plane));
   }
   c->cur = 0;
   c->prv = 1;
+  c->nnxt = 0;
   c->pn_fine_radius = -1.f;
   c->pn_passes = 1;
   CKC(cudaStreamCreateWithFlags(&c->st2, cudaStreamNonBlocking));
-  CKC(cudaEventCreateWithFlags(&c->ev_a, cudaEventDisableTiming));
   CKC(cudaEventCreateWithFlags(&c->ev_b, cudaEventDisableTiming));
   CKC(cudaMalloc(&c->d_xy, sizeof(int16_t) * 2 * (nc + nf) + 16));
   CKC(cudaMemcpy(c->d_xy, cx, sizeof(int16_t) * nc, cudaMemcpyHostToDevice));
@@ -1736,11 +1740,13 @@ extern "C" int vsbd_create(vsbd_ctx** out, int W, int H, int bpp, int blur_size,
   c->off_fine = c->off_cfb + align16((size_t)nc + 1);
   c->off_ffb = c->off_fine + align16(sizeof(vsbd_result) * (nf + 1));
   c->out_bytes = c->off_ffb + align16((size_t)nf + 1);
-  for (int k = 0; k < 2; k++) {
+  for (int k = 0; k < 3; k++) {
     CKC(cudaMalloc(&c->d_outs[k], c->out_bytes));
     CKC(cudaMallocHost(&c->h_outs[k], c->out_bytes));
+    CKC(cudaEventCreateWithFlags(&c->ev_ablk[k], cudaEventDisableTiming));
   }
   c->obuf = 0;
+  c->naq = 0;
   c->d_out = c->d_outs[0];
   c->h_out = c->h_outs[0];
   /* fine items for tuning: every fine field without offset */
@@ -1892,10 +1898,14 @@ static int stage_a_issue(vsbd_ctx* c, const uint8_t* host, int linesize, const u
   cudaStream_t st = c->st;
   uint8_t* cur = c->d_buf[ci];
   uint8_t* prv = c->d_buf[pi];
+  if (c->naq >= 3) {
+    set_msg("three stage A's already in flight");
+    return -1;
+  }
   c->a_search = search;
-  /* this stage's results go to the other output block: the previous frame's
-     stay readable until the next stage A */
-  c->obuf ^= 1;
+  /* this stage's results go to the next output block: the two earlier
+     frames' stay readable meanwhile */
+  c->obuf = (c->obuf + 1) % 3;
   c->d_out = c->d_outs[c->obuf];
   c->h_out = c->h_outs[c->obuf];
   /* the contrast flags steer the pruned and the proposal searches and mark
@@ -1985,7 +1995,10 @@ static int stage_a_issue(vsbd_ctx* c, const uint8_t* host, int linesize, const u
       CK(cudaMemcpyAsync(c->h_vres, c->d_vres, sizeof(vsbd_result) * c->nc, cudaMemcpyDeviceToHost,
                          st));
   }
-  CK(cudaEventRecord(c->ev_a, st));
+  CK(cudaEventRecord(c->ev_ablk[c->obuf], st));
+  c->aq_blk[c->naq] = c->obuf;
+  c->aq_search[c->naq] = search;
+  c->naq++;
   return 0;
 }
 
@@ -2002,15 +2015,51 @@ static int sweep_failed(vsbd_ctx* c, int k) {
   return 1;
 }
 
+/* waits for the oldest issued stage A and hands out its results */
 static int stage_a_collect(vsbd_ctx* c, const uint8_t** minmax, const vsbd_result** coarse) {
-  CK(cudaEventSynchronize(c->ev_a));
+  if (c->naq <= 0) {
+    set_msg("no stage A in flight");
+    return -1;
+  }
+  const int blk = c->aq_blk[0], search = c->aq_search[0];
+  for (int i = 1; i < c->naq; i++) {
+    c->aq_blk[i - 1] = c->aq_blk[i];
+    c->aq_search[i - 1] = c->aq_search[i];
+  }
+  c->naq--;
+  CK(cudaEventSynchronize(c->ev_ablk[blk]));
   kt_collect(c);
   if (sweep_failed(c, 0)) return -1;
-  if (c->a_search && c->pn_on)
-    proposal_tally(c, c->h_out + c->off_cfb, (const vsbd_result*)(c->h_out + c->off_coarse),
-                   c->h_vres, c->nc, 0);
-  if (minmax) *minmax = c->h_out;
-  if (coarse) *coarse = (const vsbd_result*)(c->h_out + c->off_coarse);
+  uint8_t* h = c->h_outs[blk];
+  if (search && c->pn_on)
+    proposal_tally(c, h + c->off_cfb, (const vsbd_result*)(h + c->off_coarse), c->h_vres, c->nc,
+                   0);
+  if (minmax) *minmax = h;
+  if (coarse) *coarse = (const vsbd_result*)(h + c->off_coarse);
+  return 0;
+}
+
+/* a blurred-plane slot that no frame in use holds */
+static int free_slot(const vsbd_ctx* c) {
+  for (int k = 0; k < 4; k++) {
+    bool used = k == c->cur || k == c->prv;
+    for (int i = 0; i < c->nnxt; i++) used = used || k == c->nxt[i];
+    if (!used) return k;
+  }
+  return -1;
+}
+
+/* stage A of the frame after the last one issued: blurred into a free slot,
+   searched against that frame's plane */
+static int stage_a_next(vsbd_ctx* c, const uint8_t* dev, int pitch) {
+  if (c->nnxt >= 2) {
+    set_msg("two next frames already in flight");
+    return -1;
+  }
+  const int slot = free_slot(c);
+  const int against = c->nnxt > 0 ? c->nxt[c->nnxt - 1] : c->cur;
+  if (slot < 0 || stage_a_issue(c, NULL, 0, dev, pitch, 1, slot, against) != 0) return -1;
+  c->nxt[c->nnxt++] = slot;
   return 0;
 }
 
@@ -2031,22 +2080,24 @@ extern "C" int vsbd_stage_a_issue(vsbd_ctx* c, const uint8_t* host, int linesize
 extern "C" int vsbd_stage_a_next_issue(vsbd_ctx* c, const uint8_t* host, int linesize,
                                        const uint8_t* dev, int pitch) {
   CK(cudaSetDevice(c->dev));
-  /* the next frame: blurred into the slot neither this frame nor its
-     previous one uses, searched against this frame's plane */
-  return stage_a_issue(c, host, linesize, dev, pitch, 1, 3 - c->cur - c->prv, c->cur);
+  if (host) {
+    set_msg("the next frame's stage A takes device planes (vsbd_upload for host frames)");
+    return -1;
+  }
+  return stage_a_next(c, dev, pitch);
 }
 
 extern "C" int vsbd_proposal_on(const vsbd_ctx* c) { return c && c->pn_on; }
 
 extern "C" int vsbd_upload(vsbd_ctx* c, const uint8_t* host, int linesize, int slot) {
   CK(cudaSetDevice(c->dev));
-  if (slot < 0 || slot > 1) {
-    set_msg("upload slot must be 0 or 1");
+  if (slot < 0 || slot > 2) {
+    set_msg("upload slot must be 0, 1 or 2");
     return -1;
   }
   if (!c->st3) {
     const size_t plane = (size_t)c->pitch * c->H + 256;
-    for (int k = 0; k < 2; k++) {
+    for (int k = 0; k < 3; k++) {
       if (!c->d_up[k]) CK(cudaMalloc(&c->d_up[k], plane));
       if (!c->ev_up[k]) CK(cudaEventCreateWithFlags(&c->ev_up[k], cudaEventDisableTiming));
     }
@@ -2062,13 +2113,13 @@ extern "C" int vsbd_upload(vsbd_ctx* c, const uint8_t* host, int linesize, int s
 
 extern "C" int vsbd_stage_a_next_issue_uploaded(vsbd_ctx* c, int slot) {
   CK(cudaSetDevice(c->dev));
-  if (slot < 0 || slot > 1 || !c->d_up[slot]) {
+  if (slot < 0 || slot > 2 || !c->d_up[slot]) {
     set_msg("no frame uploaded in that slot");
     return -1;
   }
   /* the next frame's stage A starts once its upload has landed */
   CK(cudaStreamWaitEvent(c->st, c->ev_up[slot], 0));
-  return stage_a_issue(c, NULL, 0, c->d_up[slot], c->pitch, 1, 3 - c->cur - c->prv, c->cur);
+  return stage_a_next(c, c->d_up[slot], c->pitch);
 }
 
 extern "C" int vsbd_stage_a_next_collect(vsbd_ctx* c, const uint8_t** minmax,
@@ -2143,10 +2194,17 @@ extern "C" int vsbd_stage_b(vsbd_ctx* c, const vsbd_item* items, int n, const vs
   return vsbd_stage_b_collect(c, fine);
 }
 
-/* the current plane becomes the previous one; the third slot takes the next
-   frame */
+/* the current plane becomes the previous one; the next frame takes the
+   slot its issued stage A blurred into, or a free one */
 extern "C" void vsbd_commit_prev(vsbd_ctx* c) {
-  const int f = 3 - c->cur - c->prv;
+  int f;
+  if (c->nnxt > 0) {
+    f = c->nxt[0];
+    c->nxt[0] = c->nxt[1];
+    c->nnxt--;
+  } else {
+    f = free_slot(c);
+  }
   c->prv = c->cur;
   c->cur = f;
 }
