@@ -827,11 +827,12 @@ long vsb_detect_run_overlapped(VSMotionDetect* md, const uint8_t* frames, long f
      are kept in flight, so frame k+2's stage A is issued right after frame
      k's fine stage, before the host waits for that stage and assembles frame
      k; the GPU then has queued work while the host does.  With a proposal
-     network only frame k+1's, issued after frame k's fine stage (the network
-     kernel fills every SM's shared memory and would hold the fine stage
-     back). */
+     network frame k+1's stage A is not issued before frame k's fine stage
+     (the network kernel fills every SM's shared memory and would hold the
+     fine stage back), and while its verification runs only one frame's
+     stage A is kept in flight. */
   const int a_first = !vsbd_proposal_on(st->dev);
-  const int depth = a_first ? 2 : 1;
+  const int depth = vsbd_pipeline_depth(st->dev);
   int issued = k; /* the last frame whose stage A is issued */
   if (!on_device && k + 1 < nframes &&
       vsbd_upload(st->dev, frames + (size_t)(k + 1) * frame_bytes, linesize, (k + 1) % 3) != 0) {

@@ -2089,6 +2089,13 @@ extern "C" int vsbd_stage_a_next_issue(vsbd_ctx* c, const uint8_t* host, int lin
 
 extern "C" int vsbd_proposal_on(const vsbd_ctx* c) { return c && c->pn_on; }
 
+/* how many frames' stage A a frame loop may keep in flight: one while the
+   proposal's verification runs (every stage A copies its full-search
+   results into the one host array the collect tallies), else two */
+extern "C" int vsbd_pipeline_depth(const vsbd_ctx* c) {
+  return c && c->pn_on && c->pn_verify ? 1 : 2;
+}
+
 extern "C" int vsbd_upload(vsbd_ctx* c, const uint8_t* host, int linesize, int slot) {
   CK(cudaSetDevice(c->dev));
   if (slot < 0 || slot > 2) {

@@ -104,6 +104,8 @@ int vsbd_stage_a_next_collect(vsbd_ctx* c, const uint8_t** minmax, const vsbd_re
 int vsbd_upload(vsbd_ctx* c, const uint8_t* host, int linesize, int slot);
 /* whether the detector searches with a proposal network */
 int vsbd_proposal_on(const vsbd_ctx* c);
+/* frames whose stage A a frame loop may keep in flight (1 or 2) */
+int vsbd_pipeline_depth(const vsbd_ctx* c);
 int vsbd_stage_a_next_issue_uploaded(vsbd_ctx* c, int slot);
 int vsbd_stage_b_issue(vsbd_ctx* c, const vsbd_item* items, int n);
 int vsbd_stage_b_collect(vsbd_ctx* c, const vsbd_result** fine);
