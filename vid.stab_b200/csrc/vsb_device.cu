@@ -32,6 +32,7 @@
 #include "vsb_search.cuh"
 #include "vsb_sweep.cuh"
 #include "vsb_blurmm.cuh"
+#include "vsb_finewarp.cuh"
 
 /* ------------------------------------------------------------------------ */
 /* error plumbing                                                            */
@@ -720,6 +721,52 @@ static int sweep_candidates(const DGeom& g, int nitems, TileCand* out, int cap) 
   const int sms = sm_count();
   const int regs = sweep_regs(g.step, g.S / 16);
   if (regs <= 0) return 0;
+  /* the plan (ncg column groups of 8, nbb lattice rows, ns field strips)
+     with its modelled time, or false when it does not fit */
+  auto make = [&](int ncg, int nbb, int ns, TileCand* c) -> bool {
+    if (g.S % ns || g.S / ns < 2) return false;
+    const int ntask = ncg * nbb * ns;
+    const int threads = (ntask + 31) & ~31;
+    if (threads > SW_MAX_THREADS || threads < 64) return false;
+    DGeom t = g;
+    t.ta = 5;
+    t.tb = 1;
+    t.nab = ncg * SW_TA;
+    t.nbb = nbb;
+    t.nta = (g.na + t.nab - 1) / t.nab;
+    t.ntb = (g.nb + nbb - 1) / nbb;
+    t.nstrip = ns;
+    t.threads = threads;
+    const SweepLayout L = sweep_layout(t);
+    if (L.total > lim) return false;
+    int cps = (int)((228 * 1024) / (L.total + 2048));
+    if (2048 / threads < cps) cps = 2048 / threads;
+    if (65536 / (threads * regs) < cps) cps = 65536 / (threads * regs);
+    if (cps < 1) return false;
+    if (cps > 4) cps = 4;
+    const long T = (long)nitems * t.nta * t.ntb;
+    t.ctas = (int)(T < (long)sms * cps ? T : (long)sms * cps);
+    const long per_cta = (T + t.ctas - 1) / t.ctas;
+    /* a tile's lane-SAD slots (padded columns and rows included), the
+       per-row loads of each thread, and a fixed cost per tile */
+    const int Rs = g.S / ns;
+    const double work = (double)t.nab * nbb * g.S * (g.S / 4) +
+                        (double)ntask * Rs * (sw_chunks(g.step, g.S / 16) + 2 * (g.S / 16) + 12);
+    const double warps = (double)cps * threads / 32.0;
+    const double occ = warps >= 12 ? 1.0 : warps / 12.0;
+    c->clk = (double)per_cta * (work / (64.0 / cps) / occ + 2500.0);
+    c->g = t;
+    return true;
+  };
+  /* plans whose one tile holds an item's whole lattice (the fine fields):
+     timed whatever the model says */
+  TileCand whole[3];
+  int nwhole = 0;
+  if (g.nb <= 48)
+    for (int ns = 1; ns <= 4 && nwhole < 3; ns *= 2)
+      if (make((g.na + SW_TA - 1) / SW_TA, g.nb, ns, &whole[nwhole])) nwhole++;
+  if (nwhole > cap / 3) nwhole = cap / 3;
+  const int mcap = cap - nwhole;
   int n = 0, ncg_prev = -1;
   for (int split = 1; split <= 3; split++) {
     const int ncg = ((g.na + split - 1) / split + SW_TA - 1) / SW_TA;
@@ -727,49 +774,21 @@ static int sweep_candidates(const DGeom& g, int nitems, TileCand* out, int cap) 
     ncg_prev = ncg;
     for (int nbb = 1; nbb <= 24 && nbb <= g.nb; nbb++)
       for (int ns = 1; ns <= 16; ns *= 2) {
-        if (g.S % ns || g.S / ns < 2) continue;
-        const int ntask = ncg * nbb * ns;
-        const int threads = (ntask + 31) & ~31;
-        if (threads > SW_MAX_THREADS || threads < 64) continue;
-        DGeom t = g;
-        t.ta = 5;
-        t.tb = 1;
-        t.nab = ncg * SW_TA;
-        t.nbb = nbb;
-        t.nta = (g.na + t.nab - 1) / t.nab;
-        t.ntb = (g.nb + nbb - 1) / nbb;
-        t.nstrip = ns;
-        t.threads = threads;
-        const SweepLayout L = sweep_layout(t);
-        if (L.total > lim) continue;
-        int cps = (int)((228 * 1024) / (L.total + 2048));
-        if (2048 / threads < cps) cps = 2048 / threads;
-        if (65536 / (threads * regs) < cps) cps = 65536 / (threads * regs);
-        if (cps < 1) continue;
-        if (cps > 4) cps = 4;
-        const long T = (long)nitems * t.nta * t.ntb;
-        t.ctas = (int)(T < (long)sms * cps ? T : (long)sms * cps);
-        const long per_cta = (T + t.ctas - 1) / t.ctas;
-        /* a tile's lane-SAD slots (padded columns and rows included), the
-           per-row loads of each thread, and a fixed cost per tile */
-        const int Rs = g.S / ns;
-        const double work = (double)t.nab * nbb * g.S * (g.S / 4) +
-                            (double)ntask * Rs * (sw_chunks(g.step, g.S / 16) + 2 * (g.S / 16) + 12);
-        const double warps = (double)cps * threads / 32.0;
-        const double occ = warps >= 12 ? 1.0 : warps / 12.0;
-        const double clk = (double)per_cta * (work / (64.0 / cps) / occ + 2500.0);
-        int pos = n < cap ? n : cap;
-        while (pos > 0 && out[pos - 1].clk > clk) {
-          if (pos < cap) out[pos] = out[pos - 1];
+        TileCand c;
+        if (!make(ncg, nbb, ns, &c)) continue;
+        if (c.g.nbb == g.nb && c.g.nab >= g.na) continue; /* already among the whole plans */
+        int pos = n < mcap ? n : mcap;
+        while (pos > 0 && out[pos - 1].clk > c.clk) {
+          if (pos < mcap) out[pos] = out[pos - 1];
           pos--;
         }
-        if (pos < cap) {
-          out[pos].clk = clk;
-          out[pos].g = t;
-          if (n < cap) n++;
+        if (pos < mcap) {
+          out[pos] = c;
+          if (n < mcap) n++;
         }
       }
   }
+  for (int k = 0; k < nwhole; k++) out[n++] = whole[k];
   return n;
 }
 
@@ -818,6 +837,45 @@ static int launch_sweep(const DGeom& g, const uint8_t* curr, const uint8_t* prev
 #undef VSB_SW_LAUNCH
   set_msg("no sweep compiled for this field geometry");
   return -1;
+}
+
+/* k_fine over items[0 .. n): one CTA of `warps` warps per item */
+static int launch_fine_warp(const GeomDev& gd, int warps, const uint8_t* curr,
+                            const uint8_t* prev, int pitch, const vsbd_item* d_items, int n,
+                            vsbd_result* d_res, cudaStream_t st) {
+  if (n <= 0) return 0;
+  const DGeom& g = gd.g;
+  if (!fw_supported(g) || warps < 1 || warps > FW_MAX_WARPS) {
+    set_msg("k_fine does not take this field geometry");
+    return -1;
+  }
+  const int nt = 32 * warps;
+  const size_t smem = fw_layout(g, nt).total;
+  if (smem > search_smem_limit()) {
+    set_msg("k_fine: the search window does not fit in shared memory");
+    return -1;
+  }
+  cudaError_t e = cudaSuccess;
+  switch (g.S) {
+    case 16:
+      e = ensure_smem((const void*)k_fine<16>, 50, smem);
+      if (e == cudaSuccess) k_fine<16><<<n, nt, smem, st>>>(curr, prev, pitch, g, d_items, d_res);
+      break;
+    case 32:
+      e = ensure_smem((const void*)k_fine<32>, 51, smem);
+      if (e == cudaSuccess) k_fine<32><<<n, nt, smem, st>>>(curr, prev, pitch, g, d_items, d_res);
+      break;
+    default:
+      e = ensure_smem((const void*)k_fine<48>, 52, smem);
+      if (e == cudaSuccess) k_fine<48><<<n, nt, smem, st>>>(curr, prev, pitch, g, d_items, d_res);
+      break;
+  }
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_err("k_fine launch", e);
+    return -1;
+  }
+  return 1;
 }
 
 /* full search of the items in list[0 .. *count), at most n of them:
@@ -1221,6 +1279,92 @@ int vsbd_plan_search(const vsbd_geom* h, int nitems, DGeom* out) {
   return 0;
 }
 
+/* The fine pass on k_fine: timed against the search the detector would
+   otherwise run (the sweep plan or the per-tile search), on the detector's
+   own buffers and every fine field; kept when faster.  Cached per device and
+   geometry.  VSB_NO_FINEWARP: never; VSB_FORCE_FINEWARP: always (tests). */
+struct FineTune {
+  int dev, S, step, na, nb, nstages, nitems, warps;
+};
+static FineTune g_fwtune[64];
+static int g_nfwtune = 0;
+
+static int autotune_fine_warp(const GeomDev& gd, const DGeom* swplan, int sw_on,
+                              const uint8_t* curr, const uint8_t* prev, int pitch,
+                              const vsbd_item* d_items, int n, unsigned long long* keys,
+                              unsigned* tickets, vsbd_result* d_res, unsigned* err,
+                              cudaStream_t st, int* warps_out) {
+  *warps_out = 0;
+  const DGeom& g = gd.g;
+  if (n <= 0 || !fw_supported(g) || getenv("VSB_NO_FINEWARP") || getenv("VSB_NO_AUTOTUNE"))
+    return 0;
+  const bool force = getenv("VSB_FORCE_FINEWARP") != NULL;
+  if (!force && getenv("VSB_FORCE_SWEEP")) return 0; /* the sweep was asked for */
+  TuneLock lock;
+  const int dev = current_device();
+  for (int i = 0; !force && i < g_nfwtune; i++) {
+    const FineTune& e = g_fwtune[i];
+    if (e.dev == dev && e.S == g.S && e.step == g.step && e.na == g.na && e.nb == g.nb &&
+        e.nstages == g.nstages && e.nitems == n) {
+      *warps_out = e.warps;
+      return 0;
+    }
+  }
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  auto time_of = [&](int warps) -> float {
+    auto one = [&]() {
+      if (warps > 0)
+        return launch_fine_warp(gd, warps, curr, prev, pitch, d_items, n, d_res, st);
+      return sw_on ? launch_sweep(*swplan, curr, prev, pitch, d_items, n, keys, tickets, d_res,
+                                  err, st)
+                   : launch_search(gd, curr, prev, pitch, d_items, n, keys, tickets, d_res, st);
+    };
+    if (one() < 0) {
+      cudaGetLastError();
+      return -1.f;
+    }
+    cudaEventRecord(e0, st);
+    for (int r = 0; r < 5; r++) one();
+    cudaEventRecord(e1, st);
+    if (cudaEventSynchronize(e1) != cudaSuccess) return -1.f;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    return ms / 5;
+  };
+  for (int w = 0; w < 3; w++) time_of(0); /* clocks up */
+  const float base = time_of(0);
+  int best_w = 0;
+  float best_ms = base > 0.f ? base : 3.0e38f;
+  for (int warps = 2; warps <= FW_MAX_WARPS; warps *= 2) {
+    const float ms = time_of(warps);
+    if (getenv("VSB_DEBUG_TUNE"))
+      fprintf(stderr, "fine tuning S=%d items=%d: k_fine %d warps %.1f us (current %.1f us)\n", g.S,
+              n, warps, 1000.f * ms, 1000.f * base);
+    if (ms > 0.f && (ms < best_ms || (force && best_w == 0))) {
+      best_ms = ms;
+      best_w = warps;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaGetLastError();
+  *warps_out = best_w;
+  if (!force && g_nfwtune < 64) {
+    FineTune& t = g_fwtune[g_nfwtune++];
+    t.dev = dev;
+    t.S = g.S;
+    t.step = g.step;
+    t.na = g.na;
+    t.nb = g.nb;
+    t.nstages = g.nstages;
+    t.nitems = n;
+    t.warps = best_w;
+  }
+  return 0;
+}
+
 extern "C" void vsbd_set_error(const char* msg) { set_msg(msg); }
 
 /* ------------------------------------------------------------------------ */
@@ -1257,6 +1401,7 @@ struct vsbd_ctx {
      its bounded waits raise ([0] coarse, [1] fine; mapped pinned memory) */
   DGeom swc, swf;
   int sw_c, sw_f;
+  int fw_f, fw_warps; /* fine pass on k_fine, warps per item */
   unsigned* h_swerr;
   unsigned* d_swerr;
   vsbd_item* d_citems;
@@ -1785,6 +1930,15 @@ extern "C" int vsbd_create(vsbd_ctx** out, int W, int H, int bpp, int blur_size,
     vsbd_destroy(c);
     return -1;
   }
+  if (c->bpp == 1 && c->nch == 1 &&
+      autotune_fine_warp(c->gf, &c->swf, c->sw_f, c->d_buf[0], c->d_buf[1], c->pitch, c->d_fitems,
+                         nf, c->d_keys + nc, c->d_tickets + nc,
+                         (vsbd_result*)(c->d_out + c->off_fine), c->d_swerr + 1, c->st,
+                         &c->fw_warps) != 0) {
+    vsbd_destroy(c);
+    return -1;
+  }
+  c->fw_f = c->fw_warps > 0;
   CKC(cudaStreamSynchronize(c->st));
 #undef CKC
   *out = c;
@@ -2161,6 +2315,8 @@ extern "C" int vsbd_stage_b_issue(vsbd_ctx* c, const vsbd_item* items, int n) {
                                      c->d_part, c->d_counts + c->nc, c->d_lists,
                                      c->d_boxes + 4 * c->nc, c->d_keys + c->nc,
                                      c->d_tickets + c->nc, fres, st)
+             : c->fw_f ? launch_fine_warp(c->gf, c->fw_warps, cur, prv, c->pitch, c->d_fitems, n,
+                                          fres, st)
              : c->sw_f ? launch_sweep(c->swf, cur, prv, c->pitch, c->d_fitems, n, c->d_keys + c->nc,
                                       c->d_tickets + c->nc, fres, c->d_swerr + 1, st)
                      : launch_search(c->gf, cur, prv, c->pitch, c->d_fitems, n, c->d_keys + c->nc,
@@ -2227,6 +2383,19 @@ extern "C" long vsbd_launches(const vsbd_ctx* c) { return c ? c->launches : 0; }
 
 extern "C" int vsbd_search_tiling(const vsbd_ctx* c, int fine, int* desc) {
   if (!c || !desc) return -1;
+  if (fine && c->fw_f) {
+    /* k_fine: layout 6, one CTA of desc[5] threads per field */
+    const DGeom& g = c->gf.g;
+    desc[0] = 1;
+    desc[1] = 6;
+    desc[2] = g.na;
+    desc[3] = g.nb;
+    desc[4] = 1;
+    desc[5] = 32 * c->fw_warps;
+    desc[6] = (int)fw_layout(g, 32 * c->fw_warps).total;
+    desc[7] = 1;
+    return 0;
+  }
   const int sw = fine ? c->sw_f : c->sw_c;
   const DGeom& g = sw ? (fine ? c->swf : c->swc) : (fine ? c->gf.g : c->gc.g);
   desc[0] = g.tb;
@@ -2458,7 +2627,10 @@ extern "C" int vsbd_search_host(const uint8_t* curr, const uint8_t* prev, int W,
   int rc = -1;
   cudaError_t e;
   /* tiles_hint < 0: the sweep, with the plan of that rank in its candidate
-     list (-1 the model's best) */
+     list (-1 the model's best); tiles_hint <= -100: k_fine with -100 -
+     tiles_hint warps per item */
+  const int fw_warps = tiles_hint <= -100 ? -100 - tiles_hint : 0;
+  if (fw_warps) tiles_hint = 0;
   DGeom swg;
   unsigned* d_err = NULL;
   unsigned h_err = 0;
@@ -2485,7 +2657,9 @@ extern "C" int vsbd_search_host(const uint8_t* curr, const uint8_t* prev, int W,
   cudaMemcpy2D(d_c, pitch, curr, (size_t)W * bpp, (size_t)W * bpp, H, cudaMemcpyHostToDevice);
   cudaMemcpy2D(d_p, pitch, prev, (size_t)W * bpp, (size_t)W * bpp, H, cudaMemcpyHostToDevice);
   cudaMemcpy(d_items, items, sizeof(vsbd_item) * n, cudaMemcpyHostToDevice);
-  if (tiles_hint < 0) {
+  if (fw_warps) {
+    if (launch_fine_warp(gd, fw_warps, d_c, d_p, pitch, d_items, n, d_res, 0) < 0) goto done;
+  } else if (tiles_hint < 0) {
     if (launch_sweep(swg, d_c, d_p, pitch, d_items, n, d_keys, d_tk, d_res, d_err, 0) < 0)
       goto done;
     if ((e = cudaMemcpy(&h_err, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost)) != cudaSuccess) { set_err("k_sweep", e); goto done; }
