@@ -856,11 +856,14 @@ def main():
         for name, fine in (("coarse", 0), ("fine", 1)):
             desc = (C.c_int * 8)()
             L.vsb_search_tiling(C.byref(det.md), fine, desc)
-            tiling[name] = {"kernel": "k_sweep" if desc[1] == 5 else "k_lattice",
+            kern = {5: "k_sweep", 6: "k_fine"}.get(desc[1], "k_lattice")
+            tiling[name] = {"kernel": kern,
                             "layout": desc[1], "lattice_cols_per_tile": desc[2],
                             "lattice_rows_per_tile": desc[3], "strips": desc[4],
                             "threads": desc[5], "smem": desc[6],
                             ("ctas" if desc[1] == 5 else "ctas_per_field"): desc[7]}
+            if desc[1] == 6:
+                tiling[name]["lattice_rows_per_thread"] = tiling[name].pop("strips")
         bdesc = (C.c_int * 4)()
         L.vsb_blur_tiling(C.byref(det.md), bdesc)
         fused = bool(bdesc[3])

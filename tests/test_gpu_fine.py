@@ -21,13 +21,17 @@ FINE = [(16, 16, 2), (32, 32, 2), (48, 48, 2), (32, 20, 2)]
 
 
 @pytest.mark.parametrize("size,ms,step", FINE)
-@pytest.mark.parametrize("warps", [1, 2, 4, 8])
-def test_fine_field_search(size, ms, step, warps):
+@pytest.mark.parametrize("warps,rows", [(1, 1), (2, 1), (4, 1), (8, 1), (1, 2), (4, 2),
+                                        (1, 4), (2, 4), (8, 4)])
+def test_fine_field_search(size, ms, step, warps, rows):
+    """rows: lattice rows per thread (the window rows are walked once for all
+    of them); the test hook's tiles value is -100 - (10 * rows + warps)"""
     w, h = 1280, 720
-    curr, prev = _blurred_pair(w, h, seed=size + warps)
-    xs, ys, ox, oy = _fields(w, h, size, ms, step, size * 5 + ms + warps)
+    curr, prev = _blurred_pair(w, h, seed=size + warps + rows)
+    xs, ys, ox, oy = _fields(w, h, size, ms, step, size * 5 + ms + warps + rows)
+    code = warps if rows == 1 else 10 * rows + warps
     sad, tx, ty, ok = V.field_search(curr, prev, xs, ys, size, ms, step, ox, oy,
-                                     tiles=-100 - warps)
+                                     tiles=-100 - code)
     for k in range(len(xs)):
         exp = orc_search(curr, prev, int(xs[k]), int(ys[k]), size, ms, step, int(ox[k]),
                          int(oy[k]))
@@ -47,11 +51,12 @@ def test_fine_ties():
     for curr, prev in [(flat, flat), (periodic, periodic), (periodic, np.roll(periodic, 3, 1)),
                        (stripes, stripes)]:
         for size, ms, step in [(32, 32, 2), (16, 16, 2)]:
-            sad, tx, ty, ok = V.field_search(curr, prev, xs, ys, size, ms, step, tiles=-102)
-            for k in range(len(xs)):
-                exp = orc_search(curr, prev, int(xs[k]), int(ys[k]), size, ms, step)
-                assert (sad[k], tx[k], ty[k], bool(ok[k])) == (exp[0], exp[1], exp[2],
-                                                               bool(exp[3]))
+            for tiles in (-102, -142):
+                sad, tx, ty, ok = V.field_search(curr, prev, xs, ys, size, ms, step, tiles=tiles)
+                for k in range(len(xs)):
+                    exp = orc_search(curr, prev, int(xs[k]), int(ys[k]), size, ms, step)
+                    assert (sad[k], tx[k], ty[k], bool(ok[k])) == (exp[0], exp[1], exp[2],
+                                                                   bool(exp[3])), tiles
 
 
 @pytest.mark.parametrize("w,h,n", [(640, 360, 5), (1920, 1080, 4), (3840, 2160, 3)])

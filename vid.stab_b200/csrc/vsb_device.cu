@@ -839,14 +839,15 @@ static int launch_sweep(const DGeom& g, const uint8_t* curr, const uint8_t* prev
   return -1;
 }
 
-/* k_fine over items[0 .. n): one CTA of `warps` warps per item */
-static int launch_fine_warp(const GeomDev& gd, int warps, const uint8_t* curr,
+/* k_fine over items[0 .. n): one CTA of `warps` warps per item, T lattice
+   rows per thread (1, 2 or 4) */
+static int launch_fine_warp(const GeomDev& gd, int warps, int T, const uint8_t* curr,
                             const uint8_t* prev, int pitch, const vsbd_item* d_items, int n,
                             vsbd_result* d_res, cudaStream_t st) {
   if (n <= 0) return 0;
   const DGeom& g = gd.g;
-  if (!fw_supported(g) || warps < 1 || warps > FW_MAX_WARPS) {
-    set_msg("k_fine does not take this field geometry");
+  if (!fw_supported(g) || warps < 1 || warps > FW_MAX_WARPS || (T != 1 && T != 2 && T != 4)) {
+    set_msg("k_fine does not take this field geometry or configuration");
     return -1;
   }
   const int nt = 32 * warps;
@@ -855,21 +856,17 @@ static int launch_fine_warp(const GeomDev& gd, int warps, const uint8_t* curr,
     set_msg("k_fine: the search window does not fit in shared memory");
     return -1;
   }
-  cudaError_t e = cudaSuccess;
-  switch (g.S) {
-    case 16:
-      e = ensure_smem((const void*)k_fine<16>, 50, smem);
-      if (e == cudaSuccess) k_fine<16><<<n, nt, smem, st>>>(curr, prev, pitch, g, d_items, d_res);
-      break;
-    case 32:
-      e = ensure_smem((const void*)k_fine<32>, 51, smem);
-      if (e == cudaSuccess) k_fine<32><<<n, nt, smem, st>>>(curr, prev, pitch, g, d_items, d_res);
-      break;
-    default:
-      e = ensure_smem((const void*)k_fine<48>, 52, smem);
-      if (e == cudaSuccess) k_fine<48><<<n, nt, smem, st>>>(curr, prev, pitch, g, d_items, d_res);
-      break;
+  cudaError_t e = cudaErrorInvalidValue;
+#define VSB_FW(SV, TV, SLOT)                                                                   \
+  if (g.S == SV && T == TV) {                                                                \
+    e = ensure_smem((const void*)k_fine<SV, TV>, SLOT, smem);                                \
+    if (e == cudaSuccess)                                                                    \
+      k_fine<SV, TV><<<n, nt, smem, st>>>(curr, prev, pitch, g, d_items, d_res);             \
   }
+  VSB_FW(16, 1, 50) VSB_FW(16, 2, 51) VSB_FW(16, 4, 52)
+  VSB_FW(32, 1, 53) VSB_FW(32, 2, 54) VSB_FW(32, 4, 55)
+  VSB_FW(48, 1, 56) VSB_FW(48, 2, 57) VSB_FW(48, 4, 58)
+#undef VSB_FW
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) {
     set_err("k_fine launch", e);
@@ -1284,7 +1281,7 @@ int vsbd_plan_search(const vsbd_geom* h, int nitems, DGeom* out) {
    own buffers and every fine field; kept when faster.  Cached per device and
    geometry.  VSB_NO_FINEWARP: never; VSB_FORCE_FINEWARP: always (tests). */
 struct FineTune {
-  int dev, S, step, na, nb, nstages, nitems, warps;
+  int dev, S, step, na, nb, nstages, nitems, warps, T;
 };
 static FineTune g_fwtune[64];
 static int g_nfwtune = 0;
@@ -1293,8 +1290,9 @@ static int autotune_fine_warp(const GeomDev& gd, const DGeom* swplan, int sw_on,
                               const uint8_t* curr, const uint8_t* prev, int pitch,
                               const vsbd_item* d_items, int n, unsigned long long* keys,
                               unsigned* tickets, vsbd_result* d_res, unsigned* err,
-                              cudaStream_t st, int* warps_out) {
+                              cudaStream_t st, int* warps_out, int* t_out) {
   *warps_out = 0;
+  *t_out = 1;
   const DGeom& g = gd.g;
   if (n <= 0 || !fw_supported(g) || getenv("VSB_NO_FINEWARP") || getenv("VSB_NO_AUTOTUNE"))
     return 0;
@@ -1307,16 +1305,17 @@ static int autotune_fine_warp(const GeomDev& gd, const DGeom* swplan, int sw_on,
     if (e.dev == dev && e.S == g.S && e.step == g.step && e.na == g.na && e.nb == g.nb &&
         e.nstages == g.nstages && e.nitems == n) {
       *warps_out = e.warps;
+      *t_out = e.T;
       return 0;
     }
   }
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
-  auto time_of = [&](int warps) -> float {
+  auto time_of = [&](int warps, int T) -> float {
     auto one = [&]() {
       if (warps > 0)
-        return launch_fine_warp(gd, warps, curr, prev, pitch, d_items, n, d_res, st);
+        return launch_fine_warp(gd, warps, T, curr, prev, pitch, d_items, n, d_res, st);
       return sw_on ? launch_sweep(*swplan, curr, prev, pitch, d_items, n, keys, tickets, d_res,
                                   err, st)
                    : launch_search(gd, curr, prev, pitch, d_items, n, keys, tickets, d_res, st);
@@ -1333,24 +1332,30 @@ static int autotune_fine_warp(const GeomDev& gd, const DGeom* swplan, int sw_on,
     cudaEventElapsedTime(&ms, e0, e1);
     return ms / 5;
   };
-  for (int w = 0; w < 3; w++) time_of(0); /* clocks up */
-  const float base = time_of(0);
-  int best_w = 0;
+  for (int w = 0; w < 3; w++) time_of(0, 1); /* clocks up */
+  const float base = time_of(0, 1);
+  int best_w = 0, best_t = 1;
   float best_ms = base > 0.f ? base : 3.0e38f;
-  for (int warps = 2; warps <= FW_MAX_WARPS; warps *= 2) {
-    const float ms = time_of(warps);
-    if (getenv("VSB_DEBUG_TUNE"))
-      fprintf(stderr, "fine tuning S=%d items=%d: k_fine %d warps %.1f us (current %.1f us)\n", g.S,
-              n, warps, 1000.f * ms, 1000.f * base);
-    if (ms > 0.f && (ms < best_ms || (force && best_w == 0))) {
-      best_ms = ms;
-      best_w = warps;
+  for (int T = 1; T <= 4; T *= 2)
+    for (int warps = 1; warps <= FW_MAX_WARPS; warps *= 2) {
+      /* at least a third of the threads have a task */
+      const int tasks = ((g.na + 7) / 8) * ((g.nb + T - 1) / T);
+      if (32 * warps > 3 * tasks + 32) continue;
+      const float ms = time_of(warps, T);
+      if (getenv("VSB_DEBUG_TUNE"))
+        fprintf(stderr, "fine tuning S=%d items=%d: k_fine %d warps x %d rows %.1f us (current %.1f us)\n",
+                g.S, n, warps, T, 1000.f * ms, 1000.f * base);
+      if (ms > 0.f && (ms < best_ms || (force && best_w == 0))) {
+        best_ms = ms;
+        best_w = warps;
+        best_t = T;
+      }
     }
-  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   cudaGetLastError();
   *warps_out = best_w;
+  *t_out = best_t;
   if (!force && g_nfwtune < 64) {
     FineTune& t = g_fwtune[g_nfwtune++];
     t.dev = dev;
@@ -1361,6 +1366,7 @@ static int autotune_fine_warp(const GeomDev& gd, const DGeom* swplan, int sw_on,
     t.nstages = g.nstages;
     t.nitems = n;
     t.warps = best_w;
+    t.T = best_t;
   }
   return 0;
 }
@@ -1401,7 +1407,7 @@ struct vsbd_ctx {
      its bounded waits raise ([0] coarse, [1] fine; mapped pinned memory) */
   DGeom swc, swf;
   int sw_c, sw_f;
-  int fw_f, fw_warps; /* fine pass on k_fine, warps per item */
+  int fw_f, fw_warps, fw_t; /* fine pass on k_fine: warps per item, lattice rows per thread */
   unsigned* h_swerr;
   unsigned* d_swerr;
   vsbd_item* d_citems;
@@ -1934,7 +1940,7 @@ extern "C" int vsbd_create(vsbd_ctx** out, int W, int H, int bpp, int blur_size,
       autotune_fine_warp(c->gf, &c->swf, c->sw_f, c->d_buf[0], c->d_buf[1], c->pitch, c->d_fitems,
                          nf, c->d_keys + nc, c->d_tickets + nc,
                          (vsbd_result*)(c->d_out + c->off_fine), c->d_swerr + 1, c->st,
-                         &c->fw_warps) != 0) {
+                         &c->fw_warps, &c->fw_t) != 0) {
     vsbd_destroy(c);
     return -1;
   }
@@ -2315,8 +2321,8 @@ extern "C" int vsbd_stage_b_issue(vsbd_ctx* c, const vsbd_item* items, int n) {
                                      c->d_part, c->d_counts + c->nc, c->d_lists,
                                      c->d_boxes + 4 * c->nc, c->d_keys + c->nc,
                                      c->d_tickets + c->nc, fres, st)
-             : c->fw_f ? launch_fine_warp(c->gf, c->fw_warps, cur, prv, c->pitch, c->d_fitems, n,
-                                          fres, st)
+             : c->fw_f ? launch_fine_warp(c->gf, c->fw_warps, c->fw_t, cur, prv, c->pitch,
+                                          c->d_fitems, n, fres, st)
              : c->sw_f ? launch_sweep(c->swf, cur, prv, c->pitch, c->d_fitems, n, c->d_keys + c->nc,
                                       c->d_tickets + c->nc, fres, c->d_swerr + 1, st)
                      : launch_search(c->gf, cur, prv, c->pitch, c->d_fitems, n, c->d_keys + c->nc,
@@ -2390,7 +2396,7 @@ extern "C" int vsbd_search_tiling(const vsbd_ctx* c, int fine, int* desc) {
     desc[1] = 6;
     desc[2] = g.na;
     desc[3] = g.nb;
-    desc[4] = 1;
+    desc[4] = c->fw_t;
     desc[5] = 32 * c->fw_warps;
     desc[6] = (int)fw_layout(g, 32 * c->fw_warps).total;
     desc[7] = 1;
@@ -2627,10 +2633,11 @@ extern "C" int vsbd_search_host(const uint8_t* curr, const uint8_t* prev, int W,
   int rc = -1;
   cudaError_t e;
   /* tiles_hint < 0: the sweep, with the plan of that rank in its candidate
-     list (-1 the model's best); tiles_hint <= -100: k_fine with -100 -
-     tiles_hint warps per item */
-  const int fw_warps = tiles_hint <= -100 ? -100 - tiles_hint : 0;
-  if (fw_warps) tiles_hint = 0;
+     list (-1 the model's best); tiles_hint <= -100: k_fine, -100 - tiles_hint
+     = 10 * T + warps (T lattice rows per thread, 1 when the tens are 0) */
+  const int fw_warps = tiles_hint <= -100 ? (-100 - tiles_hint) % 10 : 0;
+  const int fw_t = tiles_hint <= -100 && (-100 - tiles_hint) >= 10 ? (-100 - tiles_hint) / 10 : 1;
+  if (tiles_hint <= -100) tiles_hint = 0;
   DGeom swg;
   unsigned* d_err = NULL;
   unsigned h_err = 0;
@@ -2658,7 +2665,7 @@ extern "C" int vsbd_search_host(const uint8_t* curr, const uint8_t* prev, int W,
   cudaMemcpy2D(d_p, pitch, prev, (size_t)W * bpp, (size_t)W * bpp, H, cudaMemcpyHostToDevice);
   cudaMemcpy(d_items, items, sizeof(vsbd_item) * n, cudaMemcpyHostToDevice);
   if (fw_warps) {
-    if (launch_fine_warp(gd, fw_warps, d_c, d_p, pitch, d_items, n, d_res, 0) < 0) goto done;
+    if (launch_fine_warp(gd, fw_warps, fw_t, d_c, d_p, pitch, d_items, n, d_res, 0) < 0) goto done;
   } else if (tiles_hint < 0) {
     if (launch_sweep(swg, d_c, d_p, pitch, d_items, n, d_keys, d_tk, d_res, d_err, 0) < 0)
       goto done;

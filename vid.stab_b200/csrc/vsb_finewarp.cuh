@@ -31,7 +31,8 @@
 struct FWLayout {
   int WH, WW;  /* window rows, bytes per row the candidates and refinement read */
   int RP;      /* staged raw row pitch (bytes, 16-aligned, with slack) */
-  int WPW;     /* shifted-copy row pitch (words, odd) */
+  int WPW;     /* shifted-copy row pitch (words): a row's words, then room
+                  for its skew */
   size_t off_raw, off_c0, off_c1, off_f, off_red, off_part, total;
 };
 
@@ -40,8 +41,9 @@ __host__ __device__ inline FWLayout fw_layout(const DGeom& g, int threads) {
   const int R = refine_reach(g);
   L.WH = g.S + (g.nb - 1) * g.step + 2 * R;
   L.WW = g.S + (g.na - 1) * g.step + 2 * R;
-  L.WPW = ((15 + L.WW + 3) / 4 + 6) | 1;
-  L.RP = (4 * (L.WPW + 2) + 15) & ~15; /* every word the shifted copies read */
+  const int words = (15 + L.WW + 3) / 4 + 6; /* words of a copy row the sums read */
+  L.WPW = words + 4;                          /* + the row skew (0..3 words) */
+  L.RP = (4 * (words + 2) + 15) & ~15;        /* every raw word the copies read */
   L.off_raw = 0;
   L.off_c0 = L.off_raw + (size_t)L.WH * L.RP;
   L.off_c1 = L.off_c0 + (size_t)L.WH * L.WPW * 4;
@@ -59,51 +61,65 @@ __host__ __device__ inline bool fw_supported(const DGeom& g) {
          g.na <= 64 && g.nb <= 64;
 }
 
-/* The 8 candidate sums of lattice columns ag*8 .. ag*8+7 (those < na) and
-   lattice row b.  Column a = ag*8 + k reads, for field word w of row r, the
-   window bytes at e + R + a*2 + 4w: word J0 + JK(k) + w of copy (k & 1),
-   whose words start s0 (even k) or s0 ^ 2 (odd k) bytes into the raw row;
-   LO says whether s0 < 2 (odd columns then start one word earlier). */
-template <int S, bool LO>
+/* Copy row y starts (y >> sh) & 3 words into its slot of WPW words: the
+   threads of a warp read rows 2T apart (T lattice rows each), and the skew
+   spreads them over the shared-memory banks. */
+__device__ __forceinline__ int fw_row(int y, int WPW, int sh) { return y * WPW + ((y >> sh) & 3); }
+
+/* The sums of lattice columns ag*8 .. ag*8+7 and lattice rows b0 .. b0+nv-1
+   (nv <= T): acc[t*8 + k] for column ag*8 + k, row b0 + t.  Column a reads,
+   for field word w of row r, the window bytes at e + R + 2a + 4w: word
+   J0 + jo(k) + w of copy (k & 1), whose words start s0 (even k) or s0 ^ 2
+   (odd k) bytes into the raw row; LO says whether s0 < 2 (odd columns then
+   start one word earlier).  The window rows are walked once: row y0 + yr
+   serves lattice row b0 + t with field row yr - 2t. */
+template <int S, bool LO, int T>
 __device__ __forceinline__ void fw_sums(const uint32_t* __restrict__ F, const uint32_t* __restrict__ c0,
-                                        const uint32_t* __restrict__ c1, int WPW, int row0, int J0,
-                                        unsigned* acc) {
+                                        const uint32_t* __restrict__ c1, int WPW, int sh, int y0,
+                                        int nv, int J0, unsigned* acc) {
   constexpr int NW = S / 4;
 #pragma unroll
-  for (int k = 0; k < 8; k++) acc[k] = 0;
-#pragma unroll 2
-  for (int r = 0; r < S; r++) {
-    uint32_t f[NW];
-#pragma unroll
-    for (int q = 0; q < NW / 4; q++) {
-      const uint4 v = *(const uint4*)(F + r * NW + 4 * q);
-      f[4 * q] = v.x;
-      f[4 * q + 1] = v.y;
-      f[4 * q + 2] = v.z;
-      f[4 * q + 3] = v.w;
-    }
-    const uint32_t* w0 = c0 + (size_t)(row0 + r) * WPW + J0;
-    const uint32_t* w1 = c1 + (size_t)(row0 + r) * WPW + J0;
+  for (int k = 0; k < 8 * T; k++) acc[k] = 0;
+  const int ny = 2 * (nv - 1) + S;
+#pragma unroll 1
+  for (int yr = 0; yr < ny; yr++) {
+    const int rw = fw_row(y0 + yr, WPW, sh) + J0;
     uint32_t x0[NW + 4], x1[NW + 4];
 #pragma unroll
     for (int j = 0; j < NW + 4; j++) {
-      x0[j] = w0[j];
-      x1[j] = w1[j];
+      x0[j] = c0[rw + j];
+      x1[j] = c1[rw + j];
     }
 #pragma unroll
-    for (int k = 0; k < 8; k++) {
-      /* even k: copy 0, word offset k/2; odd k: copy 1, offset (k-1)/2 when
-         s0 < 2, else (k+1)/2 */
-      const int jo = (k & 1) ? (LO ? (k - 1) / 2 : (k + 1) / 2) : k / 2;
+    for (int t = 0; t < T; t++) {
+      const int r = yr - 2 * t;
+      if (t < nv && r >= 0 && r < S) {
+        uint32_t f[NW];
 #pragma unroll
-      for (int w = 0; w < NW; w++)
-        acc[k] = sad4(f[w], (k & 1) ? x1[jo + w] : x0[jo + w], acc[k]);
+        for (int q = 0; q < NW / 4; q++) {
+          const uint4 v = *(const uint4*)(F + r * NW + 4 * q);
+          f[4 * q] = v.x;
+          f[4 * q + 1] = v.y;
+          f[4 * q + 2] = v.z;
+          f[4 * q + 3] = v.w;
+        }
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+          /* even k: copy 0, word offset k/2; odd k: copy 1, offset (k-1)/2
+             when s0 < 2, else (k+1)/2 */
+          const int jo = (k & 1) ? (LO ? (k - 1) / 2 : (k + 1) / 2) : k / 2;
+#pragma unroll
+          for (int w = 0; w < NW; w++)
+            acc[8 * t + k] = sad4(f[w], (k & 1) ? x1[jo + w] : x0[jo + w], acc[8 * t + k]);
+        }
+      }
     }
   }
 }
 
-/* One CTA (blockDim.x = 32 * warps) per item of items[0 .. n). */
-template <int S>
+/* One CTA (blockDim.x = 32 * warps) per item of items[0 .. n); a thread
+   takes 8 lattice columns x T lattice rows. */
+template <int S, int T>
 __global__ void __launch_bounds__(FW_MAX_WARPS * 32) k_fine(const uint8_t* __restrict__ curr,
                                                           const uint8_t* __restrict__ prev,
                                                           int pitch, DGeom g,
@@ -160,34 +176,40 @@ __global__ void __launch_bounds__(FW_MAX_WARPS * 32) k_fine(const uint8_t* __res
   __syncthreads();
   /* the two shifted copies: word j of copy c holds raw bytes 4j + s_c .. + 3 */
   const int s0 = (e + R) & 3, s1 = s0 ^ 2;
-  for (int i = tid; i < L.WH * L.WPW; i += nt) {
-    const int r = i / L.WPW, j = i - r * L.WPW;
+  const int sh = T == 4 ? 3 : T == 2 ? 2 : 1; /* log2(2T): rows between a warp's threads */
+  const int nword = L.WPW - 4;
+  for (int i = tid; i < L.WH * nword; i += nt) {
+    const int r = i / nword, j = i - r * nword;
     const uint32_t* rw = (const uint32_t*)(raw + (size_t)r * L.RP) + j;
     const uint32_t a = rw[0], b = rw[1];
-    c0[i] = __funnelshift_r(a, b, 8 * s0);
-    c1[i] = __funnelshift_r(a, b, 8 * s1);
+    const int o = fw_row(r, L.WPW, sh) + j;
+    c0[o] = __funnelshift_r(a, b, 8 * s0);
+    c1[o] = __funnelshift_r(a, b, 8 * s1);
   }
   __syncthreads();
   /* every lattice candidate: a thread takes 8 columns of one lattice row */
-  const int ngrp = (g.na + 7) >> 3;
+  const int ngrp = (g.na + 7) >> 3, nbt = (g.nb + T - 1) / T;
   unsigned long long best = ~0ull;
-  for (int t = tid; t < ngrp * g.nb; t += nt) {
-    const int ag = t / g.nb, b = t - ag * g.nb;
+  for (int t = tid; t < ngrp * nbt; t += nt) {
+    const int ag = t / nbt, b0 = (t - ag * nbt) * T;
+    const int nv = min(T, g.nb - b0);
     const int J0 = (e + R + 16 * ag - s0) >> 2;
-    unsigned acc[8];
+    unsigned acc[8 * T];
     if (s0 < 2)
-      fw_sums<S, true>(F, c0, c1, L.WPW, R + 2 * b, J0, acc);
+      fw_sums<S, true, T>(F, c0, c1, L.WPW, sh, R + 2 * b0, nv, J0, acc);
     else
-      fw_sums<S, false>(F, c0, c1, L.WPW, R + 2 * b, J0, acc);
+      fw_sums<S, false, T>(F, c0, c1, L.WPW, sh, R + 2 * b0, nv, J0, acc);
 #pragma unroll
-    for (int k = 0; k < 8; k++) {
-      const int a = ag * 8 + k;
-      if (a < g.na) {
-        const unsigned long long key =
-            ((unsigned long long)acc[k] << 32) | (unsigned)g.order[b * g.na + a];
-        best = key < best ? key : best;
+    for (int u = 0; u < T; u++)
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        const int a = ag * 8 + k, b = b0 + u;
+        if (u < nv && a < g.na) {
+          const unsigned long long key =
+              ((unsigned long long)acc[8 * u + k] << 32) | (unsigned)g.order[b * g.na + a];
+          best = key < best ? key : best;
+        }
       }
-    }
   }
   best = warp_min64(best);
   if (lane == 0) red[warp] = best;
