@@ -863,7 +863,8 @@ def main():
                             "threads": desc[5], "smem": desc[6],
                             ("ctas" if desc[1] == 5 else "ctas_per_field"): desc[7]}
             if desc[1] == 6:
-                tiling[name]["lattice_rows_per_thread"] = tiling[name].pop("strips")
+                tiling[name]["lattice_rows_per_thread"] = desc[4]
+                tiling[name]["strips"] = tiling[name].pop("ctas_per_field")
         bdesc = (C.c_int * 4)()
         L.vsb_blur_tiling(C.byref(det.md), bdesc)
         fused = bool(bdesc[3])

@@ -20,18 +20,23 @@ pytestmark = pytest.mark.gpu
 FINE = [(16, 16, 2), (32, 32, 2), (48, 48, 2), (32, 20, 2)]
 
 
+def hook(warps, rows=1, strips=1):
+    """the test hook's tiles value of k_fine"""
+    return -100 - (warps + (100 * rows if rows > 1 else 0) + (1000 * strips if strips > 1 else 0))
+
+
 @pytest.mark.parametrize("size,ms,step", FINE)
-@pytest.mark.parametrize("warps,rows", [(1, 1), (2, 1), (4, 1), (8, 1), (1, 2), (4, 2),
-                                        (1, 4), (2, 4), (8, 4)])
-def test_fine_field_search(size, ms, step, warps, rows):
+@pytest.mark.parametrize("warps,rows,strips", [(1, 1, 1), (2, 1, 1), (8, 1, 1), (16, 1, 2),
+                                               (8, 1, 4), (1, 2, 1), (4, 2, 2), (16, 2, 4),
+                                               (2, 4, 1), (8, 4, 2)])
+def test_fine_field_search(size, ms, step, warps, rows, strips):
     """rows: lattice rows per thread (the window rows are walked once for all
-    of them); the test hook's tiles value is -100 - (10 * rows + warps)"""
+    of them); strips: the field rows split over threads, partial sums added"""
     w, h = 1280, 720
-    curr, prev = _blurred_pair(w, h, seed=size + warps + rows)
-    xs, ys, ox, oy = _fields(w, h, size, ms, step, size * 5 + ms + warps + rows)
-    code = warps if rows == 1 else 10 * rows + warps
+    curr, prev = _blurred_pair(w, h, seed=size + warps + rows + strips)
+    xs, ys, ox, oy = _fields(w, h, size, ms, step, size * 5 + ms + warps + rows + strips)
     sad, tx, ty, ok = V.field_search(curr, prev, xs, ys, size, ms, step, ox, oy,
-                                     tiles=-100 - code)
+                                     tiles=hook(warps, rows, strips))
     for k in range(len(xs)):
         exp = orc_search(curr, prev, int(xs[k]), int(ys[k]), size, ms, step, int(ox[k]),
                          int(oy[k]))
@@ -51,7 +56,7 @@ def test_fine_ties():
     for curr, prev in [(flat, flat), (periodic, periodic), (periodic, np.roll(periodic, 3, 1)),
                        (stripes, stripes)]:
         for size, ms, step in [(32, 32, 2), (16, 16, 2)]:
-            for tiles in (-102, -142):
+            for tiles in (hook(2), hook(2, 4), hook(16, 1, 4)):
                 sad, tx, ty, ok = V.field_search(curr, prev, xs, ys, size, ms, step, tiles=tiles)
                 for k in range(len(xs)):
                     exp = orc_search(curr, prev, int(xs[k]), int(ys[k]), size, ms, step)

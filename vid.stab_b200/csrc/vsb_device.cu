@@ -840,18 +840,19 @@ static int launch_sweep(const DGeom& g, const uint8_t* curr, const uint8_t* prev
 }
 
 /* k_fine over items[0 .. n): one CTA of `warps` warps per item, T lattice
-   rows per thread (1, 2 or 4) */
-static int launch_fine_warp(const GeomDev& gd, int warps, int T, const uint8_t* curr,
+   rows per thread (1, 2 or 4), the field rows in ns strips (1, 2 or 4) */
+static int launch_fine_warp(const GeomDev& gd, int warps, int T, int ns, const uint8_t* curr,
                             const uint8_t* prev, int pitch, const vsbd_item* d_items, int n,
                             vsbd_result* d_res, cudaStream_t st) {
   if (n <= 0) return 0;
   const DGeom& g = gd.g;
-  if (!fw_supported(g) || warps < 1 || warps > FW_MAX_WARPS || (T != 1 && T != 2 && T != 4)) {
+  if (!fw_supported(g) || warps < 1 || warps > FW_MAX_WARPS || (T != 1 && T != 2 && T != 4) ||
+      (ns != 1 && ns != 2 && ns != 4)) {
     set_msg("k_fine does not take this field geometry or configuration");
     return -1;
   }
   const int nt = 32 * warps;
-  const size_t smem = fw_layout(g, nt).total;
+  const size_t smem = fw_layout(g, nt, T, ns).total;
   if (smem > search_smem_limit()) {
     set_msg("k_fine: the search window does not fit in shared memory");
     return -1;
@@ -861,7 +862,7 @@ static int launch_fine_warp(const GeomDev& gd, int warps, int T, const uint8_t* 
   if (g.S == SV && T == TV) {                                                                \
     e = ensure_smem((const void*)k_fine<SV, TV>, SLOT, smem);                                \
     if (e == cudaSuccess)                                                                    \
-      k_fine<SV, TV><<<n, nt, smem, st>>>(curr, prev, pitch, g, d_items, d_res);             \
+      k_fine<SV, TV><<<n, nt, smem, st>>>(curr, prev, pitch, g, d_items, d_res, ns);         \
   }
   VSB_FW(16, 1, 50) VSB_FW(16, 2, 51) VSB_FW(16, 4, 52)
   VSB_FW(32, 1, 53) VSB_FW(32, 2, 54) VSB_FW(32, 4, 55)
@@ -1281,7 +1282,7 @@ int vsbd_plan_search(const vsbd_geom* h, int nitems, DGeom* out) {
    own buffers and every fine field; kept when faster.  Cached per device and
    geometry.  VSB_NO_FINEWARP: never; VSB_FORCE_FINEWARP: always (tests). */
 struct FineTune {
-  int dev, S, step, na, nb, nstages, nitems, warps, T;
+  int dev, S, step, na, nb, nstages, nitems, warps, T, ns;
 };
 static FineTune g_fwtune[64];
 static int g_nfwtune = 0;
@@ -1290,9 +1291,10 @@ static int autotune_fine_warp(const GeomDev& gd, const DGeom* swplan, int sw_on,
                               const uint8_t* curr, const uint8_t* prev, int pitch,
                               const vsbd_item* d_items, int n, unsigned long long* keys,
                               unsigned* tickets, vsbd_result* d_res, unsigned* err,
-                              cudaStream_t st, int* warps_out, int* t_out) {
+                              cudaStream_t st, int* warps_out, int* t_out, int* ns_out) {
   *warps_out = 0;
   *t_out = 1;
+  *ns_out = 1;
   const DGeom& g = gd.g;
   if (n <= 0 || !fw_supported(g) || getenv("VSB_NO_FINEWARP") || getenv("VSB_NO_AUTOTUNE"))
     return 0;
@@ -1306,16 +1308,17 @@ static int autotune_fine_warp(const GeomDev& gd, const DGeom* swplan, int sw_on,
         e.nstages == g.nstages && e.nitems == n) {
       *warps_out = e.warps;
       *t_out = e.T;
+      *ns_out = e.ns;
       return 0;
     }
   }
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
-  auto time_of = [&](int warps, int T) -> float {
+  auto time_of = [&](int warps, int T, int ns) -> float {
     auto one = [&]() {
       if (warps > 0)
-        return launch_fine_warp(gd, warps, T, curr, prev, pitch, d_items, n, d_res, st);
+        return launch_fine_warp(gd, warps, T, ns, curr, prev, pitch, d_items, n, d_res, st);
       return sw_on ? launch_sweep(*swplan, curr, prev, pitch, d_items, n, keys, tickets, d_res,
                                   err, st)
                    : launch_search(gd, curr, prev, pitch, d_items, n, keys, tickets, d_res, st);
@@ -1324,38 +1327,47 @@ static int autotune_fine_warp(const GeomDev& gd, const DGeom* swplan, int sw_on,
       cudaGetLastError();
       return -1.f;
     }
-    cudaEventRecord(e0, st);
-    for (int r = 0; r < 5; r++) one();
-    cudaEventRecord(e1, st);
-    if (cudaEventSynchronize(e1) != cudaSuccess) return -1.f;
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, e0, e1);
-    return ms / 5;
-  };
-  for (int w = 0; w < 3; w++) time_of(0, 1); /* clocks up */
-  const float base = time_of(0, 1);
-  int best_w = 0, best_t = 1;
-  float best_ms = base > 0.f ? base : 3.0e38f;
-  for (int T = 1; T <= 4; T *= 2)
-    for (int warps = 1; warps <= FW_MAX_WARPS; warps *= 2) {
-      /* at least a third of the threads have a task */
-      const int tasks = ((g.na + 7) / 8) * ((g.nb + T - 1) / T);
-      if (32 * warps > 3 * tasks + 32) continue;
-      const float ms = time_of(warps, T);
-      if (getenv("VSB_DEBUG_TUNE"))
-        fprintf(stderr, "fine tuning S=%d items=%d: k_fine %d warps x %d rows %.1f us (current %.1f us)\n",
-                g.S, n, warps, T, 1000.f * ms, 1000.f * base);
-      if (ms > 0.f && (ms < best_ms || (force && best_w == 0))) {
-        best_ms = ms;
-        best_w = warps;
-        best_t = T;
-      }
+    /* the best of three timings of five launches each */
+    float best = 3.0e38f;
+    for (int trial = 0; trial < 3; trial++) {
+      cudaEventRecord(e0, st);
+      for (int r = 0; r < 5; r++) one();
+      cudaEventRecord(e1, st);
+      if (cudaEventSynchronize(e1) != cudaSuccess) return -1.f;
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      best = ms / 5 < best ? ms / 5 : best;
     }
+    return best;
+  };
+  for (int w = 0; w < 3; w++) time_of(0, 1, 1); /* clocks up */
+  const float base = time_of(0, 1, 1);
+  int best_w = 0, best_t = 1, best_ns = 1;
+  float best_ms = base > 0.f ? base : 3.0e38f;
+  for (int T = 1; T <= 2; T *= 2)
+    for (int ns = 1; ns <= 4; ns *= 2)
+      for (int warps = 1; warps <= FW_MAX_WARPS; warps *= 2) {
+        /* at least a third of the threads have a task */
+        if (32 * warps > 3 * fw_tasks(g, T, ns) + 32) continue;
+        const float ms = time_of(warps, T, ns);
+        if (getenv("VSB_DEBUG_TUNE"))
+          fprintf(stderr,
+                  "fine tuning S=%d items=%d: k_fine %d warps x %d rows x %d strips %.1f us "
+                  "(current %.1f us)\n",
+                  g.S, n, warps, T, ns, 1000.f * ms, 1000.f * base);
+        if (ms > 0.f && (ms < best_ms || (force && best_w == 0))) {
+          best_ms = ms;
+          best_w = warps;
+          best_t = T;
+          best_ns = ns;
+        }
+      }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   cudaGetLastError();
   *warps_out = best_w;
   *t_out = best_t;
+  *ns_out = best_ns;
   if (!force && g_nfwtune < 64) {
     FineTune& t = g_fwtune[g_nfwtune++];
     t.dev = dev;
@@ -1367,6 +1379,7 @@ static int autotune_fine_warp(const GeomDev& gd, const DGeom* swplan, int sw_on,
     t.nitems = n;
     t.warps = best_w;
     t.T = best_t;
+    t.ns = best_ns;
   }
   return 0;
 }
@@ -1407,7 +1420,8 @@ struct vsbd_ctx {
      its bounded waits raise ([0] coarse, [1] fine; mapped pinned memory) */
   DGeom swc, swf;
   int sw_c, sw_f;
-  int fw_f, fw_warps, fw_t; /* fine pass on k_fine: warps per item, lattice rows per thread */
+  int fw_f, fw_warps, fw_t, fw_ns; /* fine pass on k_fine: warps per item, lattice rows per
+                                      thread, field-row strips */
   unsigned* h_swerr;
   unsigned* d_swerr;
   vsbd_item* d_citems;
@@ -1940,7 +1954,7 @@ extern "C" int vsbd_create(vsbd_ctx** out, int W, int H, int bpp, int blur_size,
       autotune_fine_warp(c->gf, &c->swf, c->sw_f, c->d_buf[0], c->d_buf[1], c->pitch, c->d_fitems,
                          nf, c->d_keys + nc, c->d_tickets + nc,
                          (vsbd_result*)(c->d_out + c->off_fine), c->d_swerr + 1, c->st,
-                         &c->fw_warps, &c->fw_t) != 0) {
+                         &c->fw_warps, &c->fw_t, &c->fw_ns) != 0) {
     vsbd_destroy(c);
     return -1;
   }
@@ -2321,8 +2335,8 @@ extern "C" int vsbd_stage_b_issue(vsbd_ctx* c, const vsbd_item* items, int n) {
                                      c->d_part, c->d_counts + c->nc, c->d_lists,
                                      c->d_boxes + 4 * c->nc, c->d_keys + c->nc,
                                      c->d_tickets + c->nc, fres, st)
-             : c->fw_f ? launch_fine_warp(c->gf, c->fw_warps, c->fw_t, cur, prv, c->pitch,
-                                          c->d_fitems, n, fres, st)
+             : c->fw_f ? launch_fine_warp(c->gf, c->fw_warps, c->fw_t, c->fw_ns, cur, prv,
+                                          c->pitch, c->d_fitems, n, fres, st)
              : c->sw_f ? launch_sweep(c->swf, cur, prv, c->pitch, c->d_fitems, n, c->d_keys + c->nc,
                                       c->d_tickets + c->nc, fres, c->d_swerr + 1, st)
                      : launch_search(c->gf, cur, prv, c->pitch, c->d_fitems, n, c->d_keys + c->nc,
@@ -2398,8 +2412,8 @@ extern "C" int vsbd_search_tiling(const vsbd_ctx* c, int fine, int* desc) {
     desc[3] = g.nb;
     desc[4] = c->fw_t;
     desc[5] = 32 * c->fw_warps;
-    desc[6] = (int)fw_layout(g, 32 * c->fw_warps).total;
-    desc[7] = 1;
+    desc[6] = (int)fw_layout(g, 32 * c->fw_warps, c->fw_t, c->fw_ns).total;
+    desc[7] = c->fw_ns;
     return 0;
   }
   const int sw = fine ? c->sw_f : c->sw_c;
@@ -2634,9 +2648,12 @@ extern "C" int vsbd_search_host(const uint8_t* curr, const uint8_t* prev, int W,
   cudaError_t e;
   /* tiles_hint < 0: the sweep, with the plan of that rank in its candidate
      list (-1 the model's best); tiles_hint <= -100: k_fine, -100 - tiles_hint
-     = 10 * T + warps (T lattice rows per thread, 1 when the tens are 0) */
-  const int fw_warps = tiles_hint <= -100 ? (-100 - tiles_hint) % 10 : 0;
-  const int fw_t = tiles_hint <= -100 && (-100 - tiles_hint) >= 10 ? (-100 - tiles_hint) / 10 : 1;
+     = 1000 * strips + 100 * T + warps (T lattice rows per thread; a zero
+     digit means 1) */
+  const int fw_code = tiles_hint <= -100 ? -100 - tiles_hint : 0;
+  const int fw_warps = fw_code % 100;
+  const int fw_t = (fw_code / 100) % 10 ? (fw_code / 100) % 10 : 1;
+  const int fw_ns = fw_code / 1000 ? fw_code / 1000 : 1;
   if (tiles_hint <= -100) tiles_hint = 0;
   DGeom swg;
   unsigned* d_err = NULL;
@@ -2664,8 +2681,9 @@ extern "C" int vsbd_search_host(const uint8_t* curr, const uint8_t* prev, int W,
   cudaMemcpy2D(d_c, pitch, curr, (size_t)W * bpp, (size_t)W * bpp, H, cudaMemcpyHostToDevice);
   cudaMemcpy2D(d_p, pitch, prev, (size_t)W * bpp, (size_t)W * bpp, H, cudaMemcpyHostToDevice);
   cudaMemcpy(d_items, items, sizeof(vsbd_item) * n, cudaMemcpyHostToDevice);
-  if (fw_warps) {
-    if (launch_fine_warp(gd, fw_warps, fw_t, d_c, d_p, pitch, d_items, n, d_res, 0) < 0) goto done;
+  if (fw_code) {
+    if (launch_fine_warp(gd, fw_warps, fw_t, fw_ns, d_c, d_p, pitch, d_items, n, d_res, 0) < 0)
+      goto done;
   } else if (tiles_hint < 0) {
     if (launch_sweep(swg, d_c, d_p, pitch, d_items, n, d_keys, d_tk, d_res, d_err, 0) < 0)
       goto done;

@@ -25,7 +25,7 @@
 
 #include "vsb_search.cuh"
 
-#define FW_MAX_WARPS 8
+#define FW_MAX_WARPS 16
 
 /* shared memory of one item */
 struct FWLayout {
@@ -36,7 +36,12 @@ struct FWLayout {
   size_t off_raw, off_c0, off_c1, off_f, off_red, off_part, total;
 };
 
-__host__ __device__ inline FWLayout fw_layout(const DGeom& g, int threads) {
+/* tasks of one item: 8-column groups x blocks of T lattice rows x strips */
+__host__ __device__ inline int fw_tasks(const DGeom& g, int T, int ns) {
+  return ((g.na + 7) / 8) * ((g.nb + T - 1) / T) * ns;
+}
+
+__host__ __device__ inline FWLayout fw_layout(const DGeom& g, int threads, int T, int ns) {
   FWLayout L;
   const int R = refine_reach(g);
   L.WH = g.S + (g.nb - 1) * g.step + 2 * R;
@@ -51,7 +56,9 @@ __host__ __device__ inline FWLayout fw_layout(const DGeom& g, int threads) {
   L.off_f = (L.off_f + 15) & ~(size_t)15;
   L.off_red = L.off_f + (size_t)g.S * g.S;
   L.off_part = L.off_red + FW_MAX_WARPS * 8;
-  L.total = L.off_part + (size_t)threads * 4 + 16;
+  /* the refinement's partials, or the strips' partial sums */
+  const int np = ns > 1 ? fw_tasks(g, T, ns) * 8 * T : 0;
+  L.total = L.off_part + (size_t)(threads > np ? threads : np) * 4 + 16;
   return L;
 }
 
@@ -72,17 +79,18 @@ __device__ __forceinline__ int fw_row(int y, int WPW, int sh) { return y * WPW +
    J0 + jo(k) + w of copy (k & 1), whose words start s0 (even k) or s0 ^ 2
    (odd k) bytes into the raw row; LO says whether s0 < 2 (odd columns then
    start one word earlier).  The window rows are walked once: row y0 + yr
-   serves lattice row b0 + t with field row yr - 2t. */
+   serves lattice row b0 + t with field row yr - 2t; only field rows
+   [r0, r1) (a strip) are summed. */
 template <int S, bool LO, int T>
 __device__ __forceinline__ void fw_sums(const uint32_t* __restrict__ F, const uint32_t* __restrict__ c0,
                                         const uint32_t* __restrict__ c1, int WPW, int sh, int y0,
-                                        int nv, int J0, unsigned* acc) {
+                                        int nv, int J0, int r0, int r1, unsigned* acc) {
   constexpr int NW = S / 4;
 #pragma unroll
   for (int k = 0; k < 8 * T; k++) acc[k] = 0;
-  const int ny = 2 * (nv - 1) + S;
+  const int ny = r1 + 2 * (nv - 1);
 #pragma unroll 1
-  for (int yr = 0; yr < ny; yr++) {
+  for (int yr = r0; yr < ny; yr++) {
     const int rw = fw_row(y0 + yr, WPW, sh) + J0;
     uint32_t x0[NW + 4], x1[NW + 4];
 #pragma unroll
@@ -93,7 +101,7 @@ __device__ __forceinline__ void fw_sums(const uint32_t* __restrict__ F, const ui
 #pragma unroll
     for (int t = 0; t < T; t++) {
       const int r = yr - 2 * t;
-      if (t < nv && r >= 0 && r < S) {
+      if (t < nv && r >= r0 && r < r1) {
         uint32_t f[NW];
 #pragma unroll
         for (int q = 0; q < NW / 4; q++) {
@@ -118,20 +126,21 @@ __device__ __forceinline__ void fw_sums(const uint32_t* __restrict__ F, const ui
 }
 
 /* One CTA (blockDim.x = 32 * warps) per item of items[0 .. n); a thread
-   takes 8 lattice columns x T lattice rows. */
+   takes 8 lattice columns x T lattice rows x one of ns strips of the field
+   rows (the strips' partial sums are added in shared memory). */
 template <int S, int T>
 __global__ void __launch_bounds__(FW_MAX_WARPS * 32) k_fine(const uint8_t* __restrict__ curr,
                                                           const uint8_t* __restrict__ prev,
                                                           int pitch, DGeom g,
                                                           const vsbd_item* __restrict__ items,
-                                                          vsbd_result* __restrict__ res) {
+                                                          vsbd_result* __restrict__ res, int ns) {
   extern __shared__ __align__(16) uint8_t sm[];
   __shared__ int s_tx, s_ty;
   __shared__ unsigned s_min;
   constexpr int NW = S / 4;
   const int item = blockIdx.x;
   const int nt = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const FWLayout L = fw_layout(g, nt);
+  const FWLayout L = fw_layout(g, nt, T, ns);
   const int R = refine_reach(g);
   const vsbd_item it = items[item];
   const int cx0 = it.x - S / 2, cy0 = it.y - S / 2;
@@ -188,28 +197,51 @@ __global__ void __launch_bounds__(FW_MAX_WARPS * 32) k_fine(const uint8_t* __res
   }
   __syncthreads();
   /* every lattice candidate: a thread takes 8 columns of one lattice row */
-  const int ngrp = (g.na + 7) >> 3, nbt = (g.nb + T - 1) / T;
+  const int ngrp = (g.na + 7) >> 3, nbt = (g.nb + T - 1) / T, ntask0 = ngrp * nbt;
+  const int rs = S / ns; /* field rows of a strip */
   unsigned long long best = ~0ull;
-  for (int t = tid; t < ngrp * nbt; t += nt) {
-    const int ag = t / nbt, b0 = (t - ag * nbt) * T;
+  for (int t = tid; t < ntask0 * ns; t += nt) {
+    const int strip = t / ntask0, t0 = t - strip * ntask0;
+    const int ag = t0 / nbt, b0 = (t0 - ag * nbt) * T;
     const int nv = min(T, g.nb - b0);
     const int J0 = (e + R + 16 * ag - s0) >> 2;
     unsigned acc[8 * T];
     if (s0 < 2)
-      fw_sums<S, true, T>(F, c0, c1, L.WPW, sh, R + 2 * b0, nv, J0, acc);
+      fw_sums<S, true, T>(F, c0, c1, L.WPW, sh, R + 2 * b0, nv, J0, strip * rs, strip * rs + rs,
+                          acc);
     else
-      fw_sums<S, false, T>(F, c0, c1, L.WPW, sh, R + 2 * b0, nv, J0, acc);
+      fw_sums<S, false, T>(F, c0, c1, L.WPW, sh, R + 2 * b0, nv, J0, strip * rs, strip * rs + rs,
+                           acc);
+    if (ns > 1) {
 #pragma unroll
-    for (int u = 0; u < T; u++)
+      for (int i = 0; i < 8 * T; i++) part[t * 8 * T + i] = acc[i];
+    } else {
 #pragma unroll
-      for (int k = 0; k < 8; k++) {
-        const int a = ag * 8 + k, b = b0 + u;
-        if (u < nv && a < g.na) {
-          const unsigned long long key =
-              ((unsigned long long)acc[8 * u + k] << 32) | (unsigned)g.order[b * g.na + a];
-          best = key < best ? key : best;
+      for (int u = 0; u < T; u++)
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+          const int a = ag * 8 + k, b = b0 + u;
+          if (u < nv && a < g.na) {
+            const unsigned long long key =
+                ((unsigned long long)acc[8 * u + k] << 32) | (unsigned)g.order[b * g.na + a];
+            best = key < best ? key : best;
+          }
         }
-      }
+    }
+  }
+  if (ns > 1) {
+    /* each candidate's total over the strips */
+    __syncthreads();
+    for (int q = tid; q < ntask0 * 8 * T; q += nt) {
+      const int t0 = q / (8 * T), i = q - t0 * (8 * T);
+      const int ag = t0 / nbt, b = (t0 - ag * nbt) * T + i / 8, a = ag * 8 + (i & 7);
+      if (b >= g.nb || a >= g.na) continue;
+      unsigned sum = 0;
+      for (int st = 0; st < ns; st++) sum += part[(st * ntask0 + t0) * 8 * T + i];
+      const unsigned long long key =
+          ((unsigned long long)sum << 32) | (unsigned)g.order[b * g.na + a];
+      best = key < best ? key : best;
+    }
   }
   best = warp_min64(best);
   if (lane == 0) red[warp] = best;
