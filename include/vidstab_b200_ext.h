@@ -276,6 +276,20 @@ VS_API int vsb_batch_grid(const vsb_batch* b, int* ctas, int* threads, long* sme
    (ns), field size, lattice points per field.  Returns the number of classes
    (for any k, desc untouched when k is out of range), -1 without a batch. */
 VS_API int vsb_batch_class(const vsb_batch* b, int k, int* desc);
+/* The learned search proposal (blob as for vsb_set_proposal below) for
+   every stream of the batch; NULL returns them to the dense search.  The
+   network, the global-motion prior of streams with shakiness >= 8 (two
+   network passes, as a single detector), the narrowed searches and the
+   dense search of the items that fell back all become work items of the
+   same persistent kernel: each step stays two graph launches.  A stream's
+   results equal those of a detector of its own given the same blob.  No
+   step may be in flight.  Returns VS_OK or VS_ERROR. */
+VS_API int vsb_batch_set_proposal(vsb_batch* b, const void* blob, long bytes);
+/* counts since vsb_batch_set_proposal, as vsb_proposal_stats: [0] items
+   searched with the proposal, [1] of them fell back to the full search,
+   [4], [5] coarse items / fallbacks ([2], [3], [6], [7] stay 0: the
+   batch has no verify mode and searches fine fields densely) */
+VS_API int vsb_batch_proposal_stats(const vsb_batch* b, long long* stats);
 
 /* ---- learned search proposal (no reference counterpart) ----------------
    The reference searches every field over its whole candidate lattice.  A
@@ -296,12 +310,14 @@ VS_API int vsb_set_proposal(struct _vsmotiondetect* md, const void* blob, long b
    (if not NaN) and match_bound (if >= 0) */
 VS_API int vsb_set_proposal_ex(struct _vsmotiondetect* md, const void* blob, long bytes,
                                double radius, double conf_min, double match_bound);
-/* Which fields the network serves: the coarse fields always; the fine
-   fields too with fine_net = 1.  With fine_net = 0 (the default) a fine
-   field's narrowed window is centred on the coarse model's prediction for
-   it (zero residual), with the same fallbacks.  fine_radius: the fine
-   fields' window radius in pixels (at most 16; negative: 4 px around the
-   model, the blob's radius around the network). */
+/* How the fine fields are searched with a proposal.  By default
+   (fine_net = 0, fine_radius < 0) they take the exact dense search of the
+   plain detector: their window is already centred on the coarse model's
+   prediction and small.  fine_net = 0 with fine_radius >= 0: a narrowed
+   window of that radius around the coarse model's prediction (zero
+   residual), with the same fallbacks.  fine_net = 1: the network predicts
+   them too (radius fine_radius, or the blob's radius when negative).
+   fine_radius is at most 16 pixels. */
 VS_API int vsb_set_proposal_scope(struct _vsmotiondetect* md, int fine_net, double fine_radius);
 /* Network passes over the coarse fields: 1, or 2 -- the first pass's
    predictions give the frame a global motion model (median translation,

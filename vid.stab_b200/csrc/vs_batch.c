@@ -9,6 +9,7 @@
  * streams as two persistent-kernel launches (vsb_batch.cu) with the
  * per-stream host phases in between.
  */
+#include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -27,7 +28,52 @@ struct vsb_batch {
   int* nitems;
   const vsbd_result** fres;
   FILE** trf; /* per stream: the .trf file its motions go to (NULL: none) */
+  int pn_on;  /* a learned search proposal is set */
+  long long pn_stats[8]; /* as vsb_proposal_stats */
 };
+
+/* proposal counts of stream s's collected stage A (coarse) or stage B
+   (fine, nitems items) */
+static void tally(vsb_batch* b, int s, int fine, int nitems) {
+  int ci = 0, cfb = 0, ffb = 0;
+  /* fine fields take the dense search: nothing to count */
+  if (fine) return;
+  if (!b->pn_on || vsbd_batch_proposal_counts(b->dev, s, &ci, &cfb, &ffb) != 0) return;
+  const int items = fine ? nitems : ci, fb = fine ? ffb : cfb;
+  b->pn_stats[0] += items;
+  b->pn_stats[1] += fb;
+  b->pn_stats[4 + 2 * fine] += items;
+  b->pn_stats[5 + 2 * fine] += fb;
+}
+
+int vsb_batch_set_proposal(vsb_batch* b, const void* blob, long bytes) {
+  if (!b) return VS_ERROR;
+  if (!blob) {
+    if (vsbd_batch_set_proposal(b->dev, NULL, 0, 0, 0, 0, 0, NULL) != 0) return VS_ERROR;
+    b->pn_on = 0;
+    return VS_OK;
+  }
+  vsb_pnet_settings p;
+  if (vsb_pnet_parse(blob, bytes, -1.0, NAN, -1.0, &p) != VS_OK) return VS_ERROR;
+  int* passes = (int*)malloc(sizeof(int) * (size_t)b->n);
+  if (!passes) return VS_ERROR;
+  /* as a single detector: two network passes for very shaky footage */
+  for (int s = 0; s < b->n; s++) passes[s] = b->md[s].conf.shakiness >= 8 ? 2 : 1;
+  /* fine fields: the dense search, as a single detector's default */
+  int rc = vsbd_batch_set_proposal(b->dev, p.params, p.scale, p.radius, p.conf_min,
+                                   p.match_bound, -1.0f, passes);
+  free(passes);
+  if (rc != 0) return VS_ERROR;
+  b->pn_on = 1;
+  memset(b->pn_stats, 0, sizeof(b->pn_stats));
+  return VS_OK;
+}
+
+int vsb_batch_proposal_stats(const vsb_batch* b, long long* stats) {
+  if (!b || !stats || !b->pn_on) return VS_ERROR;
+  memcpy(stats, b->pn_stats, sizeof(b->pn_stats));
+  return VS_OK;
+}
 
 /* after a stream's frame ended (frame number advanced, as vidstabdetect
    writes after vsMotionDetection): its motions to the stream's .trf */
@@ -130,6 +176,7 @@ vsb_batch* vsb_batch_create(int n, const int* widths, const int* heights, int pf
     ds[s].xy = lay[s].xy;
     ds[s].coarse = lay[s].coarse;
     ds[s].fine = lay[s].fine;
+    ds[s].coarse_thr = b->md[s].fieldscoarse.contrastThreshold;
   }
   if (ok && vsbd_batch_create(&b->dev, n, ds) != 0) ok = 0;
   for (int s = 0; lay && s < n; s++) vsb_md_layout_free(&lay[s]);
@@ -161,6 +208,7 @@ int vsb_batch_detect(vsb_batch* b, const uint8_t* const* planes, const int* pitc
     const uint8_t* mm;
     const vsbd_result* cres;
     vsbd_batch_results_a(b->dev, s, &mm, &cres);
+    tally(b, s, 0, 0);
     vsb_frame_host_a(&b->md[s], mm, cres, &b->w[s]);
     if (b->w[s].fine_pass) {
       b->items[s] = b->w[s].items;
@@ -175,6 +223,8 @@ int vsb_batch_detect(vsb_batch* b, const uint8_t* const* planes, const int* pitc
     return VS_ERROR;
   }
   double t3 = vsb_now_s();
+  for (int s = 0; s < b->n; s++)
+    if (b->search[s] && b->nitems[s] > 0) tally(b, s, 1, b->nitems[s]);
   int trf_rc = VS_OK;
   /* the host parts of every stream first: a failed allocation in one drops
      the step for all, before any stream's frame ends */
@@ -264,6 +314,7 @@ static long run_overlapped(vsb_batch* b, const uint8_t* const* clips, const long
         return -1;
       }
       vsbd_batch_results_a(b->dev, s, &mm, &cres);
+      tally(b, s, 0, 0);
       vsb_frame_host_a(&b->md[s], mm, cres, &b->w[s]);
       b->items[s] = b->w[s].fine_pass ? b->w[s].items : NULL;
       b->nitems[s] = b->w[s].fine_pass ? b->w[s].nitems : 0;
@@ -272,6 +323,9 @@ static long run_overlapped(vsb_batch* b, const uint8_t* const* clips, const long
     prof[1] = t1 - t0;
     int rc = vsbd_batch_stage_b_issue(b->dev, b->items, b->nitems);
     if (rc == 0) rc = vsbd_batch_stage_b_collect(b->dev, b->fres);
+    if (rc == 0)
+      for (int s = 0; s < b->n; s++)
+        if (b->nitems[s] > 0) tally(b, s, 1, b->nitems[s]);
     double t2 = vsb_now_s();
     prof[2] = t2 - t1;
     if (rc == 0 && k + 2 < nframes) {

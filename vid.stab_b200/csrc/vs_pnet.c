@@ -37,14 +37,8 @@ int vsb_pnet_sizes(long* n_bf16, long* n_f32, long* act_bytes_per_item,
   return vsbd_pnet_param_bytes() == 2L * PNET_NB16 + 4L * PNET_NF32 ? VS_OK : VS_ERROR;
 }
 
-int vsb_set_proposal_ex(VSMotionDetect* md, const void* blob, long bytes, double radius,
-                        double conf_min, double match_bound) {
-  vsbd_ctx* c = vsb_md_device(md);
-  if (!c) {
-    vsbd_set_error("detector has no device state (not initialised)");
-    return VS_ERROR;
-  }
-  if (!blob) return vsbd_set_proposal(c, NULL, 0, 0, 0, 0) == 0 ? VS_OK : VS_ERROR;
+int vsb_pnet_parse(const void* blob, long bytes, double radius, double conf_min,
+                   double match_bound, vsb_pnet_settings* out) {
   pnet_header h;
   if (bytes < (long)sizeof(h)) {
     vsbd_set_error("proposal network: blob shorter than its header");
@@ -56,14 +50,28 @@ int vsb_set_proposal_ex(VSMotionDetect* md, const void* blob, long bytes, double
     vsbd_set_error("proposal network: not a version-1 VSBP blob of this architecture");
     return VS_ERROR;
   }
+  out->params = (const char*)blob + sizeof(h);
+  out->scale = h.scale;
+  out->radius = (float)(radius >= 0 ? radius : h.radius);
+  out->conf_min = (float)(isnan(conf_min) ? h.conf_min : conf_min);
+  out->match_bound = (float)(match_bound >= 0 ? match_bound : h.match_bound);
+  return VS_OK;
+}
+
+int vsb_set_proposal_ex(VSMotionDetect* md, const void* blob, long bytes, double radius,
+                        double conf_min, double match_bound) {
+  vsbd_ctx* c = vsb_md_device(md);
+  if (!c) {
+    vsbd_set_error("detector has no device state (not initialised)");
+    return VS_ERROR;
+  }
+  if (!blob) return vsbd_set_proposal(c, NULL, 0, 0, 0, 0) == 0 ? VS_OK : VS_ERROR;
+  vsb_pnet_settings p;
+  if (vsb_pnet_parse(blob, bytes, radius, conf_min, match_bound, &p) != VS_OK) return VS_ERROR;
   /* very shaky footage (shakiness >= 8): the second pass around the global
      model keeps large motions inside the network's reach */
   if (vsbd_set_proposal_passes(c, md->conf.shakiness >= 8 ? 2 : 1) != 0) return VS_ERROR;
-  double r = radius >= 0 ? radius : h.radius;
-  double cm = isnan(conf_min) ? h.conf_min : conf_min;
-  double mb = match_bound >= 0 ? match_bound : h.match_bound;
-  return vsbd_set_proposal(c, (const char*)blob + sizeof(h), h.scale, (float)r, (float)cm,
-                           (float)mb) == 0
+  return vsbd_set_proposal(c, p.params, p.scale, p.radius, p.conf_min, p.match_bound) == 0
              ? VS_OK
              : VS_ERROR;
 }

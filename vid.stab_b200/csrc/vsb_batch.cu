@@ -26,6 +26,7 @@
  * at batch creation.
  */
 #include <cuda_runtime.h>
+#include <math.h>
 #include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -33,6 +34,7 @@
 
 #include "vsb_batch.h"
 #include "vsb_plan.h"
+#include "vsb_pnet_dev.cuh"
 #include "vsb_prefilter.cuh"
 #include "vsb_search.cuh"
 
@@ -64,10 +66,32 @@ struct BStream {
   uint8_t* mm;            /* out: (nc+nf) (min,max) pairs */
   vsbd_result* cres;      /* out: nc */
   vsbd_result* fres;      /* out: nf */
+  /* learned search proposal (pn == NULL: the dense search) */
+  const void* pn;         /* network parameters */
+  float* pout;            /* raw network outputs, nc x 3 */
+  vsbd_item* citems2;     /* second pass: coarse items re-centred on the prior */
+  short2* prior;          /* second pass: the prior's displacement per item */
+  uint8_t* skip;          /* coarse fields below the contrast threshold */
+  uint8_t* cfb;           /* out: coarse fallback flags (PN_FB_*) */
+  int* cfl;               /* coarse items that fell back */
+  int* ffl;               /* fine items that fell back */
+  uint8_t* ffb;           /* fine fallback flags */
+  double thr;             /* contrast threshold of the coarse fields */
+  PNSearch psc, psf;      /* narrowed-search settings of coarse and fine fields */
+  int fnarrow;            /* fine fields take the narrowed search (else the dense one) */
+  int passes;             /* network passes over the coarse fields (1 or 2) */
+  int nchunk;             /* network items (VSB_PN_CHUNK coarse fields each) */
 };
 
-/* stage-A work item: type 0 blur tile a; 1 min/max of field a; 2 coarse search
-   tile a = item * ntiles + tile */
+/* coarse fields per network work item: the CTA stages the weights once for
+   them */
+#define VSB_PN_CHUNK 8
+
+/* stage-A work item: type 0 blur tile a; 1 min/max of fields
+   a*VSB_MM_GROUP..; 2 coarse search tile a = item * ntiles + tile; with a
+   search proposal: 3 first network pass over coarse fields
+   a*VSB_PN_CHUNK..; 4 the stream's global motion prior; 5 second network
+   pass over chunk a; 6 narrowed search of coarse field a */
 struct BWork {
   int type, stream, a, pad;
 };
@@ -82,14 +106,24 @@ struct BCtl {
   unsigned head;
   unsigned err;
   unsigned blur_done[VSB_BATCH_MAX_STREAMS];
+  /* the proposal's per-stream progress: min/max items, first-pass network
+     items, priors, second-pass network items, and fallbacks appended */
+  unsigned mm_done[VSB_BATCH_MAX_STREAMS];
+  unsigned inf_done[VSB_BATCH_MAX_STREAMS];
+  unsigned prior_done[VSB_BATCH_MAX_STREAMS];
+  unsigned inf2_done[VSB_BATCH_MAX_STREAMS];
+  unsigned fbn[VSB_BATCH_MAX_STREAMS];
+  unsigned narrow_done; /* narrowed searches finished */
+  unsigned fb_head;     /* next fallback search tile */
   int nwork; /* set by the host; not cleared per launch (nor are the fields below) */
+  int nnarrow; /* narrowed searches in the list (0: no fallback phase) */
   unsigned spin_limit;    /* a wait gives up after this many polls ... */
   long long cycle_limit;  /* ... or this many SM clock cycles */
 };
 
-/* Bounded wait of one CTA until stream s has `target` blur tiles written.
-   Returns 0 if the wait gave up (the error flag is raised). */
-__device__ __forceinline__ int wait_blur(BCtl* ctl, int s, unsigned target) {
+/* Bounded wait of one CTA until the counter *p reaches target.  Returns 0
+   if the wait gave up (the error flag is raised). */
+__device__ __forceinline__ int wait_ge(BCtl* ctl, const unsigned* p, unsigned target) {
   __shared__ int s_ok;
   if (threadIdx.x == 0) {
     const long long t0 = clock64();
@@ -97,7 +131,7 @@ __device__ __forceinline__ int wait_blur(BCtl* ctl, int s, unsigned target) {
     const long long cycle_limit = ctl->cycle_limit;
     unsigned spins = 0;
     int ok = 1;
-    while (*(volatile unsigned*)&ctl->blur_done[s] < target) {
+    while (*(volatile const unsigned*)p < target) {
       if (++spins > spin_limit || clock64() - t0 > cycle_limit) {
         ok = 0;
         atomicExch(&ctl->err, 1u);
@@ -112,6 +146,20 @@ __device__ __forceinline__ int wait_blur(BCtl* ctl, int s, unsigned target) {
   return s_ok;
 }
 
+/* Bounded wait until stream s has `target` blur tiles written. */
+__device__ __forceinline__ int wait_blur(BCtl* ctl, int s, unsigned target) {
+  return wait_ge(ctl, &ctl->blur_done[s], target);
+}
+
+/* counter += 1 once the CTA's writes are visible device-wide */
+__device__ __forceinline__ void signal_done(unsigned* p) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(p, 1u);
+  }
+}
+
 /* One search tile of a layout as a called (not inlined) function: each
    layout's register allocation stays its own and the persistent kernel
    compiles in a fraction of the time an inlined body of every layout takes. */
@@ -124,6 +172,30 @@ __device__ __noinline__ void batch_tile(const uint8_t* __restrict__ cur,
                                         uint8_t* sm) {
   lattice_tile<TB, false, TA>(cur, prev, pitch, g, items, keys, tickets, res, item, tile, ntiles,
                               sm);
+}
+
+/* The proposal's bodies as called functions (their registers stay their
+   own, as with the search tiles). */
+__device__ __noinline__ void batch_infer(uint8_t* sm, const BStream& S, const vsbd_item* items,
+                                         int chunk, int staged) {
+  if (!staged) pn_infer_stage(sm, S.pn);
+  const int i0 = chunk * VSB_PN_CHUNK;
+  const int i1 = min(S.nc, i0 + VSB_PN_CHUNK);
+  pn_infer_items(sm, S.cur, S.prev, S.pitch, S.W, S.H, items, NULL, i0, i1, 1, S.pout);
+}
+
+__device__ __noinline__ void batch_prior(uint8_t* sm, const BStream& S) {
+  pn_prior_body((float*)sm, S.citems, S.pout, S.nc, S.psc.scale, S.psc.conf_min, S.skip,
+                (float)(S.W / 2), (float)(S.H / 2), S.citems2, S.prior);
+}
+
+__device__ __noinline__ void batch_narrow(uint8_t* sm, const BStream& S, const DGeom& g,
+                                          const vsbd_item* items, const float* pout,
+                                          const short2* prior, const PNSearch& ps,
+                                          const uint8_t* skip, vsbd_result* res, uint8_t* fb,
+                                          unsigned* fbn, int* fbl, int item) {
+  pn_narrow_item(sm, S.cur, S.prev, S.pitch, g, items, pout, prior, ps, skip, res, fb, (int*)fbn,
+                 fbl, item);
 }
 
 __device__ __forceinline__ void search_tile(const BStream& S, const DGeom* geoms, int cls,
@@ -152,8 +224,11 @@ __device__ __forceinline__ void search_tile(const BStream& S, const DGeom* geoms
 }
 
 /* Stage A: the static work list `work`.  Stage B (work == NULL): item w of
-   the fine search is found from the per-stream prefix sums (tile-granular)
-   and item offsets into the packed fine work list. */
+   the fine search is found from the per-stream prefix sums (tile-granular;
+   with a proposal, one narrowed search per fine item) and item offsets into
+   the packed fine work list.  With a proposal (ctl->nnarrow > 0) the CTAs
+   that find the list empty wait until every narrowed search of the launch
+   is done, then share the dense search tiles of the items that fell back. */
 template <int NT>
 __global__ void __launch_bounds__(NT, VSB_BATCH_THREADS / NT) k_batch_t(const BWork* __restrict__ work,
                                                              const BStream* __restrict__ streams,
@@ -164,16 +239,20 @@ __global__ void __launch_bounds__(NT, VSB_BATCH_THREADS / NT) k_batch_t(const BW
                                                              int nstreams) {
   extern __shared__ __align__(16) uint8_t sm[];
   __shared__ int s_w;
+  __shared__ int s_wres; /* the network's weights are staged in sm */
   __shared__ DGeom sg;
   const int nwork = ctl->nwork;
+  if (threadIdx.x == 0) s_wres = 0;
   for (;;) {
     if (threadIdx.x == 0) s_w = (int)atomicAdd(&ctl->head, 1u);
     __syncthreads();
     const int w = s_w;
     if (w >= nwork) break;
+    int keep_w = 0;
     if (work) {
       const BWork it = work[w];
       const BStream& S = streams[it.stream];
+      unsigned* done = NULL; /* progress counter this item advances */
       if (it.type == 0) {
         if (S.half <= BTF_MAXHALF)
           blur_tile_fast(S.src, S.sp, S.cur, S.pitch, S.W, S.H, S.half, S.dv, it.a % S.ntx,
@@ -181,28 +260,65 @@ __global__ void __launch_bounds__(NT, VSB_BATCH_THREADS / NT) k_batch_t(const BW
         else
           blur_tile(S.src, S.sp, S.cur, S.pitch, S.W, S.H, S.half, S.dv, it.a % S.ntx,
                     it.a / S.ntx, sm);
-        __syncthreads();
-        if (threadIdx.x == 0) {
-          __threadfence();
-          atomicAdd(&ctl->blur_done[it.stream], 1u);
-        }
-      } else if (wait_blur(ctl, it.stream, (unsigned)(S.ntx * S.nty))) {
+        done = &ctl->blur_done[it.stream];
+      } else {
+        const int ok = wait_blur(ctl, it.stream, (unsigned)(S.ntx * S.nty));
+        const unsigned ngroups = (unsigned)((S.nc + S.nf + VSB_MM_GROUP - 1) / VSB_MM_GROUP);
         if (it.type == 1) {
-          /* fields a*MM_GROUP .. +MM_GROUP, one warp each */
+          /* fields a*MM_GROUP .. +MM_GROUP, one warp each; with a proposal
+             also the coarse contrast flags (src/motiondetect.c:389-407 of
+             the reference: contrast = (max - min) / (max + min + 0.1)) */
           const int f = it.a * VSB_MM_GROUP + (int)(threadIdx.x >> 5);
-          if ((int)(threadIdx.x >> 5) < VSB_MM_GROUP && f < S.nc + S.nf) {
+          if (ok && (int)(threadIdx.x >> 5) < VSB_MM_GROUP && f < S.nc + S.nf) {
             const bool coarse = f < S.nc;
             const int x = coarse ? S.xy[f] : S.xy[2 * S.nc + (f - S.nc)];
             const int y = coarse ? S.xy[S.nc + f] : S.xy[2 * S.nc + S.nf + (f - S.nc)];
             minmax_field_warp(S.cur, S.pitch, x, y, coarse ? S.Sc : S.Sf, f, S.mm);
+            if (coarse && S.skip && (threadIdx.x & 31) == 0) {
+              const int mn = S.mm[2 * f], mx = S.mm[2 * f + 1];
+              const double con = (double)(mx - mn) / ((double)(mx + mn) + 0.1);
+              S.skip[f] = !(con >= S.thr && con > 0.0);
+            }
           }
-        } else {
-          const DGeom* gp = &geoms[S.gc];
-          const int ntiles = gp->nta * gp->ntb;
-          search_tile(S, geoms, S.gc, S.citems, S.keys, S.tickets, S.cres, it.a / ntiles,
-                      it.a % ntiles, &sg, sm);
+          done = &ctl->mm_done[it.stream];
+        } else if (it.type == 2) {
+          if (ok) {
+            const DGeom* gp = &geoms[S.gc];
+            const int ntiles = gp->nta * gp->ntb;
+            search_tile(S, geoms, S.gc, S.citems, S.keys, S.tickets, S.cres, it.a / ntiles,
+                        it.a % ntiles, &sg, sm);
+          }
+        } else if constexpr (NT == VSB_BATCH_THREADS) {
+          /* the proposal's items: every counter they wait for is advanced by
+             items earlier in the list (even when those gave up), so the
+             waits end */
+          const int s = it.stream;
+          if (it.type == 3 || it.type == 5) {
+            const int ready = ok && (it.type == 3 || wait_ge(ctl, &ctl->prior_done[s], 1u));
+            if (ready) {
+              batch_infer(sm, S, it.type == 3 ? S.citems : S.citems2, it.a, s_wres);
+              keep_w = 1;
+            }
+            done = it.type == 3 ? &ctl->inf_done[s] : &ctl->inf2_done[s];
+          } else if (it.type == 4) {
+            if (ok && wait_ge(ctl, &ctl->mm_done[s], ngroups) &&
+                wait_ge(ctl, &ctl->inf_done[s], (unsigned)S.nchunk))
+              batch_prior(sm, S);
+            done = &ctl->prior_done[s];
+          } else if (it.type == 6) {
+            unsigned* net = S.passes == 2 ? &ctl->inf2_done[s] : &ctl->inf_done[s];
+            if (ok && wait_ge(ctl, &ctl->mm_done[s], ngroups) &&
+                wait_ge(ctl, net, (unsigned)S.nchunk)) {
+              if (threadIdx.x == 0) sg = geoms[S.gc];
+              __syncthreads();
+              batch_narrow(sm, S, sg, S.citems, S.pout, S.passes == 2 ? S.prior : NULL, S.psc,
+                           S.skip, S.cres, S.cfb, &ctl->fbn[s], S.cfl, it.a);
+            }
+            done = &ctl->narrow_done;
+          }
         }
       }
+      if (done) signal_done(done);
     } else {
       /* stream of item w: largest s with prefix[s] <= w */
       int lo = 0, hi = nstreams - 1;
@@ -211,12 +327,59 @@ __global__ void __launch_bounds__(NT, VSB_BATCH_THREADS / NT) k_batch_t(const BW
         if (prefix[mid] <= w) lo = mid; else hi = mid - 1;
       }
       const BStream& S = streams[lo];
-      const DGeom* gp = &geoms[S.gf];
-      const int ntiles = gp->nta * gp->ntb;
       const int local = w - prefix[lo];
-      search_tile(S, geoms, S.gf, fitems + item_off[lo], S.keys + S.nc, S.tickets + S.nc, S.fres,
-                  local / ntiles, local % ntiles, &sg, sm);
+      if (S.fnarrow) {
+        if (threadIdx.x == 0) sg = geoms[S.gf];
+        __syncthreads();
+        batch_narrow(sm, S, sg, fitems + item_off[lo], NULL, NULL, S.psf, NULL, S.fres, S.ffb,
+                     &ctl->fbn[lo], S.ffl, local);
+        signal_done(&ctl->narrow_done);
+      } else {
+        const DGeom* gp = &geoms[S.gf];
+        const int ntiles = gp->nta * gp->ntb;
+        search_tile(S, geoms, S.gf, fitems + item_off[lo], S.keys + S.nc, S.tickets + S.nc,
+                    S.fres, local / ntiles, local % ntiles, &sg, sm);
+      }
     }
+    if (threadIdx.x == 0) s_wres = keep_w;
+    __syncthreads();
+  }
+  /* the dense search of the items whose proposal was not trusted: tile f of
+     the concatenation, stream by stream, of (fallback item x search tile) */
+  const int nnarrow = ctl->nnarrow;
+  if (nnarrow <= 0 || !wait_ge(ctl, &ctl->narrow_done, (unsigned)nnarrow)) return;
+  __shared__ int s_fs, s_fi, s_ft;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const unsigned f = atomicAdd(&ctl->fb_head, 1u);
+      int fs = -1, fi = 0, ft = 0;
+      unsigned acc = 0;
+      for (int q = 0; q < nstreams; q++) {
+        const DGeom* gp = &geoms[work ? streams[q].gc : streams[q].gf];
+        const unsigned nt = (unsigned)(gp->nta * gp->ntb);
+        const unsigned c = *(volatile const unsigned*)&ctl->fbn[q] * nt;
+        if (f < acc + c) {
+          fs = q;
+          fi = (int)((f - acc) / nt);
+          ft = (int)((f - acc) % nt);
+          break;
+        }
+        acc += c;
+      }
+      s_fs = fs;
+      s_fi = fi;
+      s_ft = ft;
+    }
+    __syncthreads();
+    const int fs = s_fs;
+    if (fs < 0) break;
+    const BStream& S = streams[fs];
+    if (work)
+      search_tile(S, geoms, S.gc, S.citems, S.keys, S.tickets, S.cres, __ldcg(S.cfl + s_fi), s_ft,
+                  &sg, sm);
+    else
+      search_tile(S, geoms, S.gf, fitems + item_off[fs], S.keys + S.nc, S.tickets + S.nc, S.fres,
+                  __ldcg(S.ffl + s_fi), s_ft, &sg, sm);
     __syncthreads();
   }
 }
@@ -296,14 +459,22 @@ struct vsbd_batch {
   unsigned wait_spins;  /* limits of the bounded waits (BCtl) */
   long long wait_cycles;
   int withheld;         /* stream whose blur items stage A's list leaves out (test hook; -1) */
+  /* learned search proposal (vsbd_batch_set_proposal) */
+  int pn_on;
+  void* d_pn;           /* network parameters */
+  uint8_t* d_pnbuf;     /* every stream's proposal buffers, one allocation */
+  unsigned* h_fbnB;     /* pinned: stage B's fallback count per stream */
+  size_t* cfb_off;      /* per stream: coarse fallback flags in the stage-A results */
+  int nnarrowA;         /* narrowed searches of a stage A (every coarse field) */
 };
 
 /* a control block as the host uploads it: zero counters, the work count and
    the wait limits */
-static BCtl ctl_init(const vsbd_batch* b, int nwork) {
+static BCtl ctl_init(const vsbd_batch* b, int nwork, int nnarrow = 0) {
   BCtl h;
   memset(&h, 0, sizeof(h));
   h.nwork = nwork;
+  h.nnarrow = nnarrow;
   h.spin_limit = b->wait_spins;
   h.cycle_limit = b->wait_cycles;
   return h;
@@ -376,11 +547,25 @@ static int class_of(vsbd_batch* b, const vsbd_geom* g, int nitems) {
   return default_tiling(b, k, nitems, VSB_BATCH_THREADS) == 0 ? k : -1;
 }
 
+/* shared memory of the narrowed search of class k's fields at radius r */
+static size_t narrow_smem(const vsbd_batch* b, int k, float r) {
+  return narrow_layout(b->cls[k].g, r).total;
+}
+
 static size_t kernel_smem(const vsbd_batch* b) {
   size_t m = BT_SMEM > BTF_SMEM ? BT_SMEM : BTF_SMEM;
   for (int k = 0; k < b->ncls; k++) {
     size_t t = tile_layout(b->cls[k].g).total;
     if (t > m) m = t;
+  }
+  if (b->pn_on) {
+    /* the network, the prior's arrays, the coarse narrowed searches */
+    if ((size_t)PI_SMEM > m) m = PI_SMEM;
+    if (sizeof(float) * 4 * PN_PRIOR_MAX > m) m = sizeof(float) * 4 * PN_PRIOR_MAX;
+    for (int s = 0; s < b->n; s++) {
+      const size_t t = narrow_smem(b, b->h_streams[s].gc, b->h_streams[s].psc.radius);
+      if (t > m) m = t;
+    }
   }
   return m;
 }
@@ -406,6 +591,12 @@ static int set_grid_b(vsbd_batch* b) {
   for (int k = 0; k < b->ncls; k++)
     if (b->cls_nt[k] == VSB_BATCH_THREADS_B && tile_layout(b->cls[k].g).total > m)
       m = tile_layout(b->cls[k].g).total;
+  if (b->pn_on)
+    for (int s = 0; s < b->n; s++) {
+      if (!b->h_streams[s].fnarrow) continue;
+      const size_t t = narrow_smem(b, b->h_streams[s].gf, b->h_streams[s].psf.radius);
+      if (t > m) m = t;
+    }
   b->smem_b = m;
   BCK(cudaFuncSetAttribute(k_batch_t<VSB_BATCH_THREADS_B>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem_b));
@@ -429,7 +620,40 @@ static int upload_geoms(vsbd_batch* b) {
 
 /* stage-A work list: blur tiles, coarse search tiles (heaviest classes
    first), min/max of every field */
+/* stage-A work list of a batch with a search proposal: blur tiles, min/max
+   groups, the first network pass, the priors and second pass of the
+   streams that take two, then one narrowed search per coarse field */
+static int build_workA_learned(vsbd_batch* b, BWork** out, int* count) {
+  long total = 0;
+  for (int s = 0; s < b->n; s++) {
+    const BStream& S = b->h_streams[s];
+    total += (long)S.ntx * S.nty + (S.nc + S.nf + VSB_MM_GROUP - 1) / VSB_MM_GROUP;
+    total += (long)S.nchunk * S.passes + (S.passes == 2) + S.nc;
+  }
+  BWork* w = (BWork*)malloc(sizeof(BWork) * (size_t)(total + 1));
+  if (!w) { vsbp_set_msg("out of host memory"); return -1; }
+  long k = 0;
+  for (int s = 0; s < b->n; s++)
+    for (int t = 0; t < b->h_streams[s].ntx * b->h_streams[s].nty; t++) w[k++] = { 0, s, t, 0 };
+  for (int s = 0; s < b->n; s++)
+    for (int g = 0; g * VSB_MM_GROUP < b->h_streams[s].nc + b->h_streams[s].nf; g++)
+      w[k++] = { 1, s, g, 0 };
+  for (int s = 0; s < b->n; s++)
+    for (int c = 0; c < b->h_streams[s].nchunk; c++) w[k++] = { 3, s, c, 0 };
+  for (int s = 0; s < b->n; s++)
+    if (b->h_streams[s].passes == 2) w[k++] = { 4, s, 0, 0 };
+  for (int s = 0; s < b->n; s++)
+    if (b->h_streams[s].passes == 2)
+      for (int c = 0; c < b->h_streams[s].nchunk; c++) w[k++] = { 5, s, c, 0 };
+  for (int s = 0; s < b->n; s++)
+    for (int i = 0; i < b->h_streams[s].nc; i++) w[k++] = { 6, s, i, 0 };
+  *out = w;
+  *count = (int)k;
+  return 0;
+}
+
 static int build_workA(vsbd_batch* b, BWork** out, int* count, int only_cls, int fine_cls_tune) {
+  if (b->pn_on && only_cls < 0) return build_workA_learned(b, out, count);
   long total = 0;
   for (int s = 0; s < b->n; s++) {
     const BStream& S = b->h_streams[s];
@@ -583,9 +807,12 @@ static int capture(vsbd_batch* b, int stageB, uint8_t* h_res, int flag, cudaGrap
     k_batch_t<VSB_BATCH_THREADS><<<b->grid, VSB_BATCH_THREADS, b->smem, b->st>>>(
         b->d_workA, b->d_streams, b->d_geoms, ctl, b->d_pre, b->d_pre + b->n + 1, b->d_fitems,
         b->n);
-  if (stageB)
+  if (stageB) {
     cudaMemcpyAsync(b->h_resB, b->d_resB, sizeof(vsbd_result) * (size_t)(b->nf_total + 1),
                     cudaMemcpyDeviceToHost, b->st);
+    if (b->pn_on && b->h_streams[0].fnarrow)
+      cudaMemcpyAsync(b->h_fbnB, ctl->fbn, sizeof(unsigned) * b->n, cudaMemcpyDeviceToHost, b->st);
+  }
   else
     cudaMemcpyAsync(h_res, b->d_resA, b->resA_bytes, cudaMemcpyDeviceToHost, b->st);
   cudaMemcpyAsync((void*)&b->h_nwork[flag], &ctl->err,
@@ -644,6 +871,10 @@ extern "C" void vsbd_batch_destroy(vsbd_batch* b) {
   cudaFree(b->d_fitems);
   cudaFreeHost(b->h_fitems);
   cudaFreeHost(b->h_nwork);
+  cudaFree(b->d_pn);
+  cudaFree(b->d_pnbuf);
+  if (b->h_fbnB) cudaFreeHost(b->h_fbnB);
+  free(b->cfb_off);
   free(b->raw);
   free(b->buf[0]);
   free(b->buf[1]);
@@ -707,6 +938,7 @@ extern "C" int vsbd_batch_create(vsbd_batch** out, int n, const vsbd_batch_strea
   b->mm_off = (size_t*)calloc(n, sizeof(size_t));
   b->cres_off = (size_t*)calloc(n, sizeof(size_t));
   b->fres_off = (size_t*)calloc(n, sizeof(size_t));
+  b->cfb_off = (size_t*)calloc(n, sizeof(size_t));
   CKB(cudaMallocHost(&b->h_streams, sizeof(BStream) * n));
   memset(b->h_streams, 0, sizeof(BStream) * n);
   CKB(cudaMalloc(&b->d_streams, sizeof(BStream) * n));
@@ -769,6 +1001,8 @@ extern "C" int vsbd_batch_create(vsbd_batch** out, int n, const vsbd_batch_strea
     resA = al16(resA + 2 * (size_t)(q.nc + q.nf));
     b->cres_off[s] = resA;
     resA = al16(resA + sizeof(vsbd_result) * (size_t)q.nc);
+    b->cfb_off[s] = resA;
+    resA = al16(resA + (size_t)q.nc);
     b->fres_off[s] = (size_t)nf_total;
     nf_total += q.nf;
   }
@@ -798,8 +1032,11 @@ extern "C" int vsbd_batch_create(vsbd_batch** out, int n, const vsbd_batch_strea
   CKB(cudaMallocHost(&b->h_pre, sizeof(int) * (2 * (size_t)n + 2)));
   CKB(cudaMalloc(&b->d_fitems, sizeof(vsbd_item) * (size_t)(nf_total + 1)));
   CKB(cudaMallocHost(&b->h_fitems, sizeof(vsbd_item) * (size_t)(nf_total + 1)));
-  CKB(cudaMallocHost(&b->h_nwork, sizeof(int) * 4));
-  memset(b->h_nwork, 0, sizeof(int) * 4);
+  /* [0] stage B's items, [1] its error flag, [2], [3] the error flags of
+     the two stage-A graphs, [4], [5] stage B's work count and narrowed
+     searches as uploaded */
+  CKB(cudaMallocHost(&b->h_nwork, sizeof(int) * 8));
+  memset(b->h_nwork, 0, sizeof(int) * 8);
   for (int s = 0; s < n; s++) {
     BStream& S = b->h_streams[s];
     S.src = b->raw[s];
@@ -813,6 +1050,8 @@ extern "C" int vsbd_batch_create(vsbd_batch** out, int n, const vsbd_batch_strea
     S.mm = b->d_resA + b->mm_off[s];
     S.cres = (vsbd_result*)(b->d_resA + b->cres_off[s]);
     S.fres = b->d_resB + b->fres_off[s];
+    S.cfb = b->d_resA + b->cfb_off[s];
+    S.thr = d[s].coarse_thr;
   }
   CKB(cudaMemcpy(b->d_streams, b->h_streams, sizeof(BStream) * n, cudaMemcpyHostToDevice));
   /* fine items for tuning: every fine field of every stream, no offset; the
@@ -1048,10 +1287,14 @@ extern "C" int vsbd_batch_stage_b_issue(vsbd_batch* b, const vsbd_item* const* i
     off[s] = nit;
     if (ni > 0) memcpy(b->h_fitems + nit, items[s], sizeof(vsbd_item) * ni);
     nit += ni;
-    total += ni * g.nta * g.ntb;
+    /* one narrowed search per item with a narrowed fine stage, else the
+       item's search tiles */
+    total += S.fnarrow ? ni : ni * g.nta * g.ntb;
   }
   pre[b->n] = total;
   b->h_nwork[0] = total;
+  b->h_nwork[4] = total;
+  b->h_nwork[5] = b->pn_on && b->h_streams[0].fnarrow ? nit : 0;
   b->b_pending = total > 0;
   if (total == 0) return 0;
   for (int s = 0; s < b->n; s++) {
@@ -1065,7 +1308,7 @@ extern "C" int vsbd_batch_stage_b_issue(vsbd_batch* b, const vsbd_item* const* i
                       cudaMemcpyHostToDevice, b->st2));
   BCK(cudaMemcpyAsync(b->d_fitems, b->h_fitems, sizeof(vsbd_item) * (size_t)nit,
                       cudaMemcpyHostToDevice, b->st2));
-  BCK(cudaMemcpyAsync(&b->d_ctlB->nwork, &b->h_nwork[0], sizeof(int), cudaMemcpyHostToDevice,
+  BCK(cudaMemcpyAsync(&b->d_ctlB->nwork, &b->h_nwork[4], 2 * sizeof(int), cudaMemcpyHostToDevice,
                       b->st2));
   BCK(cudaGraphLaunch(b->gB, b->st2));
   BCK(cudaEventRecord(b->evB, b->st2));
@@ -1101,6 +1344,166 @@ extern "C" void vsbd_batch_commit(vsbd_batch* b, int s) {
   const int f = 3 - b->cur[s] - b->prv[s];
   b->prv[s] = b->cur[s];
   b->cur[s] = f;
+}
+
+/* Gives every stream the learned search proposal (params: the network's
+   device-order parameters on the host) or, with params == NULL, the dense
+   search again.  Rebuilds stage A's work list, the grids and the captured
+   graphs; no step may be in flight. */
+extern "C" int vsbd_batch_set_proposal(vsbd_batch* b, const void* params, float scale,
+                                       float radius, float conf_min, float match_bound,
+                                       float fine_radius, const int* passes) {
+  BCK(cudaSetDevice(b->dev));
+  if (b->a_n > 0 || b->b_pending) {
+    vsbp_set_msg("batched proposal: a step is in flight");
+    return -1;
+  }
+  BCK(cudaStreamSynchronize(b->st));
+  BCK(cudaStreamSynchronize(b->st2));
+  if (params && (!(scale > 0.f) || !(radius >= 0.f) || !(match_bound >= 0.f) ||
+                 isnan(fine_radius) || fine_radius > 16.f)) {
+    vsbp_set_msg("bad proposal settings");
+    return -1;
+  }
+  if (params)
+    for (int s = 0; s < b->n; s++) {
+      const BStream& S = b->h_streams[s];
+      const DGeom& gc = b->cls[S.gc].g;
+      const DGeom& gf = b->cls[S.gf].g;
+      const int sc = narrow_span(radius, gc.step);
+      const int sf = fine_radius >= 0.f ? narrow_span(fine_radius, gf.step) : 0;
+      if (sc * sc > PN_NARROW_QMAX || sf * sf > PN_NARROW_QMAX) {
+        vsbp_set_msg("proposal radius too large for the narrowed search");
+        return -1;
+      }
+      if (S.nc > PN_PRIOR_MAX || (passes && passes[s] != 1 && passes[s] != 2)) {
+        vsbp_set_msg("batched proposal: more coarse fields than the prior takes, or bad passes");
+        return -1;
+      }
+    }
+  /* per stream: pout | citems2 | prior | skip | coarse list | fine list | fine flags */
+  size_t* off = (size_t*)malloc(sizeof(size_t) * (size_t)(b->n + 1));
+  if (!off) { vsbp_set_msg("out of host memory"); return -1; }
+  size_t tot = 0;
+  for (int s = 0; s < b->n; s++) {
+    const BStream& S = b->h_streams[s];
+    off[s] = tot;
+    tot += al16(sizeof(float) * 3 * (size_t)S.nc) + al16(sizeof(vsbd_item) * (size_t)S.nc) +
+           al16(sizeof(short2) * (size_t)S.nc) + al16((size_t)S.nc) +
+           al16(sizeof(int) * (size_t)S.nc) + al16(sizeof(int) * (size_t)S.nf) + al16((size_t)S.nf);
+  }
+  off[b->n] = tot;
+  cudaFree(b->d_pnbuf);
+  b->d_pnbuf = NULL;
+  b->pn_on = 0;
+  if (params) {
+    cudaError_t e = cudaSuccess;
+    if (!b->d_pn) e = cudaMalloc(&b->d_pn, PN_PARAM_BYTES);
+    if (e == cudaSuccess) e = cudaMemcpy(b->d_pn, params, PN_PARAM_BYTES, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_pnbuf, tot + 16);
+    if (e == cudaSuccess) e = cudaMemset(b->d_pnbuf, 0, tot + 16);
+    if (e == cudaSuccess && !b->h_fbnB) e = cudaMallocHost(&b->h_fbnB, sizeof(unsigned) * b->n);
+    if (e != cudaSuccess) {
+      free(off);
+      vsbp_set_err("batched proposal buffers", e);
+      return -1;
+    }
+    b->nnarrowA = 0;
+    for (int s = 0; s < b->n; s++) {
+      BStream& S = b->h_streams[s];
+      uint8_t* p = b->d_pnbuf + off[s];
+      S.pn = b->d_pn;
+      S.pout = (float*)p;
+      p += al16(sizeof(float) * 3 * (size_t)S.nc);
+      S.citems2 = (vsbd_item*)p;
+      p += al16(sizeof(vsbd_item) * (size_t)S.nc);
+      S.prior = (short2*)p;
+      p += al16(sizeof(short2) * (size_t)S.nc);
+      S.skip = p;
+      p += al16((size_t)S.nc);
+      S.cfl = (int*)p;
+      p += al16(sizeof(int) * (size_t)S.nc);
+      S.ffl = (int*)p;
+      p += al16(sizeof(int) * (size_t)S.nf);
+      S.ffb = p;
+      /* the SAD bound scales with the field's pixel count */
+      const double bc = (double)match_bound * b->cls[S.gc].g.S * b->cls[S.gc].g.S;
+      const double bf = (double)match_bound * b->cls[S.gf].g.S * b->cls[S.gf].g.S;
+      S.psc.scale = S.psf.scale = scale;
+      S.psc.conf_min = S.psf.conf_min = conf_min;
+      S.psc.radius = radius;
+      S.psf.radius = fine_radius;
+      S.psc.sad_bound = bc >= 4294967295.0 ? 0xffffffffu : (unsigned)bc;
+      S.psf.sad_bound = bf >= 4294967295.0 ? 0xffffffffu : (unsigned)bf;
+      S.passes = passes ? passes[s] : 1;
+      S.nchunk = (S.nc + VSB_PN_CHUNK - 1) / VSB_PN_CHUNK;
+      S.fnarrow = fine_radius >= 0.f;
+      b->nnarrowA += S.nc;
+    }
+    b->pn_on = 1;
+  } else {
+    for (int s = 0; s < b->n; s++) {
+      BStream& S = b->h_streams[s];
+      S.pn = NULL;
+      S.pout = NULL;
+      S.citems2 = NULL;
+      S.prior = NULL;
+      S.skip = NULL;
+      S.cfl = S.ffl = NULL;
+      S.ffb = NULL;
+      S.passes = 1;
+      S.nchunk = 0;
+      S.fnarrow = 0;
+    }
+    b->nnarrowA = 0;
+  }
+  free(off);
+  if (set_grid(b) != 0 || set_grid_b(b) != 0 || upload_geoms(b) != 0) return -1;
+  BWork* w = NULL;
+  int nw = 0;
+  if (build_workA(b, &w, &nw, -1, 0) != 0) return -1;
+  cudaFree(b->d_workA);
+  b->d_workA = NULL;
+  cudaError_t e = cudaMalloc(&b->d_workA, sizeof(BWork) * (size_t)(nw + 1));
+  if (e == cudaSuccess) e = cudaMemcpy(b->d_workA, w, sizeof(BWork) * nw, cudaMemcpyHostToDevice);
+  free(w);
+  BCK(e);
+  b->nworkA = nw;
+  b->withheld = -1;
+  {
+    BCtl h = ctl_init(b, nw, b->nnarrowA);
+    BCK(cudaMemcpy(b->d_ctlA, &h, sizeof(h), cudaMemcpyHostToDevice));
+    BCtl hb = ctl_init(b, 0);
+    BCK(cudaMemcpy(b->d_ctlB, &hb, sizeof(hb), cudaMemcpyHostToDevice));
+  }
+  BCK(cudaMemcpy(b->d_streams, b->h_streams, sizeof(BStream) * b->n, cudaMemcpyHostToDevice));
+  if (b->gA) cudaGraphExecDestroy(b->gA);
+  if (b->gA2) cudaGraphExecDestroy(b->gA2);
+  if (b->gB) cudaGraphExecDestroy(b->gB);
+  b->gA = b->gA2 = b->gB = NULL;
+  if (capture(b, 0, b->h_resA, 2, &b->gA) != 0 || capture(b, 0, b->h_resA2, 3, &b->gA2) != 0 ||
+      capture(b, 1, NULL, 1, &b->gB) != 0)
+    return -1;
+  return 0;
+}
+
+/* proposal counts of stream s's last collected stages: coarse fields
+   searched with the proposal and how many of them fell back (from stage
+   A's flags), and the fine items that fell back (stage B) */
+extern "C" int vsbd_batch_proposal_counts(const vsbd_batch* b, int s, int* coarse_items,
+                                          int* coarse_fb, int* fine_fb) {
+  if (!b || !b->pn_on || s < 0 || s >= b->n) return -1;
+  const uint8_t* fl = (b->res_buf ? b->h_resA2 : b->h_resA) + b->cfb_off[s];
+  int ni = 0, nfb = 0;
+  for (int i = 0; i < b->h_streams[s].nc; i++) {
+    if (fl[i] == PN_FB_UNUSED) continue;
+    ni++;
+    nfb += fl[i] == PN_FB_FULL;
+  }
+  if (coarse_items) *coarse_items = ni;
+  if (coarse_fb) *coarse_fb = nfb;
+  if (fine_fb) *fine_fb = b->h_fbnB && b->h_streams[s].fnarrow ? (int)b->h_fbnB[s] : 0;
+  return 0;
 }
 
 extern "C" long vsbd_batch_launches(const vsbd_batch* b) { return b ? b->launches : 0; }

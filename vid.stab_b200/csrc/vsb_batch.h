@@ -20,6 +20,7 @@ typedef struct {
   int nc, nf;            /* coarse / fine field counts */
   const int16_t* xy;     /* coarse x[nc], coarse y[nc], fine x[nf], fine y[nf] */
   vsbd_geom coarse, fine;
+  double coarse_thr;     /* contrast threshold of the coarse fields */
 } vsbd_batch_stream;
 
 typedef struct vsbd_batch vsbd_batch;
@@ -66,6 +67,23 @@ int vsbd_batch_set_wait_limit(vsbd_batch* b, unsigned spins, long long cycles);
 /* test hook: stage A's work list leaves out stream s's blur items (s < 0:
    the full list again), so that stream's waits run out */
 int vsbd_batch_withhold_blur(vsbd_batch* b, int stream);
+
+/* The learned search proposal for every stream (params: the network's
+   parameters in device order, on the host; NULL: the dense search again).
+   fine_radius >= 0: the fine fields take the narrowed search in a window
+   of that radius around the coarse model's prediction; < 0: the dense
+   search.
+   The network, the priors of streams with passes[s] == 2, the narrowed
+   searches and the dense search of the items that fell back all become
+   work items of the persistent kernel.  No step may be in flight. */
+int vsbd_batch_set_proposal(vsbd_batch* b, const void* params, float scale, float radius,
+                            float conf_min, float match_bound, float fine_radius,
+                            const int* passes);
+/* stream s's proposal counts of the last collected stages (coarse fields
+   searched with the proposal, those that fell back; fine items that fell
+   back) */
+int vsbd_batch_proposal_counts(const vsbd_batch* b, int s, int* coarse_items, int* coarse_fb,
+                               int* fine_fb);
 
 long vsbd_batch_launches(const vsbd_batch* b);
 /* persistent grid: CTAs, threads per CTA, dynamic shared memory per CTA */

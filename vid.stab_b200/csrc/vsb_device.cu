@@ -1965,6 +1965,13 @@ extern "C" int vsbd_create(vsbd_ctx** out, int W, int H, int bpp, int blur_size,
   return 0;
 }
 
+/* whether the fine fields take the narrowed search (the network's, or a
+   window around the coarse model's prediction); by default they take the
+   exact dense search of the plain detector */
+static bool fine_narrowed(const vsbd_ctx* c) {
+  return c->pn_on && (c->pn_fine_net || c->pn_fine_radius >= 0.f);
+}
+
 /* The proposal path of one field set: network, narrowed search, full
    search of the items that fell back (and, when verifying, the full search
    of every item into d_vres + base).  fbl: this field set's fallback count
@@ -2002,8 +2009,7 @@ static int learned_search(vsbd_ctx* c, const GeomDev& gd, const GeomDev& gfull, 
   /* the SAD bound scales with the field's pixel count */
   PNSearch ps = c->pn;
   if (base != 0) /* fine fields: 4 px around the coarse model, the blob's radius around the network */
-    ps.radius = c->pn_fine_radius >= 0.f ? c->pn_fine_radius
-                                         : (c->pn_fine_net ? c->pn.radius : 4.0f);
+    ps.radius = c->pn_fine_radius >= 0.f ? c->pn_fine_radius : c->pn.radius;
   const double bound = (double)c->pn_match_bound * gd.g.S * gd.g.S;
   ps.sad_bound = bound >= 4294967295.0 ? 0xffffffffu : (unsigned)bound;
   CK(cudaMemsetAsync(fbl, 0, sizeof(int), st));
@@ -2323,7 +2329,7 @@ extern "C" int vsbd_stage_b_issue(vsbd_ctx* c, const vsbd_item* items, int n) {
   uint8_t* prv = c->d_buf[c->prv];
   vsbd_result* fres = (vsbd_result*)(c->d_out + c->off_fine);
   size_t d2h = sizeof(vsbd_result) * n;
-  if (c->pn_on) {
+  if (fine_narrowed(c)) {
     if (learned_search(c, c->gf, c->fb_last[1] >= 8 ? c->gf : c->gff, cur, prv, st, c->d_fitems,
                        n, c->nc, NULL, c->d_keys + c->nc, c->d_tickets + c->nc, fres,
                        c->d_out + c->off_ffb, c->d_fbl + c->nc + 2) != 0)
@@ -2351,7 +2357,7 @@ extern "C" int vsbd_stage_b_issue(vsbd_ctx* c, const vsbd_item* items, int n) {
   CK(cudaMemcpyAsync(c->h_out + c->off_fine, c->d_out + c->off_fine, d2h, cudaMemcpyDeviceToHost,
                      st));
   count_d2h(d2h);
-  if (c->pn_on && c->pn_verify)
+  if (fine_narrowed(c) && c->pn_verify)
     CK(cudaMemcpyAsync(c->h_vres + c->nc, c->d_vres + c->nc, sizeof(vsbd_result) * n,
                        cudaMemcpyDeviceToHost, st));
   CK(cudaEventRecord(c->ev_b, st));
@@ -2366,7 +2372,7 @@ extern "C" int vsbd_stage_b_collect(vsbd_ctx* c, const vsbd_result** fine) {
   CK(cudaEventSynchronize(c->ev_b));
   kt_collect(c);
   if (sweep_failed(c, 1)) return -1;
-  if (c->pn_on)
+  if (fine_narrowed(c))
     proposal_tally(c, h + c->off_ffb, (const vsbd_result*)(h + c->off_fine),
                    c->h_vres ? c->h_vres + c->nc : NULL, c->b_n, 1);
   return 0;

@@ -84,6 +84,15 @@ int vsb_frame_end(VSMotionDetect* md);
 /* whether vsb_detect_run_overlapped may serve this detector (no tripod,
    no overlay, a device configuration whose stages share no scratch) */
 int vsb_can_overlap(const VSMotionDetect* md);
+
+/* a serialized proposal network ("VSBP" blob) checked and read; radius,
+   conf_min (NaN) and match_bound below zero take the blob's values */
+typedef struct {
+  const void* params; /* the device-order parameters inside the blob */
+  float scale, radius, conf_min, match_bound;
+} vsb_pnet_settings;
+int vsb_pnet_parse(const void* blob, long bytes, double radius, double conf_min,
+                   double match_bound, vsb_pnet_settings* out);
 long vsb_detect_run_overlapped(VSMotionDetect* md, const uint8_t* frames, long frame_bytes,
                                int linesize, int nframes, int on_device, LocalMotion* rec,
                                long out_cap, int* counts);

@@ -1,0 +1,713 @@
+/*
+ * vsb_pnet_dev.cuh -- device bodies of the learned search proposal: the
+ * network forward of a run of items, the narrowed search of one item and the
+ * global motion prior of a field set.  The single-stream kernels
+ * (vsb_pnet.cu) and the batched persistent kernel (vsb_batch.cu) both call
+ * them, so a batched stream computes exactly what its own detector does.
+ */
+#ifndef VSB_PNET_DEV_CUH
+#define VSB_PNET_DEV_CUH
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "vsb_pnet.h"
+#include "vsb_search.cuh"
+
+typedef __nv_bfloat16 bf16;
+
+__device__ __forceinline__ float bf(bf16 v) { return __bfloat162float(v); }
+
+struct PNPtr {
+  const bf16 *w1, *w2, *w3, *w4, *fc;
+  const float *b1, *b2, *b3, *b4, *bfc;
+};
+
+__host__ __device__ inline PNPtr pn_ptr(const void* p) {
+  const bf16* w = (const bf16*)p;
+  const float* f = (const float*)((const char*)p + PN_F32_OFFSET);
+  PNPtr r;
+  r.w1 = w;
+  r.w2 = w + PN_NW1;
+  r.w3 = w + PN_NW1 + PN_NW;
+  r.w4 = w + PN_NW1 + 2 * PN_NW;
+  r.fc = w + PN_NW1 + 3 * PN_NW;
+  r.b1 = f;
+  r.b2 = f + 32;
+  r.b3 = f + 64;
+  r.b4 = f + 96;
+  r.bfc = f + 128;
+  return r;
+}
+
+/* ------------------------------------------------------------------------ */
+/* crop: 2x2 averages of the 64x64 windows around the item in both planes   */
+/* ------------------------------------------------------------------------ */
+
+/* value of input element (ch, r, c) of item it: bf16((sum4 - 512) / 256) */
+__device__ __forceinline__ bf16 crop_value(const uint8_t* __restrict__ curr,
+                                           const uint8_t* __restrict__ prev, int pitch, int W,
+                                           int H, const vsbd_item& it, int ch, int r, int c) {
+  const uint8_t* img = ch ? prev : curr;
+  const int cx = (ch ? it.x + it.ox : it.x) - 32 + 2 * c;
+  const int cy = (ch ? it.y + it.oy : it.y) - 32 + 2 * r;
+  const int x0 = min(max(cx, 0), W - 1), x1 = min(max(cx + 1, 0), W - 1);
+  const int y0 = min(max(cy, 0), H - 1), y1 = min(max(cy + 1, 0), H - 1);
+  const uint8_t* r0 = img + (size_t)y0 * pitch;
+  const uint8_t* r1 = img + (size_t)y1 * pitch;
+  int s = (int)r0[x0] + (int)r0[x1] + (int)r1[x0] + (int)r1[x1];
+  return __float2bfloat16_rn((float)(s - 512) / 256.0f);
+}
+
+/* ------------------------------------------------------------------------ */
+/* fused inference on the tensor cores                                       */
+/* ------------------------------------------------------------------------ */
+
+/* shared memory map of k_pn_infer (bytes); 32-channel rows are 64 bytes
+   with their four 16-byte chunks XOR-swizzled by bits 1-2 of the row index,
+   so the 8 rows an ldmatrix phase reads fall in distinct bank groups */
+#define PI_SM_W1 0                       /* [32 co][32 k] */
+#define PI_SM_W2 (PI_SM_W1 + 2048)       /* [9*32 (tap,co)][32 ci] */
+#define PI_SM_W3 (PI_SM_W2 + 18432)
+#define PI_SM_W4 (PI_SM_W3 + 18432)
+#define PI_SM_FC (PI_SM_W4 + 18432)      /* [3][512] plain */
+#define PI_SM_B (PI_SM_FC + 3072)        /* f32 [131] */
+#define PI_SM_IN (PI_SM_B + 528)         /* [34][34][2] zero-bordered input */
+#define PI_SM_A1 (PI_SM_IN + 4624)       /* im2col of 512 conv1 pixels [512][32] */
+#define PI_SM_ACT1 (PI_SM_A1 + 32768)    /* [34*34][32] */
+#define PI_SM_ACT2 (PI_SM_ACT1 + 73984)  /* [18*18][32] */
+#define PI_SM_ACT3 (PI_SM_ACT2 + 20736)  /* [10*10][32] */
+#define PI_SM_ACT4 (PI_SM_ACT3 + 6400)   /* f32 [16][32] */
+#define PI_SMEM (PI_SM_ACT4 + 2048)
+#define PI_THREADS 512
+
+__device__ __forceinline__ int swz(int row, int ch) {
+  return (row << 5) | ((((ch >> 3) ^ (row >> 1)) & 3) << 3) | (ch & 7);
+}
+
+__device__ __forceinline__ void ldsm4(uint32_t& r0, uint32_t& r1, uint32_t& r2, uint32_t& r3,
+                                      const bf16* p) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(p);
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+               : "r"(a));
+}
+
+__device__ __forceinline__ void mma_bf16(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2,
+                                         uint32_t a3, uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "{%8,%9}, {%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ uint32_t pack_relu(float a, float b) {
+  __nv_bfloat162 h = __floats2bfloat162_rn(fmaxf(a, 0.f), fmaxf(b, 0.f));
+  return *(uint32_t*)&h;
+}
+
+/* One m-tile (16 output pixels) of a stride-2 32->32 conv against n-tile
+   pairs [np0, np0+NP): A rows from the swizzled input activation (padded
+   width WP); the output pixel of the lane's A row is (oy, ox). */
+template <int NP>
+__device__ __forceinline__ void conv_s2_mtile(const bf16* act, int WP, int oy, int ox,
+                                              const bf16* wsm, int np0, float (&acc)[2 * NP][4],
+                                              int lane) {
+  const int hi = lane >> 4, kq = (lane >> 3) & 1, nr = lane & 7;
+#pragma unroll
+  for (int t = 0; t < 2 * NP; t++) acc[t][0] = acc[t][1] = acc[t][2] = acc[t][3] = 0.f;
+#pragma unroll 1
+  for (int tap = 0; tap < 9; tap++) {
+    const int ky = tap / 3, kx = tap - ky * 3;
+    const int arow = (2 * oy + ky) * WP + 2 * ox + kx;
+#pragma unroll
+    for (int ks = 0; ks < 2; ks++) {
+      uint32_t a0, a1, a2, a3;
+      ldsm4(a0, a1, a2, a3, act + swz(arow, ks * 16 + hi * 8));
+#pragma unroll
+      for (int p = 0; p < NP; p++) {
+        const int wrow = tap * 32 + (2 * (np0 + p) + hi) * 8 + nr;
+        uint32_t b0, b1, b2, b3;
+        ldsm4(b0, b1, b2, b3, wsm + swz(wrow, ks * 16 + kq * 8));
+        mma_bf16(acc[2 * p], a0, a1, a2, a3, b0, b1);
+        mma_bf16(acc[2 * p + 1], a0, a1, a2, a3, b2, b3);
+      }
+    }
+  }
+}
+
+/* Stages the network's weights (swizzled 16-byte chunks) and biases in
+   shared memory and zeroes every bordered activation buffer (the borders
+   are never written again).  Block of PI_THREADS threads. */
+__device__ __forceinline__ void pn_infer_stage(uint8_t* sm, const void* params) {
+  bf16* sW1 = (bf16*)(sm + PI_SM_W1);
+  bf16* sW2 = (bf16*)(sm + PI_SM_W2);
+  bf16* sW3 = (bf16*)(sm + PI_SM_W3);
+  bf16* sW4 = (bf16*)(sm + PI_SM_W4);
+  bf16* sFC = (bf16*)(sm + PI_SM_FC);
+  float* sB = (float*)(sm + PI_SM_B);
+  const int tid = threadIdx.x;
+  const PNPtr P = pn_ptr(params);
+  for (int i = tid; i < 32 * 4; i += PI_THREADS) {
+    const int r = i >> 2, j = i & 3;
+    ((uint4*)sW1)[r * 4 + (j ^ ((r >> 1) & 3))] = ((const uint4*)P.w1)[i];
+  }
+  for (int i = tid; i < 288 * 4; i += PI_THREADS) {
+    const int r = i >> 2, j = i & 3, d = r * 4 + (j ^ ((r >> 1) & 3));
+    ((uint4*)sW2)[d] = ((const uint4*)P.w2)[i];
+    ((uint4*)sW3)[d] = ((const uint4*)P.w3)[i];
+    ((uint4*)sW4)[d] = ((const uint4*)P.w4)[i];
+  }
+  for (int i = tid; i < PN_NFC / 8; i += PI_THREADS) ((uint4*)sFC)[i] = ((const uint4*)P.fc)[i];
+  for (int i = tid; i < PN_NF32; i += PI_THREADS) sB[i] = P.b1[i];
+  for (int i = tid; i < (PI_SM_ACT4 - PI_SM_IN) / 16; i += PI_THREADS)
+    ((uint4*)(sm + PI_SM_IN))[i] = make_uint4(0, 0, 0, 0);
+  __syncthreads();
+}
+
+/* The network on items s0, s0 + ds, ... below n (raw outputs out[s][3]),
+   the weights staged by pn_infer_stage.  Crops are taken from the planes
+   (prepared == NULL) or read from prepared inputs.  Block of PI_THREADS
+   threads (16 warps). */
+__device__ __forceinline__ void pn_infer_items(uint8_t* sm, const uint8_t* __restrict__ curr,
+                                               const uint8_t* __restrict__ prev, int pitch,
+                                               int W, int H,
+                                               const vsbd_item* __restrict__ items,
+                                               const uint32_t* __restrict__ prepared, int s0,
+                                               int n, int ds, float* __restrict__ out) {
+  bf16* sW1 = (bf16*)(sm + PI_SM_W1);
+  bf16* sW2 = (bf16*)(sm + PI_SM_W2);
+  bf16* sW3 = (bf16*)(sm + PI_SM_W3);
+  bf16* sW4 = (bf16*)(sm + PI_SM_W4);
+  bf16* sFC = (bf16*)(sm + PI_SM_FC);
+  float* sB = (float*)(sm + PI_SM_B);
+  uint32_t* sIn = (uint32_t*)(sm + PI_SM_IN); /* one word = the 2 channels of a pixel */
+  bf16* sA1 = (bf16*)(sm + PI_SM_A1);
+  bf16* sAct1 = (bf16*)(sm + PI_SM_ACT1);
+  bf16* sAct2 = (bf16*)(sm + PI_SM_ACT2);
+  bf16* sAct3 = (bf16*)(sm + PI_SM_ACT3);
+  float* sAct4 = (float*)(sm + PI_SM_ACT4);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int hi = lane >> 4, kq = (lane >> 3) & 1, nr = lane & 7;
+  const int arl = (lane & 7) + kq * 8; /* the lane's A row within an m-tile */
+  const int g = lane >> 2, t2 = 2 * (lane & 3); /* accumulator row / column pair */
+
+  for (int s = s0; s < n; s += ds) {
+    /* 1. input planes */
+    if (prepared) {
+      const uint32_t* src = prepared + (size_t)s * 1024;
+      for (int i = tid; i < 1024; i += PI_THREADS) sIn[((i >> 5) + 1) * 34 + (i & 31) + 1] = src[i];
+    } else {
+      const vsbd_item it = items[s];
+      bf16* sInh = (bf16*)sIn;
+      for (int i = tid; i < 2048; i += PI_THREADS) {
+        const int r = i >> 6, c = (i >> 1) & 31, ch = i & 1;
+        sInh[((r + 1) * 34 + c + 1) * 2 + ch] = crop_value(curr, prev, pitch, W, H, it, ch, r, c);
+      }
+    }
+    __syncthreads();
+
+    /* 2. conv1 (stride 1) as an im2col GEMM, 2 chunks of 16 output rows */
+    for (int ck = 0; ck < 2; ck++) {
+      {
+        const int y = ck * 16 + (tid >> 5), x = tid & 31;
+        uint32_t wv[16];
+#pragma unroll
+        for (int tap = 0; tap < 9; tap++) wv[tap] = sIn[(y + tap / 3) * 34 + x + tap % 3];
+#pragma unroll
+        for (int j = 9; j < 16; j++) wv[j] = 0u;
+        uint4* dst = (uint4*)(sA1 + tid * 32);
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+          dst[q ^ ((tid >> 1) & 3)] = make_uint4(wv[4 * q], wv[4 * q + 1], wv[4 * q + 2], wv[4 * q + 3]);
+      }
+      __syncthreads();
+#pragma unroll 1
+      for (int mi = 0; mi < 2; mi++) {
+        const int mt = warp * 2 + mi;
+        float acc[4][4];
+#pragma unroll
+        for (int t = 0; t < 4; t++) acc[t][0] = acc[t][1] = acc[t][2] = acc[t][3] = 0.f;
+#pragma unroll
+        for (int ks = 0; ks < 2; ks++) {
+          uint32_t a0, a1, a2, a3;
+          ldsm4(a0, a1, a2, a3, sA1 + swz(mt * 16 + arl, ks * 16 + hi * 8));
+#pragma unroll
+          for (int p = 0; p < 2; p++) {
+            uint32_t b0, b1, b2, b3;
+            ldsm4(b0, b1, b2, b3, sW1 + swz((2 * p + hi) * 8 + nr, ks * 16 + kq * 8));
+            mma_bf16(acc[2 * p], a0, a1, a2, a3, b0, b1);
+            mma_bf16(acc[2 * p + 1], a0, a1, a2, a3, b2, b3);
+          }
+        }
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const int pl = mt * 16 + g + 8 * h; /* chunk-local pixel */
+          const int row = (ck * 16 + (pl >> 5) + 1) * 34 + (pl & 31) + 1;
+#pragma unroll
+          for (int t = 0; t < 4; t++) {
+            const int ch = t * 8 + t2;
+            *(uint32_t*)(sAct1 + swz(row, ch)) =
+                pack_relu(acc[t][2 * h] + sB[ch], acc[t][2 * h + 1] + sB[ch + 1]);
+          }
+        }
+      }
+      __syncthreads();
+    }
+
+    /* 3. conv2: 16x16 outputs, m-tile = output row, one per warp */
+    {
+      const int oy = warp;
+      float acc[4][4];
+      conv_s2_mtile<2>(sAct1, 34, oy, arl, sW2, 0, acc, lane);
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int row = (oy + 1) * 18 + g + 8 * h + 1;
+#pragma unroll
+        for (int t = 0; t < 4; t++) {
+          const int ch = t * 8 + t2;
+          *(uint32_t*)(sAct2 + swz(row, ch)) =
+              pack_relu(acc[t][2 * h] + sB[32 + ch], acc[t][2 * h + 1] + sB[32 + ch + 1]);
+        }
+      }
+    }
+    __syncthreads();
+
+    /* 4. conv3: 8x8 outputs = 4 m-tiles; warp (< 8): m-tile w/2, n-tiles 2(w&1).. */
+    if (warp < 8) {
+      const int mt = warp >> 1, np0 = warp & 1;
+      const int px = mt * 16 + arl;
+      float acc[2][4];
+      conv_s2_mtile<1>(sAct2, 18, px >> 3, px & 7, sW3, np0, acc, lane);
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int po = mt * 16 + g + 8 * h;
+        const int row = ((po >> 3) + 1) * 10 + (po & 7) + 1;
+#pragma unroll
+        for (int t = 0; t < 2; t++) {
+          const int ch = (2 * np0 + t) * 8 + t2;
+          *(uint32_t*)(sAct3 + swz(row, ch)) =
+              pack_relu(acc[t][2 * h] + sB[64 + ch], acc[t][2 * h + 1] + sB[64 + ch + 1]);
+        }
+      }
+    }
+    __syncthreads();
+
+    /* 5. conv4: 4x4 outputs = 1 m-tile; warps 0 and 1 take two n-tiles each */
+    if (warp < 2) {
+      float acc[2][4];
+      conv_s2_mtile<1>(sAct3, 10, arl >> 2, arl & 3, sW4, warp, acc, lane);
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int po = g + 8 * h;
+#pragma unroll
+        for (int t = 0; t < 2; t++) {
+          const int ch = (2 * warp + t) * 8 + t2;
+#pragma unroll
+          for (int e = 0; e < 2; e++)
+            sAct4[po * 32 + ch + e] = __bfloat162float(
+                __float2bfloat16_rn(fmaxf(acc[t][2 * h + e] + sB[96 + ch + e], 0.f)));
+        }
+      }
+    }
+    __syncthreads();
+
+    /* 6. head */
+    if (warp < 3) {
+      float acc = 0.f;
+      for (int k = lane; k < 512; k += 32) acc = fmaf(sAct4[k], bf(sFC[warp * 512 + k]), acc);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+      if (lane == 0) out[(size_t)s * 3 + warp] = acc + sB[128 + warp];
+    }
+    __syncthreads();
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* narrowed search                                                           */
+/* ------------------------------------------------------------------------ */
+
+/* lattice points per axis the window can hold: the bracket of prediction
+   +- radius (at most ceil(2 radius / step) + 2 points) plus the ring */
+__host__ __device__ inline int narrow_span(float radius, int step) {
+  return (int)ceilf(2.0f * radius / (float)step) + 4;
+}
+
+/* shared-memory layout of k_pn_narrow */
+struct NarrowLayout {
+  int rowW, fieldB, WP, WH, R;
+  size_t off_win, off_q, total;
+};
+
+#define PN_NARROW_QMAX 64 /* candidate sums of one round (lattice window or refinement grid) */
+
+__host__ __device__ inline NarrowLayout narrow_layout(const DGeom& g, float radius) {
+  NarrowLayout L;
+  const int rowB = g.S * g.bpp;
+  L.rowW = rowB >> 2;
+  L.fieldB = ((g.S * rowB) + 15) & ~15;
+  L.R = refine_reach(g);
+  const int span = narrow_span(radius, g.step);
+  const int wwb = rowB + ((span - 1) * g.step + 2 * L.R) * g.bpp;
+  L.WP = (((15 + wwb + 15) >> 4) + 1) << 4;
+  L.WH = g.S + (span - 1) * g.step + 2 * L.R;
+  L.off_win = (size_t)L.fieldB + 16;
+  L.off_q = L.off_win + (size_t)L.WH * L.WP + 16;
+  const int q = g.maxq > PN_NARROW_QMAX ? g.maxq : PN_NARROW_QMAX;
+  L.total = L.off_q + (size_t)q * 4 + 16;
+  return L;
+}
+
+/* One warp's share of a column of NK candidates: displacements (dx, dy0 +
+   k*hy), k < NK, relative to the staged window's origin, summed over field
+   rows [r0, r1).  A lane owns one word of the field row (several rows at
+   once when a row has fewer than 32 words), loads the field word once per
+   row and applies it to every candidate of the column; partial sums are
+   added to sums[k] in shared memory. */
+template <int NK>
+__device__ __forceinline__ void sad_column(const uint32_t* __restrict__ C, int rowW,
+                                           const uint8_t* __restrict__ win, int WP, int e, int bpp,
+                                           int dx, int dy0, int hy, int r0, int r1, int lane,
+                                           unsigned* sums) {
+  unsigned acc[NK];
+#pragma unroll
+  for (int k = 0; k < NK; k++) acc[k] = 0;
+  const int bx = e + dx * bpp;
+  const int sh = (bx & 3) << 3;
+  const int WPw = WP >> 2;
+  const int G = rowW < 32 ? 32 / rowW : 1;
+  const int g = rowW < 32 ? lane / rowW : 0;
+  const int w0 = rowW < 32 ? lane - g * rowW : lane;
+  const int hyw = hy * WPw;
+  if (g < G) {
+    for (int w = w0; w < rowW; w += 32) {
+      const uint32_t* Cw = C + w;
+      const uint32_t* Pw = (const uint32_t*)win + (bx >> 2) + w;
+      for (int r = r0 + g; r < r1; r += G) {
+        const uint32_t c = Cw[r * rowW];
+        const uint32_t* P = Pw + (r + dy0) * WPw;
+#pragma unroll
+        for (int k = 0; k < NK; k++) {
+          const uint32_t* Q = P + k * hyw;
+          acc[k] = sad4(c, __funnelshift_r(Q[0], Q[1], sh), acc[k]);
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < NK; k++) {
+    const unsigned v = __reduce_add_sync(0xffffffffu, acc[k]);
+    if (lane == 0) atomicAdd(&sums[k], v);
+  }
+}
+
+__device__ __forceinline__ void sad_column_n(int nk, const uint32_t* C, int rowW,
+                                             const uint8_t* win, int WP, int e, int bpp, int dx,
+                                             int dy0, int hy, int r0, int r1, int lane,
+                                             unsigned* sums) {
+#define VSB_SADCOL(K) \
+  case K: sad_column<K>(C, rowW, win, WP, e, bpp, dx, dy0, hy, r0, r1, lane, sums); break;
+  switch (nk) {
+    VSB_SADCOL(1) VSB_SADCOL(2) VSB_SADCOL(3) VSB_SADCOL(4)
+    VSB_SADCOL(5) VSB_SADCOL(6) VSB_SADCOL(7) VSB_SADCOL(8)
+    default: break;
+  }
+#undef VSB_SADCOL
+}
+
+/* The SADs of a grid of candidates: columns i < ncol at dx0 + i*hx, rows
+   k < nrow at dy0 + k*hy (window coordinates), into sums[i*nrow + k].  The
+   warps take (column, row chunk of <= 8, field-row strip) tasks. */
+__device__ __forceinline__ void sad_grid(const uint32_t* C, int rowW, int S, const uint8_t* win,
+                                         int WP, int e, int bpp, int dx0, int hx, int ncol,
+                                         int dy0, int hy, int nrow, unsigned* sums) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  for (int q = threadIdx.x; q < ncol * nrow; q += blockDim.x) sums[q] = 0;
+  __syncthreads();
+  const int nch = (nrow + 7) >> 3;
+  const int units = ncol * nch;
+  int strips = nwarps / units;
+  if (strips < 1) strips = 1;
+  const int rs = (S + strips - 1) / strips;
+  for (int t = warp; t < units * strips; t += nwarps) {
+    const int u = t % units, sidx = t / units;
+    const int col = u / nch, ch = u - col * nch;
+    const int k0 = ch * 8, nk = min(8, nrow - k0);
+    const int r0 = sidx * rs, r1 = min(S, r0 + rs);
+    if (r0 < r1)
+      sad_column_n(nk, C, rowW, win, WP, e, bpp, dx0 + col * hx, dy0 + k0 * hy, hy, r0, r1, lane,
+                   sums + col * nrow + k0);
+  }
+  __syncthreads();
+}
+
+/* The narrowed search of one item by the calling CTA (any multiple of 32
+   threads up to 512; sm holds narrow_layout(g, ps.radius).total bytes).
+   The lattice points that bracket the prediction +-
+   radius, plus one ring around them, get their full SAD; the lowest (SAD,
+   rank) is refined exactly as the full search refines its winner
+   (src/motiondetect.c:545-567 of the reference: i outer, j inner, centre
+   skipped, strict <) and range-tested (:573-574).  The window of the
+   previous frame all of this can touch (the candidates plus the refinement
+   reach) is staged once in shared memory with 16-byte loads.  The item
+   falls back to the full search (appended to fb_list) when the confidence
+   is below the threshold, the winner lies on the ring (the minimum may lie
+   further out), or the refined SAD exceeds the bound. */
+__device__ __forceinline__ void pn_narrow_item(uint8_t* sm, const uint8_t* __restrict__ curr,
+                                               const uint8_t* __restrict__ prev, int pitch,
+                                               const DGeom& g, const vsbd_item* __restrict__ items,
+                                               const float* __restrict__ pout,
+                                               const short2* __restrict__ prior,
+                                               const PNSearch& ps,
+                                               const uint8_t* __restrict__ skip,
+                                               vsbd_result* __restrict__ res,
+                                               uint8_t* __restrict__ fb,
+                                               int* __restrict__ fb_count,
+                                               int* __restrict__ fb_list, int item) {
+  __shared__ int s_tx, s_ty;
+  __shared__ unsigned s_min;
+  const NarrowLayout L = narrow_layout(g, ps.radius);
+  const float* po = pout ? pout + item * 3 : NULL;
+  const short2 base = prior ? prior[item] : make_short2(0, 0);
+  const float px = (po ? po[0] * ps.scale : 0.f) + (float)base.x;
+  const float py = (po ? po[1] * ps.scale : 0.f) + (float)base.y;
+  const float cf = po ? po[2] : 3.0e38f;
+  /* the bracket [lo, hi] of lattice indices covering prediction +- radius */
+  int alo = 1, ahi = 0, blo = 1, bhi = 0;
+  if (isfinite(px) && isfinite(py) && fabsf(px) < 30000.f && fabsf(py) < 30000.f) {
+    alo = max((int)floorf((px - ps.radius - g.ax0) / g.step), 0);
+    ahi = min((int)ceilf((px + ps.radius - g.ax0) / g.step), g.na - 1);
+    blo = max((int)floorf((py - ps.radius - g.by0) / g.step), 0);
+    bhi = min((int)ceilf((py + ps.radius - g.by0) / g.step), g.nb - 1);
+  }
+  const int wal = max(alo - 1, 0), wah = min(ahi + 1, g.na - 1);
+  const int wbl = max(blo - 1, 0), wbh = min(bhi + 1, g.nb - 1);
+  const int wa = wah - wal + 1, wb = wbh - wbl + 1;
+  const int span = narrow_span(ps.radius, g.step);
+  const bool unused = skip && skip[item];
+  /* prediction outside the lattice, or a window that would not fit (cannot
+     happen): no narrowed result */
+  if (unused || alo > ahi || blo > bhi || wa > span || wb > span) {
+    if (threadIdx.x == 0) {
+      vsbd_result o;
+      o.sad = 0xffffffffu;
+      o.tx = o.ty = 0;
+      o.ok = 0;
+      res[item] = o;
+      fb[item] = unused ? PN_FB_UNUSED : PN_FB_FULL;
+      if (!unused) fb_list[atomicAdd(fb_count, 1)] = item;
+    }
+    return;
+  }
+  const vsbd_item it = items[item];
+  uint32_t* C = (uint32_t*)sm;
+  uint8_t* win = sm + L.off_win;
+  unsigned* qsad = (unsigned*)(sm + L.off_q);
+  const int fx0 = (it.x - g.S / 2 + it.ox) * g.bpp, fy0 = it.y - g.S / 2 + it.oy;
+  /* window origin: displacement (ax0 + wal*step - R, by0 + wbl*step - R) */
+  const int dx0 = g.ax0 + wal * g.step - L.R, dy0 = g.by0 + wbl * g.step - L.R;
+  const int wx = fx0 + dx0 * g.bpp, wy = fy0 + dy0;
+  const int wxa = wx & ~15, e = wx - wxa;
+  {
+    const int cx0 = (it.x - g.S / 2) * g.bpp, cy0 = it.y - g.S / 2;
+    const int sh = (cx0 & 3) << 3;
+    for (int i = threadIdx.x; i < g.S * L.rowW; i += blockDim.x) {
+      const int r = i / L.rowW, w = i - r * L.rowW;
+      const uint32_t* sw = (const uint32_t*)(curr + (size_t)(cy0 + r) * pitch) + (cx0 >> 2) + w;
+      C[i] = __funnelshift_r(sw[0], sw[1], sh);
+    }
+    const int wwb = g.S * g.bpp + ((wa - 1) * g.step + 2 * L.R) * g.bpp;
+    const int wh = g.S + (wb - 1) * g.step + 2 * L.R;
+    const int nv = (e + wwb + 15) >> 4;
+    for (int i = threadIdx.x; i < wh * nv; i += blockDim.x) {
+      const int r = i / nv, v = i - r * nv;
+      *(uint4*)(win + r * L.WP + (v << 4)) =
+          *(const uint4*)(prev + (size_t)(wy + r) * pitch + wxa + (v << 4));
+    }
+  }
+  __syncthreads();
+  /* lattice window: column a - wal, row b - wbl at sums[(a-wal)*wb + (b-wbl)];
+     the lowest (SAD, visiting rank) by a block-wide reduction */
+  sad_grid(C, L.rowW, g.S, win, L.WP, e, g.bpp, L.R, g.step, wa, L.R, g.step, wb, qsad);
+  {
+    __shared__ unsigned long long red[16];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned long long best = ~0ull;
+    for (int q = threadIdx.x; q < wa * wb; q += blockDim.x) {
+      const int a = wal + q / wb, b = wbl + q % wb;
+      const unsigned long long key =
+          ((unsigned long long)qsad[q] << 32) | (unsigned)g.order[b * g.na + a];
+      best = key < best ? key : best;
+    }
+    best = warp_min64(best);
+    if (lane == 0) red[warp] = best;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int w = 1; w < (int)(blockDim.x >> 5); w++) best = red[w] < best ? red[w] : best;
+      const short2 pt = g.point[(unsigned)(best & 0xffffffffu)];
+      s_min = (unsigned)(best >> 32);
+      s_tx = pt.x;
+      s_ty = pt.y;
+    }
+    __syncthreads();
+  }
+  const int aw = (s_tx - g.ax0) / g.step, bw = (s_ty - g.by0) / g.step;
+  const bool ring = aw < alo || aw > ahi || bw < blo || bw > bhi;
+  /* refinement rounds around the winner, inside the staged window: the
+     side x side grid (centre included, ignored) */
+  for (int st = 0; st < g.nstages; st++) {
+    const int r = g.st_r[st], h = g.st_h[st];
+    const int side = (2 * r) / h + 1;
+    const int cx = s_tx, cy = s_ty;
+    sad_grid(C, L.rowW, g.S, win, L.WP, e, g.bpp, cx - r - dx0, h, side, cy - r - dy0, h, side,
+             qsad);
+    if (threadIdx.x == 0) {
+      unsigned m = s_min;
+      int tx = cx, ty = cy;
+      /* the reference's order: i (x) outer, j (y) inner */
+      for (int ii = 0; ii < side; ii++)
+        for (int jj = 0; jj < side; jj++) {
+          const int i = cx - r + ii * h, j = cy - r + jj * h;
+          if (i == cx && j == cy) continue;
+          if (qsad[ii * side + jj] < m) {
+            m = qsad[ii * side + jj];
+            tx = i;
+            ty = j;
+          }
+        }
+      s_min = m;
+      s_tx = tx;
+      s_ty = ty;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    vsbd_result o;
+    o.sad = s_min;
+    o.tx = (int16_t)s_tx;
+    o.ty = (int16_t)s_ty;
+    o.ok = !(abs(s_tx) >= g.limx || abs(s_ty) >= g.limy);
+    res[item] = o;
+    const bool trust = !ring && cf >= ps.conf_min && o.sad <= ps.sad_bound;
+    fb[item] = trust ? PN_FB_ACCEPT : PN_FB_FULL;
+    if (!trust) fb_list[atomicAdd(fb_count, 1)] = item;
+  }
+}
+
+/* Global motion prior of a frame's coarse items from the first network
+   pass.  Translation: the per-axis median of the confident predictions (the
+   non-skipped items with a finite prediction and a logit >= conf_min; all
+   non-skipped items if fewer than three are confident).  Rotation: the small
+   angle about the frame centre that best fits, in least squares, the
+   predictions within 8 px of that translation.  Every item gets the model's
+   displacement at its centre, rounded: the search offset of its second
+   network pass (items2) and the base of its proposal (prior).  Run by one
+   CTA of 256 to 1024 threads, with the same result for any block size;
+   buf is 4 * PN_PRIOR_MAX floats of its shared memory. */
+#define PN_PRIOR_MAX 1024
+__device__ __forceinline__ void pn_prior_body(float* buf, const vsbd_item* __restrict__ items,
+                                              const float* __restrict__ pout, int n, float scale,
+                                              float conf_min, const uint8_t* __restrict__ skip,
+                                              float cx, float cy, vsbd_item* __restrict__ items2,
+                                              short2* __restrict__ prior) {
+  float* vx = buf;
+  float* vy = buf + PN_PRIOR_MAX;
+  float* jx = buf + 2 * PN_PRIOR_MAX;
+  float* jy = buf + 3 * PN_PRIOR_MAX;
+  __shared__ int m;
+  __shared__ float med[2];
+  __shared__ float sums[2][8];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  /* the usable predictions in item order (warp 0, 32 items per round, so
+     the arrays and every sum below do not depend on scheduling or on the
+     block size) */
+  for (int pass = 0; pass < 2; pass++) {
+    if (warp == 0) {
+      int base = 0;
+      for (int i0 = 0; i0 < n; i0 += 32) {
+        const int i = i0 + lane;
+        float px = 0.f, py = 0.f;
+        bool use = i < n && !(skip && skip[i]);
+        if (use) {
+          px = pout[3 * i] * scale;
+          py = pout[3 * i + 1] * scale;
+          const float c = pout[3 * i + 2];
+          use = isfinite(px) && isfinite(py) && fabsf(px) <= 4096.f && fabsf(py) <= 4096.f &&
+                (pass == 1 || c >= conf_min);
+        }
+        const unsigned ball = __ballot_sync(0xffffffffu, use);
+        const int k = base + __popc(ball & ((1u << lane) - 1u));
+        if (use && k < PN_PRIOR_MAX) {
+          vx[k] = px;
+          vy[k] = py;
+          jx[k] = -((float)items[i].y - cy); /* d(displacement)/d(angle) at the centre */
+          jy[k] = (float)items[i].x - cx;
+        }
+        base += __popc(ball);
+      }
+      if (lane == 0) m = base;
+    }
+    __syncthreads();
+    if (m >= 3 || pass == 1) break;
+    __syncthreads();
+  }
+  const int cnt = min(m, PN_PRIOR_MAX);
+  /* per-axis medians: the element whose rank (ties by index) is cnt/2 */
+  if (tid == 0) med[0] = med[1] = 0.f;
+  __syncthreads();
+  for (int t = tid; t < 2 * cnt; t += blockDim.x) {
+    const int ax = t >= cnt, k = t - ax * cnt;
+    const float* v = ax ? vy : vx;
+    const float x = v[k];
+    int rank = 0;
+    for (int j = 0; j < cnt; j++) rank += v[j] < x || (v[j] == x && j < k);
+    if (rank == cnt / 2) med[ax] = x;
+  }
+  __syncthreads();
+  /* rotation about the centre from the inliers of the translation, summed
+     by the first 256 threads in a fixed order */
+  float num = 0.f, den = 0.f;
+  if (tid < 256)
+    for (int k = tid; k < cnt; k += 256) {
+      const float rx = vx[k] - med[0], ry = vy[k] - med[1];
+      if (fabsf(rx) < 8.f && fabsf(ry) < 8.f) {
+        num += rx * jx[k] + ry * jy[k];
+        den += jx[k] * jx[k] + jy[k] * jy[k];
+      }
+    }
+  for (int o = 16; o > 0; o >>= 1) {
+    num += __shfl_xor_sync(0xffffffffu, num, o);
+    den += __shfl_xor_sync(0xffffffffu, den, o);
+  }
+  if (lane == 0 && warp < 8) {
+    sums[0][warp] = num;
+    sums[1][warp] = den;
+  }
+  __syncthreads();
+  float th = 0.f;
+  {
+    float a = 0.f, b = 0.f;
+    for (int w = 0; w < 8; w++) {
+      a += sums[0][w];
+      b += sums[1][w];
+    }
+    if (b > 0.f) th = fminf(fmaxf(a / b, -0.05f), 0.05f);
+  }
+  for (int i = tid; i < n; i += blockDim.x) {
+    const vsbd_item it = items[i];
+    const float dx = med[0] + th * -((float)it.y - cy), dy = med[1] + th * ((float)it.x - cx);
+    const int ox = (int)rintf(fminf(fmaxf(dx, -4000.f), 4000.f));
+    const int oy = (int)rintf(fminf(fmaxf(dy, -4000.f), 4000.f));
+    vsbd_item o = it;
+    o.ox = (int16_t)ox;
+    o.oy = (int16_t)oy;
+    items2[i] = o;
+    prior[i] = make_short2((short)ox, (short)oy);
+  }
+}
+
+#endif

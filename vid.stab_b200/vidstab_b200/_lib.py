@@ -181,6 +181,10 @@ def lib():
     L.vsb_batch_close_trf.argtypes = [p]
     L.vsb_batch_set_wait_limit.argtypes = [p, C.c_uint, C.c_longlong]
     L.vsb_batch_test_withhold_blur.argtypes = [p, i]
+    L.vsb_batch_set_proposal.restype = i
+    L.vsb_batch_set_proposal.argtypes = [p, p, C.c_long]
+    L.vsb_batch_proposal_stats.restype = i
+    L.vsb_batch_proposal_stats.argtypes = [p, p]
     L.vsb_test_device_alloc.restype = C.c_longlong
     L.vsb_test_device_alloc.argtypes = [i, i]
     L.vsb_boxblur_host.restype = i

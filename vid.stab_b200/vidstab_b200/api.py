@@ -173,6 +173,24 @@ class Batch:
             self.L.vs_vector_del(C.byref(v))
         return out
 
+    def set_proposal(self, blob):
+        """The learned search proposal (VSBP bytes) for every stream, as work
+        items of the same persistent kernel; None: the dense search again."""
+        self._blob = C.create_string_buffer(blob, len(blob)) if blob is not None else None
+        if self.L.vsb_batch_set_proposal(self.h, self._blob, len(blob) if blob else 0) != 0:
+            raise RuntimeError("vsb_batch_set_proposal failed: %s" %
+                               self.L.vsb_last_error().decode())
+
+    def proposal_stats(self):
+        """{searched, fell_back, coarse_searched, coarse_fell_back,
+        fine_searched, fine_fell_back} since set_proposal"""
+        st = (C.c_longlong * 8)()
+        if self.L.vsb_batch_proposal_stats(self.h, st) != 0:
+            raise RuntimeError("vsb_batch_proposal_stats failed")
+        v = [int(x) for x in st]
+        return {"searched": v[0], "fell_back": v[1], "coarse_searched": v[4],
+                "coarse_fell_back": v[5], "fine_searched": v[6], "fine_fell_back": v[7]}
+
     def launches(self):
         return self.L.vsb_batch_launch_count(self.h)
 
