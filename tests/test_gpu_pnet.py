@@ -215,7 +215,8 @@ def test_detector_zero_proposal_consistent():
     plain = V.MotionDetector(w, h, V.PF_YUV420P)
     exp, ec = _run(plain, clip, w, h)
     det = V.MotionDetector(w, h, V.PF_YUV420P)
-    pnet.set_proposal(det, pnet.zero_blob(), verify=True)
+    # fine fields narrowed too (4 px around the coarse model's prediction)
+    pnet.set_proposal(det, pnet.zero_blob(), verify=True, fine_radius=4.0)
     got, gc = _run(det, clip, w, h)
     st = pnet.proposal_stats(det)
     assert st["searched"] > 0 and st["verified"] == st["searched"]

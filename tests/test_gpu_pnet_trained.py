@@ -42,7 +42,8 @@ def clip():
 def test_trained_agreement_1080p(clip):
     exp, ec, _ = _run(clip)
     got, gc, st = _run(clip, pnet.load_blob())
-    assert st["verified"] == st["searched"] > 10000
+    # the coarse fields of 39 searched frames (fine fields take the dense search)
+    assert st["verified"] == st["searched"] > 2000
     assert st["agreement"] >= 0.995, st
     assert _frames_identical(exp, ec, got, gc) >= 0.95 * len(ec)
 

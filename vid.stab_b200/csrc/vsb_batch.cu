@@ -35,6 +35,7 @@
 #include "vsb_batch.h"
 #include "vsb_plan.h"
 #include "vsb_pnet_dev.cuh"
+#include "vsb_pnet_tc.cuh"
 #include "vsb_prefilter.cuh"
 #include "vsb_search.cuh"
 
@@ -176,12 +177,33 @@ __device__ __noinline__ void batch_tile(const uint8_t* __restrict__ cur,
 
 /* The proposal's bodies as called functions (their registers stay their
    own, as with the search tiles). */
+/* tensor memory of a stage-A CTA, allocated at its first network item and
+   released when the CTA leaves the work list */
+struct BTmem {
+  uint64_t mbar;
+  uint32_t taddr, phase;
+  int on;
+};
+
 __device__ __noinline__ void batch_infer(uint8_t* sm, const BStream& S, const vsbd_item* items,
-                                         int chunk, int staged) {
-  if (!staged) pn_infer_stage(sm, S.pn);
+                                         int chunk, int staged, BTmem* tm, unsigned* err) {
+  if (!tm->on) {
+    if (threadIdx.x == 0) {
+      tc_mbar_init(&tm->mbar);
+      tm->phase = 0;
+    }
+    tc_alloc(&tm->taddr);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (threadIdx.x == 0) tm->on = 1;
+  }
+  if (!staged) pn_tc_stage(sm, S.pn);
   const int i0 = chunk * VSB_PN_CHUNK;
   const int i1 = min(S.nc, i0 + VSB_PN_CHUNK);
-  pn_infer_items(sm, S.cur, S.prev, S.pitch, S.W, S.H, items, NULL, i0, i1, 1, S.pout);
+  __syncthreads();
+  pn_tc_items(sm, tm->taddr, tc_saddr(&tm->mbar), &tm->phase, S.cur, S.prev, S.pitch, S.W, S.H,
+              items, NULL, i0, i1, 1, S.pout, err);
 }
 
 __device__ __noinline__ void batch_prior(uint8_t* sm, const BStream& S) {
@@ -241,8 +263,12 @@ __global__ void __launch_bounds__(NT, VSB_BATCH_THREADS / NT) k_batch_t(const BW
   __shared__ int s_w;
   __shared__ int s_wres; /* the network's weights are staged in sm */
   __shared__ DGeom sg;
+  __shared__ BTmem s_tm;
   const int nwork = ctl->nwork;
-  if (threadIdx.x == 0) s_wres = 0;
+  if (threadIdx.x == 0) {
+    s_wres = 0;
+    s_tm.on = 0;
+  }
   for (;;) {
     if (threadIdx.x == 0) s_w = (int)atomicAdd(&ctl->head, 1u);
     __syncthreads();
@@ -296,7 +322,8 @@ __global__ void __launch_bounds__(NT, VSB_BATCH_THREADS / NT) k_batch_t(const BW
           if (it.type == 3 || it.type == 5) {
             const int ready = ok && (it.type == 3 || wait_ge(ctl, &ctl->prior_done[s], 1u));
             if (ready) {
-              batch_infer(sm, S, it.type == 3 ? S.citems : S.citems2, it.a, s_wres);
+              batch_infer(sm, S, it.type == 3 ? S.citems : S.citems2, it.a, s_wres, &s_tm,
+                          &ctl->err);
               keep_w = 1;
             }
             done = it.type == 3 ? &ctl->inf_done[s] : &ctl->inf2_done[s];
@@ -343,6 +370,11 @@ __global__ void __launch_bounds__(NT, VSB_BATCH_THREADS / NT) k_batch_t(const BW
     }
     if (threadIdx.x == 0) s_wres = keep_w;
     __syncthreads();
+  }
+  if (s_tm.on) {
+    tc_fence_before();
+    __syncthreads();
+    tc_dealloc(s_tm.taddr);
   }
   /* the dense search of the items whose proposal was not trusted: tile f of
      the concatenation, stream by stream, of (fallback item x search tile) */
@@ -560,7 +592,7 @@ static size_t kernel_smem(const vsbd_batch* b) {
   }
   if (b->pn_on) {
     /* the network, the prior's arrays, the coarse narrowed searches */
-    if ((size_t)PI_SMEM > m) m = PI_SMEM;
+    if ((size_t)TC_SMEM > m) m = TC_SMEM;
     if (sizeof(float) * 4 * PN_PRIOR_MAX > m) m = sizeof(float) * 4 * PN_PRIOR_MAX;
     for (int s = 0; s < b->n; s++) {
       const size_t t = narrow_smem(b, b->h_streams[s].gc, b->h_streams[s].psc.radius);

@@ -1938,8 +1938,9 @@ extern "C" int vsbd_create(vsbd_ctx** out, int W, int H, int bpp, int blur_size,
     vsbd_destroy(c);
     return -1;
   }
-  CKC(cudaHostAlloc(&c->h_swerr, 2 * sizeof(unsigned), cudaHostAllocMapped));
-  c->h_swerr[0] = c->h_swerr[1] = 0;
+  /* error words: [0] coarse sweep, [1] fine sweep, [2] proposal network */
+  CKC(cudaHostAlloc(&c->h_swerr, 3 * sizeof(unsigned), cudaHostAllocMapped));
+  c->h_swerr[0] = c->h_swerr[1] = c->h_swerr[2] = 0;
   CKC(cudaHostGetDevicePointer((void**)&c->d_swerr, c->h_swerr, 0));
   if (autotune_sweep(c->gc, c->d_buf[0], c->d_buf[1], c->pitch, c->d_citems, nc, c->d_keys,
                      c->d_tickets, (vsbd_result*)(c->d_out + c->off_coarse), c->d_swerr,
@@ -1986,7 +1987,8 @@ static int learned_search(vsbd_ctx* c, const GeomDev& gd, const GeomDev& gfull, 
   if (base == 0 || c->pn_fine_net) {
     pout = c->d_pout + (size_t)3 * base;
     kt_begin(c, VSBD_KT_PNET, st);
-    if (vsbpn_infer(c->d_pn, cur, prv, c->pitch, c->W, c->H, items, NULL, n, pout, st) < 0)
+    if (vsbpn_infer(c->d_pn, cur, prv, c->pitch, c->W, c->H, items, NULL, n, pout,
+                    c->d_swerr + 2, st) < 0)
       return -1;
     c->launches++;
     count_launches(1);
@@ -1996,7 +1998,8 @@ static int learned_search(vsbd_ctx* c, const GeomDev& gd, const GeomDev& gfull, 
          plus the second prediction */
       if (vsbpn_prior(items, pout, n, c->pn.scale, c->pn.conf_min, skip, c->W, c->H, c->d_citems2,
                       c->d_prior, st) < 0 ||
-          vsbpn_infer(c->d_pn, cur, prv, c->pitch, c->W, c->H, c->d_citems2, NULL, n, pout, st) < 0)
+          vsbpn_infer(c->d_pn, cur, prv, c->pitch, c->W, c->H, c->d_citems2, NULL, n, pout,
+                      c->d_swerr + 2, st) < 0)
         return -1;
       prior = c->d_prior;
       c->launches += 2;
@@ -2210,6 +2213,11 @@ static int stage_a_collect(vsbd_ctx* c, const uint8_t** minmax, const vsbd_resul
   CK(cudaEventSynchronize(c->ev_ablk[blk]));
   kt_collect(c);
   if (sweep_failed(c, 0)) return -1;
+  if (c->h_swerr && ((volatile unsigned*)c->h_swerr)[2]) {
+    c->h_swerr[2] = 0;
+    set_msg("proposal network: a wait for the tensor cores gave up");
+    return -1;
+  }
   uint8_t* h = c->h_outs[blk];
   if (search && c->pn_on)
     proposal_tally(c, h + c->off_cfb, (const vsbd_result*)(h + c->off_coarse), c->h_vres, c->nc,

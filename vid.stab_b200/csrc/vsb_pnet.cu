@@ -19,9 +19,10 @@
  *
  * Kernels:
  *   k_pn_infer     the whole network per item, one CTA per item at a time,
- *                  every layer an implicit GEMM on the tensor cores
- *                  (mma m16n8k16 bf16 -> f32) from swizzled shared memory;
- *                  the crop is taken straight from the blurred planes
+ *                  every convolution an implicit GEMM on the fifth-generation
+ *                  tensor cores (tcgen05.mma bf16 -> f32, accumulators in
+ *                  tensor memory, vsb_pnet_tc.cuh); the crop is taken
+ *                  straight from the blurred planes
  *   k_pn_fwd_*     per-layer training forward (fp32 FMA), keeps activations
  *   k_pn_bwd_*     per-layer backward: input gradients and weight gradients
  *                  (fp32, weight gradients folded over the batch by atomics)
@@ -41,19 +42,37 @@
 #include "vsb_search.cuh"
 
 #include "vsb_pnet_dev.cuh"
+#include "vsb_pnet_tc.cuh"
 
 /* grid: up to one CTA per SM, CTAs stride over the items; block PI_THREADS
-   (16 warps) */
+   (16 warps); every layer on the tensor cores (tcgen05, accumulators in
+   tensor memory).  err (may be NULL) is raised when a wait for the tensor
+   cores gave up. */
 static __global__ void __launch_bounds__(PI_THREADS, 1) k_pn_infer(const void* __restrict__ params,
                                                             const uint8_t* __restrict__ curr,
                                                             const uint8_t* __restrict__ prev,
                                                             int pitch, int W, int H,
                                                             const vsbd_item* __restrict__ items,
                                                             const uint32_t* __restrict__ prepared,
-                                                            int n, float* __restrict__ out) {
-  extern __shared__ __align__(16) uint8_t sm[];
-  pn_infer_stage(sm, params);
-  pn_infer_items(sm, curr, prev, pitch, W, H, items, prepared, blockIdx.x, n, gridDim.x, out);
+                                                            int n, float* __restrict__ out,
+                                                            unsigned* err) {
+  extern __shared__ __align__(128) uint8_t sm[];
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t tslot, phase;
+  if (threadIdx.x == 0) {
+    tc_mbar_init(&mbar);
+    phase = 0;
+  }
+  tc_alloc(&tslot);
+  tc_fence_before();
+  pn_tc_stage(sm, params); /* ends with a barrier */
+  tc_fence_after();
+  const uint32_t taddr = tslot;
+  pn_tc_items(sm, taddr, tc_saddr(&mbar), &phase, curr, prev, pitch, W, H, items, prepared,
+              blockIdx.x, n, gridDim.x, out, err);
+  tc_fence_before();
+  __syncthreads();
+  tc_dealloc(taddr);
 }
 
 /* one CTA of 512 threads per item */
@@ -393,12 +412,12 @@ static int sm_count_cached(void) {
 
 int vsbpn_infer(const void* d_params, const uint8_t* curr, const uint8_t* prev, int pitch, int W,
                 int H, const vsbd_item* items, const void* prepared, int n, float* out,
-                cudaStream_t st) {
+                unsigned* err, cudaStream_t st) {
   if (n <= 0) return 0;
-  PCK(pn_ensure_smem((const void*)k_pn_infer, 0, PI_SMEM));
+  PCK(pn_ensure_smem((const void*)k_pn_infer, 0, TC_SMEM));
   const int grid = min(n, sm_count_cached());
-  k_pn_infer<<<grid, PI_THREADS, PI_SMEM, st>>>(d_params, curr, prev, pitch, W, H, items,
-                                         (const uint32_t*)prepared, n, out);
+  k_pn_infer<<<grid, PI_THREADS, TC_SMEM, st>>>(d_params, curr, prev, pitch, W, H, items,
+                                         (const uint32_t*)prepared, n, out, err);
   PCK(cudaGetLastError());
   return 1;
 }
@@ -536,7 +555,7 @@ extern "C" int vsbd_pnet_backward(const void* d_params, const void* d_input, con
 
 extern "C" int vsbd_pnet_infer(const void* d_params, const void* d_input, int n, float* d_out,
                                void* stream) {
-  return vsbpn_infer(d_params, NULL, NULL, 0, 0, 0, NULL, d_input, n, d_out,
+  return vsbpn_infer(d_params, NULL, NULL, 0, 0, 0, NULL, d_input, n, d_out, NULL,
                      (cudaStream_t)stream) < 0 ? -1 : 0;
 }
 
@@ -545,7 +564,7 @@ extern "C" int vsbd_pnet_infer_items(const void* d_params, const uint8_t* d_curr
                                      const void* d_items, int n, float* d_out, void* stream) {
   if (!d_curr || !d_prev || W < 1 || H < 1 || pitch < W) return pn_msg("bad plane arguments");
   return vsbpn_infer(d_params, d_curr, d_prev, pitch, W, H, (const vsbd_item*)d_items, NULL, n,
-                     d_out, (cudaStream_t)stream) < 0 ? -1 : 0;
+                     d_out, NULL, (cudaStream_t)stream) < 0 ? -1 : 0;
 }
 
 extern "C" int vsbd_pnet_crops(const uint8_t* d_curr, const uint8_t* d_prev, int pitch, int W,

@@ -46,10 +46,12 @@ struct PNSearch {
 
 /* network forward for n items: crops taken from the planes (prepared ==
    NULL; items give the centres and offsets) or read from prepared inputs
-   [n][32][32][2] bf16; raw outputs out[n][3].  Returns launches (1) or -1. */
+   [n][32][32][2] bf16; raw outputs out[n][3].  err (device-visible word,
+   may be NULL) is raised when the kernel's bounded wait for the tensor
+   cores gave up.  Returns launches (1) or -1. */
 int vsbpn_infer(const void* d_params, const uint8_t* curr, const uint8_t* prev, int pitch, int W,
                 int H, const vsbd_item* items, const void* prepared, int n, float* out,
-                cudaStream_t st);
+                unsigned* err, cudaStream_t st);
 
 /* narrowed search of n items of field set g: results into res, flags into
    fb (PN_FB_*); skip (may be NULL) marks items never used.  Items that fall

@@ -1,9 +1,10 @@
 /*
  * vsb_pnet_dev.cuh -- device bodies of the learned search proposal: the
- * network forward of a run of items, the narrowed search of one item and the
- * global motion prior of a field set.  The single-stream kernels
- * (vsb_pnet.cu) and the batched persistent kernel (vsb_batch.cu) both call
- * them, so a batched stream computes exactly what its own detector does.
+ * crop of an item, the narrowed search of one item and the global motion
+ * prior of a field set (the network's forward is in vsb_pnet_tc.cuh).  The
+ * single-stream kernels (vsb_pnet.cu) and the batched persistent kernel
+ * (vsb_batch.cu) both call them, so a batched stream computes exactly what
+ * its own detector does.
  */
 #ifndef VSB_PNET_DEV_CUH
 #define VSB_PNET_DEV_CUH
@@ -61,271 +62,8 @@ __device__ __forceinline__ bf16 crop_value(const uint8_t* __restrict__ curr,
   return __float2bfloat16_rn((float)(s - 512) / 256.0f);
 }
 
-/* ------------------------------------------------------------------------ */
-/* fused inference on the tensor cores                                       */
-/* ------------------------------------------------------------------------ */
-
-/* shared memory map of k_pn_infer (bytes); 32-channel rows are 64 bytes
-   with their four 16-byte chunks XOR-swizzled by bits 1-2 of the row index,
-   so the 8 rows an ldmatrix phase reads fall in distinct bank groups */
-#define PI_SM_W1 0                       /* [32 co][32 k] */
-#define PI_SM_W2 (PI_SM_W1 + 2048)       /* [9*32 (tap,co)][32 ci] */
-#define PI_SM_W3 (PI_SM_W2 + 18432)
-#define PI_SM_W4 (PI_SM_W3 + 18432)
-#define PI_SM_FC (PI_SM_W4 + 18432)      /* [3][512] plain */
-#define PI_SM_B (PI_SM_FC + 3072)        /* f32 [131] */
-#define PI_SM_IN (PI_SM_B + 528)         /* [34][34][2] zero-bordered input */
-#define PI_SM_A1 (PI_SM_IN + 4624)       /* im2col of 512 conv1 pixels [512][32] */
-#define PI_SM_ACT1 (PI_SM_A1 + 32768)    /* [34*34][32] */
-#define PI_SM_ACT2 (PI_SM_ACT1 + 73984)  /* [18*18][32] */
-#define PI_SM_ACT3 (PI_SM_ACT2 + 20736)  /* [10*10][32] */
-#define PI_SM_ACT4 (PI_SM_ACT3 + 6400)   /* f32 [16][32] */
-#define PI_SMEM (PI_SM_ACT4 + 2048)
+/* block size of the inference (vsb_pnet_tc.cuh) */
 #define PI_THREADS 512
-
-__device__ __forceinline__ int swz(int row, int ch) {
-  return (row << 5) | ((((ch >> 3) ^ (row >> 1)) & 3) << 3) | (ch & 7);
-}
-
-__device__ __forceinline__ void ldsm4(uint32_t& r0, uint32_t& r1, uint32_t& r2, uint32_t& r3,
-                                      const bf16* p) {
-  const unsigned a = (unsigned)__cvta_generic_to_shared(p);
-  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
-               : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
-               : "r"(a));
-}
-
-__device__ __forceinline__ void mma_bf16(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2,
-                                         uint32_t a3, uint32_t b0, uint32_t b1) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
-      "{%8,%9}, {%0,%1,%2,%3};\n"
-      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
-}
-
-__device__ __forceinline__ uint32_t pack_relu(float a, float b) {
-  __nv_bfloat162 h = __floats2bfloat162_rn(fmaxf(a, 0.f), fmaxf(b, 0.f));
-  return *(uint32_t*)&h;
-}
-
-/* One m-tile (16 output pixels) of a stride-2 32->32 conv against n-tile
-   pairs [np0, np0+NP): A rows from the swizzled input activation (padded
-   width WP); the output pixel of the lane's A row is (oy, ox). */
-template <int NP>
-__device__ __forceinline__ void conv_s2_mtile(const bf16* act, int WP, int oy, int ox,
-                                              const bf16* wsm, int np0, float (&acc)[2 * NP][4],
-                                              int lane) {
-  const int hi = lane >> 4, kq = (lane >> 3) & 1, nr = lane & 7;
-#pragma unroll
-  for (int t = 0; t < 2 * NP; t++) acc[t][0] = acc[t][1] = acc[t][2] = acc[t][3] = 0.f;
-#pragma unroll 1
-  for (int tap = 0; tap < 9; tap++) {
-    const int ky = tap / 3, kx = tap - ky * 3;
-    const int arow = (2 * oy + ky) * WP + 2 * ox + kx;
-#pragma unroll
-    for (int ks = 0; ks < 2; ks++) {
-      uint32_t a0, a1, a2, a3;
-      ldsm4(a0, a1, a2, a3, act + swz(arow, ks * 16 + hi * 8));
-#pragma unroll
-      for (int p = 0; p < NP; p++) {
-        const int wrow = tap * 32 + (2 * (np0 + p) + hi) * 8 + nr;
-        uint32_t b0, b1, b2, b3;
-        ldsm4(b0, b1, b2, b3, wsm + swz(wrow, ks * 16 + kq * 8));
-        mma_bf16(acc[2 * p], a0, a1, a2, a3, b0, b1);
-        mma_bf16(acc[2 * p + 1], a0, a1, a2, a3, b2, b3);
-      }
-    }
-  }
-}
-
-/* Stages the network's weights (swizzled 16-byte chunks) and biases in
-   shared memory and zeroes every bordered activation buffer (the borders
-   are never written again).  Block of PI_THREADS threads. */
-__device__ __forceinline__ void pn_infer_stage(uint8_t* sm, const void* params) {
-  bf16* sW1 = (bf16*)(sm + PI_SM_W1);
-  bf16* sW2 = (bf16*)(sm + PI_SM_W2);
-  bf16* sW3 = (bf16*)(sm + PI_SM_W3);
-  bf16* sW4 = (bf16*)(sm + PI_SM_W4);
-  bf16* sFC = (bf16*)(sm + PI_SM_FC);
-  float* sB = (float*)(sm + PI_SM_B);
-  const int tid = threadIdx.x;
-  const PNPtr P = pn_ptr(params);
-  for (int i = tid; i < 32 * 4; i += PI_THREADS) {
-    const int r = i >> 2, j = i & 3;
-    ((uint4*)sW1)[r * 4 + (j ^ ((r >> 1) & 3))] = ((const uint4*)P.w1)[i];
-  }
-  for (int i = tid; i < 288 * 4; i += PI_THREADS) {
-    const int r = i >> 2, j = i & 3, d = r * 4 + (j ^ ((r >> 1) & 3));
-    ((uint4*)sW2)[d] = ((const uint4*)P.w2)[i];
-    ((uint4*)sW3)[d] = ((const uint4*)P.w3)[i];
-    ((uint4*)sW4)[d] = ((const uint4*)P.w4)[i];
-  }
-  for (int i = tid; i < PN_NFC / 8; i += PI_THREADS) ((uint4*)sFC)[i] = ((const uint4*)P.fc)[i];
-  for (int i = tid; i < PN_NF32; i += PI_THREADS) sB[i] = P.b1[i];
-  for (int i = tid; i < (PI_SM_ACT4 - PI_SM_IN) / 16; i += PI_THREADS)
-    ((uint4*)(sm + PI_SM_IN))[i] = make_uint4(0, 0, 0, 0);
-  __syncthreads();
-}
-
-/* The network on items s0, s0 + ds, ... below n (raw outputs out[s][3]),
-   the weights staged by pn_infer_stage.  Crops are taken from the planes
-   (prepared == NULL) or read from prepared inputs.  Block of PI_THREADS
-   threads (16 warps). */
-__device__ __forceinline__ void pn_infer_items(uint8_t* sm, const uint8_t* __restrict__ curr,
-                                               const uint8_t* __restrict__ prev, int pitch,
-                                               int W, int H,
-                                               const vsbd_item* __restrict__ items,
-                                               const uint32_t* __restrict__ prepared, int s0,
-                                               int n, int ds, float* __restrict__ out) {
-  bf16* sW1 = (bf16*)(sm + PI_SM_W1);
-  bf16* sW2 = (bf16*)(sm + PI_SM_W2);
-  bf16* sW3 = (bf16*)(sm + PI_SM_W3);
-  bf16* sW4 = (bf16*)(sm + PI_SM_W4);
-  bf16* sFC = (bf16*)(sm + PI_SM_FC);
-  float* sB = (float*)(sm + PI_SM_B);
-  uint32_t* sIn = (uint32_t*)(sm + PI_SM_IN); /* one word = the 2 channels of a pixel */
-  bf16* sA1 = (bf16*)(sm + PI_SM_A1);
-  bf16* sAct1 = (bf16*)(sm + PI_SM_ACT1);
-  bf16* sAct2 = (bf16*)(sm + PI_SM_ACT2);
-  bf16* sAct3 = (bf16*)(sm + PI_SM_ACT3);
-  float* sAct4 = (float*)(sm + PI_SM_ACT4);
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int hi = lane >> 4, kq = (lane >> 3) & 1, nr = lane & 7;
-  const int arl = (lane & 7) + kq * 8; /* the lane's A row within an m-tile */
-  const int g = lane >> 2, t2 = 2 * (lane & 3); /* accumulator row / column pair */
-
-  for (int s = s0; s < n; s += ds) {
-    /* 1. input planes */
-    if (prepared) {
-      const uint32_t* src = prepared + (size_t)s * 1024;
-      for (int i = tid; i < 1024; i += PI_THREADS) sIn[((i >> 5) + 1) * 34 + (i & 31) + 1] = src[i];
-    } else {
-      const vsbd_item it = items[s];
-      bf16* sInh = (bf16*)sIn;
-      for (int i = tid; i < 2048; i += PI_THREADS) {
-        const int r = i >> 6, c = (i >> 1) & 31, ch = i & 1;
-        sInh[((r + 1) * 34 + c + 1) * 2 + ch] = crop_value(curr, prev, pitch, W, H, it, ch, r, c);
-      }
-    }
-    __syncthreads();
-
-    /* 2. conv1 (stride 1) as an im2col GEMM, 2 chunks of 16 output rows */
-    for (int ck = 0; ck < 2; ck++) {
-      {
-        const int y = ck * 16 + (tid >> 5), x = tid & 31;
-        uint32_t wv[16];
-#pragma unroll
-        for (int tap = 0; tap < 9; tap++) wv[tap] = sIn[(y + tap / 3) * 34 + x + tap % 3];
-#pragma unroll
-        for (int j = 9; j < 16; j++) wv[j] = 0u;
-        uint4* dst = (uint4*)(sA1 + tid * 32);
-#pragma unroll
-        for (int q = 0; q < 4; q++)
-          dst[q ^ ((tid >> 1) & 3)] = make_uint4(wv[4 * q], wv[4 * q + 1], wv[4 * q + 2], wv[4 * q + 3]);
-      }
-      __syncthreads();
-#pragma unroll 1
-      for (int mi = 0; mi < 2; mi++) {
-        const int mt = warp * 2 + mi;
-        float acc[4][4];
-#pragma unroll
-        for (int t = 0; t < 4; t++) acc[t][0] = acc[t][1] = acc[t][2] = acc[t][3] = 0.f;
-#pragma unroll
-        for (int ks = 0; ks < 2; ks++) {
-          uint32_t a0, a1, a2, a3;
-          ldsm4(a0, a1, a2, a3, sA1 + swz(mt * 16 + arl, ks * 16 + hi * 8));
-#pragma unroll
-          for (int p = 0; p < 2; p++) {
-            uint32_t b0, b1, b2, b3;
-            ldsm4(b0, b1, b2, b3, sW1 + swz((2 * p + hi) * 8 + nr, ks * 16 + kq * 8));
-            mma_bf16(acc[2 * p], a0, a1, a2, a3, b0, b1);
-            mma_bf16(acc[2 * p + 1], a0, a1, a2, a3, b2, b3);
-          }
-        }
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
-          const int pl = mt * 16 + g + 8 * h; /* chunk-local pixel */
-          const int row = (ck * 16 + (pl >> 5) + 1) * 34 + (pl & 31) + 1;
-#pragma unroll
-          for (int t = 0; t < 4; t++) {
-            const int ch = t * 8 + t2;
-            *(uint32_t*)(sAct1 + swz(row, ch)) =
-                pack_relu(acc[t][2 * h] + sB[ch], acc[t][2 * h + 1] + sB[ch + 1]);
-          }
-        }
-      }
-      __syncthreads();
-    }
-
-    /* 3. conv2: 16x16 outputs, m-tile = output row, one per warp */
-    {
-      const int oy = warp;
-      float acc[4][4];
-      conv_s2_mtile<2>(sAct1, 34, oy, arl, sW2, 0, acc, lane);
-#pragma unroll
-      for (int h = 0; h < 2; h++) {
-        const int row = (oy + 1) * 18 + g + 8 * h + 1;
-#pragma unroll
-        for (int t = 0; t < 4; t++) {
-          const int ch = t * 8 + t2;
-          *(uint32_t*)(sAct2 + swz(row, ch)) =
-              pack_relu(acc[t][2 * h] + sB[32 + ch], acc[t][2 * h + 1] + sB[32 + ch + 1]);
-        }
-      }
-    }
-    __syncthreads();
-
-    /* 4. conv3: 8x8 outputs = 4 m-tiles; warp (< 8): m-tile w/2, n-tiles 2(w&1).. */
-    if (warp < 8) {
-      const int mt = warp >> 1, np0 = warp & 1;
-      const int px = mt * 16 + arl;
-      float acc[2][4];
-      conv_s2_mtile<1>(sAct2, 18, px >> 3, px & 7, sW3, np0, acc, lane);
-#pragma unroll
-      for (int h = 0; h < 2; h++) {
-        const int po = mt * 16 + g + 8 * h;
-        const int row = ((po >> 3) + 1) * 10 + (po & 7) + 1;
-#pragma unroll
-        for (int t = 0; t < 2; t++) {
-          const int ch = (2 * np0 + t) * 8 + t2;
-          *(uint32_t*)(sAct3 + swz(row, ch)) =
-              pack_relu(acc[t][2 * h] + sB[64 + ch], acc[t][2 * h + 1] + sB[64 + ch + 1]);
-        }
-      }
-    }
-    __syncthreads();
-
-    /* 5. conv4: 4x4 outputs = 1 m-tile; warps 0 and 1 take two n-tiles each */
-    if (warp < 2) {
-      float acc[2][4];
-      conv_s2_mtile<1>(sAct3, 10, arl >> 2, arl & 3, sW4, warp, acc, lane);
-#pragma unroll
-      for (int h = 0; h < 2; h++) {
-        const int po = g + 8 * h;
-#pragma unroll
-        for (int t = 0; t < 2; t++) {
-          const int ch = (2 * warp + t) * 8 + t2;
-#pragma unroll
-          for (int e = 0; e < 2; e++)
-            sAct4[po * 32 + ch + e] = __bfloat162float(
-                __float2bfloat16_rn(fmaxf(acc[t][2 * h + e] + sB[96 + ch + e], 0.f)));
-        }
-      }
-    }
-    __syncthreads();
-
-    /* 6. head */
-    if (warp < 3) {
-      float acc = 0.f;
-      for (int k = lane; k < 512; k += 32) acc = fmaf(sAct4[k], bf(sFC[warp * 512 + k]), acc);
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-      if (lane == 0) out[(size_t)s * 3 + warp] = acc + sB[128 + warp];
-    }
-    __syncthreads();
-  }
-}
 
 /* ------------------------------------------------------------------------ */
 /* narrowed search                                                           */
