@@ -264,11 +264,36 @@ __device__ __forceinline__ int pn_tc_items(uint8_t* sm, uint32_t taddr, uint32_t
       const uint32_t* src = prepared + (size_t)s * 1024;
       for (int i = tid; i < 1024; i += PI_THREADS) sIn[((i >> 5) + 1) * 34 + (i & 31) + 1] = src[i];
     } else {
+      /* the two 64 x 64 windows, row by row into region R: 80 bytes a row
+         from the 16-byte boundary at or left of the window (raw byte e + j
+         holds column x0 + j, e = x0 mod 16), rows and columns outside the
+         frame clamped as crop_value clamps them; 16-byte loads where the
+         whole row lies inside the frame, bytes elsewhere */
       const vsbd_item it = items[s];
+      uint8_t* raw = sm + TC_R; /* [2 planes][64 rows][80] */
+      const bool vec = (((uintptr_t)curr | (uintptr_t)prev | (uintptr_t)pitch) & 15) == 0;
+      for (int i = tid; i < 2 * 64 * 5; i += PI_THREADS) {
+        const int ch = i / 320, rem = i - ch * 320, r = rem / 5, v = rem - r * 5;
+        const int x0 = (ch ? it.x + it.ox : it.x) - 32;
+        const int y0 = (ch ? it.y + it.oy : it.y) - 32;
+        const uint8_t* row = (ch ? prev : curr) + (size_t)min(max(y0 + r, 0), H - 1) * pitch;
+        const int xa = x0 & ~15;
+        uint8_t* dst = raw + (ch * 64 + r) * 80 + v * 16;
+        if (vec && xa >= 0 && xa + 80 <= W) {
+          *(uint4*)dst = *(const uint4*)(row + xa + v * 16);
+        } else {
+#pragma unroll
+          for (int b = 0; b < 16; b++) dst[b] = row[min(max(xa + v * 16 + b, 0), W - 1)];
+        }
+      }
+      __syncthreads();
       bf16* sInh = (bf16*)sIn;
       for (int i = tid; i < 2048; i += PI_THREADS) {
         const int r = i >> 6, c = (i >> 1) & 31, ch = i & 1;
-        sInh[((r + 1) * 34 + c + 1) * 2 + ch] = crop_value(curr, prev, pitch, W, H, it, ch, r, c);
+        const int x0 = (ch ? it.x + it.ox : it.x) - 32;
+        const uint8_t* q4 = raw + (ch * 64 + 2 * r) * 80 + (x0 & 15) + 2 * c;
+        const int sum = (int)q4[0] + (int)q4[1] + (int)q4[80] + (int)q4[81];
+        sInh[((r + 1) * 34 + c + 1) * 2 + ch] = __float2bfloat16_rn((float)(sum - 512) / 256.0f);
       }
     }
     __syncthreads();
