@@ -60,17 +60,25 @@ def test_overlapped_matches_reference():
         assert np.array_equal(got[k], exp[k]), k
 
 
-def test_overlapped_with_proposal():
+@pytest.mark.parametrize("on_device", [True, False])
+def test_overlapped_with_proposal(on_device):
+    """the learned frame loop, from device and from host frames, and a second
+    run of the same detector that continues its state"""
     w, h, n = 1920, 1080, 12
     clip = S.clip(w, h, n, seed=33, device="cuda")
+    host = clip.cpu().numpy()
     blob = pnet.load_blob()
     a = V.MotionDetector(w, h, V.PF_YUV420P)
     pnet.set_proposal(a, blob)
     exp, ec = _per_frame(a, clip, w, h)
     b = V.MotionDetector(w, h, V.PF_YUV420P)
     pnet.set_proposal(b, blob)
-    got, gc = _run(b, clip.data_ptr(), n, w, h, True)
+    got, gc = _run(b, clip.data_ptr() if on_device else host.ctypes.data, n, w, h, on_device)
     assert np.array_equal(gc, ec) and np.array_equal(got, exp)
+    # a second run of the same detector continues across the lanes
+    got2, gc2 = _run(b, clip.data_ptr() if on_device else host.ctypes.data, n, w, h, on_device)
+    assert ec[0] == 0 and np.array_equal(gc2[1:], ec[1:])
+    assert np.array_equal(got2[gc2[0]:], exp)
 
 
 def test_multi_detectors_equal_their_own_runs():
