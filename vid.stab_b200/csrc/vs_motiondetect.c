@@ -622,23 +622,19 @@ int vsb_frame_host_b(VSMotionDetect* md, const vsbd_result* fres, vsb_frame_work
   md_state* st = state_find(md);
   VSMotionDetectFields* ff = &md->fieldsfine;
   if (w->fine_pass) {
-    LocalMotions motions2;
-    vs_vector_init(&motions2, w->nitems > 0 ? w->nitems : 1);
+    /* the fine motions in item order, kept when their match is at most the
+       coarse motions' trimmed mean (src/motiondetect.c:268-283); each one is
+       built on the stack and only a kept one is allocated */
+    VSArray q = localmotionsGetMatch(&w->coarse);
+    double meanMatch = cleanmean(q.dat, q.len, NULL, NULL);
     for (int m = 0; m < w->nitems; m++) {
       if (!fres[m].ok) continue;
       const contrast_idx* s = &st->sel[st->item_sel[m]];
       LocalMotion lm = make_lm(&ff->fields[s->index], fres[m].tx + st->items[m].ox,
                                fres[m].ty + st->items[m].oy, s->contrast, fres[m].sad);
-      vs_vector_append_dup(&motions2, &lm, sizeof(LocalMotion));
-    }
-    VSArray q = localmotionsGetMatch(&w->coarse);
-    double meanMatch = cleanmean(q.dat, q.len, NULL, NULL);
-    for (int m = 0; m < vs_vector_size(&motions2); m++) {
-      LocalMotion* lm = LMGet(&motions2, m);
-      if (match_at_most(&meanMatch, lm)) vs_vector_append_dup(&w->fine, lm, sizeof(LocalMotion));
+      if (match_at_most(&meanMatch, &lm)) vs_vector_append_dup(&w->fine, &lm, sizeof(LocalMotion));
     }
     vs_array_free(q);
-    vs_vector_del(&motions2);
   }
   if (vsb_oom_count() != w->oom0) {
     /* an allocation through the host's hooks failed: no partial result */
@@ -657,6 +653,37 @@ int vsb_frame_host_b(VSMotionDetect* md, const vsbd_result* fres, vsb_frame_work
   vs_vector_fini(&w->coarse);
   vs_vector_fini(&w->fine);
   return VS_OK;
+}
+
+int vsb_frame_host_b_records(VSMotionDetect* md, const vsbd_result* fres, vsb_frame_work* w,
+                             LocalMotion* rec, long cap) {
+  md_state* st = state_find(md);
+  VSMotionDetectFields* ff = &md->fieldsfine;
+  long n = 0;
+  for (int i = 0; i < vs_vector_size(&w->coarse); i++, n++)
+    if (rec && n < cap) rec[n] = *LMGet(&w->coarse, i);
+  if (w->fine_pass) {
+    VSArray q = localmotionsGetMatch(&w->coarse);
+    double meanMatch = cleanmean(q.dat, q.len, NULL, NULL);
+    for (int m = 0; m < w->nitems; m++) {
+      if (!fres[m].ok) continue;
+      const contrast_idx* s = &st->sel[st->item_sel[m]];
+      LocalMotion lm = make_lm(&ff->fields[s->index], fres[m].tx + st->items[m].ox,
+                               fres[m].ty + st->items[m].oy, s->contrast, fres[m].sad);
+      if (match_at_most(&meanMatch, &lm)) {
+        if (rec && n < cap) rec[n] = lm;
+        n++;
+      }
+    }
+    vs_array_free(q);
+  }
+  const int failed = vsb_oom_count() != w->oom0;
+  vsb_frame_discard(w);
+  if (failed) {
+    vs_log_error(md->conf.modName, "out of memory in frame %i: frame dropped\n", md->frameNum);
+    return -1;
+  }
+  return (int)n;
 }
 
 void vsb_frame_discard(vsb_frame_work* w) {
@@ -870,10 +897,12 @@ long vsb_detect_run_overlapped(VSMotionDetect* md, const uint8_t* frames, long f
       vsb_frame_discard(&w);
       goto fail;
     }
-    LocalMotions lms;
-    if (vsb_frame_host_b(md, fres, &w, &lms) != VS_OK) goto fail;
+    const int nrec = vsb_frame_host_b_records(md, fres, &w, total < out_cap ? rec + total : NULL,
+                                              total < out_cap ? out_cap - total : 0);
+    if (nrec < 0) goto fail;
     if (vsb_frame_end(md)) vsbd_commit_prev(st->dev);
-    total = append_records(&lms, rec, total, out_cap, counts ? counts + k : NULL);
+    if (counts) counts[k] = nrec;
+    total += nrec;
     if (k + 1 < nframes && vsbd_stage_a_next_collect(st->dev, &mm, &cres) != 0) {
       vs_log_error(md->conf.modName, "GPU stage A failed: %s\n", vsbd_error());
       goto fail;
@@ -930,21 +959,26 @@ long vsb_detect_multi_impl(VSMotionDetect** mds, int n, const uint8_t* const* cl
         goto done;
     }
     for (int s = 0; s < n; s++) {
-      LocalMotions lms;
+      int nrec = 0;
       if (search[s]) {
         const vsbd_result* fres = NULL;
         if (vsbd_stage_b_collect(st[s]->dev, &fres) != 0) goto done;
         ok[s] = 0;
-        if (vsb_frame_host_b(mds[s], fres, &w[s], &lms) != VS_OK) {
+        nrec = vsb_frame_host_b_records(mds[s], fres, &w[s], total < out_cap ? rec + total : NULL,
+                                        total < out_cap ? out_cap - total : 0);
+        if (nrec < 0) {
           for (int q = s + 1; q < n; q++)
             if (search[q]) vsbd_stage_b_collect(st[q]->dev, &fres);
           goto done;
         }
-      } else if (vsb_frame_first(mds[s], &lms) != VS_OK) {
-        goto done;
+      } else {
+        LocalMotions lms;
+        if (vsb_frame_first(mds[s], &lms) != VS_OK) goto done;
+        vs_vector_del(&lms);
       }
       if (vsb_frame_end(mds[s])) vsbd_commit_prev(st[s]->dev);
-      total = append_records(&lms, rec, total, out_cap, counts ? counts + (size_t)k * n + s : NULL);
+      if (counts) counts[(size_t)k * n + s] = nrec;
+      total += nrec;
     }
   }
   rc = total;

@@ -78,6 +78,13 @@ int vsb_frame_host_a(VSMotionDetect* md, const uint8_t* mm, const vsbd_result* c
 int vsb_frame_host_b(VSMotionDetect* md, const vsbd_result* fres, vsb_frame_work* w,
                      LocalMotions* motions);
 void vsb_frame_discard(vsb_frame_work* w);
+/* vsb_frame_host_b for a frame loop whose output is a record array: the
+   frame's motions (coarse, then the kept fine ones) written to rec[0 ..)
+   (at most cap of them) without allocating each motion; returns their
+   number, or -1 (nothing valid, the frame to be dropped) if an allocation
+   failed.  The work's vectors are released either way. */
+int vsb_frame_host_b_records(VSMotionDetect* md, const vsbd_result* fres, vsb_frame_work* w,
+                             LocalMotion* rec, long cap);
 int vsb_frame_first(VSMotionDetect* md, LocalMotions* motions);
 int vsb_frame_end(VSMotionDetect* md);
 
