@@ -339,6 +339,34 @@ static long run_overlapped(vsb_batch* b, const uint8_t* const* clips, const long
       return -1;
     }
     int trf_rc = VS_OK;
+    if (!b->trf) {
+      /* no .trf to write: each stream's motions go straight into the
+         record array, without an allocation per motion */
+      for (int s = 0; s < b->n; s++) {
+        const int nrec = vsb_frame_host_b_records(&b->md[s], b->fres[s], &b->w[s],
+                                                  total < cap ? rec + total : NULL,
+                                                  total < cap ? cap - total : 0);
+        if (nrec < 0) {
+          for (int q = s + 1; q < b->n; q++) vsb_frame_discard(&b->w[q]);
+          vsbd_batch_drain(b->dev);
+          return -1;
+        }
+        if (counts) counts[(size_t)k * b->n + s] = nrec;
+        total += nrec;
+      }
+      for (int s = 0; s < b->n; s++)
+        if (vsb_frame_end(&b->md[s])) vsbd_batch_commit(b->dev, s);
+      double t3 = vsb_now_s();
+      prof[3] = t3 - t2;
+      if (k + 1 < nframes && vsbd_batch_stage_a_collect(b->dev) != 0) {
+        vs_log_error("vsb_batch", "GPU stage A failed: %s\n", vsbd_error());
+        vsbd_batch_drain(b->dev);
+        return -1;
+      }
+      prof[0] = vsb_now_s() - t3;
+      vsb_prof_add(prof, b->n);
+      continue;
+    }
     for (int s = 0; s < b->n; s++)
       if (vsb_frame_host_b(&b->md[s], b->fres[s], &b->w[s], &lms[s]) != VS_OK) {
         for (int q = 0; q < s; q++) vs_vector_del(&lms[q]);

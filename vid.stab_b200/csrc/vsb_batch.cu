@@ -216,7 +216,7 @@ __device__ __noinline__ void batch_narrow(uint8_t* sm, const BStream& S, const D
                                           const short2* prior, const PNSearch& ps,
                                           const uint8_t* skip, vsbd_result* res, uint8_t* fb,
                                           unsigned* fbn, int* fbl, int item) {
-  pn_narrow_item(sm, S.cur, S.prev, S.pitch, g, items, pout, prior, ps, skip, res, fb, (int*)fbn,
+  pn_narrow_item<1>(sm, S.cur, S.prev, S.pitch, g, items, pout, prior, ps, skip, res, fb, (int*)fbn,
                  fbl, item);
 }
 

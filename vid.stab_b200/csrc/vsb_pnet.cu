@@ -75,8 +75,11 @@ static __global__ void __launch_bounds__(PI_THREADS, 1) k_pn_infer(const void* _
   tc_dealloc(taddr);
 }
 
-/* one CTA of 512 threads per item */
-static __global__ void __launch_bounds__(512) k_pn_narrow(const uint8_t* __restrict__ curr,
+/* CTAs of 512 threads per item (a cluster of PN_NARROW_CL, each summing a
+   strip of the field rows into the first CTA's shared memory) */
+#define PN_NARROW_CL 4
+static __global__ void __cluster_dims__(PN_NARROW_CL, 1, 1) __launch_bounds__(512)
+    k_pn_narrow(const uint8_t* __restrict__ curr,
                                                           const uint8_t* __restrict__ prev,
                                                           int pitch, DGeom g,
                                                           const vsbd_item* __restrict__ items,
@@ -89,8 +92,8 @@ static __global__ void __launch_bounds__(512) k_pn_narrow(const uint8_t* __restr
                                                           int* __restrict__ fb_count,
                                                           int* __restrict__ fb_list) {
   extern __shared__ __align__(16) uint8_t sm[];
-  pn_narrow_item(sm, curr, prev, pitch, g, items, pout, prior, ps, skip, res, fb, fb_count,
-                 fb_list, blockIdx.x);
+  pn_narrow_item<PN_NARROW_CL>(sm, curr, prev, pitch, g, items, pout, prior, ps, skip, res, fb,
+                               fb_count, fb_list, blockIdx.x / PN_NARROW_CL);
 }
 
 /* one CTA of 256 threads */
@@ -432,8 +435,8 @@ int vsbpn_narrow(const DGeom& g, const uint8_t* curr, const uint8_t* prev, int p
     return pn_msg("proposal radius too large for the narrowed search");
   const size_t smem = narrow_layout(g, ps.radius).total;
   if (smem > 48 * 1024) PCK(pn_ensure_smem((const void*)k_pn_narrow, 1, smem));
-  k_pn_narrow<<<n, 512, smem, st>>>(curr, prev, pitch, g, items, pout, prior, ps, skip, res, fb,
-                                    fb_count, fb_list);
+  k_pn_narrow<<<n * PN_NARROW_CL, 512, smem, st>>>(curr, prev, pitch, g, items, pout, prior, ps,
+                                                   skip, res, fb, fb_count, fb_list);
   PCK(cudaGetLastError());
   return 1;
 }

@@ -9,6 +9,7 @@
 #ifndef VSB_PNET_DEV_CUH
 #define VSB_PNET_DEV_CUH
 
+#include <cooperative_groups.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <math.h>
@@ -18,6 +19,7 @@
 #include "vsb_search.cuh"
 
 typedef __nv_bfloat16 bf16;
+namespace cg = cooperative_groups;
 
 __device__ __forceinline__ float bf(bf16 v) { return __bfloat162float(v); }
 
@@ -77,7 +79,7 @@ __host__ __device__ inline int narrow_span(float radius, int step) {
 
 /* shared-memory layout of k_pn_narrow */
 struct NarrowLayout {
-  int rowW, fieldB, WP, WH, R;
+  int rowW, fieldB, WP, WH, R, nq;
   size_t off_win, off_q, total;
 };
 
@@ -95,8 +97,10 @@ __host__ __device__ inline NarrowLayout narrow_layout(const DGeom& g, float radi
   L.WH = g.S + (span - 1) * g.step + 2 * L.R;
   L.off_win = (size_t)L.fieldB + 16;
   L.off_q = L.off_win + (size_t)L.WH * L.WP + 16;
-  const int q = g.maxq > PN_NARROW_QMAX ? g.maxq : PN_NARROW_QMAX;
-  L.total = L.off_q + (size_t)q * 4 + 16;
+  L.nq = g.maxq > PN_NARROW_QMAX ? g.maxq : PN_NARROW_QMAX;
+  /* three sum buffers: two that the CTAs of a cluster add into by turns,
+     one for the totals read back */
+  L.total = L.off_q + (size_t)3 * L.nq * 4 + 16;
   return L;
 }
 
@@ -157,25 +161,30 @@ __device__ __forceinline__ void sad_column_n(int nk, const uint32_t* C, int rowW
 #undef VSB_SADCOL
 }
 
-/* The SADs of a grid of candidates: columns i < ncol at dx0 + i*hx, rows
-   k < nrow at dy0 + k*hy (window coordinates), into sums[i*nrow + k].  The
-   warps take (column, row chunk of <= 8, field-row strip) tasks. */
-__device__ __forceinline__ void sad_grid(const uint32_t* C, int rowW, int S, const uint8_t* win,
-                                         int WP, int e, int bpp, int dx0, int hx, int ncol,
-                                         int dy0, int hy, int nrow, unsigned* sums) {
+/* The SADs of a grid of candidates over field rows [rlo, rhi): columns
+   i < ncol at dx0 + i*hx, rows k < nrow at dy0 + k*hy (window
+   coordinates), added into sums[i*nrow + k] (zeroed first when `zero`;
+   sums may be another CTA's shared memory).  The warps take (column, row
+   chunk of <= 8, field-row strip) tasks. */
+__device__ __forceinline__ void sad_grid(const uint32_t* C, int rowW, int rlo, int rhi,
+                                         const uint8_t* win, int WP, int e, int bpp, int dx0,
+                                         int hx, int ncol, int dy0, int hy, int nrow,
+                                         unsigned* sums, bool zero) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  for (int q = threadIdx.x; q < ncol * nrow; q += blockDim.x) sums[q] = 0;
-  __syncthreads();
+  if (zero) {
+    for (int q = threadIdx.x; q < ncol * nrow; q += blockDim.x) sums[q] = 0;
+    __syncthreads();
+  }
   const int nch = (nrow + 7) >> 3;
   const int units = ncol * nch;
   int strips = nwarps / units;
   if (strips < 1) strips = 1;
-  const int rs = (S + strips - 1) / strips;
+  const int rs = (rhi - rlo + strips - 1) / strips;
   for (int t = warp; t < units * strips; t += nwarps) {
     const int u = t % units, sidx = t / units;
     const int col = u / nch, ch = u - col * nch;
     const int k0 = ch * 8, nk = min(8, nrow - k0);
-    const int r0 = sidx * rs, r1 = min(S, r0 + rs);
+    const int r0 = rlo + sidx * rs, r1 = min(rhi, r0 + rs);
     if (r0 < r1)
       sad_column_n(nk, C, rowW, win, WP, e, bpp, dx0 + col * hx, dy0 + k0 * hy, hy, r0, r1, lane,
                    sums + col * nrow + k0);
@@ -195,6 +204,7 @@ __device__ __forceinline__ void sad_grid(const uint32_t* C, int rowW, int S, con
    falls back to the full search (appended to fb_list) when the confidence
    is below the threshold, the winner lies on the ring (the minimum may lie
    further out), or the refined SAD exceeds the bound. */
+template <int CL>
 __device__ __forceinline__ void pn_narrow_item(uint8_t* sm, const uint8_t* __restrict__ curr,
                                                const uint8_t* __restrict__ prev, int pitch,
                                                const DGeom& g, const vsbd_item* __restrict__ items,
@@ -229,8 +239,14 @@ __device__ __forceinline__ void pn_narrow_item(uint8_t* sm, const uint8_t* __res
   const bool unused = skip && skip[item];
   /* prediction outside the lattice, or a window that would not fit (cannot
      happen): no narrowed result */
+  /* with CL > 1 the item is shared by a cluster of CL CTAs: CTA `rank`
+     sums field rows [rlo, rhi) of every candidate into rank 0's sums */
+  unsigned rank = 0;
+  if constexpr (CL > 1) rank = cg::this_cluster().block_rank();
+  const int rsz = (g.S + CL - 1) / CL;
+  const int rlo = min(g.S, (int)rank * rsz), rhi = min(g.S, rlo + rsz);
   if (unused || alo > ahi || blo > bhi || wa > span || wb > span) {
-    if (threadIdx.x == 0) {
+    if (threadIdx.x == 0 && rank == 0) {
       vsbd_result o;
       o.sad = 0xffffffffu;
       o.tx = o.ty = 0;
@@ -253,24 +269,48 @@ __device__ __forceinline__ void pn_narrow_item(uint8_t* sm, const uint8_t* __res
   {
     const int cx0 = (it.x - g.S / 2) * g.bpp, cy0 = it.y - g.S / 2;
     const int sh = (cx0 & 3) << 3;
-    for (int i = threadIdx.x; i < g.S * L.rowW; i += blockDim.x) {
+    for (int i = rlo * L.rowW + threadIdx.x; i < rhi * L.rowW; i += blockDim.x) {
       const int r = i / L.rowW, w = i - r * L.rowW;
       const uint32_t* sw = (const uint32_t*)(curr + (size_t)(cy0 + r) * pitch) + (cx0 >> 2) + w;
       C[i] = __funnelshift_r(sw[0], sw[1], sh);
     }
+    /* the window rows the CTA's field rows meet: [rlo, rhi + wh - S) */
     const int wwb = g.S * g.bpp + ((wa - 1) * g.step + 2 * L.R) * g.bpp;
     const int wh = g.S + (wb - 1) * g.step + 2 * L.R;
     const int nv = (e + wwb + 15) >> 4;
-    for (int i = threadIdx.x; i < wh * nv; i += blockDim.x) {
+    const int wr0 = rlo, wr1 = rhi + wh - g.S;
+    for (int i = wr0 * nv + threadIdx.x; i < wr1 * nv; i += blockDim.x) {
       const int r = i / nv, v = i - r * nv;
       *(uint4*)(win + r * L.WP + (v << 4)) =
           *(const uint4*)(prev + (size_t)(wy + r) * pitch + wxa + (v << 4));
     }
   }
   __syncthreads();
+  /* one round of candidate sums: qv = the totals (this CTA's qsad, or the
+     totals read back from rank 0 after the cluster has added into it) */
+  unsigned* qv = qsad;
+  int round = 0;
+  auto sums_round = [&](int dxs, int hx, int ncol, int dys, int hy, int nrow) {
+    if constexpr (CL == 1) {
+      sad_grid(C, L.rowW, 0, g.S, win, L.WP, e, g.bpp, dxs, hx, ncol, dys, hy, nrow, qsad, true);
+    } else {
+      cg::cluster_group cl = cg::this_cluster();
+      unsigned* qb = qsad + (round & 1) * L.nq;
+      if (rank == 0)
+        for (int q = threadIdx.x; q < ncol * nrow; q += blockDim.x) qb[q] = 0;
+      cl.sync();
+      unsigned* qb0 = cl.map_shared_rank(qb, 0);
+      sad_grid(C, L.rowW, rlo, rhi, win, L.WP, e, g.bpp, dxs, hx, ncol, dys, hy, nrow, qb0, false);
+      cl.sync();
+      qv = qsad + 2 * L.nq;
+      for (int q = threadIdx.x; q < ncol * nrow; q += blockDim.x) qv[q] = qb0[q];
+      __syncthreads();
+    }
+    round++;
+  };
   /* lattice window: column a - wal, row b - wbl at sums[(a-wal)*wb + (b-wbl)];
      the lowest (SAD, visiting rank) by a block-wide reduction */
-  sad_grid(C, L.rowW, g.S, win, L.WP, e, g.bpp, L.R, g.step, wa, L.R, g.step, wb, qsad);
+  sums_round(L.R, g.step, wa, L.R, g.step, wb);
   {
     __shared__ unsigned long long red[16];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -278,7 +318,7 @@ __device__ __forceinline__ void pn_narrow_item(uint8_t* sm, const uint8_t* __res
     for (int q = threadIdx.x; q < wa * wb; q += blockDim.x) {
       const int a = wal + q / wb, b = wbl + q % wb;
       const unsigned long long key =
-          ((unsigned long long)qsad[q] << 32) | (unsigned)g.order[b * g.na + a];
+          ((unsigned long long)qv[q] << 32) | (unsigned)g.order[b * g.na + a];
       best = key < best ? key : best;
     }
     best = warp_min64(best);
@@ -301,8 +341,7 @@ __device__ __forceinline__ void pn_narrow_item(uint8_t* sm, const uint8_t* __res
     const int r = g.st_r[st], h = g.st_h[st];
     const int side = (2 * r) / h + 1;
     const int cx = s_tx, cy = s_ty;
-    sad_grid(C, L.rowW, g.S, win, L.WP, e, g.bpp, cx - r - dx0, h, side, cy - r - dy0, h, side,
-             qsad);
+    sums_round(cx - r - dx0, h, side, cy - r - dy0, h, side);
     if (threadIdx.x == 0) {
       unsigned m = s_min;
       int tx = cx, ty = cy;
@@ -311,8 +350,8 @@ __device__ __forceinline__ void pn_narrow_item(uint8_t* sm, const uint8_t* __res
         for (int jj = 0; jj < side; jj++) {
           const int i = cx - r + ii * h, j = cy - r + jj * h;
           if (i == cx && j == cy) continue;
-          if (qsad[ii * side + jj] < m) {
-            m = qsad[ii * side + jj];
+          if (qv[ii * side + jj] < m) {
+            m = qv[ii * side + jj];
             tx = i;
             ty = j;
           }
@@ -323,7 +362,7 @@ __device__ __forceinline__ void pn_narrow_item(uint8_t* sm, const uint8_t* __res
     }
     __syncthreads();
   }
-  if (threadIdx.x == 0) {
+  if (threadIdx.x == 0 && rank == 0) {
     vsbd_result o;
     o.sad = s_min;
     o.tx = (int16_t)s_tx;
@@ -334,6 +373,9 @@ __device__ __forceinline__ void pn_narrow_item(uint8_t* sm, const uint8_t* __res
     fb[item] = trust ? PN_FB_ACCEPT : PN_FB_FULL;
     if (!trust) fb_list[atomicAdd(fb_count, 1)] = item;
   }
+  /* rank 0's shared memory stays until every CTA of the cluster has read
+     its last totals */
+  if constexpr (CL > 1) cg::this_cluster().sync();
 }
 
 /* Global motion prior of a frame's coarse items from the first network
