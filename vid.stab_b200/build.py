@@ -37,7 +37,7 @@ CU = ["vsb_device.cu", "vsb_noalloc.cu", "vsb_batch.cu", "vsb_pnet.cu", "vsb_l2t
 CU_EXTRA = {"vsb_l2t.cu": ["--fmad=false"]}
 
 COMMON_C = ["-std=gnu99", "-O3", "-DNDEBUG", "-fPIC", "-Wall", "-fvisibility=hidden",
-            "-I" + INCLUDE, "-I" + CSRC]
+            "-I" + INCLUDE, "-I" + CSRC, "-I" + os.path.join(CUDA_HOME, "include")]
 REFFP_FLAGS = ["-msse2", "-ffast-math"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC,-fvisibility=hidden", "-I" + INCLUDE, "-I" + CSRC]

@@ -748,7 +748,10 @@ int vsb_detect_common(VSMotionDetect* md, LocalMotions* motions, const uint8_t* 
   const uint8_t* mm = NULL;
   const vsbd_result* cres = NULL;
   double t[5] = { now_s(), 0, 0, 0, 0 };
-  if (vsbd_stage_a(st->dev, host, linesize, dev, pitch, search, &mm, &cres) != 0) {
+  VSB_RANGE("vsb device stage A");
+  const int rca = vsbd_stage_a(st->dev, host, linesize, dev, pitch, search, &mm, &cres);
+  VSB_RANGE_END();
+  if (rca != 0) {
     vs_log_error(md->conf.modName, "GPU stage A failed: %s\n", vsbd_error());
     return VS_ERROR;
   }
@@ -756,16 +759,24 @@ int vsb_detect_common(VSMotionDetect* md, LocalMotions* motions, const uint8_t* 
   t[2] = t[3] = t[1];
   if (search) {
     vsb_frame_work w;
+    VSB_RANGE("vsb host part A");
     vsb_frame_host_a(md, mm, cres, &w);
+    VSB_RANGE_END();
     t[2] = now_s();
     const vsbd_result* fres = NULL;
-    if (w.fine_pass && vsbd_stage_b(st->dev, w.items, w.nitems, &fres) != 0) {
+    VSB_RANGE("vsb device stage B");
+    const int rcb = w.fine_pass ? vsbd_stage_b(st->dev, w.items, w.nitems, &fres) : 0;
+    VSB_RANGE_END();
+    if (rcb != 0) {
       vs_log_error(md->conf.modName, "GPU stage B failed: %s\n", vsbd_error());
       vsb_frame_discard(&w);
       return VS_ERROR;
     }
     t[3] = now_s();
-    if (vsb_frame_host_b(md, fres, &w, motions) != VS_OK) return VS_ERROR;
+    VSB_RANGE("vsb host part B");
+    const int rch = vsb_frame_host_b(md, fres, &w, motions);
+    VSB_RANGE_END();
+    if (rch != VS_OK) return VS_ERROR;
   } else if (vsb_frame_first(md, motions) != VS_OK) {
     return VS_ERROR;
   }
@@ -875,7 +886,9 @@ long vsb_detect_run_overlapped(VSMotionDetect* md, const uint8_t* frames, long f
     int search = 0;
     if (vsb_frame_begin(md, &search) != VS_OK || !search) goto fail;
     vsb_frame_work w;
+    VSB_RANGE("vsb host part A");
     vsb_frame_host_a(md, mm, cres, &w);
+    VSB_RANGE_END();
     if (vsbd_stage_b_issue(st->dev, w.items, w.fine_pass ? w.nitems : 0) != 0) {
       vs_log_error(md->conf.modName, "GPU stage B failed: %s\n", vsbd_error());
       vsb_frame_discard(&w);
@@ -897,8 +910,10 @@ long vsb_detect_run_overlapped(VSMotionDetect* md, const uint8_t* frames, long f
       vsb_frame_discard(&w);
       goto fail;
     }
+    VSB_RANGE("vsb host part B");
     const int nrec = vsb_frame_host_b_records(md, fres, &w, total < out_cap ? rec + total : NULL,
                                               total < out_cap ? out_cap - total : 0);
+    VSB_RANGE_END();
     if (nrec < 0) goto fail;
     if (vsb_frame_end(md)) vsbd_commit_prev(st->dev);
     if (counts) counts[k] = nrec;

@@ -92,6 +92,13 @@ int vsb_frame_end(VSMotionDetect* md);
    no overlay, a device configuration whose stages share no scratch) */
 int vsb_can_overlap(const VSMotionDetect* md);
 
+/* NVTX ranges around the per-frame stages (header-only NVTX: no cost
+   unless a profiler is attached), so a profile of any host program shows
+   device stage A, host part A, device stage B and host part B by name */
+#include <nvtx3/nvToolsExt.h>
+#define VSB_RANGE(name) nvtxRangePushA(name)
+#define VSB_RANGE_END() nvtxRangePop()
+
 /* a serialized proposal network ("VSBP" blob) checked and read; radius,
    conf_min (NaN) and match_bound below zero take the blob's values */
 typedef struct {
