@@ -38,6 +38,7 @@
 #include "vsb_pnet_tc.cuh"
 #include "vsb_prefilter.cuh"
 #include "vsb_search.cuh"
+#include "vsb_finewarp.cuh"
 
 #define VSB_BATCH_THREADS 512
 /* stage B (fine search only) runs the same kernel with 256-thread CTAs, two
@@ -80,6 +81,7 @@ struct BStream {
   double thr;             /* contrast threshold of the coarse fields */
   PNSearch psc, psf;      /* narrowed-search settings of coarse and fine fields */
   int fnarrow;            /* fine fields take the narrowed search (else the dense one) */
+  int ffine;              /* the dense fine search runs one CTA per field (k_fine's body) */
   int passes;             /* network passes over the coarse fields (1 or 2) */
   int nchunk;             /* network items (VSB_PN_CHUNK coarse fields each) */
 };
@@ -218,6 +220,15 @@ __device__ __noinline__ void batch_narrow(uint8_t* sm, const BStream& S, const D
                                           unsigned* fbn, int* fbl, int item) {
   pn_narrow_item<1>(sm, S.cur, S.prev, S.pitch, g, items, pout, prior, ps, skip, res, fb, (int*)fbn,
                  fbl, item);
+}
+
+/* The dense search of one fine field by the CTA (k_fine's body, one
+   lattice row per thread, no strips). */
+__device__ __noinline__ void batch_fine(uint8_t* sm, const BStream& S, const DGeom& g,
+                                        const vsbd_item* items, int item) {
+  if (g.S == 16) fine_item<16, 1>(sm, S.cur, S.prev, S.pitch, g, items, S.fres, 1, item);
+  else if (g.S == 32) fine_item<32, 1>(sm, S.cur, S.prev, S.pitch, g, items, S.fres, 1, item);
+  else fine_item<48, 1>(sm, S.cur, S.prev, S.pitch, g, items, S.fres, 1, item);
 }
 
 __device__ __forceinline__ void search_tile(const BStream& S, const DGeom* geoms, int cls,
@@ -361,6 +372,10 @@ __global__ void __launch_bounds__(NT, VSB_BATCH_THREADS / NT) k_batch_t(const BW
         batch_narrow(sm, S, sg, fitems + item_off[lo], NULL, NULL, S.psf, NULL, S.fres, S.ffb,
                      &ctl->fbn[lo], S.ffl, local);
         signal_done(&ctl->narrow_done);
+      } else if (S.ffine) {
+        if (threadIdx.x == 0) sg = geoms[S.gf];
+        __syncthreads();
+        batch_fine(sm, S, sg, fitems + item_off[lo], local);
       } else {
         const DGeom* gp = &geoms[S.gf];
         const int ntiles = gp->nta * gp->ntb;
@@ -623,6 +638,11 @@ static int set_grid_b(vsbd_batch* b) {
   for (int k = 0; k < b->ncls; k++)
     if (b->cls_nt[k] == VSB_BATCH_THREADS_B && tile_layout(b->cls[k].g).total > m)
       m = tile_layout(b->cls[k].g).total;
+  for (int s = 0; s < b->n; s++)
+    if (b->h_streams[s].ffine) {
+      const size_t t = fw_layout(b->cls[b->h_streams[s].gf].g, VSB_BATCH_THREADS_B, 1, 1).total;
+      if (t > m) m = t;
+    }
   if (b->pn_on)
     for (int s = 0; s < b->n; s++) {
       if (!b->h_streams[s].fnarrow) continue;
@@ -1144,6 +1164,15 @@ extern "C" int vsbd_batch_create(vsbd_batch** out, int n, const vsbd_batch_strea
       if (rc != 0) FAILB();
     }
   }
+  /* fine fields of the geometries k_fine takes: one CTA per field in stage
+     B (VSB_BATCH_FINE_TILES: the tiles of the tuned tiling instead) */
+  for (int s = 0; s < n; s++) {
+    BStream& S = b->h_streams[s];
+    const DGeom& g = b->cls[S.gf].g;
+    S.ffine = !getenv("VSB_BATCH_FINE_TILES") && fw_supported(g) &&
+              fw_layout(g, VSB_BATCH_THREADS_B, 1, 1).total + b->static_smem + 64 <=
+                  (size_t)b->optin;
+  }
   if (set_grid(b) != 0 || set_grid_b(b) != 0 || upload_geoms(b) != 0) FAILB();
   BWork* w = NULL;
   if (build_workA(b, &w, &b->nworkA, -1, 0) != 0) FAILB();
@@ -1321,7 +1350,7 @@ extern "C" int vsbd_batch_stage_b_issue(vsbd_batch* b, const vsbd_item* const* i
     nit += ni;
     /* one narrowed search per item with a narrowed fine stage, else the
        item's search tiles */
-    total += S.fnarrow ? ni : ni * g.nta * g.ntb;
+    total += S.fnarrow || S.ffine ? ni : ni * g.nta * g.ntb;
   }
   pre[b->n] = total;
   b->h_nwork[0] = total;

@@ -125,20 +125,18 @@ __device__ __forceinline__ void fw_sums(const uint32_t* __restrict__ F, const ui
   }
 }
 
-/* One CTA (blockDim.x = 32 * warps) per item of items[0 .. n); a thread
-   takes 8 lattice columns x T lattice rows x one of ns strips of the field
-   rows (the strips' partial sums are added in shared memory). */
+/* The search of item `item` by the calling CTA (blockDim.x = 32 * warps,
+   sm holding fw_layout(g, blockDim.x, T, ns).total bytes); a thread takes
+   8 lattice columns x T lattice rows x one of ns strips of the field rows
+   (the strips' partial sums are added in shared memory). */
 template <int S, int T>
-__global__ void __launch_bounds__(FW_MAX_WARPS * 32) k_fine(const uint8_t* __restrict__ curr,
-                                                          const uint8_t* __restrict__ prev,
-                                                          int pitch, DGeom g,
-                                                          const vsbd_item* __restrict__ items,
-                                                          vsbd_result* __restrict__ res, int ns) {
-  extern __shared__ __align__(16) uint8_t sm[];
+__device__ __forceinline__ void fine_item(uint8_t* sm, const uint8_t* __restrict__ curr,
+                                          const uint8_t* __restrict__ prev, int pitch,
+                                          const DGeom& g, const vsbd_item* __restrict__ items,
+                                          vsbd_result* __restrict__ res, int ns, int item) {
   __shared__ int s_tx, s_ty;
   __shared__ unsigned s_min;
   constexpr int NW = S / 4;
-  const int item = blockIdx.x;
   const int nt = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const FWLayout L = fw_layout(g, nt, T, ns);
   const int R = refine_reach(g);
@@ -305,6 +303,17 @@ __global__ void __launch_bounds__(FW_MAX_WARPS * 32) k_fine(const uint8_t* __res
     o.ok = !(abs(s_tx) >= g.limx || abs(s_ty) >= g.limy);
     res[item] = o;
   }
+}
+
+/* One CTA (blockDim.x = 32 * warps) per item of items[0 .. n). */
+template <int S, int T>
+__global__ void __launch_bounds__(FW_MAX_WARPS * 32) k_fine(const uint8_t* __restrict__ curr,
+                                                          const uint8_t* __restrict__ prev,
+                                                          int pitch, DGeom g,
+                                                          const vsbd_item* __restrict__ items,
+                                                          vsbd_result* __restrict__ res, int ns) {
+  extern __shared__ __align__(16) uint8_t sm[];
+  fine_item<S, T>(sm, curr, prev, pitch, g, items, res, ns, blockIdx.x);
 }
 
 #endif
