@@ -1344,9 +1344,13 @@ static int autotune_fine_warp(const GeomDev& gd, const DGeom* swplan, int sw_on,
   const float base = time_of(0, 1, 1);
   int best_w = 0, best_t = 1, best_ns = 1;
   float best_ms = base > 0.f ? base : 3.0e38f;
+  /* warp counts between the powers of two too: 6 warps fit 165 tasks (33
+     lattice rows x 5 column groups) better than 8 */
+  static const int kwarps[] = { 1, 2, 4, 6, 8, 10, 12, 16 };
   for (int T = 1; T <= 2; T *= 2)
     for (int ns = 1; ns <= 4; ns *= 2)
-      for (int warps = 1; warps <= FW_MAX_WARPS; warps *= 2) {
+      for (int wi = 0; wi < (int)(sizeof(kwarps) / sizeof(kwarps[0])); wi++) {
+        const int warps = kwarps[wi];
         /* at least a third of the threads have a task */
         if (32 * warps > 3 * fw_tasks(g, T, ns) + 32) continue;
         const float ms = time_of(warps, T, ns);
