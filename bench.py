@@ -25,9 +25,16 @@ shakiness 5, mincontrast 0.25).  One step = the detect pass over the whole clip.
 * batched: 64 concurrent streams of mixed resolution through one batch,
   aggregate frames/s, against the same streams through single-stream
   detectors one after another;
-* large_shake_4k: 16 streams of 4K with large camera steps through
-  learned-proposal detectors stepped together, against the plain batch and
-  plain detectors stepped together; field agreement.
+* large_shake_4k: 16 streams of 4K with large camera steps through the
+  learned proposal inside the batched persistent kernel, against the plain
+  batch, and learned and plain detectors stepped together; field agreement
+  with the exact search, record by record;
+* per_frame: vsMotionDetection once per frame from pinned host frames (the
+  drop-in's call sequence);
+* pruned_search: the exact pruned strategy on the clip in HBM, checked
+  against the reference;
+* second_pass: vsLocalmotions2Transforms' per-frame fit over the clip's
+  motions, against the reference's.
 
 With --gpus N (torchrun), every rank runs an independent clip (seed + rank):
 no data moves between GPUs; the time is the max over ranks.
