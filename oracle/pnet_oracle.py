@@ -6,7 +6,7 @@ leg use it.  The product computes everything here in CUDA
 
 The network has no counterpart in the reference; it narrows the reference's
 per-field search (src/motiondetect.c:439-586), whose exact result stays the
-judge.  The semantics restated here, in float64 with the GPU's storage
+arbiter.  The semantics restated here, in float64 with the GPU's storage
 roundings (bf16 round-to-nearest-even of inputs, weights and stored
 activations), are:
 
